@@ -1,0 +1,369 @@
+"""Benchmark of the fiber3d hot path on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload stresslet_sphere|oseen_fibers]
+
+Default workload ``stresslet_sphere`` (the double-layer sum on a spherical
+periphery): 12000 Fibonacci-sphere nodes of radius 10 (outward normals, equal
+weights 4 pi R^2/N, density N(0,1) times the weight) summed onto the 12000
+nodes themselves (pair j == i skipped, as in
+stresslet_kernel_times_normal_times_density_numba) and onto 4096 points
+uniform in a ball of radius 9 (stresslet_kernel_source_target_numba): one
+step = 12000*11999 + 12000*4096 = 193,140,000 pair interactions, FP64.
+
+Metric: Stokes pair interactions per second (whole job; N GPUs run N
+replicas — the workload does not shard on one node in this tier).
+``value`` is measured with inputs resident in HBM, one CUDA-event pair per
+step on the launching stream, L2 flushed (256 MiB write) between steps
+outside the event pairs.  ``e2e`` is the same metric through the drop-in
+Python API (fiber3d_b200.kernels) from pinned host buffers, host<->device
+copies inside the timed region.  ``--impl reference`` times fiber3d's CPU
+algorithm for the same workload (the C/OpenMP restatement in oracle/) on
+the host cores, on a bounded sample of targets.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+FLOP_PER_PAIR = {"stresslet": 29, "oseen": 28, "rotlet": 25}
+L2_FLUSH_BYTES = 256 << 20
+
+
+# ------------------------------------------------------------------ setup --
+def dist_info():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def make_workload(name: str):
+    from fiber3d_b200 import geometry
+    if name == "stresslet_sphere":
+        nodes, normals, w, mu, vol = geometry.stresslet_sphere_workload(seed=2)
+        q = mu * w[:, None]
+        n = nodes.shape[0]
+        targets = np.concatenate([nodes, vol])
+        grp_t = np.concatenate([np.arange(n), -np.ones(vol.shape[0])]).astype(np.int32)
+        grp_s = np.arange(n, dtype=np.int32)
+        pairs = n * (n - 1) + n * vol.shape[0]
+        return dict(kind="stresslet", src=nodes, trg=targets, dens=q, nrm=normals, gs=grp_s,
+                    gt=grp_t, pairs=pairs, nodes=nodes, vol=vol,
+                    desc="stresslet double layer, 12000-node sphere R=10 -> 12000 nodes "
+                         "(j==i skipped) + 4096 ball points R=9, FP64")
+    if name == "oseen_fibers":
+        x, f = geometry.oseen_fiber_workload(seed=1)
+        n = x.shape[0]
+        grp = np.arange(n, dtype=np.int32)
+        return dict(kind="oseen", src=x, trg=x, dens=f, nrm=None, gs=grp, gt=grp,
+                    pairs=n * (n - 1), nodes=x, vol=None,
+                    desc="Oseen sum, 32 straight fibers x 32 Chebyshev-Lobatto nodes, "
+                         "j==i skipped, FP64")
+    raise SystemExit(f"unknown workload {name}")
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle sampling during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = Path(os.environ.get("TMPDIR", "/tmp")) / f"f3d_clocks_{os.getpid()}.csv"
+
+    def __enter__(self):
+        try:
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=self.fh, stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+            self.fh.close()
+
+    def summary(self):
+        if self.proc is None or not self.path.exists():
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.path.read_text().splitlines():
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        self.path.unlink(missing_ok=True)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(smax), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# -------------------------------------------------------------- GPU arm ---
+def measured_peak(L, precision: str, torch):
+    """FMA throughput (FLOP/s) of this GPU from the library's probe kernel."""
+    import ctypes
+    sink = torch.zeros(1, dtype=torch.float64, device="cuda")
+    flops = ctypes.c_double(0)
+    st = L.stream_handle()
+    prec = L.PRECISION[precision]
+    for _ in range(2):
+        L.call("f3d_probe_fma", prec, 4096, L.ptr(sink), ctypes.byref(flops), st)
+    torch.cuda.synchronize()
+    best = 0.0
+    for _ in range(5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        L.call("f3d_probe_fma", prec, 4096, L.ptr(sink), ctypes.byref(flops), st)
+        e1.record()
+        e1.synchronize()
+        best = max(best, flops.value / (e0.elapsed_time(e1) * 1e-3))
+    return best
+
+
+def gpu_arm(args, rank, world, local):
+    import torch
+    import torch.distributed as dist
+    from fiber3d_b200 import _lib as L
+    from fiber3d_b200 import kernels as K
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    wl = make_workload(args.workload)
+    kind = wl["kind"]
+    to = lambda a, dt=torch.float64: torch.as_tensor(a, dtype=dt, device=dev).contiguous()
+    src, trg, dens = to(wl["src"]), to(wl["trg"]), to(wl["dens"])
+    nrm = to(wl["nrm"]) if wl["nrm"] is not None else None
+    gs, gt = to(wl["gs"], torch.int32), to(wl["gt"], torch.int32)
+    out = torch.empty(trg.numel(), dtype=torch.float64, device=dev)
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=dev)
+
+    def step(precision="fp64"):
+        K.pair_sum(kind, src, trg, dens, nrm, self_mode="skip_group", src_group=gs, trg_group=gt,
+                   precision=precision, out=out)
+
+    def timed(precision, steps, warmup):
+        for _ in range(warmup):
+            step(precision)
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        evs = []
+        for _ in range(steps):
+            flush.fill_(1)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            step(precision)
+            e1.record()
+            evs.append((e0, e1))
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        times = [a.elapsed_time(b) for a, b in evs]
+        return times
+
+    peak64 = measured_peak(L, "fp64", torch)
+    peak32 = measured_peak(L, "fp32c", torch)
+    with ClockSampler(local) as clk:
+        t_ms = timed("fp64", args.steps, args.warmup)
+    clocks = clk.summary()
+    total_ms = sum(t_ms)
+    if world > 1:
+        t = torch.tensor([total_ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = t.item()
+    ms_step = total_ms / args.steps
+    pairs = wl["pairs"]
+    value = pairs * args.steps * world / (total_ms * 1e-3)
+
+    # FP32-compensated variant of the same step and its error vs FP64
+    step("fp64")
+    ref64 = out.clone()
+    t32 = timed("fp32c", args.steps, args.warmup)
+    err32 = float((out - ref64).abs().max() / ref64.abs().max())
+    ms32 = sum(t32) / len(t32)
+
+    # e2e through the drop-in API from pinned host buffers
+    host = {k: torch.as_tensor(wl[k]).pin_memory() for k in ("nodes", "dens", "nrm", "vol") if wl[k] is not None}
+    h2d = sum(t.numel() * t.element_size() for t in host.values())
+
+    def e2e_step():
+        if kind == "stresslet":
+            a = K.stresslet_kernel_times_normal_times_density_numba(host["nodes"], host["nrm"], host["dens"])
+            b = K.stresslet_kernel_source_target_numba(host["nodes"], host["vol"], host["nrm"], host["dens"])
+            return a.nbytes + b.nbytes
+        a = K.oseen_kernel_times_density_numba(host["nodes"], host["dens"])
+        return a.nbytes
+
+    for _ in range(args.warmup):
+        e2e_step()
+    torch.cuda.synchronize()
+    d2h = 0
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        d2h = e2e_step()
+    e1.record()
+    e1.synchronize()
+    e2e_ms = e0.elapsed_time(e1)
+    if world > 1:
+        t = torch.tensor([e2e_ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = t.item()
+    e2e_value = pairs * args.steps * world / (e2e_ms * 1e-3)
+
+    flop_pair = FLOP_PER_PAIR[kind]
+    achieved = flop_pair * pairs / (min(t_ms) * 1e-3)
+    line = {
+        "metric": "Stokes pair interactions per second (FP64)",
+        "value": value, "unit": "pairs/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+        "config": {"workload": args.workload, "description": wl["desc"], "pairs_per_step": pairs,
+                   "l2": "flushed between steps (256 MiB write, outside the event pairs)",
+                   "parallelism": f"replicas x{world}"},
+        "roofline": {"bound": "fp64", "achieved": achieved / 1e12, "peak": peak64 / 1e12,
+                     "unit": "TFLOP/s", "frac": achieved / peak64, "traffic": None,
+                     "note": f"{flop_pair} algorithmic flop per pair (rsqrt not counted); peak = "
+                             "measured FP64 FMA rate of this GPU (f3d_probe_fma)",
+                     "kernel": f"pair_kernel<{kind}, skip_group, fp64>"},
+        "fp32c": {"value": pairs / (ms32 * 1e-3) * world, "ms_per_step": ms32,
+                  "max_rel_err_vs_fp64": err32, "peak_fp32_tflops": peak32 / 1e12},
+        "e2e": {"value": e2e_value, "unit": "pairs/s", "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h,
+                "path": "fiber3d_b200.kernels drop-in calls from pinned host tensors"},
+        "clocks": clocks,
+        "gpu_launches": args.steps * 1,
+    }
+    if rank == 0 and world == 1:
+        line["cpu_baseline"] = cpu_baseline(wl, seconds=args.cpu_seconds)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+# -------------------------------------------------------------- CPU arm ---
+def cpu_sample_rate(wl, nthreads: int, seconds: float):
+    """Pairs/s of the C/OpenMP restatement of fiber3d's kernel on a prefix of
+    the targets, grown until one sample takes >= 1 s, repeated for ~seconds."""
+    from oracle import pairs_c
+    kind, src, trg, dens, nrm = wl["kind"], wl["src"], wl["trg"], wl["dens"], wl["nrm"]
+    nt = 64
+    while True:
+        t0 = time.perf_counter()
+        pairs_c.pair_sum(kind, src, trg[:nt], dens, nrm, nthreads=nthreads)
+        dt = time.perf_counter() - t0
+        if dt >= 1.0 or nt >= trg.shape[0]:
+            break
+        nt = min(trg.shape[0], nt * 2)
+    reps, best = 0, float("inf")
+    t_start = time.perf_counter()
+    while time.perf_counter() - t_start < seconds or reps == 0:
+        t0 = time.perf_counter()
+        pairs_c.pair_sum(kind, src, trg[:nt], dens, nrm, nthreads=nthreads)
+        best = min(best, time.perf_counter() - t0)
+        reps += 1
+    return nt * src.shape[0] / best, nt, reps
+
+
+def cpu_baseline(wl, seconds: float):
+    from oracle import pairs_c
+    threads = pairs_c.max_threads()
+    rate, nt, reps = cpu_sample_rate(wl, threads, seconds)
+    return {"value": rate, "unit": "pairs/s", "cores": threads, "kind": "port",
+            "sample": f"{nt} of {wl['trg'].shape[0]} targets x {wl['src'].shape[0]} sources, "
+                      f"best of {reps}; C/OpenMP restatement of fiber3d's numba loop"}
+
+
+def reference_arm(args, rank, world):
+    if rank != 0:
+        return
+    from oracle import pairs_c
+    wl = make_workload(args.workload)
+    threads = pairs_c.max_threads()
+    per_step = max(1.0, args.cpu_seconds / max(args.steps, 1))
+    rates = []
+    for _ in range(args.warmup):
+        cpu_sample_rate(wl, threads, 0.0)
+    for _ in range(args.steps):
+        r, nt, _ = cpu_sample_rate(wl, threads, per_step)
+        rates.append(r)
+    value = statistics.median(rates)
+    line = {
+        "impl": "reference",
+        "metric": "Stokes pair interactions per second (FP64)", "value": value, "unit": "pairs/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": wl["pairs"] / value * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+        "config": {"workload": args.workload, "description": wl["desc"],
+                   "pairs_per_step": wl["pairs"], "parallelism": "host cores"},
+        "cpu_baseline": {"value": value, "unit": "pairs/s", "cores": threads, "kind": "port",
+                         "sample": f"{nt} targets x {wl['src'].shape[0]} sources per step sample; "
+                                   "C/OpenMP restatement of fiber3d's numba loop (oracle/)"},
+        "e2e": {"value": value, "unit": "pairs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="stresslet_sphere", choices=["stresslet_sphere", "oseen_fibers"])
+    ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    rank, world, local = dist_info()
+    if args.impl == "reference":
+        reference_arm(args, rank, world)
+        return
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    try:
+        gpu_arm(args, rank, world, local)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

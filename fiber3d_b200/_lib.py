@@ -1,0 +1,156 @@
+"""ctypes binding of ``libfiber3d_b200.so`` (the C ABI in include/fiber3d_b200.h).
+
+The library is loaded from ``fiber3d_b200/_lib/`` (built in-tree by
+``fiber3d_b200.build``).  There is no CPU fallback: if the library or a CUDA
+device is missing, :func:`lib` raises.  Device memory, streams and the
+workspace come from PyTorch; every call goes through the C ABI with plain
+pointers.
+"""
+from __future__ import annotations
+
+import ctypes
+import threading
+from pathlib import Path
+
+import torch
+
+LIBPATH = Path(__file__).resolve().parent / "_lib" / "libfiber3d_b200.so"
+
+# status codes (f3d_status)
+F3D_OK = 0
+F3D_ERR_TIMEOUT = 8
+
+# enums
+KERNEL = {"oseen": 0, "stresslet": 1, "rotlet": 2}
+SELF_MODE = {"regularise": 0, "skip_index": 1, "skip_group": 2}
+PRECISION = {"fp64": 0, "fp32c": 1}
+
+
+class F3DError(RuntimeError):
+    """A C-ABI call returned a non-zero f3d_status."""
+
+    def __init__(self, fn: str, status: int, msg: str):
+        super().__init__(f"{fn}: status {status} ({msg})")
+        self.status = status
+
+
+class PairShape(ctypes.Structure):
+    _fields_ = [("tpt", ctypes.c_int32), ("sl", ctypes.c_int32),
+                ("nsplit", ctypes.c_int32), ("use_tma", ctypes.c_int32)]
+
+
+_lock = threading.Lock()
+_lib = None
+
+_P = ctypes.c_void_p
+_I64 = ctypes.c_int64
+_D = ctypes.c_double
+_I = ctypes.c_int
+_SZ = ctypes.c_size_t
+
+# name -> argtypes; every function returns int (f3d_status) unless listed in _RESTYPE.
+SIGNATURES: dict[str, list] = {
+    "f3d_version": [],
+    "f3d_status_string": [_I],
+    "f3d_get_device_error": [_P],
+    "f3d_probe_fma": [_I, _I, _P, ctypes.POINTER(_D), _P],
+    "f3d_pair_workspace_bytes": [_I, _I, _I64, _I64, ctypes.POINTER(PairShape), ctypes.POINTER(_SZ)],
+    "f3d_pair_sum": [_I, _I, _I, _P, _P, _P, _P, _P, _P, _P, _I64, _I64, _D, _D, _D, _I,
+                     ctypes.POINTER(PairShape), _P, _SZ, _P],
+    "f3d_oseen_source_target": [_P, _P, _P, _P, _I64, _I64, _D, _D, _D, _I, _P, _SZ, _P],
+    "f3d_oseen_times_density": [_P, _P, _P, _I64, _D, _D, _D, _I, _P, _SZ, _P],
+    "f3d_rotlet_source_target": [_P, _P, _P, _P, _I64, _I64, _D, _D, _D, _I, _P, _SZ, _P],
+    "f3d_stresslet_source_target": [_P, _P, _P, _P, _P, _I64, _I64, _D, _D, _D, _I, _P, _SZ, _P],
+    "f3d_stresslet_times_normal_times_density": [_P, _P, _P, _P, _I64, _D, _D, _D, _I, _P, _SZ, _P],
+    "f3d_stresslet_times_normal_dense": [_P, _P, _P, _I64, _I64, _D, _D, _D, _P],
+    "f3d_oseen_tensor_dense": [_P, _P, _I64, _I64, _D, _D, _D, _P],
+    "f3d_oseen_tensor_source_target_dense": [_P, _P, _P, _I64, _I64, _I64, _D, _D, _D, _P],
+    "f3d_complementary_dense": [_P, _P, _I64, _I64, _P],
+}
+_RESTYPE = {"f3d_version": ctypes.c_char_p, "f3d_status_string": ctypes.c_char_p}
+
+
+def load_library(path: Path | str = LIBPATH) -> ctypes.CDLL:
+    """Load the shared library and attach prototypes (no CUDA device needed)."""
+    path = Path(path)
+    if not path.exists():
+        raise ImportError(
+            f"fiber3d_b200 CUDA library not found at {path}; build it with "
+            "`python -m fiber3d_b200.build` (there is no CPU fallback)")
+    dll = ctypes.CDLL(str(path))
+    for name, argtypes in SIGNATURES.items():
+        fn = getattr(dll, name)
+        fn.argtypes = argtypes
+        fn.restype = _RESTYPE.get(name, ctypes.c_int)
+    return dll
+
+
+def lib() -> ctypes.CDLL:
+    """The loaded library; requires a CUDA device (the product path is GPU-only)."""
+    global _lib
+    if _lib is None:
+        with _lock:
+            if _lib is None:
+                if not torch.cuda.is_available():
+                    raise RuntimeError("fiber3d_b200 needs a CUDA device; none is visible "
+                                       "(there is no CPU fallback)")
+                _lib = load_library()
+    return _lib
+
+
+def check(fn: str, status: int) -> None:
+    if status != F3D_OK:
+        msg = lib().f3d_status_string(status).decode()
+        raise F3DError(fn, status, msg)
+
+
+def call(fn: str, *args) -> None:
+    check(fn, getattr(lib(), fn)(*args))
+
+
+def ptr(t: torch.Tensor | None) -> int | None:
+    return None if t is None else t.data_ptr()
+
+
+def stream_handle(device: torch.device | None = None) -> int:
+    return torch.cuda.current_stream(device).cuda_stream
+
+
+class Workspace:
+    """Per-device zero-initialised scratch buffer, grown on demand.
+
+    Kernels that use it return its counter words to zero, so it is zeroed only
+    when (re)allocated, or after a device-side timeout.  Calls that share a
+    workspace must be ordered on one stream.
+    """
+
+    _per_device: dict[int, "Workspace"] = {}
+
+    def __init__(self, device: torch.device):
+        self.device = device
+        self.buf = torch.zeros(0, dtype=torch.uint8, device=device)
+
+    @classmethod
+    def get(cls, device: torch.device) -> "Workspace":
+        idx = device.index if device.index is not None else torch.cuda.current_device()
+        ws = cls._per_device.get(idx)
+        if ws is None:
+            ws = cls(torch.device("cuda", idx))
+            cls._per_device[idx] = ws
+        return ws
+
+    def ensure(self, nbytes: int) -> tuple[int, int]:
+        if nbytes > self.buf.numel():
+            self.buf = torch.zeros(max(nbytes, 2 * self.buf.numel()), dtype=torch.uint8,
+                                   device=self.device)
+        if self.buf.numel() == 0:
+            return 0, 0
+        return self.buf.data_ptr(), self.buf.numel()
+
+    def reset(self) -> None:
+        self.buf.zero_()
+
+
+def device_error(device: torch.device | None = None) -> int:
+    """Read and clear the device error word (F3D_OK or F3D_ERR_TIMEOUT)."""
+    return lib().f3d_get_device_error(stream_handle(device))

@@ -1,0 +1,629 @@
+// All-pairs Stokes sums on sm_100a: Oseen (Stokeslet), stresslet (double
+// layer) and rotlet, source -> target, FP64 or FP32-compensated.
+//
+// Reference semantics (fiber3d python/kernels/kernels.py):
+//   oseen_kernel_source_target_numba            :794-846   (A1)
+//   oseen_kernel_times_density_numba            :214-287   (A2, j == i skipped)
+//   rotlet_kernel_source_target_numba           :856-908   (A6)
+//   stresslet_kernel_times_normal_times_density :1123-1183 (A4, j == i skipped)
+//   stresslet_kernel_source_target_numba        :1186-1217 (A3)
+// r = x_target - x_source.  A pair with |r| < epsilon_distance uses
+// sqrt(|r|^2 + reg^2) in place of |r|.  The prefactor (1/(8 pi eta) or
+// -3/(4 pi eta)) is applied once per target.
+//
+// Design.  One CTA owns TPB = (kBlock / SL) * TPT targets (held in registers)
+// and a contiguous range of source tiles (grid.y = source split).  Source
+// tiles of kTile points are staged in shared memory with 1-D bulk copies
+// (cp.async.bulk, TMA engine) completing on an mbarrier, double buffered, so
+// the copy of tile i+2 overlaps the arithmetic on tile i.  Within a tile a
+// target group of SL lanes strides the sources; lanes are reduced with warp
+// shuffles.  With grid.y > 1 each CTA writes a partial sum to the workspace
+// and the last CTA of a target block (self-resetting counter) adds the
+// partials in split order, so results are deterministic run to run.
+#include <algorithm>
+
+#include "f3d_common.cuh"
+
+namespace f3d {
+
+constexpr int kBlock = 128;  // threads per CTA
+constexpr int kTile = 128;   // sources per staged tile
+
+struct PairArgs {
+  const double *rs, *rt, *dens, *nrm;
+  const float *packed;  // FP32C: [ns][12] packed source records
+  const int32_t *gs, *gt;
+  double *out;
+  double *partial;          // [nsplit][nt][3]
+  unsigned int *counters;   // [gridDim.x], zero on entry, zero on exit
+  int *err;
+  int64_t ns, nt;
+  int64_t tiles_per_split;  // full tiles per split
+  int nsplit;
+  int use_tma;
+  int accumulate;
+  double eps2, reg2, scale;
+};
+
+// Shared-memory layout of one stage.
+template <int KIND, int MODE, int PREC>
+struct Stage {
+  static constexpr bool kNrm = (KIND == F3D_KERNEL_STRESSLET);
+  static constexpr bool kGrp = (MODE == F3D_SELF_SKIP_GROUP);
+  // FP64: pos[3T] dens[3T] (nrm[3T]) (grp[T]);  FP32C: rec[12T] (grp[T])
+  static constexpr size_t off_pos = 0;
+  static constexpr size_t off_dens = 24 * kTile;
+  static constexpr size_t off_nrm = 48 * kTile;
+  static constexpr size_t off_rec = 0;
+  static constexpr size_t data_bytes =
+      (PREC == F3D_FP64) ? (kNrm ? 72 * kTile : 48 * kTile) : 48 * kTile;
+  static constexpr size_t off_grp = data_bytes;
+  static constexpr size_t bytes = ((data_bytes + (kGrp ? 4 * kTile : 0)) + 127) / 128 * 128;
+};
+
+template <int KIND, int MODE, int PREC>
+constexpr size_t pair_smem_bytes() {
+  return 128 + 2 * Stage<KIND, MODE, PREC>::bytes;
+}
+
+__device__ __forceinline__ void two_sum(float &s, float &c, float x) {
+  const float t = s + x;
+  const float bp = t - s;
+  const float e = (s - (t - bp)) + (x - bp);
+  s = t;
+  c += e;
+}
+
+template <int KIND, int MODE, int PREC, int TPT, int SL>
+__global__ void __launch_bounds__(kBlock) pair_kernel(const PairArgs a) {
+  using St = Stage<KIND, MODE, PREC>;
+  constexpr int TG = kBlock / SL;
+  constexpr int TPB = TG * TPT;
+  extern __shared__ __align__(128) unsigned char smem[];
+  uint64_t *bars = reinterpret_cast<uint64_t *>(smem);
+  unsigned char *stages = smem + 128;
+
+  const int tid = threadIdx.x;
+  const int tg = tid / SL;
+  const int sl = tid % SL;
+  const int64_t tb = static_cast<int64_t>(blockIdx.x) * TPB;
+
+  // ---- targets in registers -------------------------------------------
+  double txd[TPT], tyd[TPT], tzd[TPT];
+  float txh[TPT], tyh[TPT], tzh[TPT], txl[TPT], tyl[TPT], tzl[TPT];
+  int32_t tgrp[TPT];
+  int64_t tidx[TPT];
+#pragma unroll
+  for (int k = 0; k < TPT; ++k) {
+    const int64_t t = tb + k * TG + tg;
+    tidx[k] = t;
+    double x = 0.0, y = 0.0, z = 0.0;
+    int32_t g = -1;
+    if (t < a.nt) {
+      x = a.rt[3 * t + 0];
+      y = a.rt[3 * t + 1];
+      z = a.rt[3 * t + 2];
+      if (MODE == F3D_SELF_SKIP_GROUP) g = a.gt[t];
+    }
+    tgrp[k] = g;
+    if (PREC == F3D_FP64) {
+      txd[k] = x; tyd[k] = y; tzd[k] = z;
+    } else {
+      txh[k] = static_cast<float>(x); txl[k] = static_cast<float>(x - static_cast<double>(txh[k]));
+      tyh[k] = static_cast<float>(y); tyl[k] = static_cast<float>(y - static_cast<double>(tyh[k]));
+      tzh[k] = static_cast<float>(z); tzl[k] = static_cast<float>(z - static_cast<double>(tzh[k]));
+    }
+  }
+
+  double acc[TPT][3];
+  float fs[TPT][3], fc[TPT][3], ft[TPT][3];
+#pragma unroll
+  for (int k = 0; k < TPT; ++k)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) { acc[k][c] = 0.0; fs[k][c] = 0.f; fc[k][c] = 0.f; ft[k][c] = 0.f; }
+
+  const double eps2 = a.eps2, reg2 = a.reg2;
+  const float eps2f = static_cast<float>(a.eps2), reg2f = static_cast<float>(a.reg2);
+
+  // ---- one tile of `cnt` sources starting at global index `sbase` --------
+  auto compute_tile = [&](const unsigned char *buf, int cnt, int64_t sbase) {
+    for (int s = sl; s < cnt; s += SL) {
+      if (PREC == F3D_FP64) {
+        const double *pos = reinterpret_cast<const double *>(buf + St::off_pos);
+        const double *den = reinterpret_cast<const double *>(buf + St::off_dens);
+        const double *nrm = reinterpret_cast<const double *>(buf + St::off_nrm);
+        const double sx = pos[3 * s], sy = pos[3 * s + 1], sz = pos[3 * s + 2];
+        const double d0 = den[3 * s], d1 = den[3 * s + 1], d2 = den[3 * s + 2];
+        double n0 = 0.0, n1 = 0.0, n2 = 0.0;
+        if (KIND == F3D_KERNEL_STRESSLET) { n0 = nrm[3 * s]; n1 = nrm[3 * s + 1]; n2 = nrm[3 * s + 2]; }
+        int32_t sg = 0;
+        if (MODE == F3D_SELF_SKIP_GROUP) sg = reinterpret_cast<const int32_t *>(buf + St::off_grp)[s];
+#pragma unroll
+        for (int k = 0; k < TPT; ++k) {
+          const double dx = txd[k] - sx, dy = tyd[k] - sy, dz = tzd[k] - sz;
+          double r2 = fma(dx, dx, fma(dy, dy, dz * dz));
+          r2 = (r2 < eps2) ? r2 + reg2 : r2;
+          double ri = rsqrt(r2);
+          if (MODE == F3D_SELF_SKIP_INDEX) ri = (sbase + s == tidx[k]) ? 0.0 : ri;
+          if (MODE == F3D_SELF_SKIP_GROUP) ri = (sg == tgrp[k]) ? 0.0 : ri;
+          if (KIND == F3D_KERNEL_OSEEN) {
+            const double rf = fma(dx, d0, fma(dy, d1, dz * d2));
+            const double g = ri * ri * ri * rf;
+            acc[k][0] = fma(g, dx, fma(ri, d0, acc[k][0]));
+            acc[k][1] = fma(g, dy, fma(ri, d1, acc[k][1]));
+            acc[k][2] = fma(g, dz, fma(ri, d2, acc[k][2]));
+          } else if (KIND == F3D_KERNEL_ROTLET) {
+            const double g = ri * ri * ri;
+            acc[k][0] = fma(g, dz * d1 - dy * d2, acc[k][0]);
+            acc[k][1] = fma(g, dx * d2 - dz * d0, acc[k][1]);
+            acc[k][2] = fma(g, dy * d0 - dx * d1, acc[k][2]);
+          } else {
+            const double ri2 = ri * ri;
+            const double rd = fma(dx, d0, fma(dy, d1, dz * d2));
+            const double rn = fma(dx, n0, fma(dy, n1, dz * n2));
+            const double f0 = rd * rn * (ri2 * ri2 * ri);
+            acc[k][0] = fma(f0, dx, acc[k][0]);
+            acc[k][1] = fma(f0, dy, acc[k][1]);
+            acc[k][2] = fma(f0, dz, acc[k][2]);
+          }
+        }
+      } else {
+        const float4 *rec = reinterpret_cast<const float4 *>(buf + St::off_rec);
+        const float4 q0 = rec[3 * s], q1 = rec[3 * s + 1], q2 = rec[3 * s + 2];
+        // q0 = {xh, yh, zh, xl}; q1 = {yl, zl, d0, d1}; q2 = {d2, n0, n1, n2}
+        int32_t sg = 0;
+        if (MODE == F3D_SELF_SKIP_GROUP) sg = reinterpret_cast<const int32_t *>(buf + St::off_grp)[s];
+#pragma unroll
+        for (int k = 0; k < TPT; ++k) {
+          const float dx = (txh[k] - q0.x) + (txl[k] - q0.w);
+          const float dy = (tyh[k] - q0.y) + (tyl[k] - q1.x);
+          const float dz = (tzh[k] - q0.z) + (tzl[k] - q1.y);
+          float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+          r2 = (r2 < eps2f) ? r2 + reg2f : r2;
+          float ri = rsqrtf(r2);
+          if (MODE == F3D_SELF_SKIP_INDEX) ri = (sbase + s == tidx[k]) ? 0.f : ri;
+          if (MODE == F3D_SELF_SKIP_GROUP) ri = (sg == tgrp[k]) ? 0.f : ri;
+          if (KIND == F3D_KERNEL_OSEEN) {
+            const float rf = fmaf(dx, q1.z, fmaf(dy, q1.w, dz * q2.x));
+            const float g = ri * ri * ri * rf;
+            ft[k][0] = fmaf(g, dx, fmaf(ri, q1.z, ft[k][0]));
+            ft[k][1] = fmaf(g, dy, fmaf(ri, q1.w, ft[k][1]));
+            ft[k][2] = fmaf(g, dz, fmaf(ri, q2.x, ft[k][2]));
+          } else if (KIND == F3D_KERNEL_ROTLET) {
+            const float g = ri * ri * ri;
+            ft[k][0] = fmaf(g, dz * q1.w - dy * q2.x, ft[k][0]);
+            ft[k][1] = fmaf(g, dx * q2.x - dz * q1.z, ft[k][1]);
+            ft[k][2] = fmaf(g, dy * q1.z - dx * q1.w, ft[k][2]);
+          } else {
+            const float ri2 = ri * ri;
+            const float rd = fmaf(dx, q1.z, fmaf(dy, q1.w, dz * q2.x));
+            const float rn = fmaf(dx, q2.y, fmaf(dy, q2.z, dz * q2.w));
+            const float f0 = rd * rn * (ri2 * ri2 * ri);
+            ft[k][0] = fmaf(f0, dx, ft[k][0]);
+            ft[k][1] = fmaf(f0, dy, ft[k][1]);
+            ft[k][2] = fmaf(f0, dz, ft[k][2]);
+          }
+        }
+      }
+    }
+    if (PREC != F3D_FP64) {
+#pragma unroll
+      for (int k = 0; k < TPT; ++k)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) { two_sum(fs[k][c], fc[k][c], ft[k][c]); ft[k][c] = 0.f; }
+    }
+  };
+
+  // ---- plain (non-bulk) cooperative tile load ----------------------------
+  auto load_plain = [&](unsigned char *buf, int64_t s0, int cnt) {
+    if (PREC == F3D_FP64) {
+      double *pos = reinterpret_cast<double *>(buf + St::off_pos);
+      double *den = reinterpret_cast<double *>(buf + St::off_dens);
+      double *nrm = reinterpret_cast<double *>(buf + St::off_nrm);
+      for (int i = tid; i < 3 * cnt; i += kBlock) {
+        pos[i] = a.rs[3 * s0 + i];
+        den[i] = a.dens[3 * s0 + i];
+        if (KIND == F3D_KERNEL_STRESSLET) nrm[i] = a.nrm[3 * s0 + i];
+      }
+    } else {
+      float *rec = reinterpret_cast<float *>(buf + St::off_rec);
+      for (int i = tid; i < 12 * cnt; i += kBlock) rec[i] = a.packed[12 * s0 + i];
+    }
+    if (MODE == F3D_SELF_SKIP_GROUP) {
+      int32_t *g = reinterpret_cast<int32_t *>(buf + St::off_grp);
+      for (int i = tid; i < cnt; i += kBlock) g[i] = a.gs[s0 + i];
+    }
+  };
+
+  // ---- bulk-copy issue of one full tile (thread 0 only) ------------------
+  auto issue_tile = [&](int st, int64_t tile) {
+    unsigned char *buf = stages + st * St::bytes;
+    const int64_t s0 = tile * kTile;
+    uint32_t bytes = (PREC == F3D_FP64) ? (St::kNrm ? 72u : 48u) * kTile : 48u * kTile;
+    if (MODE == F3D_SELF_SKIP_GROUP) bytes += 4u * kTile;
+    mbar_arrive_expect_tx(&bars[st], bytes);
+    if (PREC == F3D_FP64) {
+      bulk_copy_g2s(buf + St::off_pos, a.rs + 3 * s0, 24u * kTile, &bars[st]);
+      bulk_copy_g2s(buf + St::off_dens, a.dens + 3 * s0, 24u * kTile, &bars[st]);
+      if (KIND == F3D_KERNEL_STRESSLET)
+        bulk_copy_g2s(buf + St::off_nrm, a.nrm + 3 * s0, 24u * kTile, &bars[st]);
+    } else {
+      bulk_copy_g2s(buf + St::off_rec, a.packed + 12 * s0, 48u * kTile, &bars[st]);
+    }
+    if (MODE == F3D_SELF_SKIP_GROUP)
+      bulk_copy_g2s(buf + St::off_grp, a.gs + s0, 4u * kTile, &bars[st]);
+  };
+
+  // ---- source range of this split ---------------------------------------
+  const int split = blockIdx.y;
+  const int64_t nfull = a.ns / kTile;
+  const int64_t tile0 = static_cast<int64_t>(split) * a.tiles_per_split;
+  const int64_t tile1 = min(tile0 + a.tiles_per_split, nfull);
+  const int64_t ntl = (tile1 > tile0) ? (tile1 - tile0) : 0;
+  const int tail = static_cast<int>(a.ns - nfull * kTile);
+  const bool has_tail = (split == a.nsplit - 1) && tail > 0;
+
+  bool ok_all = true;
+  if (a.use_tma) {
+    if (tid == 0) {
+      mbar_init(&bars[0], 1);
+      mbar_init(&bars[1], 1);
+      fence_mbar_init();
+    }
+    __syncthreads();
+    if (tid == 0) {
+      for (int st = 0; st < 2 && st < ntl; ++st) issue_tile(st, tile0 + st);
+    }
+    for (int64_t i = 0; i < ntl; ++i) {
+      const int st = static_cast<int>(i & 1);
+      const uint32_t parity = static_cast<uint32_t>((i >> 1) & 1);
+      const bool ok = mbar_wait_bounded(&bars[st], parity);
+      if (ok) compute_tile(stages + st * St::bytes, kTile, (tile0 + i) * kTile);
+      if (__syncthreads_or(!ok)) { ok_all = false; break; }
+      if (tid == 0 && i + 2 < ntl) {
+        fence_proxy_async_smem();
+        issue_tile(st, tile0 + i + 2);
+      }
+    }
+    if (!ok_all) {
+      // Give copies still in flight a bounded chance to land before exit.
+      if (tid == 0) {
+        record_error(a.err, F3D_ERR_TIMEOUT);
+        for (int st = 0; st < 2; ++st) (void)mbar_wait_bounded(&bars[st], 0);
+      }
+      return;
+    }
+  } else {
+    for (int64_t i = 0; i < ntl; ++i) {
+      load_plain(stages, (tile0 + i) * kTile, kTile);
+      __syncthreads();
+      compute_tile(stages, kTile, (tile0 + i) * kTile);
+      __syncthreads();
+    }
+  }
+  if (has_tail) {
+    load_plain(stages, nfull * kTile, tail);
+    __syncthreads();
+    compute_tile(stages, tail, nfull * kTile);
+  }
+
+  // ---- combine lanes of a target group -----------------------------------
+  double res[TPT][3];
+#pragma unroll
+  for (int k = 0; k < TPT; ++k)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      double v = (PREC == F3D_FP64) ? acc[k][c]
+                                    : static_cast<double>(fs[k][c]) + static_cast<double>(fc[k][c]);
+#pragma unroll
+      for (int off = SL / 2; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+      res[k][c] = v;
+    }
+
+  if (a.nsplit == 1) {
+    if (sl == 0) {
+#pragma unroll
+      for (int k = 0; k < TPT; ++k) {
+        const int64_t t = tidx[k];
+        if (t < a.nt) {
+#pragma unroll
+          for (int c = 0; c < 3; ++c) {
+            const double v = a.scale * res[k][c];
+            a.out[3 * t + c] = a.accumulate ? a.out[3 * t + c] + v : v;
+          }
+        }
+      }
+    }
+    return;
+  }
+
+  // ---- multi-split: partials, then the last CTA of this target block sums --
+  if (sl == 0) {
+#pragma unroll
+    for (int k = 0; k < TPT; ++k) {
+      const int64_t t = tidx[k];
+      if (t < a.nt) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+          __stcg(&a.partial[(static_cast<int64_t>(split) * a.nt + t) * 3 + c], res[k][c]);
+      }
+    }
+  }
+  __threadfence();
+  __syncthreads();
+  __shared__ int s_last;
+  if (tid == 0) {
+    const unsigned prev = atomicAdd(&a.counters[blockIdx.x], 1u);
+    s_last = (prev == static_cast<unsigned>(a.nsplit - 1));
+  }
+  __syncthreads();
+  if (!s_last) return;
+  __threadfence();
+  const int64_t nvals = ((a.nt - tb < TPB) ? (a.nt - tb) : static_cast<int64_t>(TPB)) * 3;
+  for (int64_t i = tid; i < nvals; i += kBlock) {
+    const int64_t gi = tb * 3 + i;
+    double v = 0.0;
+    for (int sp = 0; sp < a.nsplit; ++sp) v += __ldcg(&a.partial[static_cast<int64_t>(sp) * a.nt * 3 + gi]);
+    v *= a.scale;
+    a.out[gi] = a.accumulate ? a.out[gi] + v : v;
+  }
+  if (tid == 0) a.counters[blockIdx.x] = 0u;
+}
+
+// Packs FP32C source records: {xh,yh,zh,xl},{yl,zl,d0,d1},{d2,n0,n1,n2}.
+__global__ void pack_fp32_sources(const double *rs, const double *dens, const double *nrm,
+                                  float *packed, int64_t ns) {
+  const int64_t s = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (s >= ns) return;
+  float h[3], l[3];
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    const double x = rs[3 * s + c];
+    h[c] = static_cast<float>(x);
+    l[c] = static_cast<float>(x - static_cast<double>(h[c]));
+  }
+  float4 *o = reinterpret_cast<float4 *>(packed + 12 * s);
+  const float d0 = static_cast<float>(dens[3 * s]), d1 = static_cast<float>(dens[3 * s + 1]),
+              d2 = static_cast<float>(dens[3 * s + 2]);
+  float n0 = 0.f, n1 = 0.f, n2 = 0.f;
+  if (nrm) {
+    n0 = static_cast<float>(nrm[3 * s]);
+    n1 = static_cast<float>(nrm[3 * s + 1]);
+    n2 = static_cast<float>(nrm[3 * s + 2]);
+  }
+  o[0] = make_float4(h[0], h[1], h[2], l[0]);
+  o[1] = make_float4(l[1], l[2], d0, d1);
+  o[2] = make_float4(d2, n0, n1, n2);
+}
+
+// ---------------------------------------------------------------- host ----
+struct Plan {
+  int tpt, sl, nsplit, use_tma;
+  int64_t ntb, tiles_per_split;
+  size_t off_counters, off_partial, off_packed, bytes;
+};
+
+static int make_plan(int kernel, int precision, int64_t ns, int64_t nt, const f3d_pair_shape *shape,
+                     Plan *p) {
+  if (kernel < 0 || kernel > 2 || precision < 0 || precision > 1) return F3D_ERR_ARG;
+  if (ns < 0 || nt < 0) return F3D_ERR_SHAPE;
+  int tpt = shape && shape->tpt ? shape->tpt : 0;
+  int sl = shape && shape->sl ? shape->sl : 0;
+  if (sl == 0) sl = (nt >= 4096) ? 1 : (nt >= 512 ? 8 : 32);
+  if (tpt == 0) tpt = 1;
+  if (!(tpt == 1 || tpt == 2)) return F3D_ERR_ARG;
+  if (!(sl == 1 || sl == 8 || sl == 32)) return F3D_ERR_ARG;
+  if (sl != 1 && tpt != 1) return F3D_ERR_ARG;
+  const int64_t tpb = static_cast<int64_t>(kBlock / sl) * tpt;
+  const int64_t ntb = (nt + tpb - 1) / tpb;
+  const int64_t nfull = ns / kTile;
+  int64_t nsplit = shape && shape->nsplit > 0 ? shape->nsplit : 0;
+  if (nsplit == 0) {
+    const int64_t want = 4LL * sm_count();
+    nsplit = ntb > 0 ? (want + ntb - 1) / ntb : 1;
+  }
+  nsplit = std::max<int64_t>(1, std::min<int64_t>(nsplit, std::max<int64_t>(nfull, 1)));
+  nsplit = std::min<int64_t>(nsplit, 65535);
+  int64_t tps = nfull > 0 ? (nfull + nsplit - 1) / nsplit : 0;
+  if (tps > 0) nsplit = (nfull + tps - 1) / tps;
+  if (nsplit < 1) nsplit = 1;
+  p->tpt = tpt;
+  p->sl = sl;
+  p->nsplit = static_cast<int>(nsplit);
+  p->use_tma = (shape && shape->use_tma < 0) ? 0 : 1;
+  p->ntb = ntb;
+  p->tiles_per_split = tps;
+  size_t off = 0;
+  p->off_counters = off;
+  if (p->nsplit > 1) off += round_up(static_cast<size_t>(ntb) * sizeof(unsigned), 256);
+  p->off_partial = off;
+  if (p->nsplit > 1) off += round_up(static_cast<size_t>(p->nsplit) * nt * 3 * sizeof(double), 256);
+  p->off_packed = off;
+  if (precision == F3D_FP32C) off += round_up(static_cast<size_t>(ns) * 12 * sizeof(float), 256);
+  p->bytes = off;
+  return F3D_OK;
+}
+
+template <int KIND, int MODE, int PREC, int TPT, int SL>
+static int launch_one(const PairArgs &a, int64_t ntb, int nsplit, cudaStream_t st) {
+  constexpr size_t smem = pair_smem_bytes<KIND, MODE, PREC>();
+  auto kfn = pair_kernel<KIND, MODE, PREC, TPT, SL>;
+  static bool attr_set[64] = {false};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (smem > 48 * 1024 && dev >= 0 && dev < 64 && !attr_set[dev]) {
+    if (cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             static_cast<int>(smem)) != cudaSuccess)
+      return F3D_ERR_CUDA;
+    attr_set[dev] = true;
+  }
+  dim3 grid(static_cast<unsigned>(ntb), static_cast<unsigned>(nsplit));
+  kfn<<<grid, kBlock, smem, st>>>(a);
+  return launch_status();
+}
+
+template <int KIND, int MODE, int PREC>
+static int dispatch_shape(const PairArgs &a, const Plan &p, cudaStream_t st) {
+  if (p.sl == 1 && p.tpt == 1) return launch_one<KIND, MODE, PREC, 1, 1>(a, p.ntb, p.nsplit, st);
+  if (p.sl == 1 && p.tpt == 2) return launch_one<KIND, MODE, PREC, 2, 1>(a, p.ntb, p.nsplit, st);
+  if (p.sl == 8) return launch_one<KIND, MODE, PREC, 1, 8>(a, p.ntb, p.nsplit, st);
+  return launch_one<KIND, MODE, PREC, 1, 32>(a, p.ntb, p.nsplit, st);
+}
+
+template <int KIND, int PREC>
+static int dispatch_mode(int mode, const PairArgs &a, const Plan &p, cudaStream_t st) {
+  switch (mode) {
+    case F3D_SELF_REGULARISE: return dispatch_shape<KIND, F3D_SELF_REGULARISE, PREC>(a, p, st);
+    case F3D_SELF_SKIP_INDEX: return dispatch_shape<KIND, F3D_SELF_SKIP_INDEX, PREC>(a, p, st);
+    case F3D_SELF_SKIP_GROUP: return dispatch_shape<KIND, F3D_SELF_SKIP_GROUP, PREC>(a, p, st);
+    default: return F3D_ERR_ARG;
+  }
+}
+
+template <int KIND>
+static int dispatch_prec(int prec, int mode, const PairArgs &a, const Plan &p, cudaStream_t st) {
+  if (prec == F3D_FP64) return dispatch_mode<KIND, F3D_FP64>(mode, a, p, st);
+  return dispatch_mode<KIND, F3D_FP32C>(mode, a, p, st);
+}
+
+int pair_sum_impl(int kernel, int precision, int self_mode, const double *rs, const double *rt,
+                  const double *dens, const double *nrm, const int32_t *gs, const int32_t *gt,
+                  double *out, int64_t ns, int64_t nt, double eta, double reg, double eps,
+                  int accumulate, const f3d_pair_shape *shape, void *ws, size_t ws_bytes,
+                  cudaStream_t st) {
+  Plan p;
+  int rc = make_plan(kernel, precision, ns, nt, shape, &p);
+  if (rc) return rc;
+  if (self_mode < 0 || self_mode > 2) return F3D_ERR_ARG;
+  if (nt == 0) return F3D_OK;
+  if (!rt || !out) return F3D_ERR_NULL;
+  if (ns > 0 && (!rs || !dens)) return F3D_ERR_NULL;
+  if (kernel == F3D_KERNEL_STRESSLET && ns > 0 && !nrm) return F3D_ERR_NULL;
+  if (self_mode == F3D_SELF_SKIP_GROUP && (!gt || (ns > 0 && !gs))) return F3D_ERR_NULL;
+  if (self_mode == F3D_SELF_SKIP_INDEX && ns != nt) return F3D_ERR_SHAPE;
+  if (!aligned(rs, 8) || !aligned(rt, 8) || !aligned(dens, 8) || !aligned(nrm, 8) ||
+      !aligned(out, 8) || !aligned(gs, 4) || !aligned(gt, 4))
+    return F3D_ERR_ALIGN;
+  if (ns == 0) {
+    if (!accumulate && cudaMemsetAsync(out, 0, static_cast<size_t>(nt) * 3 * sizeof(double), st) != cudaSuccess)
+      return F3D_ERR_CUDA;
+    return F3D_OK;
+  }
+  if (p.bytes > 0 && (!ws || ws_bytes < p.bytes)) return F3D_ERR_WORKSPACE;
+  if (ws && !aligned(ws, 256)) return F3D_ERR_ALIGN;
+  unsigned char *w = static_cast<unsigned char *>(ws);
+
+  PairArgs a;
+  a.rs = rs; a.rt = rt; a.dens = dens; a.nrm = nrm;
+  a.gs = gs; a.gt = gt;
+  a.out = out;
+  a.partial = p.nsplit > 1 ? reinterpret_cast<double *>(w + p.off_partial) : nullptr;
+  a.counters = p.nsplit > 1 ? reinterpret_cast<unsigned *>(w + p.off_counters) : nullptr;
+  a.packed = precision == F3D_FP32C ? reinterpret_cast<float *>(w + p.off_packed) : nullptr;
+  a.err = device_error_word();
+  a.ns = ns; a.nt = nt;
+  a.tiles_per_split = p.tiles_per_split;
+  a.nsplit = p.nsplit;
+  a.accumulate = accumulate ? 1 : 0;
+  a.eps2 = eps * eps;
+  a.reg2 = reg * reg;
+  a.scale = (kernel == F3D_KERNEL_STRESSLET) ? -3.0 / (4.0 * kPi * eta) : 1.0 / (8.0 * kPi * eta);
+  // Bulk copies need 16-byte aligned sources; otherwise stage with plain loads.
+  a.use_tma = p.use_tma;
+  if (precision == F3D_FP64 && (!aligned(rs, 16) || !aligned(dens, 16) ||
+                                (kernel == F3D_KERNEL_STRESSLET && !aligned(nrm, 16))))
+    a.use_tma = 0;
+  if (self_mode == F3D_SELF_SKIP_GROUP && !aligned(gs, 16)) a.use_tma = 0;
+
+  if (precision == F3D_FP32C) {
+    const int64_t nb = (ns + 255) / 256;
+    pack_fp32_sources<<<static_cast<unsigned>(nb), 256, 0, st>>>(
+        rs, dens, kernel == F3D_KERNEL_STRESSLET ? nrm : nullptr, const_cast<float *>(a.packed), ns);
+    if ((rc = launch_status())) return rc;
+  }
+  switch (kernel) {
+    case F3D_KERNEL_OSEEN: return dispatch_prec<F3D_KERNEL_OSEEN>(precision, self_mode, a, p, st);
+    case F3D_KERNEL_STRESSLET: return dispatch_prec<F3D_KERNEL_STRESSLET>(precision, self_mode, a, p, st);
+    default: return dispatch_prec<F3D_KERNEL_ROTLET>(precision, self_mode, a, p, st);
+  }
+}
+
+}  // namespace f3d
+
+extern "C" {
+
+int f3d_pair_workspace_bytes(int kernel, int precision, int64_t ns, int64_t nt,
+                             const f3d_pair_shape *shape, size_t *bytes) {
+  if (!bytes) return F3D_ERR_NULL;
+  f3d::Plan p;
+  int rc = f3d::make_plan(kernel, precision, ns, nt, shape, &p);
+  if (rc) return rc;
+  *bytes = p.bytes;
+  return F3D_OK;
+}
+
+int f3d_pair_sum(int kernel, int precision, int self_mode, const double *r_source,
+                 const double *r_target, const double *density, const double *normal,
+                 const int32_t *src_group, const int32_t *trg_group, double *out, int64_t ns,
+                 int64_t nt, double eta, double reg, double epsilon_distance, int accumulate,
+                 const f3d_pair_shape *shape, void *workspace, size_t workspace_bytes,
+                 void *stream) {
+  return f3d::pair_sum_impl(kernel, precision, self_mode, r_source, r_target, density, normal,
+                            src_group, trg_group, out, ns, nt, eta, reg, epsilon_distance,
+                            accumulate, shape, workspace, workspace_bytes,
+                            static_cast<cudaStream_t>(stream));
+}
+
+int f3d_oseen_source_target(const double *r_source, const double *r_target,
+                            const double *density, double *u, int64_t ns, int64_t nt,
+                            double eta, double reg, double epsilon_distance, int precision,
+                            void *workspace, size_t workspace_bytes, void *stream) {
+  return f3d::pair_sum_impl(F3D_KERNEL_OSEEN, precision, F3D_SELF_REGULARISE, r_source, r_target,
+                            density, nullptr, nullptr, nullptr, u, ns, nt, eta, reg,
+                            epsilon_distance, 0, nullptr, workspace, workspace_bytes,
+                            static_cast<cudaStream_t>(stream));
+}
+
+int f3d_oseen_times_density(const double *r_vectors, const double *density, double *u,
+                            int64_t n, double eta, double reg, double epsilon_distance,
+                            int precision, void *workspace, size_t workspace_bytes,
+                            void *stream) {
+  return f3d::pair_sum_impl(F3D_KERNEL_OSEEN, precision, F3D_SELF_SKIP_INDEX, r_vectors,
+                            r_vectors, density, nullptr, nullptr, nullptr, u, n, n, eta, reg,
+                            epsilon_distance, 0, nullptr, workspace, workspace_bytes,
+                            static_cast<cudaStream_t>(stream));
+}
+
+int f3d_rotlet_source_target(const double *r_source, const double *r_target,
+                             const double *density, double *u, int64_t ns, int64_t nt,
+                             double eta, double reg, double epsilon_distance, int precision,
+                             void *workspace, size_t workspace_bytes, void *stream) {
+  return f3d::pair_sum_impl(F3D_KERNEL_ROTLET, precision, F3D_SELF_REGULARISE, r_source, r_target,
+                            density, nullptr, nullptr, nullptr, u, ns, nt, eta, reg,
+                            epsilon_distance, 0, nullptr, workspace, workspace_bytes,
+                            static_cast<cudaStream_t>(stream));
+}
+
+int f3d_stresslet_source_target(const double *r_source, const double *r_target,
+                                const double *normal, const double *density, double *v,
+                                int64_t ns, int64_t nt, double eta, double reg,
+                                double epsilon_distance, int precision, void *workspace,
+                                size_t workspace_bytes, void *stream) {
+  return f3d::pair_sum_impl(F3D_KERNEL_STRESSLET, precision, F3D_SELF_REGULARISE, r_source,
+                            r_target, density, normal, nullptr, nullptr, v, ns, nt, eta, reg,
+                            epsilon_distance, 0, nullptr, workspace, workspace_bytes,
+                            static_cast<cudaStream_t>(stream));
+}
+
+int f3d_stresslet_times_normal_times_density(const double *r_vectors, const double *normal,
+                                             const double *density, double *v, int64_t n,
+                                             double eta, double reg, double epsilon_distance,
+                                             int precision, void *workspace,
+                                             size_t workspace_bytes, void *stream) {
+  return f3d::pair_sum_impl(F3D_KERNEL_STRESSLET, precision, F3D_SELF_SKIP_INDEX, r_vectors,
+                            r_vectors, density, normal, nullptr, nullptr, v, n, n, eta, reg,
+                            epsilon_distance, 0, nullptr, workspace, workspace_bytes,
+                            static_cast<cudaStream_t>(stream));
+}
+
+}  // extern "C"

@@ -1,0 +1,44 @@
+// Throughput probes used as measured roofline denominators: FP64 / FP32
+// fused multiply-add rate of this GPU.  Each thread runs 8 independent FMA
+// chains so the pipes, not the dependency latency, set the rate.
+#include "f3d_common.cuh"
+
+namespace f3d {
+
+template <typename T>
+__global__ void fma_probe_kernel(T *out, int iters, T a, T b) {
+  T c[8];
+#pragma unroll
+  for (int k = 0; k < 8; ++k) c[k] = static_cast<T>(threadIdx.x + k);
+  for (int i = 0; i < iters; ++i) {
+#pragma unroll
+    for (int k = 0; k < 8; ++k) c[k] = c[k] * a + b;
+  }
+  T s = 0;
+#pragma unroll
+  for (int k = 0; k < 8; ++k) s += c[k];
+  if (s == static_cast<T>(-1.2345)) out[0] = s;  // keeps the chains live
+}
+
+}  // namespace f3d
+
+extern "C" {
+
+int f3d_probe_fma(int precision, int iters, double *sink, double *flops, void *stream) {
+  if (!sink || !flops) return F3D_ERR_NULL;
+  if (iters <= 0) return F3D_ERR_SHAPE;
+  const int blocks = f3d::sm_count() * 8, threads = 256;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (precision == F3D_FP64) {
+    f3d::fma_probe_kernel<double><<<blocks, threads, 0, st>>>(sink, iters, 0.999999, 1e-7);
+  } else if (precision == F3D_FP32C) {
+    f3d::fma_probe_kernel<float><<<blocks, threads, 0, st>>>(reinterpret_cast<float *>(sink), iters,
+                                                             0.999999f, 1e-7f);
+  } else {
+    return F3D_ERR_ARG;
+  }
+  *flops = 2.0 * 8.0 * static_cast<double>(iters) * blocks * threads;
+  return f3d::launch_status();
+}
+
+}  // extern "C"

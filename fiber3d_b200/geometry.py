@@ -1,0 +1,128 @@
+"""Seeded synthetic geometry for the fiber3d hot-path workloads.
+
+* :func:`fibonacci_sphere` restates fiber3d's ``shape_gallery('sphere', N,
+  radius=R)`` (python/shape_gallery/shape_gallery.py:7-32): a latitude/longitude
+  Fibonacci lattice with outward unit normals.
+* Fiber generators: straight fibers on Chebyshev-Lobatto nodes (the Oseen
+  kernel workload), and fibers on the solver's equispaced parameter nodes
+  alpha = linspace(-1, 1, N) (python/fiber/fiber.py:128) with random transverse
+  Fourier modes (the time-step workloads).
+
+All generators take a ``numpy.random.Generator`` or an integer seed.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+
+def _rng(seed) -> np.random.Generator:
+    return seed if isinstance(seed, np.random.Generator) else np.random.default_rng(seed)
+
+
+def fibonacci_sphere(n: int, radius: float):
+    """Nodes and outward unit normals of shape_gallery('sphere', n, radius).
+
+    Node k = i + n//2 for i in [-n//2, n//2): latitude asin(2i/(2(n//2)+1)),
+    longitude (i mod phi) * 2 pi / phi wrapped into [-pi, pi], phi the golden
+    ratio (shape_gallery.py:9-22).  For odd n the last node stays at the
+    origin, as in the reference.
+    """
+    phi = (1.0 + np.sqrt(5.0)) / 2.0
+    half = n // 2
+    nodes = np.zeros((n, 3))
+    i = np.arange(-half, half)
+    lat = np.arcsin((2.0 * i) / (2 * half + 1))
+    lon = np.mod(i, phi) * 2.0 * np.pi / phi
+    lon = np.where(lon < -np.pi, 2.0 * np.pi + lon, lon)
+    lon = np.where(lon > np.pi, lon - 2.0 * np.pi, lon)
+    nodes[: 2 * half] = np.stack([np.cos(lon) * np.cos(lat), np.sin(lon) * np.cos(lat),
+                                  np.sin(lat)], axis=1)
+    nodes *= radius
+    normals = 2.0 * nodes
+    with np.errstate(invalid="ignore", divide="ignore"):
+        normals /= np.linalg.norm(normals, axis=1, keepdims=True)
+    return nodes, normals
+
+
+def uniform_ball(rng, n: int, radius: float) -> np.ndarray:
+    rng = _rng(rng)
+    v = rng.normal(size=(n, 3))
+    v /= np.linalg.norm(v, axis=1, keepdims=True)
+    r = radius * rng.random(n) ** (1.0 / 3.0)
+    return v * r[:, None]
+
+
+def uniform_directions(rng, n: int) -> np.ndarray:
+    rng = _rng(rng)
+    v = rng.normal(size=(n, 3))
+    return v / np.linalg.norm(v, axis=1, keepdims=True)
+
+
+def chebyshev_lobatto(n: int) -> np.ndarray:
+    """-cos(pi k/(n-1)), k = 0..n-1 (ascending in [-1, 1])."""
+    return -np.cos(np.pi * np.arange(n) / (n - 1))
+
+
+def straight_fibers_cheb(rng, nfib: int, npts: int, length: float, ball_radius: float):
+    """Straight fibers on Chebyshev-Lobatto nodes: x = c + (L/2) s d."""
+    rng = _rng(rng)
+    c = uniform_ball(rng, nfib, ball_radius)
+    d = uniform_directions(rng, nfib)
+    s = chebyshev_lobatto(npts)
+    x = c[:, None, :] + (length / 2.0) * s[None, :, None] * d[:, None, :]
+    return x.reshape(nfib * npts, 3)
+
+
+def perturbed_fibers(rng, nfib: int, npts, length: float, ball_radius: float,
+                     amplitude: float = 0.05, modes: int = 3):
+    """Fibers on the solver's equispaced nodes alpha = linspace(-1, 1, N):
+    straight line through a centre uniform in a ball, plus ``modes`` random
+    transverse Fourier modes sin(k pi (alpha+1)/2) of amplitude ``amplitude``.
+
+    ``npts`` is an int or a per-fiber sequence.  Returns a list of (N_k, 3)
+    arrays.
+    """
+    rng = _rng(rng)
+    if np.isscalar(npts):
+        npts = [int(npts)] * nfib
+    c = uniform_ball(rng, nfib, ball_radius)
+    d = uniform_directions(rng, nfib)
+    out = []
+    for k in range(nfib):
+        n = int(npts[k])
+        alpha = np.linspace(-1.0, 1.0, n)
+        # two unit vectors orthogonal to d
+        a = np.array([1.0, 0.0, 0.0]) if abs(d[k, 0]) < 0.9 else np.array([0.0, 1.0, 0.0])
+        e1 = np.cross(d[k], a)
+        e1 /= np.linalg.norm(e1)
+        e2 = np.cross(d[k], e1)
+        x = c[k] + (length / 2.0) * alpha[:, None] * d[k]
+        for m in range(1, modes + 1):
+            w = rng.normal(size=2)
+            w /= np.linalg.norm(w)
+            x = x + amplitude * np.sin(m * np.pi * (alpha + 1.0) / 2.0)[:, None] * (w[0] * e1 + w[1] * e2)
+        out.append(x)
+    return out
+
+
+# --------------------------------------------------------------- workloads --
+def oseen_fiber_workload(seed: int = 1, nfib: int = 32, npts: int = 32):
+    """32 straight fibers of length 2 x 32 Chebyshev-Lobatto nodes, centres
+    uniform in a ball of radius 5, directions uniform; forces N(0,1)."""
+    rng = _rng(seed)
+    x = straight_fibers_cheb(rng, nfib, npts, 2.0, 5.0)
+    f = rng.normal(size=x.shape)
+    return x, f
+
+
+def stresslet_sphere_workload(seed: int = 2, n: int = 12000, radius: float = 10.0,
+                              n_vol: int = 4096, vol_radius: float = 9.0):
+    """Spherical periphery (Fibonacci nodes, outward normals, equal weights
+    4 pi R^2 / N), double-layer density N(0,1), plus volume targets uniform
+    in a ball of radius 9."""
+    rng = _rng(seed)
+    nodes, normals = fibonacci_sphere(n, radius)
+    w = np.full(n, 4.0 * np.pi * radius**2 / n)
+    mu = rng.normal(size=(n, 3))
+    vol = uniform_ball(rng, n_vol, vol_radius)
+    return nodes, normals, w, mu, vol

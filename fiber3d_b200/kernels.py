@@ -1,0 +1,264 @@
+"""Drop-in replacement for fiber3d's ``kernels.kernels`` module on one B200.
+
+Every function keeps the name, positional/keyword signature, defaults and
+return convention of the fiber3d function it replaces
+(``python/kernels/kernels.py``), so ``sys.modules['kernels.kernels']`` can
+point at this module and the unmodified time stepper runs on the GPU.
+
+* Inputs may be numpy arrays (any shape whose size is 3N, any strides; they
+  are copied host->device) or torch tensors (CUDA tensors are used in place).
+* Outputs follow the inputs: a new flat float64 numpy array of length 3*Nt
+  when any point array came from the host, else a flat CUDA float64 tensor.
+* Inputs are never modified.
+* The work runs on the current CUDA stream through the C ABI of
+  ``libfiber3d_b200.so``; there is no CPU path.
+
+Keyword-only extensions (not in fiber3d): ``precision`` ('fp64' default or
+'fp32c') and ``shape`` (a :class:`fiber3d_b200._lib.PairShape` launch shape,
+normally chosen by :mod:`fiber3d_b200.autotune`).
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+import torch
+
+from . import _lib
+
+__all__ = [
+    "oseen_kernel_source_target_numba", "oseen_kernel_times_density_numba",
+    "rotlet_kernel_source_target_numba", "stresslet_kernel_source_target_numba",
+    "stresslet_kernel_times_normal_times_density_numba", "stresslet_kernel_times_normal_numba",
+    "oseen_tensor", "oseen_tensor_source_target", "complementary_kernel",
+    "complementary_kernel_times_density_numba", "pair_sum",
+]
+
+
+# ------------------------------------------------------------------ helpers --
+def _device() -> torch.device:
+    _lib.lib()  # raises if no CUDA device or no library
+    return torch.device("cuda", torch.cuda.current_device())
+
+
+def _to_dev(x, dev: torch.device, name: str) -> torch.Tensor:
+    """(N,3) contiguous float64 CUDA tensor from a numpy array or torch tensor."""
+    if isinstance(x, torch.Tensor):
+        t = x.detach()
+        if t.device != dev or t.dtype != torch.float64:
+            t = t.to(device=dev, dtype=torch.float64)
+    else:
+        a = np.ascontiguousarray(np.asarray(x, dtype=np.float64))
+        t = torch.from_numpy(a).to(dev)
+    if t.numel() % 3 != 0:
+        raise ValueError(f"{name}: size {t.numel()} is not a multiple of 3")
+    return t.reshape(-1, 3).contiguous()
+
+
+def _any_host(*xs) -> bool:
+    return any(not (isinstance(x, torch.Tensor) and x.is_cuda) for x in xs if x is not None)
+
+
+def _out(u: torch.Tensor, host: bool):
+    u = u.reshape(-1)
+    if host:
+        return u.cpu().numpy()
+    return u
+
+
+def _resolve_precision(precision) -> int:
+    if isinstance(precision, int):
+        return precision
+    try:
+        return _lib.PRECISION[precision]
+    except KeyError as e:
+        raise ValueError(f"precision must be one of {list(_lib.PRECISION)}") from e
+
+
+def pair_sum(kernel: str, r_source, r_target, density, normal=None, *, eta=1.0, reg=5e-3,
+             epsilon_distance=1e-5, self_mode: str = "regularise", src_group=None,
+             trg_group=None, precision="fp64", shape: _lib.PairShape | None = None,
+             out: torch.Tensor | None = None, accumulate: bool = False):
+    """General all-pairs sum on CUDA tensors (the building block of the drop-ins).
+
+    Returns a flat CUDA float64 tensor of length 3*Nt (``out`` if given).
+    """
+    dev = _device()
+    rs = _to_dev(r_source, dev, "r_source")
+    rt = _to_dev(r_target, dev, "r_target")
+    d = _to_dev(density, dev, "density")
+    if d.shape[0] != rs.shape[0]:
+        raise ValueError(f"density has {d.shape[0]} points, r_source has {rs.shape[0]}")
+    n = None
+    if kernel == "stresslet":
+        if normal is None:
+            raise ValueError("stresslet needs normals")
+        n = _to_dev(normal, dev, "normal")
+        if n.shape[0] != rs.shape[0]:
+            raise ValueError(f"normal has {n.shape[0]} points, r_source has {rs.shape[0]}")
+    gs = gt = None
+    if self_mode == "skip_group":
+        gs = torch.as_tensor(src_group, dtype=torch.int32, device=dev).contiguous()
+        gt = torch.as_tensor(trg_group, dtype=torch.int32, device=dev).contiguous()
+        if gs.numel() != rs.shape[0] or gt.numel() != rt.shape[0]:
+            raise ValueError("group id arrays must have one entry per point")
+    ns, nt = rs.shape[0], rt.shape[0]
+    if out is None:
+        out = torch.empty(3 * nt, dtype=torch.float64, device=dev)
+    elif out.numel() != 3 * nt or out.dtype != torch.float64 or not out.is_contiguous():
+        raise ValueError("out must be a contiguous float64 tensor of length 3*Nt")
+    k = _lib.KERNEL[kernel]
+    p = _resolve_precision(precision)
+    m = _lib.SELF_MODE[self_mode]
+    shp = ctypes.byref(shape) if shape is not None else None
+    nbytes = ctypes.c_size_t(0)
+    _lib.call("f3d_pair_workspace_bytes", k, p, ns, nt, shp, ctypes.byref(nbytes))
+    ws_ptr, ws_len = _lib.Workspace.get(dev).ensure(nbytes.value)
+    _lib.call("f3d_pair_sum", k, p, m, _lib.ptr(rs), _lib.ptr(rt), _lib.ptr(d), _lib.ptr(n),
+              _lib.ptr(gs), _lib.ptr(gt), _lib.ptr(out), ns, nt, float(eta), float(reg),
+              float(epsilon_distance), int(bool(accumulate)), shp, ws_ptr, ws_len,
+              _lib.stream_handle(dev))
+    return out
+
+
+# ------------------------------------------------------------ pair sums ----
+def oseen_kernel_source_target_numba(r_source, r_target, density, eta=1.0, reg=5e-3,
+                                     epsilon_distance=1e-5, *, precision="fp64", shape=None):
+    """u_t = 1/(8 pi eta) sum_s [f_s/r + (r.f_s) r/r^3], r = x_t - x_s; pairs with
+    r < epsilon_distance use sqrt(r^2 + reg^2).  fiber3d kernels.py:794-846."""
+    u = pair_sum("oseen", r_source, r_target, density, eta=eta, reg=reg,
+                 epsilon_distance=epsilon_distance, precision=precision, shape=shape)
+    return _out(u, _any_host(r_source, r_target, density))
+
+
+def oseen_kernel_times_density_numba(r_vectors, density, eta=1.0, reg=5e-3,
+                                     epsilon_distance=1e-5, *, precision="fp64", shape=None):
+    """Oseen sum over one point set with the pair j == i skipped (other close
+    pairs regularised).  fiber3d kernels.py:214-287."""
+    u = pair_sum("oseen", r_vectors, r_vectors, density, eta=eta, reg=reg,
+                 epsilon_distance=epsilon_distance, self_mode="skip_index",
+                 precision=precision, shape=shape)
+    return _out(u, _any_host(r_vectors, density))
+
+
+def rotlet_kernel_source_target_numba(r_source, r_target, density, eta=1.0, reg=5e-3,
+                                      epsilon_distance=1e-5, *, precision="fp64", shape=None):
+    """u_t = 1/(8 pi eta) sum_s tau_s x r / r^3.  fiber3d kernels.py:856-908."""
+    u = pair_sum("rotlet", r_source, r_target, density, eta=eta, reg=reg,
+                 epsilon_distance=epsilon_distance, precision=precision, shape=shape)
+    return _out(u, _any_host(r_source, r_target, density))
+
+
+def stresslet_kernel_source_target_numba(r_source, r_target, normal, density, eta=1.0,
+                                         reg=5e-3, epsilon_distance=1e-5, *, precision="fp64",
+                                         shape=None):
+    """v_t = -3/(4 pi eta) sum_s (r.d_s)(r.n_s) r / r^5.  fiber3d kernels.py:1186-1217."""
+    u = pair_sum("stresslet", r_source, r_target, density, normal, eta=eta, reg=reg,
+                 epsilon_distance=epsilon_distance, precision=precision, shape=shape)
+    return _out(u, _any_host(r_source, r_target, normal, density))
+
+
+def stresslet_kernel_times_normal_times_density_numba(r_vectors, normal, density, eta=1.0,
+                                                      reg=5e-3, epsilon_distance=1e-5, *,
+                                                      precision="fp64", shape=None):
+    """Stresslet sum over one point set, j == i skipped.  fiber3d kernels.py:1123-1183."""
+    u = pair_sum("stresslet", r_vectors, r_vectors, density, normal, eta=eta, reg=reg,
+                 epsilon_distance=epsilon_distance, self_mode="skip_index",
+                 precision=precision, shape=shape)
+    return _out(u, _any_host(r_vectors, normal, density))
+
+
+def complementary_kernel_times_density_numba(r_vectors, normal, density):
+    """u_i = n_i sum_j n_j . d_j (rank-one).  fiber3d kernels.py:1267-1283.
+
+    The reference spends O(N^2) on this O(N) product; here it is one reduction
+    and one scaling on the device.
+    """
+    dev = _device()
+    n = _to_dev(normal, dev, "normal")
+    d = _to_dev(density, dev, "density")
+    s = (n * d).sum()
+    u = n * s
+    return _out(u, _any_host(r_vectors, normal, density))
+
+
+# ------------------------------------------------------- dense operators ---
+def _dense_out(nrows: int, ncols: int, dev) -> torch.Tensor:
+    return torch.empty((nrows, ncols), dtype=torch.float64, device=dev)
+
+
+def stresslet_kernel_times_normal_numba(r_vectors, normal, eta=1.0, reg=5e-3,
+                                        epsilon_distance=1e-5):
+    """Dense 3N x 3N double-layer matrix, block S_ij = -3/(4 pi eta) (r.n_j)/r^5 r r^T,
+    r = x_i - x_j, zero diagonal blocks.  fiber3d kernels.py:1063-1120."""
+    dev = _device()
+    x = _to_dev(r_vectors, dev, "r_vectors")
+    n = _to_dev(normal, dev, "normal")
+    N = x.shape[0]
+    M = _dense_out(3 * N, 3 * N, dev)
+    _lib.call("f3d_stresslet_times_normal_dense", _lib.ptr(x), _lib.ptr(n), _lib.ptr(M), N, 3 * N,
+              float(eta), float(reg), float(epsilon_distance), _lib.stream_handle(dev))
+    return M.cpu().numpy() if _any_host(r_vectors, normal) else M
+
+
+def _xyz_to_r(x, N):
+    """'xyz' layout (x_all, y_all, z_all) -> (N, 3)."""
+    if isinstance(x, torch.Tensor):
+        return x.reshape(3, N).t().contiguous()
+    return np.ascontiguousarray(np.asarray(x, dtype=np.float64).reshape(3, N).T)
+
+
+def _perm_r_to_xyz(N: int) -> np.ndarray:
+    # row/col index in 'xyz' order -> index in 'r' (interleaved) order
+    return (np.arange(3)[:, None] + 3 * np.arange(N)[None, :]).reshape(-1)
+
+
+def oseen_tensor(r_vectors, eta=1.0, reg=5e-3, epsilon_distance=1e-5, input_format='r'):
+    """Dense 3N x 3N Oseen tensor; r <= epsilon_distance regularised (so the
+    diagonal block is I/(8 pi eta reg)).  fiber3d kernels.py:31-116."""
+    dev = _device()
+    host = _any_host(r_vectors)
+    size = r_vectors.numel() if isinstance(r_vectors, torch.Tensor) else np.size(r_vectors)
+    N = size // 3
+    xin = _xyz_to_r(r_vectors, N) if input_format != 'r' else r_vectors
+    x = _to_dev(xin, dev, "r_vectors")
+    G = _dense_out(3 * N, 3 * N, dev)
+    _lib.call("f3d_oseen_tensor_dense", _lib.ptr(x), _lib.ptr(G), N, 3 * N, float(eta),
+              float(reg), float(epsilon_distance), _lib.stream_handle(dev))
+    if input_format != 'r':
+        p = torch.as_tensor(_perm_r_to_xyz(N), device=dev)
+        G = G[p][:, p].contiguous()
+    return G.cpu().numpy() if host else G
+
+
+def oseen_tensor_source_target(r_source, r_target, eta=1.0, reg=5e-3, epsilon_distance=1e-5,
+                               input_format='r'):
+    """Dense 3Nt x 3Ns Oseen tensor.  fiber3d kernels.py:119-211."""
+    dev = _device()
+    host = _any_host(r_source, r_target)
+    sz = lambda a: a.numel() if isinstance(a, torch.Tensor) else np.size(a)
+    Ns, Nt = sz(r_source) // 3, sz(r_target) // 3
+    if input_format != 'r':
+        r_source, r_target = _xyz_to_r(r_source, Ns), _xyz_to_r(r_target, Nt)
+    xs = _to_dev(r_source, dev, "r_source")
+    xt = _to_dev(r_target, dev, "r_target")
+    G = _dense_out(3 * Nt, 3 * Ns, dev)
+    _lib.call("f3d_oseen_tensor_source_target_dense", _lib.ptr(xs), _lib.ptr(xt), _lib.ptr(G),
+              Ns, Nt, 3 * Ns, float(eta), float(reg), float(epsilon_distance),
+              _lib.stream_handle(dev))
+    if input_format != 'r':
+        pt = torch.as_tensor(_perm_r_to_xyz(Nt), device=dev)
+        ps = torch.as_tensor(_perm_r_to_xyz(Ns), device=dev)
+        G = G[pt][:, ps].contiguous()
+    return G.cpu().numpy() if host else G
+
+
+def complementary_kernel(r_vectors, normal):
+    """Dense outer(normal.flat, normal.flat).  fiber3d kernels.py:1286-1295."""
+    dev = _device()
+    n = _to_dev(normal, dev, "normal")
+    N = n.shape[0]
+    C = _dense_out(3 * N, 3 * N, dev)
+    _lib.call("f3d_complementary_dense", _lib.ptr(n), _lib.ptr(C), N, 3 * N,
+              _lib.stream_handle(dev))
+    return C.cpu().numpy() if _any_host(normal) else C

@@ -1,0 +1,187 @@
+/*
+ * fiber3d_b200 — C ABI of the B200 (sm_100a) hydrodynamic hot path of fiber3d.
+ *
+ * Every entry point takes plain device pointers, element counts and a CUDA
+ * stream (passed as void*; NULL = legacy default stream), launches
+ * asynchronously on that stream and returns an f3d_status.  No entry point
+ * allocates device memory: kernels that need scratch space take a caller
+ * workspace whose size is returned by the matching *_workspace_bytes query.
+ * A workspace must be zero-filled once when it is allocated; the kernels
+ * leave its counter words at zero when they finish.
+ *
+ * Layout conventions follow python/kernels/kernels.py of fiber3d: points,
+ * densities and normals are float64 arrays of shape (N, 3), row-major,
+ * xyz-interleaved; outputs are flat float64 arrays of length 3*Nt.
+ *
+ * Device-side failures (a bounded wait that ran out) are recorded in a
+ * per-device error word that f3d_get_device_error() reads and clears.
+ */
+#ifndef FIBER3D_B200_H
+#define FIBER3D_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+typedef enum f3d_status {
+  F3D_OK = 0,
+  F3D_ERR_NULL = 1,          /* a required pointer is NULL                 */
+  F3D_ERR_SHAPE = 2,         /* negative or inconsistent sizes             */
+  F3D_ERR_ALIGN = 3,         /* a pointer is not 8-byte aligned            */
+  F3D_ERR_WORKSPACE = 4,     /* workspace missing or too small             */
+  F3D_ERR_ARG = 5,           /* unknown enum value / bad launch shape      */
+  F3D_ERR_CUDA = 6,          /* a CUDA runtime call failed                 */
+  F3D_ERR_NONFINITE = 7,     /* non-finite input detected (checking on)    */
+  F3D_ERR_TIMEOUT = 8,       /* device-side bounded wait ran out           */
+  F3D_ERR_SINGULAR = 9,      /* zero pivot in an LU factorisation          */
+  F3D_ERR_TOO_LARGE = 10     /* size beyond a documented maximum           */
+} f3d_status;
+
+/* ---- enums ------------------------------------------------------------- */
+typedef enum f3d_kernel {
+  F3D_KERNEL_OSEEN = 0,      /* u_t = 1/(8 pi eta) sum_s [f/r + (r.f) r / r^3]      */
+  F3D_KERNEL_STRESSLET = 1,  /* v_t = -3/(4 pi eta) sum_s (r.d)(r.n) r / r^5        */
+  F3D_KERNEL_ROTLET = 2      /* u_t = 1/(8 pi eta) sum_s tau x r / r^3              */
+} f3d_kernel;
+
+typedef enum f3d_self_mode {
+  /* every pair is summed; a pair with |r| < eps uses sqrt(r^2 + reg^2)
+     (kernels.py:794-846, 856-908, 1186-1217)                                */
+  F3D_SELF_REGULARISE = 0,
+  /* sources == targets; the pair j == i is skipped, any other pair with
+     |r| < eps is regularised (kernels.py:214-287, 1123-1183)               */
+  F3D_SELF_SKIP_INDEX = 1,
+  /* pairs whose int32 group ids are equal are skipped (same fiber);
+     others are regularised as in F3D_SELF_REGULARISE. This fuses
+     flow_fibers + self_flow_fibers (tstep/tstep_utils.py:653-700, 812-851) */
+  F3D_SELF_SKIP_GROUP = 2
+} f3d_self_mode;
+
+typedef enum f3d_precision {
+  F3D_FP64 = 0,              /* IEEE float64 everywhere                               */
+  F3D_FP32C = 1              /* float32 pair terms from double-float coordinate
+                                differences; float32 per-tile sums folded into a
+                                two-sum (compensated) per-target accumulator; the
+                                result is written as float64                         */
+} f3d_precision;
+
+/* Launch shape of a pair kernel.  All-zero means "library default". */
+typedef struct f3d_pair_shape {
+  int32_t tpt;     /* targets per thread: 1 or 2                              */
+  int32_t sl;      /* source lanes per target group: 1, 8 or 32               */
+  int32_t nsplit;  /* source splits (grid.y); 0 = derive from the SM count    */
+  int32_t use_tma; /* 0 or 1: stage full source tiles with cp.async.bulk
+                      (default); -1: stage them with plain loads            */
+} f3d_pair_shape;
+
+/* ---- library ----------------------------------------------------------- */
+const char *f3d_version(void);
+const char *f3d_status_string(int status);
+/* Reads and clears the device error word of the current device (blocks on
+   the given stream).  Returns F3D_OK or F3D_ERR_TIMEOUT. */
+int f3d_get_device_error(void *stream);
+
+/* Launches an FMA-throughput probe (precision F3D_FP64 or F3D_FP32C = FP32)
+   on `stream`; *flops receives the floating-point operations it performs
+   (an FMA counts 2).  Timing it gives the measured pipe peak used as the
+   roofline denominator of the pair kernels.  `sink` is an 8-byte device
+   scratch word that is written only in a case that never occurs. */
+int f3d_probe_fma(int precision, int iters, double *sink, double *flops, void *stream);
+
+/* ---- all-pairs sums (A1, A2, A3, A4, A6) -------------------------------- */
+
+/* Workspace bytes needed by f3d_pair_sum for these sizes and launch shape. */
+int f3d_pair_workspace_bytes(int kernel, int precision, int64_t ns, int64_t nt,
+                             const f3d_pair_shape *shape, size_t *bytes);
+
+/* General source->target sum.  `normal` is read only for the stresslet.
+   `src_group`/`trg_group` are read only for F3D_SELF_SKIP_GROUP.
+   For F3D_SELF_SKIP_INDEX, r_target must hold the same points as r_source
+   (ns == nt).  If `accumulate` is non-zero the result is added to `out`,
+   otherwise `out` is overwritten. */
+int f3d_pair_sum(int kernel, int precision, int self_mode,
+                 const double *r_source, const double *r_target,
+                 const double *density, const double *normal,
+                 const int32_t *src_group, const int32_t *trg_group,
+                 double *out, int64_t ns, int64_t nt,
+                 double eta, double reg, double epsilon_distance,
+                 int accumulate, const f3d_pair_shape *shape,
+                 void *workspace, size_t workspace_bytes, void *stream);
+
+/* Named wrappers with the meaning of the fiber3d functions they replace. */
+
+/* replaces oseen_kernel_source_target_numba, python/kernels/kernels.py:794-846 */
+int f3d_oseen_source_target(const double *r_source, const double *r_target,
+                            const double *density, double *u,
+                            int64_t ns, int64_t nt, double eta, double reg,
+                            double epsilon_distance, int precision,
+                            void *workspace, size_t workspace_bytes, void *stream);
+
+/* replaces oseen_kernel_times_density_numba, python/kernels/kernels.py:214-287 */
+int f3d_oseen_times_density(const double *r_vectors, const double *density,
+                            double *u, int64_t n, double eta, double reg,
+                            double epsilon_distance, int precision,
+                            void *workspace, size_t workspace_bytes, void *stream);
+
+/* replaces rotlet_kernel_source_target_numba, python/kernels/kernels.py:856-908 */
+int f3d_rotlet_source_target(const double *r_source, const double *r_target,
+                             const double *density, double *u,
+                             int64_t ns, int64_t nt, double eta, double reg,
+                             double epsilon_distance, int precision,
+                             void *workspace, size_t workspace_bytes, void *stream);
+
+/* replaces stresslet_kernel_source_target_numba, python/kernels/kernels.py:1186-1217 */
+int f3d_stresslet_source_target(const double *r_source, const double *r_target,
+                                const double *normal, const double *density,
+                                double *v, int64_t ns, int64_t nt, double eta,
+                                double reg, double epsilon_distance, int precision,
+                                void *workspace, size_t workspace_bytes, void *stream);
+
+/* replaces stresslet_kernel_times_normal_times_density_numba,
+   python/kernels/kernels.py:1123-1183 */
+int f3d_stresslet_times_normal_times_density(const double *r_vectors,
+                                             const double *normal,
+                                             const double *density, double *v,
+                                             int64_t n, double eta, double reg,
+                                             double epsilon_distance, int precision,
+                                             void *workspace, size_t workspace_bytes,
+                                             void *stream);
+
+/* ---- dense operator builders (A5 and friends) ---------------------------- */
+
+/* replaces stresslet_kernel_times_normal_numba, python/kernels/kernels.py:1063-1120:
+   M (3n x 3n, row-major, leading dimension ld >= 3n) with block
+   S_ij = -3/(4 pi eta) (r.n_j)/|r|^5 r r^T, r = x_i - x_j, S_ii = 0. */
+int f3d_stresslet_times_normal_dense(const double *r_vectors, const double *normal,
+                                     double *M, int64_t n, int64_t ld, double eta,
+                                     double reg, double epsilon_distance, void *stream);
+
+/* replaces oseen_tensor (input_format 'r'), python/kernels/kernels.py:31-116:
+   G (3n x 3n, row-major, ld >= 3n), block G_ij = f(r) I + g(r) r r^T with
+   r = x_j - x_i, f = 1/(8 pi eta |r|), g = 1/(8 pi eta |r|^3); |r| <= eps is
+   regularised (so the diagonal block is I/(8 pi eta reg)). */
+int f3d_oseen_tensor_dense(const double *r_vectors, double *G, int64_t n, int64_t ld,
+                           double eta, double reg, double epsilon_distance,
+                           void *stream);
+
+/* replaces oseen_tensor_source_target (input_format 'r'),
+   python/kernels/kernels.py:119-211: G (3nt x 3ns, row-major, ld >= 3ns),
+   block G_ts from r = x_s - x_t with the regularisation of oseen_tensor. */
+int f3d_oseen_tensor_source_target_dense(const double *r_source, const double *r_target,
+                                         double *G, int64_t ns, int64_t nt, int64_t ld,
+                                         double eta, double reg, double epsilon_distance,
+                                         void *stream);
+
+/* replaces complementary_kernel, python/kernels/kernels.py:1286-1295:
+   C = outer(normal.flat, normal.flat), 3n x 3n, row-major, ld >= 3n. */
+int f3d_complementary_dense(const double *normal, double *C, int64_t n, int64_t ld,
+                            void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FIBER3D_B200_H */
