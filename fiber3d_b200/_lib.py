@@ -66,6 +66,9 @@ SIGNATURES: dict[str, list] = {
     "f3d_oseen_tensor_dense": [_P, _P, _I64, _I64, _D, _D, _D, _P],
     "f3d_oseen_tensor_source_target_dense": [_P, _P, _P, _I64, _I64, _I64, _D, _D, _D, _P],
     "f3d_complementary_dense": [_P, _P, _I64, _I64, _P],
+    "f3d_batched_lu_workspace_bytes": [ctypes.POINTER(_SZ)],
+    "f3d_batched_lu_factor": [_P, _P, _P, _P, _P, ctypes.c_int32, ctypes.c_int32, _P, _P, _P, _SZ, _P],
+    "f3d_batched_lu_solve": [_P, _P, _P, _P, _P, ctypes.c_int32, ctypes.c_int32, _P, _P, _P, _SZ, _P],
 }
 _RESTYPE = {"f3d_version": ctypes.c_char_p, "f3d_status_string": ctypes.c_char_p}
 

@@ -1,0 +1,81 @@
+"""Batched LU of uneven dense blocks on the GPU (the block-diagonal
+preconditioner of fiber3d's GMRES, tstep/tstep.py:950-994).
+
+:class:`BlockLU` packs a list of square blocks into one device buffer, factors
+them all in one persistent launch and solves them all in one launch, through
+``f3d_batched_lu_factor`` / ``f3d_batched_lu_solve``.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+import torch
+
+from . import _lib
+
+
+class BlockLU:
+    """Factors of ``len(sizes)`` square blocks stored back to back.
+
+    ``sizes`` fixes the layout; :meth:`load` (or :attr:`A` written by a device
+    kernel) fills the blocks, :meth:`factor` factors them in place and
+    :meth:`solve` solves ``block_b x_b = r_b`` for a packed right-hand side.
+    """
+
+    def __init__(self, sizes, device=None):
+        self.device = torch.device("cuda", torch.cuda.current_device()) if device is None else device
+        sizes = np.asarray(sizes, dtype=np.int64)
+        self.sizes_h = sizes
+        self.count = int(sizes.size)
+        self.max_n = int(sizes.max()) if self.count else 0
+        moff = np.concatenate([[0], np.cumsum(sizes * sizes)[:-1]]) if self.count else np.zeros(0, np.int64)
+        voff = np.concatenate([[0], np.cumsum(sizes)[:-1]]) if self.count else np.zeros(0, np.int64)
+        self.moff_h, self.voff_h = moff.astype(np.int64), voff.astype(np.int64)
+        self.nvec = int(sizes.sum())
+        dev = self.device
+        self.moff = torch.as_tensor(self.moff_h, device=dev)
+        self.voff = torch.as_tensor(self.voff_h, device=dev)
+        self.sizes = torch.as_tensor(sizes.astype(np.int32), device=dev)
+        self.order = torch.as_tensor(np.argsort(-sizes, kind="stable").astype(np.int32), device=dev)
+        self.A = torch.zeros(int((sizes * sizes).sum()), dtype=torch.float64, device=dev)
+        self.piv = torch.zeros(self.nvec, dtype=torch.int32, device=dev)
+        self.info = torch.zeros(max(self.count, 1), dtype=torch.int32, device=dev)
+        nb = ctypes.c_size_t(0)
+        _lib.call("f3d_batched_lu_workspace_bytes", ctypes.byref(nb))
+        self.ws = torch.zeros(nb.value, dtype=torch.uint8, device=dev)
+
+    def block(self, b: int) -> torch.Tensor:
+        n = int(self.sizes_h[b])
+        o = int(self.moff_h[b])
+        return self.A[o:o + n * n].view(n, n)
+
+    def load(self, blocks) -> None:
+        for b, M in enumerate(blocks):
+            self.block(b).copy_(torch.as_tensor(np.asarray(M, dtype=np.float64)))
+
+    def factor(self) -> None:
+        if self.count == 0:
+            return
+        _lib.call("f3d_batched_lu_factor", _lib.ptr(self.A), _lib.ptr(self.moff), _lib.ptr(self.voff),
+                  _lib.ptr(self.sizes), _lib.ptr(self.order), self.count, self.max_n,
+                  _lib.ptr(self.piv), _lib.ptr(self.info), _lib.ptr(self.ws), self.ws.numel(),
+                  _lib.stream_handle(self.device))
+
+    def check(self) -> None:
+        """Raise if any block had a zero pivot (synchronises)."""
+        bad = torch.nonzero(self.info[:self.count]).flatten()
+        if bad.numel():
+            b = int(bad[0])
+            raise ZeroDivisionError(f"block {b}: zero pivot at step {int(self.info[b])}")
+
+    def solve(self, x: torch.Tensor) -> torch.Tensor:
+        """Solve in place for a packed right-hand side of length sum(sizes)."""
+        if x.numel() != self.nvec or x.dtype != torch.float64 or not x.is_contiguous():
+            raise ValueError("right-hand side must be a contiguous float64 vector of length sum(sizes)")
+        if self.count:
+            _lib.call("f3d_batched_lu_solve", _lib.ptr(self.A), _lib.ptr(self.moff), _lib.ptr(self.voff),
+                      _lib.ptr(self.sizes), _lib.ptr(self.order), self.count, self.max_n,
+                      _lib.ptr(self.piv), _lib.ptr(x), _lib.ptr(self.ws), self.ws.numel(),
+                      _lib.stream_handle(self.device))
+        return x

@@ -28,6 +28,9 @@ namespace f3d {
 
 constexpr int kBlock = 128;  // threads per CTA
 constexpr int kTile = 128;   // sources per staged tile
+// Split-reduction counters: one word per target block, in a fixed region.
+constexpr int64_t kMaxCounters = 65536;
+constexpr size_t kCounterBytes = kMaxCounters * sizeof(unsigned);
 
 struct PairArgs {
   const double *rs, *rt, *dens, *nrm;
@@ -427,15 +430,22 @@ static int make_plan(int kernel, int precision, int64_t ns, int64_t nt, const f3
   int64_t tps = nfull > 0 ? (nfull + nsplit - 1) / nsplit : 0;
   if (tps > 0) nsplit = (nfull + tps - 1) / tps;
   if (nsplit < 1) nsplit = 1;
+  if (ntb > kMaxCounters) {
+    nsplit = 1;
+    tps = nfull;
+  }
   p->tpt = tpt;
   p->sl = sl;
   p->nsplit = static_cast<int>(nsplit);
   p->use_tma = (shape && shape->use_tma < 0) ? 0 : 1;
   p->ntb = ntb;
   p->tiles_per_split = tps;
+  // The counter words live in a fixed region at the start of the workspace
+  // that nothing else ever writes, so they stay zero between calls of any
+  // shape (each kernel returns the words it used to zero).
   size_t off = 0;
   p->off_counters = off;
-  if (p->nsplit > 1) off += round_up(static_cast<size_t>(ntb) * sizeof(unsigned), 256);
+  if (p->nsplit > 1) off += kCounterBytes;
   p->off_partial = off;
   if (p->nsplit > 1) off += round_up(static_cast<size_t>(p->nsplit) * nt * 3 * sizeof(double), 256);
   p->off_packed = off;

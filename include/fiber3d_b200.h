@@ -181,6 +181,34 @@ int f3d_oseen_tensor_source_target_dense(const double *r_source, const double *r
 int f3d_complementary_dense(const double *normal, double *C, int64_t n, int64_t ld,
                             void *stream);
 
+/* ---- batched LU for the block-diagonal preconditioner (A13) --------------- */
+
+/* Workspace bytes of the batched LU factor/solve (two queue counters each). */
+int f3d_batched_lu_workspace_bytes(size_t *bytes);
+
+/* Factors `count` row-major square matrices of uneven size in place, in one
+   persistent launch.  Matrix b has size sizes[b], starts at
+   A + matrix_offsets[b] (leading dimension sizes[b]); its pivots go to
+   piv + vector_offsets[b] (0-based: row i was swapped with row piv[i]) and
+   info[b] is 0 or the 1-based index of the first zero pivot.  `order`
+   (optional) is the processing order (largest first balances the queue);
+   max_n >= every size.  Replaces scipy.linalg.lu_factor per block
+   (tstep/tstep_utils.py:1405-1419 fibers, :1341-1386 bodies). */
+int f3d_batched_lu_factor(double *A, const int64_t *matrix_offsets,
+                          const int64_t *vector_offsets, const int32_t *sizes,
+                          const int32_t *order, int32_t count, int32_t max_n,
+                          int32_t *piv, int32_t *info, void *workspace,
+                          size_t workspace_bytes, void *stream);
+
+/* Solves every factored system in place: x + vector_offsets[b] holds the
+   right-hand side on entry and the solution on exit.  Replaces
+   scipy.linalg.lu_solve per block in P_inv (tstep/tstep.py:950-994). */
+int f3d_batched_lu_solve(const double *LU, const int64_t *matrix_offsets,
+                         const int64_t *vector_offsets, const int32_t *sizes,
+                         const int32_t *order, int32_t count, int32_t max_n,
+                         const int32_t *piv, double *x, void *workspace,
+                         size_t workspace_bytes, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -196,3 +196,16 @@ def test_config2_full_size_against_c_oracle(K):
     lhs = K.stresslet_kernel_source_target_numba(nodes, vol, normals, 2.0 * q - 0.5 * q2)
     rhs = 2.0 * v_vol - 0.5 * K.stresslet_kernel_source_target_numba(nodes, vol, normals, q2)
     assert rel_err(lhs, rhs) < 1e-13
+
+
+def test_workspace_reuse_across_shapes(K, L):
+    """A call that writes split partials, then a call with more target blocks
+    on the same workspace: the split counters must still start at zero."""
+    rng = np.random.default_rng(21)
+    xs = rng.random((1000, 3)); d = rng.normal(size=(1000, 3))
+    K.pair_sum("oseen", xs, rng.random((300, 3)), d, shape=L.PairShape(1, 1, 7, 0))
+    x = rng.random((700, 3)); f = rng.normal(size=(700, 3))
+    for shape in [(1, 32, 0, -1), (1, 32, 0, 0), (1, 8, 3, 0)]:
+        u = K.pair_sum("oseen", x, x, f, self_mode="skip_index", shape=L.PairShape(*shape))
+        ref = pairs_c.pair_sum("oseen", x, x, f, self_mode="skip_index")
+        assert rel_err(u.cpu().numpy(), ref) < TOL64
