@@ -27,7 +27,6 @@ import argparse
 import json
 import os
 import statistics
-import subprocess
 import sys
 import time
 from pathlib import Path
@@ -75,59 +74,72 @@ def make_workload(name: str):
 
 
 class ClockSampler:
-    """nvidia-smi clocks/throttle sampling during the timed region."""
+    """Samples SM clock, power and throttle reasons through NVML every 10 ms
+    in a background thread while the timed region runs (reads only)."""
 
-    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    REASONS = {"hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20, "hw_thermal_slowdown": 0x40,
+               "sw_power_cap": 0x4}
 
     def __init__(self, gpu_index: int):
         self.gpu = gpu_index
-        self.proc = None
-        self.path = Path(os.environ.get("TMPDIR", "/tmp")) / f"f3d_clocks_{os.getpid()}.csv"
+        self.samples = []
+        self.max_mhz = None
+        self._stop = None
+        self._thread = None
+        self.error = None
 
     def __enter__(self):
+        import threading
         try:
-            self.fh = open(self.path, "w")
-            self.proc = subprocess.Popen(
-                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
-                 "--format=csv,noheader,nounits", "-lms", "200"],
-                stdout=self.fh, stderr=subprocess.DEVNULL)
-        except (OSError, FileNotFoundError):
-            self.proc = None
+            import pynvml
+            pynvml.nvmlInit()
+            self._nvml = pynvml
+            self._h = pynvml.nvmlDeviceGetHandleByIndex(self.gpu)
+            self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(self._h, pynvml.NVML_CLOCK_SM)
+        except Exception as e:  # noqa: BLE001 - report, never fail the bench
+            self.error = f"nvml unavailable: {e}"
+            return self
+        self._stop = threading.Event()
+
+        def run():
+            nv = self._nvml
+            while not self._stop.is_set():
+                try:
+                    sm = nv.nvmlDeviceGetClockInfo(self._h, nv.NVML_CLOCK_SM)
+                    rs = nv.nvmlDeviceGetCurrentClocksEventReasons(self._h)
+                    self.samples.append((sm, rs))
+                except Exception:  # noqa: BLE001
+                    pass
+                self._stop.wait(0.01)
+
+        self._sample()
+        self._thread = threading.Thread(target=run, daemon=True)
+        self._thread.start()
         return self
 
+    def _sample(self):
+        try:
+            nv = self._nvml
+            self.samples.append((nv.nvmlDeviceGetClockInfo(self._h, nv.NVML_CLOCK_SM),
+                                 nv.nvmlDeviceGetCurrentClocksEventReasons(self._h)))
+        except Exception:  # noqa: BLE001
+            pass
+
     def __exit__(self, *exc):
-        if self.proc is not None:
-            self.proc.terminate()
-            try:
-                self.proc.wait(timeout=5)
-            except subprocess.TimeoutExpired:
-                self.proc.kill()
-            self.fh.close()
+        if self._thread is not None:
+            self._sample()
+            self._stop.set()
+            self._thread.join(timeout=2)
 
     def summary(self):
-        if self.proc is None or not self.path.exists():
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
-        sm, smax, reasons = [], [], set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in self.path.read_text().splitlines():
-            parts = [p.strip() for p in line.split(",")]
-            if len(parts) < 9:
-                continue
-            try:
-                sm.append(float(parts[1]))
-                smax.append(float(parts[2]))
-            except ValueError:
-                continue
-            for nm, v in zip(names, parts[5:9]):
-                if v.lower() == "active":
-                    reasons.add(nm)
-        self.path.unlink(missing_ok=True)
-        if not sm:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
-        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(smax), "reasons": sorted(reasons),
-                "samples": len(sm)}
+        if self.error:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [self.error]}
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": self.max_mhz, "reasons": ["no samples"]}
+        sm = [s for s, _ in self.samples]
+        reasons = sorted({k for _, r in self.samples for k, bit in self.REASONS.items() if r & bit})
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": self.max_mhz, "reasons": reasons,
+                "samples": len(sm), "source": "NVML every 10 ms during the timed region"}
 
 
 # -------------------------------------------------------------- GPU arm ---
@@ -169,9 +181,13 @@ def gpu_arm(args, rank, world, local):
     out = torch.empty(trg.numel(), dtype=torch.float64, device=dev)
     flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=dev)
 
+    from fiber3d_b200 import autotune
+    shapes = {p: autotune.tune(kind, src, trg, dens, nrm, self_mode="skip_group", src_group=gs,
+                               trg_group=gt, precision=p) for p in ("fp64", "fp32c")}
+
     def step(precision="fp64"):
         K.pair_sum(kind, src, trg, dens, nrm, self_mode="skip_group", src_group=gs, trg_group=gt,
-                   precision=precision, out=out)
+                   precision=precision, out=out, shape=shapes[precision])
 
     def timed(precision, steps, warmup):
         for _ in range(warmup):
@@ -253,6 +269,7 @@ def gpu_arm(args, rank, world, local):
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
         "config": {"workload": args.workload, "description": wl["desc"], "pairs_per_step": pairs,
                    "l2": "flushed between steps (256 MiB write, outside the event pairs)",
+                   "launch_shape": {p: [v.tpt, v.sl, v.nsplit, v.use_tma] for p, v in shapes.items()},
                    "parallelism": f"replicas x{world}"},
         "roofline": {"bound": "fp64", "achieved": achieved / 1e12, "peak": peak64 / 1e12,
                      "unit": "TFLOP/s", "frac": achieved / peak64, "traffic": None,
@@ -336,13 +353,69 @@ def reference_arm(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+def hydro_arm(args, rank, world, local):
+    """Full time step (config: 512 fibers x 32 points, 4 rigid spheres of 400
+    nodes, 12000-node periphery of radius 10; GMRES restart 100 to relative
+    residual 1e-8): assembly of the fiber systems and explicit flows, body
+    and fiber block LU, and the GMRES solve, plain FP64 and mixed precision.
+    The periphery preconditioner (explicit inverse of the dense shell
+    operator) is set-up per run and excluded, as in fiber3d (tstep.__init__)."""
+    import torch
+    from fiber3d_b200 import geometry, hydro as H
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    P = geometry.hydro_step_problem(seed=3, nshell=args.nshell, nfib=args.nfib)
+    t0 = time.perf_counter()
+    shell = H.ShellOperator(P.shell, P.eta, P.reg, P.eps_dist, dev)
+    torch.cuda.synchronize()
+    setup_s = time.perf_counter() - t0
+    out = {}
+    for mode in ("fp64", "mixed"):
+        times, its, resid = [], [], []
+        for step in range(args.warmup + args.steps):
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            sysd = H.HydroSystem(P, shell_op=shell, device=dev, tune=(step == 0))
+            res = sysd.solve(tol=1e-8, restart=100, mixed=(mode == "mixed"))
+            e1.record()
+            e1.synchronize()
+            if step >= args.warmup:
+                times.append(e0.elapsed_time(e1))
+                its.append(res["iterations"])
+                y = torch.empty_like(res["x"])
+                sysd.matvec(res["x"], y)
+                resid.append(float(torch.linalg.vector_norm(y - sysd.rhs) / torch.linalg.vector_norm(sysd.rhs)))
+            if mode == "fp64" and step == args.warmup:
+                x64 = res["x"].clone()
+            if mode == "mixed" and step == args.warmup:
+                xm = res["x"].clone()
+            del sysd
+        out[mode] = {"ms_per_step": statistics.median(times), "iterations": its[0],
+                     "true_rel_residual": max(resid), "refinements": res.get("refinements", 0)}
+    out["mixed"]["rel_diff_vs_fp64"] = float(torch.linalg.vector_norm(xm - x64) / torch.linalg.vector_norm(x64))
+    out["speedup_mixed_vs_fp64"] = out["fp64"]["ms_per_step"] / out["mixed"]["ms_per_step"]
+    line = {"metric": "hydro time step (ms), GMRES rel. residual 1e-8", "value": out["fp64"]["ms_per_step"],
+            "unit": "ms", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "higher_is_better": False, "dtype": "f64", "data": "synthetic (seeded)",
+            "config": {"workload": "hydro_step", "fibers": args.nfib, "points_per_fiber": 32,
+                       "bodies": 4, "body_nodes": 400, "shell_nodes": args.nshell,
+                       "system_size": int(3 * args.nshell + 4 * 1206 + 4 * 32 * args.nfib),
+                       "shell_setup_s": setup_s}, "step": out}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="stresslet_sphere", choices=["stresslet_sphere", "oseen_fibers"])
+    ap.add_argument("--workload", default="stresslet_sphere",
+                    choices=["stresslet_sphere", "oseen_fibers", "hydro_step"])
+    ap.add_argument("--nshell", type=int, default=12000)
+    ap.add_argument("--nfib", type=int, default=512)
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     args = ap.parse_args()
     if args.warmup < 3:
@@ -358,7 +431,10 @@ def main():
         torch.cuda.set_device(local)
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     try:
-        gpu_arm(args, rank, world, local)
+        if args.workload == "hydro_step":
+            hydro_arm(args, rank, world, local)
+        else:
+            gpu_arm(args, rank, world, local)
     finally:
         if world > 1:
             import torch.distributed as dist

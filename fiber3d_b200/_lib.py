@@ -39,6 +39,14 @@ class PairShape(ctypes.Structure):
                 ("nsplit", ctypes.c_int32), ("use_tma", ctypes.c_int32)]
 
 
+class FiberSetC(ctypes.Structure):
+    """f3d_fiber_set (device pointers)."""
+    _fields_ = [("nfib", ctypes.c_int32), ("n", ctypes.c_void_p), ("pt_off", ctypes.c_void_p),
+                ("mat_off", ctypes.c_void_p), ("res_off", ctypes.c_void_p),
+                ("length", ctypes.c_void_p), ("bc", ctypes.c_void_p), ("pt_fib", ctypes.c_void_p),
+                ("mats", ctypes.c_void_p), ("band", ctypes.c_int32)]
+
+
 _lock = threading.Lock()
 _lib = None
 
@@ -67,6 +75,26 @@ SIGNATURES: dict[str, list] = {
     "f3d_oseen_tensor_source_target_dense": [_P, _P, _P, _I64, _I64, _I64, _D, _D, _D, _P],
     "f3d_complementary_dense": [_P, _P, _I64, _I64, _P],
     "f3d_batched_lu_workspace_bytes": [ctypes.POINTER(_SZ)],
+    "f3d_singularity_vectors_workspace_bytes": [_I64, ctypes.POINTER(_SZ)],
+    "f3d_singularity_vectors": [_P, _P, _P, _P, _I64, _D, _D, _D, _P, _SZ, _P],
+    "f3d_shell_residual": [_P, _P, _P, _P, _P, _P, _I64, _P, _P],
+    "f3d_body_residual": [ctypes.c_int32, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P],
+    "f3d_surface_dense": [_I, _P, _P, _P, _P, _P, _P, _I64, _I64, _D, _D, _D, _P],
+    "f3d_gather_segments": [_P, _P, _P, _P, _P, ctypes.c_int32, _I64, _P],
+    "f3d_krylov_workspace_bytes": [_I64, ctypes.c_int32, ctypes.POINTER(_SZ)],
+    "f3d_krylov_multidot": [_P, _I64, _P, _P, ctypes.c_int32, _P, _I64, _I, _P, _SZ, _P],
+    "f3d_krylov_multiaxpy": [_P, _I64, _P, _P, _P, _I64, _P],
+    "f3d_krylov_combine": [_P, _I64, _P, ctypes.c_int32, _P, _I64, _I, _P],
+    "f3d_krylov_norm": [_P, _I64, _P, _P, _P, _P, _SZ, _P],
+    "f3d_krylov_scale_into": [_P, _P, _P, _P, _I64, _I64, _I, _P, _P],
+    "f3d_gemv": [_I, _P, _I64, _P, _P, _I64, _I64, _P],
+    "f3d_cast_to_float": [_P, _P, _I64, _P],
+    "f3d_fiber_geometry": [ctypes.POINTER(FiberSetC), _P, _P, _I64, _P],
+    "f3d_fiber_assemble": [ctypes.POINTER(FiberSetC), _D, _D, _D, _D, _D, _P, _P, _P, _P, _P, _P, _P,
+                           ctypes.c_int32, _P],
+    "f3d_fiber_forces": [ctypes.POINTER(FiberSetC), _D, _P, _P, _P, _I64, _I, _P],
+    "f3d_fiber_weight": [ctypes.POINTER(FiberSetC), _P, _P, _I64, _P],
+    "f3d_fiber_residual": [ctypes.POINTER(FiberSetC), _P, _P, _P, _P, _P, ctypes.c_int32, _P],
     "f3d_batched_lu_factor": [_P, _P, _P, _P, _P, ctypes.c_int32, ctypes.c_int32, _P, _P, _P, _SZ, _P],
     "f3d_batched_lu_solve": [_P, _P, _P, _P, _P, ctypes.c_int32, ctypes.c_int32, _P, _P, _P, _SZ, _P],
 }

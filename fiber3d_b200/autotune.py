@@ -1,0 +1,123 @@
+"""Launch-shape autotuner for the pair kernels.
+
+For a (kernel, precision, self mode, Ns bucket, Nt bucket) key it times a
+set of candidate shapes (targets per thread, source lanes per target, CTA
+count via source splits, bulk-copy staging on/off) with CUDA events on the
+current stream and keeps the fastest.  Results are cached in memory and in a
+JSON file (``$FIBER3D_B200_TUNE`` or ``~/.cache/fiber3d_b200/pair_shapes.json``)
+keyed by GPU name.  Candidates differ only in launch shape, so every one
+computes the same sum (bit-identical for a fixed split count; within
+rounding otherwise).
+"""
+from __future__ import annotations
+
+import json
+import math
+import os
+import threading
+from pathlib import Path
+
+import torch
+
+from . import _lib
+
+_lock = threading.Lock()
+_cache: dict[str, list[int]] = {}
+_loaded = False
+
+
+def _path() -> Path:
+    p = os.environ.get("FIBER3D_B200_TUNE")
+    if p:
+        return Path(p)
+    return Path.home() / ".cache" / "fiber3d_b200" / "pair_shapes.json"
+
+
+def _bucket(n: int) -> int:
+    """Power-of-two bucket of a point count."""
+    return 0 if n <= 0 else 1 << int(math.ceil(math.log2(n)))
+
+
+def _key(kernel, precision, self_mode, ns, nt) -> str:
+    name = torch.cuda.get_device_name().replace(" ", "_")
+    return f"{name}|{kernel}|{precision}|{self_mode}|{_bucket(ns)}|{_bucket(nt)}"
+
+
+def _load():
+    global _loaded
+    if _loaded:
+        return
+    _loaded = True
+    try:
+        _cache.update(json.loads(_path().read_text()))
+    except (OSError, ValueError):
+        pass
+
+
+def _save():
+    try:
+        p = _path()
+        p.parent.mkdir(parents=True, exist_ok=True)
+        tmp = p.with_suffix(".tmp")
+        tmp.write_text(json.dumps(_cache, indent=1, sort_keys=True))
+        tmp.replace(p)
+    except OSError:
+        pass
+
+
+def candidates(nt: int, sms: int):
+    """Candidate (tpt, sl, nsplit, use_tma) shapes for nt targets."""
+    out = []
+    for tpt, sl in ((1, 1), (2, 1), (1, 8), (1, 32)):
+        tpb = (128 // sl) * tpt
+        ntb = max(1, -(-nt // tpb))
+        for per_sm in (4, 8, 16):
+            nsplit = max(1, -(-per_sm * sms // ntb))
+            for tma in (0, -1):
+                out.append((tpt, sl, nsplit, tma))
+    return sorted(set(out))
+
+
+def tune(kernel: str, r_source, r_target, density, normal=None, *, self_mode="regularise",
+         src_group=None, trg_group=None, precision="fp64", eta=1.0, reg=5e-3,
+         epsilon_distance=1e-5, reps: int = 3, force: bool = False) -> _lib.PairShape:
+    """Best launch shape for this sum (times the candidates on first use)."""
+    from . import kernels as K
+    ns = int(r_source.shape[0] if hasattr(r_source, "shape") and len(r_source.shape) == 2 else len(r_source) // 3)
+    nt = int(r_target.shape[0] if hasattr(r_target, "shape") and len(r_target.shape) == 2 else len(r_target) // 3)
+    with _lock:
+        _load()
+        key = _key(kernel, precision, self_mode, ns, nt)
+        if key in _cache and not force:
+            return _lib.PairShape(*_cache[key])
+    sms = torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
+    kw = dict(self_mode=self_mode, src_group=src_group, trg_group=trg_group, precision=precision,
+              eta=eta, reg=reg, epsilon_distance=epsilon_distance)
+    out = K.pair_sum(kernel, r_source, r_target, density, normal, **kw)
+    best, best_t = None, float("inf")
+    for cand in candidates(nt, sms):
+        shp = _lib.PairShape(*cand)
+        K.pair_sum(kernel, r_source, r_target, density, normal, shape=shp, out=out, **kw)
+        torch.cuda.synchronize()
+        t = float("inf")
+        for _ in range(reps):
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record()
+            K.pair_sum(kernel, r_source, r_target, density, normal, shape=shp, out=out, **kw)
+            e1.record()
+            e1.synchronize()
+            t = min(t, e0.elapsed_time(e1))
+        if t < best_t:
+            best, best_t = cand, t
+    with _lock:
+        _cache[key] = list(best)
+        _save()
+    return _lib.PairShape(*best)
+
+
+def table() -> dict:
+    """The cached shapes (for reports)."""
+    with _lock:
+        _load()
+        return dict(_cache)

@@ -1,0 +1,301 @@
+// Device kernels of the GMRES solver that replaces scipy.sparse.linalg.gmres
+// behind bpm_utilities/gmres.py:9-111 (right preconditioning), plus the dense
+// matrix-vector product that applies the periphery preconditioner
+// (the dense LU solve of tstep/tstep.py:957-958, here an explicit inverse).
+//
+// Krylov basis V is stored row-major, one basis vector of length n per row.
+// The number of basis vectors in use, k, is read from device memory so that
+// one captured CUDA graph serves every Arnoldi step.
+//
+//   multidot:   h[i] = V[i] . w, i < k            (two stages, fixed order)
+//   multiaxpy:  w -= sum_{i<k} h[i] V[i]
+//   norm/scale: beta = |w|, V[k] = w / beta, H column written to `hcol`
+//   gemv:       y = M x for row-major M (FP64 or FP32 storage, FP64 sum)
+#include <algorithm>
+
+#include "f3d_common.cuh"
+
+namespace f3d {
+
+constexpr int kDotThreads = 256;
+constexpr int kMaxBasis = 256;  // rows of V handled by one multidot launch
+
+// Stage 1: CTA c sums rows i < k over its column chunk into part[c * kmax + i].
+__global__ void __launch_bounds__(kDotThreads) multidot_stage1(const double *__restrict__ V,
+                                                               const double *__restrict__ w,
+                                                               const int *kptr, int64_t n,
+                                                               int64_t ldv, double *part,
+                                                               int kmax) {
+  const int k = *kptr;
+  const int64_t chunk = (n + gridDim.x - 1) / gridDim.x;
+  const int64_t j0 = static_cast<int64_t>(blockIdx.x) * chunk;
+  const int64_t j1 = min(n, j0 + chunk);
+  __shared__ double red[kDotThreads / 32];
+  for (int i = 0; i < k; ++i) {
+    const double *v = V + static_cast<int64_t>(i) * ldv;
+    double s = 0.0;
+    for (int64_t j = j0 + threadIdx.x; j < j1; j += kDotThreads) s = fma(v[j], w[j], s);
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double t = 0.0;
+      for (int q = 0; q < kDotThreads / 32; ++q) t += red[q];
+      part[static_cast<int64_t>(blockIdx.x) * kmax + i] = t;
+    }
+    __syncthreads();
+  }
+}
+
+// Stage 2: h[i] (+)= sum_c part[c * kmax + i], c in order.
+__global__ void multidot_stage2(const double *part, int nparts, const int *kptr, int kmax,
+                                double *h, int accumulate) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= *kptr) return;
+  double s = 0.0;
+  for (int c = 0; c < nparts; ++c) s += part[static_cast<int64_t>(c) * kmax + i];
+  h[i] = accumulate ? h[i] + s : s;
+}
+
+// w[j] -= sum_{i<k} h[i] V[i][j]
+__global__ void multiaxpy_kernel(const double *__restrict__ V, const double *__restrict__ h,
+                                 const int *kptr, double *w, int64_t n, int64_t ldv) {
+  __shared__ double hs[kMaxBasis];
+  const int k = *kptr;
+  for (int i = threadIdx.x; i < k; i += blockDim.x) hs[i] = h[i];
+  __syncthreads();
+  for (int64_t j = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; j < n;
+       j += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    double s = w[j];
+    for (int i = 0; i < k; ++i) s = fma(-hs[i], V[static_cast<int64_t>(i) * ldv + j], s);
+    w[j] = s;
+  }
+}
+
+// Combination y[j] = sum_{i<k} c[i] V[i][j] (+ y[j] if accumulate)
+__global__ void combine_kernel(const double *__restrict__ V, const double *__restrict__ c,
+                               int k, double *y, int64_t n, int64_t ldv, int accumulate) {
+  __shared__ double cs[kMaxBasis];
+  for (int i = threadIdx.x; i < k; i += blockDim.x) cs[i] = c[i];
+  __syncthreads();
+  for (int64_t j = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; j < n;
+       j += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    double s = accumulate ? y[j] : 0.0;
+    for (int i = 0; i < k; ++i) s = fma(cs[i], V[static_cast<int64_t>(i) * ldv + j], s);
+    y[j] = s;
+  }
+}
+
+// Stage 1 of a norm: part[c] = sum over chunk of w^2.
+__global__ void __launch_bounds__(kDotThreads) sumsq_stage1(const double *__restrict__ w,
+                                                            int64_t n, double *part) {
+  const int64_t chunk = (n + gridDim.x - 1) / gridDim.x;
+  const int64_t j0 = static_cast<int64_t>(blockIdx.x) * chunk;
+  const int64_t j1 = min(n, j0 + chunk);
+  __shared__ double red[kDotThreads / 32];
+  double s = 0.0;
+  for (int64_t j = j0 + threadIdx.x; j < j1; j += kDotThreads) s = fma(w[j], w[j], s);
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int q = 0; q < kDotThreads / 32; ++q) t += red[q];
+    part[blockIdx.x] = t;
+  }
+}
+
+// beta = sqrt(sum part); writes hcol[k] = beta (the subdiagonal entry of the
+// Hessenberg column, whose first k entries the caller already holds).
+__global__ void norm_stage2(const double *part, int nparts, const int *kptr, double *hcol,
+                            double *beta_out) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  double s = 0.0;
+  for (int c = 0; c < nparts; ++c) s += part[c];
+  const double b = sqrt(s);
+  if (hcol) hcol[*kptr] = b;
+  if (beta_out) *beta_out = b;
+}
+
+// V[k] = w / beta (beta > 0; else zero), also into `also` if non-null.
+__global__ void scale_into_kernel(const double *__restrict__ w, const double *beta, int *kptr,
+                                  double *V, int64_t n, int64_t ldv, double *also) {
+  const int k = *kptr;
+  const double b = *beta;
+  const double inv = b > 0.0 ? 1.0 / b : 0.0;
+  double *dst = V + static_cast<int64_t>(k) * ldv;
+  for (int64_t j = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; j < n;
+       j += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const double v = w[j] * inv;
+    dst[j] = v;
+    if (also) also[j] = v;
+  }
+}
+
+__global__ void bump_kernel(int *kptr) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) *kptr += 1;
+}
+
+// y = M x, M row-major rows x cols.  Each warp owns kRowsPerWarp rows of a
+// group; x is staged through shared memory in chunks shared by the 32 rows of
+// the CTA's group, so M streams from HBM once and x mostly from L2.
+template <typename T>
+__global__ void __launch_bounds__(256) gemv_kernel(const T *__restrict__ M,
+                                                   const double *__restrict__ x, double *y,
+                                                   int64_t rows, int64_t cols, int64_t ld) {
+  constexpr int kXChunk = 4096;
+  constexpr int kRowsPerWarp = 4;
+  __shared__ double xs[kXChunk];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int warps = blockDim.x >> 5;
+  const int64_t group = static_cast<int64_t>(warps) * kRowsPerWarp;
+  for (int64_t rb = static_cast<int64_t>(blockIdx.x) * group; rb < rows;
+       rb += static_cast<int64_t>(gridDim.x) * group) {
+    double acc[kRowsPerWarp];
+#pragma unroll
+    for (int q = 0; q < kRowsPerWarp; ++q) acc[q] = 0.0;
+    const int64_t rw = rb + static_cast<int64_t>(warp) * kRowsPerWarp;
+    for (int64_t c0 = 0; c0 < cols; c0 += kXChunk) {
+      const int cw = static_cast<int>((cols - c0 < kXChunk) ? (cols - c0) : kXChunk);
+      __syncthreads();
+      for (int i = threadIdx.x; i < cw; i += blockDim.x) xs[i] = x[c0 + i];
+      __syncthreads();
+#pragma unroll
+      for (int q = 0; q < kRowsPerWarp; ++q) {
+        const int64_t r = rw + q;
+        if (r < rows) {
+          const T *row = M + r * ld + c0;
+          double a = acc[q];
+#pragma unroll 4
+          for (int i = lane; i < cw; i += 32) a = fma(static_cast<double>(row[i]), xs[i], a);
+          acc[q] = a;
+        }
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < kRowsPerWarp; ++q) {
+      double a = acc[q];
+#pragma unroll
+      for (int off = 16; off > 0; off >>= 1) a += __shfl_xor_sync(0xffffffffu, a, off);
+      if (lane == 0 && rw + q < rows) y[rw + q] = a;
+    }
+  }
+}
+
+__global__ void cast_to_float_kernel(const double *__restrict__ a, float *b, int64_t n) {
+  for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x)
+    b[i] = static_cast<float>(a[i]);
+}
+
+static unsigned grid_for(int64_t n, int threads) {
+  const int64_t g = (n + threads - 1) / threads;
+  const int64_t cap = static_cast<int64_t>(sm_count()) * 8;
+  return static_cast<unsigned>(std::max<int64_t>(1, std::min(g, cap)));
+}
+
+}  // namespace f3d
+
+extern "C" {
+
+int f3d_krylov_workspace_bytes(int64_t n, int32_t kmax, size_t *bytes) {
+  if (!bytes) return F3D_ERR_NULL;
+  if (n < 0 || kmax < 1 || kmax > f3d::kMaxBasis) return F3D_ERR_SHAPE;
+  const int parts = f3d::sm_count() * 2;
+  *bytes = f3d::round_up(static_cast<size_t>(parts) * (kmax + 1) * sizeof(double), 256);
+  return F3D_OK;
+}
+
+int f3d_krylov_multidot(const double *V, int64_t ldv, const double *w, const int32_t *k,
+                        int32_t kmax, double *h, int64_t n, int accumulate, void *workspace,
+                        size_t workspace_bytes, void *stream) {
+  if (!V || !w || !k || !h) return F3D_ERR_NULL;
+  if (n <= 0 || kmax < 1 || kmax > f3d::kMaxBasis || ldv < n) return F3D_ERR_SHAPE;
+  size_t need = 0;
+  f3d_krylov_workspace_bytes(n, kmax, &need);
+  if (!workspace || workspace_bytes < need) return F3D_ERR_WORKSPACE;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const int parts = std::max(1, std::min<int>(f3d::sm_count() * 2, static_cast<int>((n + 255) / 256)));
+  double *part = static_cast<double *>(workspace);
+  f3d::multidot_stage1<<<parts, f3d::kDotThreads, 0, st>>>(V, w, k, n, ldv, part, kmax);
+  int rc = f3d::launch_status();
+  if (rc) return rc;
+  f3d::multidot_stage2<<<(kmax + 127) / 128, 128, 0, st>>>(part, parts, k, kmax, h, accumulate);
+  return f3d::launch_status();
+}
+
+int f3d_krylov_multiaxpy(const double *V, int64_t ldv, const double *h, const int32_t *k,
+                         double *w, int64_t n, void *stream) {
+  if (!V || !w || !k || !h) return F3D_ERR_NULL;
+  if (n <= 0 || ldv < n) return F3D_ERR_SHAPE;
+  f3d::multiaxpy_kernel<<<f3d::grid_for(n, 256), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+      V, h, k, w, n, ldv);
+  return f3d::launch_status();
+}
+
+int f3d_krylov_combine(const double *V, int64_t ldv, const double *c, int32_t k, double *y,
+                       int64_t n, int accumulate, void *stream) {
+  if (!V || !c || !y) return F3D_ERR_NULL;
+  if (n <= 0 || ldv < n || k < 0 || k > f3d::kMaxBasis) return F3D_ERR_SHAPE;
+  f3d::combine_kernel<<<f3d::grid_for(n, 256), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+      V, c, k, y, n, ldv, accumulate);
+  return f3d::launch_status();
+}
+
+int f3d_krylov_norm(const double *w, int64_t n, const int32_t *k, double *hcol, double *beta,
+                    void *workspace, size_t workspace_bytes, void *stream) {
+  if (!w) return F3D_ERR_NULL;
+  if (n <= 0) return F3D_ERR_SHAPE;
+  if (!workspace || workspace_bytes < 256 * sizeof(double)) return F3D_ERR_WORKSPACE;
+  if (hcol && !k) return F3D_ERR_NULL;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const int parts = std::max(1, std::min<int>(256, static_cast<int>((n + 1023) / 1024)));
+  double *part = static_cast<double *>(workspace);
+  f3d::sumsq_stage1<<<parts, f3d::kDotThreads, 0, st>>>(w, n, part);
+  int rc = f3d::launch_status();
+  if (rc) return rc;
+  f3d::norm_stage2<<<1, 32, 0, st>>>(part, parts, k, hcol, beta);
+  return f3d::launch_status();
+}
+
+int f3d_krylov_scale_into(const double *w, const double *beta, int32_t *k, double *V,
+                          int64_t ldv, int64_t n, int bump, double *also, void *stream) {
+  if (!w || !beta || !k || !V) return F3D_ERR_NULL;
+  if (n <= 0 || ldv < n) return F3D_ERR_SHAPE;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  f3d::scale_into_kernel<<<f3d::grid_for(n, 256), 256, 0, st>>>(w, beta, k, V, n, ldv, also);
+  int rc = f3d::launch_status();
+  if (rc || !bump) return rc;
+  f3d::bump_kernel<<<1, 32, 0, st>>>(k);
+  return f3d::launch_status();
+}
+
+int f3d_gemv(int precision, const void *M, int64_t ld, const double *x, double *y, int64_t rows,
+             int64_t cols, void *stream) {
+  if (!M || !x || !y) return F3D_ERR_NULL;
+  if (rows < 0 || cols < 0 || ld < cols) return F3D_ERR_SHAPE;
+  if (rows == 0) return F3D_OK;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const unsigned grid = static_cast<unsigned>(std::max<int64_t>(
+      1, std::min<int64_t>((rows + 31) / 32, static_cast<int64_t>(f3d::sm_count()) * 4)));
+  if (precision == F3D_FP64)
+    f3d::gemv_kernel<double><<<grid, 256, 0, st>>>(static_cast<const double *>(M), x, y, rows, cols, ld);
+  else if (precision == F3D_FP32C)
+    f3d::gemv_kernel<float><<<grid, 256, 0, st>>>(static_cast<const float *>(M), x, y, rows, cols, ld);
+  else
+    return F3D_ERR_ARG;
+  return f3d::launch_status();
+}
+
+int f3d_cast_to_float(const double *a, float *b, int64_t n, void *stream) {
+  if (!a || !b) return F3D_ERR_NULL;
+  if (n < 0) return F3D_ERR_SHAPE;
+  if (n == 0) return F3D_OK;
+  f3d::cast_to_float_kernel<<<f3d::grid_for(n, 256), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+      a, b, n);
+  return f3d::launch_status();
+}
+
+}  // extern "C"

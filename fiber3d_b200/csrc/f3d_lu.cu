@@ -301,14 +301,29 @@ static size_t factor_smem(int nb, int max_n) {
   return (static_cast<size_t>(max_n) * nb + static_cast<size_t>(nb) * kChunk) * sizeof(double);
 }
 
+// Raises a kernel's dynamic shared-memory limit to the opt-in maximum once
+// per device (a host-side attribute, so later launches and stream captures
+// need no further runtime calls).
+template <typename K>
+static int allow_max_smem(K kernel, bool (&done)[64]) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return F3D_ERR_CUDA;
+  if (done[dev]) return F3D_OK;
+  int optin = 0;
+  if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess)
+    return F3D_ERR_CUDA;
+  if (cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, optin) != cudaSuccess)
+    return F3D_ERR_CUDA;
+  done[dev] = true;
+  return F3D_OK;
+}
+
 template <int NB>
 static int launch_factor(const LuArgs &a, int max_n, cudaStream_t st) {
   const size_t smem = factor_smem(NB, max_n);
   auto k = batched_lu_factor_kernel<NB>;
-  if (smem > 48 * 1024 &&
-      cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)) !=
-          cudaSuccess)
-    return F3D_ERR_CUDA;
+  static bool done[64] = {false};
+  if (allow_max_smem(k, done)) return F3D_ERR_CUDA;
   int per_sm = 0;
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kLuThreads, smem) != cudaSuccess ||
       per_sm < 1)
@@ -358,10 +373,8 @@ int f3d_batched_lu_solve(const double *LU, const int64_t *matrix_offsets,
   const size_t smem = static_cast<size_t>(f3d::kSolveWarps) * max_n * sizeof(double);
   if (smem > 200 * 1024) return F3D_ERR_TOO_LARGE;
   auto k = f3d::batched_lu_solve_kernel;
-  if (smem > 48 * 1024 &&
-      cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)) !=
-          cudaSuccess)
-    return F3D_ERR_CUDA;
+  static bool done[64] = {false};
+  if (f3d::allow_max_smem(k, done)) return F3D_ERR_CUDA;
   int per_sm = 0;
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, f3d::kSolveWarps * 32, smem) !=
           cudaSuccess ||

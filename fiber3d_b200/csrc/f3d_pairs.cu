@@ -69,6 +69,24 @@ constexpr size_t pair_smem_bytes() {
   return 128 + 2 * Stage<KIND, MODE, PREC>::bytes;
 }
 
+// 1/sqrt(x) in FP64: the hardware approximation (PTX rsqrt.approx.ftz.f64,
+// about 2^-22 relative error) refined by one third-order Householder
+// (Halley-type) step y1 = y0 (1 + e/2 + 3e^2/8), e = 1 - x y0^2, whose error
+// is O(e^3) — below double rounding for any seed better than 2^-18.
+__device__ __forceinline__ double rsqrt_refined(double x) {
+  double y;
+  asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
+  const double e = fma(-x * y, y, 1.0);
+  return fma(y * e, fma(0.375, e, 0.5), y);
+}
+
+// r2 + reg2 when r2 < eps2 (r2 >= 0): the comparison is made on the IEEE bit
+// patterns (ordered like the values for non-negative doubles) so it runs on
+// the integer pipe, leaving the FP64 pipe to the arithmetic.
+__device__ __forceinline__ double regularise(double r2, long long eps2_bits, double reg2) {
+  return r2 + ((__double_as_longlong(r2) < eps2_bits) ? reg2 : 0.0);
+}
+
 __device__ __forceinline__ void two_sum(float &s, float &c, float x) {
   const float t = s + x;
   const float bp = t - s;
@@ -125,7 +143,8 @@ __global__ void __launch_bounds__(kBlock) pair_kernel(const PairArgs a) {
 #pragma unroll
     for (int c = 0; c < 3; ++c) { acc[k][c] = 0.0; fs[k][c] = 0.f; fc[k][c] = 0.f; ft[k][c] = 0.f; }
 
-  const double eps2 = a.eps2, reg2 = a.reg2;
+  const double reg2 = a.reg2;
+  const long long eps2_bits = __double_as_longlong(a.eps2);
   const float eps2f = static_cast<float>(a.eps2), reg2f = static_cast<float>(a.reg2);
 
   // ---- one tile of `cnt` sources starting at global index `sbase` --------
@@ -144,9 +163,8 @@ __global__ void __launch_bounds__(kBlock) pair_kernel(const PairArgs a) {
 #pragma unroll
         for (int k = 0; k < TPT; ++k) {
           const double dx = txd[k] - sx, dy = tyd[k] - sy, dz = tzd[k] - sz;
-          double r2 = fma(dx, dx, fma(dy, dy, dz * dz));
-          r2 = (r2 < eps2) ? r2 + reg2 : r2;
-          double ri = rsqrt(r2);
+          const double r2 = regularise(fma(dx, dx, fma(dy, dy, dz * dz)), eps2_bits, reg2);
+          double ri = rsqrt_refined(r2);
           if (MODE == F3D_SELF_SKIP_INDEX) ri = (sbase + s == tidx[k]) ? 0.0 : ri;
           if (MODE == F3D_SELF_SKIP_GROUP) ri = (sg == tgrp[k]) ? 0.0 : ri;
           if (KIND == F3D_KERNEL_OSEEN) {
@@ -422,7 +440,7 @@ static int make_plan(int kernel, int precision, int64_t ns, int64_t nt, const f3
   const int64_t nfull = ns / kTile;
   int64_t nsplit = shape && shape->nsplit > 0 ? shape->nsplit : 0;
   if (nsplit == 0) {
-    const int64_t want = 4LL * sm_count();
+    const int64_t want = 8LL * sm_count();
     nsplit = ntb > 0 ? (want + ntb - 1) / ntb : 1;
   }
   nsplit = std::max<int64_t>(1, std::min<int64_t>(nsplit, std::max<int64_t>(nfull, 1)));

@@ -1,0 +1,315 @@
+// Surface operators: the periphery (shell) double layer with singularity
+// subtraction and its null-space correction, rigid-body rows, and their
+// dense preconditioner blocks.
+//
+// Reference (fiber3d, python/):
+//   singularity-subtraction vectors e_x, e_y, e_z   periphery/periphery.py:75-98,
+//                                                   body/body.py:325-346
+//   shell operator M = S - I_E - diag(1/w) (+ n n^T) tstep/tstep.py:327-351
+//   its application in the matvec                   tstep/tstep.py:1097-1104
+//   body rows: -E mu - K U + v ; -K^T lambda + U    tstep/tstep.py:1118-1143
+//   body preconditioner block                       tstep/tstep_utils.py:1341-1386
+// Unknown q = the weighted double-layer density (x_all slice); mu = q / w.
+// E is stored per node as a 3x3 row-major matrix E[i][a][c] = e_c(i)_a.
+#include <algorithm>
+
+#include "f3d_common.cuh"
+
+namespace f3d {
+
+int pair_sum_impl(int kernel, int precision, int self_mode, const double *rs, const double *rt,
+                  const double *dens, const double *nrm, const int32_t *gs, const int32_t *gt,
+                  double *out, int64_t ns, int64_t nt, double eta, double reg, double eps,
+                  int accumulate, const f3d_pair_shape *shape, void *ws, size_t ws_bytes,
+                  cudaStream_t st);
+
+__global__ void unit_density_kernel(const double *w, double *dens, int64_t n, int c) {
+  const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  dens[3 * i + 0] = (c == 0) ? w[i] : 0.0;
+  dens[3 * i + 1] = (c == 1) ? w[i] : 0.0;
+  dens[3 * i + 2] = (c == 2) ? w[i] : 0.0;
+}
+
+__global__ void scatter_column_kernel(const double *col, double *E, int64_t n, int c) {
+  const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+#pragma unroll
+  for (int a = 0; a < 3; ++a) E[9 * i + 3 * a + c] = col[3 * i + a];
+}
+
+// s = sum_j n_j . q_j, one CTA, fixed reduction order.
+__global__ void __launch_bounds__(1024) normal_dot_kernel(const double *nrm, const double *q,
+                                                          int64_t n, double *s) {
+  __shared__ double red[32];
+  double acc = 0.0;
+  for (int64_t i = threadIdx.x; i < n; i += blockDim.x)
+    acc += nrm[3 * i] * q[3 * i] + nrm[3 * i + 1] * q[3 * i + 1] + nrm[3 * i + 2] * q[3 * i + 2];
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    double v = (threadIdx.x < (blockDim.x >> 5)) ? red[threadIdx.x] : 0.0;
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+    if (threadIdx.x == 0) *s = v;
+  }
+}
+
+// res_i = v_i - E_i mu_i - mu_i + n_i s   (mu = q / w)
+__global__ void shell_residual_kernel(const double *__restrict__ v, const double *__restrict__ E,
+                                      const double *__restrict__ w, const double *__restrict__ nrm,
+                                      const double *__restrict__ q, const double *__restrict__ s,
+                                      double *res, int64_t n) {
+  const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double inv = 1.0 / w[i];
+  const double mu[3] = {q[3 * i] * inv, q[3 * i + 1] * inv, q[3 * i + 2] * inv};
+  const double ss = *s;
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    const double *e = E + 9 * i + 3 * a;
+    res[3 * i + a] = v[3 * i + a] - (e[0] * mu[0] + e[1] * mu[1] + e[2] * mu[2]) - mu[a] + nrm[3 * i + a] * ss;
+  }
+}
+
+// One CTA per body.  x_b = [lambda (3nb), U (3), Omega (3)].
+__global__ void __launch_bounds__(256) body_residual_kernel(
+    const int64_t *node_off, const int64_t *x_off, const double *__restrict__ nodes,
+    const double *__restrict__ center, const double *__restrict__ E, const double *__restrict__ w,
+    const double *__restrict__ v, const double *__restrict__ x, double *res) {
+  const int b = blockIdx.x;
+  const int64_t i0 = node_off[b], i1 = node_off[b + 1];
+  const int64_t xo = x_off[b];
+  const int64_t nb = i1 - i0;
+  const double *lam = x + xo;
+  const double *U = x + xo + 3 * nb;
+  const double cx = center[3 * b], cy = center[3 * b + 1], cz = center[3 * b + 2];
+  double f[6] = {0, 0, 0, 0, 0, 0};
+  for (int64_t k = threadIdx.x; k < nb; k += blockDim.x) {
+    const int64_t i = i0 + k;
+    const double r[3] = {nodes[3 * i] - cx, nodes[3 * i + 1] - cy, nodes[3 * i + 2] - cz};
+    const double l[3] = {lam[3 * k], lam[3 * k + 1], lam[3 * k + 2]};
+    const double inv = 1.0 / w[i];
+    const double mu[3] = {l[0] * inv, l[1] * inv, l[2] * inv};
+    // K U = U + Omega x r
+    const double ku[3] = {U[0] + U[4] * r[2] - U[5] * r[1], U[1] + U[5] * r[0] - U[3] * r[2],
+                          U[2] + U[3] * r[1] - U[4] * r[0]};
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      const double *e = E + 9 * i + 3 * a;
+      res[xo + 3 * k + a] = v[3 * i + a] - (e[0] * mu[0] + e[1] * mu[1] + e[2] * mu[2]) - ku[a];
+    }
+    // K^T lambda = [sum lambda, sum r x lambda]
+    f[0] += l[0]; f[1] += l[1]; f[2] += l[2];
+    f[3] += r[1] * l[2] - r[2] * l[1];
+    f[4] += r[2] * l[0] - r[0] * l[2];
+    f[5] += r[0] * l[1] - r[1] * l[0];
+  }
+  __shared__ double red[6][8];
+#pragma unroll
+  for (int c = 0; c < 6; ++c) {
+    double a = f[c];
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) a += __shfl_xor_sync(0xffffffffu, a, off);
+    if ((threadIdx.x & 31) == 0) red[c][threadIdx.x >> 5] = a;
+  }
+  __syncthreads();
+  if (threadIdx.x < 6) {
+    double a = 0.0;
+    for (int wi = 0; wi < static_cast<int>(blockDim.x >> 5); ++wi) a += red[threadIdx.x][wi];
+    res[xo + 3 * nb + threadIdx.x] = -a + U[threadIdx.x];
+  }
+}
+
+// Dense surface operator block: rows/cols 3n (+6 for a rigid body).
+// mode 0 (shell): M = S - blockdiag(E_i/w_i + I/w_i) + n n^T
+// mode 1 (body):  [[S - blockdiag(E_i/w_i), -K], [-K^T, I6]]
+__global__ void surface_dense_kernel(const double *__restrict__ x, const double *__restrict__ nrm,
+                                     const double *__restrict__ E, const double *__restrict__ w,
+                                     const double *center, double *M, int64_t n, int64_t ld,
+                                     double factor, double eps2, double reg2, int mode) {
+  const int64_t j = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  const int64_t i = blockIdx.y;
+  const int64_t nc = (mode == 1) ? n + 2 : n;  // column blocks (2 extra for U, Omega)
+  if (j >= nc) return;
+  if (i >= n) {
+    // rigid-body rows: -K^T for column blocks j < n, identity on U, Omega
+    const int64_t rb = i - n;  // 0: force rows (U), 1: torque rows (Omega)
+    double *row = M + 3 * i * ld + 3 * j;
+    if (j < n) {
+      const double r[3] = {x[3 * j] - center[0], x[3 * j + 1] - center[1], x[3 * j + 2] - center[2]};
+      // -K^T: force rows -I; torque rows -(r x .) as a matrix
+      const double T[3][3] = {{0.0, -r[2], r[1]}, {r[2], 0.0, -r[0]}, {-r[1], r[0], 0.0}};
+#pragma unroll
+      for (int a = 0; a < 3; ++a)
+#pragma unroll
+        for (int b = 0; b < 3; ++b) row[a * ld + b] = (rb == 0) ? -(a == b ? 1.0 : 0.0) : -T[a][b];
+    } else {
+#pragma unroll
+      for (int a = 0; a < 3; ++a)
+#pragma unroll
+        for (int b = 0; b < 3; ++b) row[a * ld + b] = (j - n == rb && a == b) ? 1.0 : 0.0;
+    }
+    return;
+  }
+  double *row = M + 3 * i * ld + 3 * j;
+  if (j >= n) {
+    // -K columns: U columns -I, Omega columns -(Omega x r) = -rot_i
+    const double r[3] = {x[3 * i] - center[0], x[3 * i + 1] - center[1], x[3 * i + 2] - center[2]};
+    const double rot[3][3] = {{0.0, r[2], -r[1]}, {-r[2], 0.0, r[0]}, {r[1], -r[0], 0.0}};
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+      for (int b = 0; b < 3; ++b) row[a * ld + b] = (j == n) ? -(a == b ? 1.0 : 0.0) : -rot[a][b];
+    return;
+  }
+  double blk[3][3];
+  if (i == j) {
+    const double inv = 1.0 / w[i];
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+      for (int b = 0; b < 3; ++b)
+        blk[a][b] = -E[9 * i + 3 * a + b] * inv - ((mode == 0 && a == b) ? inv : 0.0);
+  } else {
+    const double r[3] = {x[3 * i] - x[3 * j], x[3 * i + 1] - x[3 * j + 1], x[3 * i + 2] - x[3 * j + 2]};
+    double r2 = r[0] * r[0] + r[1] * r[1] + r[2] * r[2];
+    if (r2 < eps2) r2 += reg2;
+    const double rn = sqrt(r2);
+    const double rdn = r[0] * nrm[3 * j] + r[1] * nrm[3 * j + 1] + r[2] * nrm[3 * j + 2];
+    const double s = factor * rdn / (rn * rn * rn * rn * rn);
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+      for (int b = 0; b < 3; ++b) blk[a][b] = s * r[a] * r[b];
+  }
+  if (mode == 0) {
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+      for (int b = 0; b < 3; ++b) blk[a][b] += nrm[3 * i + a] * nrm[3 * j + b];
+  }
+#pragma unroll
+  for (int a = 0; a < 3; ++a)
+#pragma unroll
+    for (int b = 0; b < 3; ++b) row[a * ld + b] = blk[a][b];
+}
+
+// dst[seg_dst[s] + k] = src[seg_src[s] + k], k < seg_len[s]
+__global__ void gather_segments_kernel(const double *__restrict__ src, double *dst,
+                                       const int64_t *seg_src, const int64_t *seg_dst,
+                                       const int64_t *seg_len, int nseg) {
+  const int s = blockIdx.y;
+  if (s >= nseg) return;
+  const int64_t len = seg_len[s];
+  for (int64_t k = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; k < len;
+       k += static_cast<int64_t>(gridDim.x) * blockDim.x)
+    dst[seg_dst[s] + k] = src[seg_src[s] + k];
+}
+
+}  // namespace f3d
+
+extern "C" {
+
+int f3d_singularity_vectors_workspace_bytes(int64_t n, size_t *bytes) {
+  if (!bytes) return F3D_ERR_NULL;
+  if (n < 0) return F3D_ERR_SHAPE;
+  size_t pw = 0;
+  int rc = f3d_pair_workspace_bytes(F3D_KERNEL_STRESSLET, F3D_FP64, n, n, nullptr, &pw);
+  if (rc) return rc;
+  *bytes = f3d::round_up(static_cast<size_t>(n) * 6 * sizeof(double), 256) + pw;
+  return F3D_OK;
+}
+
+int f3d_singularity_vectors(const double *nodes, const double *normals, const double *weights,
+                            double *E, int64_t n, double eta, double reg, double epsilon_distance,
+                            void *workspace, size_t workspace_bytes, void *stream) {
+  if (n < 0) return F3D_ERR_SHAPE;
+  if (n == 0) return F3D_OK;
+  if (!nodes || !normals || !weights || !E) return F3D_ERR_NULL;
+  size_t need = 0;
+  int rc = f3d_singularity_vectors_workspace_bytes(n, &need);
+  if (rc) return rc;
+  if (!workspace || workspace_bytes < need) return F3D_ERR_WORKSPACE;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  double *dens = static_cast<double *>(workspace);
+  double *col = dens + 3 * n;
+  const size_t head = f3d::round_up(static_cast<size_t>(n) * 6 * sizeof(double), 256);
+  unsigned char *pws = static_cast<unsigned char *>(workspace) + head;
+  const unsigned nb = static_cast<unsigned>((n + 255) / 256);
+  for (int c = 0; c < 3; ++c) {
+    f3d::unit_density_kernel<<<nb, 256, 0, st>>>(weights, dens, n, c);
+    if ((rc = f3d::launch_status())) return rc;
+    rc = f3d::pair_sum_impl(F3D_KERNEL_STRESSLET, F3D_FP64, F3D_SELF_SKIP_INDEX, nodes, nodes, dens,
+                            normals, nullptr, nullptr, col, n, n, eta, reg, epsilon_distance, 0,
+                            nullptr, pws, workspace_bytes - head, st);
+    if (rc) return rc;
+    f3d::scatter_column_kernel<<<nb, 256, 0, st>>>(col, E, n, c);
+    if ((rc = f3d::launch_status())) return rc;
+  }
+  return F3D_OK;
+}
+
+int f3d_shell_residual(const double *v, const double *E, const double *weights,
+                       const double *normals, const double *q, double *res, int64_t n,
+                       double *scratch, void *stream) {
+  if (n < 0) return F3D_ERR_SHAPE;
+  if (n == 0) return F3D_OK;
+  if (!v || !E || !weights || !normals || !q || !res || !scratch) return F3D_ERR_NULL;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  f3d::normal_dot_kernel<<<1, 1024, 0, st>>>(normals, q, n, scratch);
+  int rc = f3d::launch_status();
+  if (rc) return rc;
+  f3d::shell_residual_kernel<<<static_cast<unsigned>((n + 255) / 256), 256, 0, st>>>(
+      v, E, weights, normals, q, scratch, res, n);
+  return f3d::launch_status();
+}
+
+int f3d_body_residual(int32_t nbody, const int64_t *node_off, const int64_t *x_off,
+                      const double *nodes, const double *centers, const double *E,
+                      const double *weights, const double *v, const double *x, double *res,
+                      void *stream) {
+  if (nbody < 0) return F3D_ERR_SHAPE;
+  if (nbody == 0) return F3D_OK;
+  if (!node_off || !x_off || !nodes || !centers || !E || !weights || !v || !x || !res)
+    return F3D_ERR_NULL;
+  f3d::body_residual_kernel<<<nbody, 256, 0, static_cast<cudaStream_t>(stream)>>>(
+      node_off, x_off, nodes, centers, E, weights, v, x, res);
+  return f3d::launch_status();
+}
+
+int f3d_surface_dense(int mode, const double *nodes, const double *normals, const double *E,
+                      const double *weights, const double *center, double *M, int64_t n,
+                      int64_t ld, double eta, double reg, double epsilon_distance, void *stream) {
+  if (mode != 0 && mode != 1) return F3D_ERR_ARG;
+  const int64_t dim = (mode == 1) ? 3 * n + 6 : 3 * n;
+  if (n < 0 || ld < dim) return F3D_ERR_SHAPE;
+  if (n == 0) return F3D_OK;
+  if (!nodes || !normals || !E || !weights || !M || (mode == 1 && !center)) return F3D_ERR_NULL;
+  const int64_t rows = (mode == 1) ? n + 2 : n;
+  if (rows > 65535) return F3D_ERR_TOO_LARGE;
+  const int64_t cols = rows;
+  dim3 grid(static_cast<unsigned>((cols + 127) / 128), static_cast<unsigned>(rows));
+  f3d::surface_dense_kernel<<<grid, 128, 0, static_cast<cudaStream_t>(stream)>>>(
+      nodes, normals, E, weights, center, M, n, ld, -3.0 / (4.0 * f3d::kPi * eta),
+      epsilon_distance * epsilon_distance, reg * reg, mode);
+  return f3d::launch_status();
+}
+
+int f3d_gather_segments(const double *src, double *dst, const int64_t *seg_src,
+                        const int64_t *seg_dst, const int64_t *seg_len, int32_t nseg,
+                        int64_t max_len, void *stream) {
+  if (nseg < 0 || max_len < 0) return F3D_ERR_SHAPE;
+  if (nseg == 0 || max_len == 0) return F3D_OK;
+  if (!src || !dst || !seg_src || !seg_dst || !seg_len) return F3D_ERR_NULL;
+  if (nseg > 65535) return F3D_ERR_TOO_LARGE;
+  const unsigned gx = static_cast<unsigned>(std::min<int64_t>((max_len + 255) / 256, 1024));
+  dim3 grid(gx, static_cast<unsigned>(nseg));
+  f3d::gather_segments_kernel<<<grid, 256, 0, static_cast<cudaStream_t>(stream)>>>(
+      src, dst, seg_src, seg_dst, seg_len, nseg);
+  return f3d::launch_status();
+}
+
+}  // extern "C"

@@ -126,3 +126,31 @@ def stresslet_sphere_workload(seed: int = 2, n: int = 12000, radius: float = 10.
     mu = rng.normal(size=(n, 3))
     vol = uniform_ball(rng, n_vol, vol_radius)
     return nodes, normals, w, mu, vol
+
+
+def hydro_step_problem(seed: int = 3, nfib: int = 512, npts=32, nbody: int = 4,
+                       body_nodes: int = 400, nshell: int = 12000, shell_radius: float = 10.0,
+                       length: float = 2.0, E: float = 0.0025, dt: float = 1e-3, eta: float = 1.0,
+                       force_std: float = 0.1, fiber_ball: float = 5.0, body_shell: float = 7.5):
+    """Full-step workload: `nfib` fibers (equispaced nodes, straight + 3
+    transverse modes of amplitude 0.05, centres uniform in a ball of radius
+    5), `nbody` rigid spheres of radius 0.5 (Fibonacci nodes, equal weights,
+    random orientation, centres at radius `body_shell`), a spherical periphery
+    of `nshell` nodes (inward normals as fiber3d uses them, equal weights
+    4 pi R^2 / N), and a constant external force N(0, force_std) per fiber."""
+    from .hydro import Body, Problem, Shell, quaternion_rotation
+    rng = _rng(seed)
+    fibers = perturbed_fibers(rng, nfib, npts, length, fiber_ball)
+    counts = [f.shape[0] for f in fibers]
+    ff = np.concatenate([np.tile(rng.normal(scale=force_std, size=3), (n, 1)) for n in counts])
+    bn, bnn = fibonacci_sphere(body_nodes, 0.5)
+    bw = np.full(body_nodes, 4.0 * np.pi * 0.25 / body_nodes)
+    bodies = []
+    dirs = uniform_directions(rng, nbody)
+    for k in range(nbody):
+        q = rng.normal(size=4)
+        q /= np.linalg.norm(q)
+        bodies.append(Body(body_shell * dirs[k], quaternion_rotation(q), bn, bnn, bw))
+    sn, snn = fibonacci_sphere(nshell, shell_radius)
+    sw = np.full(nshell, 4.0 * np.pi * shell_radius**2 / nshell)
+    return Problem(fibers, [length] * nfib, E, dt, eta, bodies, Shell(sn, -snn, sw), ff)

@@ -1,0 +1,237 @@
+"""Right-preconditioned restarted GMRES on the device, and mixed-precision
+iterative refinement around it.
+
+Replaces ``bpm_utilities/gmres.py:9-111`` (scipy.sparse.linalg.gmres on
+A P^-1 y = b, then x = P^-1 y) as called at ``tstep/tstep.py:1209-1216``.
+
+Arnoldi runs on the device: one step is ``z = P^-1 v_k``, ``w = A z``,
+classical Gram-Schmidt applied twice (CGS2) against the basis, ``|w|`` and
+``v_{k+1} = w / |w|`` — every vector stays in HBM and every reduction has a
+fixed order.  That step can be captured once as a CUDA graph (the basis
+count lives in device memory) and replayed for every k.  The Hessenberg
+column (k+2 numbers) comes back to the host each step, where the Givens
+rotations and the residual estimate are updated in FP64, as scipy does.
+Convergence uses the residual estimate, and is confirmed by a true residual
+``|b - A x| / |b|`` before returning (a restart follows otherwise).
+
+Mixed precision (``solve_system(mixed=True)``): outer iterative refinement
+with FP64 residuals ``r = b - A x``; each correction is an inner GMRES solve
+whose matvec uses the compensated-FP32 pair kernels (Arnoldi, Givens and the
+true residual stay FP64); the loop stops on the FP64 relative residual.
+"""
+from __future__ import annotations
+
+import ctypes
+import time
+
+import numpy as np
+import torch
+
+from . import _lib
+
+
+class DeviceGMRES:
+    """GMRES workspace for systems of size n with restart length m."""
+
+    def __init__(self, n: int, restart: int = 100, device=None):
+        dev = device or torch.device("cuda", torch.cuda.current_device())
+        self.device = dev
+        self.n, self.m = n, int(restart)
+        if self.m + 1 > 256:
+            raise ValueError("restart must be <= 255")
+        f = lambda *s: torch.zeros(*s, dtype=torch.float64, device=dev)
+        self.V = f(self.m + 1, n)
+        self.cur = f(n)      # current basis vector (input of the Arnoldi step)
+        self.z = f(n)
+        self.w = f(n)
+        self.h1 = f(self.m + 2)
+        self.h2 = f(self.m + 2)
+        self.beta = f(1)
+        self.k = torch.zeros(1, dtype=torch.int32, device=dev)
+        nb = ctypes.c_size_t(0)
+        _lib.call("f3d_krylov_workspace_bytes", n, self.m + 1, ctypes.byref(nb))
+        self.ws = torch.zeros(max(nb.value, 4096), dtype=torch.uint8, device=dev)
+        self.wsn = torch.zeros(4096, dtype=torch.uint8, device=dev)
+        self.h_host = torch.zeros(2 * (self.m + 2) + 1, dtype=torch.float64).pin_memory()
+        self.graph = {}
+
+    # ------------------------------------------------------------ kernels --
+    def _norm(self, w, beta):
+        st = _lib.stream_handle(self.device)
+        _lib.call("f3d_krylov_norm", _lib.ptr(w), self.n, None, None, _lib.ptr(beta), _lib.ptr(self.wsn),
+                  self.wsn.numel(), st)
+
+    def _arnoldi(self, matvec, pc):
+        """One Arnoldi step on the current stream (graph-capturable)."""
+        st = _lib.stream_handle(self.device)
+        n, ldv = self.n, self.n
+        pc(self.cur, self.z)
+        matvec(self.z, self.w)
+        for h in (self.h1, self.h2):
+            _lib.call("f3d_krylov_multidot", _lib.ptr(self.V), ldv, _lib.ptr(self.w), _lib.ptr(self.k),
+                      self.m + 1, _lib.ptr(h), n, 0, _lib.ptr(self.ws), self.ws.numel(), st)
+            _lib.call("f3d_krylov_multiaxpy", _lib.ptr(self.V), ldv, _lib.ptr(h), _lib.ptr(self.k),
+                      _lib.ptr(self.w), n, st)
+        _lib.call("f3d_krylov_norm", _lib.ptr(self.w), n, _lib.ptr(self.k), _lib.ptr(self.h1),
+                  _lib.ptr(self.beta), _lib.ptr(self.wsn), self.wsn.numel(), st)
+        _lib.call("f3d_krylov_scale_into", _lib.ptr(self.w), _lib.ptr(self.beta), _lib.ptr(self.k),
+                  _lib.ptr(self.V), ldv, n, 1, _lib.ptr(self.cur), st)
+        m2 = self.m + 2
+        self.h_host[:m2].copy_(self.h1, non_blocking=True)
+        self.h_host[m2:2 * m2].copy_(self.h2, non_blocking=True)
+
+    def _step(self, matvec, pc, key, use_graph):
+        if not use_graph:
+            self._arnoldi(matvec, pc)
+            return
+        g = self.graph.get(key)
+        if g is None:
+            # warm-up outside capture on a side stream (allocations, lazy init)
+            s = torch.cuda.Stream(self.device)
+            s.wait_stream(torch.cuda.current_stream(self.device))
+            with torch.cuda.stream(s):
+                saved = (self.k.clone(), self.cur.clone(), self.V.clone())
+                self._arnoldi(matvec, pc)
+                self.k.copy_(saved[0]); self.cur.copy_(saved[1]); self.V.copy_(saved[2])
+            torch.cuda.current_stream(self.device).wait_stream(s)
+            g = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(g):
+                self._arnoldi(matvec, pc)
+            self.graph[key] = g
+        self.graph[key].replay()
+
+    # ------------------------------------------------------------- solve ---
+    def solve(self, matvec, pc, b: torch.Tensor, x0: torch.Tensor | None = None, rtol=1e-8,
+              maxiter=200, use_graph=True, key="default", bnorm=None):
+        """Solve A x = b with right preconditioner pc = P^-1.
+
+        Returns (x, info, iterations, history of relative residual estimates).
+        info = 0 on convergence, else the iteration count reached.
+        """
+        n, m = self.n, self.m
+        dev = self.device
+        x = torch.zeros(n, dtype=torch.float64, device=dev) if x0 is None else x0.clone()
+        r = torch.empty(n, dtype=torch.float64, device=dev)
+        tmp = torch.empty(n, dtype=torch.float64, device=dev)
+        if bnorm is None:
+            self._norm(b, self.beta)
+            bnorm = float(self.beta.item())
+        if bnorm == 0.0:
+            return torch.zeros_like(b), 0, 0, [0.0]
+        its, hist = 0, []
+        while True:
+            # r = b - A x
+            if x0 is None and its == 0:
+                r.copy_(b)
+            else:
+                matvec(x, tmp)
+                torch.sub(b, tmp, out=r)
+            self._norm(r, self.beta)
+            rnorm = float(self.beta.item())
+            hist.append(rnorm / bnorm)
+            if rnorm <= rtol * bnorm:
+                return x, 0, its, hist
+            if its >= maxiter:
+                return x, its, its, hist
+            # V[0] = r / |r|, cur = V[0], k = 1
+            self.k.zero_()
+            st = _lib.stream_handle(dev)
+            _lib.call("f3d_krylov_scale_into", _lib.ptr(r), _lib.ptr(self.beta), _lib.ptr(self.k),
+                      _lib.ptr(self.V), n, n, 1, _lib.ptr(self.cur), st)
+            H = np.zeros((m + 1, m))
+            cs, sn = np.zeros(m), np.zeros(m)
+            g = np.zeros(m + 1)
+            g[0] = rnorm
+            j_done = 0
+            for j in range(m):
+                self._step(matvec, pc, key, use_graph)
+                torch.cuda.current_stream(dev).synchronize()
+                hh = self.h_host.numpy()
+                m2 = m + 2
+                col = hh[:j + 1] + hh[m2:m2 + j + 1]
+                col = np.append(col, hh[j + 1])          # subdiagonal |w|
+                for i in range(j):
+                    t = cs[i] * col[i] + sn[i] * col[i + 1]
+                    col[i + 1] = -sn[i] * col[i] + cs[i] * col[i + 1]
+                    col[i] = t
+                den = np.hypot(col[j], col[j + 1])
+                if den == 0.0:
+                    cs[j], sn[j] = 1.0, 0.0
+                else:
+                    cs[j], sn[j] = col[j] / den, col[j + 1] / den
+                col[j] = den
+                col[j + 1] = 0.0
+                g[j + 1] = -sn[j] * g[j]
+                g[j] = cs[j] * g[j]
+                H[:j + 1, j] = col[:j + 1]
+                its += 1
+                j_done = j + 1
+                est = abs(g[j + 1]) / bnorm
+                hist.append(est)
+                if est <= rtol or its >= maxiter or hh[j + 1] == 0.0:
+                    break
+            # y = H^-1 g ; x += P^-1 (V y)
+            y = np.zeros(j_done)
+            for i in range(j_done - 1, -1, -1):
+                y[i] = (g[i] - H[i, i + 1:j_done] @ y[i + 1:j_done]) / H[i, i]
+            yd = torch.as_tensor(y, device=dev)
+            _lib.call("f3d_krylov_combine", _lib.ptr(self.V), n, _lib.ptr(yd), j_done, _lib.ptr(tmp), n, 0,
+                      _lib.stream_handle(dev))
+            pc(tmp, r)
+            x += r
+
+
+def solve_system(system, tol=1e-8, restart=100, maxiter=200, x0=None, mixed=False,
+                 inner_tol=1e-5, max_refine=10, use_graph=True):
+    """Solve system.matvec x = system.rhs to relative residual `tol`.
+
+    Returns a dict with the solution and statistics.
+    """
+    dev = system.device
+    n = system.size
+    g = getattr(system, "_gmres", None)
+    if g is None or g.n != n or g.m != restart:
+        g = DeviceGMRES(n, restart, dev)
+        system._gmres = g
+    b = system.rhs
+    t0 = time.perf_counter()
+    if not mixed:
+        x, info, its, hist = g.solve(lambda a, o: system.matvec(a, o, "fp64"),
+                                     lambda a, o: system.pc(a, o, "fp64"), b, x0=x0, rtol=tol,
+                                     maxiter=maxiter, use_graph=use_graph, key="fp64")
+        torch.cuda.synchronize()
+        return {"x": x, "info": info, "iterations": its, "history": hist, "refinements": 0,
+                "seconds": time.perf_counter() - t0}
+    # mixed: FP64 outer residuals, FP32-compensated inner matvecs
+    x = torch.zeros(n, dtype=torch.float64, device=dev) if x0 is None else x0.clone()
+    r = torch.empty(n, dtype=torch.float64, device=dev)
+    tmp = torch.empty(n, dtype=torch.float64, device=dev)
+    g._norm(b, g.beta)
+    bnorm = float(g.beta.item())
+    total_its, hist, ref = 0, [], 0
+    info = 0
+    while True:
+        if x0 is None and ref == 0:
+            r.copy_(b)
+        else:
+            system.matvec(x, tmp, "fp64")
+            torch.sub(b, tmp, out=r)
+        g._norm(r, g.beta)
+        rel = float(g.beta.item()) / bnorm
+        hist.append(rel)
+        if rel <= tol:
+            break
+        if ref >= max_refine or total_its >= maxiter:
+            info = total_its
+            break
+        # inner tolerance relative to |r|: never ask beyond what is needed
+        inner = max(inner_tol, 0.5 * tol / rel)
+        d, _, its, _ = g.solve(lambda a, o: system.matvec(a, o, "fp32c"),
+                               lambda a, o: system.pc(a, o, "fp32c"), r, rtol=inner,
+                               maxiter=maxiter - total_its, use_graph=use_graph, key="fp32c")
+        total_its += its
+        x += d
+        ref += 1
+    torch.cuda.synchronize()
+    return {"x": x, "info": info, "iterations": total_its, "history": hist, "refinements": ref,
+            "seconds": time.perf_counter() - t0}

@@ -1,0 +1,395 @@
+"""One implicit hydrodynamic time step of fiber3d, device-resident.
+
+Mirrors ``tstep.time_step_hydro`` (python/tstep/tstep.py:628-1458) for free
+fibers, rigid bodies and a confining periphery:
+
+* unknown layout (tstep_utils.get_num_particles_and_offsets :906-931)
+  ``[shell q (3 Nsh) | body k: lambda (3 Nb_k), U, Omega | fiber k: X_x, X_y, X_z, T]``;
+* right-hand side: explicit flows of the external fiber forces
+  (tstep.py:789-846) and the fiber systems (tstep_utils.py:1238-1338);
+* matvec ``A_body_fiber_hyd`` (tstep.py:1003-1178);
+* block preconditioner ``P_inv`` (tstep.py:950-994): explicit inverse of the
+  dense periphery operator (computed once per periphery), batched LU of the
+  body and fiber blocks.
+
+All sums run in the library's pair kernels.  The matvec is two pair launches
+— Oseen from the fiber points (pairs within one fiber skipped, which fuses
+``flow_fibers`` and ``self_flow_fibers``) and one stresslet launch from the
+body and periphery nodes together — onto every point, then three row
+kernels (periphery, bodies, fibers).  ``precision='fp32c'`` runs both pair
+launches in compensated FP32 for the inner solves of mixed precision.
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass, field
+
+import numpy as np
+import torch
+
+from . import _lib
+from .blocklu import BlockLU
+from .fibers import FiberSet
+
+
+@dataclass
+class Body:
+    """Rigid body surface: reference nodes/normals rotated by `rotation` and
+    shifted to `location`; quadrature `weights`."""
+    location: np.ndarray
+    rotation: np.ndarray
+    ref_nodes: np.ndarray
+    ref_normals: np.ndarray
+    weights: np.ndarray
+
+    @property
+    def nodes(self):
+        return np.asarray(self.ref_nodes) @ np.asarray(self.rotation).T + np.asarray(self.location)
+
+    @property
+    def normals(self):
+        return np.asarray(self.ref_normals) @ np.asarray(self.rotation).T
+
+
+@dataclass
+class Shell:
+    nodes: np.ndarray
+    normals: np.ndarray
+    weights: np.ndarray
+
+
+@dataclass
+class Problem:
+    """Inputs of one time step (fiber3d defaults: epsilon 1e-3, penalty 500,
+    reg 5e-3, epsilon_distance 1e-5)."""
+    fibers: list
+    lengths: list
+    E: float
+    dt: float
+    eta: float = 1.0
+    bodies: list = field(default_factory=list)
+    shell: Shell | None = None
+    force_fibers: np.ndarray | None = None
+    epsilon: float = 1e-3
+    penalty: float = 500.0
+    reg: float = 5e-3
+    eps_dist: float = 1e-5
+
+    def mobility(self):
+        c0 = -np.log(np.e * self.epsilon ** 2) / (8.0 * np.pi * self.eta)
+        c1 = 2.0 / (8.0 * np.pi * self.eta)
+        return c0, c1
+
+
+def quaternion_rotation(q) -> np.ndarray:
+    """Rotation matrix of the unit quaternion (s, p1, p2, p3)."""
+    s, p = float(q[0]), np.asarray(q[1:4], dtype=np.float64)
+    d = s * s - 0.5
+    return 2.0 * np.array([[p[0] ** 2 + d, p[0] * p[1] - s * p[2], p[0] * p[2] + s * p[1]],
+                           [p[1] * p[0] + s * p[2], p[1] ** 2 + d, p[1] * p[2] - s * p[0]],
+                           [p[2] * p[0] - s * p[1], p[2] * p[1] + s * p[0], p[2] ** 2 + d]])
+
+
+class ShellOperator:
+    """Device data of a periphery: nodes, normals, weights, singularity
+    vectors E and the explicit inverse of the dense shell operator (FP64, and
+    an FP32 copy for mixed precision).  Built once per periphery."""
+
+    def __init__(self, shell: Shell, eta=1.0, reg=5e-3, eps_dist=1e-5, device=None,
+                 build_inverse=True):
+        dev = device or torch.device("cuda", torch.cuda.current_device())
+        self.device = dev
+        t = lambda a: torch.as_tensor(np.ascontiguousarray(a, dtype=np.float64), device=dev)
+        self.nodes = t(np.asarray(shell.nodes).reshape(-1, 3))
+        self.normals = t(np.asarray(shell.normals).reshape(-1, 3))
+        self.weights = t(np.asarray(shell.weights).reshape(-1))
+        self.n = self.nodes.shape[0]
+        self.eta, self.reg, self.eps = eta, reg, eps_dist
+        self.E = singularity_vectors(self.nodes, self.normals, self.weights, eta, reg, eps_dist)
+        self.inv64 = None
+        self.inv32 = None
+        if build_inverse:
+            self.build_inverse()
+
+    def dense(self) -> torch.Tensor:
+        m = 3 * self.n
+        M = torch.empty((m, m), dtype=torch.float64, device=self.device)
+        _lib.call("f3d_surface_dense", 0, _lib.ptr(self.nodes), _lib.ptr(self.normals), _lib.ptr(self.E),
+                  _lib.ptr(self.weights), None, _lib.ptr(M), self.n, m, self.eta, self.reg, self.eps,
+                  _lib.stream_handle(self.device))
+        return M
+
+    def build_inverse(self):
+        """Explicit inverse of the dense shell operator (one-time set-up; the
+        LU factorisation itself is cuSOLVER's via torch.linalg)."""
+        M = self.dense()
+        self.inv64 = torch.linalg.inv(M)
+        del M
+        self.inv32 = torch.empty(self.inv64.shape, dtype=torch.float32, device=self.device)
+        _lib.call("f3d_cast_to_float", _lib.ptr(self.inv64), _lib.ptr(self.inv32), self.inv64.numel(),
+                  _lib.stream_handle(self.device))
+
+
+def singularity_vectors(nodes, normals, weights, eta, reg, eps) -> torch.Tensor:
+    n = nodes.shape[0]
+    E = torch.empty((n, 9), dtype=torch.float64, device=nodes.device)
+    nb = ctypes.c_size_t(0)
+    _lib.call("f3d_singularity_vectors_workspace_bytes", n, ctypes.byref(nb))
+    ws = torch.zeros(max(nb.value, 1), dtype=torch.uint8, device=nodes.device)
+    _lib.call("f3d_singularity_vectors", _lib.ptr(nodes), _lib.ptr(normals), _lib.ptr(weights),
+              _lib.ptr(E), n, eta, reg, eps, _lib.ptr(ws), ws.numel(), _lib.stream_handle(nodes.device))
+    return E
+
+
+class _PairCall:
+    """A pre-planned pair-sum launch with fixed device pointers (so that it
+    can be captured in a CUDA graph)."""
+
+    def __init__(self, kernel, mode, src, trg, dens, nrm, gs, gt, out, eta, reg, eps, shape=None):
+        self.args = dict(kernel=kernel, mode=mode, src=src, trg=trg, dens=dens, nrm=nrm, gs=gs, gt=gt,
+                         out=out, eta=eta, reg=reg, eps=eps)
+        self.shape = {p: shape for p in ("fp64", "fp32c")}
+        self.ws = {}
+
+    def set_shape(self, precision, shape):
+        self.shape[precision] = shape
+
+    def _ws(self, precision):
+        a = self.args
+        key = precision
+        shp = self.shape.get(precision)
+        nb = ctypes.c_size_t(0)
+        _lib.call("f3d_pair_workspace_bytes", _lib.KERNEL[a["kernel"]], _lib.PRECISION[precision],
+                  a["src"].shape[0], a["trg"].shape[0], ctypes.byref(shp) if shp else None, ctypes.byref(nb))
+        cur = self.ws.get(key)
+        if cur is None or cur.numel() < nb.value:
+            cur = torch.zeros(max(nb.value, 256), dtype=torch.uint8, device=a["out"].device)
+            self.ws[key] = cur
+        return cur
+
+    def __call__(self, precision="fp64", accumulate=False):
+        a = self.args
+        ws = self._ws(precision)
+        shp = self.shape.get(precision)
+        _lib.call("f3d_pair_sum", _lib.KERNEL[a["kernel"]], _lib.PRECISION[precision],
+                  _lib.SELF_MODE[a["mode"]], _lib.ptr(a["src"]), _lib.ptr(a["trg"]), _lib.ptr(a["dens"]),
+                  _lib.ptr(a["nrm"]), _lib.ptr(a["gs"]), _lib.ptr(a["gt"]), _lib.ptr(a["out"]),
+                  a["src"].shape[0], a["trg"].shape[0], a["eta"], a["reg"], a["eps"], int(accumulate),
+                  ctypes.byref(shp) if shp else None, _lib.ptr(ws), ws.numel(),
+                  _lib.stream_handle(a["out"].device))
+
+
+class HydroSystem:
+    """Device linear system of one time step: ``rhs``, :meth:`matvec`,
+    :meth:`pc` (the right preconditioner P^-1) and :meth:`solve`."""
+
+    def __init__(self, problem: Problem, shell_op: ShellOperator | None = None, device=None,
+                 tune: bool = False):
+        self.p = problem
+        dev = device or torch.device("cuda", torch.cuda.current_device())
+        self.device = dev
+        st = lambda: _lib.stream_handle(dev)
+        f64 = lambda a: torch.as_tensor(np.ascontiguousarray(a, dtype=np.float64), device=dev)
+        P = problem
+        self.c0, self.c1 = P.mobility()
+        # ---- fibers
+        self.fs = FiberSet(P.fibers, P.lengths, device=dev)
+        nF = self.fs.total
+        self.nF = nF
+        self.x_fib = f64(np.concatenate(P.fibers) if P.fibers else np.zeros((0, 3)))
+        ff = P.force_fibers if P.force_fibers is not None else np.zeros((nF, 3))
+        self.force = f64(np.asarray(ff).reshape(-1, 3))
+        self.has_force = bool(np.any(ff))
+        self.geo = torch.empty((max(nF, 1), 9), dtype=torch.float64, device=dev)
+        if nF:
+            _lib.call("f3d_fiber_geometry", ctypes.byref(self.fs.c), _lib.ptr(self.x_fib), _lib.ptr(self.geo), nF, st())
+        # ---- bodies
+        self.nbody = len(P.bodies)
+        nb = [np.asarray(b.ref_nodes).reshape(-1, 3).shape[0] for b in P.bodies]
+        self.nb = nb
+        self.body_node_off_h = np.concatenate([[0], np.cumsum(nb)]).astype(np.int64)
+        nB = int(self.body_node_off_h[-1])
+        self.nB = nB
+        if self.nbody:
+            self.body_nodes = f64(np.concatenate([b.nodes for b in P.bodies]))
+            self.body_normals = f64(np.concatenate([b.normals for b in P.bodies]))
+            self.body_w = f64(np.concatenate([np.asarray(b.weights).reshape(-1) for b in P.bodies]))
+            self.body_centers = f64(np.stack([np.asarray(b.location, dtype=np.float64) for b in P.bodies]))
+            self.body_E = torch.empty((nB, 9), dtype=torch.float64, device=dev)
+            for k in range(self.nbody):
+                a, b = self.body_node_off_h[k], self.body_node_off_h[k + 1]
+                self.body_E[a:b] = singularity_vectors(self.body_nodes[a:b], self.body_normals[a:b],
+                                                       self.body_w[a:b], P.eta, P.reg, P.eps_dist)
+        # ---- shell
+        if P.shell is not None:
+            self.shell = shell_op or ShellOperator(P.shell, P.eta, P.reg, P.eps_dist, dev)
+            nS = self.shell.n
+        else:
+            self.shell = None
+            nS = 0
+        self.nS = nS
+        # ---- layout
+        self.o_body = [3 * nS + 3 * int(self.body_node_off_h[k]) + 6 * k for k in range(self.nbody)]
+        self.o_fib = 3 * nS + 3 * nB + 6 * self.nbody
+        self.size = self.o_fib + 4 * nF
+        self.x_off_body = torch.as_tensor(np.array(self.o_body, dtype=np.int64), device=dev) if self.nbody else None
+        self.body_node_off = torch.as_tensor(self.body_node_off_h, device=dev)
+        # ---- targets: [fibers; bodies; shell]
+        parts = [self.x_fib]
+        if self.nbody:
+            parts.append(self.body_nodes)
+        if self.shell is not None:
+            parts.append(self.shell.nodes)
+        self.trg = torch.cat(parts).contiguous()
+        self.ntrg = self.trg.shape[0]
+        grp = np.concatenate([np.repeat(np.arange(self.fs.nfib), self.fs.npts),
+                              -np.ones(self.ntrg - nF)]).astype(np.int32)
+        self.trg_grp = torch.as_tensor(grp, device=dev)
+        self.src_grp = self.trg_grp[:nF].contiguous()
+        # stresslet sources: [body nodes; shell nodes]
+        sp, sn = [], []
+        if self.nbody:
+            sp.append(self.body_nodes); sn.append(self.body_normals)
+        if self.shell is not None:
+            sp.append(self.shell.nodes); sn.append(self.shell.normals)
+        self.nstress = nB + nS
+        if self.nstress:
+            self.stress_nodes = torch.cat(sp).contiguous()
+            self.stress_normals = torch.cat(sn).contiguous()
+            self.stress_dens = torch.zeros((self.nstress, 3), dtype=torch.float64, device=dev)
+            seg_src, seg_dst, seg_len = [], [], []
+            for k in range(self.nbody):
+                seg_src.append(self.o_body[k]); seg_dst.append(3 * int(self.body_node_off_h[k])); seg_len.append(3 * nb[k])
+            if nS:
+                seg_src.append(0); seg_dst.append(3 * nB); seg_len.append(3 * nS)
+            self.seg = [torch.as_tensor(np.array(a, dtype=np.int64), device=dev) for a in (seg_src, seg_dst, seg_len)]
+            self.seg_max = max(seg_len)
+        # ---- work buffers
+        self.v = torch.zeros(3 * self.ntrg, dtype=torch.float64, device=dev)
+        self.fw = torch.zeros((max(nF, 1), 3), dtype=torch.float64, device=dev)
+        self.scratch = torch.zeros(4, dtype=torch.float64, device=dev)
+        self.oseen = _PairCall("oseen", "skip_group", self.x_fib, self.trg, self.fw, None, self.src_grp,
+                               self.trg_grp, self.v, P.eta, P.reg, P.eps_dist) if nF else None
+        self.stress = _PairCall("stresslet", "regularise", self.stress_nodes, self.trg, self.stress_dens,
+                                self.stress_normals, None, None, self.v, P.eta, P.reg, P.eps_dist) \
+            if self.nstress else None
+        if tune:
+            self.autotune()
+        # ---- right-hand side and preconditioner blocks
+        self.rhs = torch.zeros(self.size, dtype=torch.float64, device=dev)
+        sizes = [3 * n + 6 for n in nb] + list(4 * self.fs.npts)
+        self.lu = BlockLU(sizes, device=dev)
+        self.A_fib = torch.zeros(max(self.fs.mat_total, 1), dtype=torch.float64, device=dev)
+        self._assemble()
+
+    # ------------------------------------------------------------------------
+    def autotune(self):
+        from . import autotune as at
+        P = self.p
+        for call, kind in ((self.oseen, "oseen"), (self.stress, "stresslet")):
+            if call is None:
+                continue
+            a = call.args
+            for prec in ("fp64", "fp32c"):
+                shp = at.tune(kind, a["src"], a["trg"], a["dens"], a["nrm"], self_mode=a["mode"],
+                              src_group=a["gs"], trg_group=a["gt"], precision=prec, eta=P.eta,
+                              reg=P.reg, epsilon_distance=P.eps_dist)
+                call.set_shape(prec, shp)
+
+    def _assemble(self):
+        P = self.p
+        dev = self.device
+        st = _lib.stream_handle(dev)
+        nF, nB, nS = self.nF, self.nB, self.nS
+        # explicit flow of the external fiber forces (tstep.py:789-821)
+        self.v.zero_()
+        if nF and self.has_force:
+            _lib.call("f3d_fiber_weight", ctypes.byref(self.fs.c), _lib.ptr(self.force), _lib.ptr(self.fw), nF, st)
+            self.oseen("fp64")
+        v = self.v.view(-1, 3)
+        if nS:
+            self.rhs[:3 * nS] = -v[nF + nB:].reshape(-1)
+        for k in range(self.nbody):
+            a, b = int(self.body_node_off_h[k]), int(self.body_node_off_h[k + 1])
+            self.rhs[self.o_body[k]:self.o_body[k] + 3 * (b - a)] = -v[nF + a:nF + b].reshape(-1)
+        flow = v[:nF].contiguous() if nF else v[:1]
+        # fiber blocks into A_fib and (a copy) into the LU buffer after the body blocks
+        if nF:
+            lu_fib0 = int(self.lu.moff_h[self.nbody]) if self.lu.count else 0
+            A_copy = self.lu.A.data_ptr() + 8 * lu_fib0
+            _lib.call("f3d_fiber_assemble", ctypes.byref(self.fs.c), P.E, P.dt, self.c0, self.c1, P.penalty,
+                      _lib.ptr(self.x_fib), _lib.ptr(self.geo), _lib.ptr(flow), _lib.ptr(self.force),
+                      _lib.ptr(self.A_fib), A_copy, _lib.ptr(self.rhs[self.o_fib:]), self.fs.max_n, st)
+        for k in range(self.nbody):
+            a, b = int(self.body_node_off_h[k]), int(self.body_node_off_h[k + 1])
+            n = b - a
+            _lib.call("f3d_surface_dense", 1, _lib.ptr(self.body_nodes[a:b]), _lib.ptr(self.body_normals[a:b]),
+                      _lib.ptr(self.body_E[a:b]), _lib.ptr(self.body_w[a:b]), _lib.ptr(self.body_centers[k]),
+                      _lib.ptr(self.lu.block(k)), n, 3 * n + 6, P.eta, P.reg, P.eps_dist, st)
+        self.lu.factor()
+
+    # ------------------------------------------------------------------------
+    def matvec(self, x: torch.Tensor, y: torch.Tensor, precision: str = "fp64") -> torch.Tensor:
+        """y = A x (tstep.py:1003-1178)."""
+        st = _lib.stream_handle(self.device)
+        nF, nB, nS = self.nF, self.nB, self.nS
+        XT = x[self.o_fib:]
+        first = True
+        if nF:
+            _lib.call("f3d_fiber_forces", ctypes.byref(self.fs.c), self.p.E, _lib.ptr(self.geo), _lib.ptr(XT),
+                      _lib.ptr(self.fw), nF, 1, st)
+            self.oseen(precision, accumulate=False)
+            first = False
+        if self.nstress:
+            _lib.call("f3d_gather_segments", _lib.ptr(x), _lib.ptr(self.stress_dens), _lib.ptr(self.seg[0]),
+                      _lib.ptr(self.seg[1]), _lib.ptr(self.seg[2]), self.seg[0].numel(), self.seg_max, st)
+            self.stress(precision, accumulate=not first)
+            first = False
+        if first:
+            self.v.zero_()
+        v = self.v
+        if nS:
+            _lib.call("f3d_shell_residual", _lib.ptr(v[3 * (nF + nB):]), _lib.ptr(self.shell.E),
+                      _lib.ptr(self.shell.weights), _lib.ptr(self.shell.normals), _lib.ptr(x), _lib.ptr(y),
+                      nS, _lib.ptr(self.scratch), st)
+        if self.nbody:
+            _lib.call("f3d_body_residual", self.nbody, _lib.ptr(self.body_node_off), _lib.ptr(self.x_off_body),
+                      _lib.ptr(self.body_nodes), _lib.ptr(self.body_centers), _lib.ptr(self.body_E),
+                      _lib.ptr(self.body_w), _lib.ptr(v[3 * nF:]), _lib.ptr(x), _lib.ptr(y), st)
+        if nF:
+            _lib.call("f3d_fiber_residual", ctypes.byref(self.fs.c), _lib.ptr(self.A_fib), _lib.ptr(self.geo),
+                      _lib.ptr(XT), _lib.ptr(v), _lib.ptr(y[self.o_fib:]), self.fs.max_n, st)
+        return y
+
+    def pc(self, x: torch.Tensor, y: torch.Tensor, precision: str = "fp64") -> torch.Tensor:
+        """y = P^-1 x (tstep.py:950-994)."""
+        st = _lib.stream_handle(self.device)
+        nS = self.nS
+        if nS:
+            M = self.shell.inv64 if precision == "fp64" else self.shell.inv32
+            _lib.call("f3d_gemv", _lib.PRECISION[precision], _lib.ptr(M), 3 * nS, _lib.ptr(x), _lib.ptr(y),
+                      3 * nS, 3 * nS, st)
+        if self.size > 3 * nS:
+            rest = y[3 * nS:]
+            rest.copy_(x[3 * nS:])
+            self.lu.solve(rest)
+        return y
+
+    def solve(self, tol=1e-8, restart=100, maxiter=200, x0=None, mixed=False, **kw):
+        from .gmres import solve_system
+        return solve_system(self, tol=tol, restart=restart, maxiter=maxiter, x0=x0, mixed=mixed, **kw)
+
+    # ---------------------------------------------------------------- layout --
+    def split(self, sol: torch.Tensor):
+        """Solution blocks: shell density, per body (lambda, U, Omega), per
+        fiber (X (N,3), T (N,))."""
+        out = {"shell": sol[:3 * self.nS].view(-1, 3) if self.nS else None, "bodies": [], "fibers": []}
+        for k in range(self.nbody):
+            o, n = self.o_body[k], self.nb[k]
+            out["bodies"].append((sol[o:o + 3 * n].view(-1, 3), sol[o + 3 * n:o + 3 * n + 3], sol[o + 3 * n + 3:o + 3 * n + 6]))
+        for k in range(self.fs.nfib):
+            n = int(self.fs.npts[k])
+            o = self.o_fib + 4 * int(self.fs.pt_off_h[k])
+            blk = sol[o:o + 4 * n]
+            out["fibers"].append((blk[:3 * n].view(3, n).t(), blk[3 * n:]))
+        return out

@@ -209,6 +209,145 @@ int f3d_batched_lu_solve(const double *LU, const int64_t *matrix_offsets,
                          const int32_t *piv, double *x, void *workspace,
                          size_t workspace_bytes, void *stream);
 
+/* ---- fiber discretisation (A11, A12) ------------------------------------ */
+
+/* A set of fibers on the device.  Points of all fibers are concatenated;
+   fiber f has n[f] points starting at point pt_off[f], its 4n x 4n operator
+   block at mat_off[f] (row-major) and its unknowns [X_x, X_y, X_z, T] at
+   4*pt_off[f].  `mats` holds, per resolution N, the block
+   [D1_0, D2_0, D3_0, D4_0 (N x N each, finite differences on
+   alpha = linspace(-1,1,N)), P_X ((N-4) x N), P_T ((N-2) x N), w0 (N)]
+   (tstep/fiber_matrices.py:38-104); res_off[f] is the offset of fiber f's
+   block.  bc holds 4 codes per fiber (start translation, start rotation,
+   end translation, end rotation): 0 force, 1 torque, 2 velocity,
+   3 angular_velocity.  band = half-width of the finite-difference stencils
+   (n_fd + 3). */
+typedef struct f3d_fiber_set {
+  int32_t nfib;
+  const int32_t *n;
+  const int64_t *pt_off;
+  const int64_t *mat_off;
+  const int64_t *res_off;
+  const double *length;
+  const int32_t *bc;
+  const int32_t *pt_fib;   /* fiber index of every point */
+  const double *mats;
+  int32_t band;
+} f3d_fiber_set;
+
+/* geo[9p..9p+8] = (xs, xss, xsss) at every point p (D_k x, tstep.py:703-709). */
+int f3d_fiber_geometry(const f3d_fiber_set *set, const double *x, double *geo,
+                       int64_t npts, void *stream);
+
+/* Per-fiber [P_cheb A; B] and [P_cheb RHS; B_RHS]: fiber.form_linear_operator,
+   compute_RHS and apply_BC_rectangular (fiber/fiber.py:322-448, 473-582,
+   810-961) with flow = background velocity on the fiber and force = external
+   force per point.  Writes the blocks to A (and A_copy if non-NULL). */
+int f3d_fiber_assemble(const f3d_fiber_set *set, double E, double dt, double c0,
+                       double c1, double penalty, const double *x, const double *geo,
+                       const double *flow, const double *force, double *A,
+                       double *A_copy, double *rhs, int32_t max_n, void *stream);
+
+/* fw = w * (-E X_ssss + xss T + xs T_s) from the fiber unknowns XT
+   (fiber.force_operator, fiber/fiber.py:1399-1432, times the trapezoid
+   weights of flow_fibers, tstep_utils.py:653-700, when weighted != 0). */
+int f3d_fiber_forces(const f3d_fiber_set *set, double E, const double *geo,
+                     const double *XT, double *fw, int64_t npts, int weighted,
+                     void *stream);
+
+/* fw = w * f: external point forces times the trapezoid weights. */
+int f3d_fiber_weight(const f3d_fiber_set *set, const double *f, double *fw,
+                     int64_t npts, void *stream);
+
+/* Fiber rows of the matvec: res = A XT - [P_cheb [v; xs . D1 v]; 0]
+   (tstep/tstep.py:1147-1173) with v the velocity on the fiber points. */
+int f3d_fiber_residual(const f3d_fiber_set *set, const double *A, const double *geo,
+                       const double *XT, const double *v, double *res, int32_t max_n,
+                       void *stream);
+
+/* ---- surfaces: periphery (shell) and rigid bodies (A7, body rows) ------- */
+
+/* Workspace bytes of f3d_singularity_vectors for n nodes. */
+int f3d_singularity_vectors_workspace_bytes(int64_t n, size_t *bytes);
+
+/* Singularity-subtraction vectors e_c(i) = sum_{j != i} S_ij w_j e_c of one
+   surface (periphery.get_singularity_subtraction_vectors,
+   periphery/periphery.py:75-98; body.calc_vectors_singularity_subtraction,
+   body/body.py:325-346), stored as E[9i + 3a + c] = e_c(i)_a. */
+int f3d_singularity_vectors(const double *nodes, const double *normals,
+                            const double *weights, double *E, int64_t n, double eta,
+                            double reg, double epsilon_distance, void *workspace,
+                            size_t workspace_bytes, void *stream);
+
+/* Shell rows of the matvec (tstep/tstep.py:1097-1104 with the matrices of
+   tstep.py:327-347): res_i = v_i - E_i mu_i - mu_i + n_i sum_j n_j.q_j,
+   mu = q / w, where v already holds the double-layer sum of q (and every
+   other source) at the shell nodes.  `scratch` is one device double. */
+int f3d_shell_residual(const double *v, const double *E, const double *weights,
+                       const double *normals, const double *q, double *res, int64_t n,
+                       double *scratch, void *stream);
+
+/* Rigid-body rows of the matvec (tstep/tstep.py:1118-1143): for body b with
+   unknowns x[x_off[b]..] = [lambda (3nb), U, Omega]:
+   res = v - E mu - (U + Omega x r) on the nodes and -K^T lambda + (U, Omega). */
+int f3d_body_residual(int32_t nbody, const int64_t *node_off, const int64_t *x_off,
+                      const double *nodes, const double *centers, const double *E,
+                      const double *weights, const double *v, const double *x, double *res,
+                      void *stream);
+
+/* Dense preconditioner block of a surface.  mode 0 (periphery, 3n x 3n):
+   S - blockdiag(E_i/w_i + I/w_i) + n n^T (tstep/tstep.py:327-347).
+   mode 1 (rigid body, (3n+6)^2): [[S - blockdiag(E_i/w_i), -K], [-K^T, I]]
+   (tstep/tstep_utils.py:1341-1386), K = [I, rot] about `center`. */
+int f3d_surface_dense(int mode, const double *nodes, const double *normals, const double *E,
+                      const double *weights, const double *center, double *M, int64_t n,
+                      int64_t ld, double eta, double reg, double epsilon_distance,
+                      void *stream);
+
+/* dst[seg_dst[s] + k] = src[seg_src[s] + k] for k < seg_len[s] (max_len >= all). */
+int f3d_gather_segments(const double *src, double *dst, const int64_t *seg_src,
+                        const int64_t *seg_dst, const int64_t *seg_len, int32_t nseg,
+                        int64_t max_len, void *stream);
+
+/* ---- Krylov (GMRES) building blocks (A14) and the dense preconditioner ---- */
+/* Replace scipy.sparse.linalg.gmres behind bpm_utilities/gmres.py:9-111.
+   V is the Krylov basis, row-major, one vector of length n per row (ldv >= n).
+   `k` points to a device int32: the number of basis rows in use, so that one
+   captured CUDA graph serves every Arnoldi step.  kmax <= 256. */
+
+int f3d_krylov_workspace_bytes(int64_t n, int32_t kmax, size_t *bytes);
+
+/* h[i] (+)= V[i] . w for i < *k (two stages, fixed summation order). */
+int f3d_krylov_multidot(const double *V, int64_t ldv, const double *w, const int32_t *k,
+                        int32_t kmax, double *h, int64_t n, int accumulate,
+                        void *workspace, size_t workspace_bytes, void *stream);
+
+/* w -= sum_{i < *k} h[i] V[i]. */
+int f3d_krylov_multiaxpy(const double *V, int64_t ldv, const double *h, const int32_t *k,
+                         double *w, int64_t n, void *stream);
+
+/* y (+)= sum_{i < k} c[i] V[i] (k given by value). */
+int f3d_krylov_combine(const double *V, int64_t ldv, const double *c, int32_t k, double *y,
+                       int64_t n, int accumulate, void *stream);
+
+/* *beta = |w|_2; if hcol is non-NULL also hcol[*k] = |w|_2.  Workspace >= 2 KiB. */
+int f3d_krylov_norm(const double *w, int64_t n, const int32_t *k, double *hcol,
+                    double *beta, void *workspace, size_t workspace_bytes, void *stream);
+
+/* V[*k] = w / *beta (zero if beta == 0) and also into `also` if non-NULL,
+   then *k += 1 if bump. */
+int f3d_krylov_scale_into(const double *w, const double *beta, int32_t *k, double *V,
+                          int64_t ldv, int64_t n, int bump, double *also, void *stream);
+
+/* y = M x for a row-major rows x cols matrix stored as float64
+   (precision F3D_FP64) or float32 (F3D_FP32C); the sum is float64.  Applies
+   the explicit inverse of the periphery operator (tstep/tstep.py:957-958). */
+int f3d_gemv(int precision, const void *M, int64_t ld, const double *x, double *y,
+             int64_t rows, int64_t cols, void *stream);
+
+/* b = (float) a, elementwise. */
+int f3d_cast_to_float(const double *a, float *b, int64_t n, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
