@@ -312,7 +312,11 @@ static int allow_max_smem(K kernel, bool (&done)[64]) {
   int optin = 0;
   if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess)
     return F3D_ERR_CUDA;
-  if (cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, optin) != cudaSuccess)
+  // the opt-in limit covers static plus dynamic shared memory
+  cudaFuncAttributes fa;
+  if (cudaFuncGetAttributes(&fa, kernel) != cudaSuccess) return F3D_ERR_CUDA;
+  const int dyn = optin - static_cast<int>(fa.sharedSizeBytes);
+  if (cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn) != cudaSuccess)
     return F3D_ERR_CUDA;
   done[dev] = true;
   return F3D_OK;

@@ -1,0 +1,81 @@
+"""Solver-level drop-in for fiber3d's hydrodynamic time step.
+
+fiber3d builds its linear system inside ``tstep.time_step_hydro``
+(python/tstep/tstep.py:628-1458) as two closures — the matvec
+``A_body_fiber_hyd`` (:1003-1178) and the preconditioner ``P_inv``
+(:950-994) — and solves it with ``bpm_utilities.gmres.gmres``
+(:1209-1216).  :func:`install` replaces that ``gmres`` function with one that
+builds the same system on the GPU from the time stepper's own state (fibers,
+bodies, periphery, viscosity, time step), takes fiber3d's right-hand side
+``b`` as given (so every explicit force fiber3d added is kept), and solves to
+the same relative tolerance.  It returns ``(solution, info)`` in fiber3d's
+unknown layout, so the rest of ``time_step_hydro`` runs unchanged.
+
+The periphery preconditioner is built once per periphery and reused.
+"""
+from __future__ import annotations
+
+import numpy as np
+import torch
+
+from .hydro import Body, HydroSystem, Problem, Shell, ShellOperator
+
+
+def _rotation(orientation) -> np.ndarray:
+    return np.asarray(orientation.rotation_matrix(), dtype=np.float64)
+
+
+def problem_from_tstep(ts) -> Problem:
+    """Geometry and parameters of a fiber3d ``tstep`` object as a Problem
+    (free fibers; fiber3d's fiber defaults epsilon / penalty_param)."""
+    fibers = [np.asarray(f.x, dtype=np.float64) for f in ts.fibers]
+    lengths = [float(f.length) for f in ts.fibers]
+    f0 = ts.fibers[0] if ts.fibers else None
+    bodies = [Body(np.asarray(b.location, dtype=np.float64), _rotation(b.orientation),
+                   np.asarray(b.reference_configuration), np.asarray(b.reference_normals),
+                   np.asarray(b.quadrature_weights)) for b in ts.bodies]
+    shell = None
+    if getattr(ts, "shell", None) is not None:
+        shell = Shell(np.asarray(ts.trg_shell_surf).reshape(-1, 3),
+                      np.asarray(ts.normals_shell).reshape(-1, 3),
+                      np.asarray(ts.shell.quadrature_weights))
+    return Problem(fibers, lengths, float(f0.E) if f0 else 1.0, float(ts.dt), float(ts.eta), bodies,
+                   shell, None, epsilon=float(f0.epsilon) if f0 else 1e-3,
+                   penalty=float(f0.penalty_param) if f0 else 500.0)
+
+
+class GpuGmres:
+    """Callable with the signature fiber3d uses for ``gmres.gmres``."""
+
+    def __init__(self, ts, mixed: bool = False, restart: int = 100):
+        self.ts = ts
+        self.mixed = mixed
+        self.restart = restart
+        self._shell = None
+        self.last = None
+
+    def __call__(self, A, b, x0=None, tol=1e-5, atol=0, restart=None, maxiter=None, M=None,
+                 callback=None, **kw):
+        P = problem_from_tstep(self.ts)
+        if P.shell is not None and self._shell is None:
+            self._shell = ShellOperator(P.shell, P.eta, P.reg, P.eps_dist)
+        sysd = HydroSystem(P, shell_op=self._shell)
+        if sysd.size != np.size(b):
+            raise ValueError(f"system size {sysd.size} != len(b) {np.size(b)}")
+        sysd.rhs.copy_(torch.as_tensor(np.asarray(b, dtype=np.float64)))
+        res = sysd.solve(tol=tol, restart=min(restart or self.restart, 255), maxiter=maxiter or 200,
+                         mixed=self.mixed)
+        if callback is not None:
+            for h in res["history"][1:]:
+                callback(h)
+        self.last = res
+        return res["x"].cpu().numpy(), int(res["info"])
+
+
+def install(ts, mixed: bool = False):
+    """Route fiber3d's GMRES call through the GPU solver for time stepper `ts`."""
+    import importlib
+    gm = importlib.import_module("bpm_utilities.gmres")
+    solver = GpuGmres(ts, mixed=mixed)
+    gm.gmres = solver
+    return solver

@@ -81,7 +81,7 @@ def test_config1_golden(K, golden_config1):
 
 
 SHAPES = [(1, 1, 0, 0), (2, 1, 0, 0), (1, 8, 0, 0), (1, 32, 0, 0), (1, 1, 1, 0), (1, 1, 5, 0),
-          (1, 1, 3, -1), (2, 1, 0, -1), (1, 32, 7, -1)]
+          (1, 1, 3, -1), (2, 1, 0, -1), (1, 32, 7, -1), (1, 1, 19, -1), (2, 1, 38, -1)]
 
 
 @pytest.mark.parametrize("shape", SHAPES)
@@ -209,3 +209,26 @@ def test_workspace_reuse_across_shapes(K, L):
         u = K.pair_sum("oseen", x, x, f, self_mode="skip_index", shape=L.PairShape(*shape))
         ref = pairs_c.pair_sum("oseen", x, x, f, self_mode="skip_index")
         assert rel_err(u.cpu().numpy(), ref) < TOL64
+
+
+FP32_SHAPES = [(1, 1, 0, 0), (2, 1, 0, 0), (1, 8, 0, 0), (1, 32, 0, 0), (2, 1, 38, -1),
+               (1, 1, 19, -1), (2, 1, 5, 0), (1, 8, 9, -1)]
+
+
+@pytest.mark.parametrize("shape", FP32_SHAPES)
+@pytest.mark.parametrize("mode", ["regularise", "skip_group"])
+def test_fp32c_shapes(K, L, shape, mode):
+    """Every FP32C launch shape the autotuner may pick gives the FP64 result
+    to FP32C accuracy (finite everywhere)."""
+    from fiber3d_b200 import geometry
+    nodes, normals, w, mu, vol = geometry.stresslet_sphere_workload(seed=5, n=3000, n_vol=777)
+    q = mu * w[:, None]
+    trg = np.concatenate([nodes, vol])
+    gs = np.arange(3000, dtype=np.int32)
+    gt = np.concatenate([gs, -np.ones(777, np.int32)]).astype(np.int32)
+    kw = dict(self_mode=mode, src_group=gs, trg_group=gt) if mode == "skip_group" else {}
+    u64 = K.pair_sum("stresslet", nodes, trg, q, normals, **kw).cpu().numpy()
+    u32 = K.pair_sum("stresslet", nodes, trg, q, normals, precision="fp32c", shape=L.PairShape(*shape),
+                     **kw).cpu().numpy()
+    assert np.all(np.isfinite(u32))
+    assert rel_err(u32, u64) < TOL32
