@@ -89,6 +89,12 @@ SIGNATURES: dict[str, list] = {
     "f3d_krylov_scale_into": [_P, _P, _P, _P, _I64, _I64, _I, _P, _P],
     "f3d_gemv": [_I, _P, _I64, _P, _P, _I64, _I64, _P],
     "f3d_cast_to_float": [_P, _P, _I64, _P],
+    "f3d_gemm_bf16": [_P, _I64, _I64, _P, _I64, _I64, _P, _I64, ctypes.c_int32, ctypes.c_int32,
+                      ctypes.c_int32, _P, _I, _P, _I64, _P, ctypes.c_float, _I, _P],
+    "f3d_colsum": [_P, _I64, ctypes.c_int32, ctypes.c_int32, _P, _I, _P],
+    "f3d_adam": [_P, _P, _P, _P, _I64, ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_float,
+                 ctypes.c_int32, _P],
+    "f3d_mse_grad": [_P, _P, _P, _P, ctypes.c_int32, ctypes.c_int32, _P],
     "f3d_fiber_geometry": [ctypes.POINTER(FiberSetC), _P, _P, _I64, _P],
     "f3d_fiber_assemble": [ctypes.POINTER(FiberSetC), _D, _D, _D, _D, _D, _P, _P, _P, _P, _P, _P, _P,
                            ctypes.c_int32, _P],

@@ -348,6 +348,32 @@ int f3d_gemv(int precision, const void *M, int64_t ld, const double *x, double *
 /* b = (float) a, elementwise. */
 int f3d_cast_to_float(const double *a, float *b, int64_t n, void *stream);
 
+/* ---- learned warm start: tensor-core GEMM and training kernels ----------- */
+/* No counterpart in fiber3d (its GMRES always starts from zero,
+   tstep/tstep.py:1209).  C (fp32, M x N, ldc) = alpha * A B^T on the 5th-gen
+   tensor cores (tcgen05, BF16 operands rounded from the fp32 inputs, FP32
+   accumulation in tensor memory).  Element (m, k) of A is
+   A[m*a_rs + k*a_cs]; element (n, k) of B is B[n*b_rs + k*b_cs].  Optional
+   epilogue: + bias[n], copy to pre[m*ldc+n], ReLU, multiply by
+   (mask_src[m*ldm+n] > 0); accumulate adds into C.  N must be a multiple of
+   16 and at most 256. */
+int f3d_gemm_bf16(const float *A, int64_t a_rs, int64_t a_cs, const float *B, int64_t b_rs,
+                  int64_t b_cs, float *C, int64_t ldc, int32_t M, int32_t N, int32_t K,
+                  const float *bias, int relu, const float *mask_src, int64_t ldm, float *pre,
+                  float alpha, int accumulate, void *stream);
+
+/* out[n] (+)= sum_m G[m*ld + n]. */
+int f3d_colsum(const float *G, int64_t ld, int32_t M, int32_t N, float *out, int accumulate,
+               void *stream);
+
+/* One bias-corrected Adam update of n fp32 parameters (step counts from 1). */
+int f3d_adam(float *p, const float *g, float *m, float *v, int64_t n, float lr, float beta1,
+             float beta2, float eps, int32_t step, void *stream);
+
+/* D = 2 (Y - T) / (M N) and row_loss[m] = sum_n (Y - T)^2. */
+int f3d_mse_grad(const float *Y, const float *T, float *D, float *row_loss, int32_t M, int32_t N,
+                 void *stream);
+
 #ifdef __cplusplus
 }
 #endif
