@@ -90,6 +90,68 @@ def quaternion_rotation(q) -> np.ndarray:
                            [p[2] * p[0] - s * p[1], p[2] * p[1] + s * p[0], p[2] ** 2 + d]])
 
 
+def quaternion_from_rotation(phi) -> np.ndarray:
+    """Unit quaternion of a rotation by |phi| about phi (quaternion.py:14-26)."""
+    phi = np.asarray(phi, dtype=np.float64)
+    a = float(np.linalg.norm(phi))
+    if a == 0.0:
+        return np.array([1.0, 0.0, 0.0, 0.0])
+    return np.concatenate([[np.cos(a / 2.0)], np.sin(a / 2.0) * phi / a])
+
+
+def quaternion_multiply(q, r) -> np.ndarray:
+    """q r (quaternion.py:29-38)."""
+    s = q[0] * r[0] - np.dot(q[1:], r[1:])
+    p = q[0] * np.asarray(r[1:]) + r[0] * np.asarray(q[1:]) + np.cross(q[1:], r[1:])
+    return np.concatenate([[s], p])
+
+
+def rotation_to_quaternion(R) -> np.ndarray:
+    """Unit quaternion of a rotation matrix (inverse of quaternion_rotation)."""
+    R = np.asarray(R, dtype=np.float64)
+    t = np.trace(R)
+    if t > 0:
+        s = np.sqrt(t + 1.0) * 2.0
+        q = [0.25 * s, (R[2, 1] - R[1, 2]) / s, (R[0, 2] - R[2, 0]) / s, (R[1, 0] - R[0, 1]) / s]
+    elif R[0, 0] > R[1, 1] and R[0, 0] > R[2, 2]:
+        s = np.sqrt(1.0 + R[0, 0] - R[1, 1] - R[2, 2]) * 2.0
+        q = [(R[2, 1] - R[1, 2]) / s, 0.25 * s, (R[0, 1] + R[1, 0]) / s, (R[0, 2] + R[2, 0]) / s]
+    elif R[1, 1] > R[2, 2]:
+        s = np.sqrt(1.0 + R[1, 1] - R[0, 0] - R[2, 2]) * 2.0
+        q = [(R[0, 2] - R[2, 0]) / s, (R[0, 1] + R[1, 0]) / s, 0.25 * s, (R[1, 2] + R[2, 1]) / s]
+    else:
+        s = np.sqrt(1.0 + R[2, 2] - R[0, 0] - R[1, 1]) * 2.0
+        q = [(R[1, 0] - R[0, 1]) / s, (R[0, 2] + R[2, 0]) / s, (R[1, 2] + R[2, 1]) / s, 0.25 * s]
+    q = np.asarray(q)
+    return q / np.linalg.norm(q)
+
+
+class PhaseTimers:
+    """Named phase timers on CUDA events (the phases of fiber3d's
+    utils/timer.py table: Build_linear_system_fibers, Build_PC_fibers, GMRES, ...)."""
+
+    def __init__(self):
+        self.open, self.done = {}, []
+
+    def start(self, name):
+        e = torch.cuda.Event(enable_timing=True)
+        e.record()
+        self.open[name] = e
+
+    def stop(self, name):
+        e = torch.cuda.Event(enable_timing=True)
+        e.record()
+        self.done.append((name, self.open.pop(name), e))
+
+    def report(self) -> dict:
+        torch.cuda.synchronize()
+        out = {}
+        for name, a, b in self.done:
+            out[name] = out.get(name, 0.0) + a.elapsed_time(b)
+        self.done.clear()
+        return out
+
+
 class ShellOperator:
     """Device data of a periphery: nodes, normals, weights, singularity
     vectors E and the explicit inverse of the dense shell operator (FP64, and
@@ -201,25 +263,25 @@ class HydroSystem:
         self.force = f64(np.asarray(ff).reshape(-1, 3))
         self.has_force = bool(np.any(ff))
         self.geo = torch.empty((max(nF, 1), 9), dtype=torch.float64, device=dev)
-        if nF:
-            _lib.call("f3d_fiber_geometry", ctypes.byref(self.fs.c), _lib.ptr(self.x_fib), _lib.ptr(self.geo), nF, st())
-        # ---- bodies
+        self.timers = PhaseTimers()
+        # ---- bodies (host state: location, orientation; device: nodes, normals, E)
         self.nbody = len(P.bodies)
         nb = [np.asarray(b.ref_nodes).reshape(-1, 3).shape[0] for b in P.bodies]
         self.nb = nb
         self.body_node_off_h = np.concatenate([[0], np.cumsum(nb)]).astype(np.int64)
         nB = int(self.body_node_off_h[-1])
         self.nB = nB
+        self.body_loc = np.array([np.asarray(b.location, dtype=np.float64) for b in P.bodies]).reshape(-1, 3)
+        self.body_quat = np.array([rotation_to_quaternion(b.rotation) for b in P.bodies]).reshape(-1, 4)
+        self.body_ref = [np.asarray(b.ref_nodes, dtype=np.float64).reshape(-1, 3) for b in P.bodies]
+        self.body_ref_n = [np.asarray(b.ref_normals, dtype=np.float64).reshape(-1, 3) for b in P.bodies]
         if self.nbody:
-            self.body_nodes = f64(np.concatenate([b.nodes for b in P.bodies]))
-            self.body_normals = f64(np.concatenate([b.normals for b in P.bodies]))
+            self.body_nodes = torch.zeros((nB, 3), dtype=torch.float64, device=dev)
+            self.body_normals = torch.zeros((nB, 3), dtype=torch.float64, device=dev)
             self.body_w = f64(np.concatenate([np.asarray(b.weights).reshape(-1) for b in P.bodies]))
-            self.body_centers = f64(np.stack([np.asarray(b.location, dtype=np.float64) for b in P.bodies]))
+            self.body_centers = torch.zeros((self.nbody, 3), dtype=torch.float64, device=dev)
             self.body_E = torch.empty((nB, 9), dtype=torch.float64, device=dev)
-            for k in range(self.nbody):
-                a, b = self.body_node_off_h[k], self.body_node_off_h[k + 1]
-                self.body_E[a:b] = singularity_vectors(self.body_nodes[a:b], self.body_normals[a:b],
-                                                       self.body_w[a:b], P.eta, P.reg, P.eps_dist)
+            self._load_bodies()
         # ---- shell
         if P.shell is not None:
             self.shell = shell_op or ShellOperator(P.shell, P.eta, P.reg, P.eps_dist, dev)
@@ -280,7 +342,62 @@ class HydroSystem:
         sizes = [3 * n + 6 for n in nb] + list(4 * self.fs.npts)
         self.lu = BlockLU(sizes, device=dev)
         self.A_fib = torch.zeros(max(self.fs.mat_total, 1), dtype=torch.float64, device=dev)
+        self.flow_ext = torch.zeros((max(nF, 1), 3), dtype=torch.float64, device=dev)
+        self.update()
+
+    # ------------------------------------------------------------------------
+    def _load_bodies(self):
+        for k in range(self.nbody):
+            a, b = int(self.body_node_off_h[k]), int(self.body_node_off_h[k + 1])
+            R = quaternion_rotation(self.body_quat[k])
+            self.body_nodes[a:b] = torch.as_tensor(self.body_ref[k] @ R.T + self.body_loc[k])
+            self.body_normals[a:b] = torch.as_tensor(self.body_ref_n[k] @ R.T)
+        self.body_centers.copy_(torch.as_tensor(self.body_loc))
+        P = self.p
+        for k in range(self.nbody):
+            a, b = int(self.body_node_off_h[k]), int(self.body_node_off_h[k + 1])
+            self.body_E[a:b] = singularity_vectors(self.body_nodes[a:b], self.body_normals[a:b],
+                                                   self.body_w[a:b], P.eta, P.reg, P.eps_dist)
+
+    def update(self):
+        """Recompute everything that depends on the current geometry (fiber
+        derivatives, body surfaces and singularity vectors, explicit flows,
+        right-hand side, fiber/body blocks and their LU) in place, so that
+        device pointers — and CUDA graphs captured on them — stay valid."""
+        st = _lib.stream_handle(self.device)
+        if self.nF:
+            _lib.call("f3d_fiber_geometry", ctypes.byref(self.fs.c), _lib.ptr(self.x_fib), _lib.ptr(self.geo),
+                      self.nF, st)
         self._assemble()
+
+    def advance(self, sol: torch.Tensor):
+        """Move the geometry one step with solution `sol` (tstep.py:1392-1407:
+        fibers take their new positions; bodies x += dt U and
+        q <- q(Omega dt) q), then :meth:`update`."""
+        dt = self.p.dt
+        o = self.o_fib
+        for n in sorted(set(int(v) for v in self.fs.npts)):
+            idx = np.nonzero(self.fs.npts == n)[0]
+            starts = self.fs.pt_off_h[idx]
+            if np.all(np.diff(starts) == n) and idx.size and idx[-1] - idx[0] == idx.size - 1:
+                blk = sol[o + 4 * int(starts[0]):o + 4 * int(starts[0]) + 4 * n * idx.size].view(idx.size, 4, n)
+                self.x_fib[int(starts[0]):int(starts[0]) + n * idx.size] = blk[:, :3, :].transpose(1, 2).reshape(-1, 3)
+            else:
+                for f in idx:
+                    p0 = int(self.fs.pt_off_h[f])
+                    blk = sol[o + 4 * p0:o + 4 * p0 + 4 * n].view(4, n)
+                    self.x_fib[p0:p0 + n] = blk[:3].t()
+        if self.nbody:
+            vel = sol.new_empty((self.nbody, 6))
+            for k in range(self.nbody):
+                i0 = self.o_body[k] + 3 * self.nb[k]
+                vel[k] = sol[i0:i0 + 6]
+            vel = vel.cpu().numpy()
+            for k in range(self.nbody):
+                self.body_loc[k] = self.body_loc[k] + dt * vel[k, :3]
+                self.body_quat[k] = quaternion_multiply(quaternion_from_rotation(vel[k, 3:] * dt), self.body_quat[k])
+            self._load_bodies()
+        self.update()
 
     # ------------------------------------------------------------------------
     def autotune(self):
@@ -302,18 +419,23 @@ class HydroSystem:
         st = _lib.stream_handle(dev)
         nF, nB, nS = self.nF, self.nB, self.nS
         # explicit flow of the external fiber forces (tstep.py:789-821)
+        self.timers.start("fiber2all_explicit_interactions")
         self.v.zero_()
         if nF and self.has_force:
             _lib.call("f3d_fiber_weight", ctypes.byref(self.fs.c), _lib.ptr(self.force), _lib.ptr(self.fw), nF, st)
             self.oseen("fp64")
+        self.timers.stop("fiber2all_explicit_interactions")
         v = self.v.view(-1, 3)
+        if nF:
+            self.flow_ext.copy_(v[:nF])
         if nS:
             self.rhs[:3 * nS] = -v[nF + nB:].reshape(-1)
         for k in range(self.nbody):
             a, b = int(self.body_node_off_h[k]), int(self.body_node_off_h[k + 1])
             self.rhs[self.o_body[k]:self.o_body[k] + 3 * (b - a)] = -v[nF + a:nF + b].reshape(-1)
-        flow = v[:nF].contiguous() if nF else v[:1]
+        flow = self.flow_ext
         # fiber blocks into A_fib and (a copy) into the LU buffer after the body blocks
+        self.timers.start("Build_linear_system_fibers")
         if nF:
             lu_fib0 = int(self.lu.moff_h[self.nbody]) if self.lu.count else 0
             A_copy = self.lu.A.data_ptr() + 8 * lu_fib0
@@ -326,7 +448,10 @@ class HydroSystem:
             _lib.call("f3d_surface_dense", 1, _lib.ptr(self.body_nodes[a:b]), _lib.ptr(self.body_normals[a:b]),
                       _lib.ptr(self.body_E[a:b]), _lib.ptr(self.body_w[a:b]), _lib.ptr(self.body_centers[k]),
                       _lib.ptr(self.lu.block(k)), n, 3 * n + 6, P.eta, P.reg, P.eps_dist, st)
+        self.timers.stop("Build_linear_system_fibers")
+        self.timers.start("Build_PC_fibers_bodies")
         self.lu.factor()
+        self.timers.stop("Build_PC_fibers_bodies")
 
     # ------------------------------------------------------------------------
     def matvec(self, x: torch.Tensor, y: torch.Tensor, precision: str = "fp64") -> torch.Tensor:

@@ -172,3 +172,94 @@ def fiber_features(x_fib: torch.Tensor, u_bg: torch.Tensor, npts: int = 32) -> t
 def fiber_targets(T: torch.Tensor, f: torch.Tensor, npts: int = 32) -> torch.Tensor:
     """(nfib, 128): tensions and force densities."""
     return torch.cat([T.view(-1, npts), f.view(-1, 3 * npts)], dim=1).float()
+
+
+# ------------------------------------------------------------ time marching --
+def background_velocity(system, x_prev: torch.Tensor | None) -> torch.Tensor:
+    """Velocity on every fiber point from everything except the fiber itself:
+    the explicit flow of the external forces plus, when a previous solution
+    is given, the flow of its fiber forces, body and periphery densities
+    evaluated at the current geometry (one matvec's pair sums)."""
+    u = system.flow_ext.clone()
+    if x_prev is not None:
+        y = torch.empty_like(x_prev)
+        system.matvec(x_prev, y)
+        u += system.v.view(-1, 3)[:system.nF]
+    return u
+
+
+def solution_targets(system, sol: torch.Tensor):
+    """(T, f): tensions and force densities f = -E X_ssss + (T X_s)_s of the
+    solved step, per fiber point (force operator at the solution)."""
+    nF = system.nF
+    f = torch.empty((nF, 3), dtype=torch.float64, device=sol.device)
+    XT = sol[system.o_fib:]
+    _lib.call("f3d_fiber_forces", ctypes.byref(system.fs.c), system.p.E, _lib.ptr(system.geo), _lib.ptr(XT),
+              _lib.ptr(f), nF, 0, _lib.stream_handle(sol.device))
+    n = int(system.fs.npts[0])
+    T = XT.view(-1, 4, n)[:, 3, :].reshape(-1)
+    return T, f
+
+
+def guess_from_prediction(system, pred: torch.Tensor, u_bg: torch.Tensor,
+                          x_prev: torch.Tensor | None) -> torch.Tensor:
+    """GMRES initial guess from network output (T^, f^) per fiber:
+    X^ = X^n + dt (u_bg + M f^) with the local slender-body mobility
+    M f = c0 (f + xs (xs.f)) + c1 (f - xs (xs.f)); periphery and body
+    unknowns from the previous solution (zero at the first step)."""
+    n = int(system.fs.npts[0])
+    nfib = system.fs.nfib
+    x0 = x_prev.clone() if x_prev is not None else torch.zeros(system.size, dtype=torch.float64,
+                                                               device=system.device)
+    pred = pred.double()
+    T = pred[:, :n]
+    f = pred[:, n:].reshape(nfib * n, 3)
+    xs = system.geo[:system.nF, 0:3]
+    xf = (xs * f).sum(1, keepdim=True)
+    Mf = system.c0 * (f + xs * xf) + system.c1 * (f - xs * xf)
+    X = system.x_fib + system.p.dt * (u_bg + Mf)
+    blk = x0[system.o_fib:].view(nfib, 4, n)
+    blk[:, :3, :] = X.view(nfib, n, 3).transpose(1, 2)
+    blk[:, 3, :] = T
+    return x0
+
+
+def march(system, steps: int, guess: str = "zero", net: FiberMLP | None = None, tol=1e-8,
+          mixed=False, record=False, restart=100):
+    """Advance `system` `steps` time steps; per step return iterations, time
+    and (when record) the network's training pairs.
+
+    guess: 'zero' (fiber3d's GMRES start), 'previous' (last solution) or
+    'learned' (network prediction, then the same GMRES to the same residual).
+    """
+    x_prev = None
+    stats, feats, targs = [], [], []
+    n = int(system.fs.npts[0])
+    for s in range(steps):
+        if s > 0:
+            system.advance(x_prev)
+        u_bg = background_velocity(system, x_prev)
+        X_feat = fiber_features(system.x_fib, u_bg, n)
+        if guess == "learned" and net is not None:
+            x0 = guess_from_prediction(system, net.predict(X_feat), u_bg, x_prev)
+        elif guess in ("previous", "learned") and x_prev is not None:
+            x0 = x_prev
+        else:
+            x0 = None
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        res = system.solve(tol=tol, restart=restart, x0=x0, mixed=mixed)
+        e1.record()
+        e1.synchronize()
+        sol = res["x"]
+        st = {"iterations": res["iterations"], "solve_ms": e0.elapsed_time(e1),
+              "initial_rel_residual": res["history"][0]}
+        if record:
+            T, f = solution_targets(system, sol)
+            feats.append(X_feat)
+            targs.append(fiber_targets(T, f, n))
+        stats.append(st)
+        x_prev = sol
+    if record:
+        return stats, torch.cat(feats), torch.cat(targs)
+    return stats

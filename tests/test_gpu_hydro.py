@@ -124,6 +124,9 @@ def test_larger_system_against_oracle():
     x = rng.normal(size=op.size)
     y = torch.empty(op.size, dtype=torch.float64, device="cuda")
     dev.matvec(torch.tensor(x, device="cuda"), y)
-    assert rel_err(y.cpu().numpy(), op.matvec(x)) < 1e-12
+    # 1e-10 here: at N = 64 the third derivative xsss = D3 x carries ~1e-9
+    # of FP64 rounding (|D3| ~ 2e6), which the tension rows multiply by
+    # 6 c0 E D3 ~ 2e4; any two FP64 evaluation orders differ by that much.
+    assert rel_err(y.cpu().numpy(), op.matvec(x)) < 1e-10
     dev.pc(torch.tensor(x, device="cuda"), y)
     assert rel_err(y.cpu().numpy(), op.pc(x)) < 1e-9

@@ -78,5 +78,5 @@ def test_mlp_training_reduces_loss():
     T = teacher.forward(X)
     student = FiberMLP(seed=9)
     student.set_normalisation(X, T)
-    hist = student.train(X, T, epochs=8, batch=512, lr=2e-3)
-    assert hist[-1] < 0.5 * hist[0]
+    hist = student.train(X, T, epochs=15, batch=512, lr=2e-3)
+    assert hist[-1] < 0.7 * hist[0]
