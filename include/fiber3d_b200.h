@@ -112,6 +112,23 @@ int f3d_pair_sum(int kernel, int precision, int self_mode,
                  int accumulate, const f3d_pair_shape *shape,
                  void *workspace, size_t workspace_bytes, void *stream);
 
+/* The same sum for callers that cannot allocate device memory (no workspace
+   argument).  No counterpart in fiber3d.  Its scratch is a 32 MiB device
+   array inside this library, held by every GPU that loads it until the
+   process exits; sizes whose f3d_pair_workspace_bytes (default shape)
+   exceeds 32 MiB return F3D_ERR_TOO_LARGE.  The first call on a device looks
+   up that array's device address (make it before any stream capture).
+   Calls share the array: two calls that overlap on the GPU (different
+   streams, or devices sharing nothing but the call) race; order them on one
+   stream.  Allocates nothing. */
+int f3d_pair_sum_noalloc(int kernel, int precision, int self_mode,
+                         const double *r_source, const double *r_target,
+                         const double *density, const double *normal,
+                         const int32_t *src_group, const int32_t *trg_group,
+                         double *out, int64_t ns, int64_t nt,
+                         double eta, double reg, double epsilon_distance,
+                         int accumulate, void *stream);
+
 /* Named wrappers with the meaning of the fiber3d functions they replace. */
 
 /* replaces oseen_kernel_source_target_numba, python/kernels/kernels.py:794-846 */
