@@ -54,11 +54,25 @@ class BlockLU:
         for b, M in enumerate(blocks):
             self.block(b).copy_(torch.as_tensor(np.asarray(M, dtype=np.float64)))
 
-    def factor(self) -> None:
+    def factor(self, blocks=None) -> None:
+        """Factor every block, or only the listed block indices."""
         if self.count == 0:
             return
+        if blocks is None:
+            order, count = self.order, self.count
+        else:
+            key = tuple(int(b) for b in blocks)
+            cached = getattr(self, "_subset", None)
+            if cached is None or cached[0] != key:
+                sel = np.asarray(key, dtype=np.int64)
+                sel = sel[np.argsort(-self.sizes_h[sel], kind="stable")]
+                self._subset = (key, torch.as_tensor(sel.astype(np.int32), device=self.device))
+            order, count = self._subset[1], len(key)
+            if count == 0:
+                return
+        mx = self.max_n if blocks is None else int(self.sizes_h[list(blocks)].max())
         _lib.call("f3d_batched_lu_factor", _lib.ptr(self.A), _lib.ptr(self.moff), _lib.ptr(self.voff),
-                  _lib.ptr(self.sizes), _lib.ptr(self.order), self.count, self.max_n,
+                  _lib.ptr(self.sizes), _lib.ptr(order), count, mx,
                   _lib.ptr(self.piv), _lib.ptr(self.info), _lib.ptr(self.ws), self.ws.numel(),
                   _lib.stream_handle(self.device))
 

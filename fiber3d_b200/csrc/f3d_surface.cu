@@ -209,9 +209,43 @@ __global__ void gather_segments_kernel(const double *__restrict__ src, double *d
     dst[seg_dst[s] + k] = src[seg_src[s] + k];
 }
 
+// Per body b: the nvec[b] 3-vectors at x + off[b] are multiplied by R_b
+// (transpose = 0) or R_b^T (transpose = 1), R_b row-major at R + 9 b.
+__global__ void rotate_blocks_kernel(double *x, const int64_t *off, const int32_t *nvec,
+                                     const double *R, int transpose) {
+  const int b = blockIdx.x;
+  double r[9];
+#pragma unroll
+  for (int i = 0; i < 9; ++i) r[i] = R[9 * b + i];
+  double *v = x + off[b];
+  for (int k = threadIdx.x; k < nvec[b]; k += blockDim.x) {
+    const double a0 = v[3 * k], a1 = v[3 * k + 1], a2 = v[3 * k + 2];
+    if (transpose) {
+      v[3 * k] = r[0] * a0 + r[3] * a1 + r[6] * a2;
+      v[3 * k + 1] = r[1] * a0 + r[4] * a1 + r[7] * a2;
+      v[3 * k + 2] = r[2] * a0 + r[5] * a1 + r[8] * a2;
+    } else {
+      v[3 * k] = r[0] * a0 + r[1] * a1 + r[2] * a2;
+      v[3 * k + 1] = r[3] * a0 + r[4] * a1 + r[5] * a2;
+      v[3 * k + 2] = r[6] * a0 + r[7] * a1 + r[8] * a2;
+    }
+  }
+}
+
 }  // namespace f3d
 
 extern "C" {
+
+int f3d_rotate_blocks(double *x, const int64_t *offsets, const int32_t *nvec, const double *R,
+                      int32_t nbody, int transpose, void *stream) {
+  if (nbody < 0) return F3D_ERR_SHAPE;
+  if (nbody == 0) return F3D_OK;
+  if (!x || !offsets || !nvec || !R) return F3D_ERR_NULL;
+  f3d::rotate_blocks_kernel<<<nbody, 256, 0, static_cast<cudaStream_t>(stream)>>>(x, offsets, nvec, R,
+                                                                                  transpose);
+  return f3d::launch_status();
+}
+
 
 int f3d_singularity_vectors_workspace_bytes(int64_t n, size_t *bytes) {
   if (!bytes) return F3D_ERR_NULL;

@@ -73,8 +73,49 @@ def straight_fibers_cheb(rng, nfib: int, npts: int, length: float, ball_radius: 
     return x.reshape(nfib * npts, 3)
 
 
+def _segment_distances(p0, d0, P, D):
+    """Distances between segment p0 + t d0 and segments P_k + s D_k, t, s in [0, 1]."""
+    r = p0[None, :] - P
+    a = np.dot(d0, d0)
+    e = np.einsum("ij,ij->i", D, D)
+    b = D @ d0
+    c = r @ d0
+    f = np.einsum("ij,ij->i", D, r)
+    den = a * e - b * b
+    t = np.where(den > 1e-12, (b * f - c * e) / np.where(den > 1e-12, den, 1.0), 0.0)
+    t = np.clip(t, 0.0, 1.0)
+    s = np.clip((b * t + f) / e, 0.0, 1.0)
+    t = np.clip((b * s - c) / a, 0.0, 1.0)
+    q = r + t[:, None] * d0[None, :] - s[:, None] * D
+    return np.sqrt(np.einsum("ij,ij->i", q, q))
+
+
+def separated_fibers(rng, nfib: int, length: float, ball_radius: float, min_sep: float,
+                     max_tries: int = 200000):
+    """Centres and directions of `nfib` straight fibers (uniform in a ball,
+    uniform directions) whose centre lines stay at least `min_sep` apart
+    (rejection sampling)."""
+    rng = _rng(rng)
+    C, Dd = [], []
+    tries = 0
+    while len(C) < nfib:
+        tries += 1
+        if tries > max_tries:
+            raise RuntimeError(f"could only place {len(C)} of {nfib} fibers {min_sep} apart")
+        c = uniform_ball(rng, 1, ball_radius)[0]
+        d = uniform_directions(rng, 1)[0]
+        p0 = c - 0.5 * length * d
+        if C:
+            Pa = np.array(C) - 0.5 * length * np.array(Dd)
+            if np.min(_segment_distances(p0, length * d, Pa, length * np.array(Dd))) < min_sep:
+                continue
+        C.append(c)
+        Dd.append(d)
+    return np.array(C), np.array(Dd)
+
+
 def perturbed_fibers(rng, nfib: int, npts, length: float, ball_radius: float,
-                     amplitude: float = 0.05, modes: int = 3):
+                     amplitude: float = 0.05, modes: int = 3, min_sep: float | None = None):
     """Fibers on the solver's equispaced nodes alpha = linspace(-1, 1, N):
     straight line through a centre uniform in a ball, plus ``modes`` random
     transverse Fourier modes sin(k pi (alpha+1)/2) of amplitude ``amplitude``.
@@ -85,8 +126,11 @@ def perturbed_fibers(rng, nfib: int, npts, length: float, ball_radius: float,
     rng = _rng(rng)
     if np.isscalar(npts):
         npts = [int(npts)] * nfib
-    c = uniform_ball(rng, nfib, ball_radius)
-    d = uniform_directions(rng, nfib)
+    if min_sep:
+        c, d = separated_fibers(rng, nfib, length, ball_radius, min_sep + 2 * amplitude)
+    else:
+        c = uniform_ball(rng, nfib, ball_radius)
+        d = uniform_directions(rng, nfib)
     out = []
     for k in range(nfib):
         n = int(npts[k])
@@ -131,16 +175,18 @@ def stresslet_sphere_workload(seed: int = 2, n: int = 12000, radius: float = 10.
 def hydro_step_problem(seed: int = 3, nfib: int = 512, npts=32, nbody: int = 4,
                        body_nodes: int = 400, nshell: int = 12000, shell_radius: float = 10.0,
                        length: float = 2.0, E: float = 0.0025, dt: float = 1e-3, eta: float = 1.0,
-                       force_std: float = 0.1, fiber_ball: float = 5.0, body_shell: float = 7.5):
+                       force_std: float = 0.1, fiber_ball: float = 5.0, body_shell: float = 7.5,
+                       min_sep: float | None = 0.1):
     """Full-step workload: `nfib` fibers (equispaced nodes, straight + 3
     transverse modes of amplitude 0.05, centres uniform in a ball of radius
     5), `nbody` rigid spheres of radius 0.5 (Fibonacci nodes, equal weights,
     random orientation, centres at radius `body_shell`), a spherical periphery
     of `nshell` nodes (inward normals as fiber3d uses them, equal weights
-    4 pi R^2 / N), and a constant external force N(0, force_std) per fiber."""
+    4 pi R^2 / N), and a constant external force N(0, force_std) per fiber.
+    Fiber centre lines are kept `min_sep` apart (plus the mode amplitudes)."""
     from .hydro import Body, Problem, Shell, quaternion_rotation
     rng = _rng(seed)
-    fibers = perturbed_fibers(rng, nfib, npts, length, fiber_ball)
+    fibers = perturbed_fibers(rng, nfib, npts, length, fiber_ball, min_sep=min_sep)
     counts = [f.shape[0] for f in fibers]
     ff = np.concatenate([np.tile(rng.normal(scale=force_std, size=3), (n, 1)) for n in counts])
     bn, bnn = fibonacci_sphere(body_nodes, 0.5)

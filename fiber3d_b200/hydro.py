@@ -281,6 +281,7 @@ class HydroSystem:
             self.body_w = f64(np.concatenate([np.asarray(b.weights).reshape(-1) for b in P.bodies]))
             self.body_centers = torch.zeros((self.nbody, 3), dtype=torch.float64, device=dev)
             self.body_E = torch.empty((nB, 9), dtype=torch.float64, device=dev)
+            self.body_R = torch.zeros((self.nbody, 9), dtype=torch.float64, device=dev)
             self._load_bodies()
         # ---- shell
         if P.shell is not None:
@@ -339,10 +340,10 @@ class HydroSystem:
             self.autotune()
         # ---- right-hand side and preconditioner blocks
         self.rhs = torch.zeros(self.size, dtype=torch.float64, device=dev)
-        sizes = [3 * n + 6 for n in nb] + list(4 * self.fs.npts)
-        self.lu = BlockLU(sizes, device=dev)
+        self.lu = BlockLU(list(4 * self.fs.npts), device=dev)
         self.A_fib = torch.zeros(max(self.fs.mat_total, 1), dtype=torch.float64, device=dev)
         self.flow_ext = torch.zeros((max(nF, 1), 3), dtype=torch.float64, device=dev)
+        self._body_blocks()
         self.update()
 
     # ------------------------------------------------------------------------
@@ -353,11 +354,40 @@ class HydroSystem:
             self.body_nodes[a:b] = torch.as_tensor(self.body_ref[k] @ R.T + self.body_loc[k])
             self.body_normals[a:b] = torch.as_tensor(self.body_ref_n[k] @ R.T)
         self.body_centers.copy_(torch.as_tensor(self.body_loc))
+        self.body_R.copy_(torch.as_tensor(np.stack([quaternion_rotation(q).ravel() for q in self.body_quat])))
         P = self.p
         for k in range(self.nbody):
             a, b = int(self.body_node_off_h[k]), int(self.body_node_off_h[k + 1])
             self.body_E[a:b] = singularity_vectors(self.body_nodes[a:b], self.body_normals[a:b],
                                                    self.body_w[a:b], P.eta, P.reg, P.eps_dist)
+
+    def _body_blocks(self):
+        """Body preconditioner blocks in each body's own frame (location 0,
+        orientation identity), inverted once.  A rigid body's block only
+        rotates with the body, so P_b^-1 x = Q A_ref^-1 Q^T x with Q the
+        body rotation on every 3-vector — fiber3d's precompute_body_PC path
+        (A_inv_bodies, tstep.py:227-252 and 966-981)."""
+        self.body_inv = []
+        if not self.nbody:
+            return
+        P = self.p
+        st = _lib.stream_handle(self.device)
+        origin = torch.zeros(3, dtype=torch.float64, device=self.device)
+        self.rot_off = torch.as_tensor(np.array([o - 3 * self.nS for o in self.o_body], dtype=np.int64),
+                                       device=self.device)
+        self.rot_nvec = torch.as_tensor(np.array([n + 2 for n in self.nb], dtype=np.int32), device=self.device)
+        self.body_tmp = torch.zeros(self.o_fib - 3 * self.nS, dtype=torch.float64, device=self.device)
+        for k in range(self.nbody):
+            ref = torch.as_tensor(self.body_ref[k], device=self.device)
+            refn = torch.as_tensor(self.body_ref_n[k], device=self.device)
+            a, b = int(self.body_node_off_h[k]), int(self.body_node_off_h[k + 1])
+            w = self.body_w[a:b].contiguous()
+            E = singularity_vectors(ref, refn, w, P.eta, P.reg, P.eps_dist)
+            n = b - a
+            A = torch.empty((3 * n + 6, 3 * n + 6), dtype=torch.float64, device=self.device)
+            _lib.call("f3d_surface_dense", 1, _lib.ptr(ref), _lib.ptr(refn), _lib.ptr(E), _lib.ptr(w),
+                      _lib.ptr(origin), _lib.ptr(A), n, 3 * n + 6, P.eta, P.reg, P.eps_dist, st)
+            self.body_inv.append(torch.linalg.inv(A))
 
     def update(self):
         """Recompute everything that depends on the current geometry (fiber
@@ -434,24 +464,17 @@ class HydroSystem:
             a, b = int(self.body_node_off_h[k]), int(self.body_node_off_h[k + 1])
             self.rhs[self.o_body[k]:self.o_body[k] + 3 * (b - a)] = -v[nF + a:nF + b].reshape(-1)
         flow = self.flow_ext
-        # fiber blocks into A_fib and (a copy) into the LU buffer after the body blocks
+        # fiber blocks into A_fib and (a copy) into the LU buffer
         self.timers.start("Build_linear_system_fibers")
         if nF:
-            lu_fib0 = int(self.lu.moff_h[self.nbody]) if self.lu.count else 0
-            A_copy = self.lu.A.data_ptr() + 8 * lu_fib0
+            A_copy = self.lu.A.data_ptr()
             _lib.call("f3d_fiber_assemble", ctypes.byref(self.fs.c), P.E, P.dt, self.c0, self.c1, P.penalty,
                       _lib.ptr(self.x_fib), _lib.ptr(self.geo), _lib.ptr(flow), _lib.ptr(self.force),
                       _lib.ptr(self.A_fib), A_copy, _lib.ptr(self.rhs[self.o_fib:]), self.fs.max_n, st)
-        for k in range(self.nbody):
-            a, b = int(self.body_node_off_h[k]), int(self.body_node_off_h[k + 1])
-            n = b - a
-            _lib.call("f3d_surface_dense", 1, _lib.ptr(self.body_nodes[a:b]), _lib.ptr(self.body_normals[a:b]),
-                      _lib.ptr(self.body_E[a:b]), _lib.ptr(self.body_w[a:b]), _lib.ptr(self.body_centers[k]),
-                      _lib.ptr(self.lu.block(k)), n, 3 * n + 6, P.eta, P.reg, P.eps_dist, st)
         self.timers.stop("Build_linear_system_fibers")
-        self.timers.start("Build_PC_fibers_bodies")
+        self.timers.start("Build_PC_fibers")
         self.lu.factor()
-        self.timers.stop("Build_PC_fibers_bodies")
+        self.timers.stop("Build_PC_fibers")
 
     # ------------------------------------------------------------------------
     def matvec(self, x: torch.Tensor, y: torch.Tensor, precision: str = "fp64") -> torch.Tensor:
@@ -494,9 +517,21 @@ class HydroSystem:
             M = self.shell.inv64 if precision == "fp64" else self.shell.inv32
             _lib.call("f3d_gemv", _lib.PRECISION[precision], _lib.ptr(M), 3 * nS, _lib.ptr(x), _lib.ptr(y),
                       3 * nS, 3 * nS, st)
-        if self.size > 3 * nS:
-            rest = y[3 * nS:]
-            rest.copy_(x[3 * nS:])
+        if self.nbody:
+            tb = self.body_tmp
+            tb.copy_(x[3 * nS:self.o_fib])
+            _lib.call("f3d_rotate_blocks", _lib.ptr(tb), _lib.ptr(self.rot_off), _lib.ptr(self.rot_nvec),
+                      _lib.ptr(self.body_R), self.nbody, 1, st)
+            for k in range(self.nbody):
+                m = 3 * self.nb[k] + 6
+                o = self.o_body[k] - 3 * nS
+                _lib.call("f3d_gemv", 0, _lib.ptr(self.body_inv[k]), m, _lib.ptr(tb[o:]), _lib.ptr(y[3 * nS + o:]),
+                          m, m, st)
+            _lib.call("f3d_rotate_blocks", _lib.ptr(y[3 * nS:]), _lib.ptr(self.rot_off), _lib.ptr(self.rot_nvec),
+                      _lib.ptr(self.body_R), self.nbody, 0, st)
+        if self.nF:
+            rest = y[self.o_fib:]
+            rest.copy_(x[self.o_fib:])
             self.lu.solve(rest)
         return y
 

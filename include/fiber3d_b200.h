@@ -321,6 +321,14 @@ int f3d_surface_dense(int mode, const double *nodes, const double *normals, cons
                       int64_t ld, double eta, double reg, double epsilon_distance,
                       void *stream);
 
+/* Rigid-body frame change of preconditioner vectors: for body b the nvec[b]
+   3-vectors at x + offsets[b] become R_b v (transpose 0) or R_b^T v
+   (transpose 1), R_b row-major at R + 9b.  With the body block factored
+   once in the body frame this applies the body preconditioner as fiber3d's
+   precompute_body_PC path does (tstep/tstep.py:966-981, 227-252). */
+int f3d_rotate_blocks(double *x, const int64_t *offsets, const int32_t *nvec, const double *R,
+                      int32_t nbody, int transpose, void *stream);
+
 /* dst[seg_dst[s] + k] = src[seg_src[s] + k] for k < seg_len[s] (max_len >= all). */
 int f3d_gather_segments(const double *src, double *dst, const int64_t *seg_src,
                         const int64_t *seg_dst, const int64_t *seg_len, int32_t nseg,
