@@ -373,7 +373,29 @@ def hydro_arm(args, rank, world, local):
     torch.cuda.synchronize()
     setup_s = time.perf_counter() - t0
     out, xs = {}, {}
-    for mode in ("fp64", "mixed"):
+    # learned warm start: training pairs from the plain solver's own steps on
+    # seeds disjoint from the benchmark trajectory, then the network is trained
+    # on the GPU by the library's kernels
+    from fiber3d_b200 import warmstart as W
+    t0 = time.perf_counter()
+    feats, targs = [], []
+    for seed in args.train_seeds:
+        Pt = geometry.hydro_step_problem(seed=seed, nshell=args.nshell, nfib=args.nfib)
+        st_ = H.HydroSystem(Pt, shell_op=shell, device=dev)
+        _, Xf, Tf = W.march(st_, args.train_steps, guess="previous", record=True)
+        feats.append(Xf)
+        targs.append(Tf)
+        del st_
+    X_train, T_train = torch.cat(feats), torch.cat(targs)
+    net = W.FiberMLP(seed=0, device=dev)
+    net.set_normalisation(X_train, T_train)
+    hist = net.train(X_train, T_train, epochs=args.train_epochs, batch=1024, lr=1e-3)
+    torch.cuda.synchronize()
+    train = {"samples": int(X_train.shape[0]), "seconds": time.perf_counter() - t0,
+             "loss_first_last": [hist[0], hist[-1]], "seeds": list(args.train_seeds),
+             "steps_per_seed": args.train_steps}
+    for mode in ("fp64", "mixed", "learned_mixed", "previous_fp64"):
+        mixed = mode in ("mixed", "learned_mixed")
         sysd = H.HydroSystem(P, shell_op=shell, device=dev, tune=True)
         sol = None
         times, its, resid, phases = [], [], [], []
@@ -384,8 +406,16 @@ def hydro_arm(args, rank, world, local):
             e0.record()
             if sol is not None:
                 sysd.advance(sol)
+            x0 = None
+            if mode == "learned_mixed":
+                sysd.timers.start("warm_start")
+                u_bg = W.background_velocity(sysd, sol)
+                x0 = W.guess_from_prediction(sysd, net.predict(W.fiber_features(sysd.x_fib, u_bg, 32)), u_bg, sol)
+                sysd.timers.stop("warm_start")
+            elif mode == "previous_fp64":
+                x0 = sol
             sysd.timers.start("GMRES")
-            res = sysd.solve(tol=1e-8, restart=100, mixed=(mode == "mixed"))
+            res = sysd.solve(tol=1e-8, restart=100, mixed=mixed, x0=x0)
             sysd.timers.stop("GMRES")
             e1.record()
             e1.synchronize()
@@ -402,11 +432,14 @@ def hydro_arm(args, rank, world, local):
                 xs[mode] = sol.clone()
         out[mode] = {"ms_per_step": statistics.median(times), "iterations": its,
                      "true_rel_residual": max(resid), "refinements": res.get("refinements", 0),
+                     "initial_rel_residual": res["history"][0],
                      "phases_ms": {k: statistics.median([p.get(k, 0.0) for p in phases]) for k in phases[0]}}
         del sysd
-    out["mixed"]["rel_diff_vs_fp64_first_step"] = float(
-        torch.linalg.vector_norm(xs["mixed"] - xs["fp64"]) / torch.linalg.vector_norm(xs["fp64"]))
-    out["speedup_mixed_vs_fp64"] = out["fp64"]["ms_per_step"] / out["mixed"]["ms_per_step"]
+    for mode in ("mixed", "learned_mixed", "previous_fp64"):
+        out[mode]["rel_diff_vs_fp64_first_step"] = float(
+            torch.linalg.vector_norm(xs[mode] - xs["fp64"]) / torch.linalg.vector_norm(xs["fp64"]))
+        out[mode]["speedup_vs_fp64"] = out["fp64"]["ms_per_step"] / out[mode]["ms_per_step"]
+    out["training"] = train
     line = {"metric": "hydro time step (ms), GMRES rel. residual 1e-8", "value": out["fp64"]["ms_per_step"],
             "unit": "ms", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "higher_is_better": False, "dtype": "f64", "data": "synthetic (seeded)",
@@ -418,6 +451,89 @@ def hydro_arm(args, rank, world, local):
         print(json.dumps(line), flush=True)
 
 
+def block_pc_arm(args, rank, world, local):
+    """Batched block-diagonal preconditioner: 2000 fibers with point counts
+    uniform in {16, 24, 32, 48, 64} (geometry of the step workload), their
+    4N x 4N systems assembled on the device (fiber3d's fiber operator with
+    BC rows), then factor + solve of all blocks captured in one CUDA graph
+    (two persistent launches plus a copy), panel width from the autotuner.
+    Baseline: scipy.linalg.lu_factor / lu_solve per block, the calls
+    fiber3d makes (tstep_utils.py:1405-1419, tstep.py:985-988)."""
+    import torch
+    import scipy.linalg as sla
+    from fiber3d_b200 import geometry, hydro as H
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    rng = np.random.default_rng(4)
+    npts = rng.choice([16, 24, 32, 48, 64], size=args.nblocks)
+    fibers = geometry.perturbed_fibers(rng, args.nblocks, npts, 2.0, 10.0, min_sep=0.05)
+    ff = np.concatenate([np.tile(rng.normal(scale=0.1, size=3), (n, 1)) for n in npts])
+    P = H.Problem(fibers, [2.0] * args.nblocks, 0.0025, 1e-3, 1.0, [], None, ff)
+    sysd = H.HydroSystem(P, device=dev)
+    lu = sysd.lu
+    A0 = lu.A.clone()
+    rhs = torch.as_tensor(rng.normal(size=lu.nvec), device=dev)
+    x = torch.empty_like(rhs)
+    panel = lu.tune_panel()
+    flop = float(sum(2.0 / 3.0 * (4 * n) ** 3 + 2.0 * (4 * n) ** 2 for n in npts))
+    def work():
+        lu.A.copy_(A0)
+        lu.factor()
+        x.copy_(rhs)
+        lu.solve(x)
+    for _ in range(args.warmup):
+        work()
+    torch.cuda.synchronize()
+    g = torch.cuda.CUDAGraph()
+    s2 = torch.cuda.Stream(dev)
+    s2.wait_stream(torch.cuda.current_stream(dev))
+    with torch.cuda.stream(s2):
+        work()
+    torch.cuda.current_stream(dev).wait_stream(s2)
+    with torch.cuda.graph(g):
+        work()
+    for _ in range(args.warmup):
+        g.replay()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        g.replay()
+    e1.record()
+    e1.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    # parity and CPU baseline on the same blocks
+    A_h = A0.cpu().numpy()
+    rhs_h = rhs.cpu().numpy()
+    xg = x.cpu().numpy()
+    blocks = [A_h[lu.moff_h[b]:lu.moff_h[b] + lu.sizes_h[b] ** 2].reshape(lu.sizes_h[b], lu.sizes_h[b])
+              for b in range(lu.count)]
+    t0 = time.perf_counter()
+    nb_cpu = 0
+    err = 0.0
+    while True:
+        for b, Ab in enumerate(blocks):
+            o, n = int(lu.voff_h[b]), int(lu.sizes_h[b])
+            xr = sla.lu_solve(sla.lu_factor(Ab, check_finite=False), rhs_h[o:o + n])
+            if nb_cpu == 0:
+                err = max(err, float(np.max(np.abs(xr - xg[o:o + n])) / np.max(np.abs(xr))))
+        nb_cpu += 1
+        if time.perf_counter() - t0 > min(10.0, args.cpu_seconds):
+            break
+    cpu_ms = (time.perf_counter() - t0) / nb_cpu * 1e3
+    line = {"metric": "block-diagonal preconditioner factor+solve time (ms)", "value": ms, "unit": "ms",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "higher_is_better": False,
+            "dtype": "f64", "data": "synthetic (seeded)",
+            "config": {"workload": "block_pc", "blocks": args.nblocks, "block_sizes": "4N, N in {16,24,32,48,64}",
+                       "panel": panel, "graph": "copy + factor + copy + solve, one CUDA graph"},
+            "gflops": flop / (ms * 1e-3) / 1e9, "max_rel_err_vs_scipy": err,
+            "cpu_baseline": {"value": cpu_ms, "unit": "ms", "cores": os.cpu_count(), "kind": "reference",
+                             "sample": f"scipy.linalg.lu_factor + lu_solve over all {args.nblocks} blocks, "
+                                       f"{nb_cpu} pass(es)"}}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -425,7 +541,11 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="stresslet_sphere",
-                    choices=["stresslet_sphere", "oseen_fibers", "hydro_step"])
+                    choices=["stresslet_sphere", "oseen_fibers", "hydro_step", "block_pc"])
+    ap.add_argument("--nblocks", type=int, default=2000)
+    ap.add_argument("--train-seeds", type=int, nargs="*", default=[11, 12, 13, 14])
+    ap.add_argument("--train-steps", type=int, default=25)
+    ap.add_argument("--train-epochs", type=int, default=30)
     ap.add_argument("--nshell", type=int, default=12000)
     ap.add_argument("--nfib", type=int, default=512)
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
@@ -445,6 +565,8 @@ def main():
     try:
         if args.workload == "hydro_step":
             hydro_arm(args, rank, world, local)
+        elif args.workload == "block_pc":
+            block_pc_arm(args, rank, world, local)
         else:
             gpu_arm(args, rank, world, local)
     finally:

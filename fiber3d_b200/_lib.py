@@ -104,6 +104,8 @@ SIGNATURES: dict[str, list] = {
     "f3d_fiber_weight": [ctypes.POINTER(FiberSetC), _P, _P, _I64, _P],
     "f3d_fiber_residual": [ctypes.POINTER(FiberSetC), _P, _P, _P, _P, _P, ctypes.c_int32, _P],
     "f3d_batched_lu_factor": [_P, _P, _P, _P, _P, ctypes.c_int32, ctypes.c_int32, _P, _P, _P, _SZ, _P],
+    "f3d_batched_lu_factor_panel": [_P, _P, _P, _P, _P, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, _P, _P,
+                                    _P, _SZ, _P],
     "f3d_batched_lu_solve": [_P, _P, _P, _P, _P, ctypes.c_int32, ctypes.c_int32, _P, _P, _P, _SZ, _P],
 }
 _RESTYPE = {"f3d_version": ctypes.c_char_p, "f3d_status_string": ctypes.c_char_p}

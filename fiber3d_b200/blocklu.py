@@ -54,6 +54,37 @@ class BlockLU:
         for b, M in enumerate(blocks):
             self.block(b).copy_(torch.as_tensor(np.asarray(M, dtype=np.float64)))
 
+    panel = 0  # panel width of the factorisation (0: size-based default)
+
+    def tune_panel(self, reps: int = 3) -> int:
+        """Time the panel widths 8/16/32 on the current blocks and keep the
+        fastest (restores the blocks afterwards)."""
+        saved = self.A.clone()
+        best, best_t = 0, float("inf")
+        for p in (8, 16, 32):
+            from ._lib import F3DError
+            try:
+                self.A.copy_(saved)
+                self.panel = p
+                self.factor()
+                torch.cuda.synchronize()
+                t = float("inf")
+                for _ in range(reps):
+                    self.A.copy_(saved)
+                    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                    e0.record()
+                    self.factor()
+                    e1.record()
+                    e1.synchronize()
+                    t = min(t, e0.elapsed_time(e1))
+            except F3DError:
+                continue
+            if t < best_t:
+                best, best_t = p, t
+        self.A.copy_(saved)
+        self.panel = best
+        return best
+
     def factor(self, blocks=None) -> None:
         """Factor every block, or only the listed block indices."""
         if self.count == 0:
@@ -71,8 +102,8 @@ class BlockLU:
             if count == 0:
                 return
         mx = self.max_n if blocks is None else int(self.sizes_h[list(blocks)].max())
-        _lib.call("f3d_batched_lu_factor", _lib.ptr(self.A), _lib.ptr(self.moff), _lib.ptr(self.voff),
-                  _lib.ptr(self.sizes), _lib.ptr(order), count, mx,
+        _lib.call("f3d_batched_lu_factor_panel", _lib.ptr(self.A), _lib.ptr(self.moff), _lib.ptr(self.voff),
+                  _lib.ptr(self.sizes), _lib.ptr(order), count, mx, int(self.panel),
                   _lib.ptr(self.piv), _lib.ptr(self.info), _lib.ptr(self.ws), self.ws.numel(),
                   _lib.stream_handle(self.device))
 

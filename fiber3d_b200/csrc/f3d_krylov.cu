@@ -12,6 +12,7 @@
 //   norm/scale: beta = |w|, V[k] = w / beta, H column written to `hcol`
 //   gemv:       y = M x for row-major M (FP64 or FP32 storage, FP64 sum)
 #include <algorithm>
+#include <type_traits>
 
 #include "f3d_common.cuh"
 
@@ -140,14 +141,16 @@ __global__ void bump_kernel(int *kptr) {
 
 // y = M x, M row-major rows x cols.  Each warp owns kRowsPerWarp rows of a
 // group; x is staged through shared memory in chunks shared by the 32 rows of
-// the CTA's group, so M streams from HBM once and x mostly from L2.
-template <typename T>
+// the CTA's group, so M streams from HBM once and x mostly from L2.  With
+// VEC > 1 each lane loads VEC consecutive elements (16 bytes) per access; the
+// caller guarantees 16-byte aligned rows (ld and cols multiples of VEC).
+template <typename T, int VEC>
 __global__ void __launch_bounds__(256) gemv_kernel(const T *__restrict__ M,
                                                    const double *__restrict__ x, double *y,
                                                    int64_t rows, int64_t cols, int64_t ld) {
   constexpr int kXChunk = 4096;
   constexpr int kRowsPerWarp = 4;
-  __shared__ double xs[kXChunk];
+  __shared__ __align__(16) double xs[kXChunk];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int warps = blockDim.x >> 5;
   const int64_t group = static_cast<int64_t>(warps) * kRowsPerWarp;
@@ -168,8 +171,30 @@ __global__ void __launch_bounds__(256) gemv_kernel(const T *__restrict__ M,
         if (r < rows) {
           const T *row = M + r * ld + c0;
           double a = acc[q];
+          if (VEC == 1) {
 #pragma unroll 4
-          for (int i = lane; i < cw; i += 32) a = fma(static_cast<double>(row[i]), xs[i], a);
+            for (int i = lane; i < cw; i += 32) a = fma(static_cast<double>(row[i]), xs[i], a);
+          } else if constexpr (sizeof(T) == 8) {
+            const double2 *rv = reinterpret_cast<const double2 *>(row);
+            const int nv = cw / 2;
+#pragma unroll 2
+            for (int i = lane; i < nv; i += 32) {
+              const double2 d = rv[i];
+              a = fma(d.x, xs[2 * i], a);
+              a = fma(d.y, xs[2 * i + 1], a);
+            }
+          } else {
+            const float4 *rv = reinterpret_cast<const float4 *>(row);
+            const int nv = cw / 4;
+#pragma unroll 2
+            for (int i = lane; i < nv; i += 32) {
+              const float4 f = rv[i];
+              a = fma(static_cast<double>(f.x), xs[4 * i], a);
+              a = fma(static_cast<double>(f.y), xs[4 * i + 1], a);
+              a = fma(static_cast<double>(f.z), xs[4 * i + 2], a);
+              a = fma(static_cast<double>(f.w), xs[4 * i + 3], a);
+            }
+          }
           acc[q] = a;
         }
       }
@@ -280,12 +305,24 @@ int f3d_gemv(int precision, const void *M, int64_t ld, const double *x, double *
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   const unsigned grid = static_cast<unsigned>(std::max<int64_t>(
       1, std::min<int64_t>((rows + 31) / 32, static_cast<int64_t>(f3d::sm_count()) * 4)));
-  if (precision == F3D_FP64)
-    f3d::gemv_kernel<double><<<grid, 256, 0, st>>>(static_cast<const double *>(M), x, y, rows, cols, ld);
-  else if (precision == F3D_FP32C)
-    f3d::gemv_kernel<float><<<grid, 256, 0, st>>>(static_cast<const float *>(M), x, y, rows, cols, ld);
-  else
+  // 16-byte vector loads when every row starts 16-byte aligned and the x
+  // chunks (4096 elements) split into whole vectors.
+  const uintptr_t base = reinterpret_cast<uintptr_t>(M);
+  if (precision == F3D_FP64) {
+    const bool vec = (base % 16 == 0) && (ld % 2 == 0) && (cols % 2 == 0);
+    if (vec)
+      f3d::gemv_kernel<double, 2><<<grid, 256, 0, st>>>(static_cast<const double *>(M), x, y, rows, cols, ld);
+    else
+      f3d::gemv_kernel<double, 1><<<grid, 256, 0, st>>>(static_cast<const double *>(M), x, y, rows, cols, ld);
+  } else if (precision == F3D_FP32C) {
+    const bool vec = (base % 16 == 0) && (ld % 4 == 0) && (cols % 4 == 0);
+    if (vec)
+      f3d::gemv_kernel<float, 4><<<grid, 256, 0, st>>>(static_cast<const float *>(M), x, y, rows, cols, ld);
+    else
+      f3d::gemv_kernel<float, 1><<<grid, 256, 0, st>>>(static_cast<const float *>(M), x, y, rows, cols, ld);
+  } else {
     return F3D_ERR_ARG;
+  }
   return f3d::launch_status();
 }
 

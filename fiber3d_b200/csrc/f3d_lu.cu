@@ -347,23 +347,33 @@ int f3d_batched_lu_workspace_bytes(size_t *bytes) {
   return F3D_OK;
 }
 
-int f3d_batched_lu_factor(double *A, const int64_t *matrix_offsets, const int64_t *vector_offsets,
-                          const int32_t *sizes, const int32_t *order, int32_t count, int32_t max_n,
-                          int32_t *piv, int32_t *info, void *workspace, size_t workspace_bytes,
-                          void *stream) {
+int f3d_batched_lu_factor_panel(double *A, const int64_t *matrix_offsets,
+                                const int64_t *vector_offsets, const int32_t *sizes,
+                                const int32_t *order, int32_t count, int32_t max_n, int32_t panel,
+                                int32_t *piv, int32_t *info, void *workspace,
+                                size_t workspace_bytes, void *stream) {
   if (count < 0 || max_n < 0) return F3D_ERR_SHAPE;
   if (count == 0) return F3D_OK;
   if (!A || !matrix_offsets || !vector_offsets || !sizes || !piv || !info) return F3D_ERR_NULL;
   if (!workspace || workspace_bytes < 256) return F3D_ERR_WORKSPACE;
   if (!f3d::aligned(A, 8)) return F3D_ERR_ALIGN;
-  const int nb = f3d::pick_nb(max_n);
-  if (nb == 0) return F3D_ERR_TOO_LARGE;
+  if (panel != 0 && panel != 8 && panel != 16 && panel != 32) return F3D_ERR_ARG;
+  const int nb = panel ? panel : f3d::pick_nb(max_n);
+  if (nb == 0 || f3d::factor_smem(nb, max_n) > 220 * 1024) return F3D_ERR_TOO_LARGE;
   f3d::LuArgs a{A, matrix_offsets, vector_offsets, sizes, order, piv, info,
                 static_cast<unsigned *>(workspace), count};
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   if (nb == 32) return f3d::launch_factor<32>(a, max_n, st);
   if (nb == 16) return f3d::launch_factor<16>(a, max_n, st);
   return f3d::launch_factor<8>(a, max_n, st);
+}
+
+int f3d_batched_lu_factor(double *A, const int64_t *matrix_offsets, const int64_t *vector_offsets,
+                          const int32_t *sizes, const int32_t *order, int32_t count, int32_t max_n,
+                          int32_t *piv, int32_t *info, void *workspace, size_t workspace_bytes,
+                          void *stream) {
+  return f3d_batched_lu_factor_panel(A, matrix_offsets, vector_offsets, sizes, order, count, max_n, 0,
+                                     piv, info, workspace, workspace_bytes, stream);
 }
 
 int f3d_batched_lu_solve(const double *LU, const int64_t *matrix_offsets,

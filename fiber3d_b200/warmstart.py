@@ -253,13 +253,19 @@ def march(system, steps: int, guess: str = "zero", net: FiberMLP | None = None, 
         e1.synchronize()
         sol = res["x"]
         st = {"iterations": res["iterations"], "solve_ms": e0.elapsed_time(e1),
-              "initial_rel_residual": res["history"][0]}
+              "initial_rel_residual": res["history"][0], "converged": res["info"] == 0}
+        stats.append(st)
+        if res["info"] != 0 or not bool(torch.isfinite(sol).all()):
+            break  # a trajectory that stops converging ends here; its step is not recorded
         if record:
             T, f = solution_targets(system, sol)
-            feats.append(X_feat)
-            targs.append(fiber_targets(T, f, n))
-        stats.append(st)
+            y = fiber_targets(T, f, n)
+            if bool(torch.isfinite(X_feat).all() and torch.isfinite(y).all()):
+                feats.append(X_feat)
+                targs.append(y)
         x_prev = sol
     if record:
-        return stats, torch.cat(feats), torch.cat(targs)
+        empty = torch.zeros((0, 192), dtype=torch.float32, device=system.device)
+        return (stats, torch.cat(feats) if feats else empty,
+                torch.cat(targs) if targs else empty[:, :128])
     return stats

@@ -217,6 +217,14 @@ int f3d_batched_lu_factor(double *A, const int64_t *matrix_offsets,
                           int32_t *piv, int32_t *info, void *workspace,
                           size_t workspace_bytes, void *stream);
 
+/* f3d_batched_lu_factor with an explicit panel width (columns factored in
+   shared memory per step): 8, 16 or 32, or 0 for the size-based default. */
+int f3d_batched_lu_factor_panel(double *A, const int64_t *matrix_offsets,
+                                const int64_t *vector_offsets, const int32_t *sizes,
+                                const int32_t *order, int32_t count, int32_t max_n,
+                                int32_t panel, int32_t *piv, int32_t *info, void *workspace,
+                                size_t workspace_bytes, void *stream);
+
 /* Solves every factored system in place: x + vector_offsets[b] holds the
    right-hand side on entry and the solution on exit.  Replaces
    scipy.linalg.lu_solve per block in P_inv (tstep/tstep.py:950-994). */
