@@ -373,47 +373,48 @@ def hydro_arm(args, rank, world, local):
     torch.cuda.synchronize()
     setup_s = time.perf_counter() - t0
     out, xs = {}, {}
-    # learned warm start: training pairs from the plain solver's own steps on
-    # seeds disjoint from the benchmark trajectory, then the network is trained
-    # on the GPU by the library's kernels
+    # learned warm start: training pairs (history features -> correction of
+    # the quadratic extrapolation) from the solver's own steps on seeds
+    # disjoint from the benchmark trajectory; the network is trained on the
+    # GPU by the library's kernels
     from fiber3d_b200 import warmstart as W
     t0 = time.perf_counter()
     feats, targs = [], []
     for seed in args.train_seeds:
         Pt = geometry.hydro_step_problem(seed=seed, nshell=args.nshell, nfib=args.nfib)
         st_ = H.HydroSystem(Pt, shell_op=shell, device=dev)
-        _, Xf, Tf = W.march(st_, args.train_steps, guess="previous", record=True)
+        _, Xf, Tf = W.march(st_, args.train_steps, guess="extrapolate", record=True)
         feats.append(Xf)
         targs.append(Tf)
         del st_
     X_train, T_train = torch.cat(feats), torch.cat(targs)
-    net = W.FiberMLP(seed=0, device=dev)
-    net.set_normalisation(X_train, T_train)
-    hist = net.train(X_train, T_train, epochs=args.train_epochs, batch=1024, lr=1e-3)
+    net = W.LearnedWarmStart(seed=0, device=dev)
+    hist = net.fit(X_train, T_train, epochs=args.train_epochs, batch=1024, lr=1e-3)
     torch.cuda.synchronize()
     train = {"samples": int(X_train.shape[0]), "seconds": time.perf_counter() - t0,
-             "loss_first_last": [hist[0], hist[-1]], "seeds": list(args.train_seeds),
-             "steps_per_seed": args.train_steps}
-    for mode in ("fp64", "mixed", "learned_mixed", "previous_fp64"):
-        mixed = mode in ("mixed", "learned_mixed")
+             "loss_first_last": [hist[0], hist[-1]], "gain": net.gain.tolist(),
+             "seeds": list(args.train_seeds), "steps_per_seed": args.train_steps}
+    modes = {"fp64": ("zero", False), "mixed": ("zero", False), "extrapolate_fp64": ("extrapolate", False),
+             "learned_fp64": ("learned", False), "learned_mixed": ("learned", True)}
+    modes["mixed"] = ("zero", True)
+    for mode, (guess, mixed) in modes.items():
         sysd = H.HydroSystem(P, shell_op=shell, device=dev, tune=True)
-        sol = None
-        times, its, resid, phases = [], [], [], []
+        history = []
+        times, its, resid, phases, r0s = [], [], [], [], []
         for step in range(args.warmup + args.steps):
             torch.cuda.synchronize()
             sysd.timers.report()
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record()
-            if sol is not None:
-                sysd.advance(sol)
+            if history:
+                sysd.advance(history[-1])
+            sysd.timers.start("warm_start")
             x0 = None
-            if mode == "learned_mixed":
-                sysd.timers.start("warm_start")
-                u_bg = W.background_velocity(sysd, sol)
-                x0 = W.guess_from_prediction(sysd, net.predict(W.fiber_features(sysd.x_fib, u_bg, 32)), u_bg, sol)
-                sysd.timers.stop("warm_start")
-            elif mode == "previous_fp64":
-                x0 = sol
+            if guess == "extrapolate":
+                x0 = W.extrapolate(history)
+            elif guess == "learned":
+                x0 = W.learned_guess(sysd, history, net)
+            sysd.timers.stop("warm_start")
             sysd.timers.start("GMRES")
             res = sysd.solve(tol=1e-8, restart=100, mixed=mixed, x0=x0)
             sysd.timers.stop("GMRES")
@@ -421,9 +422,11 @@ def hydro_arm(args, rank, world, local):
             e1.synchronize()
             ph = sysd.timers.report()
             sol = res["x"]
+            history = (history + [sol])[-W.HISTORY:]
             if step >= args.warmup:
                 times.append(e0.elapsed_time(e1))
                 its.append(res["iterations"])
+                r0s.append(res["history"][0])
                 phases.append(ph)
                 y = torch.empty_like(sol)
                 sysd.matvec(sol, y)
@@ -432,10 +435,12 @@ def hydro_arm(args, rank, world, local):
                 xs[mode] = sol.clone()
         out[mode] = {"ms_per_step": statistics.median(times), "iterations": its,
                      "true_rel_residual": max(resid), "refinements": res.get("refinements", 0),
-                     "initial_rel_residual": res["history"][0],
+                     "initial_rel_residual": r0s,
                      "phases_ms": {k: statistics.median([p.get(k, 0.0) for p in phases]) for k in phases[0]}}
         del sysd
-    for mode in ("mixed", "learned_mixed", "previous_fp64"):
+    for mode in modes:
+        if mode == "fp64":
+            continue
         out[mode]["rel_diff_vs_fp64_first_step"] = float(
             torch.linalg.vector_norm(xs[mode] - xs["fp64"]) / torch.linalg.vector_norm(xs["fp64"]))
         out[mode]["speedup_vs_fp64"] = out["fp64"]["ms_per_step"] / out[mode]["ms_per_step"]
@@ -543,9 +548,9 @@ def main():
     ap.add_argument("--workload", default="stresslet_sphere",
                     choices=["stresslet_sphere", "oseen_fibers", "hydro_step", "block_pc"])
     ap.add_argument("--nblocks", type=int, default=2000)
-    ap.add_argument("--train-seeds", type=int, nargs="*", default=[11, 12, 13, 14])
-    ap.add_argument("--train-steps", type=int, default=25)
-    ap.add_argument("--train-epochs", type=int, default=30)
+    ap.add_argument("--train-seeds", type=int, nargs="*", default=list(range(11, 19)))
+    ap.add_argument("--train-steps", type=int, default=30)
+    ap.add_argument("--train-epochs", type=int, default=40)
     ap.add_argument("--nshell", type=int, default=12000)
     ap.add_argument("--nfib", type=int, default=512)
     ap.add_argument("--cpu-seconds", type=float, default=10.0)

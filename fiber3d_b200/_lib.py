@@ -89,6 +89,7 @@ SIGNATURES: dict[str, list] = {
     "f3d_krylov_combine": [_P, _I64, _P, ctypes.c_int32, _P, _I64, _I, _P],
     "f3d_krylov_norm": [_P, _I64, _P, _P, _P, _P, _SZ, _P],
     "f3d_krylov_scale_into": [_P, _P, _P, _P, _I64, _I64, _I, _P, _P],
+    "f3d_krylov_store": [_P, _P, ctypes.c_int32, _P, _I64, _I64, _P],
     "f3d_gemv": [_I, _P, _I64, _P, _P, _I64, _I64, _P],
     "f3d_cast_to_float": [_P, _P, _I64, _P],
     "f3d_gemm_bf16": [_P, _I64, _I64, _P, _I64, _I64, _P, _I64, ctypes.c_int32, ctypes.c_int32,
@@ -107,6 +108,10 @@ SIGNATURES: dict[str, list] = {
     "f3d_batched_lu_factor_panel": [_P, _P, _P, _P, _P, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, _P, _P,
                                     _P, _SZ, _P],
     "f3d_batched_lu_solve": [_P, _P, _P, _P, _P, ctypes.c_int32, ctypes.c_int32, _P, _P, _P, _SZ, _P],
+    "f3d_quantize_rows_f16": [_P, _I64, _I64, _I64, ctypes.c_int32, _P, _I64, _P, _P, _P],
+    "f3d_gemv_f16": [_P, _I64, _P, _P, ctypes.c_int32, _P, _P, _I64, _I64, _P],
+    "f3d_batched_inverse": [_P, _P, _P, ctypes.c_int32, ctypes.c_int32, _P, _P, _P],
+    "f3d_block_gemv": [_I, _P, _P, _P, _P, ctypes.c_int32, ctypes.c_int32, _P, _P, _P],
 }
 _RESTYPE = {"f3d_version": ctypes.c_char_p, "f3d_status_string": ctypes.c_char_p}
 

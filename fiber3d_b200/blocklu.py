@@ -114,6 +114,32 @@ class BlockLU:
             b = int(bad[0])
             raise ZeroDivisionError(f"block {b}: zero pivot at step {int(self.info[b])}")
 
+    A32 = None  # FP32 copy of the inverses (invert(fp32=True))
+
+    def invert(self, fp32: bool = True) -> None:
+        """Replace every block by its explicit inverse (Gauss-Jordan, blocks up
+        to 128), and with ``fp32`` also keep an FP32 copy; :meth:`apply` then
+        evaluates the preconditioner as one streaming pass over the blocks."""
+        if self.count == 0:
+            return
+        if fp32 and self.A32 is None:
+            self.A32 = torch.zeros(self.A.numel(), dtype=torch.float32, device=self.device)
+        _lib.call("f3d_batched_inverse", _lib.ptr(self.A), _lib.ptr(self.moff), _lib.ptr(self.sizes), self.count,
+                  self.max_n, _lib.ptr(self.A32) if fp32 else None, _lib.ptr(self.info),
+                  _lib.stream_handle(self.device))
+
+    def apply(self, x: torch.Tensor, y: torch.Tensor, precision: str = "fp64") -> torch.Tensor:
+        """y = blockdiag(inverses) x after :meth:`invert` (x, y distinct,
+        packed like the right-hand side of :meth:`solve`)."""
+        if self.count:
+            M = self.A if precision == "fp64" else self.A32
+            if M is None:
+                raise RuntimeError("no FP32 inverses: call invert(fp32=True)")
+            _lib.call("f3d_block_gemv", _lib.PRECISION[precision], _lib.ptr(M), _lib.ptr(self.moff),
+                      _lib.ptr(self.voff), _lib.ptr(self.sizes), self.count, self.max_n, _lib.ptr(x), _lib.ptr(y),
+                      _lib.stream_handle(self.device))
+        return y
+
     def solve(self, x: torch.Tensor) -> torch.Tensor:
         """Solve in place for a packed right-hand side of length sum(sizes)."""
         if x.numel() != self.nvec or x.dtype != torch.float64 or not x.is_contiguous():

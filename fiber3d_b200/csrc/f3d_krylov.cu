@@ -11,6 +11,11 @@
 //   multiaxpy:  w -= sum_{i<k} h[i] V[i]
 //   norm/scale: beta = |w|, V[k] = w / beta, H column written to `hcol`
 //   gemv:       y = M x for row-major M (FP64 or FP32 storage, FP64 sum)
+//   gemv_f16:   the same product from FP16 storage with a power-of-two scale
+//               per row and the diagonal blocks kept apart in FP64 (the
+//               preconditioner of the mixed-precision inner solves)
+#include <cuda_fp16.h>
+
 #include <algorithm>
 #include <type_traits>
 
@@ -135,6 +140,17 @@ __global__ void scale_into_kernel(const double *__restrict__ w, const double *be
   }
 }
 
+// dst[(*k + offset) * ld + j] = src[j]
+__global__ void store_row_kernel(const double *__restrict__ src, const int *kptr, int offset,
+                                 double *dst, int64_t n, int64_t ld) {
+  const int row = *kptr + offset;
+  if (row < 0) return;
+  double *d = dst + static_cast<int64_t>(row) * ld;
+  for (int64_t j = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; j < n;
+       j += static_cast<int64_t>(gridDim.x) * blockDim.x)
+    d[j] = src[j];
+}
+
 __global__ void bump_kernel(int *kptr) {
   if (threadIdx.x == 0 && blockIdx.x == 0) *kptr += 1;
 }
@@ -205,6 +221,132 @@ __global__ void __launch_bounds__(256) gemv_kernel(const T *__restrict__ M,
 #pragma unroll
       for (int off = 16; off > 0; off >>= 1) a += __shfl_xor_sync(0xffffffffu, a, off);
       if (lane == 0 && rw + q < rows) y[rw + q] = a;
+    }
+  }
+}
+
+// Row r of M (cols entries) -> FP16 row of M16 scaled by row_scale[r] = 2^e,
+// the smallest power of two >= max |M[r][c]| over the columns outside r's
+// diagonal block; the block's entries (columns db*(r/db) .. +db-1) go to
+// diag[r*db + c] in FP64 and are zero in M16.  One warp per row.
+__global__ void quantize_rows_f16_kernel(const double *__restrict__ M, int64_t ld, int64_t rows,
+                                         int64_t cols, int db, __half *__restrict__ M16,
+                                         int64_t ld16, float *__restrict__ row_scale,
+                                         double *__restrict__ diag) {
+  const int lane = threadIdx.x & 31;
+  const int64_t warp = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+  const int64_t nwarps = (static_cast<int64_t>(gridDim.x) * blockDim.x) >> 5;
+  for (int64_t r = warp; r < rows; r += nwarps) {
+    const double *row = M + r * ld;
+    const int64_t b0 = db > 0 ? (r / db) * db : -1;
+    const int64_t b1 = db > 0 ? b0 + db : -1;
+    double mx = 0.0;
+    for (int64_t c = lane; c < cols; c += 32)
+      if (c < b0 || c >= b1) mx = fmax(mx, fabs(row[c]));
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, off));
+    int e = 0;
+    if (mx > 0.0) frexp(mx, &e);  // mx = m 2^e, m in [0.5, 1)
+    const double s = ldexp(1.0, e);
+    const double inv = 1.0 / s;  // exact: a power of two
+    __half *out = M16 + r * ld16;
+    for (int64_t c = lane; c < cols; c += 32) {
+      const bool in_block = c >= b0 && c < b1;
+      out[c] = __double2half(in_block ? 0.0 : row[c] * inv);
+      if (in_block) diag[r * db + (c - b0)] = row[c];
+    }
+    if (lane == 0) row_scale[r] = static_cast<float>(s);
+  }
+}
+
+// y = diag(row_scale) M16 x + blockdiag(diag) x.  Same row/warp layout as
+// gemv_kernel; x chunk staged as FP32, products summed in FP32.
+template <int VEC>
+__global__ void __launch_bounds__(256) gemv_f16_kernel(const __half *__restrict__ M, int64_t ld,
+                                                       const float *__restrict__ row_scale,
+                                                       const double *__restrict__ diag, int db,
+                                                       const double *__restrict__ x, double *y,
+                                                       int64_t rows, int64_t cols) {
+  constexpr int kXChunk = 8192;
+  constexpr int kRowsPerWarp = 4;
+  __shared__ __align__(16) float xs[kXChunk];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int warps = blockDim.x >> 5;
+  const int64_t group = static_cast<int64_t>(warps) * kRowsPerWarp;
+  for (int64_t rb = static_cast<int64_t>(blockIdx.x) * group; rb < rows;
+       rb += static_cast<int64_t>(gridDim.x) * group) {
+    float acc[kRowsPerWarp];
+#pragma unroll
+    for (int q = 0; q < kRowsPerWarp; ++q) acc[q] = 0.0f;
+    const int64_t rw = rb + static_cast<int64_t>(warp) * kRowsPerWarp;
+    for (int64_t c0 = 0; c0 < cols; c0 += kXChunk) {
+      const int cw = static_cast<int>((cols - c0 < kXChunk) ? (cols - c0) : kXChunk);
+      __syncthreads();
+      for (int i = threadIdx.x; i < cw; i += blockDim.x) xs[i] = static_cast<float>(x[c0 + i]);
+      __syncthreads();
+      if (VEC == 1) {
+#pragma unroll
+        for (int q = 0; q < kRowsPerWarp; ++q) {
+          const int64_t r = rw + q;
+          if (r < rows) {
+            const __half *row = M + r * ld + c0;
+            float a = acc[q];
+#pragma unroll 4
+            for (int i = lane; i < cw; i += 32) a = fmaf(__half2float(row[i]), xs[i], a);
+            acc[q] = a;
+          }
+        }
+      } else {
+        // the kRowsPerWarp rows advance together: that many independent
+        // 16-byte loads in flight per lane per iteration
+        const uint4 *rv[kRowsPerWarp];
+#pragma unroll
+        for (int q = 0; q < kRowsPerWarp; ++q) {
+          const int64_t r = rw + q < rows ? rw + q : rows - 1;  // clamped rows are not stored
+          rv[q] = reinterpret_cast<const uint4 *>(M + r * ld + c0);
+        }
+        const int nv = cw / 8;
+#pragma unroll 2
+        for (int i = lane; i < nv; i += 32) {
+          uint4 u[kRowsPerWarp];
+#pragma unroll
+          for (int q = 0; q < kRowsPerWarp; ++q) u[q] = rv[q][i];
+          const float4 xa = *reinterpret_cast<const float4 *>(xs + 8 * i);
+          const float4 xb = *reinterpret_cast<const float4 *>(xs + 8 * i + 4);
+#pragma unroll
+          for (int q = 0; q < kRowsPerWarp; ++q) {
+            const float2 f0 = __half22float2(*reinterpret_cast<const __half2 *>(&u[q].x));
+            const float2 f1 = __half22float2(*reinterpret_cast<const __half2 *>(&u[q].y));
+            const float2 f2 = __half22float2(*reinterpret_cast<const __half2 *>(&u[q].z));
+            const float2 f3 = __half22float2(*reinterpret_cast<const __half2 *>(&u[q].w));
+            float a = acc[q];
+            a = fmaf(f0.x, xa.x, a);
+            a = fmaf(f0.y, xa.y, a);
+            a = fmaf(f1.x, xa.z, a);
+            a = fmaf(f1.y, xa.w, a);
+            a = fmaf(f2.x, xb.x, a);
+            a = fmaf(f2.y, xb.y, a);
+            a = fmaf(f3.x, xb.z, a);
+            a = fmaf(f3.y, xb.w, a);
+            acc[q] = a;
+          }
+        }
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < kRowsPerWarp; ++q) {
+      float a = acc[q];
+#pragma unroll
+      for (int off = 16; off > 0; off >>= 1) a += __shfl_xor_sync(0xffffffffu, a, off);
+      const int64_t r = rw + q;
+      if (lane == 0 && r < rows) {
+        double v = static_cast<double>(a) * static_cast<double>(row_scale[r]);
+        if (db > 0) {
+          const int64_t b0 = (r / db) * db;
+          for (int c = 0; c < db && b0 + c < cols; ++c) v = fma(diag[r * db + c], x[b0 + c], v);
+        }
+        y[r] = v;
+      }
     }
   }
 }
@@ -297,6 +439,15 @@ int f3d_krylov_scale_into(const double *w, const double *beta, int32_t *k, doubl
   return f3d::launch_status();
 }
 
+int f3d_krylov_store(const double *src, const int32_t *k, int32_t offset, double *dst,
+                     int64_t ld, int64_t n, void *stream) {
+  if (!src || !k || !dst) return F3D_ERR_NULL;
+  if (n <= 0 || ld < n) return F3D_ERR_SHAPE;
+  f3d::store_row_kernel<<<f3d::grid_for(n, 256), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+      src, k, offset, dst, n, ld);
+  return f3d::launch_status();
+}
+
 int f3d_gemv(int precision, const void *M, int64_t ld, const double *x, double *y, int64_t rows,
              int64_t cols, void *stream) {
   if (!M || !x || !y) return F3D_ERR_NULL;
@@ -323,6 +474,40 @@ int f3d_gemv(int precision, const void *M, int64_t ld, const double *x, double *
   } else {
     return F3D_ERR_ARG;
   }
+  return f3d::launch_status();
+}
+
+int f3d_quantize_rows_f16(const double *M, int64_t ld, int64_t rows, int64_t cols,
+                          int32_t diag_block, void *M16, int64_t ld16, float *row_scale,
+                          double *diag, void *stream) {
+  if (!M || !M16 || !row_scale) return F3D_ERR_NULL;
+  if (rows < 0 || cols < 0 || ld < cols || ld16 < cols || diag_block < 0) return F3D_ERR_SHAPE;
+  if (diag_block > 0 && (!diag || rows != cols || rows % diag_block != 0)) return F3D_ERR_ARG;
+  if (rows == 0) return F3D_OK;
+  const unsigned grid = static_cast<unsigned>(std::max<int64_t>(
+      1, std::min<int64_t>((rows + 7) / 8, static_cast<int64_t>(f3d::sm_count()) * 8)));
+  f3d::quantize_rows_f16_kernel<<<grid, 256, 0, static_cast<cudaStream_t>(stream)>>>(
+      M, ld, rows, cols, diag_block, static_cast<__half *>(M16), ld16, row_scale, diag);
+  return f3d::launch_status();
+}
+
+int f3d_gemv_f16(const void *M16, int64_t ld16, const float *row_scale, const double *diag,
+                 int32_t diag_block, const double *x, double *y, int64_t rows, int64_t cols,
+                 void *stream) {
+  if (!M16 || !row_scale || !x || !y) return F3D_ERR_NULL;
+  if (rows < 0 || cols < 0 || ld16 < cols || diag_block < 0) return F3D_ERR_SHAPE;
+  if (diag_block > 0 && !diag) return F3D_ERR_NULL;
+  if (rows == 0) return F3D_OK;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const unsigned grid = static_cast<unsigned>(std::max<int64_t>(
+      1, std::min<int64_t>((rows + 31) / 32, static_cast<int64_t>(f3d::sm_count()) * 4)));
+  const uintptr_t base = reinterpret_cast<uintptr_t>(M16);
+  const bool vec = (base % 16 == 0) && (ld16 % 8 == 0) && (cols % 8 == 0);
+  const __half *M = static_cast<const __half *>(M16);
+  if (vec)
+    f3d::gemv_f16_kernel<8><<<grid, 256, 0, st>>>(M, ld16, row_scale, diag, diag_block, x, y, rows, cols);
+  else
+    f3d::gemv_f16_kernel<1><<<grid, 256, 0, st>>>(M, ld16, row_scale, diag, diag_block, x, y, rows, cols);
   return f3d::launch_status();
 }
 

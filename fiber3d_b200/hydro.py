@@ -170,6 +170,7 @@ class ShellOperator:
         self.E = singularity_vectors(self.nodes, self.normals, self.weights, eta, reg, eps_dist)
         self.inv64 = None
         self.inv32 = None
+        self.inv16 = None
         if build_inverse:
             self.build_inverse()
 
@@ -190,6 +191,28 @@ class ShellOperator:
         self.inv32 = torch.empty(self.inv64.shape, dtype=torch.float32, device=self.device)
         _lib.call("f3d_cast_to_float", _lib.ptr(self.inv64), _lib.ptr(self.inv32), self.inv64.numel(),
                   _lib.stream_handle(self.device))
+        # FP16 rows scaled by powers of two, the 3x3 node blocks on the
+        # diagonal kept in FP64 (the inverse of this second-kind operator is
+        # dominated by them; the rest spans a few decades per row)
+        m = 3 * self.n
+        self.inv16 = torch.empty((m, m), dtype=torch.float16, device=self.device)
+        self.scale16 = torch.empty(m, dtype=torch.float32, device=self.device)
+        self.diag16 = torch.empty((m, 3), dtype=torch.float64, device=self.device)
+        _lib.call("f3d_quantize_rows_f16", _lib.ptr(self.inv64), m, m, m, 3, _lib.ptr(self.inv16), m,
+                  _lib.ptr(self.scale16), _lib.ptr(self.diag16), _lib.stream_handle(self.device))
+
+    def apply(self, x: torch.Tensor, y: torch.Tensor, storage: str = "fp64") -> torch.Tensor:
+        """y = P_shell^-1 x from the FP64, FP32 or FP16 copy of the inverse."""
+        m = 3 * self.n
+        st = _lib.stream_handle(self.device)
+        if storage == "fp16":
+            _lib.call("f3d_gemv_f16", _lib.ptr(self.inv16), m, _lib.ptr(self.scale16), _lib.ptr(self.diag16), 3,
+                      _lib.ptr(x), _lib.ptr(y), m, m, st)
+        else:
+            M = self.inv64 if storage == "fp64" else self.inv32
+            _lib.call("f3d_gemv", _lib.PRECISION["fp64" if storage == "fp64" else "fp32c"], _lib.ptr(M), m,
+                      _lib.ptr(x), _lib.ptr(y), m, m, st)
+        return y
 
 
 def singularity_vectors(nodes, normals, weights, eta, reg, eps) -> torch.Tensor:
@@ -246,7 +269,7 @@ class HydroSystem:
     :meth:`pc` (the right preconditioner P^-1) and :meth:`solve`."""
 
     def __init__(self, problem: Problem, shell_op: ShellOperator | None = None, device=None,
-                 tune: bool = False):
+                 tune: bool = False, fiber_pc: str = "auto", inner_shell_pc: str = "fp16"):
         self.p = problem
         dev = device or torch.device("cuda", torch.cuda.current_device())
         self.device = dev
@@ -341,6 +364,17 @@ class HydroSystem:
         # ---- right-hand side and preconditioner blocks
         self.rhs = torch.zeros(self.size, dtype=torch.float64, device=dev)
         self.lu = BlockLU(list(4 * self.fs.npts), device=dev)
+        # fiber blocks of the preconditioner: explicit inverses applied as a
+        # block GEMV (blocks up to 128), else LU factors and substitution
+        if fiber_pc == "auto":
+            fiber_pc = "inverse" if self.lu.max_n <= 128 else "lu"
+        if fiber_pc not in ("inverse", "lu"):
+            raise ValueError("fiber_pc must be 'auto', 'inverse' or 'lu'")
+        self.fiber_pc = fiber_pc
+        # storage of the periphery inverse read by the FP32-class preconditioner
+        if inner_shell_pc not in ("fp32", "fp16"):
+            raise ValueError("inner_shell_pc must be 'fp32' or 'fp16'")
+        self.inner_shell_pc = inner_shell_pc
         self.A_fib = torch.zeros(max(self.fs.mat_total, 1), dtype=torch.float64, device=dev)
         self.flow_ext = torch.zeros((max(nF, 1), 3), dtype=torch.float64, device=dev)
         self._body_blocks()
@@ -473,7 +507,10 @@ class HydroSystem:
                       _lib.ptr(self.A_fib), A_copy, _lib.ptr(self.rhs[self.o_fib:]), self.fs.max_n, st)
         self.timers.stop("Build_linear_system_fibers")
         self.timers.start("Build_PC_fibers")
-        self.lu.factor()
+        if self.fiber_pc == "inverse":
+            self.lu.invert(fp32=True)
+        else:
+            self.lu.factor()
         self.timers.stop("Build_PC_fibers")
 
     # ------------------------------------------------------------------------
@@ -514,9 +551,7 @@ class HydroSystem:
         st = _lib.stream_handle(self.device)
         nS = self.nS
         if nS:
-            M = self.shell.inv64 if precision == "fp64" else self.shell.inv32
-            _lib.call("f3d_gemv", _lib.PRECISION[precision], _lib.ptr(M), 3 * nS, _lib.ptr(x), _lib.ptr(y),
-                      3 * nS, 3 * nS, st)
+            self.shell.apply(x, y, "fp64" if precision == "fp64" else self.inner_shell_pc)
         if self.nbody:
             tb = self.body_tmp
             tb.copy_(x[3 * nS:self.o_fib])
@@ -530,9 +565,12 @@ class HydroSystem:
             _lib.call("f3d_rotate_blocks", _lib.ptr(y[3 * nS:]), _lib.ptr(self.rot_off), _lib.ptr(self.rot_nvec),
                       _lib.ptr(self.body_R), self.nbody, 0, st)
         if self.nF:
-            rest = y[self.o_fib:]
-            rest.copy_(x[self.o_fib:])
-            self.lu.solve(rest)
+            if self.fiber_pc == "inverse":
+                self.lu.apply(x[self.o_fib:], y[self.o_fib:], precision)
+            else:
+                rest = y[self.o_fib:]
+                rest.copy_(x[self.o_fib:])
+                self.lu.solve(rest)
         return y
 
     def solve(self, tol=1e-8, restart=100, maxiter=200, x0=None, mixed=False, **kw):

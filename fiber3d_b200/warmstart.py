@@ -1,33 +1,52 @@
-"""Learned GMRES warm start: a per-fiber network trained on the plain
-solver's own time steps.
+"""Learned GMRES warm start: a per-fiber network, trained on the solver's
+own time steps, that corrects the polynomial extrapolation of the last
+solutions.
 
-Network (per fiber of 32 points): input 192 = 32x3 positions (centred on the
-fiber's mean point) + 32x3 background velocity; 3 hidden layers of 256 with
-ReLU; output 128 = 32 tensions + 32x3 force densities.  Weights are kept in
-FP32 (master copy, Adam) and rounded to BF16 when staged for the tensor
-cores; every product runs in ``f3d_gemm_bf16`` (tcgen05, FP32 accumulation
-in tensor memory), the backward pass included.
+fiber3d starts every GMRES solve from zero (tstep/tstep.py:1209).  Along a
+trajectory the solution changes smoothly, so the quadratic extrapolation
+x_q = 3 x^n - 3 x^{n-1} + x^{n-2} of the last three solutions is already a
+close guess; what is left is mostly per fiber (its bending and tension
+dynamics).  The network predicts, per fiber of 32 points, the correction
+x^{n+1} - x_q on that fiber's unknowns (positions and tensions) from the
+fiber's recent differences, each in units of its own size so that nothing
+depends on how fast the fiber moves:
 
-Warm start for step n+1 from the prediction (T^, f^) (fiber3d's first-order
-scheme, tstep.py:628-1458):
-  fiber positions  X^ = X^n + dt (u_bg + M f^),   M f = c0 (f + xs (xs.f)) + c1 (f - xs (xs.f))
-                   (the local slender-body mobility, fiber.self_mobility, fiber.py:964-993)
-  tensions         T^
-  periphery / bodies: the previous step's values.
-Plain GMRES then runs from this guess to the same relative residual, so the
-converged answer does not depend on the network; what it changes is the
-number of iterations.
+  input  (260) = D2 X^n / s2_X (96),  D3 X^n / s3_X (96),
+                 D2 T^n / s2_T (32),  D3 T^n / s3_T (32),
+                 log10 of s3/s2 and s2/s1 for X and T (4)
+  output (128) = (X^{n+1} - X_q) / s3_X (96),  (T^{n+1} - T_q) / s3_T (32)
+
+where D1 X^n = X^n - X^{n-1}, D2 X^n = D1 X^n - D1 X^{n-1}, D3 X^n =
+X^n - 3 X^{n-1} + 3 X^{n-2} - X^{n-3} (note X^{n+1} - X_q = D3 X^{n+1}, so
+cubic extrapolation is the map output = D3 X^n / s3_X), and sk is the
+root-mean-square of Dk over the fiber.  The correction is
+projected on the first few Legendre modes along the fiber before it is used:
+a point-to-point wiggle in a position guess is multiplied by the fourth
+derivative in the bending operator, so the correction must be smooth to
+lower the residual.  A gain per unknown group (positions, tensions), fitted
+by least squares on held-out steps and kept in [0, 1], scales it; a network
+that learned nothing useful leaves the extrapolation unchanged.  Periphery
+and body unknowns take x_q.
+
+3 hidden layers of 256 with ReLU; weights kept in FP32 (master copy, Adam)
+and rounded to BF16 when staged for the tensor cores; every product runs in
+``f3d_gemm_bf16`` (tcgen05, FP32 accumulation in tensor memory), the
+backward pass included.  GMRES then runs from the corrected guess to the
+same relative residual, so the converged answer does not depend on the
+network; what it changes is the number of iterations.
 """
 from __future__ import annotations
-
-import ctypes
 
 import numpy as np
 import torch
 
 from . import _lib
 
-LAYERS = (192, 256, 256, 256, 128)
+LAYERS = (260, 256, 256, 256, 128)
+NPTS = 32          # points per fiber the network is built for
+CLIP = 50.0        # bound on normalised correction targets
+MODES = 10         # Legendre modes kept in a correction along the fiber
+HISTORY = 4        # solutions the features need
 
 
 def _gemm(A, a_rs, a_cs, B, b_rs, b_cs, C, ldc, M, N, K, bias=None, relu=False, mask=None, ldm=0,
@@ -161,91 +180,166 @@ class FiberMLP:
         return self.forward(Xn) * self.out_std + self.out_mean
 
 
-# ---------------------------------------------------------------- features --
-def fiber_features(x_fib: torch.Tensor, u_bg: torch.Tensor, npts: int = 32) -> torch.Tensor:
-    """(nfib, 192): positions centred per fiber, and background velocity."""
-    X = x_fib.view(-1, npts, 3)
-    Xc = X - X.mean(1, keepdim=True)
-    return torch.cat([Xc.reshape(-1, 3 * npts), u_bg.view(-1, 3 * npts)], dim=1).float()
+# ------------------------------------------------------- history features --
+def fiber_blocks(system, x: torch.Tensor) -> torch.Tensor:
+    """(nfib, 4, N) view of the fiber unknowns of x: rows X_x, X_y, X_z, T
+    (fiber3d's layout, tstep_utils.py:906-931)."""
+    return x[system.o_fib:].view(system.fs.nfib, 4, NPTS)
 
 
-def fiber_targets(T: torch.Tensor, f: torch.Tensor, npts: int = 32) -> torch.Tensor:
-    """(nfib, 128): tensions and force densities."""
-    return torch.cat([T.view(-1, npts), f.view(-1, 3 * npts)], dim=1).float()
+def learnable(system) -> bool:
+    """The network applies to systems whose fibers all have NPTS points."""
+    return system.fs.nfib > 0 and bool(np.all(system.fs.npts == NPTS))
 
 
-# ------------------------------------------------------------ time marching --
-def background_velocity(system, x_prev: torch.Tensor | None) -> torch.Tensor:
-    """Velocity on every fiber point from everything except the fiber itself:
-    the explicit flow of the external forces plus, when a previous solution
-    is given, the flow of its fiber forces, body and periphery densities
-    evaluated at the current geometry (one matvec's pair sums)."""
-    u = system.flow_ext.clone()
-    if x_prev is not None:
-        y = torch.empty_like(x_prev)
-        system.matvec(x_prev, y)
-        u += system.v.view(-1, 3)[:system.nF]
-    return u
+def extrapolate(history) -> torch.Tensor | None:
+    """Polynomial extrapolation of the last solutions (newest last):
+    constant, linear or quadratic with one, two or three of them."""
+    if not history:
+        return None
+    if len(history) == 1:
+        return history[-1].clone()
+    if len(history) == 2:
+        return 2.0 * history[-1] - history[-2]
+    return 3.0 * history[-1] - 3.0 * history[-2] + history[-3]
 
 
-def solution_targets(system, sol: torch.Tensor):
-    """(T, f): tensions and force densities f = -E X_ssss + (T X_s)_s of the
-    solved step, per fiber point (force operator at the solution)."""
-    nF = system.nF
-    f = torch.empty((nF, 3), dtype=torch.float64, device=sol.device)
-    XT = sol[system.o_fib:]
-    _lib.call("f3d_fiber_forces", ctypes.byref(system.fs.c), system.p.E, _lib.ptr(system.geo), _lib.ptr(XT),
-              _lib.ptr(f), nF, 0, _lib.stream_handle(sol.device))
-    n = int(system.fs.npts[0])
-    T = XT.view(-1, 4, n)[:, 3, :].reshape(-1)
-    return T, f
+def history_features(system, history):
+    """(nfib, 260) network input from the last four solutions, and the
+    per-fiber target scales s_X (nfib, 1, 1) and s_T (nfib, 1)."""
+    B = [fiber_blocks(system, h) for h in history[-4:]][::-1]  # newest first
+    X = [b[:, :3] for b in B]
+    T = [b[:, 3] for b in B]
+    d1X, d1T = X[0] - X[1], T[0] - T[1]
+    d2X, d2T = d1X - (X[1] - X[2]), d1T - (T[1] - T[2])
+    d3X = X[0] - 3.0 * X[1] + 3.0 * X[2] - X[3]
+    d3T = T[0] - 3.0 * T[1] + 3.0 * T[2] - T[3]
+    rmsX = lambda d: d.square().mean(dim=(1, 2), keepdim=True).sqrt() + 1e-300
+    rmsT = lambda d: d.square().mean(dim=1, keepdim=True).sqrt() + 1e-300
+    s1X, s2X, s3X = rmsX(d1X), rmsX(d2X), rmsX(d3X)
+    s1T, s2T, s3T = rmsT(d1T), rmsT(d2T), rmsT(d3T)
+    ratios = torch.cat([torch.log10(s3X / s2X).view(-1, 1), torch.log10(s3T / s2T),
+                        torch.log10(s2X / s1X).view(-1, 1), torch.log10(s2T / s1T)], dim=1)
+    feats = torch.cat([(d2X / s2X).flatten(1), (d3X / s3X).flatten(1), d2T / s2T, d3T / s3T, ratios], dim=1)
+    return feats.float().contiguous(), s3X, s3T
 
 
-def guess_from_prediction(system, pred: torch.Tensor, u_bg: torch.Tensor,
-                          x_prev: torch.Tensor | None) -> torch.Tensor:
-    """GMRES initial guess from network output (T^, f^) per fiber:
-    X^ = X^n + dt (u_bg + M f^) with the local slender-body mobility
-    M f = c0 (f + xs (xs.f)) + c1 (f - xs (xs.f)); periphery and body
-    unknowns from the previous solution (zero at the first step)."""
-    n = int(system.fs.npts[0])
-    nfib = system.fs.nfib
-    x0 = x_prev.clone() if x_prev is not None else torch.zeros(system.size, dtype=torch.float64,
-                                                               device=system.device)
-    pred = pred.double()
-    T = pred[:, :n]
-    f = pred[:, n:].reshape(nfib * n, 3)
-    xs = system.geo[:system.nF, 0:3]
-    xf = (xs * f).sum(1, keepdim=True)
-    Mf = system.c0 * (f + xs * xf) + system.c1 * (f - xs * xf)
-    X = system.x_fib + system.p.dt * (u_bg + Mf)
-    blk = x0[system.o_fib:].view(nfib, 4, n)
-    blk[:, :3, :] = X.view(nfib, n, 3).transpose(1, 2)
-    blk[:, 3, :] = T
+def mode_projection(npts: int = NPTS, modes: int = MODES, device=None) -> torch.Tensor:
+    """(npts, npts) orthogonal projection on the Legendre polynomials of
+    degree < modes sampled at the fiber's equispaced parameter points."""
+    s = np.linspace(-1.0, 1.0, npts)
+    V = np.polynomial.legendre.legvander(s, modes - 1)
+    Q, _ = np.linalg.qr(V)
+    return torch.as_tensor(Q @ Q.T, dtype=torch.float32, device=device)
+
+
+def correction_targets(system, x_new: torch.Tensor, x_q: torch.Tensor, sX, sT) -> torch.Tensor:
+    """(nfib, 128) normalised correction x_new - x_q on the fiber unknowns."""
+    d = fiber_blocks(system, x_new) - fiber_blocks(system, x_q)
+    t = torch.cat([(d[:, :3] / sX).flatten(1), d[:, 3] / sT], dim=1)
+    return t.clamp(-CLIP, CLIP).float().contiguous()
+
+
+def apply_correction(system, x_q: torch.Tensor, corr: torch.Tensor, sX, sT) -> torch.Tensor:
+    """x_q with a normalised correction (nfib, 128) added on the fiber unknowns."""
+    x0 = x_q.clone()
+    B = fiber_blocks(system, x0)
+    c = corr.double()
+    B[:, :3] += c[:, :3 * NPTS].view(-1, 3, NPTS) * sX
+    B[:, 3] += c[:, 3 * NPTS:] * sT
     return x0
 
 
-def march(system, steps: int, guess: str = "zero", net: FiberMLP | None = None, tol=1e-8,
+class LearnedWarmStart:
+    """FiberMLP + smoothing projection + held-out gains: the learned
+    correction of the quadratic extrapolation."""
+
+    def __init__(self, seed: int = 0, device=None, modes: int = MODES):
+        self.net = FiberMLP(seed=seed, device=device)
+        self.device = self.net.device
+        self.P = mode_projection(NPTS, modes, self.device)
+        self.gain = torch.ones(2, dtype=torch.float32, device=self.device)
+
+    def smooth(self, Y: torch.Tensor) -> torch.Tensor:
+        """Project each of the 4 rows (X, Y, Z, T) of a (B, 128) correction."""
+        return (Y.view(-1, 4, NPTS) @ self.P.T).reshape(-1, 4 * NPTS)
+
+    def predict(self, feats: torch.Tensor) -> torch.Tensor:
+        """Smoothed, gain-scaled normalised correction (B, 128)."""
+        C = self.smooth(self.net.predict(feats))
+        C[:, :3 * NPTS] *= self.gain[0]
+        C[:, 3 * NPTS:] *= self.gain[1]
+        return C
+
+    def fit(self, X: torch.Tensor, T: torch.Tensor, epochs=30, batch=1024, lr=1e-3, val_frac=0.1,
+            seed=0):
+        """Train on smoothed targets, then fit the gains on a held-out split.
+        Returns the training loss history."""
+        g = torch.Generator(device="cpu").manual_seed(seed)
+        perm = torch.randperm(X.shape[0], generator=g).to(X.device)
+        nval = max(1, int(val_frac * X.shape[0]))
+        iv, it = perm[:nval], perm[nval:]
+        Ts = self.smooth(T)
+        self.net.set_normalisation(X[it], Ts[it])
+        hist = self.net.train(X[it].contiguous(), Ts[it].contiguous(), epochs=epochs,
+                              batch=min(batch, max(1, it.numel())), lr=lr, seed=seed)
+        self.gain.fill_(1.0)
+        C = self.smooth(self.net.predict(X[iv].contiguous()))
+        Tv = T[iv]
+        for k, sl in enumerate((slice(0, 3 * NPTS), slice(3 * NPTS, 4 * NPTS))):
+            num = float((C[:, sl] * Tv[:, sl]).sum())
+            den = float((C[:, sl] * C[:, sl]).sum())
+            self.gain[k] = min(1.0, max(0.0, num / den)) if den > 0 else 0.0
+        return hist
+
+    def guess(self, system, history) -> torch.Tensor | None:
+        """The warm start: quadratic extrapolation, corrected by the network
+        once HISTORY solutions are known."""
+        x_q = extrapolate(history)
+        if x_q is None or len(history) < HISTORY or not learnable(system):
+            return x_q
+        f, sX, sT = history_features(system, history)
+        return apply_correction(system, x_q, self.predict(f), sX, sT)
+
+
+def learned_guess(system, history, model: LearnedWarmStart | None) -> torch.Tensor | None:
+    """Extrapolation plus the learned correction (plain extrapolation
+    without a model)."""
+    if model is None:
+        return extrapolate(history)
+    return model.guess(system, history)
+
+
+# ------------------------------------------------------------ time marching --
+def march(system, steps: int, guess: str = "zero", net: LearnedWarmStart | None = None, tol=1e-8,
           mixed=False, record=False, restart=100):
     """Advance `system` `steps` time steps; per step return iterations, time
     and (when record) the network's training pairs.
 
-    guess: 'zero' (fiber3d's GMRES start), 'previous' (last solution) or
-    'learned' (network prediction, then the same GMRES to the same residual).
+    guess: 'zero' (fiber3d's GMRES start), 'previous' (last solution),
+    'extrapolate' (quadratic extrapolation) or 'learned' (extrapolation plus
+    the network's correction); GMRES then runs to the same residual.
     """
-    x_prev = None
+    if guess not in ("zero", "previous", "extrapolate", "learned"):
+        raise ValueError(f"unknown guess {guess!r}")
+    history = []
     stats, feats, targs = [], [], []
-    n = int(system.fs.npts[0])
+    can_learn = learnable(system)
     for s in range(steps):
         if s > 0:
-            system.advance(x_prev)
-        u_bg = background_velocity(system, x_prev)
-        X_feat = fiber_features(system.x_fib, u_bg, n)
-        if guess == "learned" and net is not None:
-            x0 = guess_from_prediction(system, net.predict(X_feat), u_bg, x_prev)
-        elif guess in ("previous", "learned") and x_prev is not None:
-            x0 = x_prev
-        else:
+            system.advance(history[-1])
+        x_q = extrapolate(history)
+        f = None
+        if can_learn and len(history) >= HISTORY and (record or guess == "learned"):
+            f, sX, sT = history_features(system, history)
+        if guess == "zero":
             x0 = None
+        elif guess == "previous":
+            x0 = history[-1] if history else None
+        elif guess == "learned" and net is not None and f is not None:
+            x0 = apply_correction(system, x_q, net.predict(f), sX, sT)
+        else:
+            x0 = x_q
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
         res = system.solve(tol=tol, restart=restart, x0=x0, mixed=mixed)
@@ -257,15 +351,15 @@ def march(system, steps: int, guess: str = "zero", net: FiberMLP | None = None, 
         stats.append(st)
         if res["info"] != 0 or not bool(torch.isfinite(sol).all()):
             break  # a trajectory that stops converging ends here; its step is not recorded
-        if record:
-            T, f = solution_targets(system, sol)
-            y = fiber_targets(T, f, n)
-            if bool(torch.isfinite(X_feat).all() and torch.isfinite(y).all()):
-                feats.append(X_feat)
-                targs.append(y)
-        x_prev = sol
+        if record and f is not None:
+            y = correction_targets(system, sol, x_q, sX, sT)
+            ok = torch.isfinite(f).all(dim=1) & torch.isfinite(y).all(dim=1)
+            feats.append(f[ok])
+            targs.append(y[ok])
+        history = (history + [sol])[-HISTORY:]
     if record:
-        empty = torch.zeros((0, 192), dtype=torch.float32, device=system.device)
+        empty = torch.zeros((0, LAYERS[0]), dtype=torch.float32, device=system.device)
         return (stats, torch.cat(feats) if feats else empty,
-                torch.cat(targs) if targs else empty[:, :128])
+                torch.cat(targs) if targs else torch.zeros((0, LAYERS[-1]), dtype=torch.float32,
+                                                           device=system.device))
     return stats

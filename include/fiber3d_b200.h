@@ -234,6 +234,23 @@ int f3d_batched_lu_solve(const double *LU, const int64_t *matrix_offsets,
                          const int32_t *piv, double *x, void *workspace,
                          size_t workspace_bytes, void *stream);
 
+/* Replaces every block of the packed buffer by its inverse (Gauss-Jordan with
+   partial pivoting, one launch; same layout as f3d_batched_lu_factor), and
+   when A32 is non-null also writes an FP32 copy at the same offsets.
+   info[b] is 0 or the 1-based step of the first zero pivot.  max_n <= 128
+   (else F3D_ERR_TOO_LARGE: use the LU).  With f3d_block_gemv this evaluates
+   the fiber blocks of P_inv (tstep/tstep.py:950-994) as products with the
+   explicit block inverses instead of per-block lu_solve. */
+int f3d_batched_inverse(double *A, const int64_t *matrix_offsets, const int32_t *sizes,
+                        int32_t count, int32_t max_n, float *A32, int32_t *info, void *stream);
+
+/* y + vector_offsets[b] = M_b (x + vector_offsets[b]) for every block, M_b
+   row-major sizes[b] x sizes[b] at M + matrix_offsets[b]; M is double
+   (F3D_FP64) or float (F3D_FP32C); x, y double, distinct.  FP64 sums. */
+int f3d_block_gemv(int precision, const void *M, const int64_t *matrix_offsets,
+                   const int64_t *vector_offsets, const int32_t *sizes, int32_t count,
+                   int32_t max_n, const double *x, double *y, void *stream);
+
 /* ---- fiber discretisation (A11, A12) ------------------------------------ */
 
 /* A set of fibers on the device.  Points of all fibers are concatenated;
@@ -367,6 +384,12 @@ int f3d_krylov_combine(const double *V, int64_t ldv, const double *c, int32_t k,
 int f3d_krylov_norm(const double *w, int64_t n, const int32_t *k, double *hcol,
                     double *beta, void *workspace, size_t workspace_bytes, void *stream);
 
+/* Row (*k + offset) of dst (leading dimension ld) = src, n entries (the
+   preconditioned basis vector z_k = P^-1 v_k kept for the update
+   x += Z y; a negative row is skipped). */
+int f3d_krylov_store(const double *src, const int32_t *k, int32_t offset, double *dst,
+                     int64_t ld, int64_t n, void *stream);
+
 /* V[*k] = w / *beta (zero if beta == 0) and also into `also` if non-NULL,
    then *k += 1 if bump. */
 int f3d_krylov_scale_into(const double *w, const double *beta, int32_t *k, double *V,
@@ -377,6 +400,23 @@ int f3d_krylov_scale_into(const double *w, const double *beta, int32_t *k, doubl
    the explicit inverse of the periphery operator (tstep/tstep.py:957-958). */
 int f3d_gemv(int precision, const void *M, int64_t ld, const double *x, double *y,
              int64_t rows, int64_t cols, void *stream);
+
+/* FP16 copy of a row-major matrix for f3d_gemv_f16: row r is divided by
+   row_scale[r], the smallest power of two >= max |M[r][c]| over the columns
+   outside r's diagonal block, and rounded to FP16.  With diag_block = db > 0
+   (square M, rows % db == 0) the entries of the db x db diagonal block that
+   holds row r stay FP64 in diag[r*db + c] (zero in M16). */
+int f3d_quantize_rows_f16(const double *M, int64_t ld, int64_t rows, int64_t cols,
+                          int32_t diag_block, void *M16, int64_t ld16, float *row_scale,
+                          double *diag, void *stream);
+
+/* y = diag(row_scale) M16 x + blockdiag(diag) x for the output of
+   f3d_quantize_rows_f16 (FP32 products and sums, FP64 result): the
+   periphery preconditioner of the mixed-precision inner solves, read at
+   2 bytes per entry. */
+int f3d_gemv_f16(const void *M16, int64_t ld16, const float *row_scale, const double *diag,
+                 int32_t diag_block, const double *x, double *y, int64_t rows, int64_t cols,
+                 void *stream);
 
 /* b = (float) a, elementwise. */
 int f3d_cast_to_float(const double *a, float *b, int64_t n, void *stream);

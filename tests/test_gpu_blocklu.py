@@ -89,3 +89,57 @@ def test_fiber_blocks_of_reference_step():
     for x, px in zip(g["probe_x"], g["probe_Px"]):
         y = lu.solve(torch.tensor(x[o:], device="cuda")).cpu().numpy()
         assert rel_err(y, px[o:]) < 1e-10
+
+
+@pytest.mark.parametrize("sizes", [[128] * 40, [4, 16, 33, 64, 100, 128, 7], [32, 1, 32, 17]])
+def test_inverse_and_block_gemv_match_numpy(sizes):
+    from fiber3d_b200.blocklu import BlockLU
+    rng = np.random.default_rng(sum(sizes))
+    blocks = random_blocks(rng, sizes)
+    lu = BlockLU(sizes)
+    lu.load(blocks)
+    lu.invert(fp32=True)
+    lu.check()
+    for b, A in enumerate(blocks):
+        ref = np.linalg.inv(A)
+        # forward error of an inverse: a few ulps times the condition number
+        assert rel_err(lu.block(b).cpu().numpy(), ref) < max(1e-12, 1e-14 * np.linalg.cond(A))
+    x = torch.tensor(rng.normal(size=sum(sizes)), device="cuda")
+    y64 = lu.apply(x, torch.empty_like(x), "fp64").cpu().numpy()
+    y32 = lu.apply(x, torch.empty_like(x), "fp32c").cpu().numpy()
+    off = 0
+    for A, n in zip(blocks, sizes):
+        ref = np.linalg.solve(A, x[off:off + n].cpu().numpy())
+        assert rel_err(y64[off:off + n], ref) < max(1e-12, 1e-14 * np.linalg.cond(A))
+        assert rel_err(y32[off:off + n], ref) < 1e-5
+        off += n
+
+
+def test_inverse_zero_pivot_reported():
+    from fiber3d_b200.blocklu import BlockLU
+    A = np.eye(8)
+    A[3, :] = 0.0
+    lu = BlockLU([8, 8])
+    lu.load([np.eye(8), A])
+    lu.invert()
+    with pytest.raises(ZeroDivisionError):
+        lu.check()
+
+
+def test_inverse_of_reference_fiber_blocks():
+    """Applying the explicit inverses of the fiber blocks of fiber3d's step
+    gives fiber3d's lu_solve-based preconditioner output on those rows."""
+    from fiber3d_b200.blocklu import BlockLU
+    from test_oracle_system import build_from_golden
+    g = load_golden("step_small.npz")
+    sys_ = build_from_golden(g)
+    sizes = [A.shape[0] for A in sys_.A_fib]
+    lu = BlockLU(sizes)
+    lu.load(sys_.A_fib)
+    lu.invert()
+    lu.check()
+    o = sys_.o_fib
+    for x, px in zip(g["probe_x"], g["probe_Px"]):
+        xd = torch.tensor(x[o:], device="cuda")
+        y = lu.apply(xd, torch.empty_like(xd)).cpu().numpy()
+        assert rel_err(y, px[o:]) < 1e-10

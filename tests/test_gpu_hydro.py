@@ -66,6 +66,62 @@ def test_preconditioner(system, golden_step):
         assert rel_err(y.cpu().numpy(), px) < 1e-9
 
 
+def test_preconditioner_lu_path(golden_step):
+    """The LU-factor/substitution evaluation of the fiber blocks (fiber3d's
+    own, used for blocks above 128) gives the same preconditioner."""
+    from fiber3d_b200.hydro import HydroSystem
+    s = HydroSystem(problem_from_golden(golden_step), fiber_pc="lu")
+    assert s.fiber_pc == "lu"
+    y = torch.empty(s.size, dtype=torch.float64, device="cuda")
+    for x, px in zip(golden_step["probe_x"], golden_step["probe_Px"]):
+        s.pc(torch.tensor(x, device="cuda"), y)
+        assert rel_err(y.cpu().numpy(), px) < 1e-9
+
+
+@pytest.mark.parametrize("storage", ["fp32", "fp16"])
+def test_preconditioner_inner_precision(golden_step, storage):
+    """The FP32-class preconditioner of the inner solves (FP32 inverses of the
+    fiber blocks; FP32 or row-scaled FP16 periphery inverse) stays close to
+    fiber3d's P^-1 x."""
+    from fiber3d_b200.hydro import HydroSystem
+    s = HydroSystem(problem_from_golden(golden_step), inner_shell_pc=storage)
+    y = torch.empty(s.size, dtype=torch.float64, device="cuda")
+    tol = 1e-5 if storage == "fp32" else 2e-3
+    for x, px in zip(golden_step["probe_x"], golden_step["probe_Px"]):
+        s.pc(torch.tensor(x, device="cuda"), y, "fp32c")
+        assert rel_err(y.cpu().numpy(), px) < tol
+
+
+def test_gemv_f16_row_scaled():
+    """FP16 rows scaled by powers of two plus FP64 3x3 diagonal blocks, against
+    an FP64 product, on a matrix whose rows span several decades."""
+    from fiber3d_b200 import _lib
+    g = torch.Generator(device="cpu").manual_seed(5)
+    m = 3 * 700
+    M = torch.randn((m, m), generator=g, dtype=torch.float64) * 1e-4
+    M *= torch.logspace(-3, 3, m, dtype=torch.float64)[:, None]
+    for i in range(0, m, 3):
+        M[i:i + 3, i:i + 3] += torch.randn((3, 3), generator=g, dtype=torch.float64) * 1e3
+    M = M.cuda()
+    x = torch.randn(m, generator=g, dtype=torch.float64).cuda()
+    M16 = torch.empty((m, m), dtype=torch.float16, device="cuda")
+    sc = torch.empty(m, dtype=torch.float32, device="cuda")
+    dg = torch.empty((m, 3), dtype=torch.float64, device="cuda")
+    st = _lib.stream_handle()
+    _lib.call("f3d_quantize_rows_f16", _lib.ptr(M), m, m, m, 3, _lib.ptr(M16), m, _lib.ptr(sc), _lib.ptr(dg), st)
+    y = torch.empty(m, dtype=torch.float64, device="cuda")
+    _lib.call("f3d_gemv_f16", _lib.ptr(M16), m, _lib.ptr(sc), _lib.ptr(dg), 3, _lib.ptr(x), _lib.ptr(y), m, m, st)
+    ref = M @ x
+    off = M.clone()
+    for i in range(0, m, 3):
+        off[i:i + 3, i:i + 3] = 0
+    # the diagonal blocks are exact; the rest carries FP16 rounding per entry
+    err = (y - ref).abs().cpu()
+    bound = 2e-3 * (off.abs() @ x.abs()).cpu() + 1e-12 * ref.abs().cpu()
+    assert bool((err <= bound).all())
+    assert bool(torch.all(torch.log2(sc.cpu()) == torch.round(torch.log2(sc.cpu()))))
+
+
 @pytest.mark.parametrize("use_graph", [False, True])
 def test_solve_fp64(system, golden_step, use_graph):
     res = system.solve(tol=1e-10, use_graph=use_graph)
@@ -89,6 +145,20 @@ def test_solve_mixed(system, golden_step):
     rr = float(torch.linalg.vector_norm(y - system.rhs) / torch.linalg.vector_norm(system.rhs))
     assert rr < 1e-10
     assert rel_err(x.cpu().numpy(), golden_step["sol"]) < 1e-7
+
+
+def test_fp32c_pair_error_bound(system, golden_step):
+    """The FP32C pair sums of the matvec stay within the relative error the
+    mixed solver assumes when it tests convergence on FP32C residuals."""
+    from fiber3d_b200.gmres import FP32C_PAIR_REL_ERR
+    y = torch.empty(system.size, dtype=torch.float64, device="cuda")
+    for x in golden_step["probe_x"]:
+        xd = torch.tensor(x, device="cuda")
+        system.matvec(xd, y, "fp64")
+        v64 = system.v.clone()
+        system.matvec(xd, y, "fp32c")
+        err = float(torch.linalg.vector_norm(system.v - v64) / torch.linalg.vector_norm(v64))
+        assert err < 0.2 * FP32C_PAIR_REL_ERR
 
 
 def test_graph_and_eager_agree(system):

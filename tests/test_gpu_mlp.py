@@ -12,6 +12,7 @@ import torch
 
 from conftest import rel_err
 from oracle import mlp as OM
+from fiber3d_b200.warmstart import LAYERS
 
 pytestmark = pytest.mark.gpu
 
@@ -56,8 +57,8 @@ def test_mlp_gradients_against_cpu_oracle():
     from fiber3d_b200.warmstart import FiberMLP
     net = FiberMLP(seed=4)
     rng = np.random.default_rng(8)
-    X = rng.normal(size=(384, 192)).astype(np.float32)
-    T = rng.normal(size=(384, 128)).astype(np.float32)
+    X = rng.normal(size=(384, LAYERS[0])).astype(np.float32)
+    T = rng.normal(size=(384, LAYERS[-1])).astype(np.float32)
     loss, gr = net.grads(torch.tensor(X, device="cuda"), torch.tensor(T, device="cuda"))
     W = [w.cpu().numpy() for w in net.W]
     b = [x.cpu().numpy() for x in net.b]
@@ -74,7 +75,7 @@ def test_mlp_training_reduces_loss():
     from fiber3d_b200.warmstart import FiberMLP
     teacher = FiberMLP(seed=1)
     g = torch.Generator(device="cpu").manual_seed(2)
-    X = torch.randn(4096, 192, generator=g).cuda()
+    X = torch.randn(4096, LAYERS[0], generator=g).cuda()
     T = teacher.forward(X)
     student = FiberMLP(seed=9)
     student.set_normalisation(X, T)
