@@ -110,6 +110,9 @@ SIGNATURES: dict[str, list] = {
     "f3d_batched_lu_solve": [_P, _P, _P, _P, _P, ctypes.c_int32, ctypes.c_int32, _P, _P, _P, _SZ, _P],
     "f3d_quantize_rows_f16": [_P, _I64, _I64, _I64, ctypes.c_int32, _P, _I64, _P, _P, _P],
     "f3d_gemv_f16": [_P, _I64, _P, _P, ctypes.c_int32, _P, _P, _I64, _I64, _P],
+    "f3d_warmstart_features": [_P, _P, _P, _P, _I64, _I64, ctypes.c_int32, ctypes.c_int32, _P, _P, _P, _P, _P,
+                               _P],
+    "f3d_warmstart_guess": [_P, _P, _P, _I64, _I64, ctypes.c_int32, ctypes.c_int32, _P, _P, _P, _P, _P],
     "f3d_batched_inverse": [_P, _P, _P, ctypes.c_int32, ctypes.c_int32, _P, _P, _P],
     "f3d_block_gemv": [_I, _P, _P, _P, _P, ctypes.c_int32, ctypes.c_int32, _P, _P, _P],
 }

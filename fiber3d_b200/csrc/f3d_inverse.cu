@@ -11,8 +11,8 @@
 // operator as fiber3d's (to rounding); only how it is evaluated changes.
 //
 // Inverse: Gauss-Jordan with partial (row) pivoting, in place.  Step k picks
-// the first row p >= k of largest |a_pk|, swaps rows k and p, and pivots on
-// (k, k):
+// a row p >= k of (to 2^-20) largest |a_pk|, swaps rows k and p, and pivots
+// on (k, k):
 //   a_kk <- 1/a_kk,  a_kj <- a_kj / a_kk,  a_ik <- -a_ik / a_kk,
 //   a_ij <- a_ij - a_ik a_kj / a_kk      (i != k, j != k, old values).
 // After n steps the array holds (PA)^-1; swapping columns k and p_k for
@@ -42,6 +42,18 @@ struct InvShape {
   static constexpr int kThreads = kColTiles * kRowTiles;
 };
 
+// 1/x for the pivot: the hardware approximation (rcp.approx.ftz.f64, about
+// 2^-22 relative error) refined by one third-order Newton step
+// y1 = y0 (1 + e + e^2), e = 1 - x y0, whose error is O(e^3): within an ulp
+// or so of the correctly rounded quotient, in 4 dependent operations.
+// Pivots below the normal range are reported as zero pivots by the caller.
+__device__ __forceinline__ double reciprocal(double x) {
+  double y;
+  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
+  const double e = fma(-x, y, 1.0);
+  return fma(y, fma(e, e, e), y);
+}
+
 // Step k = kb + M of the Gauss-Jordan sweep on the register tiles.
 // Column k is published to shared memory and zeroed in the tiles; the pivot
 // row is read back with its column-k entry taken as 1, so that one update
@@ -67,24 +79,23 @@ __device__ __forceinline__ void inverse_step(double (&a)[kInvTR][kInvTC], int kb
     }
   }
   __syncthreads();
-  // (b) pivot: first row p >= k of largest magnitude, found by every warp
-  double best = -1.0;
-  int bi = NMAX;
+  // (b) pivot, found by every warp: the first row p >= k whose magnitude
+  // has the largest leading 32 bits (sign, exponent, 20 mantissa bits), i.e.
+  // a pivot within a factor 1 - 2^-20 of the column maximum -- threshold
+  // partial pivoting, as stable as the exact maximum.  Two warp reductions.
+  unsigned key = 0u, row = 0xFFFFFFFFu;
 #pragma unroll
   for (int q = 0; q < NMAX / 32; ++q) {
     const int r = lane + 32 * q;
     if (r >= k && r < n) {
-      const double v = fabs(s_col[par][r]);
-      if (v > best) { best = v; bi = r; }
+      const unsigned kq =
+          static_cast<unsigned>(static_cast<unsigned long long>(__double_as_longlong(fabs(s_col[par][r]))) >> 32);
+      if (row == 0xFFFFFFFFu || kq > key) { key = kq; row = static_cast<unsigned>(r); }
     }
   }
-#pragma unroll
-  for (int off = 16; off > 0; off >>= 1) {
-    const double ov = __shfl_xor_sync(0xffffffffu, best, off);
-    const int oi = __shfl_xor_sync(0xffffffffu, bi, off);
-    if (ov > best || (ov == best && oi < bi)) { best = ov; bi = oi; }
-  }
-  const int p = bi < n ? bi : k;
+  const unsigned kmax = __reduce_max_sync(0xffffffffu, row != 0xFFFFFFFFu ? key : 0u);
+  const unsigned pmin = __reduce_min_sync(0xffffffffu, (row != 0xFFFFFFFFu && key == kmax) ? row : 0xFFFFFFFFu);
+  const int p = pmin < static_cast<unsigned>(n) ? static_cast<int>(pmin) : k;
   // (c) publish rows k and p (column k already zero)
   if (rt == k / kInvTR) {
 #pragma unroll
@@ -104,8 +115,9 @@ __device__ __forceinline__ void inverse_step(double (&a)[kInvTR][kInvTC], int kb
   __syncthreads();
   // (d) swap rows k and p, then the update
   const double pv = s_col[par][p];
-  if (pv == 0.0 && first_zero == 0) first_zero = k + 1;
-  const double pinv = pv != 0.0 ? 1.0 / pv : 0.0;
+  const bool zero_pivot = !(fabs(pv) >= 2.2250738585072014e-308);  // zero, subnormal or NaN
+  if (zero_pivot && first_zero == 0) first_zero = k + 1;
+  const double pinv = zero_pivot ? 0.0 : reciprocal(pv);
   double u[kInvTC];
 #pragma unroll
   for (int j = 0; j < kInvTC; ++j) u[j] = s_row[par][1][c0 + j];

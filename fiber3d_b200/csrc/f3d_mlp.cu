@@ -13,8 +13,9 @@
 // tcgen05.commit signals an mbarrier that the CTA waits on (bounded by
 // %globaltimer).  The epilogue reads TMEM with tcgen05.ld.32x32b (warp w owns
 // lanes 32w..32w+31 = rows) and fuses bias, ReLU and the ReLU mask of the
-// backward pass.  One CTA (128 threads) computes a 128-row x N tile; no TMA
-// multicast, no clusters.
+// backward pass.  One CTA (128 threads) computes a 128-row x ntile tile
+// (grid.y splits N into ntile-column tiles when there are too few row tiles to
+// fill the GPU); no TMA multicast, no clusters.
 #include <cuda_bf16.h>
 
 #include "f3d_common.cuh"
@@ -34,6 +35,7 @@ struct GemmArgs {
   float *pre;             // [M x ldc]: pre-activation copy when non-null
   int64_t a_rs, a_cs, b_rs, b_cs, ldc, ldm;
   int M, N, K;
+  int ntile;       // columns per CTA (multiple of 16, <= 256)
   int relu;        // apply max(0, .) in the epilogue
   int accumulate;  // C += result
   float alpha;
@@ -97,7 +99,8 @@ __global__ void __launch_bounds__(kGemmThreads) gemm_bf16_tcgen05_kernel(const G
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int m0 = blockIdx.x * 128;
   const int mvalid = min(128, g.M - m0);
-  const int N = g.N;  // multiple of 16, <= 256
+  const int n0 = blockIdx.y * g.ntile;
+  const int N = min(g.ntile, g.N - n0);  // multiple of 16, <= 256
 
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
@@ -124,7 +127,7 @@ __global__ void __launch_bounds__(kGemmThreads) gemm_bf16_tcgen05_kernel(const G
   for (int c = 0; c < nchunks; ++c) {
     const int k0 = c * kKChunk;
     stage_operand(sA, g.A + static_cast<int64_t>(m0) * g.a_rs, g.a_rs, g.a_cs, mvalid, 128, k0, g.K);
-    stage_operand(sB, g.B, g.b_rs, g.b_cs, N, N, k0, g.K);
+    stage_operand(sB, g.B + static_cast<int64_t>(n0) * g.b_rs, g.b_rs, g.b_cs, N, N, k0, g.K);
     fence_proxy_async_smem();  // generic-proxy stores -> async-proxy (MMA) reads
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -171,7 +174,7 @@ __global__ void __launch_bounds__(kGemmThreads) gemm_bf16_tcgen05_kernel(const G
       if (m < g.M) {
 #pragma unroll
         for (int j = 0; j < 16; ++j) {
-          const int n = c0 + j;
+          const int n = n0 + c0 + j;
           float v = g.alpha * __uint_as_float(r[j]);
           if (g.bias) v += g.bias[n];
           if (g.pre) g.pre[static_cast<int64_t>(m) * g.ldc + n] = v;
@@ -253,8 +256,13 @@ int f3d_gemm_bf16(const float *A, int64_t a_rs, int64_t a_cs, const float *B, in
   if (M == 0) return F3D_OK;
   if (K == 0) return F3D_ERR_SHAPE;
   if (mask_src && ldm < N) return F3D_ERR_SHAPE;
+  // Few row tiles (small batches, e.g. one time step's fibers): split N so
+  // that more CTAs run; each re-stages its A tile (an L2 hit).
+  const int mtiles = (M + 127) / 128;
+  int ntile = N;
+  while (ntile > 32 && ntile % 32 == 0 && mtiles * (N / ntile) < f3d::sm_count()) ntile /= 2;
   f3d::GemmArgs g{A, B, C, bias, mask_src, pre, a_rs, a_cs, b_rs, b_cs, ldc, ldm,
-                  M, N, K, relu, accumulate, alpha, f3d::device_error_word()};
+                  M, N, K, ntile, relu, accumulate, alpha, f3d::device_error_word()};
   // 48 KB of operand tiles; ~100 KB is requested so that at most two CTAs
   // share an SM and their two 256-column TMEM allocations always fit.
   const size_t smem = 100 * 1024;
@@ -267,7 +275,7 @@ int f3d_gemm_bf16(const float *A, int64_t a_rs, int64_t a_cs, const float *B, in
       return F3D_ERR_CUDA;
     attr[dev] = true;
   }
-  const unsigned grid = static_cast<unsigned>((M + 127) / 128);
+  const dim3 grid(static_cast<unsigned>(mtiles), static_cast<unsigned>((N + ntile - 1) / ntile));
   f3d::gemm_bf16_tcgen05_kernel<<<grid, f3d::kGemmThreads, smem, static_cast<cudaStream_t>(stream)>>>(g);
   return f3d::launch_status();
 }

@@ -460,10 +460,13 @@ static int make_plan(int kernel, int precision, int64_t ns, int64_t nt, const f3
   p->tiles_per_split = tps;
   // The counter words live in a fixed region at the start of the workspace
   // that nothing else ever writes, so they stay zero between calls of any
-  // shape (each kernel returns the words it used to zero).
+  // shape (each kernel returns the words it used to zero).  The region is
+  // reserved whenever the call uses the workspace at all, also by calls that
+  // need no counters themselves (FP32C with one split packs its sources
+  // behind it), because one workspace serves calls of every shape.
   size_t off = 0;
   p->off_counters = off;
-  if (p->nsplit > 1) off += kCounterBytes;
+  if (p->nsplit > 1 || precision == F3D_FP32C) off += kCounterBytes;
   p->off_partial = off;
   if (p->nsplit > 1) off += round_up(static_cast<size_t>(p->nsplit) * nt * 3 * sizeof(double), 256);
   p->off_packed = off;

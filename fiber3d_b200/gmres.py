@@ -24,9 +24,10 @@ Givens stay FP64).  The outer residual is itself evaluated with the FP32C
 pair sums when that cannot change the convergence test: every other part of
 the matvec is FP64, and the pair sums v carry a relative error below
 ``FP32C_PAIR_REL_ERR``, so the residual is off by at most
-``FP32C_PAIR_REL_ERR * |v|``; while that is below ``0.1 * tol * |b|`` the
-FP32C residual decides convergence as an FP64 one would, otherwise the
-residual is recomputed in FP64 (and stays FP64 for the rest of the solve).
+``e = FP32C_PAIR_REL_ERR * |v| / |b|`` (relative).  The solve stops when
+``|r| / |b| + e <= tol``, which bounds the FP64 residual by tol as well;
+while ``e <= tol / 2`` the residual stays FP32C, otherwise it is recomputed
+in FP64 (and stays FP64 for the rest of the solve).
 """
 from __future__ import annotations
 
@@ -38,9 +39,10 @@ import torch
 
 from . import _lib
 
-# Bound on |v_fp32c - v_fp64| / |v_fp64| (2-norms) of the FP32C pair sums,
-# with margin over what the tests measure.
-FP32C_PAIR_REL_ERR = 1e-6
+# Bound on |v_fp32c - v_fp64| / |v_fp64| (2-norms) of the FP32C pair sums:
+# about 4x the largest value measured on the solver's own matvecs (4.3e-7);
+# the tests hold the pair sums to a quarter of it.
+FP32C_PAIR_REL_ERR = 2e-6
 
 
 class DeviceGMRES:
@@ -233,14 +235,16 @@ def solve_system(system, tol=1e-8, restart=100, maxiter=200, x0=None, mixed=Fals
     outer = "fp32c"
     fp64_residuals = 0
     while True:
+        bound = 0.0  # bound on |r_computed - r_fp64| / |b|
         if x0 is None and ref == 0:
             r.copy_(b)
         else:
             system.matvec(x, tmp, outer)
             if outer == "fp32c":
                 g._norm(system.v, g.beta)
-                if FP32C_PAIR_REL_ERR * float(g.beta.item()) > 0.1 * tol * bnorm:
-                    outer = "fp64"
+                bound = FP32C_PAIR_REL_ERR * float(g.beta.item()) / bnorm
+                if bound > 0.5 * tol:
+                    outer, bound = "fp64", 0.0
                     system.matvec(x, tmp, outer)
             if outer == "fp64":
                 fp64_residuals += 1
@@ -248,13 +252,13 @@ def solve_system(system, tol=1e-8, restart=100, maxiter=200, x0=None, mixed=Fals
         g._norm(r, g.beta)
         rel = float(g.beta.item()) / bnorm
         hist.append(rel)
-        if rel <= tol:
+        if rel + bound <= tol:  # the FP64 residual is <= tol as well
             break
         if ref >= max_refine or total_its >= maxiter:
             info = total_its
             break
         # inner tolerance relative to |r|: never ask beyond what is needed
-        inner = max(inner_tol, 0.5 * tol / rel)
+        inner = max(inner_tol, 0.7 * (tol - bound) / rel)
         d, _, its, _ = g.solve(lambda a, o: system.matvec(a, o, "fp32c"),
                                lambda a, o: system.pc(a, o, "fp32c"), r, rtol=inner,
                                maxiter=maxiter - total_its, use_graph=use_graph, key="fp32c",

@@ -382,18 +382,35 @@ class HydroSystem:
 
     # ------------------------------------------------------------------------
     def _load_bodies(self):
-        for k in range(self.nbody):
-            a, b = int(self.body_node_off_h[k]), int(self.body_node_off_h[k + 1])
-            R = quaternion_rotation(self.body_quat[k])
-            self.body_nodes[a:b] = torch.as_tensor(self.body_ref[k] @ R.T + self.body_loc[k])
-            self.body_normals[a:b] = torch.as_tensor(self.body_ref_n[k] @ R.T)
-        self.body_centers.copy_(torch.as_tensor(self.body_loc))
-        self.body_R.copy_(torch.as_tensor(np.stack([quaternion_rotation(q).ravel() for q in self.body_quat])))
-        P = self.p
-        for k in range(self.nbody):
-            a, b = int(self.body_node_off_h[k]), int(self.body_node_off_h[k + 1])
-            self.body_E[a:b] = singularity_vectors(self.body_nodes[a:b], self.body_normals[a:b],
-                                                   self.body_w[a:b], P.eta, P.reg, P.eps_dist)
+        """Body nodes, normals and singularity vectors at the current
+        location/orientation, on the device.  A rigid body's singularity
+        vectors are those of its reference surface rotated with it: the
+        3 x 3 map E_i (unit density -> velocity at node i) of the rotated
+        surface is R E_i^ref R^T (the stresslet sum is rotation-equivariant
+        and translation-invariant), so the pair sum runs once per body, at
+        set-up, not every step."""
+        dev = self.device
+        Rh = np.stack([quaternion_rotation(q) for q in self.body_quat])
+        RL = torch.as_tensor(np.concatenate([Rh.reshape(-1, 9), self.body_loc], axis=1), device=dev)
+        R = RL[:, :9].reshape(-1, 3, 3)
+        loc = RL[:, 9:]
+        if not hasattr(self, "_body_idx"):
+            self._body_idx = torch.as_tensor(np.repeat(np.arange(self.nbody), self.nb), device=dev)
+            self._ref_nodes = torch.as_tensor(np.concatenate(self.body_ref), device=dev)
+            self._ref_normals = torch.as_tensor(np.concatenate(self.body_ref_n), device=dev)
+            P = self.p
+            E = []
+            for k in range(self.nbody):
+                a, b = int(self.body_node_off_h[k]), int(self.body_node_off_h[k + 1])
+                E.append(singularity_vectors(self._ref_nodes[a:b], self._ref_normals[a:b], self.body_w[a:b],
+                                             P.eta, P.reg, P.eps_dist))
+            self._ref_E = torch.cat(E).view(-1, 3, 3)
+        Rn = R[self._body_idx]
+        self.body_nodes.copy_(torch.einsum("nij,nj->ni", Rn, self._ref_nodes) + loc[self._body_idx])
+        self.body_normals.copy_(torch.einsum("nij,nj->ni", Rn, self._ref_normals))
+        self.body_E.copy_((Rn @ self._ref_E @ Rn.transpose(1, 2)).reshape(-1, 9))
+        self.body_centers.copy_(loc)
+        self.body_R.copy_(R.reshape(-1, 9))
 
     def _body_blocks(self):
         """Body preconditioner blocks in each body's own frame (location 0,

@@ -11,22 +11,26 @@ x^{n+1} - x_q on that fiber's unknowns (positions and tensions) from the
 fiber's recent differences, each in units of its own size so that nothing
 depends on how fast the fiber moves:
 
-  input  (260) = D2 X^n / s2_X (96),  D3 X^n / s3_X (96),
-                 D2 T^n / s2_T (32),  D3 T^n / s3_T (32),
+  input  (260) = D2 X^n / s2_X (96),  D3 X^n / s2_X (96),
+                 D2 T^n / s2_T (32),  D3 T^n / s2_T (32),
                  log10 of s3/s2 and s2/s1 for X and T (4)
-  output (128) = (X^{n+1} - X_q) / s3_X (96),  (T^{n+1} - T_q) / s3_T (32)
+  output (128) = (X^{n+1} - X_q) / s2_X (96),  (T^{n+1} - T_q) / s2_T (32)
 
 where D1 X^n = X^n - X^{n-1}, D2 X^n = D1 X^n - D1 X^{n-1}, D3 X^n =
 X^n - 3 X^{n-1} + 3 X^{n-2} - X^{n-3} (note X^{n+1} - X_q = D3 X^{n+1}, so
-cubic extrapolation is the map output = D3 X^n / s3_X), and sk is the
+cubic extrapolation is the map output = D3 X^n / s2_X), and sk is the
 root-mean-square of Dk over the fiber.  The correction is
 projected on the first few Legendre modes along the fiber before it is used:
 a point-to-point wiggle in a position guess is multiplied by the fourth
 derivative in the bending operator, so the correction must be smooth to
 lower the residual.  A gain per unknown group (positions, tensions), fitted
-by least squares on held-out steps and kept in [0, 1], scales it; a network
-that learned nothing useful leaves the extrapolation unchanged.  Periphery
-and body unknowns take x_q.
+by least squares on held-out steps and kept in [0, 1], scales it, and an
+overall factor is then chosen among a few candidates (0 included) by the
+GMRES iterations it gives on held-out trajectories: a correction that does
+not shorten GMRES there is switched off, and the guess is the extrapolation.
+Periphery and body unknowns take x_q.  At inference the features, the
+network (output statistics, smoothing and gains folded into its last
+layer) and the guess take six kernel launches.
 
 3 hidden layers of 256 with ReLU; weights kept in FP32 (master copy, Adam)
 and rounded to BF16 when staged for the tensor cores; every product runs in
@@ -109,7 +113,7 @@ class FiberMLP:
 
     # ------------------------------------------------------------- passes --
     def forward(self, X: torch.Tensor, keep=False):
-        """X: (B, 192) normalised inputs -> (B, 128) normalised outputs."""
+        """X: (B, LAYERS[0]) normalised inputs -> (B, LAYERS[-1]) normalised outputs."""
         acts, pres = [X.contiguous()], []
         h = acts[0]
         L = len(self.W)
@@ -134,8 +138,14 @@ class FiberMLP:
         gW, gb = [None] * len(self.W), [None] * len(self.W)
         for k in range(len(self.W) - 1, -1, -1):
             Ain = acts[k]
-            # dW = D^T Ain  (M = out, N = in, K = batch)
-            gW[k] = gemm(D, Ain, transpose_a=True, transpose_b=False)
+            # dW = D^T Ain  (M = out, N = in, K = batch); the GEMM's N is a
+            # multiple of 16 up to 256, so a wider or ragged input layer
+            # takes (Ain^T D)^T instead
+            n_in = Ain.shape[1]
+            if n_in <= 256 and n_in % 16 == 0:
+                gW[k] = gemm(D, Ain, transpose_a=True, transpose_b=False)
+            else:
+                gW[k] = gemm(Ain, D, transpose_a=True, transpose_b=False).t().contiguous()
             gb[k] = torch.empty(self.b[k].shape, dtype=torch.float32, device=X.device)
             _lib.call("f3d_colsum", _lib.ptr(D), D.shape[1], B, D.shape[1], _lib.ptr(gb[k]), 0,
                       _lib.stream_handle(X.device))
@@ -206,7 +216,7 @@ def extrapolate(history) -> torch.Tensor | None:
 
 def history_features(system, history):
     """(nfib, 260) network input from the last four solutions, and the
-    per-fiber target scales s_X (nfib, 1, 1) and s_T (nfib, 1)."""
+    per-fiber scales s2_X (nfib, 1, 1) and s2_T (nfib, 1) of the targets."""
     B = [fiber_blocks(system, h) for h in history[-4:]][::-1]  # newest first
     X = [b[:, :3] for b in B]
     T = [b[:, 3] for b in B]
@@ -220,8 +230,8 @@ def history_features(system, history):
     s1T, s2T, s3T = rmsT(d1T), rmsT(d2T), rmsT(d3T)
     ratios = torch.cat([torch.log10(s3X / s2X).view(-1, 1), torch.log10(s3T / s2T),
                         torch.log10(s2X / s1X).view(-1, 1), torch.log10(s2T / s1T)], dim=1)
-    feats = torch.cat([(d2X / s2X).flatten(1), (d3X / s3X).flatten(1), d2T / s2T, d3T / s3T, ratios], dim=1)
-    return feats.float().contiguous(), s3X, s3T
+    feats = torch.cat([(d2X / s2X).flatten(1), (d3X / s2X).flatten(1), d2T / s2T, d3T / s2T, ratios], dim=1)
+    return feats.float().contiguous(), s2X, s2T
 
 
 def mode_projection(npts: int = NPTS, modes: int = MODES, device=None) -> torch.Tensor:
@@ -259,6 +269,8 @@ class LearnedWarmStart:
         self.device = self.net.device
         self.P = mode_projection(NPTS, modes, self.device)
         self.gain = torch.ones(2, dtype=torch.float32, device=self.device)
+        self.scale = 1.0          # overall factor chosen on held-out trajectories
+        self._fold = None         # inference weights (see _folded)
 
     def smooth(self, Y: torch.Tensor) -> torch.Tensor:
         """Project each of the 4 rows (X, Y, Z, T) of a (B, 128) correction."""
@@ -267,8 +279,8 @@ class LearnedWarmStart:
     def predict(self, feats: torch.Tensor) -> torch.Tensor:
         """Smoothed, gain-scaled normalised correction (B, 128)."""
         C = self.smooth(self.net.predict(feats))
-        C[:, :3 * NPTS] *= self.gain[0]
-        C[:, 3 * NPTS:] *= self.gain[1]
+        C[:, :3 * NPTS] *= self.gain[0] * self.scale
+        C[:, 3 * NPTS:] *= self.gain[1] * self.scale
         return C
 
     def fit(self, X: torch.Tensor, T: torch.Tensor, epochs=30, batch=1024, lr=1e-3, val_frac=0.1,
@@ -290,16 +302,75 @@ class LearnedWarmStart:
             num = float((C[:, sl] * Tv[:, sl]).sum())
             den = float((C[:, sl] * C[:, sl]).sum())
             self.gain[k] = min(1.0, max(0.0, num / den)) if den > 0 else 0.0
+        self._fold = None
         return hist
 
-    def guess(self, system, history) -> torch.Tensor | None:
-        """The warm start: quadratic extrapolation, corrected by the network
-        once HISTORY solutions are known."""
+    def select_scale(self, make_system, steps: int, candidates=(0.0, 0.5, 1.0), tol=1e-8) -> dict:
+        """Pick the overall factor with the fewest GMRES iterations over
+        held-out trajectories (ties: the lower geometric-mean initial
+        residual; then the smaller factor).  ``make_system()`` returns a
+        fresh system at the trajectory's first step."""
+        score = {}
+        for c in candidates:
+            self.scale = c
+            self._fold = None
+            st = march(make_system(), steps, guess="learned", net=self, tol=tol)
+            acting = st[HISTORY:] or st
+            its = sum(x["iterations"] for x in acting)
+            r0 = float(np.exp(np.mean(np.log([max(x["initial_rel_residual"], 1e-300) for x in acting]))))
+            score[c] = (its, r0, c)
+        self.scale = min(score, key=lambda c: score[c])
+        self._fold = None
+        return {c: {"iterations": v[0], "r0_geomean": v[1]} for c, v in score.items()}
+
+    def _folded(self):
+        """Inference weights: the output un-normalisation, the smoothing
+        projection and the gains folded into the last layer (FP32 master
+        values; the GEMM rounds them to BF16 like every weight)."""
+        if self._fold is None:
+            net = self.net
+            Pi = torch.block_diag(self.P, self.P, self.P, self.P)
+            g = torch.cat([self.gain[0].expand(3 * NPTS), self.gain[1].expand(NPTS)]) * self.scale
+            M = g[:, None] * Pi
+            W = list(net.W[:-1]) + [(M @ (net.out_std[:, None] * net.W[-1])).contiguous()]
+            b = list(net.b[:-1]) + [(M @ (net.out_std * net.b[-1] + net.out_mean)).contiguous()]
+            self._fold = (W, b)
+        return self._fold
+
+    def guess_reference(self, system, history) -> torch.Tensor | None:
+        """The same guess from PyTorch ops around the network (test reference
+        of :meth:`guess`)."""
         x_q = extrapolate(history)
-        if x_q is None or len(history) < HISTORY or not learnable(system):
+        if len(history) < HISTORY or not learnable(system) or self.scale == 0.0:
             return x_q
         f, sX, sT = history_features(system, history)
         return apply_correction(system, x_q, self.predict(f), sX, sT)
+
+    def guess(self, system, history) -> torch.Tensor | None:
+        """The warm start: quadratic extrapolation, corrected by the network
+        once HISTORY solutions are known.  Six launches: the feature kernel
+        (standardised inputs), four tensor-core GEMMs (the last one with the
+        smoothing and gains folded in) and the guess kernel."""
+        if len(history) < HISTORY or not learnable(system) or self.scale == 0.0:
+            return extrapolate(history)
+        W, b = self._folded()
+        h0, h1, h2, h3 = (h.contiguous() for h in history[-HISTORY:])
+        nfib = system.fs.nfib
+        dev = h3.device
+        st = _lib.stream_handle(dev)
+        feats = torch.empty((nfib, LAYERS[0]), dtype=torch.float32, device=dev)
+        sx = torch.empty(nfib, dtype=torch.float64, device=dev)
+        sT = torch.empty(nfib, dtype=torch.float64, device=dev)
+        _lib.call("f3d_warmstart_features", _lib.ptr(h0), _lib.ptr(h1), _lib.ptr(h2), _lib.ptr(h3), h3.numel(),
+                  system.o_fib, nfib, NPTS, _lib.ptr(self.net.in_mean), _lib.ptr(self.net.in_std), _lib.ptr(feats),
+                  _lib.ptr(sx), _lib.ptr(sT), st)
+        h = feats
+        for k in range(len(W)):
+            h = gemm(h, W[k], bias=b[k], relu=k < len(W) - 1)
+        x0 = torch.empty_like(h3)
+        _lib.call("f3d_warmstart_guess", _lib.ptr(h1), _lib.ptr(h2), _lib.ptr(h3), h3.numel(), system.o_fib, nfib,
+                  NPTS, _lib.ptr(h), _lib.ptr(sx), _lib.ptr(sT), _lib.ptr(x0), st)
+        return x0
 
 
 def learned_guess(system, history, model: LearnedWarmStart | None) -> torch.Tensor | None:
@@ -330,14 +401,14 @@ def march(system, steps: int, guess: str = "zero", net: LearnedWarmStart | None 
             system.advance(history[-1])
         x_q = extrapolate(history)
         f = None
-        if can_learn and len(history) >= HISTORY and (record or guess == "learned"):
+        if can_learn and len(history) >= HISTORY and record:
             f, sX, sT = history_features(system, history)
         if guess == "zero":
             x0 = None
         elif guess == "previous":
             x0 = history[-1] if history else None
-        elif guess == "learned" and net is not None and f is not None:
-            x0 = apply_correction(system, x_q, net.predict(f), sX, sT)
+        elif guess == "learned" and net is not None:
+            x0 = net.guess(system, history)
         else:
             x0 = x_q
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)

@@ -237,7 +237,9 @@ int f3d_batched_lu_solve(const double *LU, const int64_t *matrix_offsets,
 /* Replaces every block of the packed buffer by its inverse (Gauss-Jordan with
    partial pivoting, one launch; same layout as f3d_batched_lu_factor), and
    when A32 is non-null also writes an FP32 copy at the same offsets.
-   info[b] is 0 or the 1-based step of the first zero pivot.  max_n <= 128
+   info[b] is 0 or the 1-based step of the first zero (or subnormal) pivot.
+   Pivoting takes a row whose |a_pk| is within a factor 1 - 2^-20 of the
+   column maximum (the first such row).  max_n <= 128
    (else F3D_ERR_TOO_LARGE: use the LU).  With f3d_block_gemv this evaluates
    the fiber blocks of P_inv (tstep/tstep.py:950-994) as products with the
    explicit block inverses instead of per-block lu_solve. */
@@ -434,6 +436,26 @@ int f3d_gemm_bf16(const float *A, int64_t a_rs, int64_t a_cs, const float *B, in
                   int64_t b_cs, float *C, int64_t ldc, int32_t M, int32_t N, int32_t K,
                   const float *bias, int relu, const float *mask_src, int64_t ldm, float *pre,
                   float alpha, int accumulate, void *stream);
+
+/* Warm-start input for the per-fiber network from the last four solutions
+   h0 (oldest) .. h3 (newest) of length n, fibers of npts = 32 points whose
+   blocks start at o_fib (fiber3d's layout): per fiber 4 npts + 4 floats
+   (second and third differences of positions and tensions, scaled by the
+   RMS second difference, and four log10 ratios of difference RMS), each
+   standardised as (v - mean[j]) / stdev[j] when mean/stdev are non-NULL;
+   scale_x/scale_t receive the RMS second differences (the output units). */
+int f3d_warmstart_features(const double *h0, const double *h1, const double *h2, const double *h3,
+                           int64_t n, int64_t o_fib, int32_t nfib, int32_t npts, const float *mean,
+                           const float *stdev, float *feats, double *scale_x, double *scale_t,
+                           void *stream);
+
+/* x0 = 3 h3 - 3 h2 + h1 (quadratic extrapolation) plus, when corr is
+   non-NULL, the network's correction corr[f][k] (4 npts per fiber, rows X_x,
+   X_y, X_z, T) times scale_x[f] (positions) or scale_t[f] (tensions) on
+   fiber block f. */
+int f3d_warmstart_guess(const double *h1, const double *h2, const double *h3, int64_t n,
+                        int64_t o_fib, int32_t nfib, int32_t npts, const float *corr,
+                        const double *scale_x, const double *scale_t, double *x0, void *stream);
 
 /* out[n] (+)= sum_m G[m*ld + n]. */
 int f3d_colsum(const float *G, int64_t ld, int32_t M, int32_t N, float *out, int accumulate,

@@ -70,6 +70,11 @@ def test_workspace_query_and_argument_checks(dll):
     # nothing to do: OK without touching the device
     assert dll.f3d_oseen_source_target(None, None, None, None, 10, 0, 1.0, 5e-3, 1e-5, 0,
                                        None, 0, None) == 0
+    # every workspace keeps the split-counter region (256 KiB) at its start,
+    # also an FP32C single-split one whose packed sources follow it
+    one = _lib.PairShape(1, 8, 1, 0)
+    assert dll.f3d_pair_workspace_bytes(1, 1, 1000, 100, ctypes.byref(one), ctypes.byref(nbytes)) == 0
+    assert nbytes.value >= (256 << 10) + 1000 * 12 * 4
     # skip-index needs ns == nt
     assert dll.f3d_pair_sum(0, 0, 1, 8, 8, 8, None, None, None, 8, 10, 11, 1.0, 5e-3, 1e-5, 0,
                             None, None, 0, None) == 2

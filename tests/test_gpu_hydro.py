@@ -158,7 +158,7 @@ def test_fp32c_pair_error_bound(system, golden_step):
         v64 = system.v.clone()
         system.matvec(xd, y, "fp32c")
         err = float(torch.linalg.vector_norm(system.v - v64) / torch.linalg.vector_norm(v64))
-        assert err < 0.2 * FP32C_PAIR_REL_ERR
+        assert err < 0.25 * FP32C_PAIR_REL_ERR
 
 
 def test_graph_and_eager_agree(system):

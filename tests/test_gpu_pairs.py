@@ -232,3 +232,22 @@ def test_fp32c_shapes(K, L, shape, mode):
                      **kw).cpu().numpy()
     assert np.all(np.isfinite(u32))
     assert rel_err(u32, u64) < TOL32
+
+
+def test_fp32c_single_split_keeps_shared_counters(K, L):
+    """One workspace serves calls of every shape: an FP32C call with a single
+    split (which packs its sources in the workspace) must leave the split
+    counters of later multi-split calls untouched."""
+    rng = np.random.default_rng(31)
+    x = rng.random((3000, 3)) * 4.0
+    y = rng.random((2000, 3)) * 4.0
+    n = rng.normal(size=(3000, 3))
+    d = rng.normal(size=(3000, 3))
+    ref = pairs_c.pair_sum("stresslet", x, y, d, n)
+    for _ in range(2):
+        K.pair_sum("stresslet", x, y, d, n, precision="fp32c", shape=L.PairShape(1, 8, 1, -1))
+        u = K.pair_sum("stresslet", x, y, d, n, shape=L.PairShape(1, 1, 7, -1)).cpu().numpy()
+        assert rel_err(u, ref) < TOL64
+        u = K.pair_sum("stresslet", x, y, d, n, precision="fp32c",
+                       shape=L.PairShape(2, 1, 5, 0)).cpu().numpy()
+        assert rel_err(u, ref) < TOL32
