@@ -304,7 +304,8 @@ def gpu_arm(args, rank, world, local):
             "plain_fp64_ms": st["fp64"]["ms_per_step"],
             "learned_mixed_ms": st["learned_mixed"]["ms_per_step"],
             "speedup_learned_mixed_vs_plain_fp64": st["learned_mixed"]["speedup_vs_fp64"],
-            "modes": {m: {k: v[k] for k in ("ms_per_step", "iterations", "true_rel_residual",
+            "modes": {m: {k: v[k] for k in ("ms_per_step", "ms_per_step_last_half", "iterations", "long_solves",
+                                            "true_rel_residual",
                                             "rel_err_vs_fp64_1e-12_solve", "speedup_vs_fp64", "phases_ms")}
                       for m, v in st.items() if m != "training"},
             "training": st["training"],
@@ -408,33 +409,39 @@ def hydro_arm(args, rank, world, local, warmup=None, steps=None, emit=True):
     for seed in args.train_seeds:
         Pt = geometry.hydro_step_problem(seed=seed, nshell=args.nshell, nfib=args.nfib)
         st_ = H.HydroSystem(Pt, shell_op=shell, device=dev)
-        _, Xf, Tf = W.march(st_, args.train_steps, guess="extrapolate", record=True)
+        _, Xf, Tf = W.march(st_, args.train_steps, guess="extrapolate", record=True,
+                            record_from=args.train_skip)
         feats.append(Xf)
         targs.append(Tf)
         del st_
     X_train, T_train = torch.cat(feats), torch.cat(targs)
     net = W.LearnedWarmStart(seed=0, device=dev)
     hist = net.fit(X_train, T_train, epochs=args.train_epochs, batch=1024, lr=1e-3)
-    # overall correction factor chosen by GMRES iterations on a held-out trajectory
-    val_seed = max(args.train_seeds) + 1
-    Pv = geometry.hydro_step_problem(seed=val_seed, nshell=args.nshell, nfib=args.nfib)
-    sel = net.select_scale(lambda: H.HydroSystem(Pv, shell_op=shell, device=dev), args.train_steps // 2 + 4)
+    # correction factors chosen by GMRES iterations on held-out trajectories
+    val_seeds = [max(args.train_seeds) + 1, max(args.train_seeds) + 2]
+    Pvs = [geometry.hydro_step_problem(seed=sd, nshell=args.nshell, nfib=args.nfib) for sd in val_seeds]
+    sel = net.select_scale(lambda: [H.HydroSystem(Pv, shell_op=shell, device=dev) for Pv in Pvs],
+                           args.train_steps, count_from=args.train_skip)
     torch.cuda.synchronize()
     train = {"samples": int(X_train.shape[0]), "seconds": time.perf_counter() - t0,
              "loss_first_last": [hist[0], hist[-1]], "gain": net.gain.tolist(), "scale": net.scale,
-             "scale_selection": sel, "validation_seed": val_seed,
-             "seeds": list(args.train_seeds), "steps_per_seed": args.train_steps}
+             "scale_selection": sel, "validation_seeds": val_seeds,
+             "seeds": list(args.train_seeds), "steps_per_seed": args.train_steps,
+             "skipped_steps": args.train_skip}
     modes = {"fp64": ("zero", False), "mixed": ("zero", True), "extrapolate_fp64": ("extrapolate", False),
              "extrapolate_mixed": ("extrapolate", True), "learned_fp64": ("learned", False),
              "learned_mixed": ("learned", True)}
     for mode, (guess, mixed) in modes.items():
         sysd = H.HydroSystem(P, shell_op=shell, device=dev, tune=True)
         history = []
-        times, its, resid, phases, r0s = [], [], [], [], []
+        times, its, resid, phases, r0s, worst = [], [], [], [], [], []
         for step in range(warmup + steps):
             torch.cuda.synchronize()
             sysd.timers.report()
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            timed_step = step >= warmup
+            if timed_step:
+                torch.cuda.nvtx.range_push(f"timed_step_{mode}")
             e0.record()
             if history:
                 sysd.advance(history[-1])
@@ -450,12 +457,19 @@ def hydro_arm(args, rank, world, local, warmup=None, steps=None, emit=True):
             sysd.timers.stop("GMRES")
             e1.record()
             e1.synchronize()
+            if timed_step:
+                torch.cuda.nvtx.range_pop()
             ph = sysd.timers.report()
             sol = res["x"]
             history = (history + [sol])[-W.HISTORY:]
             if step >= warmup:
                 times.append(e0.elapsed_time(e1))
                 its.append(res["iterations"])
+                if res["iterations"] > 10:  # record the details of an unusually long solve
+                    worst.append({"step": step, "iterations": res["iterations"],
+                                  "refinements": res.get("refinements", 0),
+                                  "fp64_residuals": res.get("fp64_residuals", 0),
+                                  "history": [float(f"{h:.3g}") for h in res["history"]]})
                 r0s.append(res["history"][0])
                 phases.append(ph)
                 y = torch.empty_like(sol)
@@ -467,8 +481,9 @@ def hydro_arm(args, rank, world, local, warmup=None, steps=None, emit=True):
                 ref = sysd.solve(tol=1e-12, restart=100)["x"]
                 xs[mode] = float(torch.linalg.vector_norm(sol - ref) / torch.linalg.vector_norm(ref))
         out[mode] = {"ms_per_step": statistics.median(times), "iterations": its,
+                     "ms_per_step_last_half": statistics.median(times[len(times) // 2:]),
                      "true_rel_residual": max(resid), "refinements": res.get("refinements", 0),
-                     "initial_rel_residual": r0s,
+                     "initial_rel_residual": r0s, "long_solves": worst,
                      "phases_ms": {k: statistics.median([p.get(k, 0.0) for p in phases]) for k in phases[0]}}
         del sysd
     for mode in modes:
@@ -580,15 +595,17 @@ def main():
                     choices=["stresslet_sphere", "oseen_fibers", "hydro_step", "block_pc"])
     ap.add_argument("--nblocks", type=int, default=2000)
     ap.add_argument("--train-seeds", type=int, nargs="*", default=list(range(11, 19)))
-    ap.add_argument("--train-steps", type=int, default=30)
+    ap.add_argument("--train-steps", type=int, default=40)
     ap.add_argument("--train-epochs", type=int, default=40)
+    ap.add_argument("--train-skip", type=int, default=8,
+                    help="steps at the start of each trajectory left out of training and selection")
     ap.add_argument("--nshell", type=int, default=12000)
     ap.add_argument("--nfib", type=int, default=512)
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-step", action="store_true",
                     help="pair throughput only (skip the embedded time-step comparison)")
     ap.add_argument("--step-warmup", type=int, default=8)
-    ap.add_argument("--step-steps", type=int, default=12)
+    ap.add_argument("--step-steps", type=int, default=20)
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -96,20 +96,24 @@ __device__ __forceinline__ void inverse_step(double (&a)[kInvTR][kInvTC], int kb
   const unsigned kmax = __reduce_max_sync(0xffffffffu, row != 0xFFFFFFFFu ? key : 0u);
   const unsigned pmin = __reduce_min_sync(0xffffffffu, (row != 0xFFFFFFFFu && key == kmax) ? row : 0xFFFFFFFFu);
   const int p = pmin < static_cast<unsigned>(n) ? static_cast<int>(pmin) : k;
-  // (c) publish rows k and p (column k already zero)
+  // (c) publish rows k and p (column k already zero); 16-byte stores
   if (rt == k / kInvTR) {
-#pragma unroll
-    for (int j = 0; j < kInvTC; ++j) s_row[par][0][c0 + j] = a[II][j];
+    double2 *dst = reinterpret_cast<double2 *>(&s_row[par][0][c0]);
+    dst[0] = make_double2(a[II][0], a[II][1]);
+    dst[1] = make_double2(a[II][2], a[II][3]);
   }
   if (rt == p / kInvTR) {
     const int ip = p % kInvTR;
+    double v[kInvTC];
 #pragma unroll
     for (int j = 0; j < kInvTC; ++j) {
-      double v = a[0][j];
+      v[j] = a[0][j];
 #pragma unroll
-      for (int i = 1; i < kInvTR; ++i) v = (ip == i) ? a[i][j] : v;
-      s_row[par][1][c0 + j] = v;
+      for (int i = 1; i < kInvTR; ++i) v[j] = (ip == i) ? a[i][j] : v[j];
     }
+    double2 *dst = reinterpret_cast<double2 *>(&s_row[par][1][c0]);
+    dst[0] = make_double2(v[0], v[1]);
+    dst[1] = make_double2(v[2], v[3]);
   }
   if (tid == 0) s_piv[k] = p;
   __syncthreads();
@@ -119,9 +123,22 @@ __device__ __forceinline__ void inverse_step(double (&a)[kInvTR][kInvTC], int kb
   if (zero_pivot && first_zero == 0) first_zero = k + 1;
   const double pinv = zero_pivot ? 0.0 : reciprocal(pv);
   double u[kInvTC];
-#pragma unroll
-  for (int j = 0; j < kInvTC; ++j) u[j] = s_row[par][1][c0 + j];
+  {
+    const double2 *src = reinterpret_cast<const double2 *>(&s_row[par][1][c0]);
+    const double2 u01 = src[0], u23 = src[1];
+    u[0] = u01.x; u[1] = u01.y; u[2] = u23.x; u[3] = u23.y;
+  }
   if (ct == k / kInvTC) u[JJ] = 1.0;
+  double c[kInvTR];
+  {
+    const double2 *src = reinterpret_cast<const double2 *>(&s_col[par][r0]);
+#pragma unroll
+    for (int i = 0; i < kInvTR / 2; ++i) {
+      const double2 cc = src[i];
+      c[2 * i] = cc.x;
+      c[2 * i + 1] = cc.y;
+    }
+  }
 #pragma unroll
   for (int i = 0; i < kInvTR; ++i) {
     const int r = r0 + i;
@@ -131,11 +148,12 @@ __device__ __forceinline__ void inverse_step(double (&a)[kInvTR][kInvTC], int kb
     } else {
       double ci;
       if (r == p) {
-#pragma unroll
-        for (int j = 0; j < kInvTC; ++j) a[i][j] = s_row[par][0][c0 + j];
+        const double2 *src = reinterpret_cast<const double2 *>(&s_row[par][0][c0]);
+        const double2 w01 = src[0], w23 = src[1];
+        a[i][0] = w01.x; a[i][1] = w01.y; a[i][2] = w23.x; a[i][3] = w23.y;
         ci = s_col[par][k];
       } else {
-        ci = s_col[par][r];
+        ci = c[i];
       }
       const double f = ci * pinv;
 #pragma unroll
@@ -150,8 +168,8 @@ __global__ void __launch_bounds__(InvShape<NMAX>::kThreads, 1)
                            const int32_t *__restrict__ sizes, int count, float *__restrict__ A32,
                            int32_t *__restrict__ info) {
   using S = InvShape<NMAX>;
-  __shared__ double s_col[2][NMAX];
-  __shared__ double s_row[2][2][NMAX];  // [parity][0: old row k, 1: old row p][col]
+  __shared__ __align__(16) double s_col[2][NMAX];
+  __shared__ __align__(16) double s_row[2][2][NMAX];  // [parity][0: old row k, 1: old row p][col]
   __shared__ int s_piv[NMAX];
   __shared__ int s_dest[NMAX];
   const int b = blockIdx.x;

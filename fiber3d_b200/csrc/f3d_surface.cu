@@ -211,6 +211,57 @@ __global__ void gather_segments_kernel(const double *__restrict__ src, double *d
 
 // Per body b: the nvec[b] 3-vectors at x + off[b] are multiplied by R_b
 // (transpose = 0) or R_b^T (transpose = 1), R_b row-major at R + 9 b.
+// Rigid-body surfaces at a new location/orientation: node i of body b
+// (body_of[i]) gets x = R_b x_ref + c_b, n = R_b n_ref and, for the 3 x 3
+// singularity-vector map E_i (E[9i + 3a + c] = e_c(i)_a), E = R_b E_ref R_b^T.
+// One thread per node.
+__global__ void rigid_body_update_kernel(const int32_t *__restrict__ body_of,
+                                         const double *__restrict__ R, const double *__restrict__ loc,
+                                         const double *__restrict__ ref_nodes,
+                                         const double *__restrict__ ref_normals,
+                                         const double *__restrict__ ref_E, int64_t nnodes,
+                                         double *__restrict__ nodes, double *__restrict__ normals,
+                                         double *__restrict__ E) {
+  const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= nnodes) return;
+  const int b = body_of[i];
+  double r[9];
+#pragma unroll
+  for (int q = 0; q < 9; ++q) r[q] = R[9 * b + q];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    double x = loc[3 * b + a], nn = 0.0;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      x = fma(r[3 * a + c], ref_nodes[3 * i + c], x);
+      nn = fma(r[3 * a + c], ref_normals[3 * i + c], nn);
+    }
+    nodes[3 * i + a] = x;
+    normals[3 * i + a] = nn;
+  }
+  if (ref_E && E) {
+    double t[9];  // t = R E_ref
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        double v = 0.0;
+#pragma unroll
+        for (int m = 0; m < 3; ++m) v = fma(r[3 * a + m], ref_E[9 * i + 3 * m + c], v);
+        t[3 * a + c] = v;
+      }
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        double v = 0.0;
+#pragma unroll
+        for (int m = 0; m < 3; ++m) v = fma(t[3 * a + m], r[3 * c + m], v);
+        E[9 * i + 3 * a + c] = v;
+      }
+  }
+}
+
 __global__ void rotate_blocks_kernel(double *x, const int64_t *off, const int32_t *nvec,
                                      const double *R, int transpose) {
   const int b = blockIdx.x;
@@ -235,6 +286,19 @@ __global__ void rotate_blocks_kernel(double *x, const int64_t *off, const int32_
 }  // namespace f3d
 
 extern "C" {
+
+int f3d_rigid_body_update(const int32_t *body_of, const double *R, const double *loc,
+                          const double *ref_nodes, const double *ref_normals, const double *ref_E,
+                          int64_t nnodes, double *nodes, double *normals, double *E, void *stream) {
+  if (nnodes < 0) return F3D_ERR_SHAPE;
+  if (nnodes == 0) return F3D_OK;
+  if (!body_of || !R || !loc || !ref_nodes || !ref_normals || !nodes || !normals) return F3D_ERR_NULL;
+  if ((ref_E == nullptr) != (E == nullptr)) return F3D_ERR_NULL;
+  const unsigned grid = static_cast<unsigned>((nnodes + 127) / 128);
+  f3d::rigid_body_update_kernel<<<grid, 128, 0, static_cast<cudaStream_t>(stream)>>>(
+      body_of, R, loc, ref_nodes, ref_normals, ref_E, nnodes, nodes, normals, E);
+  return f3d::launch_status();
+}
 
 int f3d_rotate_blocks(double *x, const int64_t *offsets, const int32_t *nvec, const double *R,
                       int32_t nbody, int transpose, void *stream) {

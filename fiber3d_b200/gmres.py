@@ -27,7 +27,11 @@ the matvec is FP64, and the pair sums v carry a relative error below
 ``e = FP32C_PAIR_REL_ERR * |v| / |b|`` (relative).  The solve stops when
 ``|r| / |b| + e <= tol``, which bounds the FP64 residual by tol as well;
 while ``e <= tol / 2`` the residual stays FP32C, otherwise it is recomputed
-in FP64 (and stays FP64 for the rest of the solve).
+in FP64 (and stays FP64 for the rest of the solve).  After an inner solve
+the new residual is bounded without a matvec: by the inner GMRES estimate
+``|r - A32 d|`` plus e plus ``FP32C_PAIR_REL_ERR * sum_j |y_j| |v(z_j)|``
+(the FP32C error of the matvecs that built d = sum_j y_j z_j); when that sum
+is below tol the solve ends there, else the residual is computed.
 """
 from __future__ import annotations
 
@@ -68,22 +72,33 @@ class DeviceGMRES:
         _lib.call("f3d_krylov_workspace_bytes", n, self.m + 1, ctypes.byref(nb))
         self.ws = torch.zeros(max(nb.value, 4096), dtype=torch.uint8, device=dev)
         self.wsn = torch.zeros(4096, dtype=torch.uint8, device=dev)
-        self.h_host = torch.zeros(2 * (self.m + 2) + 1, dtype=torch.float64).pin_memory()
+        self.aux = f(self.m + 2)      # aux[j + 1] = |aux vector| after the matvec of step j
+        self.auxbeta = f(1)
+        self.h_host = torch.zeros(3 * (self.m + 2) + 1, dtype=torch.float64).pin_memory()
         self.graph = {}
+        self.last_aux_sum = 0.0
 
     # ------------------------------------------------------------ kernels --
     def _norm(self, w, beta):
+        """beta = |w|_2 over all of w (any length, contiguous float64)."""
+        if w.dtype != torch.float64 or not w.is_contiguous():
+            raise ValueError("norm of a contiguous float64 vector")
         st = _lib.stream_handle(self.device)
-        _lib.call("f3d_krylov_norm", _lib.ptr(w), self.n, None, None, _lib.ptr(beta), _lib.ptr(self.wsn),
+        _lib.call("f3d_krylov_norm", _lib.ptr(w), w.numel(), None, None, _lib.ptr(beta), _lib.ptr(self.wsn),
                   self.wsn.numel(), st)
 
-    def _arnoldi(self, matvec, pc):
-        """One Arnoldi step on the current stream (graph-capturable)."""
+    def _arnoldi(self, matvec, pc, aux=None):
+        """One Arnoldi step on the current stream (graph-capturable).  With
+        `aux` (a device vector the matvec writes, e.g. its pair sums) its
+        norm after the matvec is recorded for the step."""
         st = _lib.stream_handle(self.device)
         n, ldv = self.n, self.n
         pc(self.cur, self.z)
         _lib.call("f3d_krylov_store", _lib.ptr(self.z), _lib.ptr(self.k), -1, _lib.ptr(self.Z), n, n, st)
         matvec(self.z, self.w)
+        if aux is not None:
+            _lib.call("f3d_krylov_norm", _lib.ptr(aux), aux.numel(), _lib.ptr(self.k), _lib.ptr(self.aux),
+                      _lib.ptr(self.auxbeta), _lib.ptr(self.wsn), self.wsn.numel(), st)
         for h in (self.h1, self.h2):
             _lib.call("f3d_krylov_multidot", _lib.ptr(self.V), ldv, _lib.ptr(self.w), _lib.ptr(self.k),
                       self.m + 1, _lib.ptr(h), n, 0, _lib.ptr(self.ws), self.ws.numel(), st)
@@ -96,11 +111,14 @@ class DeviceGMRES:
         m2 = self.m + 2
         self.h_host[:m2].copy_(self.h1, non_blocking=True)
         self.h_host[m2:2 * m2].copy_(self.h2, non_blocking=True)
+        if aux is not None:
+            self.h_host[2 * m2:3 * m2].copy_(self.aux, non_blocking=True)
 
-    def _step(self, matvec, pc, key, use_graph):
+    def _step(self, matvec, pc, key, use_graph, aux=None):
         if not use_graph:
-            self._arnoldi(matvec, pc)
+            self._arnoldi(matvec, pc, aux)
             return
+        key = (key, aux is not None)
         g = self.graph.get(key)
         if g is None:
             # warm-up outside capture on a side stream (allocations, lazy init)
@@ -108,28 +126,33 @@ class DeviceGMRES:
             s.wait_stream(torch.cuda.current_stream(self.device))
             with torch.cuda.stream(s):
                 saved = (self.k.clone(), self.cur.clone(), self.V.clone(), self.Z.clone())
-                self._arnoldi(matvec, pc)
+                self._arnoldi(matvec, pc, aux)
                 self.k.copy_(saved[0]); self.cur.copy_(saved[1]); self.V.copy_(saved[2])
                 self.Z.copy_(saved[3])
             torch.cuda.current_stream(self.device).wait_stream(s)
             g = torch.cuda.CUDAGraph()
             with torch.cuda.graph(g):
-                self._arnoldi(matvec, pc)
+                self._arnoldi(matvec, pc, aux)
             self.graph[key] = g
         self.graph[key].replay()
 
     # ------------------------------------------------------------- solve ---
     def solve(self, matvec, pc, b: torch.Tensor, x0: torch.Tensor | None = None, rtol=1e-8,
-              maxiter=200, use_graph=True, key="default", bnorm=None, verify=True):
+              maxiter=200, use_graph=True, key="default", bnorm=None, verify=True, aux=None):
         """Solve A x = b with right preconditioner pc = P^-1.
 
         Returns (x, info, iterations, history of relative residual estimates).
         info = 0 on convergence, else the iteration count reached.  With
         verify=False the first cycle whose residual estimate meets rtol
         returns without recomputing the true residual (the caller judges the
-        result itself, as the mixed-precision refinement does).
+        result itself, as the mixed-precision refinement does).  With `aux`,
+        ``self.last_aux_sum`` is set to sum_j |y_j| |aux after A z_j| over the
+        correction x - x0 = sum_j y_j z_j (an error bound's ingredient).
         """
+        self.last_aux_sum = 0.0
         n, m = self.n, self.m
+        if b.numel() != n or (x0 is not None and x0.numel() != n):
+            raise ValueError(f"right-hand side and guess must have {n} entries")
         dev = self.device
         x = torch.zeros(n, dtype=torch.float64, device=dev) if x0 is None else x0.clone()
         r = torch.empty(n, dtype=torch.float64, device=dev)
@@ -165,7 +188,7 @@ class DeviceGMRES:
             g[0] = rnorm
             j_done = 0
             for j in range(m):
-                self._step(matvec, pc, key, use_graph)
+                self._step(matvec, pc, key, use_graph, aux)
                 torch.cuda.current_stream(dev).synchronize()
                 hh = self.h_host.numpy()
                 m2 = m + 2
@@ -195,6 +218,9 @@ class DeviceGMRES:
             y = np.zeros(j_done)
             for i in range(j_done - 1, -1, -1):
                 y[i] = (g[i] - H[i, i + 1:j_done] @ y[i + 1:j_done]) / H[i, i]
+            if aux is not None:
+                an = self.h_host.numpy()[2 * (m + 2):2 * (m + 2) + j_done + 1]
+                self.last_aux_sum += float(np.sum(np.abs(y) * an[1:j_done + 1]))
             yd = torch.as_tensor(y, device=dev)
             _lib.call("f3d_krylov_combine", _lib.ptr(self.Z), n, _lib.ptr(yd), j_done, _lib.ptr(r), n, 0,
                       _lib.stream_handle(dev))
@@ -234,9 +260,12 @@ def solve_system(system, tol=1e-8, restart=100, maxiter=200, x0=None, mixed=Fals
     info = 0
     outer = "fp32c"
     fp64_residuals = 0
+    known = None  # a bound on the FP64 relative residual of x, when one is at hand
     while True:
         bound = 0.0  # bound on |r_computed - r_fp64| / |b|
-        if x0 is None and ref == 0:
+        if known is not None:
+            rel, bound = known
+        elif x0 is None and ref == 0:
             r.copy_(b)
         else:
             system.matvec(x, tmp, outer)
@@ -249,9 +278,11 @@ def solve_system(system, tol=1e-8, restart=100, maxiter=200, x0=None, mixed=Fals
             if outer == "fp64":
                 fp64_residuals += 1
             torch.sub(b, tmp, out=r)
-        g._norm(r, g.beta)
-        rel = float(g.beta.item()) / bnorm
-        hist.append(rel)
+        if known is None:
+            g._norm(r, g.beta)
+            rel = float(g.beta.item()) / bnorm
+        known = None
+        hist.append(rel + bound)
         if rel + bound <= tol:  # the FP64 residual is <= tol as well
             break
         if ref >= max_refine or total_its >= maxiter:
@@ -259,13 +290,22 @@ def solve_system(system, tol=1e-8, restart=100, maxiter=200, x0=None, mixed=Fals
             break
         # inner tolerance relative to |r|: never ask beyond what is needed
         inner = max(inner_tol, 0.7 * (tol - bound) / rel)
-        d, _, its, _ = g.solve(lambda a, o: system.matvec(a, o, "fp32c"),
-                               lambda a, o: system.pc(a, o, "fp32c"), r, rtol=inner,
-                               maxiter=maxiter - total_its, use_graph=use_graph, key="fp32c",
-                               verify=False)
+        d, _, its, ihist = g.solve(lambda a, o: system.matvec(a, o, "fp32c"),
+                                   lambda a, o: system.pc(a, o, "fp32c"), r, rtol=inner,
+                                   maxiter=maxiter - total_its, use_graph=use_graph, key="fp32c",
+                                   verify=False, aux=system.v if outer == "fp32c" else None)
         total_its += its
         x += d
         ref += 1
+        if outer == "fp32c":
+            # |b - A64 (x + d)| <= |r - A32 d| + |(A32 - A64) x| + |(A32 - A64) d|:
+            # the inner GMRES estimate, the bound of the residual r, and the
+            # FP32C error of the matvecs that built d = sum_j y_j z_j
+            # (linear in y); no further matvec when this settles convergence.
+            est = ihist[-1] * rel
+            bd = FP32C_PAIR_REL_ERR * g.last_aux_sum / bnorm
+            if est + bound + bd <= tol:
+                known = (est, bound + bd)
     torch.cuda.synchronize()
     return {"x": x, "info": info, "iterations": total_its, "history": hist, "refinements": ref,
             "outer_residuals": outer, "fp64_residuals": fp64_residuals, "seconds": time.perf_counter() - t0}

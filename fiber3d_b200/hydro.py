@@ -383,19 +383,15 @@ class HydroSystem:
     # ------------------------------------------------------------------------
     def _load_bodies(self):
         """Body nodes, normals and singularity vectors at the current
-        location/orientation, on the device.  A rigid body's singularity
-        vectors are those of its reference surface rotated with it: the
-        3 x 3 map E_i (unit density -> velocity at node i) of the rotated
-        surface is R E_i^ref R^T (the stresslet sum is rotation-equivariant
-        and translation-invariant), so the pair sum runs once per body, at
-        set-up, not every step."""
+        location/orientation, on the device (one kernel).  A rigid body's
+        singularity vectors are those of its reference surface rotated with
+        it: the 3 x 3 map E_i (unit density -> velocity at node i) of the
+        rotated surface is R E_i^ref R^T (the stresslet sum is
+        rotation-equivariant and translation-invariant), so the pair sum runs
+        once per body, at set-up, not every step."""
         dev = self.device
-        Rh = np.stack([quaternion_rotation(q) for q in self.body_quat])
-        RL = torch.as_tensor(np.concatenate([Rh.reshape(-1, 9), self.body_loc], axis=1), device=dev)
-        R = RL[:, :9].reshape(-1, 3, 3)
-        loc = RL[:, 9:]
-        if not hasattr(self, "_body_idx"):
-            self._body_idx = torch.as_tensor(np.repeat(np.arange(self.nbody), self.nb), device=dev)
+        if not hasattr(self, "_body_of"):
+            self._body_of = torch.as_tensor(np.repeat(np.arange(self.nbody), self.nb).astype(np.int32), device=dev)
             self._ref_nodes = torch.as_tensor(np.concatenate(self.body_ref), device=dev)
             self._ref_normals = torch.as_tensor(np.concatenate(self.body_ref_n), device=dev)
             P = self.p
@@ -404,13 +400,22 @@ class HydroSystem:
                 a, b = int(self.body_node_off_h[k]), int(self.body_node_off_h[k + 1])
                 E.append(singularity_vectors(self._ref_nodes[a:b], self._ref_normals[a:b], self.body_w[a:b],
                                              P.eta, P.reg, P.eps_dist))
-            self._ref_E = torch.cat(E).view(-1, 3, 3)
-        Rn = R[self._body_idx]
-        self.body_nodes.copy_(torch.einsum("nij,nj->ni", Rn, self._ref_nodes) + loc[self._body_idx])
-        self.body_normals.copy_(torch.einsum("nij,nj->ni", Rn, self._ref_normals))
-        self.body_E.copy_((Rn @ self._ref_E @ Rn.transpose(1, 2)).reshape(-1, 9))
-        self.body_centers.copy_(loc)
-        self.body_R.copy_(R.reshape(-1, 9))
+            self._ref_E = torch.cat(E).contiguous()
+            self._rl_host = torch.zeros((self.nbody, 12), dtype=torch.float64).pin_memory()
+            self._rl_dev = torch.zeros((self.nbody, 12), dtype=torch.float64, device=dev)
+            self._rl_done = torch.cuda.Event()
+        self._rl_done.synchronize()  # the previous copy out of the pinned buffer has run
+        rl = self._rl_host.numpy()
+        rl[:, :9] = np.stack([quaternion_rotation(q).reshape(9) for q in self.body_quat])
+        rl[:, 9:] = self.body_loc
+        self._rl_dev.copy_(self._rl_host, non_blocking=True)
+        self._rl_done.record()
+        self.body_R.copy_(self._rl_dev[:, :9])
+        self.body_centers.copy_(self._rl_dev[:, 9:])
+        _lib.call("f3d_rigid_body_update", _lib.ptr(self._body_of), _lib.ptr(self.body_R), _lib.ptr(self.body_centers),
+                  _lib.ptr(self._ref_nodes), _lib.ptr(self._ref_normals), _lib.ptr(self._ref_E), self.nB,
+                  _lib.ptr(self.body_nodes), _lib.ptr(self.body_normals), _lib.ptr(self.body_E),
+                  _lib.stream_handle(dev))
 
     def _body_blocks(self):
         """Body preconditioner blocks in each body's own frame (location 0,
@@ -469,11 +474,10 @@ class HydroSystem:
                     blk = sol[o + 4 * p0:o + 4 * p0 + 4 * n].view(4, n)
                     self.x_fib[p0:p0 + n] = blk[:3].t()
         if self.nbody:
-            vel = sol.new_empty((self.nbody, 6))
-            for k in range(self.nbody):
-                i0 = self.o_body[k] + 3 * self.nb[k]
-                vel[k] = sol[i0:i0 + 6]
-            vel = vel.cpu().numpy()
+            if not hasattr(self, "_vel_idx"):
+                idx = np.array([[self.o_body[k] + 3 * self.nb[k] + c for c in range(6)] for k in range(self.nbody)])
+                self._vel_idx = torch.as_tensor(idx, device=sol.device)
+            vel = sol[self._vel_idx].cpu().numpy()
             for k in range(self.nbody):
                 self.body_loc[k] = self.body_loc[k] + dt * vel[k, :3]
                 self.body_quat[k] = quaternion_multiply(quaternion_from_rotation(vel[k, 3:] * dt), self.body_quat[k])

@@ -24,10 +24,11 @@ projected on the first few Legendre modes along the fiber before it is used:
 a point-to-point wiggle in a position guess is multiplied by the fourth
 derivative in the bending operator, so the correction must be smooth to
 lower the residual.  A gain per unknown group (positions, tensions), fitted
-by least squares on held-out steps and kept in [0, 1], scales it, and an
-overall factor is then chosen among a few candidates (0 included) by the
+by least squares on held-out steps and kept in [0, 1], scales it, and a
+factor per group is then chosen among a few candidates (0 included) by the
 GMRES iterations it gives on held-out trajectories: a correction that does
-not shorten GMRES there is switched off, and the guess is the extrapolation.
+not strictly shorten GMRES there is switched off, and where both are off the
+guess is the extrapolation.
 Periphery and body unknowns take x_q.  At inference the features, the
 network (output statistics, smoothing and gains folded into its last
 layer) and the guess take six kernel launches.
@@ -269,7 +270,7 @@ class LearnedWarmStart:
         self.device = self.net.device
         self.P = mode_projection(NPTS, modes, self.device)
         self.gain = torch.ones(2, dtype=torch.float32, device=self.device)
-        self.scale = 1.0          # overall factor chosen on held-out trajectories
+        self.scale = (1.0, 1.0)   # factors on the position / tension correction, chosen on held-out trajectories
         self._fold = None         # inference weights (see _folded)
 
     def smooth(self, Y: torch.Tensor) -> torch.Tensor:
@@ -279,8 +280,8 @@ class LearnedWarmStart:
     def predict(self, feats: torch.Tensor) -> torch.Tensor:
         """Smoothed, gain-scaled normalised correction (B, 128)."""
         C = self.smooth(self.net.predict(feats))
-        C[:, :3 * NPTS] *= self.gain[0] * self.scale
-        C[:, 3 * NPTS:] *= self.gain[1] * self.scale
+        C[:, :3 * NPTS] *= self.gain[0] * self.scale[0]
+        C[:, 3 * NPTS:] *= self.gain[1] * self.scale[1]
         return C
 
     def fit(self, X: torch.Tensor, T: torch.Tensor, epochs=30, batch=1024, lr=1e-3, val_frac=0.1,
@@ -305,23 +306,31 @@ class LearnedWarmStart:
         self._fold = None
         return hist
 
-    def select_scale(self, make_system, steps: int, candidates=(0.0, 0.5, 1.0), tol=1e-8) -> dict:
-        """Pick the overall factor with the fewest GMRES iterations over
-        held-out trajectories (ties: the lower geometric-mean initial
-        residual; then the smaller factor).  ``make_system()`` returns a
-        fresh system at the trajectory's first step."""
+    def select_scale(self, make_systems, steps: int, candidates=(0.0, 0.5, 1.0), tol=1e-8,
+                     count_from: int = HISTORY) -> dict:
+        """Pick the (position, tension) correction factors with the fewest
+        GMRES iterations over held-out trajectories, counted where the
+        network acts.  ``make_systems()`` returns fresh systems at the
+        trajectories' first steps; steps from `count_from` on are counted.
+        A correction must strictly lower the
+        iteration count to be kept: on a tie the smaller factors win, so a
+        network that does not shorten GMRES is switched off (the guess is
+        then the extrapolation)."""
         score = {}
-        for c in candidates:
-            self.scale = c
-            self._fold = None
-            st = march(make_system(), steps, guess="learned", net=self, tol=tol)
-            acting = st[HISTORY:] or st
-            its = sum(x["iterations"] for x in acting)
-            r0 = float(np.exp(np.mean(np.log([max(x["initial_rel_residual"], 1e-300) for x in acting]))))
-            score[c] = (its, r0, c)
-        self.scale = min(score, key=lambda c: score[c])
+        for cx in candidates:
+            for ct in candidates:
+                self.scale = (cx, ct)
+                self._fold = None
+                its, lr0 = 0, []
+                for sysd in make_systems():
+                    st = march(sysd, steps, guess="learned", net=self, tol=tol)
+                    acting = st[max(count_from, HISTORY):]
+                    its += sum(x["iterations"] for x in acting)
+                    lr0 += [np.log(max(x["initial_rel_residual"], 1e-300)) for x in acting]
+                score[(cx, ct)] = (its, cx + ct, float(np.exp(np.mean(lr0))) if lr0 else 1.0)
+        self.scale = min(score, key=lambda c: score[c][:2])
         self._fold = None
-        return {c: {"iterations": v[0], "r0_geomean": v[1]} for c, v in score.items()}
+        return {f"{c[0]},{c[1]}": {"iterations": v[0], "r0_geomean": v[2]} for c, v in score.items()}
 
     def _folded(self):
         """Inference weights: the output un-normalisation, the smoothing
@@ -330,7 +339,7 @@ class LearnedWarmStart:
         if self._fold is None:
             net = self.net
             Pi = torch.block_diag(self.P, self.P, self.P, self.P)
-            g = torch.cat([self.gain[0].expand(3 * NPTS), self.gain[1].expand(NPTS)]) * self.scale
+            g = torch.cat([self.gain[0].expand(3 * NPTS) * self.scale[0], self.gain[1].expand(NPTS) * self.scale[1]])
             M = g[:, None] * Pi
             W = list(net.W[:-1]) + [(M @ (net.out_std[:, None] * net.W[-1])).contiguous()]
             b = list(net.b[:-1]) + [(M @ (net.out_std * net.b[-1] + net.out_mean)).contiguous()]
@@ -341,7 +350,7 @@ class LearnedWarmStart:
         """The same guess from PyTorch ops around the network (test reference
         of :meth:`guess`)."""
         x_q = extrapolate(history)
-        if len(history) < HISTORY or not learnable(system) or self.scale == 0.0:
+        if len(history) < HISTORY or not learnable(system) or self.scale == (0.0, 0.0):
             return x_q
         f, sX, sT = history_features(system, history)
         return apply_correction(system, x_q, self.predict(f), sX, sT)
@@ -351,7 +360,7 @@ class LearnedWarmStart:
         once HISTORY solutions are known.  Six launches: the feature kernel
         (standardised inputs), four tensor-core GEMMs (the last one with the
         smoothing and gains folded in) and the guess kernel."""
-        if len(history) < HISTORY or not learnable(system) or self.scale == 0.0:
+        if len(history) < HISTORY or not learnable(system) or self.scale == (0.0, 0.0):
             return extrapolate(history)
         W, b = self._folded()
         h0, h1, h2, h3 = (h.contiguous() for h in history[-HISTORY:])
@@ -383,9 +392,10 @@ def learned_guess(system, history, model: LearnedWarmStart | None) -> torch.Tens
 
 # ------------------------------------------------------------ time marching --
 def march(system, steps: int, guess: str = "zero", net: LearnedWarmStart | None = None, tol=1e-8,
-          mixed=False, record=False, restart=100):
+          mixed=False, record=False, restart=100, record_from: int = 0):
     """Advance `system` `steps` time steps; per step return iterations, time
-    and (when record) the network's training pairs.
+    and (when record) the network's training pairs from step `record_from`
+    on.
 
     guess: 'zero' (fiber3d's GMRES start), 'previous' (last solution),
     'extrapolate' (quadratic extrapolation) or 'learned' (extrapolation plus
@@ -401,7 +411,7 @@ def march(system, steps: int, guess: str = "zero", net: LearnedWarmStart | None 
             system.advance(history[-1])
         x_q = extrapolate(history)
         f = None
-        if can_learn and len(history) >= HISTORY and record:
+        if can_learn and len(history) >= HISTORY and record and s >= record_from:
             f, sX, sT = history_features(system, history)
         if guess == "zero":
             x0 = None

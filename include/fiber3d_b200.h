@@ -348,6 +348,16 @@ int f3d_surface_dense(int mode, const double *nodes, const double *normals, cons
                       int64_t ld, double eta, double reg, double epsilon_distance,
                       void *stream);
 
+/* Rigid bodies at a new location/orientation (tstep.py:1392-1407 moves them;
+   body.get_r_vectors / get_normals give the surfaces): node i of body
+   b = body_of[i] gets nodes = R_b ref_nodes + loc_b, normals = R_b
+   ref_normals and, when ref_E/E are non-NULL, E_i = R_b E_ref,i R_b^T (the
+   singularity vectors of the rotated surface; 9 per node as
+   f3d_singularity_vectors writes them).  R: nbody row-major 3 x 3. */
+int f3d_rigid_body_update(const int32_t *body_of, const double *R, const double *loc,
+                          const double *ref_nodes, const double *ref_normals, const double *ref_E,
+                          int64_t nnodes, double *nodes, double *normals, double *E, void *stream);
+
 /* Rigid-body frame change of preconditioner vectors: for body b the nvec[b]
    3-vectors at x + offsets[b] become R_b v (transpose 0) or R_b^T v
    (transpose 1), R_b row-major at R + 9b.  With the body block factored

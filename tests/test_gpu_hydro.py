@@ -161,6 +161,19 @@ def test_fp32c_pair_error_bound(system, golden_step):
         assert err < 0.25 * FP32C_PAIR_REL_ERR
 
 
+def test_norm_of_vectors_of_any_length(system):
+    """The GMRES workspace's norm reads exactly the vector it is given (the
+    mixed solver takes the norm of the pair sums, which are shorter than the
+    unknown vector)."""
+    from fiber3d_b200.gmres import DeviceGMRES
+    g = DeviceGMRES(system.size, 10)
+    beta = torch.zeros(1, dtype=torch.float64, device="cuda")
+    for n in (1, 7, 1000, system.size - 3, system.size):
+        w = torch.randn(n, dtype=torch.float64, device="cuda")
+        g._norm(w, beta)
+        assert abs(float(beta) - float(torch.linalg.vector_norm(w))) <= 1e-14 * float(torch.linalg.vector_norm(w))
+
+
 def test_graph_and_eager_agree(system):
     a = system.solve(tol=1e-9, use_graph=False)["x"]
     b = system.solve(tol=1e-9, use_graph=True)["x"]
