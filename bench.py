@@ -200,9 +200,11 @@ def gpu_arm(args, rank, world, local):
         for _ in range(steps):
             flush.fill_(1)
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.nvtx.range_push(f"timed_pairs_{precision}")
             e0.record()
             step(precision)
             e1.record()
+            torch.cuda.nvtx.range_pop()
             evs.append((e0, e1))
         torch.cuda.synchronize()
         if world > 1:
@@ -428,11 +430,13 @@ def hydro_arm(args, rank, world, local, warmup=None, steps=None, emit=True):
              "scale_selection": sel, "validation_seeds": val_seeds,
              "seeds": list(args.train_seeds), "steps_per_seed": args.train_steps,
              "skipped_steps": args.train_skip}
-    modes = {"fp64": ("zero", False), "mixed": ("zero", True), "extrapolate_fp64": ("extrapolate", False),
-             "extrapolate_mixed": ("extrapolate", True), "learned_fp64": ("learned", False),
-             "learned_mixed": ("learned", True)}
-    for mode, (guess, mixed) in modes.items():
-        sysd = H.HydroSystem(P, shell_op=shell, device=dev, tune=True)
+    # mode: (guess, mixed precision, preconditioner refresh interval)
+    modes = {"fp64": ("zero", False, 1), "mixed": ("zero", True, 1),
+             "extrapolate_fp64": ("extrapolate", False, 1), "extrapolate_mixed": ("extrapolate", True, 1),
+             "learned_fp64": ("learned", False, 1), "learned_mixed": ("learned", True, 1),
+             "learned_mixed_pc4": ("learned", True, 4)}
+    for mode, (guess, mixed, pc_refresh) in modes.items():
+        sysd = H.HydroSystem(P, shell_op=shell, device=dev, tune=True, pc_refresh=pc_refresh)
         history = []
         times, its, resid, phases, r0s, worst = [], [], [], [], [], []
         for step in range(warmup + steps):

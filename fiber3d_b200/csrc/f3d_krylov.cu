@@ -54,14 +54,19 @@ __global__ void __launch_bounds__(kDotThreads) multidot_stage1(const double *__r
   }
 }
 
-// Stage 2: h[i] (+)= sum_c part[c * kmax + i], c in order.
+// Stage 2: h[i] (+)= sum_c part[c * kmax + i].  One warp per i: lane l sums
+// c = l, l + 32, ... in order, then a fixed butterfly; the order is the same
+// on every call.
 __global__ void multidot_stage2(const double *part, int nparts, const int *kptr, int kmax,
                                 double *h, int accumulate) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int lane = threadIdx.x & 31;
+  const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   if (i >= *kptr) return;
   double s = 0.0;
-  for (int c = 0; c < nparts; ++c) s += part[static_cast<int64_t>(c) * kmax + i];
-  h[i] = accumulate ? h[i] + s : s;
+  for (int c = lane; c < nparts; c += 32) s += part[static_cast<int64_t>(c) * kmax + i];
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
+  if (lane == 0) h[i] = accumulate ? h[i] + s : s;
 }
 
 // w[j] -= sum_{i<k} h[i] V[i][j]
@@ -117,9 +122,14 @@ __global__ void __launch_bounds__(kDotThreads) sumsq_stage1(const double *__rest
 // Hessenberg column, whose first k entries the caller already holds).
 __global__ void norm_stage2(const double *part, int nparts, const int *kptr, double *hcol,
                             double *beta_out) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  // one warp: lane l sums parts l, l + 32, ... in order, then a fixed butterfly
+  const int lane = threadIdx.x & 31;
+  if (threadIdx.x >= 32 || blockIdx.x != 0) return;
   double s = 0.0;
-  for (int c = 0; c < nparts; ++c) s += part[c];
+  for (int c = lane; c < nparts; c += 32) s += part[c];
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
+  if (lane != 0) return;
   const double b = sqrt(s);
   if (hcol) hcol[*kptr] = b;
   if (beta_out) *beta_out = b;
@@ -389,7 +399,7 @@ int f3d_krylov_multidot(const double *V, int64_t ldv, const double *w, const int
   f3d::multidot_stage1<<<parts, f3d::kDotThreads, 0, st>>>(V, w, k, n, ldv, part, kmax);
   int rc = f3d::launch_status();
   if (rc) return rc;
-  f3d::multidot_stage2<<<(kmax + 127) / 128, 128, 0, st>>>(part, parts, k, kmax, h, accumulate);
+  f3d::multidot_stage2<<<(kmax + 7) / 8, 256, 0, st>>>(part, parts, k, kmax, h, accumulate);
   return f3d::launch_status();
 }
 

@@ -23,13 +23,17 @@ preconditioner reads FP32/FP16 copies of the block inverses (Arnoldi and
 Givens stay FP64).  The outer residual is itself evaluated with the FP32C
 pair sums when that cannot change the convergence test: every other part of
 the matvec is FP64, and the pair sums v carry a relative error below
-``FP32C_PAIR_REL_ERR``, so the residual is off by at most
-``e = FP32C_PAIR_REL_ERR * |v| / |b|`` (relative).  The solve stops when
+``FP32C_PAIR_REL_ERR``; they enter the matvec through a linear map of norm
+at most G (``system.v_gain``: 1 on periphery and body rows, the norm of the
+projected value-and-derivative rows on fibers), so the residual is off by at
+most ``e = FP32C_PAIR_REL_ERR * G * |v| / |b|`` (relative).  The solve stops when
 ``|r| / |b| + e <= tol``, which bounds the FP64 residual by tol as well;
 while ``e <= tol / 2`` the residual stays FP32C, otherwise it is recomputed
-in FP64 (and stays FP64 for the rest of the solve).  After an inner solve
+in FP64 (and stays FP64 for the rest of the solve and for later solves of
+the same system, whose |v| / |b| changes little from step to step).  After an inner solve
 the new residual is bounded without a matvec: by the inner GMRES estimate
-``|r - A32 d|`` plus e plus ``FP32C_PAIR_REL_ERR * sum_j |y_j| |v(z_j)|``
+``|r - A32 d|`` plus e (0 for an FP64 residual) plus
+``FP32C_PAIR_REL_ERR * G * sum_j |y_j| |v(z_j)|``
 (the FP32C error of the matvecs that built d = sum_j y_j z_j); when that sum
 is below tol the solve ends there, else the residual is computed.
 """
@@ -258,8 +262,13 @@ def solve_system(system, tol=1e-8, restart=100, maxiter=200, x0=None, mixed=Fals
     bnorm = float(g.beta.item())
     total_its, hist, ref = 0, [], 0
     info = 0
-    outer = "fp32c"
+    # outer residuals start FP32C unless an earlier solve of this system found
+    # their bound too loose (the ratio |v| / |b| changes little between steps)
+    outer = "fp64" if getattr(system, "_outer_fp64", False) else "fp32c"
     fp64_residuals = 0
+    # |A32 x - A64 x| <= eps_v |v(x)|: the pair-sum error times the gain of
+    # the map from the pair sums to the matvec's rows
+    eps_v = FP32C_PAIR_REL_ERR * getattr(system, "v_gain", 1.0)
     known = None  # a bound on the FP64 relative residual of x, when one is at hand
     while True:
         bound = 0.0  # bound on |r_computed - r_fp64| / |b|
@@ -271,9 +280,10 @@ def solve_system(system, tol=1e-8, restart=100, maxiter=200, x0=None, mixed=Fals
             system.matvec(x, tmp, outer)
             if outer == "fp32c":
                 g._norm(system.v, g.beta)
-                bound = FP32C_PAIR_REL_ERR * float(g.beta.item()) / bnorm
+                bound = eps_v * float(g.beta.item()) / bnorm
                 if bound > 0.5 * tol:
                     outer, bound = "fp64", 0.0
+                    system._outer_fp64 = True
                     system.matvec(x, tmp, outer)
             if outer == "fp64":
                 fp64_residuals += 1
@@ -293,19 +303,18 @@ def solve_system(system, tol=1e-8, restart=100, maxiter=200, x0=None, mixed=Fals
         d, _, its, ihist = g.solve(lambda a, o: system.matvec(a, o, "fp32c"),
                                    lambda a, o: system.pc(a, o, "fp32c"), r, rtol=inner,
                                    maxiter=maxiter - total_its, use_graph=use_graph, key="fp32c",
-                                   verify=False, aux=system.v if outer == "fp32c" else None)
+                                   verify=False, aux=system.v)
         total_its += its
         x += d
         ref += 1
-        if outer == "fp32c":
-            # |b - A64 (x + d)| <= |r - A32 d| + |(A32 - A64) x| + |(A32 - A64) d|:
-            # the inner GMRES estimate, the bound of the residual r, and the
-            # FP32C error of the matvecs that built d = sum_j y_j z_j
-            # (linear in y); no further matvec when this settles convergence.
-            est = ihist[-1] * rel
-            bd = FP32C_PAIR_REL_ERR * g.last_aux_sum / bnorm
-            if est + bound + bd <= tol:
-                known = (est, bound + bd)
+        # |b - A64 (x + d)| <= |r - A32 d| + |r - r64| + |(A32 - A64) d|: the
+        # inner GMRES estimate, the bound of the residual r (0 when FP64),
+        # and the FP32C error of the matvecs that built d = sum_j y_j z_j
+        # (linear in y); no further matvec when this settles convergence.
+        est = ihist[-1] * rel
+        bd = eps_v * g.last_aux_sum / bnorm
+        if est + bound + bd <= tol:
+            known = (est, bound + bd)
     torch.cuda.synchronize()
     return {"x": x, "info": info, "iterations": total_its, "history": hist, "refinements": ref,
             "outer_residuals": outer, "fp64_residuals": fp64_residuals, "seconds": time.perf_counter() - t0}

@@ -269,7 +269,8 @@ class HydroSystem:
     :meth:`pc` (the right preconditioner P^-1) and :meth:`solve`."""
 
     def __init__(self, problem: Problem, shell_op: ShellOperator | None = None, device=None,
-                 tune: bool = False, fiber_pc: str = "auto", inner_shell_pc: str = "fp16"):
+                 tune: bool = False, fiber_pc: str = "auto", inner_shell_pc: str = "fp16",
+                 pc_refresh: int = 1):
         self.p = problem
         dev = device or torch.device("cuda", torch.cuda.current_device())
         self.device = dev
@@ -287,6 +288,7 @@ class HydroSystem:
         self.has_force = bool(np.any(ff))
         self.geo = torch.empty((max(nF, 1), 9), dtype=torch.float64, device=dev)
         self.timers = PhaseTimers()
+        self.v_gain = self._flow_to_residual_gain(P.lengths)
         # ---- bodies (host state: location, orientation; device: nodes, normals, E)
         self.nbody = len(P.bodies)
         nb = [np.asarray(b.ref_nodes).reshape(-1, 3).shape[0] for b in P.bodies]
@@ -375,10 +377,33 @@ class HydroSystem:
         if inner_shell_pc not in ("fp32", "fp16"):
             raise ValueError("inner_shell_pc must be 'fp32' or 'fp16'")
         self.inner_shell_pc = inner_shell_pc
+        # the fiber blocks of the preconditioner are rebuilt every pc_refresh
+        # steps (fiber3d: every step); in between the last ones are kept --
+        # still a fixed operator within each solve, of a geometry at most
+        # pc_refresh - 1 steps old
+        if pc_refresh < 1:
+            raise ValueError("pc_refresh must be >= 1")
+        self.pc_refresh = int(pc_refresh)
+        self._pc_age = None
         self.A_fib = torch.zeros(max(self.fs.mat_total, 1), dtype=torch.float64, device=dev)
         self.flow_ext = torch.zeros((max(nF, 1), 3), dtype=torch.float64, device=dev)
         self._body_blocks()
         self.update()
+
+    def _flow_to_residual_gain(self, lengths) -> float:
+        """Bound on |d(matvec)| / |d v| for a change d v of the pair sums v at
+        the targets: 1 on periphery and body rows; on a fiber's rows v enters
+        as P_X v (positions) and P_T (x_s . (2/L) D1 v) (tensions), whose
+        2-norm is at most sqrt(|P_X|^2 + ((2/L) |P_T| |D1|)^2) (|x_s| = 1)."""
+        g = 1.0
+        lengths = np.asarray(lengths, dtype=np.float64).reshape(-1)
+        for n, res in self.fs.resolutions.items():
+            Lmin = float(lengths[self.fs.npts == n].min()) if lengths.size else 1.0
+            nx = np.linalg.norm(res.PX, 2)
+            nt = np.linalg.norm(res.PT, 2)
+            nd = np.linalg.norm(res.D0[0], 2)
+            g = max(g, float(np.sqrt(nx ** 2 + (2.0 / Lmin * nt * nd) ** 2)))
+        return g
 
     # ------------------------------------------------------------------------
     def _load_bodies(self):
@@ -520,19 +545,24 @@ class HydroSystem:
             self.rhs[self.o_body[k]:self.o_body[k] + 3 * (b - a)] = -v[nF + a:nF + b].reshape(-1)
         flow = self.flow_ext
         # fiber blocks into A_fib and (a copy) into the LU buffer
+        refresh = self._pc_age is None or self._pc_age >= self.pc_refresh - 1
         self.timers.start("Build_linear_system_fibers")
         if nF:
-            A_copy = self.lu.A.data_ptr()
+            A_copy = self.lu.A.data_ptr() if refresh else None
             _lib.call("f3d_fiber_assemble", ctypes.byref(self.fs.c), P.E, P.dt, self.c0, self.c1, P.penalty,
                       _lib.ptr(self.x_fib), _lib.ptr(self.geo), _lib.ptr(flow), _lib.ptr(self.force),
                       _lib.ptr(self.A_fib), A_copy, _lib.ptr(self.rhs[self.o_fib:]), self.fs.max_n, st)
         self.timers.stop("Build_linear_system_fibers")
-        self.timers.start("Build_PC_fibers")
-        if self.fiber_pc == "inverse":
-            self.lu.invert(fp32=True)
+        if refresh:
+            self.timers.start("Build_PC_fibers")
+            if self.fiber_pc == "inverse":
+                self.lu.invert(fp32=True)
+            else:
+                self.lu.factor()
+            self.timers.stop("Build_PC_fibers")
+            self._pc_age = 0
         else:
-            self.lu.factor()
-        self.timers.stop("Build_PC_fibers")
+            self._pc_age += 1
 
     # ------------------------------------------------------------------------
     def matvec(self, x: torch.Tensor, y: torch.Tensor, precision: str = "fp64") -> torch.Tensor:

@@ -156,9 +156,13 @@ def test_fp32c_pair_error_bound(system, golden_step):
         xd = torch.tensor(x, device="cuda")
         system.matvec(xd, y, "fp64")
         v64 = system.v.clone()
+        y64 = y.clone()
         system.matvec(xd, y, "fp32c")
         err = float(torch.linalg.vector_norm(system.v - v64) / torch.linalg.vector_norm(v64))
         assert err < 0.25 * FP32C_PAIR_REL_ERR
+        # the matvec itself moves by at most eps G |v| (G = system.v_gain)
+        dy = float(torch.linalg.vector_norm(y - y64))
+        assert dy <= FP32C_PAIR_REL_ERR * system.v_gain * float(torch.linalg.vector_norm(v64))
 
 
 def test_norm_of_vectors_of_any_length(system):
