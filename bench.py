@@ -447,8 +447,9 @@ def hydro_arm(args, rank, world, local, warmup=None, steps=None, emit=True):
             if timed_step:
                 torch.cuda.nvtx.range_push(f"timed_step_{mode}")
             e0.record()
-            if history:
-                sysd.advance(history[-1])
+            # the guess needs only the previous solutions: formed first, it is
+            # handed to advance(), which sums its Oseen flow in the same pass
+            # as the explicit flow
             sysd.timers.start("warm_start")
             x0 = None
             if guess == "extrapolate":
@@ -456,6 +457,8 @@ def hydro_arm(args, rank, world, local, warmup=None, steps=None, emit=True):
             elif guess == "learned":
                 x0 = W.learned_guess(sysd, history, net)
             sysd.timers.stop("warm_start")
+            if history:
+                sysd.advance(history[-1], x0=x0)
             sysd.timers.start("GMRES")
             res = sysd.solve(tol=1e-8, restart=100, mixed=mixed, x0=x0)
             sysd.timers.stop("GMRES")

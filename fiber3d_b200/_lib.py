@@ -65,6 +65,9 @@ SIGNATURES: dict[str, list] = {
     "f3d_pair_workspace_bytes": [_I, _I, _I64, _I64, ctypes.POINTER(PairShape), ctypes.POINTER(_SZ)],
     "f3d_pair_sum": [_I, _I, _I, _P, _P, _P, _P, _P, _P, _P, _I64, _I64, _D, _D, _D, _I,
                      ctypes.POINTER(PairShape), _P, _SZ, _P],
+    "f3d_oseen_dual_workspace_bytes": [_I64, _I64, ctypes.POINTER(PairShape), ctypes.POINTER(_SZ)],
+    "f3d_oseen_dual": [_I, _P, _P, _P, _P, _P, _P, _P, _P, _I64, _I64, _D, _D, _D, _I, ctypes.POINTER(PairShape), _P,
+                       _SZ, _P],
     "f3d_pair_sum_noalloc": [_I, _I, _I, _P, _P, _P, _P, _P, _P, _P, _I64, _I64, _D, _D, _D, _I, _P],
     "f3d_oseen_source_target": [_P, _P, _P, _P, _I64, _I64, _D, _D, _D, _I, _P, _SZ, _P],
     "f3d_oseen_times_density": [_P, _P, _P, _I64, _D, _D, _D, _I, _P, _SZ, _P],

@@ -34,10 +34,12 @@ constexpr size_t kCounterBytes = kMaxCounters * sizeof(unsigned);
 
 struct PairArgs {
   const double *rs, *rt, *dens, *nrm;
+  const double *dens2;  // dual sums: the second density (FP64 only)
   const float *packed;  // FP32C: [ns][12] packed source records
   const int32_t *gs, *gt;
   double *out;
-  double *partial;          // [nsplit][nt][3]
+  double *out2;             // dual sums: the second output
+  double *partial;          // [nsplit][nt][3] (dual: a second such array follows)
   unsigned int *counters;   // [gridDim.x], zero on entry, zero on exit
   int *err;
   int64_t ns, nt;
@@ -49,24 +51,25 @@ struct PairArgs {
 };
 
 // Shared-memory layout of one stage.
-template <int KIND, int MODE, int PREC>
+template <int KIND, int MODE, int PREC, bool DUAL = false>
 struct Stage {
   static constexpr bool kNrm = (KIND == F3D_KERNEL_STRESSLET);
   static constexpr bool kGrp = (MODE == F3D_SELF_SKIP_GROUP);
-  // FP64: pos[3T] dens[3T] (nrm[3T]) (grp[T]);  FP32C: rec[12T] (grp[T])
+  // FP64: pos[3T] dens[3T] (nrm[3T]) (dens2[3T]) (grp[T]);  FP32C: rec[12T] (grp[T])
   static constexpr size_t off_pos = 0;
   static constexpr size_t off_dens = 24 * kTile;
   static constexpr size_t off_nrm = 48 * kTile;
+  static constexpr size_t off_dens2 = (kNrm ? 72 : 48) * kTile;
   static constexpr size_t off_rec = 0;
   static constexpr size_t data_bytes =
-      (PREC == F3D_FP64) ? (kNrm ? 72 * kTile : 48 * kTile) : 48 * kTile;
+      (PREC == F3D_FP64) ? (kNrm ? 72 * kTile : 48 * kTile) + (DUAL ? 24 * kTile : 0) : 48 * kTile;
   static constexpr size_t off_grp = data_bytes;
   static constexpr size_t bytes = ((data_bytes + (kGrp ? 4 * kTile : 0)) + 127) / 128 * 128;
 };
 
-template <int KIND, int MODE, int PREC>
+template <int KIND, int MODE, int PREC, bool DUAL = false>
 constexpr size_t pair_smem_bytes() {
-  return 128 + 2 * Stage<KIND, MODE, PREC>::bytes;
+  return 128 + 2 * Stage<KIND, MODE, PREC, DUAL>::bytes;
 }
 
 // 1/sqrt(x) in FP64: the hardware approximation (PTX rsqrt.approx.ftz.f64,
@@ -95,9 +98,13 @@ __device__ __forceinline__ void two_sum(float &s, float &c, float x) {
   c += e;
 }
 
-template <int KIND, int MODE, int PREC, int TPT, int SL>
+// DUAL (FP64 Oseen only): the same pairs summed against two densities, dens
+// into out and dens2 into out2, each with exactly the arithmetic of a single
+// sum -- the geometry (r, 1/r, 1/r^3) is computed once for both.
+template <int KIND, int MODE, int PREC, int TPT, int SL, bool DUAL = false>
 __global__ void __launch_bounds__(kBlock) pair_kernel(const PairArgs a) {
-  using St = Stage<KIND, MODE, PREC>;
+  static_assert(!DUAL || (PREC == F3D_FP64 && KIND == F3D_KERNEL_OSEEN), "dual sums: FP64 Oseen");
+  using St = Stage<KIND, MODE, PREC, DUAL>;
   constexpr int TG = kBlock / SL;
   constexpr int TPB = TG * TPT;
   extern __shared__ __align__(128) unsigned char smem[];
@@ -136,12 +143,14 @@ __global__ void __launch_bounds__(kBlock) pair_kernel(const PairArgs a) {
     }
   }
 
-  double acc[TPT][3];
+  double acc[TPT][3], acc2[TPT][3];
   float fs[TPT][3], fc[TPT][3], ft[TPT][3];
 #pragma unroll
   for (int k = 0; k < TPT; ++k)
 #pragma unroll
-    for (int c = 0; c < 3; ++c) { acc[k][c] = 0.0; fs[k][c] = 0.f; fc[k][c] = 0.f; ft[k][c] = 0.f; }
+    for (int c = 0; c < 3; ++c) {
+      acc[k][c] = 0.0; acc2[k][c] = 0.0; fs[k][c] = 0.f; fc[k][c] = 0.f; ft[k][c] = 0.f;
+    }
 
   const double reg2 = a.reg2;
   const long long eps2_bits = __double_as_longlong(a.eps2);
@@ -158,6 +167,11 @@ __global__ void __launch_bounds__(kBlock) pair_kernel(const PairArgs a) {
         const double d0 = den[3 * s], d1 = den[3 * s + 1], d2 = den[3 * s + 2];
         double n0 = 0.0, n1 = 0.0, n2 = 0.0;
         if (KIND == F3D_KERNEL_STRESSLET) { n0 = nrm[3 * s]; n1 = nrm[3 * s + 1]; n2 = nrm[3 * s + 2]; }
+        double e0 = 0.0, e1 = 0.0, e2 = 0.0;
+        if (DUAL) {
+          const double *den2 = reinterpret_cast<const double *>(buf + St::off_dens2);
+          e0 = den2[3 * s]; e1 = den2[3 * s + 1]; e2 = den2[3 * s + 2];
+        }
         int32_t sg = 0;
         if (MODE == F3D_SELF_SKIP_GROUP) sg = reinterpret_cast<const int32_t *>(buf + St::off_grp)[s];
 #pragma unroll
@@ -168,11 +182,19 @@ __global__ void __launch_bounds__(kBlock) pair_kernel(const PairArgs a) {
           if (MODE == F3D_SELF_SKIP_INDEX) ri = (sbase + s == tidx[k]) ? 0.0 : ri;
           if (MODE == F3D_SELF_SKIP_GROUP) ri = (sg == tgrp[k]) ? 0.0 : ri;
           if (KIND == F3D_KERNEL_OSEEN) {
+            const double ri3 = ri * ri * ri;
             const double rf = fma(dx, d0, fma(dy, d1, dz * d2));
-            const double g = ri * ri * ri * rf;
+            const double g = ri3 * rf;
             acc[k][0] = fma(g, dx, fma(ri, d0, acc[k][0]));
             acc[k][1] = fma(g, dy, fma(ri, d1, acc[k][1]));
             acc[k][2] = fma(g, dz, fma(ri, d2, acc[k][2]));
+            if (DUAL) {
+              const double re = fma(dx, e0, fma(dy, e1, dz * e2));
+              const double g2 = ri3 * re;
+              acc2[k][0] = fma(g2, dx, fma(ri, e0, acc2[k][0]));
+              acc2[k][1] = fma(g2, dy, fma(ri, e1, acc2[k][1]));
+              acc2[k][2] = fma(g2, dz, fma(ri, e2, acc2[k][2]));
+            }
           } else if (KIND == F3D_KERNEL_ROTLET) {
             const double g = ri * ri * ri;
             acc[k][0] = fma(g, dz * d1 - dy * d2, acc[k][0]);
@@ -241,10 +263,12 @@ __global__ void __launch_bounds__(kBlock) pair_kernel(const PairArgs a) {
       double *pos = reinterpret_cast<double *>(buf + St::off_pos);
       double *den = reinterpret_cast<double *>(buf + St::off_dens);
       double *nrm = reinterpret_cast<double *>(buf + St::off_nrm);
+      double *den2 = reinterpret_cast<double *>(buf + St::off_dens2);
       for (int i = tid; i < 3 * cnt; i += kBlock) {
         pos[i] = a.rs[3 * s0 + i];
         den[i] = a.dens[3 * s0 + i];
         if (KIND == F3D_KERNEL_STRESSLET) nrm[i] = a.nrm[3 * s0 + i];
+        if (DUAL) den2[i] = a.dens2[3 * s0 + i];
       }
     } else {
       float *rec = reinterpret_cast<float *>(buf + St::off_rec);
@@ -261,6 +285,7 @@ __global__ void __launch_bounds__(kBlock) pair_kernel(const PairArgs a) {
     unsigned char *buf = stages + st * St::bytes;
     const int64_t s0 = tile * kTile;
     uint32_t bytes = (PREC == F3D_FP64) ? (St::kNrm ? 72u : 48u) * kTile : 48u * kTile;
+    if (DUAL) bytes += 24u * kTile;
     if (MODE == F3D_SELF_SKIP_GROUP) bytes += 4u * kTile;
     mbar_arrive_expect_tx(&bars[st], bytes);
     if (PREC == F3D_FP64) {
@@ -268,6 +293,7 @@ __global__ void __launch_bounds__(kBlock) pair_kernel(const PairArgs a) {
       bulk_copy_g2s(buf + St::off_dens, a.dens + 3 * s0, 24u * kTile, &bars[st]);
       if (KIND == F3D_KERNEL_STRESSLET)
         bulk_copy_g2s(buf + St::off_nrm, a.nrm + 3 * s0, 24u * kTile, &bars[st]);
+      if (DUAL) bulk_copy_g2s(buf + St::off_dens2, a.dens2 + 3 * s0, 24u * kTile, &bars[st]);
     } else {
       bulk_copy_g2s(buf + St::off_rec, a.packed + 12 * s0, 48u * kTile, &bars[st]);
     }
@@ -329,16 +355,21 @@ __global__ void __launch_bounds__(kBlock) pair_kernel(const PairArgs a) {
   }
 
   // ---- combine lanes of a target group -----------------------------------
-  double res[TPT][3];
+  double res[TPT][3], res2[TPT][3];
 #pragma unroll
   for (int k = 0; k < TPT; ++k)
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
       double v = (PREC == F3D_FP64) ? acc[k][c]
                                     : static_cast<double>(fs[k][c]) + static_cast<double>(fc[k][c]);
+      double v2 = acc2[k][c];
 #pragma unroll
-      for (int off = SL / 2; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+      for (int off = SL / 2; off > 0; off >>= 1) {
+        v += __shfl_xor_sync(0xffffffffu, v, off);
+        if (DUAL) v2 += __shfl_xor_sync(0xffffffffu, v2, off);
+      }
       res[k][c] = v;
+      res2[k][c] = v2;
     }
 
   if (a.nsplit == 1) {
@@ -351,6 +382,10 @@ __global__ void __launch_bounds__(kBlock) pair_kernel(const PairArgs a) {
           for (int c = 0; c < 3; ++c) {
             const double v = a.scale * res[k][c];
             a.out[3 * t + c] = a.accumulate ? a.out[3 * t + c] + v : v;
+            if (DUAL) {
+              const double v2 = a.scale * res2[k][c];
+              a.out2[3 * t + c] = a.accumulate ? a.out2[3 * t + c] + v2 : v2;
+            }
           }
         }
       }
@@ -365,8 +400,11 @@ __global__ void __launch_bounds__(kBlock) pair_kernel(const PairArgs a) {
       const int64_t t = tidx[k];
       if (t < a.nt) {
 #pragma unroll
-        for (int c = 0; c < 3; ++c)
+        for (int c = 0; c < 3; ++c) {
           __stcg(&a.partial[(static_cast<int64_t>(split) * a.nt + t) * 3 + c], res[k][c]);
+          if (DUAL)
+            __stcg(&a.partial[(static_cast<int64_t>(a.nsplit + split) * a.nt + t) * 3 + c], res2[k][c]);
+        }
       }
     }
   }
@@ -387,6 +425,13 @@ __global__ void __launch_bounds__(kBlock) pair_kernel(const PairArgs a) {
     for (int sp = 0; sp < a.nsplit; ++sp) v += __ldcg(&a.partial[static_cast<int64_t>(sp) * a.nt * 3 + gi]);
     v *= a.scale;
     a.out[gi] = a.accumulate ? a.out[gi] + v : v;
+    if (DUAL) {
+      double v2 = 0.0;
+      for (int sp = 0; sp < a.nsplit; ++sp)
+        v2 += __ldcg(&a.partial[static_cast<int64_t>(a.nsplit + sp) * a.nt * 3 + gi]);
+      v2 *= a.scale;
+      a.out2[gi] = a.accumulate ? a.out2[gi] + v2 : v2;
+    }
   }
   if (tid == 0) a.counters[blockIdx.x] = 0u;
 }
@@ -425,7 +470,7 @@ struct Plan {
 };
 
 static int make_plan(int kernel, int precision, int64_t ns, int64_t nt, const f3d_pair_shape *shape,
-                     Plan *p) {
+                     Plan *p, bool dual = false) {
   if (kernel < 0 || kernel > 2 || precision < 0 || precision > 1) return F3D_ERR_ARG;
   if (ns < 0 || nt < 0) return F3D_ERR_SHAPE;
   int tpt = shape && shape->tpt ? shape->tpt : 0;
@@ -468,17 +513,18 @@ static int make_plan(int kernel, int precision, int64_t ns, int64_t nt, const f3
   p->off_counters = off;
   if (p->nsplit > 1 || precision == F3D_FP32C) off += kCounterBytes;
   p->off_partial = off;
-  if (p->nsplit > 1) off += round_up(static_cast<size_t>(p->nsplit) * nt * 3 * sizeof(double), 256);
+  if (p->nsplit > 1)
+    off += round_up(static_cast<size_t>(p->nsplit) * nt * 3 * sizeof(double) * (dual ? 2 : 1), 256);
   p->off_packed = off;
   if (precision == F3D_FP32C) off += round_up(static_cast<size_t>(ns) * 12 * sizeof(float), 256);
   p->bytes = off;
   return F3D_OK;
 }
 
-template <int KIND, int MODE, int PREC, int TPT, int SL>
+template <int KIND, int MODE, int PREC, int TPT, int SL, bool DUAL = false>
 static int launch_one(const PairArgs &a, int64_t ntb, int nsplit, cudaStream_t st) {
-  constexpr size_t smem = pair_smem_bytes<KIND, MODE, PREC>();
-  auto kfn = pair_kernel<KIND, MODE, PREC, TPT, SL>;
+  constexpr size_t smem = pair_smem_bytes<KIND, MODE, PREC, DUAL>();
+  auto kfn = pair_kernel<KIND, MODE, PREC, TPT, SL, DUAL>;
   static bool attr_set[64] = {false};
   int dev = 0;
   cudaGetDevice(&dev);
@@ -493,12 +539,12 @@ static int launch_one(const PairArgs &a, int64_t ntb, int nsplit, cudaStream_t s
   return launch_status();
 }
 
-template <int KIND, int MODE, int PREC>
+template <int KIND, int MODE, int PREC, bool DUAL = false>
 static int dispatch_shape(const PairArgs &a, const Plan &p, cudaStream_t st) {
-  if (p.sl == 1 && p.tpt == 1) return launch_one<KIND, MODE, PREC, 1, 1>(a, p.ntb, p.nsplit, st);
-  if (p.sl == 1 && p.tpt == 2) return launch_one<KIND, MODE, PREC, 2, 1>(a, p.ntb, p.nsplit, st);
-  if (p.sl == 8) return launch_one<KIND, MODE, PREC, 1, 8>(a, p.ntb, p.nsplit, st);
-  return launch_one<KIND, MODE, PREC, 1, 32>(a, p.ntb, p.nsplit, st);
+  if (p.sl == 1 && p.tpt == 1) return launch_one<KIND, MODE, PREC, 1, 1, DUAL>(a, p.ntb, p.nsplit, st);
+  if (p.sl == 1 && p.tpt == 2) return launch_one<KIND, MODE, PREC, 2, 1, DUAL>(a, p.ntb, p.nsplit, st);
+  if (p.sl == 8) return launch_one<KIND, MODE, PREC, 1, 8, DUAL>(a, p.ntb, p.nsplit, st);
+  return launch_one<KIND, MODE, PREC, 1, 32, DUAL>(a, p.ntb, p.nsplit, st);
 }
 
 template <int KIND, int PREC>
@@ -517,13 +563,18 @@ static int dispatch_prec(int prec, int mode, const PairArgs &a, const Plan &p, c
   return dispatch_mode<KIND, F3D_FP32C>(mode, a, p, st);
 }
 
-int pair_sum_impl(int kernel, int precision, int self_mode, const double *rs, const double *rt,
-                  const double *dens, const double *nrm, const int32_t *gs, const int32_t *gt,
-                  double *out, int64_t ns, int64_t nt, double eta, double reg, double eps,
-                  int accumulate, const f3d_pair_shape *shape, void *ws, size_t ws_bytes,
-                  cudaStream_t st) {
+// One sum, or with dens2/out2 the dual FP64 Oseen sum (both outputs from
+// one pass over the pairs).
+static int pair_sum_core(int kernel, int precision, int self_mode, const double *rs,
+                         const double *rt, const double *dens, const double *nrm,
+                         const int32_t *gs, const int32_t *gt, double *out, int64_t ns,
+                         int64_t nt, double eta, double reg, double eps, int accumulate,
+                         const f3d_pair_shape *shape, void *ws, size_t ws_bytes, cudaStream_t st,
+                         const double *dens2, double *out2) {
+  const bool dual = out2 != nullptr;
+  if (dual && (kernel != F3D_KERNEL_OSEEN || precision != F3D_FP64)) return F3D_ERR_ARG;
   Plan p;
-  int rc = make_plan(kernel, precision, ns, nt, shape, &p);
+  int rc = make_plan(kernel, precision, ns, nt, shape, &p, dual);
   if (rc) return rc;
   if (self_mode < 0 || self_mode > 2) return F3D_ERR_ARG;
   if (nt == 0) return F3D_OK;
@@ -535,8 +586,13 @@ int pair_sum_impl(int kernel, int precision, int self_mode, const double *rs, co
   if (!aligned(rs, 8) || !aligned(rt, 8) || !aligned(dens, 8) || !aligned(nrm, 8) ||
       !aligned(out, 8) || !aligned(gs, 4) || !aligned(gt, 4))
     return F3D_ERR_ALIGN;
+  if (dual && (!out2 || (ns > 0 && !dens2))) return F3D_ERR_NULL;
+  if (dual && (!aligned(out2, 8) || !aligned(dens2, 8))) return F3D_ERR_ALIGN;
   if (ns == 0) {
     if (!accumulate && cudaMemsetAsync(out, 0, static_cast<size_t>(nt) * 3 * sizeof(double), st) != cudaSuccess)
+      return F3D_ERR_CUDA;
+    if (dual && !accumulate &&
+        cudaMemsetAsync(out2, 0, static_cast<size_t>(nt) * 3 * sizeof(double), st) != cudaSuccess)
       return F3D_ERR_CUDA;
     return F3D_OK;
   }
@@ -548,6 +604,8 @@ int pair_sum_impl(int kernel, int precision, int self_mode, const double *rs, co
   a.rs = rs; a.rt = rt; a.dens = dens; a.nrm = nrm;
   a.gs = gs; a.gt = gt;
   a.out = out;
+  a.dens2 = dens2;
+  a.out2 = out2;
   a.partial = p.nsplit > 1 ? reinterpret_cast<double *>(w + p.off_partial) : nullptr;
   a.counters = p.nsplit > 1 ? reinterpret_cast<unsigned *>(w + p.off_counters) : nullptr;
   a.packed = precision == F3D_FP32C ? reinterpret_cast<float *>(w + p.off_packed) : nullptr;
@@ -562,7 +620,8 @@ int pair_sum_impl(int kernel, int precision, int self_mode, const double *rs, co
   // Bulk copies need 16-byte aligned sources; otherwise stage with plain loads.
   a.use_tma = p.use_tma;
   if (precision == F3D_FP64 && (!aligned(rs, 16) || !aligned(dens, 16) ||
-                                (kernel == F3D_KERNEL_STRESSLET && !aligned(nrm, 16))))
+                                (kernel == F3D_KERNEL_STRESSLET && !aligned(nrm, 16)) ||
+                                (dual && !aligned(dens2, 16))))
     a.use_tma = 0;
   if (self_mode == F3D_SELF_SKIP_GROUP && !aligned(gs, 16)) a.use_tma = 0;
 
@@ -572,11 +631,30 @@ int pair_sum_impl(int kernel, int precision, int self_mode, const double *rs, co
         rs, dens, kernel == F3D_KERNEL_STRESSLET ? nrm : nullptr, const_cast<float *>(a.packed), ns);
     if ((rc = launch_status())) return rc;
   }
+  if (dual) {
+    switch (self_mode) {
+      case F3D_SELF_REGULARISE:
+        return dispatch_shape<F3D_KERNEL_OSEEN, F3D_SELF_REGULARISE, F3D_FP64, true>(a, p, st);
+      case F3D_SELF_SKIP_INDEX:
+        return dispatch_shape<F3D_KERNEL_OSEEN, F3D_SELF_SKIP_INDEX, F3D_FP64, true>(a, p, st);
+      default:
+        return dispatch_shape<F3D_KERNEL_OSEEN, F3D_SELF_SKIP_GROUP, F3D_FP64, true>(a, p, st);
+    }
+  }
   switch (kernel) {
     case F3D_KERNEL_OSEEN: return dispatch_prec<F3D_KERNEL_OSEEN>(precision, self_mode, a, p, st);
     case F3D_KERNEL_STRESSLET: return dispatch_prec<F3D_KERNEL_STRESSLET>(precision, self_mode, a, p, st);
     default: return dispatch_prec<F3D_KERNEL_ROTLET>(precision, self_mode, a, p, st);
   }
+}
+
+int pair_sum_impl(int kernel, int precision, int self_mode, const double *rs, const double *rt,
+                  const double *dens, const double *nrm, const int32_t *gs, const int32_t *gt,
+                  double *out, int64_t ns, int64_t nt, double eta, double reg, double eps,
+                  int accumulate, const f3d_pair_shape *shape, void *ws, size_t ws_bytes,
+                  cudaStream_t st) {
+  return pair_sum_core(kernel, precision, self_mode, rs, rt, dens, nrm, gs, gt, out, ns, nt, eta,
+                       reg, eps, accumulate, shape, ws, ws_bytes, st, nullptr, nullptr);
 }
 
 }  // namespace f3d
@@ -655,6 +733,29 @@ int f3d_stresslet_times_normal_times_density(const double *r_vectors, const doub
                             r_vectors, density, normal, nullptr, nullptr, v, n, n, eta, reg,
                             epsilon_distance, 0, nullptr, workspace, workspace_bytes,
                             static_cast<cudaStream_t>(stream));
+}
+
+int f3d_oseen_dual_workspace_bytes(int64_t ns, int64_t nt, const f3d_pair_shape *shape,
+                                   size_t *bytes) {
+  if (!bytes) return F3D_ERR_NULL;
+  f3d::Plan p;
+  int rc = f3d::make_plan(F3D_KERNEL_OSEEN, F3D_FP64, ns, nt, shape, &p, true);
+  if (rc) return rc;
+  *bytes = p.bytes;
+  return F3D_OK;
+}
+
+int f3d_oseen_dual(int self_mode, const double *r_source, const double *r_target,
+                   const double *density, const double *density2, const int32_t *src_group,
+                   const int32_t *trg_group, double *out, double *out2, int64_t ns, int64_t nt,
+                   double eta, double reg, double epsilon_distance, int accumulate,
+                   const f3d_pair_shape *shape, void *workspace, size_t workspace_bytes,
+                   void *stream) {
+  if (!out2) return F3D_ERR_NULL;
+  return f3d::pair_sum_core(F3D_KERNEL_OSEEN, F3D_FP64, self_mode, r_source, r_target, density, nullptr,
+                            src_group, trg_group, out, ns, nt, eta, reg, epsilon_distance, accumulate,
+                            shape, workspace, workspace_bytes, static_cast<cudaStream_t>(stream),
+                            density2, out2);
 }
 
 }  // extern "C"

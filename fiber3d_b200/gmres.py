@@ -142,7 +142,8 @@ class DeviceGMRES:
 
     # ------------------------------------------------------------- solve ---
     def solve(self, matvec, pc, b: torch.Tensor, x0: torch.Tensor | None = None, rtol=1e-8,
-              maxiter=200, use_graph=True, key="default", bnorm=None, verify=True, aux=None):
+              maxiter=200, use_graph=True, key="default", bnorm=None, verify=True, aux=None,
+              r0: torch.Tensor | None = None):
         """Solve A x = b with right preconditioner pc = P^-1.
 
         Returns (x, info, iterations, history of relative residual estimates).
@@ -152,6 +153,7 @@ class DeviceGMRES:
         result itself, as the mixed-precision refinement does).  With `aux`,
         ``self.last_aux_sum`` is set to sum_j |y_j| |aux after A z_j| over the
         correction x - x0 = sum_j y_j z_j (an error bound's ingredient).
+        `r0` (optional) is b - A x0, already computed by the caller.
         """
         self.last_aux_sum = 0.0
         n, m = self.n, self.m
@@ -171,6 +173,8 @@ class DeviceGMRES:
             # r = b - A x
             if x0 is None and its == 0:
                 r.copy_(b)
+            elif r0 is not None and its == 0:
+                r.copy_(r0)
             else:
                 matvec(x, tmp)
                 torch.sub(b, tmp, out=r)
@@ -247,10 +251,19 @@ def solve_system(system, tol=1e-8, restart=100, maxiter=200, x0=None, mixed=Fals
         system._gmres = g
     b = system.rhs
     t0 = time.perf_counter()
+    # the Oseen flow of x0's fiber forces may already be summed (update(x0))
+    pending = x0 is not None and hasattr(system, "pending_oseen") and system.pending_oseen(x0)
+    if hasattr(system, "_pending_x0"):
+        system._pending_x0 = None
     if not mixed:
+        r0 = None
+        if pending:
+            r0 = torch.empty_like(b)
+            system.matvec(x0, r0, "fp64", oseen_done=True)
+            torch.sub(b, r0, out=r0)
         x, info, its, hist = g.solve(lambda a, o: system.matvec(a, o, "fp64"),
                                      lambda a, o: system.pc(a, o, "fp64"), b, x0=x0, rtol=tol,
-                                     maxiter=maxiter, use_graph=use_graph, key="fp64")
+                                     maxiter=maxiter, use_graph=use_graph, key="fp64", r0=r0)
         torch.cuda.synchronize()
         return {"x": x, "info": info, "iterations": its, "history": hist, "refinements": 0,
                 "seconds": time.perf_counter() - t0}
@@ -277,14 +290,14 @@ def solve_system(system, tol=1e-8, restart=100, maxiter=200, x0=None, mixed=Fals
         elif x0 is None and ref == 0:
             r.copy_(b)
         else:
-            system.matvec(x, tmp, outer)
+            system.matvec(x, tmp, outer, oseen_done=pending and ref == 0)
             if outer == "fp32c":
                 g._norm(system.v, g.beta)
                 bound = eps_v * float(g.beta.item()) / bnorm
                 if bound > 0.5 * tol:
                     outer, bound = "fp64", 0.0
                     system._outer_fp64 = True
-                    system.matvec(x, tmp, outer)
+                    system.matvec(x, tmp, outer, oseen_done=pending and ref == 0)
             if outer == "fp64":
                 fp64_residuals += 1
             torch.sub(b, tmp, out=r)

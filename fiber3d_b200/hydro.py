@@ -355,6 +355,13 @@ class HydroSystem:
         # ---- work buffers
         self.v = torch.zeros(3 * self.ntrg, dtype=torch.float64, device=dev)
         self.fw = torch.zeros((max(nF, 1), 3), dtype=torch.float64, device=dev)
+        # the fiber forces of a guess x0 and their Oseen flow, summed in the
+        # same pass as the explicit flow (update(x0)); used by the solve's
+        # first residual
+        self.fw2 = torch.zeros((max(nF, 1), 3), dtype=torch.float64, device=dev)
+        self.v2 = torch.zeros(3 * self.ntrg, dtype=torch.float64, device=dev)
+        self._pending_x0 = None
+        self._dual_ws = None
         self.scratch = torch.zeros(4, dtype=torch.float64, device=dev)
         self.oseen = _PairCall("oseen", "skip_group", self.x_fib, self.trg, self.fw, None, self.src_grp,
                                self.trg_grp, self.v, P.eta, P.reg, P.eps_dist) if nF else None
@@ -470,21 +477,27 @@ class HydroSystem:
                       _lib.ptr(origin), _lib.ptr(A), n, 3 * n + 6, P.eta, P.reg, P.eps_dist, st)
             self.body_inv.append(torch.linalg.inv(A))
 
-    def update(self):
+    def update(self, x0: torch.Tensor | None = None):
         """Recompute everything that depends on the current geometry (fiber
         derivatives, body surfaces and singularity vectors, explicit flows,
         right-hand side, fiber/body blocks and their LU) in place, so that
-        device pointers — and CUDA graphs captured on them — stay valid."""
+        device pointers — and CUDA graphs captured on them — stay valid.
+
+        With the initial guess `x0` of the coming solve, the Oseen flow of
+        x0's fiber forces is summed in the same pass over the fiber pairs as
+        the explicit flow of the external forces (``f3d_oseen_dual``); a
+        :meth:`solve` given this same tensor, unmodified, starts from it
+        instead of a fresh Oseen sum (the residual is bit-for-bit the same)."""
         st = _lib.stream_handle(self.device)
         if self.nF:
             _lib.call("f3d_fiber_geometry", ctypes.byref(self.fs.c), _lib.ptr(self.x_fib), _lib.ptr(self.geo),
                       self.nF, st)
-        self._assemble()
+        self._assemble(x0)
 
-    def advance(self, sol: torch.Tensor):
+    def advance(self, sol: torch.Tensor, x0: torch.Tensor | None = None):
         """Move the geometry one step with solution `sol` (tstep.py:1392-1407:
         fibers take their new positions; bodies x += dt U and
-        q <- q(Omega dt) q), then :meth:`update`."""
+        q <- q(Omega dt) q), then :meth:`update` (with the next guess x0)."""
         dt = self.p.dt
         o = self.o_fib
         for n in sorted(set(int(v) for v in self.fs.npts)):
@@ -507,7 +520,7 @@ class HydroSystem:
                 self.body_loc[k] = self.body_loc[k] + dt * vel[k, :3]
                 self.body_quat[k] = quaternion_multiply(quaternion_from_rotation(vel[k, 3:] * dt), self.body_quat[k])
             self._load_bodies()
-        self.update()
+        self.update(x0)
 
     # ------------------------------------------------------------------------
     def autotune(self):
@@ -523,7 +536,28 @@ class HydroSystem:
                               reg=P.reg, epsilon_distance=P.eps_dist)
                 call.set_shape(prec, shp)
 
-    def _assemble(self):
+    def _oseen_dual(self):
+        """v = Oseen flow of fw (external forces), v2 = that of fw2, one pass;
+        the FP64 Oseen call's launch shape, so that each equals its single
+        sum bit for bit."""
+        a = self.oseen.args
+        shp = self.oseen.shape.get("fp64")
+        nb = ctypes.c_size_t(0)
+        _lib.call("f3d_oseen_dual_workspace_bytes", a["src"].shape[0], a["trg"].shape[0],
+                  ctypes.byref(shp) if shp else None, ctypes.byref(nb))
+        if self._dual_ws is None or self._dual_ws.numel() < nb.value:
+            self._dual_ws = torch.zeros(max(nb.value, 256), dtype=torch.uint8, device=self.device)
+        _lib.call("f3d_oseen_dual", _lib.SELF_MODE[a["mode"]], _lib.ptr(a["src"]), _lib.ptr(a["trg"]),
+                  _lib.ptr(self.fw), _lib.ptr(self.fw2), _lib.ptr(a["gs"]), _lib.ptr(a["gt"]), _lib.ptr(self.v),
+                  _lib.ptr(self.v2), a["src"].shape[0], a["trg"].shape[0], a["eta"], a["reg"], a["eps"], 0,
+                  ctypes.byref(shp) if shp else None, _lib.ptr(self._dual_ws), self._dual_ws.numel(),
+                  _lib.stream_handle(self.device))
+
+    def pending_oseen(self, x: torch.Tensor) -> bool:
+        """Whether update() already summed the Oseen flow of x's fiber forces."""
+        return self._pending_x0 is not None and x is self._pending_x0
+
+    def _assemble(self, x0=None):
         P = self.p
         dev = self.device
         st = _lib.stream_handle(dev)
@@ -531,9 +565,16 @@ class HydroSystem:
         # explicit flow of the external fiber forces (tstep.py:789-821)
         self.timers.start("fiber2all_explicit_interactions")
         self.v.zero_()
+        self._pending_x0 = None
         if nF and self.has_force:
             _lib.call("f3d_fiber_weight", ctypes.byref(self.fs.c), _lib.ptr(self.force), _lib.ptr(self.fw), nF, st)
-            self.oseen("fp64")
+            if x0 is not None:
+                _lib.call("f3d_fiber_forces", ctypes.byref(self.fs.c), P.E, _lib.ptr(self.geo),
+                          _lib.ptr(x0[self.o_fib:]), _lib.ptr(self.fw2), nF, 1, st)
+                self._oseen_dual()
+                self._pending_x0 = x0
+            else:
+                self.oseen("fp64")
         self.timers.stop("fiber2all_explicit_interactions")
         v = self.v.view(-1, 3)
         if nF:
@@ -565,16 +606,22 @@ class HydroSystem:
             self._pc_age += 1
 
     # ------------------------------------------------------------------------
-    def matvec(self, x: torch.Tensor, y: torch.Tensor, precision: str = "fp64") -> torch.Tensor:
-        """y = A x (tstep.py:1003-1178)."""
+    def matvec(self, x: torch.Tensor, y: torch.Tensor, precision: str = "fp64",
+               oseen_done: bool = False) -> torch.Tensor:
+        """y = A x (tstep.py:1003-1178).  With `oseen_done` the FP64 Oseen
+        flow of x's fiber forces is the one update(x) summed (see
+        :meth:`pending_oseen`)."""
         st = _lib.stream_handle(self.device)
         nF, nB, nS = self.nF, self.nB, self.nS
         XT = x[self.o_fib:]
         first = True
         if nF:
-            _lib.call("f3d_fiber_forces", ctypes.byref(self.fs.c), self.p.E, _lib.ptr(self.geo), _lib.ptr(XT),
-                      _lib.ptr(self.fw), nF, 1, st)
-            self.oseen(precision, accumulate=False)
+            if oseen_done:
+                self.v.copy_(self.v2)
+            else:
+                _lib.call("f3d_fiber_forces", ctypes.byref(self.fs.c), self.p.E, _lib.ptr(self.geo),
+                          _lib.ptr(XT), _lib.ptr(self.fw), nF, 1, st)
+                self.oseen(precision, accumulate=False)
             first = False
         if self.nstress:
             _lib.call("f3d_gather_segments", _lib.ptr(x), _lib.ptr(self.stress_dens), _lib.ptr(self.seg[0]),

@@ -407,8 +407,9 @@ def march(system, steps: int, guess: str = "zero", net: LearnedWarmStart | None 
     stats, feats, targs = [], [], []
     can_learn = learnable(system)
     for s in range(steps):
-        if s > 0:
-            system.advance(history[-1])
+        # the guess depends only on the previous solutions, so it is formed
+        # before the geometry moves and handed to advance() (which then sums
+        # its Oseen flow together with the explicit flow)
         x_q = extrapolate(history)
         f = None
         if can_learn and len(history) >= HISTORY and record and s >= record_from:
@@ -421,6 +422,8 @@ def march(system, steps: int, guess: str = "zero", net: LearnedWarmStart | None 
             x0 = net.guess(system, history)
         else:
             x0 = x_q
+        if s > 0:
+            system.advance(history[-1], x0=x0)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
         res = system.solve(tol=tol, restart=restart, x0=x0, mixed=mixed)

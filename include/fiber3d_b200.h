@@ -129,6 +129,24 @@ int f3d_pair_sum_noalloc(int kernel, int precision, int self_mode,
                          double eta, double reg, double epsilon_distance,
                          int accumulate, void *stream);
 
+/* Two FP64 Oseen sums over the same sources, targets and self mode, with
+   densities `density` -> `out` and `density2` -> `out2`, in one pass: each
+   output carries exactly the arithmetic of f3d_pair_sum (F3D_KERNEL_OSEEN,
+   F3D_FP64) with that density, the pair geometry being computed once.  No
+   counterpart function in fiber3d; it evaluates in one pass the two Oseen
+   sums a time step makes over the same fibers -- the explicit flow of the
+   external forces (tstep.py:789-821) and the fiber forces of GMRES's initial
+   guess in the first matvec (tstep.py:1003-1178).  Workspace from
+   f3d_oseen_dual_workspace_bytes. */
+int f3d_oseen_dual_workspace_bytes(int64_t ns, int64_t nt, const f3d_pair_shape *shape,
+                                   size_t *bytes);
+int f3d_oseen_dual(int self_mode, const double *r_source, const double *r_target,
+                   const double *density, const double *density2, const int32_t *src_group,
+                   const int32_t *trg_group, double *out, double *out2, int64_t ns, int64_t nt,
+                   double eta, double reg, double epsilon_distance, int accumulate,
+                   const f3d_pair_shape *shape, void *workspace, size_t workspace_bytes,
+                   void *stream);
+
 /* Named wrappers with the meaning of the fiber3d functions they replace. */
 
 /* replaces oseen_kernel_source_target_numba, python/kernels/kernels.py:794-846 */

@@ -178,6 +178,25 @@ def test_norm_of_vectors_of_any_length(system):
         assert abs(float(beta) - float(torch.linalg.vector_norm(w))) <= 1e-14 * float(torch.linalg.vector_norm(w))
 
 
+@pytest.mark.parametrize("mixed", [False, True])
+def test_guess_flow_summed_in_update(golden_step, mixed):
+    """update(x0) sums the Oseen flow of the guess with the explicit flow in
+    one pass; the solve that starts from it returns exactly what it returns
+    when it sums that flow itself."""
+    from fiber3d_b200.hydro import HydroSystem
+    P = problem_from_golden(golden_step)
+    a, b = HydroSystem(P), HydroSystem(P)
+    x0 = torch.tensor(golden_step["probe_x"][0], device="cuda") * 1e-3 + torch.tensor(golden_step["sol"],
+                                                                                     device="cuda")
+    a.update(x0)
+    assert a.pending_oseen(x0)
+    assert torch.equal(a.rhs, b.rhs)
+    ra = a.solve(tol=1e-10, x0=x0, mixed=mixed)
+    rb = b.solve(tol=1e-10, x0=x0, mixed=mixed)
+    assert not a.pending_oseen(x0)
+    assert torch.equal(ra["x"], rb["x"]) and ra["iterations"] == rb["iterations"]
+
+
 def test_graph_and_eager_agree(system):
     a = system.solve(tol=1e-9, use_graph=False)["x"]
     b = system.solve(tol=1e-9, use_graph=True)["x"]

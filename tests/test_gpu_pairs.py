@@ -251,3 +251,33 @@ def test_fp32c_single_split_keeps_shared_counters(K, L):
         u = K.pair_sum("stresslet", x, y, d, n, precision="fp32c",
                        shape=L.PairShape(2, 1, 5, 0)).cpu().numpy()
         assert rel_err(u, ref) < TOL32
+
+
+@pytest.mark.parametrize("shape", [(1, 1, 0, 0), (2, 1, 5, -1), (1, 8, 3, 0), (1, 32, 0, -1), (2, 1, 1, 0)])
+@pytest.mark.parametrize("mode", ["regularise", "skip_group"])
+def test_oseen_dual_equals_two_sums(L, shape, mode):
+    """f3d_oseen_dual gives, bit for bit, the two FP64 Oseen sums it fuses."""
+    import ctypes
+    import torch
+    from fiber3d_b200 import kernels as K
+    rng = np.random.default_rng(41)
+    xs = torch.tensor(rng.random((2000, 3)) * 4.0, device="cuda")
+    xt = torch.tensor(rng.random((1500, 3)) * 4.0, device="cuda")
+    d1 = torch.tensor(rng.normal(size=(2000, 3)), device="cuda")
+    d2 = torch.tensor(rng.normal(size=(2000, 3)), device="cuda")
+    gs = torch.tensor(np.arange(2000) // 20, dtype=torch.int32, device="cuda")
+    gt = torch.tensor(np.arange(1500) // 20, dtype=torch.int32, device="cuda")
+    kw = dict(self_mode=mode, src_group=gs, trg_group=gt) if mode == "skip_group" else {}
+    shp = L.PairShape(*shape)
+    r1 = K.pair_sum("oseen", xs, xt, d1, shape=shp, **kw).clone()
+    r2 = K.pair_sum("oseen", xs, xt, d2, shape=shp, **kw).clone()
+    nb = ctypes.c_size_t(0)
+    L.call("f3d_oseen_dual_workspace_bytes", 2000, 1500, ctypes.byref(shp), ctypes.byref(nb))
+    ws = torch.zeros(max(nb.value, 256), dtype=torch.uint8, device="cuda")
+    o1 = torch.empty_like(r1)
+    o2 = torch.empty_like(r2)
+    for _ in range(2):  # the split counters return to zero between calls
+        L.call("f3d_oseen_dual", L.SELF_MODE[mode], L.ptr(xs), L.ptr(xt), L.ptr(d1), L.ptr(d2), L.ptr(gs),
+               L.ptr(gt), L.ptr(o1), L.ptr(o2), 2000, 1500, 1.0, 5e-3, 1e-5, 0, ctypes.byref(shp), L.ptr(ws),
+               ws.numel(), L.stream_handle())
+        assert torch.equal(o1, r1) and torch.equal(o2, r2)
