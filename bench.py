@@ -42,10 +42,8 @@ L2_FLUSH_BYTES = 256 << 20
 
 # ------------------------------------------------------------------ setup --
 def dist_info():
-    rank = int(os.environ.get("RANK", "0"))
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    return rank, world, local
+    from fiber3d_b200 import replicas
+    return replicas.rank_info()
 
 
 def make_workload(name: str):
@@ -166,8 +164,8 @@ def measured_peak(L, precision: str, torch):
 
 def gpu_arm(args, rank, world, local):
     import torch
-    import torch.distributed as dist
     from fiber3d_b200 import _lib as L
+    from fiber3d_b200 import replicas
     from fiber3d_b200 import kernels as K
 
     torch.cuda.set_device(local)
@@ -193,8 +191,7 @@ def gpu_arm(args, rank, world, local):
         for _ in range(warmup):
             step(precision)
         torch.cuda.synchronize()
-        if world > 1:
-            dist.barrier()
+        replicas.barrier()
         torch.cuda.synchronize()
         evs = []
         for _ in range(steps):
@@ -207,8 +204,7 @@ def gpu_arm(args, rank, world, local):
             torch.cuda.nvtx.range_pop()
             evs.append((e0, e1))
         torch.cuda.synchronize()
-        if world > 1:
-            dist.barrier()
+        replicas.barrier()
         times = [a.elapsed_time(b) for a, b in evs]
         return times
 
@@ -217,14 +213,10 @@ def gpu_arm(args, rank, world, local):
     with ClockSampler(local) as clk:
         t_ms = timed("fp64", args.steps, args.warmup)
     clocks = clk.summary()
-    total_ms = sum(t_ms)
-    if world > 1:
-        t = torch.tensor([total_ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = t.item()
+    total_ms, = replicas.max_over_ranks([sum(t_ms)], dev)
     ms_step = total_ms / args.steps
     pairs = wl["pairs"]
-    value = pairs * args.steps * world / (total_ms * 1e-3)
+    value = replicas.aggregate_rate(pairs, args.steps, world, total_ms)
 
     # the timed launches' output against the library-default launch shape
     timed_out = out.clone()
@@ -259,12 +251,8 @@ def gpu_arm(args, rank, world, local):
         d2h = e2e_step()
     e1.record()
     e1.synchronize()
-    e2e_ms = e0.elapsed_time(e1)
-    if world > 1:
-        t = torch.tensor([e2e_ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = t.item()
-    e2e_value = pairs * args.steps * world / (e2e_ms * 1e-3)
+    e2e_ms, = replicas.max_over_ranks([e0.elapsed_time(e1)], dev)
+    e2e_value = replicas.aggregate_rate(pairs, args.steps, world, e2e_ms)
 
     flop_pair = FLOP_PER_PAIR[kind]
     achieved = flop_pair * pairs / (min(t_ms) * 1e-3)
@@ -390,12 +378,13 @@ def hydro_arm(args, rank, world, local, warmup=None, steps=None, emit=True):
     the dense shell operator) is per-run set-up, as in fiber3d's
     tstep.__init__, and is excluded."""
     import torch
-    from fiber3d_b200 import geometry, hydro as H
+    from fiber3d_b200 import geometry, hydro as H, replicas
     warmup = args.warmup if warmup is None else warmup
     steps = args.steps if steps is None else steps
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
-    P = geometry.hydro_step_problem(seed=3, nshell=args.nshell, nfib=args.nfib)
+    P = geometry.hydro_step_problem(seed=3, nshell=args.nshell, nfib=args.nfib, shell_radius=args.shell_radius,
+        fiber_ball=args.fiber_ball, body_shell=args.body_shell)
     t0 = time.perf_counter()
     shell = H.ShellOperator(P.shell, P.eta, P.reg, P.eps_dist, dev)
     torch.cuda.synchronize()
@@ -409,7 +398,9 @@ def hydro_arm(args, rank, world, local, warmup=None, steps=None, emit=True):
     t0 = time.perf_counter()
     feats, targs = [], []
     for seed in args.train_seeds:
-        Pt = geometry.hydro_step_problem(seed=seed, nshell=args.nshell, nfib=args.nfib)
+        Pt = geometry.hydro_step_problem(seed=seed, nshell=args.nshell, nfib=args.nfib,
+                                         shell_radius=args.shell_radius,
+        fiber_ball=args.fiber_ball, body_shell=args.body_shell)
         st_ = H.HydroSystem(Pt, shell_op=shell, device=dev)
         _, Xf, Tf = W.march(st_, args.train_steps, guess="extrapolate", record=True,
                             record_from=args.train_skip)
@@ -421,7 +412,9 @@ def hydro_arm(args, rank, world, local, warmup=None, steps=None, emit=True):
     hist = net.fit(X_train, T_train, epochs=args.train_epochs, batch=1024, lr=1e-3)
     # correction factors chosen by GMRES iterations on held-out trajectories
     val_seeds = [max(args.train_seeds) + 1, max(args.train_seeds) + 2]
-    Pvs = [geometry.hydro_step_problem(seed=sd, nshell=args.nshell, nfib=args.nfib) for sd in val_seeds]
+    Pvs = [geometry.hydro_step_problem(seed=sd, nshell=args.nshell, nfib=args.nfib,
+                                       shell_radius=args.shell_radius,
+        fiber_ball=args.fiber_ball, body_shell=args.body_shell) for sd in val_seeds]
     sel = net.select_scale(lambda: [H.HydroSystem(Pv, shell_op=shell, device=dev) for Pv in Pvs],
                            args.train_steps, count_from=args.train_skip)
     torch.cuda.synchronize()
@@ -437,6 +430,8 @@ def hydro_arm(args, rank, world, local, warmup=None, steps=None, emit=True):
              "learned_mixed_pc4": ("learned", True, 4)}
     for mode, (guess, mixed, pc_refresh) in modes.items():
         sysd = H.HydroSystem(P, shell_op=shell, device=dev, tune=True, pc_refresh=pc_refresh)
+        torch.cuda.synchronize()
+        replicas.barrier()
         history = []
         times, its, resid, phases, r0s, worst = [], [], [], [], [], []
         for step in range(warmup + steps):
@@ -493,6 +488,10 @@ def hydro_arm(args, rank, world, local, warmup=None, steps=None, emit=True):
                      "initial_rel_residual": r0s, "long_solves": worst,
                      "phases_ms": {k: statistics.median([p.get(k, 0.0) for p in phases]) for k in phases[0]}}
         del sysd
+    # each replica's median step; the job's is the slowest replica's
+    slowest = replicas.max_over_ranks([out[m]["ms_per_step"] for m in modes], dev)
+    for mode, ms in zip(modes, slowest):
+        out[mode]["ms_per_step"] = ms
     for mode in modes:
         out[mode]["rel_err_vs_fp64_1e-12_solve"] = xs[mode]
         out[mode]["speedup_vs_fp64"] = out["fp64"]["ms_per_step"] / out[mode]["ms_per_step"]
@@ -502,6 +501,8 @@ def hydro_arm(args, rank, world, local, warmup=None, steps=None, emit=True):
             "higher_is_better": False, "dtype": "f64", "data": "synthetic (seeded)",
             "config": {"workload": "hydro_step", "fibers": args.nfib, "points_per_fiber": 32,
                        "bodies": 4, "body_nodes": 400, "shell_nodes": args.nshell,
+                       "shell_radius": args.shell_radius, "fiber_ball": args.fiber_ball,
+                       "body_shell": args.body_shell,
                        "system_size": int(3 * args.nshell + 4 * 1206 + 4 * 32 * args.nfib),
                        "shell_setup_s": setup_s}, "step": out}
     if rank == 0 and emit:
@@ -519,7 +520,7 @@ def block_pc_arm(args, rank, world, local):
     fiber3d makes (tstep_utils.py:1405-1419, tstep.py:985-988)."""
     import torch
     import scipy.linalg as sla
-    from fiber3d_b200 import geometry, hydro as H
+    from fiber3d_b200 import geometry, hydro as H, replicas
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
     rng = np.random.default_rng(4)
@@ -553,13 +554,15 @@ def block_pc_arm(args, rank, world, local):
     for _ in range(args.warmup):
         g.replay()
     torch.cuda.synchronize()
+    replicas.barrier()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record()
     for _ in range(args.steps):
         g.replay()
     e1.record()
     e1.synchronize()
-    ms = e0.elapsed_time(e1) / args.steps
+    replicas.barrier()
+    ms, = replicas.max_over_ranks([e0.elapsed_time(e1) / args.steps], dev)
     # parity and CPU baseline on the same blocks
     A_h = A0.cpu().numpy()
     rhs_h = rhs.cpu().numpy()
@@ -608,6 +611,9 @@ def main():
                     help="steps at the start of each trajectory left out of training and selection")
     ap.add_argument("--nshell", type=int, default=12000)
     ap.add_argument("--nfib", type=int, default=512)
+    ap.add_argument("--shell-radius", type=float, default=10.0)
+    ap.add_argument("--fiber-ball", type=float, default=5.0, help="radius of the ball holding the fiber centres")
+    ap.add_argument("--body-shell", type=float, default=7.5, help="distance of the body centres from the origin")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-step", action="store_true",
                     help="pair throughput only (skip the embedded time-step comparison)")

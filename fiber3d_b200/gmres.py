@@ -30,7 +30,10 @@ most ``e = FP32C_PAIR_REL_ERR * G * |v| / |b|`` (relative).  The solve stops whe
 ``|r| / |b| + e <= tol``, which bounds the FP64 residual by tol as well;
 while ``e <= tol / 2`` the residual stays FP32C, otherwise it is recomputed
 in FP64 (and stays FP64 for the rest of the solve and for later solves of
-the same system, whose |v| / |b| changes little from step to step).  After an inner solve
+the same system, whose |v| / |b| changes little from step to step).  When update(x0) already
+summed the Oseen flow of the guess in FP64 (the dual pass), the first
+residual adds only the stresslet flow in FP32C, and e counts only that part
+of v.  After an inner solve
 the new residual is bounded without a matvec: by the inner GMRES estimate
 ``|r - A32 d|`` plus e (0 for an FP64 residual) plus
 ``FP32C_PAIR_REL_ERR * G * sum_j |y_j| |v(z_j)|``
@@ -289,6 +292,18 @@ def solve_system(system, tol=1e-8, restart=100, maxiter=200, x0=None, mixed=Fals
             rel, bound = known
         elif x0 is None and ref == 0:
             r.copy_(b)
+        elif pending and ref == 0 and not getattr(system, "_stress_fp64", False):
+            # the Oseen flow of x0 is FP64 already (update(x0)); the stresslet
+            # part in FP32C is bounded by its own flow: eps_v |v - v_oseen|
+            system.matvec(x, tmp, "fp32c", oseen_done=True)
+            g._norm(system.v - system.v2, g.beta)
+            bound = eps_v * float(g.beta.item()) / bnorm
+            if bound > 0.5 * tol:
+                bound = 0.0
+                system._stress_fp64 = True
+                system.matvec(x, tmp, "fp64", oseen_done=True)
+                fp64_residuals += 1
+            torch.sub(b, tmp, out=r)
         else:
             system.matvec(x, tmp, outer, oseen_done=pending and ref == 0)
             if outer == "fp32c":
