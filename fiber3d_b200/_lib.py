@@ -85,6 +85,7 @@ SIGNATURES: dict[str, list] = {
     "f3d_body_residual": [ctypes.c_int32, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P],
     "f3d_surface_dense": [_I, _P, _P, _P, _P, _P, _P, _I64, _I64, _D, _D, _D, _P],
     "f3d_rotate_blocks": [_P, _P, _P, _P, ctypes.c_int32, _I, _P],
+    "f3d_body_advance": [_P, _P, ctypes.c_int32, _D, _P, _P, _P, _P],
     "f3d_rigid_body_update": [_P, _P, _P, _P, _P, _P, _I64, _P, _P, _P, _P],
     "f3d_gather_segments": [_P, _P, _P, _P, _P, ctypes.c_int32, _I64, _P],
     "f3d_krylov_workspace_bytes": [_I64, ctypes.c_int32, ctypes.POINTER(_SZ)],

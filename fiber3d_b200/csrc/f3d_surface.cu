@@ -262,6 +262,40 @@ __global__ void rigid_body_update_kernel(const int32_t *__restrict__ body_of,
   }
 }
 
+// One thread per rigid body: the time-step update of tstep.py:1403-1407
+// from the body's velocities in the solution (U at sol[vel_off[b]], Omega at
+// sol[vel_off[b] + 3]): loc += dt U; q <- q_dt q with q_dt = (cos(a/2),
+// sin(a/2) phi/a), phi = dt Omega, a = |phi| (the identity when a == 0;
+// quaternion.py:14-38); then R(q) (quaternion.py:41-53) into R.
+__global__ void body_advance_kernel(const double *__restrict__ sol, const int64_t *__restrict__ vel_off,
+                                    int nbody, double dt, double *__restrict__ loc,
+                                    double *__restrict__ quat, double *__restrict__ R) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= nbody) return;
+  const double *u = sol + vel_off[b];
+  for (int c = 0; c < 3; ++c) loc[3 * b + c] = __dadd_rn(loc[3 * b + c], __dmul_rn(dt, u[c]));
+  const double f0 = u[3] * dt, f1 = u[4] * dt, f2 = u[5] * dt;
+  const double a = sqrt(f0 * f0 + f1 * f1 + f2 * f2);
+  double qs = 1.0, q0 = 0.0, q1 = 0.0, q2 = 0.0;
+  if (a != 0.0) {
+    double sh, ch;
+    sincos(0.5 * a, &sh, &ch);
+    qs = ch;
+    q0 = sh * (f0 / a); q1 = sh * (f1 / a); q2 = sh * (f2 / a);
+  }
+  const double rs = quat[4 * b], r0 = quat[4 * b + 1], r1 = quat[4 * b + 2], r2 = quat[4 * b + 3];
+  const double s = qs * rs - (q0 * r0 + q1 * r1 + q2 * r2);
+  const double p0 = qs * r0 + rs * q0 + (q1 * r2 - q2 * r1);
+  const double p1 = qs * r1 + rs * q1 + (q2 * r0 - q0 * r2);
+  const double p2 = qs * r2 + rs * q2 + (q0 * r1 - q1 * r0);
+  quat[4 * b] = s; quat[4 * b + 1] = p0; quat[4 * b + 2] = p1; quat[4 * b + 3] = p2;
+  const double d = s * s - 0.5;
+  double *m = R + 9 * b;
+  m[0] = 2.0 * (p0 * p0 + d); m[1] = 2.0 * (p0 * p1 - s * p2); m[2] = 2.0 * (p0 * p2 + s * p1);
+  m[3] = 2.0 * (p1 * p0 + s * p2); m[4] = 2.0 * (p1 * p1 + d); m[5] = 2.0 * (p1 * p2 - s * p0);
+  m[6] = 2.0 * (p2 * p0 - s * p1); m[7] = 2.0 * (p2 * p1 + s * p0); m[8] = 2.0 * (p2 * p2 + d);
+}
+
 __global__ void rotate_blocks_kernel(double *x, const int64_t *off, const int32_t *nvec,
                                      const double *R, int transpose) {
   const int b = blockIdx.x;
@@ -297,6 +331,17 @@ int f3d_rigid_body_update(const int32_t *body_of, const double *R, const double 
   const unsigned grid = static_cast<unsigned>((nnodes + 127) / 128);
   f3d::rigid_body_update_kernel<<<grid, 128, 0, static_cast<cudaStream_t>(stream)>>>(
       body_of, R, loc, ref_nodes, ref_normals, ref_E, nnodes, nodes, normals, E);
+  return f3d::launch_status();
+}
+
+int f3d_body_advance(const double *sol, const int64_t *vel_off, int32_t nbody, double dt, double *loc,
+                     double *quat, double *R, void *stream) {
+  if (nbody < 0) return F3D_ERR_SHAPE;
+  if (nbody == 0) return F3D_OK;
+  if (!sol || !vel_off || !loc || !quat || !R) return F3D_ERR_NULL;
+  const unsigned grid = static_cast<unsigned>((nbody + 127) / 128);
+  f3d::body_advance_kernel<<<grid, 128, 0, static_cast<cudaStream_t>(stream)>>>(sol, vel_off, nbody, dt, loc,
+                                                                               quat, R);
   return f3d::launch_status();
 }
 

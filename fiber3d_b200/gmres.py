@@ -82,6 +82,13 @@ class DeviceGMRES:
         self.aux = f(self.m + 2)      # aux[j + 1] = |aux vector| after the matvec of step j
         self.auxbeta = f(1)
         self.h_host = torch.zeros(3 * (self.m + 2) + 1, dtype=torch.float64).pin_memory()
+        # y of the update x += Z y goes up through a pinned buffer
+        self.y_host = torch.zeros(self.m, dtype=torch.float64).pin_memory()
+        self.y_dev = f(self.m)
+        self.y_done = torch.cuda.Event()
+        # two norms read back together (|b| and a residual's)
+        self.pair = f(2)
+        self.pair_host = torch.zeros(2, dtype=torch.float64).pin_memory()
         self.graph = {}
         self.last_aux_sum = 0.0
 
@@ -143,10 +150,15 @@ class DeviceGMRES:
             self.graph[key] = g
         self.graph[key].replay()
 
+    def read_pair(self):
+        """The two norms in self.pair, on the host (one synchronisation)."""
+        self.pair_host.copy_(self.pair)
+        return float(self.pair_host[0]), float(self.pair_host[1])
+
     # ------------------------------------------------------------- solve ---
     def solve(self, matvec, pc, b: torch.Tensor, x0: torch.Tensor | None = None, rtol=1e-8,
               maxiter=200, use_graph=True, key="default", bnorm=None, verify=True, aux=None,
-              r0: torch.Tensor | None = None):
+              r0: torch.Tensor | None = None, rnorm0: float | None = None):
         """Solve A x = b with right preconditioner pc = P^-1.
 
         Returns (x, info, iterations, history of relative residual estimates).
@@ -156,14 +168,18 @@ class DeviceGMRES:
         result itself, as the mixed-precision refinement does).  With `aux`,
         ``self.last_aux_sum`` is set to sum_j |y_j| |aux after A z_j| over the
         correction x - x0 = sum_j y_j z_j (an error bound's ingredient).
-        `r0` (optional) is b - A x0, already computed by the caller.
+        `r0` (optional) is b - A x0, already computed by the caller, and
+        `rnorm0` (optional) the norm of the first residual (b itself when
+        x0 is None) when the caller knows it.
         """
         self.last_aux_sum = 0.0
         n, m = self.n, self.m
         if b.numel() != n or (x0 is not None and x0.numel() != n):
             raise ValueError(f"right-hand side and guess must have {n} entries")
         dev = self.device
-        x = torch.zeros(n, dtype=torch.float64, device=dev) if x0 is None else x0.clone()
+        # x starts as zero implicitly (the first update overwrites it) when x0 is None
+        x_zero = x0 is None
+        x = torch.empty(n, dtype=torch.float64, device=dev) if x_zero else x0.clone()
         r = torch.empty(n, dtype=torch.float64, device=dev)
         tmp = torch.empty(n, dtype=torch.float64, device=dev)
         if bnorm is None:
@@ -174,24 +190,29 @@ class DeviceGMRES:
         its, hist = 0, []
         while True:
             # r = b - A x
-            if x0 is None and its == 0:
-                r.copy_(b)
+            if x_zero:
+                res = b
             elif r0 is not None and its == 0:
-                r.copy_(r0)
+                res = r0
             else:
                 matvec(x, tmp)
                 torch.sub(b, tmp, out=r)
-            self._norm(r, self.beta)
-            rnorm = float(self.beta.item())
+                res = r
+            if its == 0 and rnorm0 is not None:
+                rnorm = float(rnorm0)
+                self.beta.fill_(rnorm)
+            else:
+                self._norm(res, self.beta)
+                rnorm = float(self.beta.item())
             hist.append(rnorm / bnorm)
-            if rnorm <= rtol * bnorm:
-                return x, 0, its, hist
-            if its >= maxiter:
-                return x, its, its, hist
+            if rnorm <= rtol * bnorm or its >= maxiter:
+                if x_zero:
+                    x.zero_()
+                return x, (0 if rnorm <= rtol * bnorm else its), its, hist
             # V[0] = r / |r|, cur = V[0], k = 1
             self.k.zero_()
             st = _lib.stream_handle(dev)
-            _lib.call("f3d_krylov_scale_into", _lib.ptr(r), _lib.ptr(self.beta), _lib.ptr(self.k),
+            _lib.call("f3d_krylov_scale_into", _lib.ptr(res), _lib.ptr(self.beta), _lib.ptr(self.k),
                       _lib.ptr(self.V), n, n, 1, _lib.ptr(self.cur), st)
             H = np.zeros((m + 1, m))
             cs, sn = np.zeros(m), np.zeros(m)
@@ -232,10 +253,13 @@ class DeviceGMRES:
             if aux is not None:
                 an = self.h_host.numpy()[2 * (m + 2):2 * (m + 2) + j_done + 1]
                 self.last_aux_sum += float(np.sum(np.abs(y) * an[1:j_done + 1]))
-            yd = torch.as_tensor(y, device=dev)
-            _lib.call("f3d_krylov_combine", _lib.ptr(self.Z), n, _lib.ptr(yd), j_done, _lib.ptr(r), n, 0,
-                      _lib.stream_handle(dev))
-            x += r
+            self.y_done.synchronize()  # the previous upload out of y_host has run
+            self.y_host[:j_done].copy_(torch.from_numpy(y))
+            self.y_dev[:j_done].copy_(self.y_host[:j_done], non_blocking=True)
+            self.y_done.record()
+            _lib.call("f3d_krylov_combine", _lib.ptr(self.Z), n, _lib.ptr(self.y_dev), j_done, _lib.ptr(x), n,
+                      0 if x_zero else 1, _lib.stream_handle(dev))
+            x_zero = False
             if not verify and hist[-1] <= rtol:
                 return x, 0, its, hist
 
@@ -274,8 +298,21 @@ def solve_system(system, tol=1e-8, restart=100, maxiter=200, x0=None, mixed=Fals
     x = torch.zeros(n, dtype=torch.float64, device=dev) if x0 is None else x0.clone()
     r = torch.empty(n, dtype=torch.float64, device=dev)
     tmp = torch.empty(n, dtype=torch.float64, device=dev)
-    g._norm(b, g.beta)
-    bnorm = float(g.beta.item())
+    # |b| stays on the device until the first residual's norm is read with it
+    g._norm(b, g.pair[0:1])
+    bnorm = None
+
+    def norm_rel(w):
+        """|w| / |b| (reading |b| too on the first call)."""
+        nonlocal bnorm
+        if bnorm is None:
+            g._norm(w, g.pair[1:2])
+            bnorm, wn = g.read_pair()
+        else:
+            g._norm(w, g.beta)
+            wn = float(g.beta.item())
+        return wn / bnorm if bnorm > 0.0 else 0.0, wn
+
     total_its, hist, ref = 0, [], 0
     info = 0
     # outer residuals start FP32C unless an earlier solve of this system found
@@ -296,8 +333,7 @@ def solve_system(system, tol=1e-8, restart=100, maxiter=200, x0=None, mixed=Fals
             # the Oseen flow of x0 is FP64 already (update(x0)); the stresslet
             # part in FP32C is bounded by its own flow: eps_v |v - v_oseen|
             system.matvec(x, tmp, "fp32c", oseen_done=True)
-            g._norm(system.v - system.v2, g.beta)
-            bound = eps_v * float(g.beta.item()) / bnorm
+            bound = eps_v * norm_rel(system.v - system.v2)[0]
             if bound > 0.5 * tol:
                 bound = 0.0
                 system._stress_fp64 = True
@@ -307,8 +343,7 @@ def solve_system(system, tol=1e-8, restart=100, maxiter=200, x0=None, mixed=Fals
         else:
             system.matvec(x, tmp, outer, oseen_done=pending and ref == 0)
             if outer == "fp32c":
-                g._norm(system.v, g.beta)
-                bound = eps_v * float(g.beta.item()) / bnorm
+                bound = eps_v * norm_rel(system.v)[0]
                 if bound > 0.5 * tol:
                     outer, bound = "fp64", 0.0
                     system._outer_fp64 = True
@@ -317,8 +352,7 @@ def solve_system(system, tol=1e-8, restart=100, maxiter=200, x0=None, mixed=Fals
                 fp64_residuals += 1
             torch.sub(b, tmp, out=r)
         if known is None:
-            g._norm(r, g.beta)
-            rel = float(g.beta.item()) / bnorm
+            rel, rnorm = norm_rel(r)
         known = None
         hist.append(rel + bound)
         if rel + bound <= tol:  # the FP64 residual is <= tol as well
@@ -331,7 +365,7 @@ def solve_system(system, tol=1e-8, restart=100, maxiter=200, x0=None, mixed=Fals
         d, _, its, ihist = g.solve(lambda a, o: system.matvec(a, o, "fp32c"),
                                    lambda a, o: system.pc(a, o, "fp32c"), r, rtol=inner,
                                    maxiter=maxiter - total_its, use_graph=use_graph, key="fp32c",
-                                   verify=False, aux=system.v)
+                                   verify=False, aux=system.v, bnorm=rnorm, rnorm0=rnorm)
         total_its += its
         x += d
         ref += 1
@@ -340,9 +374,9 @@ def solve_system(system, tol=1e-8, restart=100, maxiter=200, x0=None, mixed=Fals
         # and the FP32C error of the matvecs that built d = sum_j y_j z_j
         # (linear in y); no further matvec when this settles convergence.
         est = ihist[-1] * rel
-        bd = eps_v * g.last_aux_sum / bnorm
-        if est + bound + bd <= tol:
-            known = (est, bound + bd)
+        bd = bound + eps_v * g.last_aux_sum / bnorm
+        if est + bd <= tol:  # the same sum as the convergence test above
+            known = (est, bd)
     torch.cuda.synchronize()
     return {"x": x, "info": info, "iterations": total_its, "history": hist, "refinements": ref,
             "outer_residuals": outer, "fp64_residuals": fp64_residuals, "seconds": time.perf_counter() - t0}

@@ -282,32 +282,22 @@ class HydroSystem:
         self.fs = FiberSet(P.fibers, P.lengths, device=dev)
         nF = self.fs.total
         self.nF = nF
-        self.x_fib = f64(np.concatenate(P.fibers) if P.fibers else np.zeros((0, 3)))
+        x_fib0 = np.concatenate(P.fibers) if P.fibers else np.zeros((0, 3))
         ff = P.force_fibers if P.force_fibers is not None else np.zeros((nF, 3))
         self.force = f64(np.asarray(ff).reshape(-1, 3))
         self.has_force = bool(np.any(ff))
         self.geo = torch.empty((max(nF, 1), 9), dtype=torch.float64, device=dev)
         self.timers = PhaseTimers()
         self.v_gain = self._flow_to_residual_gain(P.lengths)
-        # ---- bodies (host state: location, orientation; device: nodes, normals, E)
+        # ---- bodies (device state: location, orientation quaternion, nodes, normals, E)
         self.nbody = len(P.bodies)
         nb = [np.asarray(b.ref_nodes).reshape(-1, 3).shape[0] for b in P.bodies]
         self.nb = nb
         self.body_node_off_h = np.concatenate([[0], np.cumsum(nb)]).astype(np.int64)
         nB = int(self.body_node_off_h[-1])
         self.nB = nB
-        self.body_loc = np.array([np.asarray(b.location, dtype=np.float64) for b in P.bodies]).reshape(-1, 3)
-        self.body_quat = np.array([rotation_to_quaternion(b.rotation) for b in P.bodies]).reshape(-1, 4)
         self.body_ref = [np.asarray(b.ref_nodes, dtype=np.float64).reshape(-1, 3) for b in P.bodies]
         self.body_ref_n = [np.asarray(b.ref_normals, dtype=np.float64).reshape(-1, 3) for b in P.bodies]
-        if self.nbody:
-            self.body_nodes = torch.zeros((nB, 3), dtype=torch.float64, device=dev)
-            self.body_normals = torch.zeros((nB, 3), dtype=torch.float64, device=dev)
-            self.body_w = f64(np.concatenate([np.asarray(b.weights).reshape(-1) for b in P.bodies]))
-            self.body_centers = torch.zeros((self.nbody, 3), dtype=torch.float64, device=dev)
-            self.body_E = torch.empty((nB, 9), dtype=torch.float64, device=dev)
-            self.body_R = torch.zeros((self.nbody, 9), dtype=torch.float64, device=dev)
-            self._load_bodies()
         # ---- shell
         if P.shell is not None:
             self.shell = shell_op or ShellOperator(P.shell, P.eta, P.reg, P.eps_dist, dev)
@@ -322,28 +312,51 @@ class HydroSystem:
         self.size = self.o_fib + 4 * nF
         self.x_off_body = torch.as_tensor(np.array(self.o_body, dtype=np.int64), device=dev) if self.nbody else None
         self.body_node_off = torch.as_tensor(self.body_node_off_h, device=dev)
-        # ---- targets: [fibers; bodies; shell]
-        parts = [self.x_fib]
+        # ---- positions, one buffer: targets [fibers; bodies; shell].  The
+        # fiber points (the Oseen sources), the body nodes and the stresslet
+        # sources [bodies; shell] are views of it, so moving the geometry in
+        # place moves every sum's sources and targets together.
+        self.trg = torch.empty((nF + nB + nS, 3), dtype=torch.float64, device=dev)
+        self.x_fib = self.trg[:nF]
+        self.x_fib.copy_(f64(x_fib0.reshape(-1, 3)))
+        if nS:
+            self.trg[nF + nB:].copy_(self.shell.nodes)
+        # fiber point p0 + i, coordinate c is entry o_fib + 4 p0 + c n + i of a solution
+        gat = np.empty((nF, 3), dtype=np.int64)
+        for f in range(self.fs.nfib):
+            n, p0 = int(self.fs.npts[f]), int(self.fs.pt_off_h[f])
+            gat[p0:p0 + n] = self.o_fib + 4 * p0 + np.arange(3)[None, :] * n + np.arange(n)[:, None]
+        self._x_fib_from_sol = torch.as_tensor(gat.reshape(-1), device=dev)
         if self.nbody:
-            parts.append(self.body_nodes)
-        if self.shell is not None:
-            parts.append(self.shell.nodes)
-        self.trg = torch.cat(parts).contiguous()
+            self.body_nodes = self.trg[nF:nF + nB]
+            self.stress_normals = torch.zeros((nB + nS, 3), dtype=torch.float64, device=dev)
+            self.body_normals = self.stress_normals[:nB]
+            self.body_w = f64(np.concatenate([np.asarray(b.weights).reshape(-1) for b in P.bodies]))
+            self.body_E = torch.empty((nB, 9), dtype=torch.float64, device=dev)
+            self.body_R = torch.zeros((self.nbody, 9), dtype=torch.float64, device=dev)
+            self.body_centers = f64(np.array([np.asarray(b.location, dtype=np.float64)
+                                              for b in P.bodies]).reshape(-1, 3))
+            self.body_quat = f64(np.array([rotation_to_quaternion(b.rotation)
+                                           for b in P.bodies]).reshape(-1, 4))
+            self._vel_off = torch.as_tensor(np.array([self.o_body[k] + 3 * nb[k] for k in range(self.nbody)],
+                                                     dtype=np.int64), device=dev)
+            # body node i of body k -> rows o_body[k] + 3 (i - first node of k) .. +3
+            self._rhs_body_idx = torch.as_tensor(np.concatenate(
+                [self.o_body[k] + np.arange(3 * nb[k]) for k in range(self.nbody)]).astype(np.int64), device=dev)
+            self._load_bodies()
         self.ntrg = self.trg.shape[0]
         grp = np.concatenate([np.repeat(np.arange(self.fs.nfib), self.fs.npts),
                               -np.ones(self.ntrg - nF)]).astype(np.int32)
         self.trg_grp = torch.as_tensor(grp, device=dev)
         self.src_grp = self.trg_grp[:nF].contiguous()
-        # stresslet sources: [body nodes; shell nodes]
-        sp, sn = [], []
-        if self.nbody:
-            sp.append(self.body_nodes); sn.append(self.body_normals)
-        if self.shell is not None:
-            sp.append(self.shell.nodes); sn.append(self.shell.normals)
+        # stresslet sources: [body nodes; shell nodes] (a view of the targets)
         self.nstress = nB + nS
         if self.nstress:
-            self.stress_nodes = torch.cat(sp).contiguous()
-            self.stress_normals = torch.cat(sn).contiguous()
+            self.stress_nodes = self.trg[nF:]
+            if not self.nbody:
+                self.stress_normals = torch.zeros((nS, 3), dtype=torch.float64, device=dev)
+            if nS:
+                self.stress_normals[nB:].copy_(self.shell.normals)
             self.stress_dens = torch.zeros((self.nstress, 3), dtype=torch.float64, device=dev)
             seg_src, seg_dst, seg_len = [], [], []
             for k in range(self.nbody):
@@ -414,40 +427,34 @@ class HydroSystem:
 
     # ------------------------------------------------------------------------
     def _load_bodies(self):
-        """Body nodes, normals and singularity vectors at the current
-        location/orientation, on the device (one kernel).  A rigid body's
-        singularity vectors are those of its reference surface rotated with
-        it: the 3 x 3 map E_i (unit density -> velocity at node i) of the
-        rotated surface is R E_i^ref R^T (the stresslet sum is
-        rotation-equivariant and translation-invariant), so the pair sum runs
-        once per body, at set-up, not every step."""
+        """Body nodes, normals and singularity vectors at the initial
+        location/orientation, on the device.  A rigid body's singularity
+        vectors are those of its reference surface rotated with it: the
+        3 x 3 map E_i (unit density -> velocity at node i) of the rotated
+        surface is R E_i^ref R^T (the stresslet sum is rotation-equivariant
+        and translation-invariant), so the pair sum runs once per body, at
+        set-up, not every step."""
         dev = self.device
-        if not hasattr(self, "_body_of"):
-            self._body_of = torch.as_tensor(np.repeat(np.arange(self.nbody), self.nb).astype(np.int32), device=dev)
-            self._ref_nodes = torch.as_tensor(np.concatenate(self.body_ref), device=dev)
-            self._ref_normals = torch.as_tensor(np.concatenate(self.body_ref_n), device=dev)
-            P = self.p
-            E = []
-            for k in range(self.nbody):
-                a, b = int(self.body_node_off_h[k]), int(self.body_node_off_h[k + 1])
-                E.append(singularity_vectors(self._ref_nodes[a:b], self._ref_normals[a:b], self.body_w[a:b],
-                                             P.eta, P.reg, P.eps_dist))
-            self._ref_E = torch.cat(E).contiguous()
-            self._rl_host = torch.zeros((self.nbody, 12), dtype=torch.float64).pin_memory()
-            self._rl_dev = torch.zeros((self.nbody, 12), dtype=torch.float64, device=dev)
-            self._rl_done = torch.cuda.Event()
-        self._rl_done.synchronize()  # the previous copy out of the pinned buffer has run
-        rl = self._rl_host.numpy()
-        rl[:, :9] = np.stack([quaternion_rotation(q).reshape(9) for q in self.body_quat])
-        rl[:, 9:] = self.body_loc
-        self._rl_dev.copy_(self._rl_host, non_blocking=True)
-        self._rl_done.record()
-        self.body_R.copy_(self._rl_dev[:, :9])
-        self.body_centers.copy_(self._rl_dev[:, 9:])
+        self._body_of = torch.as_tensor(np.repeat(np.arange(self.nbody), self.nb).astype(np.int32), device=dev)
+        self._ref_nodes = torch.as_tensor(np.concatenate(self.body_ref), device=dev)
+        self._ref_normals = torch.as_tensor(np.concatenate(self.body_ref_n), device=dev)
+        P = self.p
+        E = []
+        for k in range(self.nbody):
+            a, b = int(self.body_node_off_h[k]), int(self.body_node_off_h[k + 1])
+            E.append(singularity_vectors(self._ref_nodes[a:b], self._ref_normals[a:b], self.body_w[a:b],
+                                         P.eta, P.reg, P.eps_dist))
+        self._ref_E = torch.cat(E).contiguous()
+        R = np.stack([quaternion_rotation(q).reshape(9) for q in self.body_quat.cpu().numpy()])
+        self.body_R.copy_(torch.as_tensor(R, device=dev))
+        self._place_bodies()
+
+    def _place_bodies(self):
+        """Nodes, normals and E of every body from body_R / body_centers (one kernel)."""
         _lib.call("f3d_rigid_body_update", _lib.ptr(self._body_of), _lib.ptr(self.body_R), _lib.ptr(self.body_centers),
                   _lib.ptr(self._ref_nodes), _lib.ptr(self._ref_normals), _lib.ptr(self._ref_E), self.nB,
                   _lib.ptr(self.body_nodes), _lib.ptr(self.body_normals), _lib.ptr(self.body_E),
-                  _lib.stream_handle(dev))
+                  _lib.stream_handle(self.device))
 
     def _body_blocks(self):
         """Body preconditioner blocks in each body's own frame (location 0,
@@ -497,30 +504,25 @@ class HydroSystem:
     def advance(self, sol: torch.Tensor, x0: torch.Tensor | None = None):
         """Move the geometry one step with solution `sol` (tstep.py:1392-1407:
         fibers take their new positions; bodies x += dt U and
-        q <- q(Omega dt) q), then :meth:`update` (with the next guess x0)."""
-        dt = self.p.dt
-        o = self.o_fib
-        for n in sorted(set(int(v) for v in self.fs.npts)):
-            idx = np.nonzero(self.fs.npts == n)[0]
-            starts = self.fs.pt_off_h[idx]
-            if np.all(np.diff(starts) == n) and idx.size and idx[-1] - idx[0] == idx.size - 1:
-                blk = sol[o + 4 * int(starts[0]):o + 4 * int(starts[0]) + 4 * n * idx.size].view(idx.size, 4, n)
-                self.x_fib[int(starts[0]):int(starts[0]) + n * idx.size] = blk[:, :3, :].transpose(1, 2).reshape(-1, 3)
-            else:
-                for f in idx:
-                    p0 = int(self.fs.pt_off_h[f])
-                    blk = sol[o + 4 * p0:o + 4 * p0 + 4 * n].view(4, n)
-                    self.x_fib[p0:p0 + n] = blk[:3].t()
+        q <- q(Omega dt) q), then :meth:`update` (with the next guess x0).
+        Everything stays on the device: one gather for the fiber points, one
+        kernel for the body states and one for their surfaces."""
+        if sol.dtype != torch.float64 or not sol.is_contiguous() or sol.numel() != self.size:
+            raise ValueError(f"solution must be a contiguous float64 vector of {self.size} entries")
+        if self.nF:
+            torch.index_select(sol, 0, self._x_fib_from_sol, out=self.x_fib.view(-1))
         if self.nbody:
-            if not hasattr(self, "_vel_idx"):
-                idx = np.array([[self.o_body[k] + 3 * self.nb[k] + c for c in range(6)] for k in range(self.nbody)])
-                self._vel_idx = torch.as_tensor(idx, device=sol.device)
-            vel = sol[self._vel_idx].cpu().numpy()
-            for k in range(self.nbody):
-                self.body_loc[k] = self.body_loc[k] + dt * vel[k, :3]
-                self.body_quat[k] = quaternion_multiply(quaternion_from_rotation(vel[k, 3:] * dt), self.body_quat[k])
-            self._load_bodies()
+            _lib.call("f3d_body_advance", _lib.ptr(sol), _lib.ptr(self._vel_off), self.nbody, self.p.dt,
+                      _lib.ptr(self.body_centers), _lib.ptr(self.body_quat), _lib.ptr(self.body_R),
+                      _lib.stream_handle(self.device))
+            self._place_bodies()
         self.update(x0)
+
+    def body_state(self):
+        """(locations (nbody, 3), quaternions (nbody, 4)) of the bodies, on the host."""
+        if not self.nbody:
+            return np.zeros((0, 3)), np.zeros((0, 4))
+        return self.body_centers.cpu().numpy(), self.body_quat.cpu().numpy()
 
     # ------------------------------------------------------------------------
     def autotune(self):
@@ -580,10 +582,9 @@ class HydroSystem:
         if nF:
             self.flow_ext.copy_(v[:nF])
         if nS:
-            self.rhs[:3 * nS] = -v[nF + nB:].reshape(-1)
-        for k in range(self.nbody):
-            a, b = int(self.body_node_off_h[k]), int(self.body_node_off_h[k + 1])
-            self.rhs[self.o_body[k]:self.o_body[k] + 3 * (b - a)] = -v[nF + a:nF + b].reshape(-1)
+            torch.neg(v[nF + nB:].reshape(-1), out=self.rhs[:3 * nS])
+        if self.nbody:
+            self.rhs.index_copy_(0, self._rhs_body_idx, v[nF:nF + nB].reshape(-1).neg())
         flow = self.flow_ext
         # fiber blocks into A_fib and (a copy) into the LU buffer
         refresh = self._pc_age is None or self._pc_age >= self.pc_refresh - 1

@@ -376,6 +376,15 @@ int f3d_rigid_body_update(const int32_t *body_of, const double *R, const double 
                           const double *ref_nodes, const double *ref_normals, const double *ref_E,
                           int64_t nnodes, double *nodes, double *normals, double *E, void *stream);
 
+/* Rigid-body time-step update on the device (tstep/tstep.py:1399-1407,
+   quaternion/quaternion.py:14-53): body b's velocities are U = sol[vel_off[b]
+   .. +3) and Omega = sol[vel_off[b]+3 .. +6); loc_b += dt U, quat_b <-
+   q(dt Omega) quat_b (Hamilton product; quaternions (s, p1, p2, p3)) and
+   R_b = R(quat_b), row-major.  loc (nbody x 3) and quat (nbody x 4) are the
+   bodies' state, read and written; R (nbody x 9) is written. */
+int f3d_body_advance(const double *sol, const int64_t *vel_off, int32_t nbody, double dt, double *loc,
+                     double *quat, double *R, void *stream);
+
 /* Rigid-body frame change of preconditioner vectors: for body b the nvec[b]
    3-vectors at x + offsets[b] become R_b v (transpose 0) or R_b^T v
    (transpose 1), R_b row-major at R + 9b.  With the body block factored

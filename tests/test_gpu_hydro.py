@@ -206,6 +206,53 @@ def test_guess_flow_summed_in_update(golden_step, mixed):
         assert rel_err(ra["x"].cpu().numpy(), rb["x"].cpu().numpy()) < 1e-7
 
 
+def test_advance_equals_fresh_system(golden_step):
+    """A system moved by advance(sol) equals one built from scratch at the
+    moved geometry (fibers at the positions in sol; bodies moved by
+    tstep.py:1403-1407 on the host): the right-hand side and the matvec at
+    1e-12, the bodies' states at 1e-14.  The step is exaggerated (fiber
+    points shifted by up to 0.02, bodies translated by 0.05 and turned by
+    0.1 rad) so that any sum left at the old geometry shows."""
+    from fiber3d_b200 import hydro as H
+    P = problem_from_golden(golden_step)
+    s = H.HydroSystem(P)
+    rng = np.random.default_rng(7)
+    sol = golden_step["sol"].copy()
+    dt = P.dt
+    for k in range(s.nbody):
+        o = s.o_body[k] + 3 * s.nb[k]
+        u = rng.normal(size=3)
+        w = rng.normal(size=3)
+        sol[o:o + 3] = 0.05 / dt * u / np.linalg.norm(u)
+        sol[o + 3:o + 6] = 0.1 / dt * w / np.linalg.norm(w)
+    fibers = []
+    for f in range(s.fs.nfib):
+        n, p0 = int(s.fs.npts[f]), int(s.fs.pt_off_h[f])
+        o = s.o_fib + 4 * p0
+        sol[o:o + 3 * n] += rng.uniform(-0.02, 0.02, size=3 * n)
+        fibers.append(sol[o:o + 3 * n].reshape(3, n).T.copy())
+    loc0, q0 = s.body_state()
+    s.advance(torch.tensor(sol, device="cuda"))
+    bodies = []
+    for k, b in enumerate(P.bodies):
+        o = s.o_body[k] + 3 * s.nb[k]
+        loc = loc0[k] + dt * sol[o:o + 3]
+        q = H.quaternion_multiply(H.quaternion_from_rotation(sol[o + 3:o + 6] * dt), q0[k])
+        bodies.append(H.Body(loc, H.quaternion_rotation(q), b.ref_nodes, b.ref_normals, b.weights))
+        loc_d, q_d = s.body_state()
+        assert np.max(np.abs(loc_d[k] - loc)) < 1e-14 and np.max(np.abs(q_d[k] - q)) < 1e-14
+    moved = H.Problem(fibers, P.lengths, P.E, P.dt, P.eta, bodies, P.shell, P.force_fibers)
+    fresh = H.HydroSystem(moved)
+    assert rel_err(s.rhs.cpu().numpy(), fresh.rhs.cpu().numpy()) < 1e-12
+    assert rel_err(s.rhs.cpu().numpy(), H.HydroSystem(P).rhs.cpu().numpy()) > 1e-6
+    y, z = (torch.empty(s.size, dtype=torch.float64, device="cuda") for _ in range(2))
+    for x in golden_step["probe_x"]:
+        xt = torch.tensor(x, device="cuda")
+        s.matvec(xt, y)
+        fresh.matvec(xt, z)
+        assert rel_err(y.cpu().numpy(), z.cpu().numpy()) < 1e-12
+
+
 def test_graph_and_eager_agree(system):
     a = system.solve(tol=1e-9, use_graph=False)["x"]
     b = system.solve(tol=1e-9, use_graph=True)["x"]
