@@ -295,7 +295,7 @@ def gpu_arm(args, rank, world, local):
             "learned_mixed_ms": st["learned_mixed"]["ms_per_step"],
             "speedup_learned_mixed_vs_plain_fp64": st["learned_mixed"]["speedup_vs_fp64"],
             "modes": {m: {k: v[k] for k in ("ms_per_step", "ms_per_step_last_half", "iterations", "long_solves",
-                                            "true_rel_residual",
+                                            "true_rel_residual", "tol", "fiber_pc_rebuilt",
                                             "rel_err_vs_fp64_1e-12_solve", "speedup_vs_fp64", "phases_ms")}
                       for m, v in st.items() if m != "training"},
             "training": st["training"],
@@ -423,17 +423,20 @@ def hydro_arm(args, rank, world, local, warmup=None, steps=None, emit=True):
              "scale_selection": sel, "validation_seeds": val_seeds,
              "seeds": list(args.train_seeds), "steps_per_seed": args.train_steps,
              "skipped_steps": args.train_skip}
-    # mode: (guess, mixed precision, preconditioner refresh interval)
-    modes = {"fp64": ("zero", False, 1), "mixed": ("zero", True, 1),
-             "extrapolate_fp64": ("extrapolate", False, 1), "extrapolate_mixed": ("extrapolate", True, 1),
-             "learned_fp64": ("learned", False, 1), "learned_mixed": ("learned", True, 1),
-             "learned_mixed_pc4": ("learned", True, 4)}
-    for mode, (guess, mixed, pc_refresh) in modes.items():
+    # mode: (guess, mixed precision, preconditioner refresh interval, GMRES tolerance)
+    modes = {"fp64": ("zero", False, 1, 1e-8), "mixed": ("zero", True, 1, 1e-8),
+             "extrapolate_fp64": ("extrapolate", False, 1, 1e-8),
+             "extrapolate_mixed": ("extrapolate", True, 1, 1e-8),
+             "learned_fp64": ("learned", False, 1, 1e-8),
+             "learned_mixed_pc1": ("learned", True, 1, 1e-8),
+             "learned_mixed": ("learned", True, "auto", 1e-8),
+             "learned_mixed_tol1e-9": ("learned", True, "auto", 1e-9)}
+    for mode, (guess, mixed, pc_refresh, tol) in modes.items():
         sysd = H.HydroSystem(P, shell_op=shell, device=dev, tune=True, pc_refresh=pc_refresh)
         torch.cuda.synchronize()
         replicas.barrier()
         history = []
-        times, its, resid, phases, r0s, worst = [], [], [], [], [], []
+        times, its, resid, phases, r0s, worst, finals, fresh = [], [], [], [], [], [], [], []
         for step in range(warmup + steps):
             torch.cuda.synchronize()
             sysd.timers.report()
@@ -455,7 +458,8 @@ def hydro_arm(args, rank, world, local, warmup=None, steps=None, emit=True):
             if history:
                 sysd.advance(history[-1], x0=x0)
             sysd.timers.start("GMRES")
-            res = sysd.solve(tol=1e-8, restart=100, mixed=mixed, x0=x0)
+            refreshed = sysd._pc_age == 0
+            res = sysd.solve(tol=tol, restart=100, mixed=mixed, x0=x0)
             sysd.timers.stop("GMRES")
             e1.record()
             e1.synchronize()
@@ -473,6 +477,8 @@ def hydro_arm(args, rank, world, local, warmup=None, steps=None, emit=True):
                                   "fp64_residuals": res.get("fp64_residuals", 0),
                                   "history": [float(f"{h:.3g}") for h in res["history"]]})
                 r0s.append(res["history"][0])
+                finals.append(res["history"][-1])
+                fresh.append(bool(refreshed))
                 phases.append(ph)
                 y = torch.empty_like(sol)
                 sysd.matvec(sol, y)
@@ -485,7 +491,8 @@ def hydro_arm(args, rank, world, local, warmup=None, steps=None, emit=True):
         out[mode] = {"ms_per_step": statistics.median(times), "iterations": its,
                      "ms_per_step_last_half": statistics.median(times[len(times) // 2:]),
                      "true_rel_residual": max(resid), "refinements": res.get("refinements", 0),
-                     "initial_rel_residual": r0s, "long_solves": worst,
+                     "initial_rel_residual": r0s, "final_rel_residual_bound": finals,
+                     "fiber_pc_rebuilt": fresh, "tol": tol, "long_solves": worst,
                      "phases_ms": {k: statistics.median([p.get(k, 0.0) for p in phases]) for k in phases[0]}}
         del sysd
     # each replica's median step; the job's is the slowest replica's
@@ -618,7 +625,7 @@ def main():
     ap.add_argument("--no-step", action="store_true",
                     help="pair throughput only (skip the embedded time-step comparison)")
     ap.add_argument("--step-warmup", type=int, default=8)
-    ap.add_argument("--step-steps", type=int, default=20)
+    ap.add_argument("--step-steps", type=int, default=40)
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

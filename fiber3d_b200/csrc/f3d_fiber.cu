@@ -180,9 +180,89 @@ __device__ double assemble_element(int r, int col, int n, const double *__restri
   return 0.0;
 }
 
+// Collocation rows of the operator by columns.  Element (row i of row
+// block br, column j of column block bcb) of the 4n - 14 collocation rows is
+//   e P_br[i][j] + sum_{|k - j| <= band} P_br[i][k] w[k],
+// P_br = P_X (br < 3) or P_T (br = 3), with e and w fixed by (br, column):
+//   br, bcb < 3:     e = [br == bcb] / dt,        w[k] = c_ab(k) D4[k][j] s4,
+//                    c_aa = E c0 (1 + xs_a^2) + E c1 (1 - xs_a^2), c_ab = (E c0 - E c1) xs_a xs_b
+//   br < 3, bcb = 3: e = -(c0 + c1) xss_a(j),     w[k] = -2 c0 xs_a(k) D1[k][j] s1
+//   br = 3, bcb < 3: e = 0,  w[k] = -(c1 + 7 c0) E xss_b(k) D4 s4 - 6 c0 E xsss_b(k) D3 s3
+//                                   - penalty xs_b(k) D1 s1
+//   br = 3, bcb = 3: e = (c1 + c0) |xss(j)|^2,   w[k] = -2 c0 D2[k][j] s2
+// (the same terms as assemble_element, fiber.py:322-448 projected as in
+// fiber.py:810-961).  A thread owns one column: it forms w for one row block
+// at a time (2 band + 1 values) and sweeps that block's rows, reading the
+// projection rows from shared memory.
+constexpr int kAsmMaxBand = 7;
+
+template <int MAXBAND>
+__device__ void assemble_columns(int n, int col, int ph, int tpc, const double *__restrict__ m,
+                                 const ResLayout &R, const double *__restrict__ g,
+                                 const double *__restrict__ xss2, const double *__restrict__ sPx,
+                                 const double *__restrict__ sPt, const FiberPhys &ph_, double s1,
+                                 int band, double *Af, double *Ac) {
+  constexpr int W = 2 * MAXBAND + 1;
+  const int nn = 4 * n;
+  const double s2 = s1 * s1, s3 = s2 * s1, s4 = s3 * s1;
+  const double E = ph_.E, c0 = ph_.c0, c1 = ph_.c1;
+  const int bcb = col / n, j = col - bcb * n;
+  const int kbase = j - band;
+  for (int br = 0; br < 4; ++br) {
+    double w[W];
+    double e = 0.0;
+#pragma unroll
+    for (int q = 0; q < W; ++q) {
+      const int k = kbase + q;
+      double v = 0.0;
+      if (q <= 2 * band && k >= 0 && k < n) {
+        const double *gk = g + 9 * k;
+        if (br < 3 && bcb < 3) {
+          const double xa = gk[br], xb = gk[bcb];
+          const double c = (br == bcb) ? E * c0 * (1.0 + xa * xa) + E * c1 * (1.0 - xa * xa)
+                                       : (E * c0 - E * c1) * xa * xb;
+          v = c * (m[R.d4 + static_cast<int64_t>(k) * n + j] * s4);
+        } else if (br < 3) {
+          v = (-2.0 * c0 * gk[br]) * (m[R.d1 + static_cast<int64_t>(k) * n + j] * s1);
+        } else if (bcb < 3) {
+          v = -(c1 + 7.0 * c0) * E * gk[3 + bcb] * (m[R.d4 + static_cast<int64_t>(k) * n + j] * s4) -
+              6.0 * c0 * E * gk[6 + bcb] * (m[R.d3 + static_cast<int64_t>(k) * n + j] * s3) -
+              ph_.penalty * gk[bcb] * (m[R.d1 + static_cast<int64_t>(k) * n + j] * s1);
+        } else {
+          v = (-2.0 * c0) * (m[R.d2 + static_cast<int64_t>(k) * n + j] * s2);
+        }
+      }
+      w[q] = v;
+    }
+    if (br < 3 && bcb < 3) e = (br == bcb) ? 1.0 / ph_.dt : 0.0;
+    else if (br < 3) e = -(c0 + c1) * g[9 * j + 3 + br];
+    else if (bcb == 3) e = (c1 + c0) * xss2[j];
+    const int rows = (br < 3) ? n - 4 : n - 2;
+    const int r0 = br * (n - 4);
+    const double *P = (br < 3) ? sPx : sPt;
+    for (int i = ph; i < rows; i += tpc) {
+      const double *Pi = P + i * n;
+      double s = e * Pi[j];
+#pragma unroll
+      for (int q = 0; q < W; ++q) {
+        const int k = kbase + q;
+        const int kc = k < 0 ? 0 : (k >= n ? n - 1 : k);  // w is 0 outside the fiber
+        s = fma(Pi[kc], w[q], s);
+      }
+      const int64_t idx = static_cast<int64_t>(r0 + i) * nn + col;
+      Af[idx] = s;
+      if (Ac) Ac[idx] = s;
+    }
+  }
+}
+
 // One CTA per fiber.  Writes the operator block to A (and to A_copy if
-// non-null) and the right-hand side block to rhs.
-__global__ void __launch_bounds__(256) fiber_assemble_kernel(
+// non-null) and the right-hand side block to rhs.  BANDED: the collocation
+// rows by columns (assemble_columns, projection matrices staged in shared
+// memory; needs 4n <= blockDim and band <= kAsmMaxBand), else element by
+// element.
+template <bool BANDED>
+__global__ void __launch_bounds__(256, 2) fiber_assemble_kernel(
     FiberSet fs, FiberPhys ph, const double *__restrict__ x, const double *__restrict__ geo,
     const double *__restrict__ flow, const double *__restrict__ force, double *A, double *A_copy,
     double *rhs) {
@@ -198,7 +278,10 @@ __global__ void __launch_bounds__(256) fiber_assemble_kernel(
   double *g = sm;                  // 9n geometry
   double *xss2 = g + 9 * n;        // n   |xss|^2
   double *rfull = xss2 + n;        // 4n  unprojected right-hand side
+  double *sP = rfull + 4 * n;      // BANDED: P_X ((n-4) x n) then P_T ((n-2) x n)
   for (int i = threadIdx.x; i < 9 * n; i += blockDim.x) g[i] = geo[9 * p0 + i];
+  if (BANDED)
+    for (int i = threadIdx.x; i < (2 * n - 6) * n; i += blockDim.x) sP[i] = m[R.px + i];
   __syncthreads();
   for (int k = threadIdx.x; k < n; k += blockDim.x) {
     const double *gk = g + 9 * k;
@@ -228,11 +311,26 @@ __global__ void __launch_bounds__(256) fiber_assemble_kernel(
   const int nn = 4 * n;
   double *Af = A + fs.mat_off[f];
   double *Ac = A_copy ? A_copy + fs.mat_off[f] : nullptr;
-  for (int idx = threadIdx.x; idx < nn * nn; idx += blockDim.x) {
-    const int r = idx / nn, col = idx - r * nn;
-    const double v = assemble_element(r, col, n, m, R, g, xss2, bc, ph, s1, fs.band);
-    Af[idx] = v;
-    if (Ac) Ac[idx] = v;
+  if (BANDED) {
+    const int tpc = blockDim.x / nn;  // threads per column
+    const int col = threadIdx.x % nn, phs = threadIdx.x / nn;
+    if (phs < tpc) {
+      assemble_columns<kAsmMaxBand>(n, col, phs, tpc, m, R, g, xss2, sP, sP + (n - 4) * n, ph, s1, fs.band,
+                                    Af, Ac);
+      // the 14 boundary rows
+      for (int r = nn - 14 + phs; r < nn; r += tpc) {
+        const double v = assemble_element(r, col, n, m, R, g, xss2, bc, ph, s1, fs.band);
+        Af[static_cast<int64_t>(r) * nn + col] = v;
+        if (Ac) Ac[static_cast<int64_t>(r) * nn + col] = v;
+      }
+    }
+  } else {
+    for (int idx = threadIdx.x; idx < nn * nn; idx += blockDim.x) {
+      const int r = idx / nn, col = idx - r * nn;
+      const double v = assemble_element(r, col, n, m, R, g, xss2, bc, ph, s1, fs.band);
+      Af[idx] = v;
+      if (Ac) Ac[idx] = v;
+    }
   }
   // projected right-hand side and boundary values
   double *rf = rhs + 4 * p0;
@@ -421,10 +519,23 @@ int f3d_fiber_assemble(const f3d_fiber_set *set, double E, double dt, double c0,
   if (rc || fs.nfib == 0) return rc;
   if (!x || !geo || !flow || !force || !A || !rhs) return F3D_ERR_NULL;
   if (max_n < 5) return F3D_ERR_SHAPE;
-  const size_t smem = static_cast<size_t>(14) * max_n * sizeof(double);
   f3d::FiberPhys ph{E, dt, c0, c1, penalty};
-  f3d::fiber_assemble_kernel<<<fs.nfib, 256, smem, static_cast<cudaStream_t>(stream)>>>(
-      fs, ph, x, geo, flow, force, A, A_copy, rhs);
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  constexpr int kThreads = 256;
+  if (4 * max_n <= kThreads && fs.band <= f3d::kAsmMaxBand) {
+    // columns of every fiber fit one CTA: projection matrices staged in shared memory
+    const size_t smem = (static_cast<size_t>(14) * max_n + static_cast<size_t>(2 * max_n - 6) * max_n) * sizeof(double);
+    if (smem > 48 * 1024) {
+      cudaError_t e = cudaFuncSetAttribute(f3d::fiber_assemble_kernel<true>,
+                                           cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+      if (e != cudaSuccess) return F3D_ERR_CUDA;
+    }
+    f3d::fiber_assemble_kernel<true><<<fs.nfib, kThreads, smem, st>>>(fs, ph, x, geo, flow, force, A, A_copy, rhs);
+  } else {
+    const size_t smem = static_cast<size_t>(14) * max_n * sizeof(double);
+    f3d::fiber_assemble_kernel<false><<<fs.nfib, kThreads, smem, st>>>(fs, ph, x, geo, flow, force, A, A_copy,
+                                                                        rhs);
+  }
   return f3d::launch_status();
 }
 

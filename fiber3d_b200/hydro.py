@@ -268,9 +268,12 @@ class HydroSystem:
     """Device linear system of one time step: ``rhs``, :meth:`matvec`,
     :meth:`pc` (the right preconditioner P^-1) and :meth:`solve`."""
 
+    PC_AUTO_MARGIN = 0.5   # pc_refresh="auto": rebuild after a solve that ended above this * tol
+    PC_AUTO_MAX_AGE = 8    # ... and at least every this many steps
+
     def __init__(self, problem: Problem, shell_op: ShellOperator | None = None, device=None,
                  tune: bool = False, fiber_pc: str = "auto", inner_shell_pc: str = "fp16",
-                 pc_refresh: int = 1):
+                 pc_refresh: int | str = 1):
         self.p = problem
         dev = device or torch.device("cuda", torch.cuda.current_device())
         self.device = dev
@@ -400,11 +403,14 @@ class HydroSystem:
         # the fiber blocks of the preconditioner are rebuilt every pc_refresh
         # steps (fiber3d: every step); in between the last ones are kept --
         # still a fixed operator within each solve, of a geometry at most
-        # pc_refresh - 1 steps old
-        if pc_refresh < 1:
-            raise ValueError("pc_refresh must be >= 1")
-        self.pc_refresh = int(pc_refresh)
+        # pc_refresh - 1 steps old.  "auto": rebuilt for the next step when
+        # the last solve needed more than one GMRES iteration or ended above
+        # PC_AUTO_MARGIN * tol, and at least every PC_AUTO_MAX_AGE steps.
+        if pc_refresh != "auto" and (isinstance(pc_refresh, str) or int(pc_refresh) < 1):
+            raise ValueError("pc_refresh must be >= 1 or 'auto'")
+        self.pc_refresh = pc_refresh if pc_refresh == "auto" else int(pc_refresh)
         self._pc_age = None
+        self._pc_stale = False  # set by solve() under pc_refresh="auto"
         self.A_fib = torch.zeros(max(self.fs.mat_total, 1), dtype=torch.float64, device=dev)
         self.flow_ext = torch.zeros((max(nF, 1), 3), dtype=torch.float64, device=dev)
         self._body_blocks()
@@ -587,7 +593,10 @@ class HydroSystem:
             self.rhs.index_copy_(0, self._rhs_body_idx, v[nF:nF + nB].reshape(-1).neg())
         flow = self.flow_ext
         # fiber blocks into A_fib and (a copy) into the LU buffer
-        refresh = self._pc_age is None or self._pc_age >= self.pc_refresh - 1
+        if self.pc_refresh == "auto":
+            refresh = self._pc_age is None or self._pc_stale or self._pc_age >= self.PC_AUTO_MAX_AGE - 1
+        else:
+            refresh = self._pc_age is None or self._pc_age >= self.pc_refresh - 1
         self.timers.start("Build_linear_system_fibers")
         if nF:
             A_copy = self.lu.A.data_ptr() if refresh else None
@@ -674,7 +683,10 @@ class HydroSystem:
 
     def solve(self, tol=1e-8, restart=100, maxiter=200, x0=None, mixed=False, **kw):
         from .gmres import solve_system
-        return solve_system(self, tol=tol, restart=restart, maxiter=maxiter, x0=x0, mixed=mixed, **kw)
+        res = solve_system(self, tol=tol, restart=restart, maxiter=maxiter, x0=x0, mixed=mixed, **kw)
+        if self.pc_refresh == "auto":
+            self._pc_stale = res["iterations"] > 1 or res["history"][-1] > self.PC_AUTO_MARGIN * tol
+        return res
 
     # ---------------------------------------------------------------- layout --
     def split(self, sol: torch.Tensor):

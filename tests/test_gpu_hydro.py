@@ -253,6 +253,35 @@ def test_advance_equals_fresh_system(golden_step):
         assert rel_err(y.cpu().numpy(), z.cpu().numpy()) < 1e-12
 
 
+def test_pc_refresh_auto(golden_step):
+    """pc_refresh="auto" keeps the fiber-block inverses while solves end in
+    one iteration with margin, rebuilds them after any other solve, and
+    every step still reaches the tolerance in FP64."""
+    from fiber3d_b200 import hydro as H, warmstart as W
+    P = problem_from_golden(golden_step)
+    for bad in (0, "sometimes"):
+        with pytest.raises(ValueError):
+            H.HydroSystem(P, pc_refresh=bad)
+    s = H.HydroSystem(P, pc_refresh="auto")
+    history, rebuilt = [], []
+    y = torch.empty(s.size, dtype=torch.float64, device="cuda")
+    for step in range(6):
+        x0 = W.extrapolate(history)
+        stale, age = s._pc_stale, s._pc_age
+        if history:
+            s.advance(history[-1], x0=x0)
+            expect = stale or age + 1 >= s.PC_AUTO_MAX_AGE
+            assert s._pc_age == (0 if expect else age + 1)
+        rebuilt.append(s._pc_age == 0)
+        res = s.solve(tol=1e-9, x0=x0, mixed=True)
+        assert res["info"] == 0
+        assert s._pc_stale == (res["iterations"] > 1 or res["history"][-1] > s.PC_AUTO_MARGIN * 1e-9)
+        s.matvec(res["x"], y)
+        assert float(torch.linalg.vector_norm(y - s.rhs) / torch.linalg.vector_norm(s.rhs)) <= 1e-9
+        history = (history + [res["x"]])[-3:]
+    assert rebuilt[0]
+
+
 def test_graph_and_eager_agree(system):
     a = system.solve(tol=1e-9, use_graph=False)["x"]
     b = system.solve(tol=1e-9, use_graph=True)["x"]
