@@ -98,6 +98,40 @@ __device__ __forceinline__ void two_sum(float &s, float &c, float x) {
   c += e;
 }
 
+// Packed two-lane FP32 arithmetic (PTX f32x2, sm_100): one instruction
+// applies the same IEEE round-to-nearest operation to two floats held in a
+// 64-bit register pair, so a pair of sources costs one issue slot per
+// operation instead of two.
+typedef unsigned long long f32x2;
+__device__ __forceinline__ f32x2 pk2(float a, float b) {
+  f32x2 r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a), "f"(b));
+  return r;
+}
+__device__ __forceinline__ void up2(f32x2 v, float &a, float &b) {
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(v));
+}
+__device__ __forceinline__ f32x2 add2(f32x2 a, f32x2 b) {
+  f32x2 d;
+  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+  return d;
+}
+__device__ __forceinline__ f32x2 sub2(f32x2 a, f32x2 b) {
+  f32x2 d;
+  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+  return d;
+}
+__device__ __forceinline__ f32x2 mul2(f32x2 a, f32x2 b) {
+  f32x2 d;
+  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+  return d;
+}
+__device__ __forceinline__ f32x2 fma2(f32x2 a, f32x2 b, f32x2 c) {
+  f32x2 d;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+  return d;
+}
+
 // DUAL (FP64 Oseen only): the same pairs summed against two densities, dens
 // into out and dens2 into out2, each with exactly the arithmetic of a single
 // sum -- the geometry (r, 1/r, 1/r^3) is computed once for both.
@@ -142,14 +176,24 @@ __global__ void __launch_bounds__(kBlock) pair_kernel(const PairArgs a) {
       tzh[k] = static_cast<float>(z); tzl[k] = static_cast<float>(z - static_cast<double>(tzh[k]));
     }
   }
+  // FP32C: each target coordinate twice, against a pair of sources
+  f32x2 pxh[TPT], pyh[TPT], pzh[TPT], pxl[TPT], pyl[TPT], pzl[TPT];
+  if (PREC != F3D_FP64) {
+#pragma unroll
+    for (int k = 0; k < TPT; ++k) {
+      pxh[k] = pk2(txh[k], txh[k]); pyh[k] = pk2(tyh[k], tyh[k]); pzh[k] = pk2(tzh[k], tzh[k]);
+      pxl[k] = pk2(txl[k], txl[k]); pyl[k] = pk2(tyl[k], tyl[k]); pzl[k] = pk2(tzl[k], tzl[k]);
+    }
+  }
 
   double acc[TPT][3], acc2[TPT][3];
-  float fs[TPT][3], fc[TPT][3], ft[TPT][3];
+  float fs[TPT][3], fc[TPT][3];
+  f32x2 ft[TPT][3];  // FP32C tile sums: {even sources, odd sources}
 #pragma unroll
   for (int k = 0; k < TPT; ++k)
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-      acc[k][c] = 0.0; acc2[k][c] = 0.0; fs[k][c] = 0.f; fc[k][c] = 0.f; ft[k][c] = 0.f;
+      acc[k][c] = 0.0; acc2[k][c] = 0.0; fs[k][c] = 0.f; fc[k][c] = 0.f; ft[k][c] = 0ull;
     }
 
   const double reg2 = a.reg2;
@@ -158,8 +202,8 @@ __global__ void __launch_bounds__(kBlock) pair_kernel(const PairArgs a) {
 
   // ---- one tile of `cnt` sources starting at global index `sbase` --------
   auto compute_tile = [&](const unsigned char *buf, int cnt, int64_t sbase) {
-    for (int s = sl; s < cnt; s += SL) {
-      if (PREC == F3D_FP64) {
+    if (PREC == F3D_FP64) {
+      for (int s = sl; s < cnt; s += SL) {
         const double *pos = reinterpret_cast<const double *>(buf + St::off_pos);
         const double *den = reinterpret_cast<const double *>(buf + St::off_dens);
         const double *nrm = reinterpret_cast<const double *>(buf + St::off_nrm);
@@ -210,50 +254,77 @@ __global__ void __launch_bounds__(kBlock) pair_kernel(const PairArgs a) {
             acc[k][2] = fma(f0, dz, acc[k][2]);
           }
         }
-      } else {
-        const float4 *rec = reinterpret_cast<const float4 *>(buf + St::off_rec);
-        const float4 q0 = rec[3 * s], q1 = rec[3 * s + 1], q2 = rec[3 * s + 2];
-        // q0 = {xh, yh, zh, xl}; q1 = {yl, zl, d0, d1}; q2 = {d2, n0, n1, n2}
-        int32_t sg = 0;
-        if (MODE == F3D_SELF_SKIP_GROUP) sg = reinterpret_cast<const int32_t *>(buf + St::off_grp)[s];
+      }
+    } else {
+      // sources in pairs (2q, 2q + 1); a record of 6 x 16 bytes holds
+      // {xh,yh},{zh,xl},{yl,zl},{d0,d1},{d2,n0},{n1,n2}, each component as
+      // {even, odd}.  An odd count ends on the packer's pad source (far
+      // away, zero density), whose terms are exactly zero.
+      const ulonglong2 *rec = reinterpret_cast<const ulonglong2 *>(buf + St::off_rec);
+      const int npair = (cnt + 1) >> 1;
+      for (int q = sl; q < npair; q += SL) {
+        const ulonglong2 u0 = rec[6 * q], u1 = rec[6 * q + 1], u2 = rec[6 * q + 2];
+        const ulonglong2 u3 = rec[6 * q + 3], u4 = rec[6 * q + 4];
+        const f32x2 sxh = u0.x, syh = u0.y, szh = u1.x, sxl = u1.y, syl = u2.x, szl = u2.y;
+        const f32x2 d0 = u3.x, d1 = u3.y, d2 = u4.x;
+        f32x2 n0 = 0ull, n1 = 0ull, n2 = 0ull;
+        if (KIND == F3D_KERNEL_STRESSLET) {
+          const ulonglong2 u5 = rec[6 * q + 5];
+          n0 = u4.y; n1 = u5.x; n2 = u5.y;
+        }
+        int2 sg = make_int2(0, 0);
+        if (MODE == F3D_SELF_SKIP_GROUP) sg = reinterpret_cast<const int2 *>(buf + St::off_grp)[q];
 #pragma unroll
         for (int k = 0; k < TPT; ++k) {
-          const float dx = (txh[k] - q0.x) + (txl[k] - q0.w);
-          const float dy = (tyh[k] - q0.y) + (tyl[k] - q1.x);
-          const float dz = (tzh[k] - q0.z) + (tzl[k] - q1.y);
-          float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-          r2 = (r2 < eps2f) ? r2 + reg2f : r2;
-          float ri = rsqrtf(r2);
-          if (MODE == F3D_SELF_SKIP_INDEX) ri = (sbase + s == tidx[k]) ? 0.f : ri;
-          if (MODE == F3D_SELF_SKIP_GROUP) ri = (sg == tgrp[k]) ? 0.f : ri;
+          const f32x2 dx = add2(sub2(pxh[k], sxh), sub2(pxl[k], sxl));
+          const f32x2 dy = add2(sub2(pyh[k], syh), sub2(pyl[k], syl));
+          const f32x2 dz = add2(sub2(pzh[k], szh), sub2(pzl[k], szl));
+          float ra, rb;
+          up2(fma2(dx, dx, fma2(dy, dy, mul2(dz, dz))), ra, rb);
+          ra = (ra < eps2f) ? ra + reg2f : ra;
+          rb = (rb < eps2f) ? rb + reg2f : rb;
+          float ia = rsqrtf(ra), ib = rsqrtf(rb);
+          if (MODE == F3D_SELF_SKIP_INDEX) {
+            const int64_t s0 = sbase + 2 * q;
+            ia = (s0 == tidx[k]) ? 0.f : ia;
+            ib = (s0 + 1 == tidx[k]) ? 0.f : ib;
+          }
+          if (MODE == F3D_SELF_SKIP_GROUP) {
+            ia = (sg.x == tgrp[k]) ? 0.f : ia;
+            ib = (sg.y == tgrp[k]) ? 0.f : ib;
+          }
+          const f32x2 ri = pk2(ia, ib);
           if (KIND == F3D_KERNEL_OSEEN) {
-            const float rf = fmaf(dx, q1.z, fmaf(dy, q1.w, dz * q2.x));
-            const float g = ri * ri * ri * rf;
-            ft[k][0] = fmaf(g, dx, fmaf(ri, q1.z, ft[k][0]));
-            ft[k][1] = fmaf(g, dy, fmaf(ri, q1.w, ft[k][1]));
-            ft[k][2] = fmaf(g, dz, fmaf(ri, q2.x, ft[k][2]));
+            const f32x2 rf = fma2(dx, d0, fma2(dy, d1, mul2(dz, d2)));
+            const f32x2 g = mul2(mul2(mul2(ri, ri), ri), rf);
+            ft[k][0] = fma2(g, dx, fma2(ri, d0, ft[k][0]));
+            ft[k][1] = fma2(g, dy, fma2(ri, d1, ft[k][1]));
+            ft[k][2] = fma2(g, dz, fma2(ri, d2, ft[k][2]));
           } else if (KIND == F3D_KERNEL_ROTLET) {
-            const float g = ri * ri * ri;
-            ft[k][0] = fmaf(g, dz * q1.w - dy * q2.x, ft[k][0]);
-            ft[k][1] = fmaf(g, dx * q2.x - dz * q1.z, ft[k][1]);
-            ft[k][2] = fmaf(g, dy * q1.z - dx * q1.w, ft[k][2]);
+            const f32x2 g = mul2(mul2(ri, ri), ri);
+            ft[k][0] = fma2(g, sub2(mul2(dz, d1), mul2(dy, d2)), ft[k][0]);
+            ft[k][1] = fma2(g, sub2(mul2(dx, d2), mul2(dz, d0)), ft[k][1]);
+            ft[k][2] = fma2(g, sub2(mul2(dy, d0), mul2(dx, d1)), ft[k][2]);
           } else {
-            const float ri2 = ri * ri;
-            const float rd = fmaf(dx, q1.z, fmaf(dy, q1.w, dz * q2.x));
-            const float rn = fmaf(dx, q2.y, fmaf(dy, q2.z, dz * q2.w));
-            const float f0 = rd * rn * (ri2 * ri2 * ri);
-            ft[k][0] = fmaf(f0, dx, ft[k][0]);
-            ft[k][1] = fmaf(f0, dy, ft[k][1]);
-            ft[k][2] = fmaf(f0, dz, ft[k][2]);
+            const f32x2 ri2 = mul2(ri, ri);
+            const f32x2 rd = fma2(dx, d0, fma2(dy, d1, mul2(dz, d2)));
+            const f32x2 rn = fma2(dx, n0, fma2(dy, n1, mul2(dz, n2)));
+            const f32x2 f0 = mul2(mul2(rd, rn), mul2(mul2(ri2, ri2), ri));
+            ft[k][0] = fma2(f0, dx, ft[k][0]);
+            ft[k][1] = fma2(f0, dy, ft[k][1]);
+            ft[k][2] = fma2(f0, dz, ft[k][2]);
           }
         }
       }
-    }
-    if (PREC != F3D_FP64) {
 #pragma unroll
       for (int k = 0; k < TPT; ++k)
 #pragma unroll
-        for (int c = 0; c < 3; ++c) { two_sum(fs[k][c], fc[k][c], ft[k][c]); ft[k][c] = 0.f; }
+        for (int c = 0; c < 3; ++c) {
+          float e, o;
+          up2(ft[k][c], e, o);
+          two_sum(fs[k][c], fc[k][c], e + o);
+          ft[k][c] = 0ull;
+        }
     }
   };
 
@@ -271,12 +342,15 @@ __global__ void __launch_bounds__(kBlock) pair_kernel(const PairArgs a) {
         if (DUAL) den2[i] = a.dens2[3 * s0 + i];
       }
     } else {
+      // whole source pairs (the packer pads an odd count)
       float *rec = reinterpret_cast<float *>(buf + St::off_rec);
-      for (int i = tid; i < 12 * cnt; i += kBlock) rec[i] = a.packed[12 * s0 + i];
+      const int cp = (cnt + 1) & ~1;
+      for (int i = tid; i < 12 * cp; i += kBlock) rec[i] = a.packed[12 * s0 + i];
     }
     if (MODE == F3D_SELF_SKIP_GROUP) {
       int32_t *g = reinterpret_cast<int32_t *>(buf + St::off_grp);
       for (int i = tid; i < cnt; i += kBlock) g[i] = a.gs[s0 + i];
+      if ((cnt & 1) && tid == 0) g[cnt] = INT32_MIN;  // the pad source's group
     }
   };
 
@@ -436,30 +510,36 @@ __global__ void __launch_bounds__(kBlock) pair_kernel(const PairArgs a) {
   if (tid == 0) a.counters[blockIdx.x] = 0u;
 }
 
-// Packs FP32C source records: {xh,yh,zh,xl},{yl,zl,d0,d1},{d2,n0,n1,n2}.
+// Packs FP32C source records by pairs of sources (2q, 2q + 1): 24 floats
+// {xh,yh,zh,xl,yl,zl,d0,d1,d2,n0,n1,n2} interleaved as {even, odd} per
+// component, in the order the kernel reads them: {xh_e,xh_o,yh_e,yh_o},
+// {zh_e,zh_o,xl_e,xl_o}, {yl_e,yl_o,zl_e,zl_o}, {d0_e,d0_o,d1_e,d1_o},
+// {d2_e,d2_o,n0_e,n0_o}, {n1_e,n1_o,n2_e,n2_o}.  One thread per source;
+// with an odd count the source index ns is a pad at 1e30 with zero density
+// and normal, whose pair terms are exactly zero (r^2 overflows to inf,
+// rsqrt gives 0, and every term carries a zero factor).
 __global__ void pack_fp32_sources(const double *rs, const double *dens, const double *nrm,
                                   float *packed, int64_t ns) {
   const int64_t s = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-  if (s >= ns) return;
-  float h[3], l[3];
+  const int64_t npad = (ns + 1) & ~static_cast<int64_t>(1);
+  if (s >= npad) return;
+  float v[12];
+  if (s < ns) {
 #pragma unroll
-  for (int c = 0; c < 3; ++c) {
-    const double x = rs[3 * s + c];
-    h[c] = static_cast<float>(x);
-    l[c] = static_cast<float>(x - static_cast<double>(h[c]));
+    for (int c = 0; c < 3; ++c) {
+      const double x = rs[3 * s + c];
+      v[c] = static_cast<float>(x);
+      v[3 + c] = static_cast<float>(x - static_cast<double>(v[c]));
+      v[6 + c] = static_cast<float>(dens[3 * s + c]);
+      v[9 + c] = nrm ? static_cast<float>(nrm[3 * s + c]) : 0.f;
+    }
+  } else {
+#pragma unroll
+    for (int c = 0; c < 12; ++c) v[c] = (c < 3) ? 1e30f : 0.f;
   }
-  float4 *o = reinterpret_cast<float4 *>(packed + 12 * s);
-  const float d0 = static_cast<float>(dens[3 * s]), d1 = static_cast<float>(dens[3 * s + 1]),
-              d2 = static_cast<float>(dens[3 * s + 2]);
-  float n0 = 0.f, n1 = 0.f, n2 = 0.f;
-  if (nrm) {
-    n0 = static_cast<float>(nrm[3 * s]);
-    n1 = static_cast<float>(nrm[3 * s + 1]);
-    n2 = static_cast<float>(nrm[3 * s + 2]);
-  }
-  o[0] = make_float4(h[0], h[1], h[2], l[0]);
-  o[1] = make_float4(l[1], l[2], d0, d1);
-  o[2] = make_float4(d2, n0, n1, n2);
+  float *o = packed + 24 * (s >> 1) + (s & 1);
+#pragma unroll
+  for (int c = 0; c < 12; ++c) o[2 * c] = v[c];
 }
 
 // ---------------------------------------------------------------- host ----
@@ -516,7 +596,7 @@ static int make_plan(int kernel, int precision, int64_t ns, int64_t nt, const f3
   if (p->nsplit > 1)
     off += round_up(static_cast<size_t>(p->nsplit) * nt * 3 * sizeof(double) * (dual ? 2 : 1), 256);
   p->off_packed = off;
-  if (precision == F3D_FP32C) off += round_up(static_cast<size_t>(ns) * 12 * sizeof(float), 256);
+  if (precision == F3D_FP32C) off += round_up(static_cast<size_t>((ns + 1) & ~int64_t(1)) * 12 * sizeof(float), 256);
   p->bytes = off;
   return F3D_OK;
 }
@@ -626,7 +706,7 @@ static int pair_sum_core(int kernel, int precision, int self_mode, const double 
   if (self_mode == F3D_SELF_SKIP_GROUP && !aligned(gs, 16)) a.use_tma = 0;
 
   if (precision == F3D_FP32C) {
-    const int64_t nb = (ns + 255) / 256;
+    const int64_t nb = (ns + 1 + 255) / 256;
     pack_fp32_sources<<<static_cast<unsigned>(nb), 256, 0, st>>>(
         rs, dens, kernel == F3D_KERNEL_STRESSLET ? nrm : nullptr, const_cast<float *>(a.packed), ns);
     if ((rc = launch_status())) return rc;
