@@ -282,6 +282,26 @@ def test_pc_refresh_auto(golden_step):
     assert rebuilt[0]
 
 
+def test_speculative_first_inner_step_is_exact(golden_step):
+    """Launching the inner solve's first Arnoldi step before the host reads
+    the first residual's norm changes the order of host reads only: the
+    solution is bit-for-bit the one of the plain order."""
+    from fiber3d_b200.hydro import HydroSystem
+    P = problem_from_golden(golden_step)
+    x0 = torch.tensor(golden_step["probe_x"][0], device="cuda") * 1e-3 + torch.tensor(golden_step["sol"],
+                                                                                     device="cuda")
+    out = []
+    for spec in (False, True):
+        s = HydroSystem(P)
+        s.update(x0)
+        s._spec_first = spec
+        res = s.solve(tol=1e-10, x0=x0, mixed=True)
+        assert res["info"] == 0 and res["iterations"] >= 1
+        out.append(res)
+    assert torch.equal(out[0]["x"], out[1]["x"])
+    assert out[0]["iterations"] == out[1]["iterations"] and out[0]["history"] == out[1]["history"]
+
+
 def test_graph_and_eager_agree(system):
     a = system.solve(tol=1e-9, use_graph=False)["x"]
     b = system.solve(tol=1e-9, use_graph=True)["x"]
