@@ -297,8 +297,9 @@ def gpu_arm(args, rank, world, local):
             "modes": {m: {k: v[k] for k in ("ms_per_step", "ms_per_step_last_half", "iterations", "long_solves",
                                             "true_rel_residual", "tol", "fiber_pc_rebuilt",
                                             "rel_err_vs_fp64_1e-12_solve", "speedup_vs_fp64", "phases_ms")}
-                      for m, v in st.items() if m != "training"},
+                      for m, v in st.items() if m not in ("training", "grid_velocity")},
             "training": st["training"],
+            "grid_velocity": st.get("grid_velocity"),
         }
     if rank == 0:
         print(json.dumps(line), flush=True)
@@ -494,6 +495,22 @@ def hydro_arm(args, rank, world, local, warmup=None, steps=None, emit=True):
                      "initial_rel_residual": r0s, "final_rel_residual_bound": finals,
                      "fiber_pc_rebuilt": fresh, "tol": tol, "long_solves": worst,
                      "phases_ms": {k: statistics.median([p.get(k, 0.0) for p in phases]) for k in phases[0]}}
+        if mode == "learned_mixed":
+            # velocity field on fiber3d's own grid (tstep.py:1240-1270) for the
+            # last step's solution, as the time step's optional output
+            # evaluates it; outside the per-step timings
+            grid = torch.as_tensor(geometry.ellipsoid_grid(), device=dev)
+            for _ in range(2):
+                sysd.grid_velocity(sol, grid, body0_radius=0.5)
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            for _ in range(5):
+                vg = sysd.grid_velocity(sol, grid, body0_radius=0.5)
+            e1.record()
+            e1.synchronize()
+            out["grid_velocity"] = {"grid_points": int(grid.shape[0]), "ms": e0.elapsed_time(e1) / 5,
+                                    "finite": bool(torch.isfinite(vg).all())}
         del sysd
     # each replica's median step; the job's is the slowest replica's
     slowest = replicas.max_over_ranks([out[m]["ms_per_step"] for m in modes], dev)

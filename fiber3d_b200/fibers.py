@@ -98,6 +98,16 @@ class Resolution:
     def packed(self) -> np.ndarray:
         return np.concatenate([d.ravel() for d in self.D0] + [self.PX.ravel(), self.PT.ravel(), self.w0])
 
+    def upsampling(self, rate: int = 2) -> np.ndarray:
+        """[P_up (rate*N x N), w_up (rate*N)]: barycentric resampling onto
+        rate*N equispaced nodes and their unit-length trapezoid weights
+        (fiber3d's P_kerUp and weights_0_up, tstep/fiber_matrices.py:84-92)."""
+        m = rate * self.n
+        P = barycentric(self.alpha, np.linspace(-1.0, 1.0, m))
+        w = np.full(m, 2.0 / (m - 1))
+        w[0] = w[-1] = 1.0 / (m - 1)
+        return np.concatenate([P.ravel(), w])
+
 
 BC_CODES = {"force": 0, "torque": 1, "velocity": 2, "angular_velocity": 3}
 
@@ -151,6 +161,23 @@ class FiberSet:
         self.pt_fib = t(pt_fib, torch.int32)
         self.mats = t(np.concatenate(blocks) if blocks else np.zeros(1), torch.float64)
         self.max_n = int(self.npts.max()) if self.nfib else 0
+        self._up = {}
         self.c = _lib.FiberSetC(self.nfib, _lib.ptr(self.n), _lib.ptr(self.pt_off), _lib.ptr(self.mat_off),
                                 _lib.ptr(self.res_off), _lib.ptr(self.length), _lib.ptr(self.bc),
                                 _lib.ptr(self.pt_fib), _lib.ptr(self.mats), n_fd + 3)
+
+    def upsampling(self, rate: int = 2):
+        """(up_mats, up_off) on the device: every resolution's
+        Resolution.upsampling(rate) back to back, and each fiber's offset."""
+        if rate not in self._up:
+            blocks, offs, o = [], {}, 0
+            for n, r in self.resolutions.items():
+                p = r.upsampling(rate)
+                offs[n] = o
+                blocks.append(p)
+                o += p.size
+            up = torch.as_tensor(np.concatenate(blocks) if blocks else np.zeros(1), dtype=torch.float64,
+                                 device=self.device)
+            off = torch.as_tensor(np.array([offs[n] for n in self.npts], dtype=np.int64), device=self.device)
+            self._up[rate] = (up, off)
+        return self._up[rate]

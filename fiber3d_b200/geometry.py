@@ -200,3 +200,17 @@ def hydro_step_problem(seed: int = 3, nfib: int = 512, npts=32, nbody: int = 4,
     sn, snn = fibonacci_sphere(nshell, shell_radius)
     sw = np.full(nshell, 4.0 * np.pi * shell_radius**2 / nshell)
     return Problem(fibers, [length] * nfib, E, dt, eta, bodies, Shell(sn, -snn, sw), ff)
+
+
+def ellipsoid_grid(b: float = 5.5, c: float = 5.5, dx: float = 0.25) -> np.ndarray:
+    """Grid points at which fiber3d evaluates the velocity field
+    (tstep.py:1240-1270): the ij-meshgrid of arange(-b, b + dx, dx) (x, y)
+    and arange(-c, c + dx, dx) (z), kept where
+    sqrt(x^2/c^2 + y^2/b^2 + z^2/c^2) <= 0.99, in meshgrid order."""
+    xs = np.arange(-b, b + dx, dx)
+    ys = np.arange(-b, b + dx, dx)
+    zs = np.arange(-c, c + dx, dx)
+    xv, yv, zv = np.meshgrid(xs, ys, zs, sparse=False, indexing="ij")
+    xv, yv, zv = xv.ravel(), yv.ravel(), zv.ravel()
+    keep = np.sqrt(xv ** 2 / c ** 2 + yv ** 2 / b ** 2 + zv ** 2 / c ** 2) <= 0.99
+    return np.stack([xv[keep], yv[keep], zv[keep]], axis=1)

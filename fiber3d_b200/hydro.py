@@ -688,6 +688,72 @@ class HydroSystem:
             self._pc_stale = res["iterations"] > 1 or res["history"][-1] > self.PC_AUTO_MARGIN * tol
         return res
 
+    # --------------------------------------------------------- grid velocity --
+    def grid_velocity(self, sol: torch.Tensor, grid_points, body0_radius: float | None = None,
+                      near: float = 0.2, uprate: int = 2) -> torch.Tensor:
+        """Velocity field (ngrid, 3) at grid points for the solution `sol` of
+        the current step, as fiber3d's time step evaluates it before moving
+        the geometry (compute_velocity, tstep.py:1273-1381, and
+        tstep.py:1414-1448); free fibers, no fiber-body links, no external
+        body forces:
+          * periphery and body double layers of their densities in sol
+            (stresslet source -> target);
+          * the fibers' Oseen flow of their implicit forces (force operator
+            of sol, trapezoid-weighted; flow_fibers, tstep_utils.py:653-700),
+            where a grid point within `near` of a fiber node takes instead
+            that fiber's self-flow at its nearest node, with `uprate`-fold
+            upsampled quadrature (f3d_fiber_self_flow_up,
+            f3d_grid_near_fiber); the last such fiber in fiber order wins;
+          * the Oseen flow of the external fiber forces;
+          * with body0_radius, rigid motion U + W x (g - c) inside the first
+            body, moved to c = location + dt U (f3d_grid_rigid_override)."""
+        from . import kernels as K
+        dev = self.device
+        P = self.p
+        st = _lib.stream_handle(dev)
+        if sol.dtype != torch.float64 or not sol.is_contiguous() or sol.numel() != self.size:
+            raise ValueError(f"solution must be a contiguous float64 vector of {self.size} entries")
+        g = torch.as_tensor(grid_points, dtype=torch.float64, device=dev).reshape(-1, 3).contiguous()
+        ng = g.shape[0]
+        kw = dict(eta=P.eta, reg=P.reg, epsilon_distance=P.eps_dist, self_mode="regularise")
+        v = torch.zeros(3 * ng, dtype=torch.float64, device=dev)
+        if ng == 0:
+            return v.view(0, 3)
+        nF, nS = self.nF, self.nS
+        if nS:
+            K.pair_sum("stresslet", self.shell.nodes, g, sol[:3 * nS].view(-1, 3), self.shell.normals,
+                       out=v, accumulate=True, **kw)
+        if self.nbody:
+            dens = torch.cat([sol[self.o_body[k]:self.o_body[k] + 3 * self.nb[k]] for k in range(self.nbody)])
+            K.pair_sum("stresslet", self.body_nodes, g, dens.view(-1, 3), self.body_normals, out=v,
+                       accumulate=True, **kw)
+        if nF:
+            f = torch.empty((nF, 3), dtype=torch.float64, device=dev)
+            _lib.call("f3d_fiber_forces", ctypes.byref(self.fs.c), P.E, _lib.ptr(self.geo),
+                      _lib.ptr(sol[self.o_fib:]), _lib.ptr(f), nF, 0, st)
+            fw = torch.empty_like(f)
+            _lib.call("f3d_fiber_weight", ctypes.byref(self.fs.c), _lib.ptr(f), _lib.ptr(fw), nF, st)
+            vfib = K.pair_sum("oseen", self.x_fib, g, fw, **kw)
+            up, up_off = self.fs.upsampling(uprate)
+            vself = torch.empty((nF, 3), dtype=torch.float64, device=dev)
+            _lib.call("f3d_fiber_self_flow_up", _lib.ptr(self.fs.n), _lib.ptr(self.fs.pt_off),
+                      _lib.ptr(self.fs.length), self.fs.nfib, self.fs.max_n, _lib.ptr(self.x_fib), _lib.ptr(f),
+                      _lib.ptr(up), _lib.ptr(up_off), uprate, P.eta, P.reg, P.eps_dist, _lib.ptr(vself), st)
+            _lib.call("f3d_grid_near_fiber", _lib.ptr(g), ng, _lib.ptr(self.x_fib), _lib.ptr(self.fs.pt_off),
+                      self.fs.nfib, _lib.ptr(vself), near, _lib.ptr(vfib), st)
+            v += vfib
+            if self.has_force:
+                fe = torch.empty_like(f)
+                _lib.call("f3d_fiber_weight", ctypes.byref(self.fs.c), _lib.ptr(self.force), _lib.ptr(fe), nF, st)
+                K.pair_sum("oseen", self.x_fib, g, fe, out=v, accumulate=True, **kw)
+        if self.nbody and body0_radius is not None:
+            o = self.o_body[0] + 3 * self.nb[0]
+            uw = sol[o:o + 6].contiguous()
+            center = (self.body_centers[0] + uw[:3] * P.dt).contiguous()
+            _lib.call("f3d_grid_rigid_override", _lib.ptr(g), ng, _lib.ptr(center), _lib.ptr(uw),
+                      float(body0_radius), _lib.ptr(v), st)
+        return v.view(ng, 3)
+
     # ---------------------------------------------------------------- layout --
     def split(self, sol: torch.Tensor):
         """Solution blocks: shell density, per body (lambda, U, Omega), per

@@ -385,6 +385,37 @@ int f3d_rigid_body_update(const int32_t *body_of, const double *R, const double 
 int f3d_body_advance(const double *sol, const int64_t *vel_off, int32_t nbody, double dt, double *loc,
                      double *quat, double *R, void *stream);
 
+/* ---- velocity field at grid points (fiber3d's compute_velocity,
+   tstep/tstep.py:1273-1381, post-processing :1414-1448) ---------------------
+   The sums are f3d_pair_sum source -> target calls; these three entries are
+   the rest. */
+
+/* Self-flow of each fiber at its own nodes with uprate-fold upsampled
+   quadrature (tstep.py:1352-1357): with M = uprate * n equispaced nodes,
+   x_up = P_up x, f_up = (P_up f) * w_up * (L/2), vself_i = sum_u
+   G(x_up,u - x_i) f_up,u, G the Oseen tensor with 1/r, 1/r^3 (r >
+   epsilon_distance) or sqrt(r^2 + reg^2) in place of r (kernels.py:119-200).
+   up_mats + up_off[k]: P_up (M x n row-major) then the unit-length trapezoid
+   weights w_up (M) of fiber k's resolution (fiber_matrices.py:84-92).  f:
+   the unweighted fiber force per point (npts, 3); vself (npts, 3).
+   6 * max_n * (1 + uprate) doubles must fit 48 KiB (F3D_ERR_TOO_LARGE). */
+int f3d_fiber_self_flow_up(const int32_t *npts, const int64_t *pt_off, const double *length, int32_t nfib,
+                           int32_t max_n, const double *x, const double *f, const double *up_mats,
+                           const int64_t *up_off, int32_t uprate, double eta, double reg,
+                           double epsilon_distance, double *vself, void *stream);
+
+/* For each grid point (ngrid, 3): if some node of fiber k lies within
+   `near` (distance formed as fiber3d forms it), the point takes vself at
+   k's nearest node (first minimum); the last such fiber wins
+   (tstep.py:1341-1365).  Other rows of vfib are left as they are. */
+int f3d_grid_near_fiber(const double *grid, int64_t ngrid, const double *x, const int64_t *pt_off,
+                        int32_t nfib, const double *vself, double near, double *vfib, void *stream);
+
+/* Rigid motion inside a sphere (tstep.py:1438-1448): grid points with
+   |g - center|^2 <= radius^2 get v = U + W x (g - center), uw = (U, W). */
+int f3d_grid_rigid_override(const double *grid, int64_t ngrid, const double *center, const double *uw,
+                            double radius, double *v, void *stream);
+
 /* Rigid-body frame change of preconditioner vectors: for body b the nvec[b]
    3-vectors at x + offsets[b] become R_b v (transpose 0) or R_b^T v
    (transpose 1), R_b row-major at R + 9b.  With the body block factored

@@ -282,6 +282,77 @@ class HydroSystem:
             res[i0:i0 + 4 * n] = self.A_fib[k] @ XT[4 * a:4 * b] - vT_in
         return res
 
+    # ----------------------------------------------------- grid velocity --
+    def grid_velocity(self, x_all, grid_points, body0_radius=None, near=2e-1, uprate=2):
+        """Velocity field at grid points for the solution x_all, as fiber3d's
+        time step evaluates it (compute_velocity, tstep.py:1273-1381, and the
+        post-processing at tstep.py:1414-1448), free fibers, no fiber-body
+        links, no external body forces:
+          periphery and body double layers (stresslet source->target of
+          their densities), the fibers' Oseen flow of their implicit forces
+          (force operator of x_all, trapezoid-weighted, flow_fibers
+          tstep_utils.py:653-700), where each grid point within `near` of a
+          fiber's node takes instead the fiber's self-flow at its nearest
+          node, evaluated with `uprate`-fold upsampled quadrature
+          (fiber_matrices.py:84-92: P_kerUp, weights_0_up), the last such
+          fiber in fiber order winning; plus the Oseen flow of the external
+          fiber forces; and, with body0_radius, rigid motion U + W x (g - c)
+          at grid points inside the first body moved to c = loc + dt U."""
+        eta = self.eta
+        g = np.asarray(grid_points, dtype=np.float64).reshape(-1, 3)
+        nB = self.off_b[-1]
+        vgrid = np.zeros_like(g)
+        if self.shell is not None:
+            q = x_all[:3 * self.nshell].reshape(-1, 3)
+            vgrid += KN.stresslet_kernel_source_target(self.shell.nodes, g, self.shell.normals, q,
+                                                       eta=eta).reshape(-1, 3)
+        vel = np.zeros((len(self.bodies), 6))
+        if self.bodies:
+            dens = np.zeros((nB, 3))
+            for k in range(len(self.bodies)):
+                i0 = self.o_body_k(k)
+                dens[self.off_b[k]:self.off_b[k + 1]] = x_all[i0:i0 + 3 * self.nb[k]].reshape(-1, 3)
+                vel[k] = x_all[i0 + 3 * self.nb[k]:i0 + 3 * self.nb[k] + 6]
+            vgrid += KN.stresslet_kernel_source_target(self.trg_bdy, g, self.nrm_bdy, dens,
+                                                       eta=eta).reshape(-1, 3)
+        if self.fibers:
+            XT = x_all[self.o_fib:]
+            f = np.concatenate([(self.Fop[k] @ XT[4 * self.off_f[k]:4 * self.off_f[k + 1]]).reshape(3, -1).T
+                                for k in range(len(self.fibers))])
+            fw = np.concatenate([f[self.off_f[k]:self.off_f[k + 1]] * self.fms[n].weights(self.lengths[k])[:, None]
+                                 for k, n in enumerate(self.npts)])
+            vfib = KN.oseen_kernel_source_target(self.trg_fib, g, fw, eta=eta).reshape(-1, 3)
+            for i in range(g.shape[0]):
+                for k, xk in enumerate(self.fibers):
+                    dist = np.sqrt((g[i, 0] - xk[:, 0]) ** 2 + (g[i, 1] - xk[:, 1]) ** 2 + (g[i, 2] - xk[:, 2]) ** 2)
+                    if (dist <= near).any():
+                        n, L = self.npts[k], self.lengths[k]
+                        a_up = np.linspace(-1.0, 1.0, uprate * n)
+                        P_up = F.barycentric_matrix(self.fms[n].alpha, a_up)
+                        w_up = np.full(uprate * n, 2.0)
+                        w_up[0] = w_up[-1] = 1.0
+                        w_up *= (L / 2.0) / (uprate * n - 1)
+                        fup = (P_up @ f[self.off_f[k]:self.off_f[k + 1]]) * w_up[:, None]
+                        G = KN.oseen_tensor_source_target(P_up @ xk, xk, eta=eta)
+                        vself = (G @ fup.reshape(-1)).reshape(-1, 3)
+                        vfib[i] = vself[np.argmin(dist)]
+            vgrid += vfib
+            if np.any(self.force_fibers):
+                fe = np.concatenate([self.force_fibers[self.off_f[k]:self.off_f[k + 1]]
+                                     * self.fms[n].weights(self.lengths[k])[:, None]
+                                     for k, n in enumerate(self.npts)])
+                vgrid += KN.oseen_kernel_source_target(self.trg_fib, g, fe, eta=eta).reshape(-1, 3)
+        if self.bodies and body0_radius is not None:
+            U, W = vel[0, :3], vel[0, 3:]
+            c = self.bodies[0].location + U * self.dt
+            ids = (g[:, 0] - c[0]) ** 2 + (c[1] - g[:, 1]) ** 2 + (c[2] - g[:, 2]) ** 2 <= body0_radius ** 2
+            vgrid[ids] = U
+            r = g[ids] - c
+            vgrid[ids, 0] += W[1] * r[:, 2] - W[2] * r[:, 1]
+            vgrid[ids, 1] += W[2] * r[:, 0] - W[0] * r[:, 2]
+            vgrid[ids, 2] += W[0] * r[:, 1] - W[1] * r[:, 0]
+        return vgrid
+
     # ------------------------------------------------------ preconditioner --
     def pc(self, x):
         """P_inv (tstep.py:950-994)."""

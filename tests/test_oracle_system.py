@@ -56,3 +56,24 @@ def test_solve(step):
     res = np.linalg.norm(sys_.matvec(sol) - sys_.rhs) / np.linalg.norm(sys_.rhs)
     assert res < 1e-9
     assert rel_err(sol, g["sol"]) < 1e-7
+
+
+def test_grid_velocity_against_fiber3d():
+    """The oracle's grid velocity against the field fiber3d's own time step
+    writes (tests/golden/make_golden_grid.py): every kept grid point, the
+    near-fiber and inside-body ones included."""
+    g = load_golden("step_small.npz")
+    gg = load_golden("grid_small.npz")
+    sys_ = build_from_golden(g)
+    v = sys_.grid_velocity(gg["sol"], gg["grid_points"], body0_radius=float(gg["body0_radius"]))
+    assert rel_err(v, gg["grid_velocity"]) < 1e-12
+
+
+def test_reference_grid():
+    """geometry.ellipsoid_grid is fiber3d's grid (tstep.py:1240-1270): the
+    fixture's kept points at their indices."""
+    from fiber3d_b200 import geometry
+    gg = load_golden("grid_small.npz")
+    g = geometry.ellipsoid_grid()
+    assert g.shape[0] == int(gg["grid_count"])
+    assert np.array_equal(g[gg["grid_index"]], gg["grid_points"])
