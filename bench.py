@@ -295,7 +295,8 @@ def gpu_arm(args, rank, world, local):
             "learned_mixed_ms": st["learned_mixed"]["ms_per_step"],
             "speedup_learned_mixed_vs_plain_fp64": st["learned_mixed"]["speedup_vs_fp64"],
             "modes": {m: {k: v[k] for k in ("ms_per_step", "ms_per_step_last_half", "iterations", "long_solves",
-                                            "true_rel_residual", "tol", "fiber_pc_rebuilt",
+                                            "true_rel_residual", "tol", "fiber_pc_rebuilt", "fp64_residuals",
+                                            "first_residual_bound_max",
                                             "rel_err_vs_fp64_1e-12_solve", "speedup_vs_fp64", "phases_ms")}
                       for m, v in st.items() if m not in ("training", "grid_velocity")},
             "training": st["training"],
@@ -437,7 +438,7 @@ def hydro_arm(args, rank, world, local, warmup=None, steps=None, emit=True):
         torch.cuda.synchronize()
         replicas.barrier()
         history = []
-        times, its, resid, phases, r0s, worst, finals, fresh = [], [], [], [], [], [], [], []
+        times, its, resid, phases, r0s, worst, finals, fresh, fp64r, fbounds = [], [], [], [], [], [], [], [], [], []
         for step in range(warmup + steps):
             torch.cuda.synchronize()
             sysd.timers.report()
@@ -479,6 +480,8 @@ def hydro_arm(args, rank, world, local, warmup=None, steps=None, emit=True):
                                   "history": [float(f"{h:.3g}") for h in res["history"]]})
                 r0s.append(res["history"][0])
                 finals.append(res["history"][-1])
+                fp64r.append(res.get("fp64_residuals", 0))
+                fbounds.append(res.get("first_residual_bound"))
                 fresh.append(bool(refreshed))
                 phases.append(ph)
                 y = torch.empty_like(sol)
@@ -494,6 +497,8 @@ def hydro_arm(args, rank, world, local, warmup=None, steps=None, emit=True):
                      "true_rel_residual": max(resid), "refinements": res.get("refinements", 0),
                      "initial_rel_residual": r0s, "final_rel_residual_bound": finals,
                      "fiber_pc_rebuilt": fresh, "tol": tol, "long_solves": worst,
+                     "fp64_residuals": sum(fp64r),
+                     "first_residual_bound_max": max((x for x in fbounds if x is not None), default=None),
                      "phases_ms": {k: statistics.median([p.get(k, 0.0) for p in phases]) for k in phases[0]}}
         if mode == "learned_mixed":
             # velocity field on fiber3d's own grid (tstep.py:1240-1270) for the

@@ -81,17 +81,42 @@ __global__ void fiber_self_flow_up_kernel(const int32_t *__restrict__ npts, cons
 // One thread per grid point.  Distances as fiber3d forms them:
 // sqrt(((g_x - x)^2 + (g_y - y)^2) + (g_z - z)^2), rounded operation by
 // operation (no contraction), so the <= near test and the first-minimum
-// node are the reference's.
+// node are the reference's.  A fiber is skipped without looking at its
+// nodes when |g - x_0| - R > near (1 + 2^-40), R = max_i |x_i - x_0| (the
+// CTA forms every fiber's x_0 and R first): every node is then farther than
+// near, so the fiber can be neither the hit nor the nearest-node source.
+constexpr int kNearMaxFibers = 2048;
+
 __global__ void grid_near_fiber_kernel(const double *__restrict__ grid, int64_t ngrid,
                                        const double *__restrict__ x, const int64_t *__restrict__ pt_off,
                                        int nfib, const double *__restrict__ vself, double near,
                                        double *__restrict__ vfib) {
+  __shared__ double s_rad[kNearMaxFibers];
+  const bool bounded = nfib <= kNearMaxFibers;
+  if (bounded) {
+    for (int k = threadIdx.x; k < nfib; k += blockDim.x) {
+      const int64_t p0 = pt_off[k], p1 = pt_off[k + 1];
+      double r2 = 0.0;
+      for (int64_t p = p0 + 1; p < p1; ++p) {
+        const double dx = x[3 * p] - x[3 * p0], dy = x[3 * p + 1] - x[3 * p0 + 1], dz = x[3 * p + 2] - x[3 * p0 + 2];
+        r2 = fmax(r2, dx * dx + dy * dy + dz * dz);
+      }
+      s_rad[k] = sqrt(r2);
+    }
+    __syncthreads();
+  }
   const int64_t g = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
   if (g >= ngrid) return;
   const double gx = grid[3 * g], gy = grid[3 * g + 1], gz = grid[3 * g + 2];
+  const double reach = near * (1.0 + 0x1p-40) + 0x1p-40;
   int64_t best = -1;
   for (int k = 0; k < nfib; ++k) {
     const int64_t p0 = pt_off[k], p1 = pt_off[k + 1];
+    if (bounded) {
+      const double ax = gx - x[3 * p0], ay = gy - x[3 * p0 + 1], az = gz - x[3 * p0 + 2];
+      const double d0 = sqrt(ax * ax + ay * ay + az * az);
+      if (d0 - s_rad[k] * (1.0 + 0x1p-40) > reach) continue;
+    }
     double dmin = 0.0;
     int64_t imin = p0;
     bool hit = false;

@@ -384,6 +384,17 @@ class HydroSystem:
         self.stress = _PairCall("stresslet", "regularise", self.stress_nodes, self.trg, self.stress_dens,
                                 self.stress_normals, None, None, self.v, P.eta, P.reg, P.eps_dist) \
             if self.nstress else None
+        # the same sum split by target block (fibers | bodies and periphery),
+        # for residuals that take the two blocks in different precisions
+        self.stress_fib = self.stress_rest = None
+        if self.nstress and nF:
+            self.stress_fib = _PairCall("stresslet", "regularise", self.stress_nodes, self.trg[:nF],
+                                        self.stress_dens, self.stress_normals, None, None, self.v[:3 * nF],
+                                        P.eta, P.reg, P.eps_dist)
+            if nB + nS:
+                self.stress_rest = _PairCall("stresslet", "regularise", self.stress_nodes, self.trg[nF:],
+                                             self.stress_dens, self.stress_normals, None, None, self.v[3 * nF:],
+                                             P.eta, P.reg, P.eps_dist)
         if tune:
             self.autotune()
         # ---- right-hand side and preconditioner blocks
@@ -534,11 +545,14 @@ class HydroSystem:
     def autotune(self):
         from . import autotune as at
         P = self.p
-        for call, kind in ((self.oseen, "oseen"), (self.stress, "stresslet")):
+        for call, kind, precs in ((self.oseen, "oseen", ("fp64", "fp32c")),
+                                  (self.stress, "stresslet", ("fp64", "fp32c")),
+                                  (self.stress_fib, "stresslet", ("fp64",)),
+                                  (self.stress_rest, "stresslet", ("fp32c",))):
             if call is None:
                 continue
             a = call.args
-            for prec in ("fp64", "fp32c"):
+            for prec in precs:
                 shp = at.tune(kind, a["src"], a["trg"], a["dens"], a["nrm"], self_mode=a["mode"],
                               src_group=a["gs"], trg_group=a["gt"], precision=prec, eta=P.eta,
                               reg=P.reg, epsilon_distance=P.eps_dist)
@@ -620,10 +634,13 @@ class HydroSystem:
                oseen_done: bool = False) -> torch.Tensor:
         """y = A x (tstep.py:1003-1178).  With `oseen_done` the FP64 Oseen
         flow of x's fiber forces is the one update(x) summed (see
-        :meth:`pending_oseen`)."""
+        :meth:`pending_oseen`).  precision "split": FP64 pair sums on the
+        fiber targets, FP32C stresslet sums on the body and periphery
+        targets (whose rows take the flow with gain 1)."""
         st = _lib.stream_handle(self.device)
         nF, nB, nS = self.nF, self.nB, self.nS
         XT = x[self.o_fib:]
+        split = precision == "split"
         first = True
         if nF:
             if oseen_done:
@@ -631,12 +648,19 @@ class HydroSystem:
             else:
                 _lib.call("f3d_fiber_forces", ctypes.byref(self.fs.c), self.p.E, _lib.ptr(self.geo),
                           _lib.ptr(XT), _lib.ptr(self.fw), nF, 1, st)
-                self.oseen(precision, accumulate=False)
+                self.oseen("fp64" if split else precision, accumulate=False)
             first = False
         if self.nstress:
             _lib.call("f3d_gather_segments", _lib.ptr(x), _lib.ptr(self.stress_dens), _lib.ptr(self.seg[0]),
                       _lib.ptr(self.seg[1]), _lib.ptr(self.seg[2]), self.seg[0].numel(), self.seg_max, st)
-            self.stress(precision, accumulate=not first)
+            if split and self.stress_fib is not None:
+                if first:
+                    self.v.zero_()
+                self.stress_fib("fp64", accumulate=True)
+                if self.stress_rest is not None:
+                    self.stress_rest("fp32c", accumulate=True)
+            else:
+                self.stress("fp32c" if split else precision, accumulate=not first)
             first = False
         if first:
             self.v.zero_()
@@ -733,7 +757,24 @@ class HydroSystem:
                       _lib.ptr(sol[self.o_fib:]), _lib.ptr(f), nF, 0, st)
             fw = torch.empty_like(f)
             _lib.call("f3d_fiber_weight", ctypes.byref(self.fs.c), _lib.ptr(f), _lib.ptr(fw), nF, st)
-            vfib = K.pair_sum("oseen", self.x_fib, g, fw, **kw)
+            vfib = torch.empty(3 * ng, dtype=torch.float64, device=dev)
+            vext = None
+            if self.has_force:
+                # the implicit- and external-force flows over the same pairs: one dual pass
+                fe = torch.empty_like(f)
+                _lib.call("f3d_fiber_weight", ctypes.byref(self.fs.c), _lib.ptr(self.force), _lib.ptr(fe), nF, st)
+                vext = torch.empty_like(vfib)
+                nb = ctypes.c_size_t(0)
+                _lib.call("f3d_oseen_dual_workspace_bytes", nF, ng, None, ctypes.byref(nb))
+                ws = getattr(self, "_grid_ws", None)
+                if ws is None or ws.numel() < nb.value:
+                    # zeroed: the split-sum counters at its start must be zero on entry
+                    ws = self._grid_ws = torch.zeros(max(nb.value, 256), dtype=torch.uint8, device=dev)
+                _lib.call("f3d_oseen_dual", _lib.SELF_MODE["regularise"], _lib.ptr(self.x_fib), _lib.ptr(g),
+                          _lib.ptr(fw), _lib.ptr(fe), None, None, _lib.ptr(vfib), _lib.ptr(vext), nF, ng, P.eta,
+                          P.reg, P.eps_dist, 0, None, _lib.ptr(ws), ws.numel(), st)
+            else:
+                K.pair_sum("oseen", self.x_fib, g, fw, out=vfib, **kw)
             up, up_off = self.fs.upsampling(uprate)
             vself = torch.empty((nF, 3), dtype=torch.float64, device=dev)
             _lib.call("f3d_fiber_self_flow_up", _lib.ptr(self.fs.n), _lib.ptr(self.fs.pt_off),
@@ -742,10 +783,8 @@ class HydroSystem:
             _lib.call("f3d_grid_near_fiber", _lib.ptr(g), ng, _lib.ptr(self.x_fib), _lib.ptr(self.fs.pt_off),
                       self.fs.nfib, _lib.ptr(vself), near, _lib.ptr(vfib), st)
             v += vfib
-            if self.has_force:
-                fe = torch.empty_like(f)
-                _lib.call("f3d_fiber_weight", ctypes.byref(self.fs.c), _lib.ptr(self.force), _lib.ptr(fe), nF, st)
-                K.pair_sum("oseen", self.x_fib, g, fe, out=v, accumulate=True, **kw)
+            if vext is not None:
+                v += vext
         if self.nbody and body0_radius is not None:
             o = self.o_body[0] + 3 * self.nb[0]
             uw = sol[o:o + 6].contiguous()

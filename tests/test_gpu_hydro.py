@@ -165,6 +165,32 @@ def test_fp32c_pair_error_bound(system, golden_step):
         assert dy <= FP32C_PAIR_REL_ERR * system.v_gain * float(torch.linalg.vector_norm(v64))
 
 
+def test_split_residual_bound(system, golden_step):
+    """matvec(precision="split") (FP64 sums on the fiber targets, FP32C
+    stresslet sums on the body and periphery targets) moves the matvec by at
+    most FP32C_PAIR_REL_ERR times the stresslet flow on those targets (their
+    rows take the flow with gain 1) -- the bound the mixed solver uses for
+    its first residual -- with a factor 4 to spare."""
+    from fiber3d_b200.gmres import FP32C_PAIR_REL_ERR
+    nf3 = 3 * system.nF
+    y64 = torch.empty(system.size, dtype=torch.float64, device="cuda")
+    ys = torch.empty_like(y64)
+    for x in golden_step["probe_x"]:
+        xd = torch.tensor(x, device="cuda")
+        system.matvec(xd, y64, "fp64")
+        system.matvec(xd, ys, "split")
+        xs = xd.clone()
+        xs[system.o_fib:] = 0.0  # no fiber forces: v is the stresslet flow alone
+        system.matvec(xs, torch.empty_like(y64), "fp64")
+        vs_rest = float(torch.linalg.vector_norm(system.v[nf3:]))
+        assert vs_rest > 0.0
+        dy = float(torch.linalg.vector_norm(ys - y64))
+        assert dy <= 0.25 * FP32C_PAIR_REL_ERR * vs_rest
+        # the fiber rows see FP64 sums only (split into a launch of their
+        # own, so equal to rounding)
+        assert rel_err(ys[system.o_fib:].cpu().numpy(), y64[system.o_fib:].cpu().numpy()) < 1e-12
+
+
 def test_norm_of_vectors_of_any_length(system):
     """The GMRES workspace's norm reads exactly the vector it is given (the
     mixed solver takes the norm of the pair sums, which are shorter than the
