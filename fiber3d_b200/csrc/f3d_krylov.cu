@@ -361,6 +361,80 @@ __global__ void __launch_bounds__(256) gemv_f16_kernel(const __half *__restrict_
   }
 }
 
+// gemv_f16_kernel with all of x staged once (FP32, cols <= kGemvF16FullX)
+// in a persistent CTA of 1024 threads per SM: no restaging barriers inside
+// the row loop, and 32 warps x 4 rows of 16-byte loads (64 KB) in flight per
+// SM.  Each lane sums its columns in the same order as
+// gemv_f16_kernel<8> (whose x chunks are whole multiples of 32 lanes x 8
+// columns), so the two give the same results.
+constexpr int64_t kGemvF16FullX = 45056;
+
+__global__ void __launch_bounds__(1024, 1) gemv_f16_fullx_kernel(const __half *__restrict__ M, int64_t ld,
+                                                                 const float *__restrict__ row_scale,
+                                                                 const double *__restrict__ diag, int db,
+                                                                 const double *__restrict__ x, double *y,
+                                                                 int64_t rows, int64_t cols) {
+  constexpr int kRowsPerWarp = 4;
+  extern __shared__ __align__(16) float xs_all[];
+  for (int64_t i = threadIdx.x; i < cols; i += blockDim.x) xs_all[i] = static_cast<float>(x[i]);
+  __syncthreads();
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int64_t nwarps = static_cast<int64_t>(gridDim.x) * (blockDim.x >> 5);
+  const int nv = static_cast<int>(cols / 8);
+  for (int64_t grp = static_cast<int64_t>(blockIdx.x) * (blockDim.x >> 5) + warp; grp * kRowsPerWarp < rows;
+       grp += nwarps) {
+    const int64_t rw = grp * kRowsPerWarp;
+    float acc[kRowsPerWarp];
+    const uint4 *rv[kRowsPerWarp];
+#pragma unroll
+    for (int q = 0; q < kRowsPerWarp; ++q) {
+      acc[q] = 0.0f;
+      const int64_t r = rw + q < rows ? rw + q : rows - 1;  // clamped rows are not stored
+      rv[q] = reinterpret_cast<const uint4 *>(M + r * ld);
+    }
+#pragma unroll 1
+    for (int i = lane; i < nv; i += 32) {
+      uint4 u[kRowsPerWarp];
+#pragma unroll
+      for (int q = 0; q < kRowsPerWarp; ++q) u[q] = rv[q][i];
+      const float4 xa = *reinterpret_cast<const float4 *>(xs_all + 8 * i);
+      const float4 xb = *reinterpret_cast<const float4 *>(xs_all + 8 * i + 4);
+#pragma unroll
+      for (int q = 0; q < kRowsPerWarp; ++q) {
+        const float2 f0 = __half22float2(*reinterpret_cast<const __half2 *>(&u[q].x));
+        const float2 f1 = __half22float2(*reinterpret_cast<const __half2 *>(&u[q].y));
+        const float2 f2 = __half22float2(*reinterpret_cast<const __half2 *>(&u[q].z));
+        const float2 f3 = __half22float2(*reinterpret_cast<const __half2 *>(&u[q].w));
+        float a = acc[q];
+        a = fmaf(f0.x, xa.x, a);
+        a = fmaf(f0.y, xa.y, a);
+        a = fmaf(f1.x, xa.z, a);
+        a = fmaf(f1.y, xa.w, a);
+        a = fmaf(f2.x, xb.x, a);
+        a = fmaf(f2.y, xb.y, a);
+        a = fmaf(f3.x, xb.z, a);
+        a = fmaf(f3.y, xb.w, a);
+        acc[q] = a;
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < kRowsPerWarp; ++q) {
+      float a = acc[q];
+#pragma unroll
+      for (int off = 16; off > 0; off >>= 1) a += __shfl_xor_sync(0xffffffffu, a, off);
+      const int64_t r = rw + q;
+      if (lane == 0 && r < rows) {
+        double v = static_cast<double>(a) * static_cast<double>(row_scale[r]);
+        if (db > 0) {
+          const int64_t b0 = (r / db) * db;
+          for (int c = 0; c < db && b0 + c < cols; ++c) v = fma(diag[r * db + c], x[b0 + c], v);
+        }
+        y[r] = v;
+      }
+    }
+  }
+}
+
 __global__ void cast_to_float_kernel(const double *__restrict__ a, float *b, int64_t n) {
   for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
        i += static_cast<int64_t>(gridDim.x) * blockDim.x)
@@ -514,7 +588,20 @@ int f3d_gemv_f16(const void *M16, int64_t ld16, const float *row_scale, const do
   const uintptr_t base = reinterpret_cast<uintptr_t>(M16);
   const bool vec = (base % 16 == 0) && (ld16 % 8 == 0) && (cols % 8 == 0);
   const __half *M = static_cast<const __half *>(M16);
-  if (vec)
+  if (vec && cols <= f3d::kGemvF16FullX) {
+    static bool attr_set[64] = {false};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return F3D_ERR_CUDA;
+    const size_t smem = static_cast<size_t>(cols) * sizeof(float);
+    if (dev < 0 || dev >= 64 || !attr_set[dev]) {
+      if (cudaFuncSetAttribute(f3d::gemv_f16_fullx_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               static_cast<int>(f3d::kGemvF16FullX * sizeof(float))) != cudaSuccess)
+        return F3D_ERR_CUDA;
+      if (dev >= 0 && dev < 64) attr_set[dev] = true;
+    }
+    f3d::gemv_f16_fullx_kernel<<<static_cast<unsigned>(f3d::sm_count()), 1024, smem, st>>>(
+        M, ld16, row_scale, diag, diag_block, x, y, rows, cols);
+  } else if (vec)
     f3d::gemv_f16_kernel<8><<<grid, 256, 0, st>>>(M, ld16, row_scale, diag, diag_block, x, y, rows, cols);
   else
     f3d::gemv_f16_kernel<1><<<grid, 256, 0, st>>>(M, ld16, row_scale, diag, diag_block, x, y, rows, cols);

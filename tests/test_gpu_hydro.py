@@ -92,12 +92,14 @@ def test_preconditioner_inner_precision(golden_step, storage):
         assert rel_err(y.cpu().numpy(), px) < tol
 
 
-def test_gemv_f16_row_scaled():
+@pytest.mark.parametrize("m", [3 * 700, 3 * 704, 3 * 2000])
+def test_gemv_f16_row_scaled(m):
     """FP16 rows scaled by powers of two plus FP64 3x3 diagonal blocks, against
-    an FP64 product, on a matrix whose rows span several decades."""
+    an FP64 product, on a matrix whose rows span several decades (2100
+    columns: the element-wise kernel; 2112 and 6000: 16-byte rows, x staged
+    whole)."""
     from fiber3d_b200 import _lib
     g = torch.Generator(device="cpu").manual_seed(5)
-    m = 3 * 700
     M = torch.randn((m, m), generator=g, dtype=torch.float64) * 1e-4
     M *= torch.logspace(-3, 3, m, dtype=torch.float64)[:, None]
     for i in range(0, m, 3):
