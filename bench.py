@@ -266,7 +266,11 @@ def gpu_arm(args, rank, world, local):
                    "launch_shape": {p: [v.tpt, v.sl, v.nsplit, v.use_tma] for p, v in shapes.items()},
                    "parallelism": f"replicas x{world}"},
         "roofline": {"bound": "fp64", "achieved": achieved / 1e12, "peak": peak64 / 1e12,
-                     "unit": "TFLOP/s", "frac": achieved / peak64, "traffic": None,
+                     "unit": "TFLOP/s", "frac": achieved / peak64,
+                     # DRAM bytes per launch of this kernel on this workload, from an ncu capture
+                     # of it (read 1.391 MB, write 0): the sources stay in L2
+                     "traffic": 1391104 if args.workload == "stresslet_sphere" else None,
+                     "traffic_unit": "bytes per launch (ncu dram__bytes_read.sum + dram__bytes_write.sum)",
                      "note": f"{flop_pair} algorithmic flop per pair (rsqrt not counted); peak = "
                              "measured FP64 FMA rate of this GPU (f3d_probe_fma)",
                      "kernel": f"pair_kernel<{kind}, skip_group, fp64>"},
