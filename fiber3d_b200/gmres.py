@@ -43,6 +43,7 @@ is below tol the solve ends there, else the residual is computed.
 from __future__ import annotations
 
 import ctypes
+import math
 import time
 
 import numpy as np
@@ -222,48 +223,54 @@ class DeviceGMRES:
             prestarted = first_step_done and its == 0
             if not prestarted:
                 self.start_cycle(res, self.beta)
-            H = np.zeros((m + 1, m))
-            cs, sn = np.zeros(m), np.zeros(m)
-            g = np.zeros(m + 1)
-            g[0] = rnorm
+            # Givens rotations and the least-squares solve on the host, in
+            # Python floats (a handful of scalar operations per step)
+            m2 = m + 2
+            hh = self.h_host.numpy()
+            Hc = []            # Hc[k] = column k of the triangular factor (rows 0..k)
+            cs, sn = [], []
+            gv = [rnorm]
             j_done = 0
             for j in range(m):
                 if not (prestarted and j == 0):
                     self._step(matvec, pc, key, use_graph, aux)
                 torch.cuda.current_stream(dev).synchronize()
-                hh = self.h_host.numpy()
-                m2 = m + 2
-                col = hh[:j + 1] + hh[m2:m2 + j + 1]
-                col = np.append(col, hh[j + 1])          # subdiagonal |w|
+                col = (hh[:j + 1] + hh[m2:m2 + j + 1]).tolist()
+                sub = float(hh[j + 1])           # subdiagonal |w|
+                col.append(sub)
                 for i in range(j):
                     t = cs[i] * col[i] + sn[i] * col[i + 1]
                     col[i + 1] = -sn[i] * col[i] + cs[i] * col[i + 1]
                     col[i] = t
-                den = np.hypot(col[j], col[j + 1])
+                den = math.hypot(col[j], col[j + 1])
                 if den == 0.0:
-                    cs[j], sn[j] = 1.0, 0.0
+                    c_, s_ = 1.0, 0.0
                 else:
-                    cs[j], sn[j] = col[j] / den, col[j + 1] / den
+                    c_, s_ = col[j] / den, col[j + 1] / den
+                cs.append(c_)
+                sn.append(s_)
                 col[j] = den
-                col[j + 1] = 0.0
-                g[j + 1] = -sn[j] * g[j]
-                g[j] = cs[j] * g[j]
-                H[:j + 1, j] = col[:j + 1]
+                gv.append(-s_ * gv[j])
+                gv[j] = c_ * gv[j]
+                Hc.append(col[:j + 1])
                 its += 1
                 j_done = j + 1
-                est = abs(g[j + 1]) / bnorm
+                est = abs(gv[j + 1]) / bnorm
                 hist.append(est)
-                if est <= rtol or its >= maxiter or hh[j + 1] == 0.0:
+                if est <= rtol or its >= maxiter or sub == 0.0:
                     break
             # y = H^-1 g ; x += Z y  (= P^-1 (V y))
-            y = np.zeros(j_done)
+            y = [0.0] * j_done
             for i in range(j_done - 1, -1, -1):
-                y[i] = (g[i] - H[i, i + 1:j_done] @ y[i + 1:j_done]) / H[i, i]
+                acc = gv[i]
+                for k in range(i + 1, j_done):
+                    acc -= Hc[k][i] * y[k]
+                y[i] = acc / Hc[i][i]
             if aux is not None:
-                an = self.h_host.numpy()[2 * (m + 2):2 * (m + 2) + j_done + 1]
-                self.last_aux_sum += float(np.sum(np.abs(y) * an[1:j_done + 1]))
+                an = hh[2 * m2:2 * m2 + j_done + 1].tolist()
+                self.last_aux_sum += sum(abs(y[i]) * an[i + 1] for i in range(j_done))
             self.y_done.synchronize()  # the previous upload out of y_host has run
-            self.y_host[:j_done].copy_(torch.from_numpy(y))
+            self.y_host.numpy()[:j_done] = y
             self.y_dev[:j_done].copy_(self.y_host[:j_done], non_blocking=True)
             self.y_done.record()
             _lib.call("f3d_krylov_combine", _lib.ptr(self.Z), n, _lib.ptr(self.y_dev), j_done, _lib.ptr(x), n,
@@ -300,7 +307,6 @@ def solve_system(system, tol=1e-8, restart=100, maxiter=200, x0=None, mixed=Fals
         x, info, its, hist = g.solve(lambda a, o: system.matvec(a, o, "fp64"),
                                      lambda a, o: system.pc(a, o, "fp64"), b, x0=x0, rtol=tol,
                                      maxiter=maxiter, use_graph=use_graph, key="fp64", r0=r0)
-        torch.cuda.synchronize()
         return {"x": x, "info": info, "iterations": its, "history": hist, "refinements": 0,
                 "seconds": time.perf_counter() - t0}
     # mixed: FP32C inner solves; outer residuals FP32C while the bound holds
@@ -419,7 +425,6 @@ def solve_system(system, tol=1e-8, restart=100, maxiter=200, x0=None, mixed=Fals
         if est + bd <= tol:  # the same sum as the convergence test above
             known = (est, bd)
     system._spec_first = x0 is not None and hist[0] > 2.0 * tol
-    torch.cuda.synchronize()
     return {"x": x, "info": info, "iterations": total_its, "history": hist, "refinements": ref,
             "outer_residuals": outer, "fp64_residuals": fp64_residuals, "first_residual_bound": first_bound,
             "seconds": time.perf_counter() - t0}
