@@ -87,9 +87,9 @@ class DeviceGMRES:
         self.y_host = torch.zeros(self.m, dtype=torch.float64).pin_memory()
         self.y_dev = f(self.m)
         self.y_done = torch.cuda.Event()
-        # two norms read back together (|b| and a residual's)
-        self.pair = f(2)
-        self.pair_host = torch.zeros(2, dtype=torch.float64).pin_memory()
+        # norms read back together (|b|, a residual's, the split residual's FP32C flow)
+        self.pair = f(3)
+        self.pair_host = torch.zeros(3, dtype=torch.float64).pin_memory()
         self.graph = {}
         self.last_aux_sum = 0.0
 
@@ -158,9 +158,14 @@ class DeviceGMRES:
                   _lib.ptr(self.V), self.n, self.n, 1, _lib.ptr(self.cur), _lib.stream_handle(self.device))
 
     def read_pair(self):
-        """The two norms in self.pair, on the host (one synchronisation)."""
+        """The first two norms in self.pair, on the host (one synchronisation)."""
+        return self.read_norms()[:2]
+
+    def read_norms(self):
+        """The three norms in self.pair, on the host (one synchronisation)."""
         self.pair_host.copy_(self.pair)
-        return float(self.pair_host[0]), float(self.pair_host[1])
+        h = self.pair_host.tolist()
+        return h[0], h[1], h[2]
 
     # ------------------------------------------------------------- solve ---
     def solve(self, matvec, pc, b: torch.Tensor, x0: torch.Tensor | None = None, rtol=1e-8,
@@ -343,6 +348,7 @@ def solve_system(system, tol=1e-8, restart=100, maxiter=200, x0=None, mixed=Fals
     first_bound = None
     while True:
         bound = 0.0  # bound on |r_computed - r_fp64| / |b|
+        split_pending = False
         if known is not None:
             rel, bound = known
         elif x0 is None and ref == 0:
@@ -362,12 +368,10 @@ def solve_system(system, tol=1e-8, restart=100, maxiter=200, x0=None, mixed=Fals
             if getattr(system, "_stress_fp64", False):
                 system.matvec(x, tmp, "split", oseen_done=True)
                 nf3 = 3 * getattr(system, "nF", 0)
-                bound = FP32C_PAIR_REL_ERR * norm_rel((system.v - system.v2)[nf3:])[0]
-                if bound > 0.5 * tol:
-                    bound = 0.0
-                    system._split_fp64 = True
-                    system.matvec(x, tmp, "fp64", oseen_done=True)
-                    fp64_residuals += 1
+                # the norm stays on the device; it is read together with |r|
+                # below, and the bound decided there
+                g._norm((system.v - system.v2)[nf3:], g.pair[2:3])
+                split_pending = True
             torch.sub(b, tmp, out=r)
         else:
             system.matvec(x, tmp, outer, oseen_done=pending and ref == 0)
@@ -386,16 +390,30 @@ def solve_system(system, tol=1e-8, restart=100, maxiter=200, x0=None, mixed=Fals
             # first one is launched before the host reads |r|, which it takes
             # from the device, so that read does not leave the GPU idle
             spec = ref == 0 and getattr(system, "_spec_first", False)
-            if spec:
+            if spec or split_pending:
                 # |r| goes to pair[1], which the Arnoldi step does not write
-                # (it overwrites beta with the next basis vector's norm)
+                # (it overwrites beta with the next basis vector's norm); |b|,
+                # |r| and the split residual's FP32C flow norm come back in
+                # one read, after the speculative step has been launched
                 g._norm(r, g.pair[1:2])
-                g.start_cycle(r, g.pair[1:2])
-                g._step(mv32, pc32, "fp32c", use_graph, aux=system.v)
-                bn, rnorm = g.read_pair()
+                if spec:
+                    g.start_cycle(r, g.pair[1:2])
+                    g._step(mv32, pc32, "fp32c", use_graph, aux=system.v)
+                bn, rnorm, vrest = g.read_norms()
                 if bnorm is None:
                     bnorm = bn
                 rel = rnorm / bnorm if bnorm > 0.0 else 0.0
+                if split_pending:
+                    bound = FP32C_PAIR_REL_ERR * vrest / bnorm if bnorm > 0.0 else 0.0
+                    if bound > 0.5 * tol:
+                        # too loose: the residual in FP64; a speculative step
+                        # taken on the split residual is dropped
+                        bound, spec = 0.0, False
+                        system._split_fp64 = True
+                        system.matvec(x, tmp, "fp64", oseen_done=True)
+                        fp64_residuals += 1
+                        torch.sub(b, tmp, out=r)
+                        rel, rnorm = norm_rel(r)
             else:
                 rel, rnorm = norm_rel(r)
         known = None
