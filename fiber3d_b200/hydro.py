@@ -586,8 +586,9 @@ class HydroSystem:
         nF, nB, nS = self.nF, self.nB, self.nS
         # explicit flow of the external fiber forces (tstep.py:789-821)
         self.timers.start("fiber2all_explicit_interactions")
-        self.v.zero_()
         self._pending_x0 = None
+        if not (nF and self.has_force):
+            self.v.zero_()  # no explicit flow (else the pass below overwrites v)
         if nF and self.has_force:
             _lib.call("f3d_fiber_weight", ctypes.byref(self.fs.c), _lib.ptr(self.force), _lib.ptr(self.fw), nF, st)
             if x0 is not None:

@@ -281,3 +281,31 @@ def test_oseen_dual_equals_two_sums(L, shape, mode):
                L.ptr(gt), L.ptr(o1), L.ptr(o2), 2000, 1500, 1.0, 5e-3, 1e-5, 0, ctypes.byref(shp), L.ptr(ws),
                ws.numel(), L.stream_handle())
         assert torch.equal(o1, r1) and torch.equal(o2, r2)
+
+
+@pytest.mark.parametrize("ns", [1, 129, 2999])
+@pytest.mark.parametrize("kind", ["oseen", "stresslet", "rotlet"])
+@pytest.mark.parametrize("mode", ["regularise", "skip_index", "skip_group"])
+def test_fp32c_odd_source_counts(K, ns, kind, mode):
+    """FP32C takes sources in pairs; an odd count ends on a padding source
+    whose terms are exactly zero, in every kernel and self mode, in a full
+    tile or a partial one, alone or not."""
+    rng = np.random.default_rng(ns)
+    xs = rng.uniform(-2.0, 2.0, size=(ns, 3))
+    d = rng.normal(size=(ns, 3))
+    n = rng.normal(size=(ns, 3)) if kind == "stresslet" else None
+    if mode == "skip_index":
+        xt = xs
+    else:
+        xt = rng.uniform(-2.0, 2.0, size=(ns + 37, 3))
+    kw = {"self_mode": mode}
+    if mode == "skip_group":
+        kw.update(src_group=np.arange(ns, dtype=np.int32) // 3,
+                  trg_group=(np.arange(xt.shape[0], dtype=np.int32) // 5).astype(np.int32))
+    u64 = K.pair_sum(kind, xs, xt, d, n, **kw).cpu().numpy()
+    u32 = K.pair_sum(kind, xs, xt, d, n, precision="fp32c", **kw).cpu().numpy()
+    assert np.all(np.isfinite(u32))
+    if np.abs(u64).max() == 0.0:
+        assert np.abs(u32).max() == 0.0
+    else:
+        assert rel_err(u32, u64) < TOL32
