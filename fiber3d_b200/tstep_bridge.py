@@ -12,6 +12,14 @@ the same relative tolerance.  It returns ``(solution, info)`` in fiber3d's
 unknown layout, so the rest of ``time_step_hydro`` runs unchanged.
 
 The periphery preconditioner is built once per periphery and reused.
+
+fiber3d starts GMRES from zero (tstep.py:1209).  With
+``warm_start="extrapolate"`` the solver keeps the last three solutions of
+its own calls and starts from their quadratic extrapolation
+(``warmstart.extrapolate``); GMRES still runs to fiber3d's tolerance, so a
+history that does not match the step (a rejected step, a changed system)
+costs iterations, never accuracy.  The history is dropped whenever the
+system size changes.
 """
 from __future__ import annotations
 
@@ -47,10 +55,14 @@ def problem_from_tstep(ts) -> Problem:
 class GpuGmres:
     """Callable with the signature fiber3d uses for ``gmres.gmres``."""
 
-    def __init__(self, ts, mixed: bool = False, restart: int = 100):
+    def __init__(self, ts, mixed: bool = False, restart: int = 100, warm_start: str | None = None):
+        if warm_start not in (None, "extrapolate"):
+            raise ValueError("warm_start must be None or 'extrapolate'")
         self.ts = ts
         self.mixed = mixed
         self.restart = restart
+        self.warm_start = warm_start
+        self._history = []
         self._shell = None
         self.last = None
 
@@ -63,8 +75,17 @@ class GpuGmres:
         if sysd.size != np.size(b):
             raise ValueError(f"system size {sysd.size} != len(b) {np.size(b)}")
         sysd.rhs.copy_(torch.as_tensor(np.asarray(b, dtype=np.float64)))
+        x0 = None
+        if self.warm_start is not None:
+            if self._history and self._history[-1].numel() != sysd.size:
+                self._history = []
+            if self._history:
+                from .warmstart import extrapolate
+                x0 = extrapolate(self._history)
         res = sysd.solve(tol=tol, restart=min(restart or self.restart, 255), maxiter=maxiter or 200,
-                         mixed=self.mixed)
+                         mixed=self.mixed, x0=x0)
+        if self.warm_start is not None:
+            self._history = (self._history + [res["x"]])[-3:]
         if callback is not None:
             for h in res["history"][1:]:
                 callback(h)
@@ -72,10 +93,10 @@ class GpuGmres:
         return res["x"].cpu().numpy(), int(res["info"])
 
 
-def install(ts, mixed: bool = False):
+def install(ts, mixed: bool = False, warm_start: str | None = None):
     """Route fiber3d's GMRES call through the GPU solver for time stepper `ts`."""
     import importlib
     gm = importlib.import_module("bpm_utilities.gmres")
-    solver = GpuGmres(ts, mixed=mixed)
+    solver = GpuGmres(ts, mixed=mixed, warm_start=warm_start)
     gm.gmres = solver
     return solver

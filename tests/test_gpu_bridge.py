@@ -50,3 +50,22 @@ def test_bridge_solves_fibers3d_step(mixed):
     x2, info2 = solver(None, g["rhs"], tol=tol)
     assert solver._shell is shell and info2 == 0
     assert np.array_equal(x, x2)
+
+
+@pytest.mark.parametrize("mixed", [False, True])
+def test_bridge_warm_start(mixed):
+    """With warm_start="extrapolate" a repeated call on the same system starts
+    from the previous solution: no more iterations than the first call, and
+    the same answer to the tolerance."""
+    from fiber3d_b200.tstep_bridge import GpuGmres
+    g = load_golden("step_small.npz")
+    solver = GpuGmres(fake_tstep(g), mixed=mixed, warm_start="extrapolate")
+    tol = float(g["tol"])
+    x1, info1 = solver(None, g["rhs"], tol=tol)
+    its1 = solver.last["iterations"]
+    x2, info2 = solver(None, g["rhs"], tol=tol)
+    assert info1 == 0 and info2 == 0
+    assert solver.last["iterations"] <= its1
+    assert rel_err(x2, g["sol"]) < 1e-7
+    with pytest.raises(ValueError):
+        GpuGmres(fake_tstep(g), warm_start="learned")
