@@ -86,6 +86,7 @@ SIGNATURES: dict[str, list] = {
     "f3d_surface_dense": [_I, _P, _P, _P, _P, _P, _P, _I64, _I64, _D, _D, _D, _P],
     "f3d_rotate_blocks": [_P, _P, _P, _P, ctypes.c_int32, _I, _P],
     "f3d_body_advance": [_P, _P, ctypes.c_int32, _D, _P, _P, _P, _P],
+    "f3d_gemv_batched": [_P, _P, _P, _P, _P, ctypes.c_int32, _I64, _I, _P, _P, _P],
     "f3d_fiber_self_flow_up": [_P, _P, _P, ctypes.c_int32, ctypes.c_int32, _P, _P, _P, _P, ctypes.c_int32, _D, _D,
                                _D, _P, _P],
     "f3d_grid_near_fiber": [_P, _I64, _P, _P, ctypes.c_int32, _P, _D, _P, _P],

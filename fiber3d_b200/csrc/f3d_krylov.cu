@@ -171,17 +171,15 @@ __global__ void bump_kernel(int *kptr) {
 // VEC > 1 each lane loads VEC consecutive elements (16 bytes) per access; the
 // caller guarantees 16-byte aligned rows (ld and cols multiples of VEC).
 template <typename T, int VEC>
-__global__ void __launch_bounds__(256) gemv_kernel(const T *__restrict__ M,
-                                                   const double *__restrict__ x, double *y,
-                                                   int64_t rows, int64_t cols, int64_t ld) {
+__device__ __forceinline__ void gemv_rows(const T *__restrict__ M, const double *__restrict__ x, double *y,
+                                          int64_t rows, int64_t cols, int64_t ld, int64_t bx, int64_t gx) {
   constexpr int kXChunk = 4096;
   constexpr int kRowsPerWarp = 4;
   __shared__ __align__(16) double xs[kXChunk];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int warps = blockDim.x >> 5;
   const int64_t group = static_cast<int64_t>(warps) * kRowsPerWarp;
-  for (int64_t rb = static_cast<int64_t>(blockIdx.x) * group; rb < rows;
-       rb += static_cast<int64_t>(gridDim.x) * group) {
+  for (int64_t rb = bx * group; rb < rows; rb += gx * group) {
     double acc[kRowsPerWarp];
 #pragma unroll
     for (int q = 0; q < kRowsPerWarp; ++q) acc[q] = 0.0;
@@ -233,6 +231,28 @@ __global__ void __launch_bounds__(256) gemv_kernel(const T *__restrict__ M,
       if (lane == 0 && rw + q < rows) y[rw + q] = a;
     }
   }
+}
+
+
+template <typename T, int VEC>
+__global__ void __launch_bounds__(256) gemv_kernel(const T *__restrict__ M,
+                                                   const double *__restrict__ x, double *y,
+                                                   int64_t rows, int64_t cols, int64_t ld) {
+  gemv_rows<T, VEC>(M, x, y, rows, cols, ld, blockIdx.x, gridDim.x);
+}
+
+// count square FP64 matrices in one launch: matrix b (n[b] x n[b], row-major
+// at M + m_off[b]) times x + x_off[b] into y + y_off[b]; blockIdx.y = b.
+template <int VEC>
+__global__ void __launch_bounds__(256) gemv_batched_kernel(const double *__restrict__ M,
+                                                           const int64_t *__restrict__ m_off,
+                                                           const int64_t *__restrict__ n,
+                                                           const int64_t *__restrict__ x_off,
+                                                           const int64_t *__restrict__ y_off,
+                                                           const double *__restrict__ x, double *y) {
+  const int b = blockIdx.y;
+  const int64_t nb = n[b];
+  gemv_rows<double, VEC>(M + m_off[b], x + x_off[b], y + y_off[b], nb, nb, nb, blockIdx.x, gridDim.x);
 }
 
 // Row r of M (cols entries) -> FP16 row of M16 scaled by row_scale[r] = 2^e,
@@ -529,6 +549,24 @@ int f3d_krylov_store(const double *src, const int32_t *k, int32_t offset, double
   if (n <= 0 || ld < n) return F3D_ERR_SHAPE;
   f3d::store_row_kernel<<<f3d::grid_for(n, 256), 256, 0, static_cast<cudaStream_t>(stream)>>>(
       src, k, offset, dst, n, ld);
+  return f3d::launch_status();
+}
+
+int f3d_gemv_batched(const double *M, const int64_t *m_off, const int64_t *n, const int64_t *x_off,
+                     const int64_t *y_off, int32_t count, int64_t max_n, int vec, const double *x, double *y,
+                     void *stream) {
+  if (count < 0 || max_n < 0) return F3D_ERR_SHAPE;
+  if (count == 0 || max_n == 0) return F3D_OK;
+  if (!M || !m_off || !n || !x_off || !y_off || !x || !y) return F3D_ERR_NULL;
+  if (vec && reinterpret_cast<uintptr_t>(M) % 16 != 0) return F3D_ERR_ALIGN;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const int64_t per = std::max<int64_t>(1, std::min<int64_t>((max_n + 31) / 32,
+                                                             (static_cast<int64_t>(f3d::sm_count()) * 4 + count - 1) / count));
+  const dim3 grid(static_cast<unsigned>(per), static_cast<unsigned>(count));
+  if (vec)
+    f3d::gemv_batched_kernel<2><<<grid, 256, 0, st>>>(M, m_off, n, x_off, y_off, x, y);
+  else
+    f3d::gemv_batched_kernel<1><<<grid, 256, 0, st>>>(M, m_off, n, x_off, y_off, x, y);
   return f3d::launch_status();
 }
 

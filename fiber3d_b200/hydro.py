@@ -500,6 +500,14 @@ class HydroSystem:
             _lib.call("f3d_surface_dense", 1, _lib.ptr(ref), _lib.ptr(refn), _lib.ptr(E), _lib.ptr(w),
                       _lib.ptr(origin), _lib.ptr(A), n, 3 * n + 6, P.eta, P.reg, P.eps_dist, st)
             self.body_inv.append(torch.linalg.inv(A))
+        # all body inverses back to back, applied by one batched GEMV
+        m = np.array([3 * n + 6 for n in self.nb], dtype=np.int64)
+        moff = np.concatenate([[0], np.cumsum(m * m)[:-1]]).astype(np.int64)
+        self.body_inv_all = torch.cat([bi.reshape(-1) for bi in self.body_inv]).contiguous()
+        self._binv = [torch.as_tensor(a, device=self.device) for a in
+                      (moff, m, np.array([o - 3 * self.nS for o in self.o_body], dtype=np.int64))]
+        self._binv_max = int(m.max())
+        self._binv_vec = int(bool(np.all(m % 2 == 0)) and bool(np.all(moff % 2 == 0)))
 
     def update(self, x0: torch.Tensor | None = None):
         """Recompute everything that depends on the current geometry (fiber
@@ -690,11 +698,10 @@ class HydroSystem:
             tb.copy_(x[3 * nS:self.o_fib])
             _lib.call("f3d_rotate_blocks", _lib.ptr(tb), _lib.ptr(self.rot_off), _lib.ptr(self.rot_nvec),
                       _lib.ptr(self.body_R), self.nbody, 1, st)
-            for k in range(self.nbody):
-                m = 3 * self.nb[k] + 6
-                o = self.o_body[k] - 3 * nS
-                _lib.call("f3d_gemv", 0, _lib.ptr(self.body_inv[k]), m, _lib.ptr(tb[o:]), _lib.ptr(y[3 * nS + o:]),
-                          m, m, st)
+            moff, m, off = self._binv
+            _lib.call("f3d_gemv_batched", _lib.ptr(self.body_inv_all), _lib.ptr(moff), _lib.ptr(m), _lib.ptr(off),
+                      _lib.ptr(off), self.nbody, self._binv_max, self._binv_vec, _lib.ptr(tb),
+                      _lib.ptr(y[3 * nS:]), st)
             _lib.call("f3d_rotate_blocks", _lib.ptr(y[3 * nS:]), _lib.ptr(self.rot_off), _lib.ptr(self.rot_nvec),
                       _lib.ptr(self.body_R), self.nbody, 0, st)
         if self.nF:

@@ -465,6 +465,16 @@ int f3d_krylov_store(const double *src, const int32_t *k, int32_t offset, double
 int f3d_krylov_scale_into(const double *w, const double *beta, int32_t *k, double *V,
                           int64_t ldv, int64_t n, int bump, double *also, void *stream);
 
+/* count square FP64 products in one launch: y[y_off[b] ..] = M_b x[x_off[b] ..]
+   with M_b the n[b] x n[b] row-major matrix at M + m_off[b] (offsets in
+   doubles, device arrays; max_n >= every n[b]).  vec = 1 reads 16-byte
+   pairs: every m_off[b] and n[b] even and M 16-byte aligned.  Applies the
+   body-frame inverses of all rigid bodies' preconditioner blocks at once
+   (fiber3d's A_inv_bodies, tstep/tstep.py:966-981). */
+int f3d_gemv_batched(const double *M, const int64_t *m_off, const int64_t *n, const int64_t *x_off,
+                     const int64_t *y_off, int32_t count, int64_t max_n, int vec, const double *x, double *y,
+                     void *stream);
+
 /* y = M x for a row-major rows x cols matrix stored as float64
    (precision F3D_FP64) or float32 (F3D_FP32C); the sum is float64.  Applies
    the explicit inverse of the periphery operator (tstep/tstep.py:957-958). */
