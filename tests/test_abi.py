@@ -78,3 +78,32 @@ def test_workspace_query_and_argument_checks(dll):
     # skip-index needs ns == nt
     assert dll.f3d_pair_sum(0, 0, 1, 8, 8, 8, None, None, None, 8, 10, 11, 1.0, 5e-3, 1e-5, 0,
                             None, None, 0, None) == 2
+
+
+def test_argument_checks_of_newer_entries(dll):
+    """Shape, null-pointer and size checks of the body advance, batched
+    GEMV and grid-velocity entries return before any launch."""
+    NULL, SHAPE, TOO_LARGE = 1, 2, 10
+    # nothing to do: OK without a device
+    assert dll.f3d_body_advance(None, None, 0, 1e-3, None, None, None, None) == 0
+    assert dll.f3d_gemv_batched(None, None, None, None, None, 0, 10, 0, None, None, None) == 0
+    assert dll.f3d_grid_near_fiber(None, 0, None, None, 5, None, 0.2, None, None) == 0
+    assert dll.f3d_grid_rigid_override(None, 0, None, None, 0.5, None, None) == 0
+    assert dll.f3d_fiber_self_flow_up(None, None, None, 0, 32, None, None, None, None, 2, 1.0, 5e-3, 1e-5,
+                                      None, None) == 0
+    # negative sizes and null pointers with work to do
+    assert dll.f3d_body_advance(None, None, -1, 1e-3, None, None, None, None) == SHAPE
+    assert dll.f3d_body_advance(None, None, 2, 1e-3, None, None, None, None) == NULL
+    assert dll.f3d_gemv_batched(None, None, None, None, None, -1, 10, 0, None, None, None) == SHAPE
+    assert dll.f3d_gemv_batched(None, None, None, None, None, 2, 10, 0, None, None, None) == NULL
+    assert dll.f3d_grid_near_fiber(None, -1, None, None, 5, None, 0.2, None, None) == SHAPE
+    assert dll.f3d_grid_near_fiber(None, 10, None, None, 5, None, 0.2, None, None) == NULL
+    assert dll.f3d_grid_rigid_override(None, 10, None, None, 0.5, None, None) == NULL
+    assert dll.f3d_fiber_self_flow_up(None, None, None, 3, 32, None, None, None, None, 0, 1.0, 5e-3, 1e-5,
+                                      None, None) == SHAPE
+    assert dll.f3d_fiber_self_flow_up(None, None, None, 3, 32, None, None, None, None, 2, 1.0, 5e-3, 1e-5,
+                                      None, None) == NULL
+    # shared-memory limit of the self-flow kernel: rejected before any launch
+    # (the pointers are placeholders that the check never dereferences)
+    p = ctypes.c_void_p(256)
+    assert dll.f3d_fiber_self_flow_up(p, p, p, 3, 1024, p, p, p, p, 2, 1.0, 5e-3, 1e-5, p, None) == TOO_LARGE
