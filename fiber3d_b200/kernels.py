@@ -14,8 +14,12 @@ point at this module and the unmodified time stepper runs on the GPU.
   ``libfiber3d_b200.so``; there is no CPU path.
 
 Keyword-only extensions (not in fiber3d): ``precision`` ('fp64' default or
-'fp32c') and ``shape`` (a :class:`fiber3d_b200._lib.PairShape` launch shape,
-normally chosen by :mod:`fiber3d_b200.autotune`).
+'fp32c') and ``shape`` (a :class:`fiber3d_b200._lib.PairShape` launch shape).
+Without ``shape`` the pair-sum drop-ins take the launch shape
+:mod:`fiber3d_b200.autotune` found for the sum's kernel, mode and size
+bucket, timing the candidates on the first call of a bucket (tens of
+milliseconds, once per bucket and GPU model; cached on disk) while
+``AUTOTUNE`` is true, else the library's default shape.
 """
 from __future__ import annotations
 
@@ -35,6 +39,10 @@ __all__ = [
 ]
 
 
+# Launch shapes of the pair-sum drop-ins come from the autotuner (see above).
+AUTOTUNE = True
+
+
 # ------------------------------------------------------------------ helpers --
 def _device() -> torch.device:
     _lib.lib()  # raises if no CUDA device or no library
@@ -46,7 +54,9 @@ def _to_dev(x, dev: torch.device, name: str) -> torch.Tensor:
     if isinstance(x, torch.Tensor):
         t = x.detach()
         if t.device != dev or t.dtype != torch.float64:
-            t = t.to(device=dev, dtype=torch.float64)
+            # from page-locked memory the copy is queued on the stream like
+            # the kernel that reads it; the result comes back synchronously
+            t = t.to(device=dev, dtype=torch.float64, non_blocking=t.device.type == "cpu" and t.is_pinned())
     else:
         a = np.ascontiguousarray(np.asarray(x, dtype=np.float64))
         t = torch.from_numpy(a).to(dev)
@@ -85,7 +95,7 @@ def pair_sum(kernel: str, r_source, r_target, density, normal=None, *, eta=1.0, 
     """
     dev = _device()
     rs = _to_dev(r_source, dev, "r_source")
-    rt = _to_dev(r_target, dev, "r_target")
+    rt = rs if r_target is r_source else _to_dev(r_target, dev, "r_target")
     d = _to_dev(density, dev, "density")
     if d.shape[0] != rs.shape[0]:
         raise ValueError(f"density has {d.shape[0]} points, r_source has {rs.shape[0]}")
@@ -121,51 +131,63 @@ def pair_sum(kernel: str, r_source, r_target, density, normal=None, *, eta=1.0, 
     return out
 
 
+def _drop_in(kernel, r_source, r_target, density, normal, self_mode, eta, reg, epsilon_distance,
+             precision, shape):
+    """A pair-sum drop-in: inputs to the device once, the autotuned launch
+    shape unless one is given, the sum, the output back like the inputs."""
+    host = _any_host(r_source, r_target, density, normal)
+    dev = _device()
+    rs = _to_dev(r_source, dev, "r_source")
+    rt = rs if r_target is r_source else _to_dev(r_target, dev, "r_target")
+    d = _to_dev(density, dev, "density")
+    n = _to_dev(normal, dev, "normal") if normal is not None else None
+    if shape is None and AUTOTUNE and rs.shape[0] and rt.shape[0]:
+        from . import autotune
+        shape = autotune.tune(kernel, rs, rt, d, n, self_mode=self_mode, precision=precision, eta=eta,
+                              reg=reg, epsilon_distance=epsilon_distance)
+    u = pair_sum(kernel, rs, rt, d, n, eta=eta, reg=reg, epsilon_distance=epsilon_distance,
+                 self_mode=self_mode, precision=precision, shape=shape)
+    return _out(u, host)
+
+
 # ------------------------------------------------------------ pair sums ----
 def oseen_kernel_source_target_numba(r_source, r_target, density, eta=1.0, reg=5e-3,
                                      epsilon_distance=1e-5, *, precision="fp64", shape=None):
     """u_t = 1/(8 pi eta) sum_s [f_s/r + (r.f_s) r/r^3], r = x_t - x_s; pairs with
     r < epsilon_distance use sqrt(r^2 + reg^2).  fiber3d kernels.py:794-846."""
-    u = pair_sum("oseen", r_source, r_target, density, eta=eta, reg=reg,
-                 epsilon_distance=epsilon_distance, precision=precision, shape=shape)
-    return _out(u, _any_host(r_source, r_target, density))
+    return _drop_in("oseen", r_source, r_target, density, None, "regularise", eta, reg, epsilon_distance,
+                    precision, shape)
 
 
 def oseen_kernel_times_density_numba(r_vectors, density, eta=1.0, reg=5e-3,
                                      epsilon_distance=1e-5, *, precision="fp64", shape=None):
     """Oseen sum over one point set with the pair j == i skipped (other close
     pairs regularised).  fiber3d kernels.py:214-287."""
-    u = pair_sum("oseen", r_vectors, r_vectors, density, eta=eta, reg=reg,
-                 epsilon_distance=epsilon_distance, self_mode="skip_index",
-                 precision=precision, shape=shape)
-    return _out(u, _any_host(r_vectors, density))
+    return _drop_in("oseen", r_vectors, r_vectors, density, None, "skip_index", eta, reg, epsilon_distance,
+                    precision, shape)
 
 
 def rotlet_kernel_source_target_numba(r_source, r_target, density, eta=1.0, reg=5e-3,
                                       epsilon_distance=1e-5, *, precision="fp64", shape=None):
     """u_t = 1/(8 pi eta) sum_s tau_s x r / r^3.  fiber3d kernels.py:856-908."""
-    u = pair_sum("rotlet", r_source, r_target, density, eta=eta, reg=reg,
-                 epsilon_distance=epsilon_distance, precision=precision, shape=shape)
-    return _out(u, _any_host(r_source, r_target, density))
+    return _drop_in("rotlet", r_source, r_target, density, None, "regularise", eta, reg, epsilon_distance,
+                    precision, shape)
 
 
 def stresslet_kernel_source_target_numba(r_source, r_target, normal, density, eta=1.0,
                                          reg=5e-3, epsilon_distance=1e-5, *, precision="fp64",
                                          shape=None):
     """v_t = -3/(4 pi eta) sum_s (r.d_s)(r.n_s) r / r^5.  fiber3d kernels.py:1186-1217."""
-    u = pair_sum("stresslet", r_source, r_target, density, normal, eta=eta, reg=reg,
-                 epsilon_distance=epsilon_distance, precision=precision, shape=shape)
-    return _out(u, _any_host(r_source, r_target, normal, density))
+    return _drop_in("stresslet", r_source, r_target, density, normal, "regularise", eta, reg,
+                    epsilon_distance, precision, shape)
 
 
 def stresslet_kernel_times_normal_times_density_numba(r_vectors, normal, density, eta=1.0,
                                                       reg=5e-3, epsilon_distance=1e-5, *,
                                                       precision="fp64", shape=None):
     """Stresslet sum over one point set, j == i skipped.  fiber3d kernels.py:1123-1183."""
-    u = pair_sum("stresslet", r_vectors, r_vectors, density, normal, eta=eta, reg=reg,
-                 epsilon_distance=epsilon_distance, self_mode="skip_index",
-                 precision=precision, shape=shape)
-    return _out(u, _any_host(r_vectors, normal, density))
+    return _drop_in("stresslet", r_vectors, r_vectors, density, normal, "skip_index", eta, reg,
+                    epsilon_distance, precision, shape)
 
 
 def complementary_kernel_times_density_numba(r_vectors, normal, density):
