@@ -58,7 +58,7 @@ def _save():
     try:
         p = _path()
         p.parent.mkdir(parents=True, exist_ok=True)
-        tmp = p.with_suffix(".tmp")
+        tmp = p.with_suffix(f".{os.getpid()}.tmp")  # one per process: ranks may write at once
         tmp.write_text(json.dumps(_cache, indent=1, sort_keys=True))
         tmp.replace(p)
     except OSError:
