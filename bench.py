@@ -543,6 +543,101 @@ def hydro_arm(args, rank, world, local, warmup=None, steps=None, emit=True):
     return line
 
 
+def _quadrature_problem(args):
+    from scipy.spatial import ConvexHull
+    from fiber3d_b200 import geometry
+    nodes, _ = geometry.fibonacci_sphere(args.nshell, args.shell_radius)
+    tri = ConvexHull(nodes).simplices.astype(np.int32)
+    return nodes, tri, 2.0 * nodes  # gradh of |x|^2 - R^2 (shape_gallery's sphere)
+
+
+def cpu_quadrature_rate(nodes, tri, grad, seconds: float):
+    """Triangles/s of the CPU restatement (oracle/quadrature.py: the
+    neighbour search, the local system and LAPACK's solve of each triangle)
+    on consecutive triangles for about `seconds`."""
+    from oracle import quadrature as OQ
+    ts = np.sort(tri, axis=1)
+    tn = OQ.triangle_normals(nodes, ts)
+    en = OQ.edge_normals(ts, tn)
+    mids = (nodes[ts[:, 0]] + nodes[ts[:, 1]] + nodes[ts[:, 2]]) / 3
+    done, t0 = 0, time.perf_counter()
+    while time.perf_counter() - t0 < seconds or done == 0:
+        s = done % len(ts)
+        nni = OQ.nearest_neighbors(nodes, mids[s:s + 64])
+        for k in range(len(nni)):
+            M, r, d = OQ.triangle_system(nodes, grad, ts[s + k], tn[s + k], en[s + k], nni[k])
+            np.linalg.solve(M, r)
+        done += len(nni)
+    return done / (time.perf_counter() - t0), done
+
+
+def quadrature_arm(args, rank, world, local):
+    """RBF surface quadrature of the periphery (fiber3d's set-up step,
+    quadratures/Smooth_Closed_Surface_Quadrature_RBF.py with the exact
+    gradient, tstep/tstep.py:285-300): args.nshell nodes of shape_gallery's
+    sphere of radius args.shell_radius, triangles from scipy's ConvexHull.  A
+    step is one full call: triangle preparation, edge normals, the 80-nearest
+    search, the 116 x 116 local solves and the per-node sums."""
+    import torch
+    from fiber3d_b200 import quadrature as Qd, replicas
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    nodes, tri, grad = _quadrature_problem(args)
+    X = torch.as_tensor(nodes, device=dev)
+    T = torch.as_tensor(tri, device=dev)
+    G = torch.as_tensor(grad, device=dev)
+    for _ in range(args.warmup):
+        Qd.surface_quadrature_weights(X, T, G)
+    times = []
+    with ClockSampler(local) as clk:
+        replicas.barrier()
+        for _ in range(args.steps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            w = Qd.surface_quadrature_weights(X, T, G)
+            e1.record()
+            e1.synchronize()
+            times.append(e0.elapsed_time(e1))
+        replicas.barrier()
+    ms = replicas.max_over_ranks([statistics.median(times)], dev)[0]
+    # end to end from host arrays, as fiber3d calls it
+    e2e = []
+    for _ in range(max(3, args.steps // 2)):
+        t0 = time.perf_counter()
+        wh = Qd.surface_quadrature_weights(nodes, tri, grad, device=dev).cpu().numpy()
+        e2e.append((time.perf_counter() - t0) * 1e3)
+    ntri = len(tri)
+    # LU of the 116 x 116 system with the right-hand side appended:
+    # sum_{m<116} m (m + 1) multiply-adds per triangle
+    flops = 2.0 * sum(m * (m + 1) for m in range(116)) * ntri
+    R = args.shell_radius
+    line = {"metric": "surface quadrature set-up (ms)", "value": ms, "unit": "ms", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (shape_gallery sphere)",
+            "config": {"workload": "surface_quadrature", "nodes": int(args.nshell), "triangles": int(ntri),
+                       "radius": R, "neighbors": 80, "poly_order": 7, "l2": "inputs 0.9 MB, L2-resident"},
+            "roofline": {"bound": "fp64", "achieved": flops / (ms * 1e-3) / 1e12, "peak": 33.5,
+                         "unit": "TFLOP/s", "frac": flops / (ms * 1e-3) / 1e12 / 33.5, "traffic": None,
+                         "note": "algorithmic LU flops over the whole call (all eight kernels); "
+                                 "peak = measured FP64 FMA rate"},
+            "e2e": {"value": statistics.median(e2e), "unit": "ms",
+                    "h2d_bytes_per_step": int(nodes.nbytes + grad.nbytes + tri.nbytes),
+                    "d2h_bytes_per_step": int(wh.nbytes)},
+            "gpu_launches": 8 * args.steps,
+            "clocks": clk.summary(),
+            "checks": {"area_rel_err": float(wh.sum() / (4 * np.pi * R * R) - 1),
+                       "x2_rel_err": float((wh * nodes[:, 0] ** 2).sum() / (4 * np.pi * R ** 4 / 3) - 1),
+                       "bitwise_repeatable": bool(torch.equal(w, Qd.surface_quadrature_weights(X, T, G)))}}
+    if rank == 0 and world == 1:
+        rate, done = cpu_quadrature_rate(nodes, tri, grad, args.cpu_seconds)
+        line["cpu_baseline"] = {"value": ntri / rate * 1e3, "unit": "ms", "cores": 1, "kind": "port",
+                                "sample": f"{done} of {ntri} triangles, extrapolated; numpy/LAPACK "
+                                          "restatement (fiber3d's own loop ran 4.8 ms per triangle here)"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    return line
+
+
 def block_pc_arm(args, rank, world, local):
     """Batched block-diagonal preconditioner: 2000 fibers with point counts
     uniform in {16, 24, 32, 48, 64} (geometry of the step workload), their
@@ -635,7 +730,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="stresslet_sphere",
-                    choices=["stresslet_sphere", "oseen_fibers", "hydro_step", "block_pc"])
+                    choices=["stresslet_sphere", "oseen_fibers", "hydro_step", "block_pc",
+                             "surface_quadrature"])
     ap.add_argument("--nblocks", type=int, default=2000)
     ap.add_argument("--train-seeds", type=int, nargs="*", default=list(range(11, 19)))
     ap.add_argument("--train-steps", type=int, default=40)
@@ -670,6 +766,8 @@ def main():
             hydro_arm(args, rank, world, local)
         elif args.workload == "block_pc":
             block_pc_arm(args, rank, world, local)
+        elif args.workload == "surface_quadrature":
+            quadrature_arm(args, rank, world, local)
         else:
             gpu_arm(args, rank, world, local)
     finally:

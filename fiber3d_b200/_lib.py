@@ -91,6 +91,8 @@ SIGNATURES: dict[str, list] = {
                                _D, _P, _P],
     "f3d_grid_near_fiber": [_P, _I64, _P, _P, ctypes.c_int32, _P, _D, _P, _P],
     "f3d_grid_rigid_override": [_P, _I64, _P, _P, _D, _P, _P],
+    "f3d_surface_quadrature_workspace_bytes": [_I64, _I64, ctypes.POINTER(_SZ)],
+    "f3d_surface_quadrature": [_P, _I64, _P, _I64, _P, _P, _P, _P, _SZ, _P],
     "f3d_rigid_body_update": [_P, _P, _P, _P, _P, _P, _I64, _P, _P, _P, _P],
     "f3d_gather_segments": [_P, _P, _P, _P, _P, ctypes.c_int32, _I64, _P],
     "f3d_krylov_workspace_bytes": [_I64, ctypes.c_int32, ctypes.POINTER(_SZ)],

@@ -547,6 +547,23 @@ int f3d_adam(float *p, const float *g, float *m, float *v, int64_t n, float lr, 
 int f3d_mse_grad(const float *Y, const float *T, float *D, float *row_loss, int32_t M, int32_t N,
                  void *stream);
 
+/* ---- surface quadrature (set-up) ------------------------------------------
+   Replaces Smooth_Closed_Surface_Quadrature_RBF(nodes, triangles, h, gradh)
+   (python/quadratures/Smooth_Closed_Surface_Quadrature_RBF.py:3-470), the
+   branch with the exact surface gradient that every fiber3d caller takes
+   (tstep/tstep.py:297-300, body/body.py:104-107): phs RBF r^7 plus degree-7
+   polynomials on the 80 nodes nearest each triangle, projected onto the
+   triangle's plane.  nodes (n x 3), gradient (n x 3, gradh at the nodes),
+   triangles (ntri x 3, any vertex order; a closed surface, every edge shared
+   by exactly two triangles) -> weights (n).  neighbors (ntri x 80, nearest
+   first) receives each triangle's nodes when non-NULL.  80 <= n <= 26000.
+   Bad triangulations and zero pivots are reported through the device error
+   word (F3D_ERR_ARG, F3D_ERR_SINGULAR; f3d_get_device_error). */
+int f3d_surface_quadrature_workspace_bytes(int64_t n, int64_t ntri, size_t *bytes);
+int f3d_surface_quadrature(const double *nodes, int64_t n, const int32_t *triangles, int64_t ntri,
+                           const double *gradient, double *weights, int32_t *neighbors, void *workspace,
+                           size_t workspace_bytes, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
