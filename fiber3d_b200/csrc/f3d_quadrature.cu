@@ -17,10 +17,10 @@
 //   4. quad_triangle: per triangle, the projection onto the triangle's plane
 //      (:162-236), the exact integrals of r^7 (:262-309) and of the degree-7
 //      monomials (:473-622, here by Gauss-Legendre on Green's-theorem line
-//      integrals) and the 116 x 116 saddle-point solve (:334-336), LU with
-//      partial pivoting held in registers (16 x 16 threads, an 8 x 8 tile
-//      each), the right-hand side eliminated along as column 116; then the
-//      area-element distortion (:431-447).
+//      integrals) and the 116 x 116 saddle-point solve (:334-336),
+//      Gauss-Jordan elimination with partial pivoting held in registers
+//      (16 x 16 threads, an 8 x 8 tile each), the right-hand side carried
+//      along as column 116; then the area-element distortion (:431-447).
 //   5. quad_count / quad_scan / quad_fill / quad_sum: the per-node sum of the
 //      triangle weights in triangle order (:460-468), deterministic.
 #include <algorithm>
@@ -302,12 +302,126 @@ struct TriShared {
   double ys[128];
   double x[kQuadDim];
   double piv[kQuadDim];
+  double recip[kQuadDim];
   int order[kQuadDim];
   int where[128];
   double xp[3], rot[9], shift[2], v[3][2], height;
   int prow;
-  double recip;
 };
+
+// The pivot row's entries in register columns KB..7 go to S.u (u_j = 0 for
+// j <= k in column block KB).
+template <int KB>
+__device__ __forceinline__ void stage_row(const double (&row)[8], TriShared &S, int tx, int k) {
+  const int j = tx + 16 * KB;
+  S.u[j] = j > k ? row[KB] : 0.0;
+#pragma unroll
+  for (int b = KB + 1; b < 8; ++b) S.u[tx + 16 * b] = row[b];
+}
+
+// Pivot of column k (register column C of the threads with tx == k % 16,
+// one half-warp): the largest |a_ik| over the rows not yet pivoted (`used`:
+// bit a for row ty + 16 a), the first in the current row order on ties
+// (LAPACK's choice); its lane stores the pivot and its reciprocal, lane 0
+// exchanges the rows.
+template <int C>
+__device__ __forceinline__ void pivot_column(const double (&M)[8][8], TriShared &S, unsigned used, int k, int ty,
+                                             int tx, int *err) {
+  const unsigned half = (tx & 1) ? 0xffff0000u : 0x0000ffffu;
+  double best = -1.0, mine = 0.0;
+  int ia = -1;
+#pragma unroll
+  for (int a = 0; a < 8; ++a) {
+    const int i = ty + 16 * a;
+    if (i < kQuadDim && !((used >> a) & 1u)) {
+      const double av = fabs(M[a][C]);
+      if (av > best || (av == best && S.where[i] < S.where[ty + 16 * ia])) best = av, ia = a, mine = M[a][C];
+    }
+  }
+  int bpos = ia >= 0 ? S.where[ty + 16 * ia] : 0x7fffffff;
+  const int my_pos = bpos;
+  const double my_recip = 1.0 / mine;  // formed while the reduction runs
+#pragma unroll
+  for (int o = 8; o > 0; o >>= 1) {
+    const double ob = __shfl_xor_sync(half, best, o, 16);
+    const int op = __shfl_xor_sync(half, bpos, o, 16);
+    if (ob > best || (ob == best && op < bpos)) best = ob, bpos = op;
+  }
+  if (my_pos == bpos && bpos != 0x7fffffff) {
+    S.piv[k] = mine;
+    S.recip[k] = my_recip;
+  }
+  __syncwarp(half);
+  if (ty == 0) {
+    if (!(best > 0.0)) {
+      record_error(err, F3D_ERR_SINGULAR);
+      bpos = k;
+      S.piv[k] = 1.0;
+      S.recip[k] = 1.0;
+    }
+    const int rk = S.order[k], rp = S.order[bpos];
+    S.order[k] = rp, S.order[bpos] = rk;
+    S.where[rp] = k, S.where[rk] = bpos;
+    S.prow = rp;
+  }
+}
+
+// Gauss-Jordan steps k = 16 KB .. 16 KB + ncol - 1 (the pivot of step k
+// already chosen): every row but the pivot row loses l_i = a_ik / a_pk times
+// the pivot row, so that after the last step row order[k] holds u_kk in
+// column k and y_k in column 116, and x_k = y_k / u_kk (no back
+// substitution).  Columns up to k are left as they are.  The pivot column is
+// register column KB of the threads with tx == k % 16: a static index, so it
+// never leaves registers; column blocks before KB are skipped.  After its own
+// update, the half-warp that owns column k + 1 chooses that column's pivot
+// while the other warps finish theirs.
+template <int KB>
+__device__ __forceinline__ void gj_columns(double (&M)[8][8], TriShared &S, unsigned &used, int ncol, int ty, int tx,
+                                           int *err) {
+  for (int kk = 0; kk < ncol; ++kk) {
+    const int k = 16 * KB + kk;
+    const int prow = S.prow;
+    if (ty == (prow & 15)) used |= 1u << (prow >> 4);
+    if (tx == kk) {
+      const double r = S.recip[k];
+#pragma unroll
+      for (int a = 0; a < 8; ++a) {
+        const int i = ty + 16 * a;
+        S.l[i] = (i < kQuadDim && i != prow) ? M[a][KB] * r : 0.0;
+      }
+    }
+    if (ty == (prow & 15)) {
+      switch (prow >> 4) {
+        case 0: stage_row<KB>(M[0], S, tx, k); break;
+        case 1: stage_row<KB>(M[1], S, tx, k); break;
+        case 2: stage_row<KB>(M[2], S, tx, k); break;
+        case 3: stage_row<KB>(M[3], S, tx, k); break;
+        case 4: stage_row<KB>(M[4], S, tx, k); break;
+        case 5: stage_row<KB>(M[5], S, tx, k); break;
+        case 6: stage_row<KB>(M[6], S, tx, k); break;
+        default: stage_row<KB>(M[7], S, tx, k); break;
+      }
+    }
+    __syncthreads();
+    double ur[8 - KB];
+#pragma unroll
+    for (int b = KB; b < 8; ++b) ur[b - KB] = S.u[tx + 16 * b];
+#pragma unroll
+    for (int a = 0; a < 8; ++a) {
+      const double lr = -S.l[ty + 16 * a];
+#pragma unroll
+      for (int b = KB; b < 8; ++b) M[a][b] = fma(lr, ur[b - KB], M[a][b]);
+    }
+    if (k + 1 < kQuadDim) {
+      if (kk + 1 < 16) {
+        if (tx == kk + 1) pivot_column<KB>(M, S, used, k + 1, ty, tx, err);
+      } else if constexpr (KB < 7) {
+        if (tx == 0) pivot_column<KB + 1>(M, S, used, k + 1, ty, tx, err);
+      }
+    }
+    __syncthreads();
+  }
+}
 
 __global__ void __launch_bounds__(kTriThreads, 1) quad_triangle_kernel(const double *__restrict__ X,
                                                                        const double *__restrict__ grad, int ntri,
@@ -488,105 +602,25 @@ __global__ void __launch_bounds__(kTriThreads, 1) quad_triangle_kernel(const dou
       }
     }
 
-    // LU with partial pivoting (rows stay in place; order/where hold the
-    // row exchanges), the right-hand side eliminated along
-    for (int k = 0; k < kQuadDim; ++k) {
-      const int bk = k >> 4;
-      if (tx == (k & 15)) {
-        double best = -1.0, bval = 0.0;
-        int bpos = 0x7fffffff;
-#pragma unroll
-        for (int a = 0; a < 8; ++a) {
-          const int i = ty + 16 * a;
-          double v = 0.0;
-#pragma unroll
-          for (int b = 0; b < 8; ++b) v = (b == bk) ? M[a][b] : v;
-          if (i < kQuadDim) {
-            const int pos = S.where[i];
-            const double av = fabs(v);
-            if (pos >= k && (av > best || (av == best && pos < bpos))) best = av, bval = v, bpos = pos;
-          }
-        }
-        const unsigned half = (tx & 1) ? 0xffff0000u : 0x0000ffffu;  // this column's half-warp
-#pragma unroll
-        for (int o = 8; o > 0; o >>= 1) {
-          const double ob = __shfl_xor_sync(half, best, o, 16);
-          const double ov = __shfl_xor_sync(half, bval, o, 16);
-          const int op = __shfl_xor_sync(half, bpos, o, 16);
-          if (ob > best || (ob == best && op < bpos)) best = ob, bval = ov, bpos = op;
-        }
-        if (ty == 0) {
-          if (!(best > 0.0)) {
-            record_error(err, F3D_ERR_SINGULAR);
-            bpos = k;
-            bval = 1.0;
-          }
-          const int rk = S.order[k], rp = S.order[bpos];
-          S.order[k] = rp, S.order[bpos] = rk;
-          S.where[rp] = k, S.where[rk] = bpos;
-          S.prow = rp;
-          S.piv[k] = bval;
-          S.recip = 1.0 / bval;
-        }
-      }
-      __syncthreads();
-      const int prow = S.prow;
-      if (tx == (k & 15)) {
-#pragma unroll
-        for (int a = 0; a < 8; ++a) {
-          const int i = ty + 16 * a;
-          double v = 0.0;
-#pragma unroll
-          for (int b = 0; b < 8; ++b) v = (b == bk) ? M[a][b] : v;
-          S.l[i] = (i < kQuadDim && S.where[i] > k) ? v * S.recip : 0.0;
-        }
-      }
-      if (ty == (prow & 15)) {
-        const int ap = prow >> 4;
-#pragma unroll
-        for (int b = 0; b < 8; ++b) {
-          const int j = tx + 16 * b;
-          double v = 0.0;
-#pragma unroll
-          for (int a = 0; a < 8; ++a) v = (a == ap) ? M[a][b] : v;
-          S.u[j] = (j > k && j <= kQuadRhsCol) ? v : 0.0;
-        }
-      }
-      __syncthreads();
-      double lr[8], ur[8];
-#pragma unroll
-      for (int a = 0; a < 8; ++a) lr[a] = -S.l[ty + 16 * a];
-#pragma unroll
-      for (int b = 0; b < 8; ++b) ur[b] = S.u[tx + 16 * b];
-#pragma unroll
-      for (int a = 0; a < 8; ++a)
-#pragma unroll
-        for (int b = 0; b < 8; ++b) M[a][b] = fma(lr[a], ur[b], M[a][b]);
-    }
-
-    // back substitution on U x = y (column 116 holds y)
+    // Gauss-Jordan elimination with partial pivoting (rows stay in place;
+    // order/where hold the row exchanges), the right-hand side carried along
+    unsigned used = 0;
+    if (tx == 0) pivot_column<0>(M, S, used, 0, ty, tx, err);
+    __syncthreads();
+    gj_columns<0>(M, S, used, 16, ty, tx, err);
+    gj_columns<1>(M, S, used, 16, ty, tx, err);
+    gj_columns<2>(M, S, used, 16, ty, tx, err);
+    gj_columns<3>(M, S, used, 16, ty, tx, err);
+    gj_columns<4>(M, S, used, 16, ty, tx, err);
+    gj_columns<5>(M, S, used, 16, ty, tx, err);
+    gj_columns<6>(M, S, used, 16, ty, tx, err);
+    gj_columns<7>(M, S, used, kQuadDim - 112, ty, tx, err);
     if (tx == (kQuadRhsCol & 15)) {
 #pragma unroll
       for (int a = 0; a < 8; ++a) S.ys[ty + 16 * a] = M[a][kQuadRhsCol >> 4];
     }
     __syncthreads();
-    for (int k = kQuadDim - 1; k >= 0; --k) {
-      if (tid == 0) S.x[k] = S.ys[S.order[k]] / S.piv[k];
-      __syncthreads();
-      if (tx == (k & 15)) {
-        const int bk = k >> 4;
-        const double xk = S.x[k];
-#pragma unroll
-        for (int a = 0; a < 8; ++a) {
-          const int i = ty + 16 * a;
-          double v = 0.0;
-#pragma unroll
-          for (int b = 0; b < 8; ++b) v = (b == bk) ? M[a][b] : v;
-          if (i < kQuadDim && S.where[i] < k) S.ys[i] = fma(-xk, v, S.ys[i]);
-        }
-      }
-      __syncthreads();
-    }
+    if (tid < kQuadNbr) S.x[tid] = S.ys[S.order[tid]] / S.piv[tid];
     if (tid < kQuadNbr) w.wt[static_cast<int64_t>(t) * kQuadNbr + tid] = __dmul_rn(S.x[tid], S.dist[tid]);
     __syncthreads();
   }
