@@ -369,3 +369,34 @@ def test_larger_system_against_oracle():
     assert rel_err(y.cpu().numpy(), op.matvec(x)) < 1e-10
     dev.pc(torch.tensor(x, device="cuda"), y)
     assert rel_err(y.cpu().numpy(), op.pc(x)) < 1e-9
+
+
+def test_output_records_from_marched_system(golden_step, tmp_path):
+    """A step marched on the device is written in fiber3d's layout: the
+    fibers file holds the solution's positions and tensions, the velocity
+    file the bodies' U and Omega, the clones file the advanced poses."""
+    from fiber3d_b200 import hydro as H
+    from fiber3d_b200.output import OutputWriter, records_from_solution
+    P = problem_from_golden(golden_step)
+    s = H.HydroSystem(P)
+    sol = golden_step["sol"].copy()
+    s.advance(torch.tensor(sol, device="cuda"))
+    fibers, bodies = records_from_solution(s, sol, P.E, P.lengths, body_radius=[0.5] * s.nbody)
+    out = str(tmp_path / "run")
+    with OutputWriter(out, True, P.dt, 1) as w:
+        w.write(P.dt, 1, 0, fibers, bodies)
+    rows = np.loadtxt(out + "_one_fibers.txt")
+    r = 1
+    for f in range(s.fs.nfib):
+        n, p0 = int(s.fs.npts[f]), int(s.fs.pt_off_h[f])
+        blk = sol[s.o_fib + 4 * p0:s.o_fib + 4 * (p0 + n)].reshape(4, n)
+        assert rows[r][0] == n and rows[r][1] == P.E
+        assert np.array_equal(rows[r + 1:r + 1 + n], blk.T)
+        r += 1 + n
+    vel = np.loadtxt(out + "_onevelocity_clones.txt")[1:]
+    locs, quats = s.body_state()
+    clones = np.loadtxt(out + "_one_clones.txt")[1:].reshape(s.nbody, 2, 7)
+    for k in range(s.nbody):
+        o = s.o_body[k] + 3 * s.nb[k]
+        assert np.array_equal(vel[k], sol[o:o + 6])
+        assert np.array_equal(clones[k, 1], np.concatenate([locs[k], quats[k]]))
