@@ -213,5 +213,6 @@ class Workspace:
 
 
 def device_error(device: torch.device | None = None) -> int:
-    """Read and clear the device error word (F3D_OK or F3D_ERR_TIMEOUT)."""
+    """Read and clear the device error word (F3D_OK, or the first failing status a kernel
+    recorded: F3D_ERR_TIMEOUT, F3D_ERR_ARG, F3D_ERR_SINGULAR, F3D_ERR_TOO_LARGE)."""
     return lib().f3d_get_device_error(stream_handle(device))

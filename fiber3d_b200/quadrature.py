@@ -40,7 +40,9 @@ def surface_quadrature_weights(nodes, triangles, gradient, device=None, return_n
     (ntri, 80) int32 nodes nearest each triangle's midpoint, nearest first.
     Raises ``ValueError`` for fewer than 80 nodes (fiber3d's neighbour
     search needs 80) and ``F3DError`` for a triangulation that is not a closed
-    surface or a singular local system.
+    surface or a singular local system.  The device error word is read (and
+    cleared) after the call, so an error an earlier kernel left there is
+    raised here too rather than lost.
     """
     if device is None:
         device = nodes.device if isinstance(nodes, torch.Tensor) and nodes.is_cuda else torch.device("cuda", 0)
@@ -59,7 +61,6 @@ def surface_quadrature_weights(nodes, triangles, gradient, device=None, return_n
     w = torch.empty(n, dtype=torch.float64, device=device)
     nni = torch.empty((ntri, N_NEIGHBORS), dtype=torch.int32, device=device) if return_neighbors else None
     with torch.cuda.device(device):
-        _lib.device_error(device)
         _lib.call("f3d_surface_quadrature", _lib.ptr(X), n, _lib.ptr(T), ntri, _lib.ptr(G), _lib.ptr(w),
                   _lib.ptr(nni), _lib.ptr(ws), nbytes.value, _lib.stream_handle(device))
         torch.cuda.current_stream(device).synchronize()
