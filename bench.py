@@ -346,6 +346,9 @@ def cpu_baseline(wl, seconds: float):
 def reference_arm(args, rank, world):
     if rank != 0:
         return
+    if args.workload == "surface_quadrature":
+        quadrature_reference_arm(args, world)
+        return
     from oracle import pairs_c
     wl = make_workload(args.workload)
     threads = pairs_c.max_threads()
@@ -569,6 +572,28 @@ def cpu_quadrature_rate(nodes, tri, grad, seconds: float):
             np.linalg.solve(M, r)
         done += len(nni)
     return done / (time.perf_counter() - t0), done
+
+
+def quadrature_reference_arm(args, world):
+    """The CPU restatement of fiber3d's quadrature loop (one core), each step
+    a bounded sample of triangles extrapolated to the whole surface."""
+    nodes, tri, grad = _quadrature_problem(args)
+    per_step = max(1.0, args.cpu_seconds / max(args.steps, 1))
+    for _ in range(args.warmup):
+        cpu_quadrature_rate(nodes, tri, grad, 0.0)
+    samples = [cpu_quadrature_rate(nodes, tri, grad, per_step) for _ in range(args.steps)]
+    ms = statistics.median(len(tri) / r * 1e3 for r, _ in samples)
+    line = {"impl": "reference", "metric": "surface quadrature set-up (ms)", "value": ms, "unit": "ms",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+            "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (shape_gallery sphere)",
+            "config": {"workload": "surface_quadrature", "nodes": int(args.nshell), "triangles": int(len(tri)),
+                       "radius": args.shell_radius, "parallelism": "one host core"},
+            "cpu_baseline": {"value": ms, "unit": "ms", "cores": 1, "kind": "port",
+                             "sample": f"{samples[0][1]} triangles per step sample, extrapolated to {len(tri)}; "
+                                       "numpy/LAPACK restatement of fiber3d's loop (oracle/quadrature.py)"},
+            "e2e": {"value": ms, "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
 
 
 def quadrature_arm(args, rank, world, local):
