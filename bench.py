@@ -439,7 +439,8 @@ def hydro_arm(args, rank, world, local, warmup=None, steps=None, emit=True):
              "learned_fp64": ("learned", False, 1, 1e-8),
              "learned_mixed_pc1": ("learned", True, 1, 1e-8),
              "learned_mixed": ("learned", True, "auto", 1e-8),
-             "learned_mixed_tol1e-9": ("learned", True, "auto", 1e-9)}
+             "learned_mixed_tol1e-9": ("learned", True, "auto", 1e-9),
+             "learned_mixed_tol1e-10": ("learned", True, "auto", 1e-10)}
     for mode, (guess, mixed, pc_refresh, tol) in modes.items():
         sysd = H.HydroSystem(P, shell_op=shell, device=dev, tune=True, pc_refresh=pc_refresh)
         torch.cuda.synchronize()
