@@ -6,7 +6,7 @@
 // body/body.py:104-107).
 //
 // The reference loops over triangles in Python (about 5 ms each).  Here the
-// whole computation is six kernels on one stream:
+// whole computation is eight kernels on one stream:
 //   1. quad_prep: per triangle, sorted vertices, unit normal and midpoint;
 //      its three edges go into a device hash table (key = i * n + j).
 //   2. quad_edges: per triangle edge, the partner triangle from the table and
@@ -14,6 +14,7 @@
 //   3. quad_knn: per triangle, the 80 nodes nearest its midpoint (:114-115),
 //      an exact radix select over the float-rounded squared distances held
 //      in shared memory, ties resolved on the double distances, then index.
+//      All n squared distances sit in shared memory: n <= 26000.
 //   4. quad_triangle: per triangle, the projection onto the triangle's plane
 //      (:162-236), the exact integrals of r^7 (:262-309) and of the degree-7
 //      monomials (:473-622, here by Gauss-Legendre on Green's-theorem line
