@@ -14,7 +14,7 @@
 //   3. quad_knn: per triangle, the 80 nodes nearest its midpoint (:114-115),
 //      an exact radix select over the float-rounded squared distances held
 //      in shared memory, ties resolved on the double distances, then index.
-//      All n squared distances sit in shared memory: n <= 26000.
+//      The nodes go in tiles of 24576, the best 80 carried from tile to tile.
 //   4. quad_triangle: per triangle, the projection onto the triangle's plane
 //      (:162-236), the exact integrals of r^7 (:262-309) and of the degree-7
 //      monomials (:473-622, here by Gauss-Legendre on Green's-theorem line
@@ -38,7 +38,7 @@ constexpr int kQuadRhsCol = kQuadDim;        // column 116 holds the right-hand 
 constexpr int kKnnThreads = 256;
 constexpr int kKnnBins = 2048;
 constexpr int kKnnCand = 256;
-constexpr int kQuadMaxNodes = 26000;         // the k-NN keeps all squared distances in shared memory
+constexpr int kKnnTile = 24576;             // nodes per k-NN pass (squared distances in shared memory)
 constexpr double kEpsMult = 1e-4;
 constexpr double kDblEps = 2.220446049250313e-16;
 
@@ -172,108 +172,125 @@ __global__ void quad_edges_kernel(int n, int ntri, QuadWs w, int *err) {
 // ----------------------------------------------------------------- 3. kNN --
 __device__ __forceinline__ unsigned fkey(double d) { return __float_as_uint(__double2float_rn(d)); }
 
+// The nodes are taken in tiles of `tile`: each tile's squared distances,
+// together with the best 80 of the earlier tiles, go through the select, so
+// a surface of any size fits the shared memory; a surface of at most `tile`
+// nodes is one pass.
 __global__ void __launch_bounds__(kKnnThreads) quad_knn_kernel(const double *__restrict__ X, int n,
-                                                               const double *__restrict__ mid, int ntri,
+                                                               const double *__restrict__ mid, int ntri, int tile,
                                                                int32_t *__restrict__ nni, int *err) {
   extern __shared__ __align__(16) unsigned char knn_smem[];
-  double *dist = reinterpret_cast<double *>(knn_smem);
-  double *cd = dist + n;                                   // kKnnCand candidate distances
+  double *dist = reinterpret_cast<double *>(knn_smem);     // tile + 80
+  double *cd = dist + tile + kQuadNbr;                     // kKnnCand candidate distances
   int *cj = reinterpret_cast<int *>(cd + kKnnCand);        // kKnnCand candidate indices
-  int *hist = cj + kKnnCand;                               // kKnnBins
+  int *pj = cj + kKnnCand;                                 // 80: indices of the earlier tiles' best
+  int *hist = pj + kQuadNbr;                               // kKnnBins
   __shared__ int s_part[kKnnThreads / 32];
   __shared__ int s_bin, s_below, s_ncand;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   for (int t = blockIdx.x; t < ntri; t += gridDim.x) {
     const double q0 = mid[3 * t], q1 = mid[3 * t + 1], q2 = mid[3 * t + 2];
-    for (int j = tid; j < n; j += kKnnThreads) {
-      const double dx = __dsub_rn(q0, X[3 * j]), dy = __dsub_rn(q1, X[3 * j + 1]), dz = __dsub_rn(q2, X[3 * j + 2]);
-      dist[j] = __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
-    }
-    unsigned prefix = 0;
-    int kk = kQuadNbr;  // rank (1-based) still to find among keys matching the prefix
-    const int shifts[3] = {21, 10, 0}, widths[3] = {11, 11, 10};
-    for (int pass = 0; pass < 3; ++pass) {
-      const int shift = shifts[pass], width = widths[pass];
-      for (int b = tid; b < kKnnBins; b += kKnnThreads) hist[b] = 0;
-      __syncthreads();
-      for (int base = 0; base < n; base += kKnnThreads) {
-        const int j = base + tid;
-        int bin = -1 - lane;  // distinct per lane when not counted
-        if (j < n) {
-          const unsigned key = fkey(dist[j]);
-          if (pass == 0 || (key >> (shift + width)) == prefix) bin = static_cast<int>((key >> shift) & ((1u << width) - 1u));
-        }
-        const unsigned peers = __match_any_sync(0xffffffffu, bin);
-        if (bin >= 0 && lane == __ffs(peers) - 1) atomicAdd(hist + bin, __popc(peers));
+    int nprev = 0;
+    for (int base = 0; base < n; base += tile) {
+      const int tl = min(tile, n - base);
+      for (int j = tid; j < tl; j += kKnnThreads) {
+        const int g = base + j;
+        const double dx = __dsub_rn(q0, X[3 * g]), dy = __dsub_rn(q1, X[3 * g + 1]), dz = __dsub_rn(q2, X[3 * g + 2]);
+        dist[j] = __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
       }
-      __syncthreads();
-      // the bin where the running count reaches kk
-      int local = 0;
-      for (int b = 0; b < kKnnBins / kKnnThreads; ++b) local += hist[tid * (kKnnBins / kKnnThreads) + b];
-      int incl = local;
-      for (int o = 1; o < 32; o <<= 1) {
-        const int v = __shfl_up_sync(0xffffffffu, incl, o);
-        if (lane >= o) incl += v;
+      for (int p = tid; p < nprev; p += kKnnThreads) {
+        dist[tl + p] = cd[p];
+        pj[p] = cj[p];
       }
-      if (lane == 31) s_part[warp] = incl;
+      const int m = tl + nprev;  // >= 80: the first tile has min(n, tile) >= 80 nodes
       __syncthreads();
-      int before = 0;
-      for (int w2 = 0; w2 < warp; ++w2) before += s_part[w2];
-      const int excl = before + incl - local;
-      if (excl < kk && excl + local >= kk) {
-        int c = excl;
-        for (int b = 0; b < kKnnBins / kKnnThreads; ++b) {
-          const int bin = tid * (kKnnBins / kKnnThreads) + b;
-          if (c + hist[bin] >= kk) {
-            s_bin = bin;
-            s_below = c;
-            break;
+      unsigned prefix = 0;
+      int kk = kQuadNbr;  // rank (1-based) still to find among keys matching the prefix
+      for (int pass = 0; pass < 3; ++pass) {
+        const int shift = pass == 0 ? 21 : (pass == 1 ? 10 : 0), width = pass == 2 ? 10 : 11;
+        for (int b = tid; b < kKnnBins; b += kKnnThreads) hist[b] = 0;
+        __syncthreads();
+        for (int pb = 0; pb < m; pb += kKnnThreads) {
+          const int j = pb + tid;
+          int bin = -1 - lane;  // distinct per lane when not counted
+          if (j < m) {
+            const unsigned key = fkey(dist[j]);
+            if (pass == 0 || (key >> (shift + width)) == prefix)
+              bin = static_cast<int>((key >> shift) & ((1u << width) - 1u));
           }
-          c += hist[bin];
+          const unsigned peers = __match_any_sync(0xffffffffu, bin);
+          if (bin >= 0 && lane == __ffs(peers) - 1) atomicAdd(hist + bin, __popc(peers));
         }
-      }
-      __syncthreads();
-      prefix = (prefix << width) | static_cast<unsigned>(s_bin);
-      kk -= s_below;
-      __syncthreads();
-    }
-    // prefix is now the float key of the 80th smallest distance: every node
-    // at or below it is a candidate (rounding to float is monotone)
-    if (tid == 0) s_ncand = 0;
-    __syncthreads();
-    for (int j = tid; j < n; j += kKnnThreads) {
-      if (fkey(dist[j]) <= prefix) {
-        const int slot = atomicAdd(&s_ncand, 1);
-        if (slot < kKnnCand) {
-          cd[slot] = dist[j];
-          cj[slot] = j;
+        __syncthreads();
+        // the bin where the running count reaches kk
+        int local = 0;
+        for (int b = 0; b < kKnnBins / kKnnThreads; ++b) local += hist[tid * (kKnnBins / kKnnThreads) + b];
+        int incl = local;
+        for (int o = 1; o < 32; o <<= 1) {
+          const int v = __shfl_up_sync(0xffffffffu, incl, o);
+          if (lane >= o) incl += v;
         }
-      }
-    }
-    __syncthreads();
-    const int nc = s_ncand;
-    if (nc > kKnnCand && tid == 0) record_error(err, F3D_ERR_TOO_LARGE);
-    for (int s = nc + tid; s < kKnnCand; s += kKnnThreads) {
-      cd[s] = __longlong_as_double(0x7ff0000000000000ll);
-      cj[s] = 0x7fffffff;
-    }
-    __syncthreads();
-    // bitonic sort of the candidates by (distance, index)
-    for (int size = 2; size <= kKnnCand; size <<= 1) {
-      for (int stride = size >> 1; stride > 0; stride >>= 1) {
-        const int i = tid, p = i ^ stride;
-        if (p > i) {
-          const bool up = (i & size) == 0;
-          const double di = cd[i], dp = cd[p];
-          const int ji = cj[i], jp = cj[p];
-          const bool gt = di > dp || (di == dp && ji > jp);
-          if (gt == up) {
-            cd[i] = dp, cd[p] = di;
-            cj[i] = jp, cj[p] = ji;
+        if (lane == 31) s_part[warp] = incl;
+        __syncthreads();
+        int before = 0;
+        for (int w2 = 0; w2 < warp; ++w2) before += s_part[w2];
+        const int excl = before + incl - local;
+        if (excl < kk && excl + local >= kk) {
+          int c = excl;
+          for (int b = 0; b < kKnnBins / kKnnThreads; ++b) {
+            const int bin = tid * (kKnnBins / kKnnThreads) + b;
+            if (c + hist[bin] >= kk) {
+              s_bin = bin;
+              s_below = c;
+              break;
+            }
+            c += hist[bin];
           }
         }
         __syncthreads();
+        prefix = (prefix << width) | static_cast<unsigned>(s_bin);
+        kk -= s_below;
+        __syncthreads();
       }
+      // prefix is now the float key of the 80th smallest distance: every
+      // node at or below it is a candidate (rounding to float is monotone)
+      if (tid == 0) s_ncand = 0;
+      __syncthreads();
+      for (int j = tid; j < m; j += kKnnThreads) {
+        if (fkey(dist[j]) <= prefix) {
+          const int slot = atomicAdd(&s_ncand, 1);
+          if (slot < kKnnCand) {
+            cd[slot] = dist[j];
+            cj[slot] = j < tl ? base + j : pj[j - tl];
+          }
+        }
+      }
+      __syncthreads();
+      const int nc = s_ncand;
+      if (nc > kKnnCand && tid == 0) record_error(err, F3D_ERR_TOO_LARGE);
+      for (int c = nc + tid; c < kKnnCand; c += kKnnThreads) {
+        cd[c] = __longlong_as_double(0x7ff0000000000000ll);
+        cj[c] = 0x7fffffff;
+      }
+      __syncthreads();
+      // bitonic sort of the candidates by (distance, index)
+      for (int size = 2; size <= kKnnCand; size <<= 1) {
+        for (int stride = size >> 1; stride > 0; stride >>= 1) {
+          const int i = tid, p = i ^ stride;
+          if (p > i) {
+            const bool up = (i & size) == 0;
+            const double di = cd[i], dp = cd[p];
+            const int ji = cj[i], jp = cj[p];
+            const bool gt = di > dp || (di == dp && ji > jp);
+            if (gt == up) {
+              cd[i] = dp, cd[p] = di;
+              cj[i] = jp, cj[p] = ji;
+            }
+          }
+          __syncthreads();
+        }
+      }
+      nprev = kQuadNbr;
     }
     if (tid < kQuadNbr) nni[static_cast<int64_t>(t) * kQuadNbr + tid] = cj[tid] < n ? cj[tid] : 0;
     __syncthreads();
@@ -735,7 +752,7 @@ int f3d_surface_quadrature(const double *nodes, int64_t n, const int32_t *triang
                            const double *gradient, double *weights, int32_t *neighbors, void *workspace,
                            size_t workspace_bytes, void *stream) {
   if (n < f3d::kQuadNbr || ntri < 1 || ntri > (1ll << 24)) return F3D_ERR_SHAPE;
-  if (n > f3d::kQuadMaxNodes) return F3D_ERR_TOO_LARGE;
+  if (n > (1ll << 30)) return F3D_ERR_TOO_LARGE;
   if (!nodes || !triangles || !gradient || !weights || !workspace) return F3D_ERR_NULL;
   if (!f3d::aligned(nodes, 8) || !f3d::aligned(gradient, 8) || !f3d::aligned(weights, 8) ||
       !f3d::aligned(workspace, 256) || !f3d::aligned(triangles, 4) || (neighbors && !f3d::aligned(neighbors, 4)))
@@ -755,7 +772,9 @@ int f3d_surface_quadrature(const double *nodes, int64_t n, const int32_t *triang
   const int nt = static_cast<int>(ntri), nn = static_cast<int>(n);
   f3d::quad_prep_kernel<<<(nt + 127) / 128, 128, 0, st>>>(nodes, nn, triangles, nt, w, err);
   f3d::quad_edges_kernel<<<(3 * nt + 127) / 128, 128, 0, st>>>(nn, nt, w, err);
-  const size_t knn_smem = sizeof(double) * (n + f3d::kKnnCand) + sizeof(int) * (f3d::kKnnCand + f3d::kKnnBins);
+  const int tile = static_cast<int>(std::min<int64_t>(n, f3d::kKnnTile));
+  const size_t knn_smem = sizeof(double) * (tile + f3d::kQuadNbr + f3d::kKnnCand) +
+                          sizeof(int) * (f3d::kKnnCand + f3d::kQuadNbr + f3d::kKnnBins);
   // the opt-in limit counts the kernel's static shared memory too: ask for
   // what this call needs
   static size_t attr_bytes[64] = {0};
@@ -774,7 +793,7 @@ int f3d_surface_quadrature(const double *nodes, int64_t n, const int32_t *triang
     return F3D_ERR_CUDA;
   const int64_t knn_grid = std::min<int64_t>(ntri, static_cast<int64_t>(per_sm) * f3d::sm_count());
   f3d::quad_knn_kernel<<<static_cast<unsigned>(knn_grid), f3d::kKnnThreads, knn_smem, st>>>(nodes, nn, w.mid, nt,
-                                                                                            w.nni, err);
+                                                                                            tile, w.nni, err);
   const int64_t tri_grid = std::min<int64_t>(ntri, f3d::sm_count());
   f3d::quad_triangle_kernel<<<static_cast<unsigned>(tri_grid), f3d::kTriThreads, 0, st>>>(nodes, gradient, nt, w, err);
   const int64_t m = f3d::kQuadNbr * ntri;

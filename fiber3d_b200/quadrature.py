@@ -23,7 +23,6 @@ import torch
 from . import _lib
 
 N_NEIGHBORS = 80
-MAX_NODES = 26000
 
 
 def _as_device(a, dtype, device) -> torch.Tensor:

@@ -556,7 +556,7 @@ int f3d_mse_grad(const float *Y, const float *T, float *D, float *row_loss, int3
    triangle's plane.  nodes (n x 3), gradient (n x 3, gradh at the nodes),
    triangles (ntri x 3, any vertex order; a closed surface, every edge shared
    by exactly two triangles) -> weights (n).  neighbors (ntri x 80, nearest
-   first) receives each triangle's nodes when non-NULL.  80 <= n <= 26000.
+   first) receives each triangle's nodes when non-NULL.  n >= 80.
    Bad triangulations and zero pivots are reported through the device error
    word (F3D_ERR_ARG, F3D_ERR_SINGULAR; f3d_get_device_error). */
 int f3d_surface_quadrature_workspace_bytes(int64_t n, int64_t ntri, size_t *bytes);

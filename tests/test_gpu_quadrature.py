@@ -119,3 +119,25 @@ def test_bad_triangulations_raise(gq, q):
     # the device stays usable
     w = q.surface_quadrature_weights(nodes, tri, grad).cpu().numpy()
     assert _rel(w, gq["body_w"]) <= W_TOL["body"]
+
+
+def test_surface_larger_than_one_tile(q):
+    """30000 nodes: the neighbour search goes in two tiles (24576 nodes each
+    at most), carrying the best 80 across.  The neighbour lists of a sample
+    of triangles equal the oracle's brute force; the weights integrate 1 and
+    x^2 over the sphere and repeat bit for bit."""
+    from scipy.spatial import ConvexHull
+    from fiber3d_b200 import geometry
+    R = 12.0
+    nodes, _ = geometry.fibonacci_sphere(30000, R)
+    tri = ConvexHull(nodes).simplices
+    w, nni = q.surface_quadrature_weights(nodes, tri, 2 * nodes, return_neighbors=True)
+    ts = np.sort(tri, axis=1)
+    pick = np.arange(0, len(ts), 97)
+    mids = (nodes[ts[pick, 0]] + nodes[ts[pick, 1]] + nodes[ts[pick, 2]]) / 3
+    assert np.array_equal(nni.cpu().numpy()[pick], OQ.nearest_neighbors(nodes, mids).astype(np.int32))
+    assert torch.equal(w, q.surface_quadrature_weights(nodes, tri, 2 * nodes))
+    w = w.cpu().numpy()
+    assert (w > 0).all()
+    assert abs(w.sum() / (4 * np.pi * R ** 2) - 1) < 1e-9
+    assert abs((w * nodes[:, 0] ** 2).sum() / (4 * np.pi * R ** 4 / 3) - 1) < 1e-9
