@@ -107,3 +107,21 @@ def test_argument_checks_of_newer_entries(dll):
     # (the pointers are placeholders that the check never dereferences)
     p = ctypes.c_void_p(256)
     assert dll.f3d_fiber_self_flow_up(p, p, p, 3, 1024, p, p, p, p, 2, 1.0, 5e-3, 1e-5, p, None) == TOO_LARGE
+
+
+def test_argument_checks_of_surface_quadrature(dll):
+    SHAPE, NULL, ALIGN, WORKSPACE = 2, 1, 3, 4
+    nbytes = ctypes.c_size_t(0)
+    assert dll.f3d_surface_quadrature_workspace_bytes(12000, 23996, ctypes.byref(nbytes)) == 0
+    # triangles x 80 neighbours and weights dominate the workspace
+    assert nbytes.value >= 23996 * 80 * (4 + 8 + 4)
+    assert dll.f3d_surface_quadrature_workspace_bytes(-1, 10, ctypes.byref(nbytes)) == SHAPE
+    assert dll.f3d_surface_quadrature_workspace_bytes(100, 10, None) == NULL
+    # fewer nodes than the 80 neighbours, no triangles: shape errors before any launch
+    assert dll.f3d_surface_quadrature(None, 79, None, 10, None, None, None, None, 0, None) == SHAPE
+    assert dll.f3d_surface_quadrature(None, 400, None, 0, None, None, None, None, 0, None) == SHAPE
+    assert dll.f3d_surface_quadrature(None, 400, None, 796, None, None, None, None, 0, None) == NULL
+    # placeholder pointers the checks never dereference: misaligned, then a short workspace
+    p8, p_odd = ctypes.c_void_p(4096), ctypes.c_void_p(4100)
+    assert dll.f3d_surface_quadrature(p8, 400, p8, 796, p8, p8, None, p_odd, 1 << 30, None) == ALIGN
+    assert dll.f3d_surface_quadrature(p8, 400, p8, 796, p8, p8, None, p8, 16, None) == WORKSPACE
