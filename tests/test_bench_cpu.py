@@ -22,3 +22,19 @@ def test_quadrature_reference_arm_prints_one_line():
     assert d["config"]["workload"] == "surface_quadrature" and d["config"]["triangles"] == 796
     assert d["value"] > 0 and d["e2e"]["value"] == d["value"]
     assert d["cpu_baseline"]["kind"] == "port" and d["cpu_baseline"]["cores"] == 1
+
+
+def test_default_reference_arm_prints_one_line():
+    """The arm the driver runs beside the GPU one: the C restatement of
+    fiber3d's pair loop on the default workload's metric and config."""
+    cmd = [sys.executable, str(ROOT / "bench.py"), "--impl", "reference", "--steps", "1", "--warmup", "3",
+           "--cpu-seconds", "0.5"]
+    res = subprocess.run(cmd, capture_output=True, text=True, timeout=600, cwd=ROOT)
+    assert res.returncode == 0, res.stderr
+    lines = [ln for ln in res.stdout.splitlines() if ln.startswith("{")]
+    assert len(lines) == 1
+    d = json.loads(lines[0])
+    assert d["impl"] == "reference" and d["metric"] == "Stokes pair interactions per second (FP64)"
+    assert d["unit"] == "pairs/s" and d["value"] > 0 and d["higher_is_better"] is True
+    assert d["config"]["workload"] == "stresslet_sphere"
+    assert d["e2e"] == {"value": d["value"], "unit": "pairs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
