@@ -38,3 +38,15 @@ def test_default_reference_arm_prints_one_line():
     assert d["unit"] == "pairs/s" and d["value"] > 0 and d["higher_is_better"] is True
     assert d["config"]["workload"] == "stresslet_sphere"
     assert d["e2e"] == {"value": d["value"], "unit": "pairs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
+
+
+def test_reference_arm_other_ranks_exit_without_work():
+    """Under torchrun only rank 0 runs the reference arm; the others exit 0
+    and print nothing."""
+    import os
+    env = dict(os.environ, RANK="1", LOCAL_RANK="1", WORLD_SIZE="2")
+    cmd = [sys.executable, str(ROOT / "bench.py"), "--impl", "reference", "--gpus", "2", "--steps", "1",
+           "--warmup", "3"]
+    res = subprocess.run(cmd, capture_output=True, text=True, timeout=120, cwd=ROOT, env=env)
+    assert res.returncode == 0, res.stderr
+    assert not [ln for ln in res.stdout.splitlines() if ln.startswith("{")]
