@@ -21,8 +21,8 @@ F3D_OK = 0
 F3D_ERR_TIMEOUT = 8
 
 # enums
-KERNEL = {"oseen": 0, "stresslet": 1, "rotlet": 2}
-SELF_MODE = {"regularise": 0, "skip_index": 1, "skip_group": 2}
+KERNEL = {"oseen": 0, "stresslet": 1, "rotlet": 2, "traction": 3}
+SELF_MODE = {"regularise": 0, "skip_index": 1, "skip_group": 2, "skip_close": 3}
 PRECISION = {"fp64": 0, "fp32c": 1}
 
 
@@ -61,6 +61,9 @@ SIGNATURES: dict[str, list] = {
     "f3d_version": [],
     "f3d_status_string": [_I],
     "f3d_get_device_error": [_P],
+    "f3d_set_wait_limit_ns": [ctypes.c_uint64],
+    "f3d_wait_limit_ns": [],
+    "f3d_selftest_bounded_wait": [ctypes.c_uint64, _P],
     "f3d_probe_fma": [_I, _I, _P, ctypes.POINTER(_D), _P],
     "f3d_pair_workspace_bytes": [_I, _I, _I64, _I64, ctypes.POINTER(PairShape), ctypes.POINTER(_SZ)],
     "f3d_pair_sum": [_I, _I, _I, _P, _P, _P, _P, _P, _P, _P, _I64, _I64, _D, _D, _D, _I,
@@ -78,6 +81,7 @@ SIGNATURES: dict[str, list] = {
     "f3d_oseen_tensor_dense": [_P, _P, _I64, _I64, _D, _D, _D, _P],
     "f3d_oseen_tensor_source_target_dense": [_P, _P, _P, _I64, _I64, _I64, _D, _D, _D, _P],
     "f3d_complementary_dense": [_P, _P, _I64, _I64, _P],
+    "f3d_stresslet_tensor_dense": [_P, _P, _I64, _D, _D, _D, _P],
     "f3d_batched_lu_workspace_bytes": [ctypes.POINTER(_SZ)],
     "f3d_singularity_vectors_workspace_bytes": [_I64, ctypes.POINTER(_SZ)],
     "f3d_singularity_vectors": [_P, _P, _P, _P, _I64, _D, _D, _D, _P, _SZ, _P],
@@ -128,7 +132,8 @@ SIGNATURES: dict[str, list] = {
     "f3d_batched_inverse": [_P, _P, _P, ctypes.c_int32, ctypes.c_int32, _P, _P, _P],
     "f3d_block_gemv": [_I, _P, _P, _P, _P, ctypes.c_int32, ctypes.c_int32, _P, _P, _P],
 }
-_RESTYPE = {"f3d_version": ctypes.c_char_p, "f3d_status_string": ctypes.c_char_p}
+_RESTYPE = {"f3d_version": ctypes.c_char_p, "f3d_status_string": ctypes.c_char_p,
+            "f3d_wait_limit_ns": ctypes.c_uint64}
 
 
 def load_library(path: Path | str = LIBPATH) -> ctypes.CDLL:
@@ -211,8 +216,39 @@ class Workspace:
     def reset(self) -> None:
         self.buf.zero_()
 
+    @classmethod
+    def reset_all(cls) -> None:
+        for ws in cls._per_device.values():
+            ws.reset()
+
 
 def device_error(device: torch.device | None = None) -> int:
     """Read and clear the device error word (F3D_OK, or the first failing status a kernel
     recorded: F3D_ERR_TIMEOUT, F3D_ERR_ARG, F3D_ERR_SINGULAR, F3D_ERR_TOO_LARGE)."""
     return lib().f3d_get_device_error(stream_handle(device))
+
+
+def check_device_error(what: str, device: torch.device | None = None, on_error=None) -> None:
+    """Raise F3DError if a kernel recorded a failure since the last read.
+
+    A kernel whose bounded wait ran out returns early and may leave the split
+    counters of a workspace non-zero, which would make later sums wrong; so
+    on any recorded failure every shared pair workspace is zeroed (and
+    ``on_error``, e.g. a solver's own workspace reset, is called) before the
+    error is raised.  The next call then starts from a clean state.
+    """
+    status = device_error(device)
+    if status != F3D_OK:
+        Workspace.reset_all()
+        if on_error is not None:
+            on_error()
+        raise F3DError(what, status, lib().f3d_status_string(status).decode())
+
+
+def set_wait_limit_ns(limit_ns: int) -> None:
+    """Limit (ns) of the kernels' bounded waits for later calls; 0 restores 2 s."""
+    lib().f3d_set_wait_limit_ns(int(limit_ns))
+
+
+def wait_limit_ns() -> int:
+    return int(lib().f3d_wait_limit_ns())

@@ -12,8 +12,15 @@
 
 namespace f3d {
 
-// A bounded wait gives up after this many nanoseconds of %globaltimer.
+// A bounded wait gives up after this many nanoseconds of %globaltimer by
+// default; f3d_set_wait_limit_ns changes the limit the entry points pass to
+// their kernels.
 constexpr uint64_t kWaitLimitNs = 2000000000ull;  // 2 s
+
+// Split-reduction counters of the pair sums: one word per target block, in
+// a fixed region at the start of the pair workspace.
+constexpr int64_t kMaxCounters = 65536;
+constexpr size_t kCounterBytes = kMaxCounters * sizeof(unsigned);
 
 // ---------------------------------------------------------------- device --
 __device__ __forceinline__ uint32_t smem_addr(const void *p) {
@@ -71,13 +78,13 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
   return ok != 0;
 }
 
-// Waits for phase `parity` of `bar` to complete, for at most kWaitLimitNs.
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity) {
+// Waits for phase `parity` of `bar` to complete, for at most limit_ns.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity, uint64_t limit_ns) {
   if (mbar_try_wait(bar, parity)) return true;
   const uint64_t t0 = global_timer_ns();
   while (true) {
     if (mbar_try_wait(bar, parity)) return true;
-    if (global_timer_ns() - t0 > kWaitLimitNs) return false;
+    if (global_timer_ns() - t0 > limit_ns) return false;
   }
 }
 
@@ -88,6 +95,9 @@ __device__ __forceinline__ void record_error(int *err, int code) {
 // ------------------------------------------------------------------ host --
 // Device address of this device's error word (set up on first use per device).
 int *device_error_word();
+
+// The limit (ns) that entry points hand to their kernels' bounded waits.
+uint64_t wait_limit_ns();
 
 inline bool aligned(const void *p, uintptr_t a) {
   return (reinterpret_cast<uintptr_t>(p) & (a - 1)) == 0;

@@ -6,6 +6,7 @@
 //   stresslet_kernel_times_normal_numba  python/kernels/kernels.py:1063-1120
 //   oseen_tensor (input_format 'r')      python/kernels/kernels.py:31-116
 //   complementary_kernel                 python/kernels/kernels.py:1286-1295
+//   stresslet_kernel (input_format 'r')  python/kernels/kernels.py:911-992
 #include "f3d_common.cuh"
 
 namespace f3d {
@@ -58,6 +59,32 @@ __global__ void oseen_tensor_dense_kernel(const double *__restrict__ xs,
   for (int a = 0; a < 3; ++a)
 #pragma unroll
     for (int b = 0; b < 3; ++b) row[a * ld + b] = (a == b ? fr : 0.0) + gr * r[a] * r[b];
+}
+
+// The 3-index stresslet tensor: S[3i+a, 3j+b, c] = fr dr_a dr_b dr_c with
+// dr = x_j - x_i, fr = -3/(4 pi eta dr^5) for dr > eps and
+// -3/(4 pi eta (dr^2 + reg^2)^(5/2)) otherwise (the diagonal blocks are then
+// zero because dr = 0).  One thread writes the 27 entries of pair (i, j):
+// for each a, nine consecutive doubles, so a warp writes 32 x 72 contiguous
+// bytes per row.
+__global__ void stresslet_tensor_dense_kernel(const double *__restrict__ x, double *S, int64_t n,
+                                              double factor, double eps, double reg2) {
+  const int64_t j = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  const int64_t i = blockIdx.y;
+  if (j >= n) return;
+  const double dr[3] = {x[3 * j] - x[3 * i], x[3 * j + 1] - x[3 * i + 1], x[3 * j + 2] - x[3 * i + 2]};
+  const double r2 = dr[0] * dr[0] + dr[1] * dr[1] + dr[2] * dr[2];
+  const double d = sqrt(r2);
+  const double fr = (d > eps) ? factor / pow(d, 5.0) : factor / pow(r2 + reg2, 2.5);
+  const int64_t ld = 9 * n;  // doubles per row (3n columns x 3)
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    double *row = S + (3 * i + a) * ld + 9 * j;
+#pragma unroll
+    for (int b = 0; b < 3; ++b)
+#pragma unroll
+      for (int c = 0; c < 3; ++c) row[3 * b + c] = fr * dr[a] * dr[b] * dr[c];
+  }
 }
 
 __global__ void complementary_dense_kernel(const double *__restrict__ nrm, double *C, int64_t m,
@@ -120,6 +147,17 @@ int f3d_oseen_tensor_source_target_dense(const double *r_source, const double *r
   f3d::oseen_tensor_dense_kernel<<<grid, 128, 0, static_cast<cudaStream_t>(stream)>>>(
       r_source, r_target, G, ns, ld, 1.0 / (8.0 * f3d::kPi * eta),
       epsilon_distance * epsilon_distance, reg * reg);
+  return f3d::launch_status();
+}
+
+int f3d_stresslet_tensor_dense(const double *r_vectors, double *S, int64_t n, double eta, double reg,
+                               double epsilon_distance, void *stream) {
+  int rc = f3d::check_dense(r_vectors, S, n, 3 * n);
+  if (rc) return rc;
+  if (n == 0) return F3D_OK;
+  dim3 grid(static_cast<unsigned>((n + 127) / 128), static_cast<unsigned>(n));
+  f3d::stresslet_tensor_dense_kernel<<<grid, 128, 0, static_cast<cudaStream_t>(stream)>>>(
+      r_vectors, S, n, -3.0 / (4.0 * f3d::kPi * eta), epsilon_distance, reg * reg);
   return f3d::launch_status();
 }
 

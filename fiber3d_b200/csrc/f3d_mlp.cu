@@ -40,6 +40,7 @@ struct GemmArgs {
   int accumulate;  // C += result
   float alpha;
   int *err;
+  uint64_t wait_ns;  // limit of each bounded mbarrier wait
 };
 
 __device__ __forceinline__ uint64_t umma_smem_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
@@ -149,7 +150,7 @@ __global__ void __launch_bounds__(kGemmThreads) gemm_bf16_tcgen05_kernel(const G
                    : "memory");
     }
     // all threads wait for the MMAs of this chunk (shared memory is reused next round)
-    const bool done = mbar_wait_bounded(&mbar, phase);
+    const bool done = mbar_wait_bounded(&mbar, phase, g.wait_ns);
     phase ^= 1u;
     if (!done) s_fail = 1;
     __syncthreads();
@@ -187,7 +188,7 @@ __global__ void __launch_bounds__(kGemmThreads) gemm_bf16_tcgen05_kernel(const G
     }
   } else if (threadIdx.x == 0) {
     record_error(g.err, F3D_ERR_TIMEOUT);
-    (void)mbar_wait_bounded(&mbar, phase ^ 1u);  // MMAs still in flight, bounded
+    (void)mbar_wait_bounded(&mbar, phase ^ 1u, g.wait_ns);  // MMAs still in flight, bounded
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
@@ -262,7 +263,8 @@ int f3d_gemm_bf16(const float *A, int64_t a_rs, int64_t a_cs, const float *B, in
   int ntile = N;
   while (ntile > 32 && ntile % 32 == 0 && mtiles * (N / ntile) < f3d::sm_count()) ntile /= 2;
   f3d::GemmArgs g{A, B, C, bias, mask_src, pre, a_rs, a_cs, b_rs, b_cs, ldc, ldm,
-                  M, N, K, ntile, relu, accumulate, alpha, f3d::device_error_word()};
+                  M, N, K, ntile, relu, accumulate, alpha, f3d::device_error_word(),
+                  f3d::wait_limit_ns()};
   // 48 KB of operand tiles; ~100 KB is requested so that at most two CTAs
   // share an SM and their two 256-column TMEM allocations always fit.
   const size_t smem = 100 * 1024;

@@ -7,9 +7,13 @@
 //   rotlet_kernel_source_target_numba           :856-908   (A6)
 //   stresslet_kernel_times_normal_times_density :1123-1183 (A4, j == i skipped)
 //   stresslet_kernel_source_target_numba        :1186-1217 (A3)
+//   traction_kernel_times_normal_times_density  :1221-1264 (the normal of the target)
+//   oseen_kernel_source_target_pycuda           :849 -> kernels_pycuda.py:22-66
+//                                               (pairs closer than eps skipped)
 // r = x_target - x_source.  A pair with |r| < epsilon_distance uses
-// sqrt(|r|^2 + reg^2) in place of |r|.  The prefactor (1/(8 pi eta) or
-// -3/(4 pi eta)) is applied once per target.
+// sqrt(|r|^2 + reg^2) in place of |r| (F3D_SELF_SKIP_CLOSE: contributes
+// zero instead).  The prefactor (1/(8 pi eta) or -3/(4 pi eta)) is applied
+// once per target.
 //
 // Design.  One CTA owns TPB = (kBlock / SL) * TPT targets (held in registers)
 // and a contiguous range of source tiles (grid.y = source split).  Source
@@ -28,12 +32,9 @@ namespace f3d {
 
 constexpr int kBlock = 128;  // threads per CTA
 constexpr int kTile = 128;   // sources per staged tile
-// Split-reduction counters: one word per target block, in a fixed region.
-constexpr int64_t kMaxCounters = 65536;
-constexpr size_t kCounterBytes = kMaxCounters * sizeof(unsigned);
 
 struct PairArgs {
-  const double *rs, *rt, *dens, *nrm;
+  const double *rs, *rt, *dens, *nrm;  // nrm: source normals (traction: target normals)
   const double *dens2;  // dual sums: the second density (FP64 only)
   const float *packed;  // FP32C: [ns][12] packed source records
   const int32_t *gs, *gt;
@@ -48,6 +49,7 @@ struct PairArgs {
   int use_tma;
   int accumulate;
   double eps2, reg2, scale;
+  uint64_t wait_ns;  // limit of each bounded mbarrier wait
 };
 
 // Shared-memory layout of one stage.
@@ -72,22 +74,48 @@ constexpr size_t pair_smem_bytes() {
   return 128 + 2 * Stage<KIND, MODE, PREC, DUAL>::bytes;
 }
 
-// 1/sqrt(x) in FP64: the hardware approximation (PTX rsqrt.approx.ftz.f64,
-// about 2^-22 relative error) refined by one third-order Householder
-// (Halley-type) step y1 = y0 (1 + e/2 + 3e^2/8), e = 1 - x y0^2, whose error
-// is O(e^3) — below double rounding for any seed better than 2^-18.
-__device__ __forceinline__ double rsqrt_refined(double x) {
+// Reciprocal square roots in FP64.  y0 = rsqrt.approx.ftz.f64(x) (PTX; about
+// 2^-22 relative error) is a seed; with u = y0^2 and e = 1 - x u (one FMA,
+// exact to rounding), x^(-1/2) = y0 (1 - e)^(-1/2) and x^(-5/2) =
+// y0 u^2 (1 - e)^(-5/2).  The binomial series to second order,
+//   (1 - e)^(-1/2) = 1 + e/2 + 3e^2/8,   (1 - e)^(-5/2) = 1 + 5e/2 + 35e^2/8,
+// leaves O(e^3) ~ 2^-66: below double rounding.  (The first is one
+// Halley-type step for 1/sqrt(x); folding the second into the power r^-5
+// that the stresslet needs saves the separate refinement.)  For x = 0 the
+// result is not finite; callers discard such pairs with a select.
+__device__ __forceinline__ double rsqrt_seed(double x) {
   double y;
   asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
-  const double e = fma(-x * y, y, 1.0);
+  return y;
+}
+
+__device__ __forceinline__ double rsqrt_refined(double x) {
+  const double y = rsqrt_seed(x);
+  const double e = fma(-x, y * y, 1.0);
   return fma(y * e, fma(0.375, e, 0.5), y);
 }
 
-// r2 + reg2 when r2 < eps2 (r2 >= 0): the comparison is made on the IEEE bit
-// patterns (ordered like the values for non-negative doubles) so it runs on
-// the integer pipe, leaving the FP64 pipe to the arithmetic.
-__device__ __forceinline__ double regularise(double r2, long long eps2_bits, double reg2) {
-  return r2 + ((__double_as_longlong(r2) < eps2_bits) ? reg2 : 0.0);
+// q * x^(-5/2) for x > 0.
+__device__ __forceinline__ double times_rsqrt5(double q, double x) {
+  const double y = rsqrt_seed(x);
+  const double u = y * y;
+  const double e = fma(-x, u, 1.0);
+  const double qy5 = (q * y) * (u * u);
+  return fma(qy5 * e, fma(4.375, e, 2.5), qy5);
+}
+
+// Adds reg2 to r2 where r2 < eps2 (compared on the IEEE bit patterns, which
+// order like the values for non-negative doubles, on the integer pipe).  Such
+// pairs are rare, so the add runs in a branch that a warp takes only when one
+// of its lanes needs it: the common path spends no FP64 instruction on it.
+// The vote covers exactly the lanes executing it, and each lane's own
+// predicate is part of its vote, so the result does not depend on
+// convergence.
+__device__ __forceinline__ double regularise(double r2, bool close, double reg2) {
+  if (__any_sync(__activemask(), close)) {
+    if (close) r2 += reg2;
+  }
+  return r2;
 }
 
 __device__ __forceinline__ void two_sum(float &s, float &c, float x) {
@@ -151,7 +179,9 @@ __global__ void __launch_bounds__(kBlock) pair_kernel(const PairArgs a) {
   const int64_t tb = static_cast<int64_t>(blockIdx.x) * TPB;
 
   // ---- targets in registers -------------------------------------------
+  constexpr bool kTrac = (KIND == F3D_KERNEL_TRACTION);
   double txd[TPT], tyd[TPT], tzd[TPT];
+  double tn0[TPT], tn1[TPT], tn2[TPT];  // traction: the target's normal
   float txh[TPT], tyh[TPT], tzh[TPT], txl[TPT], tyl[TPT], tzl[TPT];
   int32_t tgrp[TPT];
   int64_t tidx[TPT];
@@ -161,11 +191,17 @@ __global__ void __launch_bounds__(kBlock) pair_kernel(const PairArgs a) {
     tidx[k] = t;
     double x = 0.0, y = 0.0, z = 0.0;
     int32_t g = -1;
+    tn0[k] = tn1[k] = tn2[k] = 0.0;
     if (t < a.nt) {
       x = a.rt[3 * t + 0];
       y = a.rt[3 * t + 1];
       z = a.rt[3 * t + 2];
       if (MODE == F3D_SELF_SKIP_GROUP) g = a.gt[t];
+      if (kTrac) {
+        tn0[k] = a.nrm[3 * t + 0];
+        tn1[k] = a.nrm[3 * t + 1];
+        tn2[k] = a.nrm[3 * t + 2];
+      }
     }
     tgrp[k] = g;
     if (PREC == F3D_FP64) {
@@ -176,13 +212,18 @@ __global__ void __launch_bounds__(kBlock) pair_kernel(const PairArgs a) {
       tzh[k] = static_cast<float>(z); tzl[k] = static_cast<float>(z - static_cast<double>(tzh[k]));
     }
   }
-  // FP32C: each target coordinate twice, against a pair of sources
+  // FP32C: each target coordinate (and traction normal) twice, against a
+  // pair of sources
   f32x2 pxh[TPT], pyh[TPT], pzh[TPT], pxl[TPT], pyl[TPT], pzl[TPT];
+  f32x2 pn0[TPT], pn1[TPT], pn2[TPT];
   if (PREC != F3D_FP64) {
 #pragma unroll
     for (int k = 0; k < TPT; ++k) {
       pxh[k] = pk2(txh[k], txh[k]); pyh[k] = pk2(tyh[k], tyh[k]); pzh[k] = pk2(tzh[k], tzh[k]);
       pxl[k] = pk2(txl[k], txl[k]); pyl[k] = pk2(tyl[k], tyl[k]); pzl[k] = pk2(tzl[k], tzl[k]);
+      const float m0 = static_cast<float>(tn0[k]), m1 = static_cast<float>(tn1[k]),
+                  m2 = static_cast<float>(tn2[k]);
+      pn0[k] = pk2(m0, m0); pn1[k] = pk2(m1, m1); pn2[k] = pk2(m2, m2);
     }
   }
 
@@ -221,34 +262,44 @@ __global__ void __launch_bounds__(kBlock) pair_kernel(const PairArgs a) {
 #pragma unroll
         for (int k = 0; k < TPT; ++k) {
           const double dx = txd[k] - sx, dy = tyd[k] - sy, dz = tzd[k] - sz;
-          const double r2 = regularise(fma(dx, dx, fma(dy, dy, dz * dz)), eps2_bits, reg2);
-          double ri = rsqrt_refined(r2);
-          if (MODE == F3D_SELF_SKIP_INDEX) ri = (sbase + s == tidx[k]) ? 0.0 : ri;
-          if (MODE == F3D_SELF_SKIP_GROUP) ri = (sg == tgrp[k]) ? 0.0 : ri;
-          if (KIND == F3D_KERNEL_OSEEN) {
+          double r2 = fma(dx, dx, fma(dy, dy, dz * dz));
+          // skipped pairs (and, in SKIP_CLOSE, close ones) are dropped by a
+          // select on the final factor, so their r2 may stay 0
+          bool skip = false;
+          if (MODE == F3D_SELF_SKIP_INDEX) skip = (sbase + s == tidx[k]);
+          if (MODE == F3D_SELF_SKIP_GROUP) skip = (sg == tgrp[k]);
+          const bool close = !skip && (__double_as_longlong(r2) < eps2_bits);
+          if (MODE == F3D_SELF_SKIP_CLOSE) skip = close;
+          else r2 = regularise(r2, close, reg2);
+          if (KIND == F3D_KERNEL_OSEEN || KIND == F3D_KERNEL_ROTLET) {
+            double ri = rsqrt_refined(r2);
+            if (MODE != F3D_SELF_REGULARISE) ri = skip ? 0.0 : ri;
             const double ri3 = ri * ri * ri;
-            const double rf = fma(dx, d0, fma(dy, d1, dz * d2));
-            const double g = ri3 * rf;
-            acc[k][0] = fma(g, dx, fma(ri, d0, acc[k][0]));
-            acc[k][1] = fma(g, dy, fma(ri, d1, acc[k][1]));
-            acc[k][2] = fma(g, dz, fma(ri, d2, acc[k][2]));
-            if (DUAL) {
-              const double re = fma(dx, e0, fma(dy, e1, dz * e2));
-              const double g2 = ri3 * re;
-              acc2[k][0] = fma(g2, dx, fma(ri, e0, acc2[k][0]));
-              acc2[k][1] = fma(g2, dy, fma(ri, e1, acc2[k][1]));
-              acc2[k][2] = fma(g2, dz, fma(ri, e2, acc2[k][2]));
+            if (KIND == F3D_KERNEL_OSEEN) {
+              const double rf = fma(dx, d0, fma(dy, d1, dz * d2));
+              const double g = ri3 * rf;
+              acc[k][0] = fma(g, dx, fma(ri, d0, acc[k][0]));
+              acc[k][1] = fma(g, dy, fma(ri, d1, acc[k][1]));
+              acc[k][2] = fma(g, dz, fma(ri, d2, acc[k][2]));
+              if (DUAL) {
+                const double re = fma(dx, e0, fma(dy, e1, dz * e2));
+                const double g2 = ri3 * re;
+                acc2[k][0] = fma(g2, dx, fma(ri, e0, acc2[k][0]));
+                acc2[k][1] = fma(g2, dy, fma(ri, e1, acc2[k][1]));
+                acc2[k][2] = fma(g2, dz, fma(ri, e2, acc2[k][2]));
+              }
+            } else {
+              acc[k][0] = fma(ri3, dz * d1 - dy * d2, acc[k][0]);
+              acc[k][1] = fma(ri3, dx * d2 - dz * d0, acc[k][1]);
+              acc[k][2] = fma(ri3, dy * d0 - dx * d1, acc[k][2]);
             }
-          } else if (KIND == F3D_KERNEL_ROTLET) {
-            const double g = ri * ri * ri;
-            acc[k][0] = fma(g, dz * d1 - dy * d2, acc[k][0]);
-            acc[k][1] = fma(g, dx * d2 - dz * d0, acc[k][1]);
-            acc[k][2] = fma(g, dy * d0 - dx * d1, acc[k][2]);
           } else {
-            const double ri2 = ri * ri;
+            // stresslet: normal of the source; traction: normal of the target
+            const double m0 = kTrac ? tn0[k] : n0, m1 = kTrac ? tn1[k] : n1, m2 = kTrac ? tn2[k] : n2;
             const double rd = fma(dx, d0, fma(dy, d1, dz * d2));
-            const double rn = fma(dx, n0, fma(dy, n1, dz * n2));
-            const double f0 = rd * rn * (ri2 * ri2 * ri);
+            const double rn = fma(dx, m0, fma(dy, m1, dz * m2));
+            double f0 = times_rsqrt5(rd * rn, r2);
+            if (MODE != F3D_SELF_REGULARISE) f0 = skip ? 0.0 : f0;
             acc[k][0] = fma(f0, dx, acc[k][0]);
             acc[k][1] = fma(f0, dy, acc[k][1]);
             acc[k][2] = fma(f0, dz, acc[k][2]);
@@ -281,9 +332,19 @@ __global__ void __launch_bounds__(kBlock) pair_kernel(const PairArgs a) {
           const f32x2 dz = add2(sub2(pzh[k], szh), sub2(pzl[k], szl));
           float ra, rb;
           up2(fma2(dx, dx, fma2(dy, dy, mul2(dz, dz))), ra, rb);
-          ra = (ra < eps2f) ? ra + reg2f : ra;
-          rb = (rb < eps2f) ? rb + reg2f : rb;
+          // SKIP_CLOSE drops r <= eps here, so that a coincident pair is
+          // dropped even when eps^2 underflows in float
+          const bool ca = (MODE == F3D_SELF_SKIP_CLOSE) ? !(ra > eps2f) : (ra < eps2f);
+          const bool cb = (MODE == F3D_SELF_SKIP_CLOSE) ? !(rb > eps2f) : (rb < eps2f);
+          if (MODE != F3D_SELF_SKIP_CLOSE) {
+            ra = ca ? ra + reg2f : ra;
+            rb = cb ? rb + reg2f : rb;
+          }
           float ia = rsqrtf(ra), ib = rsqrtf(rb);
+          if (MODE == F3D_SELF_SKIP_CLOSE) {
+            ia = ca ? 0.f : ia;
+            ib = cb ? 0.f : ib;
+          }
           if (MODE == F3D_SELF_SKIP_INDEX) {
             const int64_t s0 = sbase + 2 * q;
             ia = (s0 == tidx[k]) ? 0.f : ia;
@@ -308,7 +369,8 @@ __global__ void __launch_bounds__(kBlock) pair_kernel(const PairArgs a) {
           } else {
             const f32x2 ri2 = mul2(ri, ri);
             const f32x2 rd = fma2(dx, d0, fma2(dy, d1, mul2(dz, d2)));
-            const f32x2 rn = fma2(dx, n0, fma2(dy, n1, mul2(dz, n2)));
+            const f32x2 rn = kTrac ? fma2(dx, pn0[k], fma2(dy, pn1[k], mul2(dz, pn2[k])))
+                                   : fma2(dx, n0, fma2(dy, n1, mul2(dz, n2)));
             const f32x2 f0 = mul2(mul2(rd, rn), mul2(mul2(ri2, ri2), ri));
             ft[k][0] = fma2(f0, dx, ft[k][0]);
             ft[k][1] = fma2(f0, dy, ft[k][1]);
@@ -398,7 +460,7 @@ __global__ void __launch_bounds__(kBlock) pair_kernel(const PairArgs a) {
     for (int64_t i = 0; i < ntl; ++i) {
       const int st = static_cast<int>(i & 1);
       const uint32_t parity = static_cast<uint32_t>((i >> 1) & 1);
-      const bool ok = mbar_wait_bounded(&bars[st], parity);
+      const bool ok = mbar_wait_bounded(&bars[st], parity, a.wait_ns);
       if (ok) compute_tile(stages + st * St::bytes, kTile, (tile0 + i) * kTile);
       if (__syncthreads_or(!ok)) { ok_all = false; break; }
       if (tid == 0 && i + 2 < ntl) {
@@ -410,7 +472,7 @@ __global__ void __launch_bounds__(kBlock) pair_kernel(const PairArgs a) {
       // Give copies still in flight a bounded chance to land before exit.
       if (tid == 0) {
         record_error(a.err, F3D_ERR_TIMEOUT);
-        for (int st = 0; st < 2; ++st) (void)mbar_wait_bounded(&bars[st], 0);
+        for (int st = 0; st < 2; ++st) (void)mbar_wait_bounded(&bars[st], 0, a.wait_ns);
       }
       return;
     }
@@ -551,7 +613,7 @@ struct Plan {
 
 static int make_plan(int kernel, int precision, int64_t ns, int64_t nt, const f3d_pair_shape *shape,
                      Plan *p, bool dual = false) {
-  if (kernel < 0 || kernel > 2 || precision < 0 || precision > 1) return F3D_ERR_ARG;
+  if (kernel < 0 || kernel > 3 || precision < 0 || precision > 1) return F3D_ERR_ARG;
   if (ns < 0 || nt < 0) return F3D_ERR_SHAPE;
   int tpt = shape && shape->tpt ? shape->tpt : 0;
   int sl = shape && shape->sl ? shape->sl : 0;
@@ -633,6 +695,7 @@ static int dispatch_mode(int mode, const PairArgs &a, const Plan &p, cudaStream_
     case F3D_SELF_REGULARISE: return dispatch_shape<KIND, F3D_SELF_REGULARISE, PREC>(a, p, st);
     case F3D_SELF_SKIP_INDEX: return dispatch_shape<KIND, F3D_SELF_SKIP_INDEX, PREC>(a, p, st);
     case F3D_SELF_SKIP_GROUP: return dispatch_shape<KIND, F3D_SELF_SKIP_GROUP, PREC>(a, p, st);
+    case F3D_SELF_SKIP_CLOSE: return dispatch_shape<KIND, F3D_SELF_SKIP_CLOSE, PREC>(a, p, st);
     default: return F3D_ERR_ARG;
   }
 }
@@ -656,11 +719,13 @@ static int pair_sum_core(int kernel, int precision, int self_mode, const double 
   Plan p;
   int rc = make_plan(kernel, precision, ns, nt, shape, &p, dual);
   if (rc) return rc;
-  if (self_mode < 0 || self_mode > 2) return F3D_ERR_ARG;
+  if (self_mode < 0 || self_mode > 3) return F3D_ERR_ARG;
+  if (dual && self_mode == F3D_SELF_SKIP_CLOSE) return F3D_ERR_ARG;
   if (nt == 0) return F3D_OK;
   if (!rt || !out) return F3D_ERR_NULL;
   if (ns > 0 && (!rs || !dens)) return F3D_ERR_NULL;
   if (kernel == F3D_KERNEL_STRESSLET && ns > 0 && !nrm) return F3D_ERR_NULL;
+  if (kernel == F3D_KERNEL_TRACTION && !nrm) return F3D_ERR_NULL;  // target normals
   if (self_mode == F3D_SELF_SKIP_GROUP && (!gt || (ns > 0 && !gs))) return F3D_ERR_NULL;
   if (self_mode == F3D_SELF_SKIP_INDEX && ns != nt) return F3D_ERR_SHAPE;
   if (!aligned(rs, 8) || !aligned(rt, 8) || !aligned(dens, 8) || !aligned(nrm, 8) ||
@@ -690,13 +755,15 @@ static int pair_sum_core(int kernel, int precision, int self_mode, const double 
   a.counters = p.nsplit > 1 ? reinterpret_cast<unsigned *>(w + p.off_counters) : nullptr;
   a.packed = precision == F3D_FP32C ? reinterpret_cast<float *>(w + p.off_packed) : nullptr;
   a.err = device_error_word();
+  a.wait_ns = wait_limit_ns();
   a.ns = ns; a.nt = nt;
   a.tiles_per_split = p.tiles_per_split;
   a.nsplit = p.nsplit;
   a.accumulate = accumulate ? 1 : 0;
   a.eps2 = eps * eps;
   a.reg2 = reg * reg;
-  a.scale = (kernel == F3D_KERNEL_STRESSLET) ? -3.0 / (4.0 * kPi * eta) : 1.0 / (8.0 * kPi * eta);
+  a.scale = (kernel == F3D_KERNEL_STRESSLET || kernel == F3D_KERNEL_TRACTION) ? -3.0 / (4.0 * kPi * eta)
+                                                                                : 1.0 / (8.0 * kPi * eta);
   // Bulk copies need 16-byte aligned sources; otherwise stage with plain loads.
   a.use_tma = p.use_tma;
   if (precision == F3D_FP64 && (!aligned(rs, 16) || !aligned(dens, 16) ||
@@ -724,6 +791,7 @@ static int pair_sum_core(int kernel, int precision, int self_mode, const double 
   switch (kernel) {
     case F3D_KERNEL_OSEEN: return dispatch_prec<F3D_KERNEL_OSEEN>(precision, self_mode, a, p, st);
     case F3D_KERNEL_STRESSLET: return dispatch_prec<F3D_KERNEL_STRESSLET>(precision, self_mode, a, p, st);
+    case F3D_KERNEL_TRACTION: return dispatch_prec<F3D_KERNEL_TRACTION>(precision, self_mode, a, p, st);
     default: return dispatch_prec<F3D_KERNEL_ROTLET>(precision, self_mode, a, p, st);
   }
 }

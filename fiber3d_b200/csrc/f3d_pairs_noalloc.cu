@@ -27,7 +27,6 @@ int pair_sum_impl(int kernel, int precision, int self_mode, const double *rs, co
                   cudaStream_t st);
 
 constexpr size_t kNoAllocScratchBytes = size_t(32) << 20;  // 32 MiB per device
-constexpr size_t kNoAllocCounterBytes = size_t(256) << 10;  // split counters (first 256 KiB)
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
 
@@ -65,7 +64,7 @@ int f3d_pair_sum_noalloc(int kernel, int precision, int self_mode, const double 
     if ((rc = f3d::noalloc_scratch(&scratch))) return rc;
     // The array keeps whatever the previous call left; the split counters
     // must start at zero, so clear them on this call's stream.
-    const size_t clear = need < f3d::kNoAllocCounterBytes ? need : f3d::kNoAllocCounterBytes;
+    const size_t clear = need < f3d::kCounterBytes ? need : f3d::kCounterBytes;
     if (cudaMemsetAsync(scratch, 0, clear, static_cast<cudaStream_t>(stream)) != cudaSuccess)
       return F3D_ERR_CUDA;
   }

@@ -30,6 +30,10 @@
 
 namespace f3d {
 
+// Node coordinates are addressed as 3 * node in 32-bit int arithmetic, so a
+// surface has at most INT32_MAX / 3 nodes.
+constexpr int64_t kQuadMaxNodes = 0x7fffffffLL / 3;
+
 constexpr int kQuadNbr = 80;                 // nearest neighbours (n in the paper)
 constexpr int kQuadOrder = 7;                // polynomial degree (m)
 constexpr int kQuadPoly = 36;                // (m + 1)(m + 2) / 2
@@ -744,6 +748,7 @@ extern "C" {
 int f3d_surface_quadrature_workspace_bytes(int64_t n, int64_t ntri, size_t *bytes) {
   if (!bytes) return F3D_ERR_NULL;
   if (n < 0 || ntri < 0) return F3D_ERR_SHAPE;
+  if (n > f3d::kQuadMaxNodes) return F3D_ERR_TOO_LARGE;
   *bytes = f3d::quad_layout(n, ntri, nullptr, nullptr);
   return F3D_OK;
 }
@@ -752,7 +757,7 @@ int f3d_surface_quadrature(const double *nodes, int64_t n, const int32_t *triang
                            const double *gradient, double *weights, int32_t *neighbors, void *workspace,
                            size_t workspace_bytes, void *stream) {
   if (n < f3d::kQuadNbr || ntri < 1 || ntri > (1ll << 24)) return F3D_ERR_SHAPE;
-  if (n > (1ll << 30)) return F3D_ERR_TOO_LARGE;
+  if (n > f3d::kQuadMaxNodes) return F3D_ERR_TOO_LARGE;
   if (!nodes || !triangles || !gradient || !weights || !workspace) return F3D_ERR_NULL;
   if (!f3d::aligned(nodes, 8) || !f3d::aligned(gradient, 8) || !f3d::aligned(weights, 8) ||
       !f3d::aligned(workspace, 256) || !f3d::aligned(triangles, 4) || (neighbors && !f3d::aligned(neighbors, 4)))

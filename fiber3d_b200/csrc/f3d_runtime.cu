@@ -1,4 +1,6 @@
-// Library-level plumbing: version, status strings, the per-device error word.
+// Library-level plumbing: version, status strings, the per-device error
+// word, the bounded-wait limit and a self-test of the bounded wait.
+#include <atomic>
 #include <mutex>
 
 #include "f3d_common.cuh"
@@ -23,9 +25,41 @@ int *device_error_word() {
   return addr[dev];
 }
 
+static std::atomic<uint64_t> g_wait_limit_ns{kWaitLimitNs};
+
+uint64_t wait_limit_ns() { return g_wait_limit_ns.load(std::memory_order_relaxed); }
+
+// One CTA waits on an mbarrier that nothing ever arrives on, for at most
+// limit_ns, then records F3D_ERR_TIMEOUT like a kernel whose copy never
+// landed.  No copy is issued, so nothing is in flight when the CTA exits.
+__global__ void bounded_wait_selftest_kernel(uint64_t limit_ns, int *err) {
+  __shared__ __align__(8) uint64_t bar;
+  if (threadIdx.x == 0) {
+    mbar_init(&bar, 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+  if (threadIdx.x == 0 && !mbar_wait_bounded(&bar, 0, limit_ns)) record_error(err, F3D_ERR_TIMEOUT);
+}
+
 }  // namespace f3d
 
 extern "C" {
+
+int f3d_set_wait_limit_ns(uint64_t limit_ns) {
+  f3d::g_wait_limit_ns.store(limit_ns ? limit_ns : f3d::kWaitLimitNs, std::memory_order_relaxed);
+  return F3D_OK;
+}
+
+uint64_t f3d_wait_limit_ns(void) { return f3d::wait_limit_ns(); }
+
+int f3d_selftest_bounded_wait(uint64_t limit_ns, void *stream) {
+  if (limit_ns == 0 || limit_ns > f3d::kWaitLimitNs) return F3D_ERR_ARG;
+  int *err = f3d::device_error_word();
+  if (!err) return F3D_ERR_CUDA;
+  f3d::bounded_wait_selftest_kernel<<<1, 32, 0, static_cast<cudaStream_t>(stream)>>>(limit_ns, err);
+  return f3d::launch_status();
+}
 
 const char *f3d_version(void) { return "fiber3d_b200 0.1.0 (sm_100a)"; }
 

@@ -713,9 +713,26 @@ class HydroSystem:
                 self.lu.solve(rest)
         return y
 
+    def reset_workspaces(self) -> None:
+        """Zero every pair-sum workspace of this system (their split counters
+        must start at zero; a kernel that gave up on a bounded wait may have
+        left some set)."""
+        for name in ("oseen", "stress", "stress_fib", "stress_rest"):
+            call = getattr(self, name, None)
+            for t in (call.ws.values() if call is not None else ()):
+                t.zero_()
+        for name in ("_dual_ws", "_grid_ws"):
+            t = getattr(self, name, None)
+            if t is not None:
+                t.zero_()
+
     def solve(self, tol=1e-8, restart=100, maxiter=200, x0=None, mixed=False, **kw):
         from .gmres import solve_system
         res = solve_system(self, tol=tol, restart=restart, maxiter=maxiter, x0=x0, mixed=mixed, **kw)
+        # a kernel whose bounded wait ran out has returned early: its sums are
+        # incomplete, so the solve is not trusted (raises F3DError after
+        # zeroing the workspaces)
+        _lib.check_device_error("HydroSystem.solve", self.device, on_error=self.reset_workspaces)
         if self.pc_refresh == "auto":
             self._pc_stale = res["iterations"] > 1 or res["history"][-1] > self.PC_AUTO_MARGIN * tol
         return res

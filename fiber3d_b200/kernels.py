@@ -34,9 +34,18 @@ __all__ = [
     "oseen_kernel_source_target_numba", "oseen_kernel_times_density_numba",
     "rotlet_kernel_source_target_numba", "stresslet_kernel_source_target_numba",
     "stresslet_kernel_times_normal_times_density_numba", "stresslet_kernel_times_normal_numba",
-    "oseen_tensor", "oseen_tensor_source_target", "complementary_kernel",
-    "complementary_kernel_times_density_numba", "pair_sum",
+    "traction_kernel_times_normal_times_density_numba", "stresslet_kernel",
+    "stresslet_kernel_times_normal", "oseen_tensor", "oseen_tensor_source_target",
+    "complementary_kernel", "complementary_kernel_times_density_numba",
+    "oseen_kernel_source_target_pycuda", "oseen_kernel_source_target_stkfmm",
+    "stresslet_kernel_source_target_stkfmm", "single_double_layer_kernel_source_target_stkfmm",
+    "pair_sum",
 ]
+
+# The FMM-backed functions (STKFMM) leave out a source that coincides with
+# the target; the direct sums that stand in for them drop pairs closer than
+# this distance (squared: 1e-300, a normal double) and regularise nothing.
+COINCIDENT = 1e-150
 
 
 # Launch shapes of the pair-sum drop-ins come from the autotuner (see above).
@@ -100,12 +109,14 @@ def pair_sum(kernel: str, r_source, r_target, density, normal=None, *, eta=1.0, 
     if d.shape[0] != rs.shape[0]:
         raise ValueError(f"density has {d.shape[0]} points, r_source has {rs.shape[0]}")
     n = None
-    if kernel == "stresslet":
+    if kernel in ("stresslet", "traction"):
         if normal is None:
-            raise ValueError("stresslet needs normals")
+            raise ValueError(f"{kernel} needs normals")
         n = _to_dev(normal, dev, "normal")
-        if n.shape[0] != rs.shape[0]:
-            raise ValueError(f"normal has {n.shape[0]} points, r_source has {rs.shape[0]}")
+        # the stresslet takes the sources' normals, the traction the targets'
+        want, who = (rs.shape[0], "r_source") if kernel == "stresslet" else (rt.shape[0], "r_target")
+        if n.shape[0] != want:
+            raise ValueError(f"normal has {n.shape[0]} points, {who} has {want}")
     gs = gt = None
     if self_mode == "skip_group":
         gs = torch.as_tensor(src_group, dtype=torch.int32, device=dev).contiguous()
@@ -147,7 +158,12 @@ def _drop_in(kernel, r_source, r_target, density, normal, self_mode, eta, reg, e
                               reg=reg, epsilon_distance=epsilon_distance)
     u = pair_sum(kernel, rs, rt, d, n, eta=eta, reg=reg, epsilon_distance=epsilon_distance,
                  self_mode=self_mode, precision=precision, shape=shape)
-    return _out(u, host)
+    res = _out(u, host)
+    if host:
+        # the copy back has synchronised the stream: a bounded wait that ran
+        # out in this sum is reported here rather than returned as numbers
+        _lib.check_device_error(kernel)
+    return res
 
 
 # ------------------------------------------------------------ pair sums ----
@@ -190,6 +206,78 @@ def stresslet_kernel_times_normal_times_density_numba(r_vectors, normal, density
                     epsilon_distance, precision, shape)
 
 
+def traction_kernel_times_normal_times_density_numba(r_vectors, normal, density, eta=1.0,
+                                                     reg=5e-3, epsilon_distance=1e-5, *,
+                                                     precision="fp64", shape=None):
+    """t_i = -3/(4 pi eta) sum_{j != i} (r.d_j)(r.n_i) r / r^5, r = x_i - x_j:
+    the stresslet contracted with the normal of the TARGET (the traction of
+    the single layer).  fiber3d kernels.py:1221-1264; its ``eta = 1.0`` at
+    :1232 comes after the prefactor is formed, so the eta passed in is the
+    one that counts."""
+    return _drop_in("traction", r_vectors, r_vectors, density, normal, "skip_index", eta, reg,
+                    epsilon_distance, precision, shape)
+
+
+def oseen_kernel_source_target_pycuda(r_source, r_target, density, eta=1.0, epsilon_distance=1e-5):
+    """Oseen source -> target sum in which pairs closer than epsilon_distance
+    contribute nothing (no regularisation): the semantics of fiber3d's PyCUDA
+    kernel (kernels.py:849 -> kernels_pycuda.py:22-66, which skips a pair
+    when 1/|r| > 1/epsilon_distance).  The output starts from zero."""
+    return _drop_in("oseen", r_source, r_target, density, None, "skip_close", eta, 0.0,
+                    epsilon_distance, "fp64", None)
+
+
+def oseen_kernel_source_target_stkfmm(r_source, r_target, density, eta=1.0, reg=5e-3,
+                                      epsilon_distance=1e-5, *args, **kwargs):
+    """Stand-in for fiber3d's STKFMM Stokeslet (kernels.py:1298-1364): the
+    same velocity, u_t = 1/(8 pi eta) sum_s [f/r + (r.f) r/r^3], by direct
+    summation on the GPU (exact, where the FMM is accurate to its expansion
+    order).  Like the FMM's kernel it regularises nothing and leaves out
+    coincident source-target pairs.  ``reg``, ``epsilon_distance`` and the
+    FMM handle (``fmm_PVel``) are accepted and unused, as in fiber3d."""
+    return _drop_in("oseen", r_source, r_target, density, None, "skip_close", eta, 0.0,
+                    COINCIDENT, "fp64", None)
+
+
+def stresslet_kernel_source_target_stkfmm(r_source, r_target, normal, density, eta=1.0, reg=5e-3,
+                                          epsilon_distance=1e-5, *args, **kwargs):
+    """Stand-in for fiber3d's STKFMM double layer (kernels.py:1367-1419):
+    v_t = -3/(4 pi eta) sum_s (r.n_s)(r.d_s) r / r^5 by direct summation.
+    fiber3d hands the FMM the double-layer tensor 2 (n (x) d) (:1410) because
+    STKFMM's double-layer kernel carries half of fiber3d's prefactor; the
+    product is this stresslet sum, the one fiber3d checks the FMM against
+    (kernels/test_stkfmm.py).  Coincident pairs are left out, nothing is
+    regularised."""
+    return _drop_in("stresslet", r_source, r_target, density, normal, "skip_close", eta, 0.0,
+                    COINCIDENT, "fp64", None)
+
+
+def single_double_layer_kernel_source_target_stkfmm(r_source_SL, r_source_DL, r_target, normal,
+                                                    density_SL, density_DL, eta=1.0, reg=5e-3,
+                                                    epsilon_distance=1e-5, *args, **kwargs):
+    """Stand-in for fiber3d's combined STKFMM evaluation (kernels.py:1422-1485):
+    the Stokeslet sum of density_SL at r_source_SL plus the double layer of
+    (normal, density_DL) at r_source_DL (fiber3d's 2 (n (x) d) tensor, :1476),
+    on the same targets, by direct summation; coincident pairs left out."""
+    host = _any_host(r_source_SL, r_source_DL, r_target, normal, density_SL, density_DL)
+    dev = _device()
+    rt = _to_dev(r_target, dev, "r_target")
+    u = torch.zeros(3 * rt.shape[0], dtype=torch.float64, device=dev)
+    rsl = _to_dev(r_source_SL, dev, "r_source_SL")
+    if rsl.shape[0]:
+        pair_sum("oseen", rsl, rt, _to_dev(density_SL, dev, "density_SL"), eta=eta, reg=0.0,
+                 epsilon_distance=COINCIDENT, self_mode="skip_close", out=u, accumulate=True)
+    rdl = _to_dev(r_source_DL, dev, "r_source_DL")
+    if rdl.shape[0]:
+        pair_sum("stresslet", rdl, rt, _to_dev(density_DL, dev, "density_DL"), _to_dev(normal, dev, "normal"),
+                 eta=eta, reg=0.0, epsilon_distance=COINCIDENT, self_mode="skip_close", out=u,
+                 accumulate=True)
+    res = _out(u, host)
+    if host:
+        _lib.check_device_error("single_double_layer")
+    return res
+
+
 def complementary_kernel_times_density_numba(r_vectors, normal, density):
     """u_i = n_i sum_j n_j . d_j (rank-one).  fiber3d kernels.py:1267-1283.
 
@@ -221,6 +309,33 @@ def stresslet_kernel_times_normal_numba(r_vectors, normal, eta=1.0, reg=5e-3,
     _lib.call("f3d_stresslet_times_normal_dense", _lib.ptr(x), _lib.ptr(n), _lib.ptr(M), N, 3 * N,
               float(eta), float(reg), float(epsilon_distance), _lib.stream_handle(dev))
     return M.cpu().numpy() if _any_host(r_vectors, normal) else M
+
+
+def stresslet_kernel_times_normal(r_vectors, normal, eta=1.0, reg=5e-3, epsilon_distance=1e-5):
+    """Dense 3N x 3N stresslet contracted with the source normals: block
+    (i, j) = 3/(4 pi eta) (dr.n_j) dr dr^T / dr^5 with dr = x_j - x_i, which
+    is the same matrix as stresslet_kernel_times_normal_numba (r = -dr), zero
+    diagonal blocks; pairs closer than epsilon_distance regularised.  fiber3d
+    kernels.py:995-1060 (numpy form)."""
+    return stresslet_kernel_times_normal_numba(r_vectors, normal, eta, reg, epsilon_distance)
+
+
+def stresslet_kernel(r_vectors, eta=1.0, reg=5e-3, epsilon_distance=1e-5, input_format='r'):
+    """Dense 3-index stresslet tensor, (3N) x (3N) x 3: S[3i+a, 3j+b, c] =
+    fr dr_a dr_b dr_c, dr = x_j - x_i, fr = -3/(4 pi eta dr^5) (dr <=
+    epsilon_distance: (dr^2 + reg^2)^(5/2) in place of dr^5), zero diagonal
+    blocks.  input_format 'r' ((N, 3) points) or 'xyz' (x_all, y_all, z_all).
+    fiber3d kernels.py:911-992."""
+    dev = _device()
+    host = _any_host(r_vectors)
+    size = r_vectors.numel() if isinstance(r_vectors, torch.Tensor) else np.size(r_vectors)
+    N = size // 3
+    xin = _xyz_to_r(r_vectors, N) if input_format != 'r' else r_vectors
+    x = _to_dev(xin, dev, "r_vectors")
+    S = torch.empty((3 * N, 3 * N, 3), dtype=torch.float64, device=dev)
+    _lib.call("f3d_stresslet_tensor_dense", _lib.ptr(x), _lib.ptr(S), N, float(eta), float(reg),
+              float(epsilon_distance), _lib.stream_handle(dev))
+    return S.cpu().numpy() if host else S
 
 
 def _xyz_to_r(x, N):

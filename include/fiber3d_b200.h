@@ -45,7 +45,10 @@ typedef enum f3d_status {
 typedef enum f3d_kernel {
   F3D_KERNEL_OSEEN = 0,      /* u_t = 1/(8 pi eta) sum_s [f/r + (r.f) r / r^3]      */
   F3D_KERNEL_STRESSLET = 1,  /* v_t = -3/(4 pi eta) sum_s (r.d)(r.n) r / r^5        */
-  F3D_KERNEL_ROTLET = 2      /* u_t = 1/(8 pi eta) sum_s tau x r / r^3              */
+  F3D_KERNEL_ROTLET = 2,     /* u_t = 1/(8 pi eta) sum_s tau x r / r^3              */
+  F3D_KERNEL_TRACTION = 3    /* t_t = -3/(4 pi eta) sum_s (r.d_s)(r.n_t) r / r^5:
+                                the normal is the TARGET's (kernels.py:1221-1264);
+                                `normal` then holds nt target normals             */
 } f3d_kernel;
 
 typedef enum f3d_self_mode {
@@ -58,7 +61,11 @@ typedef enum f3d_self_mode {
   /* pairs whose int32 group ids are equal are skipped (same fiber);
      others are regularised as in F3D_SELF_REGULARISE. This fuses
      flow_fibers + self_flow_fibers (tstep/tstep_utils.py:653-700, 812-851) */
-  F3D_SELF_SKIP_GROUP = 2
+  F3D_SELF_SKIP_GROUP = 2,
+  /* pairs with |r| < eps contribute exactly zero; no regularisation (the
+     PyCUDA Oseen kernel, kernels/kernels_pycuda.py:22-66; with a tiny eps,
+     the coincident-point exclusion of the STKFMM sums, kernels.py:1298-1485) */
+  F3D_SELF_SKIP_CLOSE = 3
 } f3d_self_mode;
 
 typedef enum f3d_precision {
@@ -84,6 +91,21 @@ const char *f3d_status_string(int status);
 /* Reads and clears the device error word of the current device (blocks on
    the given stream).  Returns F3D_OK or F3D_ERR_TIMEOUT. */
 int f3d_get_device_error(void *stream);
+
+/* Bounded waits.  Every kernel that waits on an mbarrier (a bulk copy or a
+   tensor-core MMA landing) gives up after a limit, records F3D_ERR_TIMEOUT in
+   the device error word and returns, so the context stays usable.
+   f3d_set_wait_limit_ns sets the limit that later calls pass to their
+   kernels (0 restores the default, 2 s); f3d_wait_limit_ns reads it.
+   No counterpart in fiber3d (its kernels run on the CPU). */
+int f3d_set_wait_limit_ns(uint64_t limit_ns);
+uint64_t f3d_wait_limit_ns(void);
+
+/* Self-test of the bounded wait: one CTA waits, for limit_ns (1 ns .. 2 s),
+   on an mbarrier that nothing arrives on (no copy is issued), then records
+   F3D_ERR_TIMEOUT in the device error word.  It exercises the timeout
+   reporting path without any fault.  No counterpart in fiber3d. */
+int f3d_selftest_bounded_wait(uint64_t limit_ns, void *stream);
 
 /* Launches an FMA-throughput probe (precision F3D_FP64 or F3D_FP32C = FP32)
    on `stream`; *flops receives the floating-point operations it performs
@@ -118,9 +140,12 @@ int f3d_pair_sum(int kernel, int precision, int self_mode,
    process exits; sizes whose f3d_pair_workspace_bytes (default shape)
    exceeds 32 MiB return F3D_ERR_TOO_LARGE.  The first call on a device looks
    up that array's device address (make it before any stream capture).
-   Calls share the array: two calls that overlap on the GPU (different
-   streams, or devices sharing nothing but the call) race; order them on one
-   stream.  Allocates nothing. */
+   Each device has its own copy of the array, so calls on different devices
+   never interfere; calls on the same device share it, and two of them that
+   overlap on that GPU (different streams) race: order them on one stream.
+   The cached address belongs to the device's current context: the library
+   must not be used across a cudaDeviceReset of that device.  Allocates
+   nothing. */
 int f3d_pair_sum_noalloc(int kernel, int precision, int self_mode,
                          const double *r_source, const double *r_target,
                          const double *density, const double *normal,
@@ -210,6 +235,14 @@ int f3d_oseen_tensor_source_target_dense(const double *r_source, const double *r
                                          double *G, int64_t ns, int64_t nt, int64_t ld,
                                          double eta, double reg, double epsilon_distance,
                                          void *stream);
+
+/* The 3-index stresslet tensor of N points (replaces stresslet_kernel,
+   python/kernels/kernels.py:911-992, input_format 'r'; the Python drop-in
+   reorders 'xyz' input): S is (3N) x (3N) x 3, row-major, S[3i+a, 3j+b, c] =
+   fr dr_a dr_b dr_c, dr = x_j - x_i, fr = -3/(4 pi eta dr^5) when dr > eps,
+   else -3/(4 pi eta (dr^2 + reg^2)^(5/2)).  N <= 65535. */
+int f3d_stresslet_tensor_dense(const double *r_vectors, double *S, int64_t n, double eta, double reg,
+                               double epsilon_distance, void *stream);
 
 /* replaces complementary_kernel, python/kernels/kernels.py:1286-1295:
    C = outer(normal.flat, normal.flat), 3n x 3n, row-major, ld >= 3n. */
@@ -556,7 +589,9 @@ int f3d_mse_grad(const float *Y, const float *T, float *D, float *row_loss, int3
    triangle's plane.  nodes (n x 3), gradient (n x 3, gradh at the nodes),
    triangles (ntri x 3, any vertex order; a closed surface, every edge shared
    by exactly two triangles) -> weights (n).  neighbors (ntri x 80, nearest
-   first) receives each triangle's nodes when non-NULL.  n >= 80.
+   first) receives each triangle's nodes when non-NULL.  80 <= n <=
+   715827882 (INT32_MAX / 3: node coordinates are indexed in 32-bit
+   arithmetic), 1 <= ntri <= 2^24; larger n returns F3D_ERR_TOO_LARGE.
    Bad triangulations and zero pivots are reported through the device error
    word (F3D_ERR_ARG, F3D_ERR_SINGULAR; f3d_get_device_error). */
 int f3d_surface_quadrature_workspace_bytes(int64_t n, int64_t ntri, size_t *bytes);

@@ -170,3 +170,75 @@ def complementary_kernel_times_density(r_vectors, normal, density):
     """complementary_kernel_times_density_numba, kernels.py:1267-1283."""
     n, d = _pts(normal), _pts(density)
     return (n * np.sum(n * d)).reshape(-1)
+
+
+def traction_kernel_times_normal_times_density(r_vectors, normal, density, eta=1.0, reg=5e-3,
+                                               epsilon_distance=1e-5):
+    """traction_kernel_times_normal_times_density_numba, kernels.py:1221-1264:
+    t_i = -3/(4 pi eta) sum_{j != i} (r.d_j)(r.n_i) r / r^5, r = x_i - x_j (the
+    normal of the target; the eta = 1.0 at :1232 follows the prefactor)."""
+    x, n, d = _pts(r_vectors), _pts(normal), _pts(density)
+    factor = -3.0 / (4.0 * np.pi * eta)
+    v = np.zeros_like(x)
+    for t0 in range(0, x.shape[0], CHUNK):
+        t1 = min(t0 + CHUNK, x.shape[0])
+        r, rn = _pair_geometry(x[t0:t1], x, reg, epsilon_distance)
+        w = factor / rn**5 * np.einsum("tsk,sk->ts", r, d) * np.einsum("tsk,tk->ts", r, n[t0:t1])
+        idx = np.arange(t0, t1)
+        w[idx - t0, idx] = 0.0
+        v[t0:t1] = np.einsum("ts,tsk->tk", w, r)
+    return v.reshape(-1)
+
+
+def stresslet_kernel(r_vectors, eta=1.0, reg=5e-3, epsilon_distance=1e-5, input_format='r'):
+    """stresslet_kernel, kernels.py:911-992: S[3i+a, 3j+b, c] = fr dr_a dr_b dr_c,
+    dr = x_j - x_i, fr = -3/(4 pi eta dr^5) for dr > eps, -3/(4 pi eta
+    (dr^2 + reg^2)^2.5) otherwise."""
+    N = np.size(r_vectors) // 3
+    x = _pts(r_vectors) if input_format == 'r' else np.asarray(r_vectors, dtype=np.float64).reshape(3, N).T
+    dr = x[None, :, :] - x[:, None, :]
+    d = np.sqrt(np.einsum("ijk,ijk->ij", dr, dr))
+    fr = np.where(d > epsilon_distance, -3.0 / (4.0 * np.pi * eta * np.where(d > 0, d, 1.0) ** 5),
+                  -3.0 / (4.0 * np.pi * eta * np.power(d**2 + reg**2, 2.5)))
+    S = np.einsum("ij,ija,ijb,ijc->iajbc", fr, dr, dr, dr)
+    return S.reshape(3 * N, 3 * N, 3)
+
+
+def oseen_kernel_source_target_skip_close(r_source, r_target, density, eta=1.0, epsilon_distance=1e-5):
+    """Oseen source -> target sum without regularisation in which pairs with
+    |r| < epsilon_distance contribute nothing: fiber3d's PyCUDA kernel
+    (kernels/kernels_pycuda.py:22-66, reached from kernels.py:849) and, with
+    a vanishing epsilon_distance, the coincident-point exclusion of the
+    STKFMM-backed sums (kernels.py:1298-1364)."""
+    xs, xt, f = _pts(r_source), _pts(r_target), _pts(density)
+    factor = 1.0 / (8.0 * np.pi * eta)
+    u = np.zeros_like(xt)
+    for t0 in range(0, xt.shape[0], CHUNK):
+        t1 = min(t0 + CHUNK, xt.shape[0])
+        r = xt[t0:t1, None, :] - xs[None, :, :]
+        rn = np.sqrt(np.einsum("tsk,tsk->ts", r, r))
+        keep = rn >= epsilon_distance
+        rs = np.where(keep, rn, 1.0)
+        fr = np.where(keep, factor / rs, 0.0)
+        gr = np.where(keep, factor / rs**3, 0.0)
+        u[t0:t1] = fr @ f + np.einsum("ts,tsk->tk", gr * np.einsum("tsk,sk->ts", r, f), r)
+    return u.reshape(-1)
+
+
+def stresslet_kernel_source_target_skip_close(r_source, r_target, normal, density, eta=1.0,
+                                              epsilon_distance=1e-150):
+    """Stresslet source -> target sum without regularisation, pairs with
+    |r| < epsilon_distance left out: the direct-sum value of fiber3d's
+    STKFMM double layer with its 2 (n (x) d) density (kernels.py:1367-1419)."""
+    xs, xt, n, d = _pts(r_source), _pts(r_target), _pts(normal), _pts(density)
+    factor = -3.0 / (4.0 * np.pi * eta)
+    v = np.zeros_like(xt)
+    for t0 in range(0, xt.shape[0], CHUNK):
+        t1 = min(t0 + CHUNK, xt.shape[0])
+        r = xt[t0:t1, None, :] - xs[None, :, :]
+        rn = np.sqrt(np.einsum("tsk,tsk->ts", r, r))
+        keep = rn >= epsilon_distance
+        rs = np.where(keep, rn, 1.0)
+        w = np.where(keep, factor / rs**5, 0.0) * np.einsum("tsk,sk->ts", r, d) * np.einsum("tsk,sk->ts", r, n)
+        v[t0:t1] = np.einsum("ts,tsk->tk", w, r)
+    return v.reshape(-1)

@@ -18,10 +18,13 @@ import os
 import sys
 import types
 
-REFERENCE_PY = os.environ.get("FIBER3D_REFERENCE", "/root/reference/python")
+REFERENCE_PY = os.environ.get("FIBER3D_REFERENCE")
 
 
 def install() -> str:
+    if not REFERENCE_PY:
+        raise RuntimeError("set FIBER3D_REFERENCE to the python/ folder of a fiber3d checkout "
+                           "(the fixture generators run fiber3d's own code)")
     if "imp" not in sys.modules:
         imp = types.ModuleType("imp")
 

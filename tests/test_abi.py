@@ -125,3 +125,16 @@ def test_argument_checks_of_surface_quadrature(dll):
     p8, p_odd = ctypes.c_void_p(4096), ctypes.c_void_p(4100)
     assert dll.f3d_surface_quadrature(p8, 400, p8, 796, p8, p8, None, p_odd, 1 << 30, None) == ALIGN
     assert dll.f3d_surface_quadrature(p8, 400, p8, 796, p8, p8, None, p8, 16, None) == WORKSPACE
+
+
+def test_wait_limit_setting_and_selftest_checks(dll):
+    """The bounded-wait limit is a host-side setting (no device needed); the
+    self-test rejects a zero or over-long limit before any launch."""
+    try:
+        assert dll.f3d_set_wait_limit_ns(123456) == 0
+        assert dll.f3d_wait_limit_ns() == 123456
+    finally:
+        assert dll.f3d_set_wait_limit_ns(0) == 0
+    assert dll.f3d_wait_limit_ns() == 2_000_000_000
+    assert dll.f3d_selftest_bounded_wait(0, None) == 5
+    assert dll.f3d_selftest_bounded_wait(3_000_000_000, None) == 5

@@ -309,3 +309,37 @@ def test_fp32c_odd_source_counts(K, ns, kind, mode):
         assert np.abs(u32).max() == 0.0
     else:
         assert rel_err(u32, u64) < TOL32
+
+
+@pytest.mark.parametrize("shape", [(1, 1, 0, 0), (2, 1, 0, 0), (1, 8, 4, 0), (1, 32, 0, -1), (1, 1, 7, -1)])
+@pytest.mark.parametrize("n", [1, 129, 700])
+def test_traction_shapes(K, L, shape, n):
+    """Traction (normal of the target, j == i skipped) at every launch shape."""
+    rng = np.random.default_rng(n + 31)
+    x = rng.random((n, 3))
+    if n > 20:
+        x[10] = x[11]
+    d = rng.normal(size=(n, 3)); nr = rng.normal(size=(n, 3))
+    ref = O.traction_kernel_times_normal_times_density(x, nr, d)
+    u = K.pair_sum("traction", x, x, d, nr, self_mode="skip_index", shape=L.PairShape(*shape))
+    assert rel_err(u.cpu().numpy(), ref) < TOL64
+
+
+@pytest.mark.parametrize("shape", [(1, 1, 0, 0), (2, 1, 3, 0), (1, 8, 0, -1), (1, 32, 5, 0)])
+@pytest.mark.parametrize("kind", ["oseen", "stresslet"])
+def test_skip_close_shapes(K, L, shape, kind):
+    """Pairs closer than eps contribute zero (coincident ones included), at
+    every launch shape, FP64 against the oracle."""
+    rng = np.random.default_rng(99)
+    xs = rng.random((400, 3)); xt = rng.random((333, 3))
+    xt[:5] = xs[:5]
+    xt[5:9] = xs[5:9] + 2e-6 * rng.normal(size=(4, 3))
+    d = rng.normal(size=(400, 3)); nr = rng.normal(size=(400, 3))
+    if kind == "oseen":
+        ref = O.oseen_kernel_source_target_skip_close(xs, xt, d, epsilon_distance=1e-5)
+        u = K.pair_sum("oseen", xs, xt, d, self_mode="skip_close", epsilon_distance=1e-5, shape=L.PairShape(*shape))
+    else:
+        ref = O.stresslet_kernel_source_target_skip_close(xs, xt, nr, d, epsilon_distance=1e-5)
+        u = K.pair_sum("stresslet", xs, xt, d, nr, self_mode="skip_close", epsilon_distance=1e-5,
+                       shape=L.PairShape(*shape))
+    assert rel_err(u.cpu().numpy(), ref) < TOL64
