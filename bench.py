@@ -57,9 +57,10 @@ def make_workload(name: str):
         grp_s = np.arange(n, dtype=np.int32)
         pairs = n * (n - 1) + n * vol.shape[0]
         return dict(kind="stresslet", src=nodes, trg=targets, dens=q, nrm=normals, gs=grp_s,
-                    gt=grp_t, pairs=pairs, nodes=nodes, vol=vol,
+                    gt=grp_t, pairs=pairs, nodes=nodes, vol=vol, w=w,
                     desc="stresslet double layer, 12000-node sphere R=10 -> 12000 nodes "
-                         "(j==i skipped) + 4096 ball points R=9, FP64")
+                         "(j==i skipped, then the O(N) singularity subtraction of the periphery "
+                         "operator) + 4096 ball points R=9, FP64")
     if name == "oseen_fibers":
         x, f = geometry.oseen_fiber_workload(seed=1)
         n = x.shape[0]
@@ -69,6 +70,23 @@ def make_workload(name: str):
                     desc="Oseen sum, 32 straight fibers x 32 Chebyshev-Lobatto nodes, "
                          "j==i skipped, FP64")
     raise SystemExit(f"unknown workload {name}")
+
+
+def workload_config(name: str, wl) -> dict:
+    """The `config` of a pair-sum line; identical in both arms."""
+    return {"workload": name, "description": wl["desc"], "pairs_per_step": wl["pairs"],
+            "l2": "flushed between steps (256 MiB write, outside the event pairs)"}
+
+
+def host_cores() -> dict:
+    """Threads the CPU legs use and the host's physical cores."""
+    from oracle import pairs_c
+    try:
+        import psutil
+        phys = psutil.cpu_count(logical=False)
+    except Exception:  # noqa: BLE001
+        phys = None
+    return {"threads": pairs_c.max_threads(), "physical_cores": phys, "logical_cpus": os.cpu_count()}
 
 
 class ClockSampler:
@@ -182,12 +200,32 @@ def gpu_arm(args, rank, world, local):
     from fiber3d_b200 import autotune
     shapes = {p: autotune.tune(kind, src, trg, dens, nrm, self_mode="skip_group", src_group=gs,
                                trg_group=gt, precision=p) for p in ("fp64", "fp32c")}
+    launches_per_step = 1
+    subtract = None
+    if kind == "stresslet":
+        # the periphery operator's rows on the node targets (tstep.py:1097-1104):
+        # res = v - E mu - mu + n sum(n.q), E the singularity-subtraction vectors
+        from fiber3d_b200.hydro import singularity_vectors
+        n_nodes = wl["nodes"].shape[0]
+        wts = to(wl["w"])
+        E = singularity_vectors(src, nrm, wts, 1.0, 5e-3, 1e-5)
+        res = torch.empty(3 * n_nodes, dtype=torch.float64, device=dev)
+        scratch = torch.zeros(1, dtype=torch.float64, device=dev)
+        launches_per_step = 2
+
+        def subtract():
+            L.call("f3d_shell_residual", L.ptr(out), L.ptr(E), L.ptr(wts), L.ptr(nrm), L.ptr(dens), L.ptr(res),
+                   n_nodes, L.ptr(scratch), L.stream_handle(dev))
 
     def step(precision="fp64"):
         K.pair_sum(kind, src, trg, dens, nrm, self_mode="skip_group", src_group=gs, trg_group=gt,
                    precision=precision, out=out, shape=shapes[precision])
+        if subtract is not None:
+            subtract()
 
-    def timed(precision, steps, warmup):
+    def timed(precision, steps, warmup, kernel_times=None):
+        """Per-step device times (ms); with kernel_times, also the pair
+        kernel's own time in each step (an event between the two launches)."""
         for _ in range(warmup):
             step(precision)
         torch.cuda.synchronize()
@@ -196,22 +234,28 @@ def gpu_arm(args, rank, world, local):
         evs = []
         for _ in range(steps):
             flush.fill_(1)
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
             torch.cuda.nvtx.range_push(f"timed_pairs_{precision}")
             e0.record()
-            step(precision)
+            K.pair_sum(kind, src, trg, dens, nrm, self_mode="skip_group", src_group=gs, trg_group=gt,
+                       precision=precision, out=out, shape=shapes[precision])
             e1.record()
+            if subtract is not None:
+                subtract()
+            e2.record()
             torch.cuda.nvtx.range_pop()
-            evs.append((e0, e1))
+            evs.append((e0, e1, e2))
         torch.cuda.synchronize()
         replicas.barrier()
-        times = [a.elapsed_time(b) for a, b in evs]
-        return times
+        if kernel_times is not None:
+            kernel_times.extend(a.elapsed_time(b) for a, b, _ in evs)
+        return [a.elapsed_time(c) for a, _, c in evs]
 
     peak64 = measured_peak(L, "fp64", torch)
     peak32 = measured_peak(L, "fp32c", torch)
+    kern_ms = []
     with ClockSampler(local) as clk:
-        t_ms = timed("fp64", args.steps, args.warmup)
+        t_ms = timed("fp64", args.steps, args.warmup, kernel_times=kern_ms)
     clocks = clk.summary()
     total_ms, = replicas.max_over_ranks([sum(t_ms)], dev)
     ms_step = total_ms / args.steps
@@ -255,18 +299,19 @@ def gpu_arm(args, rank, world, local):
     e2e_value = replicas.aggregate_rate(pairs, args.steps, world, e2e_ms)
 
     flop_pair = FLOP_PER_PAIR[kind]
-    achieved = flop_pair * pairs / (min(t_ms) * 1e-3)
+    kern_avg = sum(kern_ms) / len(kern_ms)
+    achieved = flop_pair * pairs / (kern_avg * 1e-3)
     line = {
         "metric": "Stokes pair interactions per second (FP64)",
         "value": value, "unit": "pairs/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
-        "config": {"workload": args.workload, "description": wl["desc"], "pairs_per_step": pairs,
-                   "l2": "flushed between steps (256 MiB write, outside the event pairs)",
-                   "launch_shape": {p: [v.tpt, v.sl, v.nsplit, v.use_tma] for p, v in shapes.items()},
-                   "parallelism": f"replicas x{world}"},
+        "config": workload_config(args.workload, wl),
+        "parallelism": f"replicas x{world}",
+        "launch_shape": {p: [v.tpt, v.sl, v.nsplit, v.use_tma] for p, v in shapes.items()},
         "roofline": {"bound": "fp64", "achieved": achieved / 1e12, "peak": peak64 / 1e12,
                      "unit": "TFLOP/s", "frac": achieved / peak64,
+                     "kernel_ms_avg": kern_avg,
                      # DRAM bytes per launch of this kernel on this workload, from an ncu capture
                      # of it (read 1.391 MB, write 0): the sources stay in L2
                      "traffic": 1391104 if args.workload == "stresslet_sphere" else None,
@@ -281,10 +326,13 @@ def gpu_arm(args, rank, world, local):
                 "d2h_bytes_per_step": d2h,
                 "path": "fiber3d_b200.kernels drop-in calls from pinned host tensors"},
         "clocks": clocks,
-        "gpu_launches": args.steps * 1,
+        "gpu_launches": args.steps * launches_per_step,
     }
     if rank == 0 and world == 1:
         line["cpu_baseline"] = cpu_baseline(wl, seconds=args.cpu_seconds)
+    summary = {"cfg2_pairs_fp64": {"ms_per_step": ms_step, "kernel_ms": kern_avg, "gpairs_per_s": value / 1e9,
+                                   "e2e_gpairs_per_s": e2e_value / 1e9, "roofline_frac": achieved / peak64,
+                                   "fp32c_max_rel_err": err32}}
     if args.workload == "stresslet_sphere" and not args.no_step:
         # the other half of the headline: full time step (512 fibers x 32
         # points, 4 spheres, 12000-node periphery, GMRES rel. residual 1e-8),
@@ -300,12 +348,40 @@ def gpu_arm(args, rank, world, local):
             "speedup_learned_mixed_vs_plain_fp64": st["learned_mixed"]["speedup_vs_fp64"],
             "modes": {m: {k: v[k] for k in ("ms_per_step", "ms_per_step_last_half", "iterations", "long_solves",
                                             "true_rel_residual", "tol", "fiber_pc_rebuilt", "fp64_residuals",
-                                            "first_residual_bound_max",
-                                            "rel_err_vs_fp64_1e-12_solve", "speedup_vs_fp64", "phases_ms")}
+                                            "first_residual_bound_max", "oracle",
+                                            "rel_err_vs_fp64_1e-12_solve", "speedup_vs_fp64", "phases_ms")
+                          if k in v}
                       for m, v in st.items() if m not in ("training", "grid_velocity")},
             "training": st["training"],
             "grid_velocity": st.get("grid_velocity"),
         }
+        s3 = {"fp64_ms": st["fp64"]["ms_per_step"]}
+        for m in ("learned_mixed", "learned_mixed_tol1e-9", "extrapolate_mixed"):
+            s3[f"{m}_ms"] = st[m]["ms_per_step"]
+            s3[f"{m}_speedup"] = st[m]["speedup_vs_fp64"]
+            s3[f"{m}_err_vs_fp64_solve"] = st[m]["rel_err_vs_fp64_1e-12_solve"]
+        for m in ORACLE_MODES:
+            o = st[m].get("oracle")
+            if o:
+                s3[f"{m}_oracle_true_residual"] = o["true_rel_residual"]
+        cpu = st["fp64"].get("oracle", {}).get("cpu_step")
+        if cpu:
+            s3["cpu_step_s"] = cpu["value_s"]
+            s3["cpu_threads"] = cpu["threads"]
+        s3["learned_correction_scale"] = st["training"]["scale"]
+        summary["cfg3_step"] = s3
+        # config 4: the batched block-diagonal preconditioner
+        bp = block_pc_measure(args, dev, 10, 3, args.cpu_seconds)
+        line["block_pc"] = {"config": f"{args.nblocks} fibers, N uniform in {{16,24,32,48,64}}, 4N x 4N blocks, "
+                                      "factor + solve in one CUDA graph", **bp}
+        summary["cfg4_block_pc"] = {k: bp[k] for k in ("ms", "gflops", "max_rel_err_vs_scipy", "cpu_ms", "cpu_cores")}
+        # config 1: the 1024-point Oseen sum
+        of = oseen_fibers_measure(args, dev, 50, 5, args.cpu_seconds)
+        line["oseen_fibers"] = {"config": "32 fibers x 32 Chebyshev-Lobatto nodes, Oseen j != i, FP64", **of}
+        summary["cfg1_oseen_1024"] = {k: of[k] for k in ("us_per_call", "hbm_gbs", "e2e_us_per_call",
+                                                         "cpu_pairs_per_s")}
+    # last, so that a tail of the line carries it
+    line["summary"] = summary
     if rank == 0:
         print(json.dumps(line), flush=True)
 
@@ -335,12 +411,12 @@ def cpu_sample_rate(wl, nthreads: int, seconds: float):
 
 
 def cpu_baseline(wl, seconds: float):
-    from oracle import pairs_c
-    threads = pairs_c.max_threads()
-    rate, nt, reps = cpu_sample_rate(wl, threads, seconds)
-    return {"value": rate, "unit": "pairs/s", "cores": threads, "kind": "port",
+    hc = host_cores()
+    rate, nt, reps = cpu_sample_rate(wl, hc["threads"], seconds)
+    return {"value": rate, "unit": "pairs/s", "cores": hc["threads"], **hc, "kind": "port",
             "sample": f"{nt} of {wl['trg'].shape[0]} targets x {wl['src'].shape[0]} sources, "
-                      f"best of {reps}; C/OpenMP restatement of fiber3d's numba loop"}
+                      f"best of {reps}; C/OpenMP restatement of fiber3d's numba loop "
+                      "(cores = OpenMP threads used)"}
 
 
 def reference_arm(args, rank, world):
@@ -349,9 +425,9 @@ def reference_arm(args, rank, world):
     if args.workload == "surface_quadrature":
         quadrature_reference_arm(args, world)
         return
-    from oracle import pairs_c
     wl = make_workload(args.workload)
-    threads = pairs_c.max_threads()
+    hc = host_cores()
+    threads = hc["threads"]
     per_step = max(1.0, args.cpu_seconds / max(args.steps, 1))
     rates = []
     for _ in range(args.warmup):
@@ -366,14 +442,72 @@ def reference_arm(args, rank, world):
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": wl["pairs"] / value * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
-        "config": {"workload": args.workload, "description": wl["desc"],
-                   "pairs_per_step": wl["pairs"], "parallelism": "host cores"},
-        "cpu_baseline": {"value": value, "unit": "pairs/s", "cores": threads, "kind": "port",
+        "config": workload_config(args.workload, wl),
+        "parallelism": f"host cores (rank 0 of {world})",
+        "cpu_baseline": {"value": value, "unit": "pairs/s", "cores": threads, **hc, "kind": "port",
                          "sample": f"{nt} targets x {wl['src'].shape[0]} sources per step sample; "
                                    "C/OpenMP restatement of fiber3d's numba loop (oracle/)"},
         "e2e": {"value": value, "unit": "pairs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
+
+
+# modes whose first timed step is checked against the CPU oracle
+ORACLE_MODES = ("fp64", "learned_mixed", "learned_mixed_tol1e-9")
+
+
+def step_oracle(P, snap, cpu_time=False, iterations=None):
+    """The CPU oracle's matrix-free restatement of fiber3d's step
+    (oracle/system.py) at a marched step's geometry: the true relative
+    residual ||b - A x|| / ||b|| of the device solution x with the ORACLE's
+    A and b, the device right-hand side against the oracle's, and the device
+    solution against the device FP64 solve to 1e-12.  With cpu_time, fiber3d's
+    method timed on the host (the step's CPU baseline): building the system
+    (explicit flows, right-hand side, fiber operators and their LU, the
+    singularity vectors), one matvec, one fiber+body preconditioner apply,
+    and the periphery LU apply estimated from a dense 12000^2 matvec scaled to
+    (3 Nshell)^2 (memory bound, like the two triangular solves of lu_solve);
+    total = build + (iterations + 1) x (matvec + preconditioner)."""
+    from oracle import system as S
+    from fiber3d_b200.hydro import quaternion_rotation
+    n_f = [np.asarray(f).reshape(-1, 3).shape[0] for f in P.fibers]
+    offs = np.concatenate([[0], np.cumsum(n_f)])
+    xf = snap["x_fib"].reshape(-1, 3)
+    fibers = [xf[offs[k]:offs[k + 1]] for k in range(len(n_f))]
+    rots = [quaternion_rotation(q) for q in snap["quats"]]
+    t0 = time.perf_counter()
+    op = S.system_at(P, fibers, snap["locs"], rots)
+    t_build = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    res = op.true_residual(snap["sol"])
+    t_mv = time.perf_counter() - t0
+    out = {"true_rel_residual": res,
+           "rhs_rel_err_vs_oracle": float(np.max(np.abs(snap["rhs"] - op.rhs)) / np.max(np.abs(op.rhs))),
+           "fp64_1e-12_solve_true_rel_residual": op.true_residual(snap["ref"]),
+           "geometry": "first timed step (marched)"}
+    if cpu_time:
+        x = snap["sol"]
+        t0 = time.perf_counter()
+        op.pc(x)
+        t_pc = time.perf_counter() - t0
+        m = 12000
+        A = np.random.default_rng(0).random((m, m))
+        v = np.ones(m)
+        A @ v
+        t0 = time.perf_counter()
+        for _ in range(3):
+            A @ v
+        t_small = (time.perf_counter() - t0) / 3
+        del A
+        t_shell = t_small * (3 * op.nshell / m) ** 2
+        its = iterations if iterations is not None else 4
+        total = t_build + (its + 1) * (t_mv + t_pc + t_shell)
+        out["cpu_step"] = {"value_s": total, "build_s": t_build, "matvec_s": t_mv, "pc_fibers_bodies_s": t_pc,
+                           "pc_shell_est_s": t_shell, "iterations": its, **host_cores(),
+                           "kind": "port", "how": "oracle/system.py (C/OpenMP pair sums + numpy/scipy) on the "
+                                                 "host; build + (iterations+1) x (matvec + PC), shell PC "
+                                                 "apply scaled from a 12000^2 dense matvec"}
+    return out
 
 
 def hydro_arm(args, rank, world, local, warmup=None, steps=None, emit=True):
@@ -441,6 +575,7 @@ def hydro_arm(args, rank, world, local, warmup=None, steps=None, emit=True):
              "learned_mixed": ("learned", True, "auto", 1e-8),
              "learned_mixed_tol1e-9": ("learned", True, "auto", 1e-9),
              "learned_mixed_tol1e-10": ("learned", True, "auto", 1e-10)}
+    snap = {}
     for mode, (guess, mixed, pc_refresh, tol) in modes.items():
         sysd = H.HydroSystem(P, shell_op=shell, device=dev, tune=True, pc_refresh=pc_refresh)
         torch.cuda.synchronize()
@@ -500,7 +635,18 @@ def hydro_arm(args, rank, world, local, warmup=None, steps=None, emit=True):
                 # (outside the timed region) is the reference solution
                 ref = sysd.solve(tol=1e-12, restart=100)["x"]
                 xs[mode] = float(torch.linalg.vector_norm(sol - ref) / torch.linalg.vector_norm(ref))
-        out[mode] = {"ms_per_step": statistics.median(times), "iterations": its,
+                if mode in ORACLE_MODES and rank == 0 and world == 1 and not args.no_oracle:
+                    # this step's geometry and solution, for the CPU oracle after the loop
+                    locs, quats = sysd.body_state()
+                    snap[mode] = dict(x_fib=sysd.x_fib.cpu().numpy().copy(), locs=locs, quats=quats,
+                                      sol=sol.cpu().numpy(), rhs=sysd.rhs.cpu().numpy(),
+                                      ref=ref.cpu().numpy())
+        if mode in snap:
+            # checked against the oracle's matrix-free step at this geometry
+            # (and, for fiber3d's method, its CPU time): outside every timing
+            out.setdefault(mode, {})["oracle"] = step_oracle(P, snap.pop(mode), cpu_time=(mode == "fp64"),
+                                                             iterations=statistics.median(its))
+        out[mode] = {**out.get(mode, {}), "ms_per_step": statistics.median(times), "iterations": its,
                      "ms_per_step_last_half": statistics.median(times[len(times) // 2:]),
                      "true_rel_residual": max(resid), "refinements": res.get("refinements", 0),
                      "initial_rel_residual": r0s, "final_rel_residual_bound": finals,
@@ -664,19 +810,17 @@ def quadrature_arm(args, rank, world, local):
     return line
 
 
-def block_pc_arm(args, rank, world, local):
-    """Batched block-diagonal preconditioner: 2000 fibers with point counts
-    uniform in {16, 24, 32, 48, 64} (geometry of the step workload), their
-    4N x 4N systems assembled on the device (fiber3d's fiber operator with
-    BC rows), then factor + solve of all blocks captured in one CUDA graph
-    (two persistent launches plus a copy), panel width from the autotuner.
-    Baseline: scipy.linalg.lu_factor / lu_solve per block, the calls
-    fiber3d makes (tstep_utils.py:1405-1419, tstep.py:985-988)."""
+def block_pc_measure(args, dev, steps, warmup, cpu_seconds):
+    """Batched block-diagonal preconditioner (config 4): 2000 fibers with
+    point counts uniform in {16, 24, 32, 48, 64} (geometry of the step
+    workload), their 4N x 4N systems assembled on the device (fiber3d's
+    fiber operator with BC rows), then factor + solve of all blocks captured
+    in one CUDA graph (two persistent launches plus a copy), panel width from
+    the autotuner.  Baseline: scipy.linalg.lu_factor / lu_solve per block,
+    the calls fiber3d makes (tstep_utils.py:1405-1419, tstep.py:985-988)."""
     import torch
     import scipy.linalg as sla
     from fiber3d_b200 import geometry, hydro as H, replicas
-    torch.cuda.set_device(local)
-    dev = torch.device("cuda", local)
     rng = np.random.default_rng(4)
     npts = rng.choice([16, 24, 32, 48, 64], size=args.nblocks)
     fibers = geometry.perturbed_fibers(rng, args.nblocks, npts, 2.0, 10.0, min_sep=0.05)
@@ -688,13 +832,16 @@ def block_pc_arm(args, rank, world, local):
     rhs = torch.as_tensor(rng.normal(size=lu.nvec), device=dev)
     x = torch.empty_like(rhs)
     panel = lu.tune_panel()
-    flop = float(sum(2.0 / 3.0 * (4 * n) ** 3 + 2.0 * (4 * n) ** 2 for n in npts))
+    flop_factor = float(sum(2.0 / 3.0 * (4 * n) ** 3 for n in npts))
+    flop = flop_factor + float(sum(2.0 * (4 * n) ** 2 for n in npts))
+    bytes_blocks = float(sum(8 * (4 * n) ** 2 for n in npts))
+
     def work():
         lu.A.copy_(A0)
         lu.factor()
         x.copy_(rhs)
         lu.solve(x)
-    for _ in range(args.warmup):
+    for _ in range(warmup):
         work()
     torch.cuda.synchronize()
     g = torch.cuda.CUDAGraph()
@@ -705,18 +852,18 @@ def block_pc_arm(args, rank, world, local):
     torch.cuda.current_stream(dev).wait_stream(s2)
     with torch.cuda.graph(g):
         work()
-    for _ in range(args.warmup):
+    for _ in range(warmup):
         g.replay()
     torch.cuda.synchronize()
     replicas.barrier()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record()
-    for _ in range(args.steps):
+    for _ in range(steps):
         g.replay()
     e1.record()
     e1.synchronize()
     replicas.barrier()
-    ms, = replicas.max_over_ranks([e0.elapsed_time(e1) / args.steps], dev)
+    ms, = replicas.max_over_ranks([e0.elapsed_time(e1) / steps], dev)
     # parity and CPU baseline on the same blocks
     A_h = A0.cpu().numpy()
     rhs_h = rhs.cpu().numpy()
@@ -733,20 +880,74 @@ def block_pc_arm(args, rank, world, local):
             if nb_cpu == 0:
                 err = max(err, float(np.max(np.abs(xr - xg[o:o + n])) / np.max(np.abs(xr))))
         nb_cpu += 1
-        if time.perf_counter() - t0 > min(10.0, args.cpu_seconds):
+        if time.perf_counter() - t0 > min(10.0, cpu_seconds):
             break
     cpu_ms = (time.perf_counter() - t0) / nb_cpu * 1e3
-    line = {"metric": "block-diagonal preconditioner factor+solve time (ms)", "value": ms, "unit": "ms",
+    del g
+    return {"ms": ms, "gflops": flop / (ms * 1e-3) / 1e9, "factor_gflop": flop_factor / 1e9,
+            "block_bytes_gb": bytes_blocks / 1e9, "max_rel_err_vs_scipy": err, "panel": panel,
+            "cpu_ms": cpu_ms, "cpu_cores": os.cpu_count(),
+            "cpu_sample": f"scipy.linalg.lu_factor + lu_solve over all {args.nblocks} blocks, {nb_cpu} pass(es)"}
+
+
+def block_pc_arm(args, rank, world, local):
+    import torch
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    r = block_pc_measure(args, dev, args.steps, args.warmup, args.cpu_seconds)
+    line = {"metric": "block-diagonal preconditioner factor+solve time (ms)", "value": r["ms"], "unit": "ms",
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "higher_is_better": False,
             "dtype": "f64", "data": "synthetic (seeded)",
             "config": {"workload": "block_pc", "blocks": args.nblocks, "block_sizes": "4N, N in {16,24,32,48,64}",
-                       "panel": panel, "graph": "copy + factor + copy + solve, one CUDA graph"},
-            "gflops": flop / (ms * 1e-3) / 1e9, "max_rel_err_vs_scipy": err,
-            "cpu_baseline": {"value": cpu_ms, "unit": "ms", "cores": os.cpu_count(), "kind": "reference",
-                             "sample": f"scipy.linalg.lu_factor + lu_solve over all {args.nblocks} blocks, "
-                                       f"{nb_cpu} pass(es)"}}
+                       "panel": r["panel"], "graph": "copy + factor + copy + solve, one CUDA graph"},
+            "gflops": r["gflops"], "max_rel_err_vs_scipy": r["max_rel_err_vs_scipy"],
+            "cpu_baseline": {"value": r["cpu_ms"], "unit": "ms", "cores": r["cpu_cores"], "kind": "reference",
+                             "sample": r["cpu_sample"]}}
     if rank == 0:
         print(json.dumps(line), flush=True)
+
+
+def oseen_fibers_measure(args, dev, steps, warmup, cpu_seconds):
+    """Config 1: the Oseen sum of 32 fibers x 32 Chebyshev-Lobatto nodes
+    (1024 points, j == i skipped; kernels.py:214-287), FP64.  Latency bound:
+    device time per call, the HBM rate of its 73.7 KB of algorithmic I/O,
+    the drop-in call from pinned host buffers, and the C/OpenMP port."""
+    import torch
+    from fiber3d_b200 import autotune, kernels as K
+    wl = make_workload("oseen_fibers")
+    x = torch.as_tensor(wl["src"], device=dev)
+    f = torch.as_tensor(wl["dens"], device=dev)
+    shape = autotune.tune("oseen", x, x, f, self_mode="skip_index")
+    out = torch.empty(x.numel(), dtype=torch.float64, device=dev)
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=dev)
+    for _ in range(warmup):
+        K.pair_sum("oseen", x, x, f, self_mode="skip_index", shape=shape, out=out)
+    torch.cuda.synchronize()
+    evs = []
+    for _ in range(steps):
+        flush.fill_(1)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        K.pair_sum("oseen", x, x, f, self_mode="skip_index", shape=shape, out=out)
+        e1.record()
+        evs.append((e0, e1))
+    torch.cuda.synchronize()
+    us = statistics.median(a.elapsed_time(b) for a, b in evs) * 1e3
+    io_bytes = 3 * x.numel() * 8  # x, f in; u out
+    xh, fh = torch.as_tensor(wl["src"]).pin_memory(), torch.as_tensor(wl["dens"]).pin_memory()
+    for _ in range(warmup):
+        K.oseen_kernel_times_density_numba(xh, fh)
+    ts = []
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        K.oseen_kernel_times_density_numba(xh, fh)
+        ts.append(time.perf_counter() - t0)
+    e2e_us = statistics.median(ts) * 1e6
+    cpu_rate, _, _ = cpu_sample_rate(wl, host_cores()["threads"], min(2.0, cpu_seconds))
+    return {"us_per_call": us, "pairs_per_s": wl["pairs"] / (us * 1e-6), "io_bytes": io_bytes,
+            "hbm_gbs": io_bytes / (us * 1e-6) / 1e9, "e2e_us_per_call": e2e_us,
+            "e2e_pairs_per_s": wl["pairs"] / (e2e_us * 1e-6), "cpu_pairs_per_s": cpu_rate,
+            "launch_shape": [shape.tpt, shape.sl, shape.nsplit, shape.use_tma]}
 
 
 def main():
@@ -772,6 +973,8 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-step", action="store_true",
                     help="pair throughput only (skip the embedded time-step comparison)")
+    ap.add_argument("--no-oracle", action="store_true",
+                    help="skip the CPU-oracle check (and CPU time) of the step's solutions")
     ap.add_argument("--step-warmup", type=int, default=8)
     ap.add_argument("--step-steps", type=int, default=40)
     args = ap.parse_args()

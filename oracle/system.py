@@ -95,6 +95,10 @@ class HydroSystem:
     force_fibers: np.ndarray | None = None   # (sum N, 3) external force per point
     epsilon: float = 1e-3
     penalty: float = 500.0
+    # False: no dense shell matrix and no LU of it (36000^2 at 12000 nodes);
+    # the shell block of pc() is then unavailable and shell_pc_residual()
+    # checks a preconditioned vector against the matrix-free operator
+    dense_shell: bool = True
 
     def __post_init__(self):
         self.c0, self.c1 = F.mobility_constants(self.epsilon, self.eta)
@@ -202,7 +206,7 @@ class HydroSystem:
             A[3 * nb:, :3 * nb] = -self.K_bdy[k].T
             A[3 * nb:, 3 * nb:] = np.eye(6)
             self.lu_bdy.append(sla.lu_factor(A))
-        if self.shell is not None:
+        if self.shell is not None and self.dense_shell:
             self.M_shell = self.shell_dense()
             self.lu_shell = sla.lu_factor(self.M_shell)
 
@@ -354,11 +358,21 @@ class HydroSystem:
         return vgrid
 
     # ------------------------------------------------------ preconditioner --
+    def shell_pc_residual(self, y_shell, x_shell):
+        """||M_shell y - x|| / ||x||: how well y solves the shell block of the
+        preconditioner (tstep.py:327-351, the LU of M_shell applied to x),
+        measured with the matrix-free operator, so no dense matrix is needed."""
+        r = self.shell_apply(np.asarray(y_shell)) - np.asarray(x_shell)
+        return float(np.linalg.norm(r) / np.linalg.norm(x_shell))
+
     def pc(self, x):
-        """P_inv (tstep.py:950-994)."""
+        """P_inv (tstep.py:950-994).  Without the dense shell the shell block
+        of the result is NaN (use shell_pc_residual for it)."""
         y = np.empty_like(x)
-        if self.shell is not None:
+        if self.shell is not None and self.dense_shell:
             y[:3 * self.nshell] = sla.lu_solve(self.lu_shell, x[:3 * self.nshell])
+        elif self.shell is not None:
+            y[:3 * self.nshell] = np.nan
         for k in range(len(self.bodies)):
             i0 = self.o_body_k(k)
             i1 = i0 + 3 * self.nb[k] + 6
@@ -370,6 +384,10 @@ class HydroSystem:
         return y
 
     # --------------------------------------------------------------- solve --
+    def true_residual(self, x):
+        """||b - A x|| / ||b|| with this oracle's matvec and right-hand side."""
+        return float(np.linalg.norm(self.rhs - self.matvec(np.asarray(x))) / np.linalg.norm(self.rhs))
+
     def solve(self, tol=1e-8, restart=150, maxiter=200):
         """Right-preconditioned GMRES (bpm_utilities/gmres.py:94-111)."""
         n = self.size
@@ -382,3 +400,30 @@ class HydroSystem:
         y, info = spla.gmres(APinv, self.rhs, rtol=tol, atol=0.0, restart=restart, maxiter=maxiter,
                              callback=cb, callback_type="pr_norm")
         return self.pc(y), info, its[0]
+
+
+def system_at(problem, fibers, body_locations=None, body_rotations=None, dense_shell=False) -> HydroSystem:
+    """The oracle's system for `problem` (any object with the fields of a step
+    problem: lengths, E, dt, eta, bodies with ref_nodes / ref_normals /
+    weights, shell with nodes / normals / weights, force_fibers, epsilon,
+    penalty) at the given fiber positions and body poses (defaults: the
+    problem's own).  Without the dense shell (the default) it stays
+    matrix-free at any periphery size."""
+    bodies = []
+    for k, b in enumerate(problem.bodies or []):
+        loc = b.location if body_locations is None else body_locations[k]
+        rot = b.rotation if body_rotations is None else body_rotations[k]
+        bodies.append(Body(np.asarray(loc, dtype=np.float64), np.asarray(rot, dtype=np.float64),
+                           np.asarray(b.ref_nodes).reshape(-1, 3), np.asarray(b.ref_normals).reshape(-1, 3),
+                           np.asarray(b.weights).reshape(-1)))
+    shell = None
+    if problem.shell is not None:
+        sh = problem.shell
+        shell = Shell(np.asarray(sh.nodes).reshape(-1, 3), np.asarray(sh.normals).reshape(-1, 3),
+                      np.asarray(sh.weights).reshape(-1))
+    ff = problem.force_fibers
+    return HydroSystem([np.asarray(f, dtype=np.float64).reshape(-1, 3) for f in fibers], list(problem.lengths),
+                       problem.E, problem.dt, problem.eta, bodies, shell,
+                       None if ff is None else np.asarray(ff, dtype=np.float64).reshape(-1, 3),
+                       getattr(problem, "epsilon", 1e-3), getattr(problem, "penalty", 500.0),
+                       dense_shell=dense_shell)

@@ -37,6 +37,10 @@ def test_default_reference_arm_prints_one_line():
     assert d["impl"] == "reference" and d["metric"] == "Stokes pair interactions per second (FP64)"
     assert d["unit"] == "pairs/s" and d["value"] > 0 and d["higher_is_better"] is True
     assert d["config"]["workload"] == "stresslet_sphere"
+    # the same config dict as the GPU arm's (bench.workload_config)
+    assert set(d["config"]) == {"workload", "description", "pairs_per_step", "l2"}
+    cb = d["cpu_baseline"]
+    assert cb["cores"] == cb["threads"] and "physical_cores" in cb
     assert d["e2e"] == {"value": d["value"], "unit": "pairs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
 
 

@@ -1,0 +1,70 @@
+"""The full time-step configuration (512 fibers x 32 points of length 2,
+4 rigid spheres x 400 nodes, the 12000-node periphery of radius 10) against
+the CPU oracle's matrix-free restatement of fiber3d's step (oracle/system.py:
+tstep.py:1003-1178 matvec, :950-994 preconditioner, :745-846 right-hand
+side), at full size:
+
+* right-hand side and A x on seeded probes: 1e-12 norm-wise relative;
+* the fiber and body blocks of P^-1 x: 1e-9 (LU pivots as LAPACK's, rounding
+  differs); the periphery block through its defining equation,
+  ||M_shell y - x|| / ||x|| with the oracle's matrix-free shell operator;
+* the mixed-precision solve to 1e-9 meets that residual against the
+  oracle's operator, and the FP64 solve to 1e-8 its own.
+"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+import torch
+
+from conftest import rel_err
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def systems():
+    from fiber3d_b200 import geometry, hydro as H
+    from oracle import system as S
+    torch.cuda.set_device(0)
+    P = geometry.hydro_step_problem(seed=3)
+    dev = H.HydroSystem(P)
+    op = S.system_at(P, P.fibers)
+    return dev, op
+
+
+def test_sizes_and_rhs(systems):
+    dev, op = systems
+    assert dev.size == op.size == 106360
+    assert rel_err(dev.rhs.cpu().numpy(), op.rhs) < 1e-12
+
+
+@pytest.mark.parametrize("seed", [1, 2])
+def test_matvec(systems, seed):
+    dev, op = systems
+    x = np.random.default_rng(seed).normal(size=op.size)
+    y = torch.empty(op.size, dtype=torch.float64, device="cuda")
+    dev.matvec(torch.tensor(x, device="cuda"), y)
+    assert rel_err(y.cpu().numpy(), op.matvec(x)) < 1e-12
+
+
+@pytest.mark.parametrize("seed", [3, 4])
+def test_preconditioner(systems, seed):
+    dev, op = systems
+    x = np.random.default_rng(seed).normal(size=op.size)
+    y = torch.empty(op.size, dtype=torch.float64, device="cuda")
+    dev.pc(torch.tensor(x, device="cuda"), y)
+    y = y.cpu().numpy()
+    ns = 3 * op.nshell
+    ref = op.pc(x)
+    assert rel_err(y[ns:], ref[ns:]) < 1e-9
+    assert op.shell_pc_residual(y[:ns], x[:ns]) < 1e-11
+
+
+def test_solutions_against_oracle_operator(systems):
+    dev, op = systems
+    x64 = dev.solve(tol=1e-8, restart=100)["x"].cpu().numpy()
+    assert op.true_residual(x64) < 1e-8
+    xm = dev.solve(tol=1e-9, restart=100, mixed=True)["x"].cpu().numpy()
+    assert op.true_residual(xm) < 1e-9
+    assert np.linalg.norm(xm - x64) / np.linalg.norm(x64) < 1e-6
