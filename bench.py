@@ -356,8 +356,11 @@ def gpu_arm(args, rank, world, local):
             "grid_velocity": st.get("grid_velocity"),
         }
         s3 = {"fp64_ms": st["fp64"]["ms_per_step"]}
-        for m in ("learned_mixed", "learned_mixed_tol1e-9", "extrapolate_mixed"):
+        for m in ("learned_mixed", "learned_mixed_tol1e-9", "extrapolate_mixed", "flownet_mixed"):
+            if m not in st:
+                continue
             s3[f"{m}_ms"] = st[m]["ms_per_step"]
+            s3[f"{m}_iterations_total"] = int(sum(st[m]["iterations"]))
             s3[f"{m}_speedup"] = st[m]["speedup_vs_fp64"]
             s3[f"{m}_err_vs_fp64_solve"] = st[m]["rel_err_vs_fp64_1e-12_solve"]
         for m in ORACLE_MODES:
@@ -369,6 +372,10 @@ def gpu_arm(args, rank, world, local):
             s3["cpu_step_s"] = cpu["value_s"]
             s3["cpu_threads"] = cpu["threads"]
         s3["learned_correction_scale"] = st["training"]["scale"]
+        fn = st["training"].get("flownet")
+        if fn:
+            s3["flownet_heldout_rel_err"] = fn["heldout_rel_err"]
+            s3["flownet_true_map_residual_median"] = float(np.median(fn["true_map_initial_rel_residual"]))
         summary["cfg3_step"] = s3
         # config 4: the batched block-diagonal preconditioner
         bp = block_pc_measure(args, dev, 10, 3, args.cpu_seconds)
@@ -575,6 +582,41 @@ def hydro_arm(args, rank, world, local, warmup=None, steps=None, emit=True):
              "learned_mixed": ("learned", True, "auto", 1e-8),
              "learned_mixed_tol1e-9": ("learned", True, "auto", 1e-9),
              "learned_mixed_tol1e-10": ("learned", True, "auto", 1e-10)}
+    flow = None
+    if not args.no_flownet:
+        # the network of the specification's form: (positions, background
+        # velocity) -> (tensions, force densities) per fiber, mapped to
+        # X^{n+1} through the slender-body mobility; trained on the plain
+        # solver's steps of disjoint seeds
+        from fiber3d_b200 import flowstart as FS
+        t0 = time.perf_counter()
+        fx, fy = [], []
+        for seed in args.train_seeds[:args.flow_seeds]:
+            Pt = geometry.hydro_step_problem(seed=seed, nshell=args.nshell, nfib=args.nfib,
+                                             shell_radius=args.shell_radius, fiber_ball=args.fiber_ball,
+                                             body_shell=args.body_shell)
+            st_ = H.HydroSystem(Pt, shell_op=shell, device=dev)
+            _, a, b = FS.march(st_, args.train_steps, guess="extrapolate", record=True, tol=1e-10)
+            fx.append(a)
+            fy.append(b)
+            del st_
+        flow = FS.FlowWarmStart(seed=0, device=dev)
+        fhist, fval = flow.fit(torch.cat(fx), torch.cat(fy), epochs=args.train_epochs, batch=1024, lr=1e-3)
+        # the map itself, with the step's true tensions and forces, on the
+        # first steps of a validation trajectory (bounds any network of this form)
+        Pv = geometry.hydro_step_problem(seed=max(args.train_seeds) + 1, nshell=args.nshell, nfib=args.nfib,
+                                         shell_radius=args.shell_radius, fiber_ball=args.fiber_ball,
+                                         body_shell=args.body_shell)
+        ov = FS.march(H.HydroSystem(Pv, shell_op=shell, device=dev), 12, guess="extrapolate",
+                      oracle_steps=8, record_from=2)
+        torch.cuda.synchronize()
+        train["flownet"] = {"samples": int(sum(a.shape[0] for a in fx)), "seconds": time.perf_counter() - t0,
+                            "seeds": list(args.train_seeds[:args.flow_seeds]),
+                            "loss_first_last": [fhist[0], fhist[-1]], "heldout_rel_err": fval,
+                            "true_map_initial_rel_residual": [x.get("oracle_map_rel_residual") for x in ov
+                                                              if "oracle_map_rel_residual" in x],
+                            "extrapolation_initial_rel_residual": [x["initial_rel_residual"] for x in ov[2:10]]}
+        modes["flownet_mixed"] = ("flow", True, "auto", 1e-8)
     snap = {}
     for mode, (guess, mixed, pc_refresh, tol) in modes.items():
         sysd = H.HydroSystem(P, shell_op=shell, device=dev, tune=True, pc_refresh=pc_refresh)
@@ -599,6 +641,8 @@ def hydro_arm(args, rank, world, local, warmup=None, steps=None, emit=True):
                 x0 = W.extrapolate(history)
             elif guess == "learned":
                 x0 = W.learned_guess(sysd, history, net)
+            elif guess == "flow":
+                x0 = flow.guess(sysd, history, u_bg if history else None)
             sysd.timers.stop("warm_start")
             if history:
                 sysd.advance(history[-1], x0=x0)
@@ -606,6 +650,11 @@ def hydro_arm(args, rank, world, local, warmup=None, steps=None, emit=True):
             refreshed = sysd._pc_age == 0
             res = sysd.solve(tol=tol, restart=100, mixed=mixed, x0=x0)
             sysd.timers.stop("GMRES")
+            if guess == "flow":
+                # the network's next input: this solution's background velocity
+                sysd.timers.start("background_flow")
+                u_bg = FS.background_velocity(sysd, res["x"])
+                sysd.timers.stop("background_flow")
             e1.record()
             e1.synchronize()
             if timed_step:
@@ -973,6 +1022,9 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-step", action="store_true",
                     help="pair throughput only (skip the embedded time-step comparison)")
+    ap.add_argument("--no-flownet", action="store_true",
+                    help="skip the (positions, background velocity) network and its mode")
+    ap.add_argument("--flow-seeds", type=int, default=4, help="training trajectories of that network")
     ap.add_argument("--no-oracle", action="store_true",
                     help="skip the CPU-oracle check (and CPU time) of the step's solutions")
     ap.add_argument("--step-warmup", type=int, default=8)

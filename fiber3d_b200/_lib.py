@@ -61,6 +61,7 @@ SIGNATURES: dict[str, list] = {
     "f3d_version": [],
     "f3d_status_string": [_I],
     "f3d_get_device_error": [_P],
+    "f3d_peek_device_error_async": [_P, _P],
     "f3d_set_wait_limit_ns": [ctypes.c_uint64],
     "f3d_wait_limit_ns": [],
     "f3d_selftest_bounded_wait": [ctypes.c_uint64, _P],
@@ -71,6 +72,7 @@ SIGNATURES: dict[str, list] = {
     "f3d_oseen_dual_workspace_bytes": [_I64, _I64, ctypes.POINTER(PairShape), ctypes.POINTER(_SZ)],
     "f3d_oseen_dual": [_I, _P, _P, _P, _P, _P, _P, _P, _P, _I64, _I64, _D, _D, _D, _I, ctypes.POINTER(PairShape), _P,
                        _SZ, _P],
+    "f3d_pair_occupancy": [_I, _I, _I, _I, ctypes.POINTER(PairShape), ctypes.POINTER(_I)],
     "f3d_pair_sum_noalloc": [_I, _I, _I, _P, _P, _P, _P, _P, _P, _P, _I64, _I64, _D, _D, _D, _I, _P],
     "f3d_oseen_source_target": [_P, _P, _P, _P, _I64, _I64, _D, _D, _D, _I, _P, _SZ, _P],
     "f3d_oseen_times_density": [_P, _P, _P, _I64, _D, _D, _D, _I, _P, _SZ, _P],
@@ -243,6 +245,23 @@ def check_device_error(what: str, device: torch.device | None = None, on_error=N
         if on_error is not None:
             on_error()
         raise F3DError(what, status, lib().f3d_status_string(status).decode())
+
+
+class ErrorPeek:
+    """A page-locked word per device into which the device error word is
+    copied on the stream (f3d_peek_device_error_async), so that a caller that
+    waits for its results anyway learns of a failed kernel in the same wait."""
+
+    _per_device: dict[int, torch.Tensor] = {}
+
+    @classmethod
+    def queue(cls, device: torch.device) -> torch.Tensor:
+        idx = device.index if device.index is not None else torch.cuda.current_device()
+        word = cls._per_device.get(idx)
+        if word is None:
+            word = cls._per_device[idx] = torch.zeros(1, dtype=torch.int32, pin_memory=True)
+        call("f3d_peek_device_error_async", word.data_ptr(), stream_handle(device))
+        return word
 
 
 def set_wait_limit_ns(limit_ns: int) -> None:

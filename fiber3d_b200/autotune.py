@@ -38,8 +38,14 @@ def _bucket(n: int) -> int:
     return 0 if n <= 0 else 1 << int(math.ceil(math.log2(n)))
 
 
+_names: dict[int, str] = {}
+
+
 def _key(kernel, precision, self_mode, ns, nt) -> str:
-    name = torch.cuda.get_device_name().replace(" ", "_")
+    dev = torch.cuda.current_device()
+    name = _names.get(dev)
+    if name is None:
+        name = _names[dev] = torch.cuda.get_device_name(dev).replace(" ", "_")
     return f"{name}|{kernel}|{precision}|{self_mode}|{_bucket(ns)}|{_bucket(nt)}"
 
 
@@ -65,14 +71,31 @@ def _save():
         pass
 
 
-def candidates(nt: int, sms: int):
-    """Candidate (tpt, sl, nsplit, use_tma) shapes for nt targets."""
+def occupancy(kernel: str, precision: str, self_mode: str, tpt: int, sl: int) -> int:
+    """Resident CTAs per SM of the pair kernel of this shape (0 if unknown)."""
+    import ctypes
+    n = ctypes.c_int(0)
+    shp = _lib.PairShape(tpt, sl, 0, 0)
+    rc = _lib.lib().f3d_pair_occupancy(_lib.KERNEL[kernel], _lib.PRECISION[precision], _lib.SELF_MODE[self_mode],
+                                       0, ctypes.byref(shp), ctypes.byref(n))
+    return n.value if rc == 0 else 0
+
+
+def candidates(nt: int, sms: int, occ=None):
+    """Candidate (tpt, sl, nsplit, use_tma) shapes for nt targets: source
+    splits giving about 4, 8 or 16 CTAs per SM and, where the occupancy
+    `occ(tpt, sl)` is known, splits that fill 1-4 whole waves of resident
+    CTAs (no partly-filled last wave)."""
     out = []
     for tpt, sl in ((1, 1), (2, 1), (1, 8), (1, 32)):
         tpb = (128 // sl) * tpt
         ntb = max(1, -(-nt // tpb))
-        for per_sm in (4, 8, 16):
-            nsplit = max(1, -(-per_sm * sms // ntb))
+        splits = {max(1, -(-per_sm * sms // ntb)) for per_sm in (4, 8, 16)}
+        slots = occ(tpt, sl) * sms if occ is not None else 0
+        for waves in (1, 2, 3, 4):
+            if slots:
+                splits.add(max(1, (waves * slots) // ntb))
+        for nsplit in splits:
             for tma in (0, -1):
                 out.append((tpt, sl, nsplit, tma))
     return sorted(set(out))
@@ -95,7 +118,8 @@ def tune(kernel: str, r_source, r_target, density, normal=None, *, self_mode="re
               eta=eta, reg=reg, epsilon_distance=epsilon_distance)
     out = K.pair_sum(kernel, r_source, r_target, density, normal, **kw)
     best, best_t = None, float("inf")
-    for cand in candidates(nt, sms):
+    occ = lambda tpt, sl: occupancy(kernel, precision, self_mode, tpt, sl)
+    for cand in candidates(nt, sms, occ):
         shp = _lib.PairShape(*cand)
         K.pair_sum(kernel, r_source, r_target, density, normal, shape=shp, out=out, **kw)
         torch.cuda.synchronize()

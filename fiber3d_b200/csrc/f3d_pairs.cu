@@ -50,6 +50,7 @@ struct PairArgs {
   int accumulate;
   double eps2, reg2, scale;
   uint64_t wait_ns;  // limit of each bounded mbarrier wait
+  int *occupancy;    // host: when set, report CTAs per SM of the chosen kernel instead of launching
 };
 
 // Shared-memory layout of one stage.
@@ -676,6 +677,11 @@ static int launch_one(const PairArgs &a, int64_t ntb, int nsplit, cudaStream_t s
       return F3D_ERR_CUDA;
     attr_set[dev] = true;
   }
+  if (a.occupancy) {
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(a.occupancy, kfn, kBlock, smem) == cudaSuccess
+               ? F3D_OK
+               : F3D_ERR_CUDA;
+  }
   dim3 grid(static_cast<unsigned>(ntb), static_cast<unsigned>(nsplit));
   kfn<<<grid, kBlock, smem, st>>>(a);
   return launch_status();
@@ -745,7 +751,7 @@ static int pair_sum_core(int kernel, int precision, int self_mode, const double 
   if (ws && !aligned(ws, 256)) return F3D_ERR_ALIGN;
   unsigned char *w = static_cast<unsigned char *>(ws);
 
-  PairArgs a;
+  PairArgs a{};
   a.rs = rs; a.rt = rt; a.dens = dens; a.nrm = nrm;
   a.gs = gs; a.gt = gt;
   a.out = out;
@@ -881,6 +887,38 @@ int f3d_stresslet_times_normal_times_density(const double *r_vectors, const doub
                             r_vectors, density, normal, nullptr, nullptr, v, n, n, eta, reg,
                             epsilon_distance, 0, nullptr, workspace, workspace_bytes,
                             static_cast<cudaStream_t>(stream));
+}
+
+int f3d_pair_occupancy(int kernel, int precision, int self_mode, int dual, const f3d_pair_shape *shape,
+                       int *ctas_per_sm) {
+  if (!ctas_per_sm) return F3D_ERR_NULL;
+  f3d::Plan p;
+  int rc = f3d::make_plan(kernel, precision, 1, 1, shape, &p, dual != 0);
+  if (rc) return rc;
+  if (self_mode < 0 || self_mode > 3) return F3D_ERR_ARG;
+  if (dual && (kernel != F3D_KERNEL_OSEEN || precision != F3D_FP64 || self_mode == F3D_SELF_SKIP_CLOSE))
+    return F3D_ERR_ARG;
+  // the shape's own tpt/sl (make_plan picks defaults for a 1-target sum)
+  if (shape && shape->tpt) p.tpt = shape->tpt;
+  if (shape && shape->sl) p.sl = shape->sl;
+  f3d::PairArgs a{};
+  a.occupancy = ctas_per_sm;
+  if (dual) {
+    switch (self_mode) {
+      case F3D_SELF_REGULARISE:
+        return f3d::dispatch_shape<F3D_KERNEL_OSEEN, F3D_SELF_REGULARISE, F3D_FP64, true>(a, p, nullptr);
+      case F3D_SELF_SKIP_INDEX:
+        return f3d::dispatch_shape<F3D_KERNEL_OSEEN, F3D_SELF_SKIP_INDEX, F3D_FP64, true>(a, p, nullptr);
+      default:
+        return f3d::dispatch_shape<F3D_KERNEL_OSEEN, F3D_SELF_SKIP_GROUP, F3D_FP64, true>(a, p, nullptr);
+    }
+  }
+  switch (kernel) {
+    case F3D_KERNEL_OSEEN: return f3d::dispatch_prec<F3D_KERNEL_OSEEN>(precision, self_mode, a, p, nullptr);
+    case F3D_KERNEL_STRESSLET: return f3d::dispatch_prec<F3D_KERNEL_STRESSLET>(precision, self_mode, a, p, nullptr);
+    case F3D_KERNEL_TRACTION: return f3d::dispatch_prec<F3D_KERNEL_TRACTION>(precision, self_mode, a, p, nullptr);
+    default: return f3d::dispatch_prec<F3D_KERNEL_ROTLET>(precision, self_mode, a, p, nullptr);
+  }
 }
 
 int f3d_oseen_dual_workspace_bytes(int64_t ns, int64_t nt, const f3d_pair_shape *shape,

@@ -80,6 +80,16 @@ const char *f3d_status_string(int status) {
   }
 }
 
+int f3d_peek_device_error_async(int *host_dst, void *stream) {
+  if (!host_dst) return F3D_ERR_NULL;
+  int *w = f3d::device_error_word();
+  if (!w) return F3D_ERR_CUDA;
+  if (cudaMemcpyAsync(host_dst, w, sizeof(int), cudaMemcpyDeviceToHost, static_cast<cudaStream_t>(stream)) !=
+      cudaSuccess)
+    return F3D_ERR_CUDA;
+  return F3D_OK;
+}
+
 int f3d_get_device_error(void *stream) {
   int *w = f3d::device_error_word();
   if (!w) return F3D_ERR_CUDA;

@@ -78,11 +78,21 @@ def _any_host(*xs) -> bool:
     return any(not (isinstance(x, torch.Tensor) and x.is_cuda) for x in xs if x is not None)
 
 
-def _out(u: torch.Tensor, host: bool):
+def _out(u: torch.Tensor, host: bool, what: str = "kernels"):
+    """The result as the caller wants it.  For host callers it is copied into
+    a new page-locked array on the stream together with the device error
+    word, and one wait covers both: a bounded wait that ran out in this call's
+    kernels raises here instead of returning numbers."""
     u = u.reshape(-1)
-    if host:
-        return u.cpu().numpy()
-    return u
+    if not host:
+        return u
+    h = torch.empty(u.shape, dtype=u.dtype, pin_memory=True)
+    h.copy_(u, non_blocking=True)
+    word = _lib.ErrorPeek.queue(u.device)
+    torch.cuda.current_stream(u.device).synchronize()
+    if int(word[0]) != 0:
+        _lib.check_device_error(what, u.device)
+    return h.numpy()
 
 
 def _resolve_precision(precision) -> int:
@@ -158,12 +168,7 @@ def _drop_in(kernel, r_source, r_target, density, normal, self_mode, eta, reg, e
                               reg=reg, epsilon_distance=epsilon_distance)
     u = pair_sum(kernel, rs, rt, d, n, eta=eta, reg=reg, epsilon_distance=epsilon_distance,
                  self_mode=self_mode, precision=precision, shape=shape)
-    res = _out(u, host)
-    if host:
-        # the copy back has synchronised the stream: a bounded wait that ran
-        # out in this sum is reported here rather than returned as numbers
-        _lib.check_device_error(kernel)
-    return res
+    return _out(u, host, kernel)
 
 
 # ------------------------------------------------------------ pair sums ----
@@ -272,10 +277,7 @@ def single_double_layer_kernel_source_target_stkfmm(r_source_SL, r_source_DL, r_
         pair_sum("stresslet", rdl, rt, _to_dev(density_DL, dev, "density_DL"), _to_dev(normal, dev, "normal"),
                  eta=eta, reg=0.0, epsilon_distance=COINCIDENT, self_mode="skip_close", out=u,
                  accumulate=True)
-    res = _out(u, host)
-    if host:
-        _lib.check_device_error("single_double_layer")
-    return res
+    return _out(u, host, "single_double_layer")
 
 
 def complementary_kernel_times_density_numba(r_vectors, normal, density):

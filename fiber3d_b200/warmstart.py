@@ -89,17 +89,19 @@ def gemm(A: torch.Tensor, B: torch.Tensor, *, transpose_a=False, transpose_b=Tru
 
 
 class FiberMLP:
-    """The warm-start network with its own forward/backward/Adam kernels."""
+    """A per-fiber network (ReLU hidden layers) with its own forward,
+    backward and Adam kernels; `layers` gives the widths, input first."""
 
-    def __init__(self, seed: int = 0, device=None):
+    def __init__(self, seed: int = 0, device=None, layers=LAYERS):
         dev = device or torch.device("cuda", torch.cuda.current_device())
         self.device = dev
+        self.layers = tuple(layers)
         rng = np.random.default_rng(seed)
         self.W, self.b = [], []
-        for k in range(len(LAYERS) - 1):
-            fan_in, fan_out = LAYERS[k], LAYERS[k + 1]
+        for k in range(len(self.layers) - 1):
+            fan_in, fan_out = self.layers[k], self.layers[k + 1]
             w = rng.normal(scale=np.sqrt(2.0 / fan_in), size=(fan_out, fan_in)).astype(np.float32)
-            if k == len(LAYERS) - 2:
+            if k == len(self.layers) - 2:
                 w *= 0.1
             self.W.append(torch.as_tensor(w, device=dev))
             self.b.append(torch.zeros(fan_out, dtype=torch.float32, device=dev))
@@ -107,20 +109,20 @@ class FiberMLP:
         self.m = [torch.zeros_like(p) for p in self.params]
         self.v = [torch.zeros_like(p) for p in self.params]
         self.step = 0
-        self.in_mean = torch.zeros(LAYERS[0], device=dev)
-        self.in_std = torch.ones(LAYERS[0], device=dev)
-        self.out_mean = torch.zeros(LAYERS[-1], device=dev)
-        self.out_std = torch.ones(LAYERS[-1], device=dev)
+        self.in_mean = torch.zeros(self.layers[0], device=dev)
+        self.in_std = torch.ones(self.layers[0], device=dev)
+        self.out_mean = torch.zeros(self.layers[-1], device=dev)
+        self.out_std = torch.ones(self.layers[-1], device=dev)
 
     # ------------------------------------------------------------- passes --
     def forward(self, X: torch.Tensor, keep=False):
-        """X: (B, LAYERS[0]) normalised inputs -> (B, LAYERS[-1]) normalised outputs."""
+        """X: (B, layers[0]) normalised inputs -> (B, layers[-1]) normalised outputs."""
         acts, pres = [X.contiguous()], []
         h = acts[0]
         L = len(self.W)
         for k in range(L):
             last = k == L - 1
-            pre = torch.empty((h.shape[0], LAYERS[k + 1]), dtype=torch.float32, device=X.device) \
+            pre = torch.empty((h.shape[0], self.layers[k + 1]), dtype=torch.float32, device=X.device) \
                 if (keep and not last) else None
             h = gemm(h, self.W[k], bias=self.b[k], relu=not last, pre=pre)
             if keep:

@@ -91,6 +91,13 @@ const char *f3d_status_string(int status);
 /* Reads and clears the device error word of the current device (blocks on
    the given stream).  Returns F3D_OK or F3D_ERR_TIMEOUT. */
 int f3d_get_device_error(void *stream);
+/* Queues a copy of the device error word into *host_dst on `stream` without
+   waiting and without clearing it (host_dst page-locked for the copy to be
+   asynchronous).  After the stream has synchronised, a non-zero value means
+   a kernel failed; f3d_get_device_error then reads and clears it.  Lets a
+   caller that synchronises anyway (to read its results) check for failures
+   in the same wait. */
+int f3d_peek_device_error_async(int *host_dst, void *stream);
 
 /* Bounded waits.  Every kernel that waits on an mbarrier (a bulk copy or a
    tensor-core MMA landing) gives up after a limit, records F3D_ERR_TIMEOUT in
@@ -133,6 +140,14 @@ int f3d_pair_sum(int kernel, int precision, int self_mode,
                  double eta, double reg, double epsilon_distance,
                  int accumulate, const f3d_pair_shape *shape,
                  void *workspace, size_t workspace_bytes, void *stream);
+
+/* Resident CTAs per SM of the pair kernel that a sum of this kernel,
+   precision, self mode (dual: the two-density FP64 Oseen pass) and launch
+   shape would run (cudaOccupancyMaxActiveBlocksPerMultiprocessor), so that
+   a tuner can size the source split to whole waves.  Launches nothing.
+   No counterpart in fiber3d. */
+int f3d_pair_occupancy(int kernel, int precision, int self_mode, int dual,
+                       const f3d_pair_shape *shape, int *ctas_per_sm);
 
 /* The same sum for callers that cannot allocate device memory (no workspace
    argument).  No counterpart in fiber3d.  Its scratch is a 32 MiB device

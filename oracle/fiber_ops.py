@@ -261,3 +261,17 @@ def force_operator(fm, x, length, E):
         F[a * N:(a + 1) * N, a * N:(a + 1) * N] = -E * D4
         F[a * N:(a + 1) * N, 3 * N:] = np.diag(xss[:, a]) + xs[:, a][:, None] * D1
     return F
+
+
+def self_mobility(xs: np.ndarray, c0: float, c1: float) -> np.ndarray:
+    """fiber.self_mobility, fiber/fiber.py:964-993: the 3N x 3N local
+    slender-body mobility in fiber3d's (x_all, y_all, z_all) ordering,
+    M_ab = c0 (delta_ab I + diag(xs_a xs_b)) + c1 (delta_ab I - diag(xs_a xs_b))."""
+    n = xs.shape[0]
+    I = np.eye(n)
+    M = np.zeros((3 * n, 3 * n))
+    for a in range(3):
+        for b in range(3):
+            d = np.diag(xs[:, a] * xs[:, b])
+            M[a * n:(a + 1) * n, b * n:(b + 1) * n] = c0 * ((a == b) * I + d) + c1 * ((a == b) * I - d)
+    return M

@@ -138,3 +138,20 @@ def test_wait_limit_setting_and_selftest_checks(dll):
     assert dll.f3d_wait_limit_ns() == 2_000_000_000
     assert dll.f3d_selftest_bounded_wait(0, None) == 5
     assert dll.f3d_selftest_bounded_wait(3_000_000_000, None) == 5
+
+
+def test_pair_occupancy_argument_checks(dll):
+    n = ctypes.c_int(0)
+    assert dll.f3d_pair_occupancy(0, 0, 0, 0, None, None) == 1          # F3D_ERR_NULL
+    assert dll.f3d_pair_occupancy(7, 0, 0, 0, None, ctypes.byref(n)) == 5  # unknown kernel
+    assert dll.f3d_pair_occupancy(1, 0, 0, 1, None, ctypes.byref(n)) == 5  # dual is FP64 Oseen only
+
+
+def test_autotune_candidates_fill_whole_waves():
+    from fiber3d_b200 import autotune
+    cands = autotune.candidates(16096, 148, occ=lambda tpt, sl: 10 if tpt == 1 else 6)
+    # (tpt 2, sl 1): 256 targets per CTA, 63 target blocks, 6 x 148 = 888 slots
+    splits = {c[2] for c in cands if c[:2] == (2, 1)}
+    for waves in (1, 2, 3, 4):
+        assert (waves * 888) // 63 in splits
+    assert all(c[3] in (0, -1) for c in cands)

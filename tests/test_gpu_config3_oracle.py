@@ -4,12 +4,19 @@ the CPU oracle's matrix-free restatement of fiber3d's step (oracle/system.py:
 tstep.py:1003-1178 matvec, :950-994 preconditioner, :745-846 right-hand
 side), at full size:
 
-* right-hand side and A x on seeded probes: 1e-12 norm-wise relative;
+* right-hand side: 1e-12 norm-wise relative; A x: 1e-12 on the step's own
+  FP64 solution (a smooth vector) and 1e-10 on N(0, 1) probes, whose
+  point-to-point noise in the fiber positions is differentiated four times
+  by the bending operator (|D4| ~ 1e6 at 32 points of length 2), so any two
+  FP64 evaluation orders differ there by ~1e-11 (measured 1.2e-11);
 * the fiber and body blocks of P^-1 x: 1e-9 (LU pivots as LAPACK's, rounding
   differs); the periphery block through its defining equation,
   ||M_shell y - x|| / ||x|| with the oracle's matrix-free shell operator;
-* the mixed-precision solve to 1e-9 meets that residual against the
-  oracle's operator, and the FP64 solve to 1e-8 its own.
+* the FP64 solve to 1e-8 and the mixed-precision solve to 1e-9 meet their
+  tolerances as true residuals of the ORACLE's operator and right-hand
+  side, and the mixed solution is within 1e-6 of an FP64 solve to 1e-11
+  (the operator's conditioning turns a 1e-9 residual into an error of
+  ~1e-8 to 1e-7).
 """
 from __future__ import annotations
 
@@ -40,12 +47,20 @@ def test_sizes_and_rhs(systems):
 
 
 @pytest.mark.parametrize("seed", [1, 2])
-def test_matvec(systems, seed):
+def test_matvec_random_probes(systems, seed):
     dev, op = systems
     x = np.random.default_rng(seed).normal(size=op.size)
     y = torch.empty(op.size, dtype=torch.float64, device="cuda")
     dev.matvec(torch.tensor(x, device="cuda"), y)
-    assert rel_err(y.cpu().numpy(), op.matvec(x)) < 1e-12
+    assert rel_err(y.cpu().numpy(), op.matvec(x)) < 1e-10
+
+
+def test_matvec_of_the_solution(systems):
+    dev, op = systems
+    x = dev.solve(tol=1e-10, restart=100)["x"]
+    y = torch.empty_like(x)
+    dev.matvec(x, y)
+    assert rel_err(y.cpu().numpy(), op.matvec(x.cpu().numpy())) < 1e-12
 
 
 @pytest.mark.parametrize("seed", [3, 4])
@@ -67,4 +82,5 @@ def test_solutions_against_oracle_operator(systems):
     assert op.true_residual(x64) < 1e-8
     xm = dev.solve(tol=1e-9, restart=100, mixed=True)["x"].cpu().numpy()
     assert op.true_residual(xm) < 1e-9
-    assert np.linalg.norm(xm - x64) / np.linalg.norm(x64) < 1e-6
+    xr = dev.solve(tol=1e-11, restart=100)["x"].cpu().numpy()
+    assert np.linalg.norm(xm - xr) / np.linalg.norm(xr) < 1e-6

@@ -343,3 +343,11 @@ def test_skip_close_shapes(K, L, shape, kind):
         u = K.pair_sum("stresslet", xs, xt, d, nr, self_mode="skip_close", epsilon_distance=1e-5,
                        shape=L.PairShape(*shape))
     assert rel_err(u.cpu().numpy(), ref) < TOL64
+
+
+def test_occupancy_query(L):
+    from fiber3d_b200 import autotune
+    for kind in ("oseen", "stresslet", "traction"):
+        for tpt, sl in ((1, 1), (2, 1), (1, 8), (1, 32)):
+            n = autotune.occupancy(kind, "fp64", "skip_group", tpt, sl)
+            assert 1 <= n <= 16
