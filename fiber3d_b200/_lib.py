@@ -72,6 +72,9 @@ SIGNATURES: dict[str, list] = {
     "f3d_oseen_dual_workspace_bytes": [_I64, _I64, ctypes.POINTER(PairShape), ctypes.POINTER(_SZ)],
     "f3d_oseen_dual": [_I, _P, _P, _P, _P, _P, _P, _P, _P, _I64, _I64, _D, _D, _D, _I, ctypes.POINTER(PairShape), _P,
                        _SZ, _P],
+    "f3d_pair_host_bytes": [_I, _I64, _I64, _I, ctypes.POINTER(_SZ)],
+    "f3d_pair_sum_host": [_I, _I, _I, _P, _P, _P, _P, _P, _I64, _I64, _D, _D, _D, ctypes.POINTER(PairShape), _P,
+                          _SZ, _P, _SZ, _P],
     "f3d_pair_occupancy": [_I, _I, _I, _I, ctypes.POINTER(PairShape), ctypes.POINTER(_I)],
     "f3d_pair_sum_noalloc": [_I, _I, _I, _P, _P, _P, _P, _P, _P, _P, _I64, _I64, _D, _D, _D, _I, _P],
     "f3d_oseen_source_target": [_P, _P, _P, _P, _I64, _I64, _D, _D, _D, _I, _P, _SZ, _P],
@@ -245,6 +248,18 @@ def check_device_error(what: str, device: torch.device | None = None, on_error=N
         if on_error is not None:
             on_error()
         raise F3DError(what, status, lib().f3d_status_string(status).decode())
+
+
+class Staging(Workspace):
+    """Per-device buffer that host-side sums stage their inputs and result
+    in (f3d_pair_sum_host); grown on demand, never needs zeroing."""
+
+    _per_device: dict[int, "Staging"] = {}
+
+    def ensure(self, nbytes: int) -> tuple[int, int]:
+        if nbytes > self.buf.numel():
+            self.buf = torch.empty(max(nbytes, 2 * self.buf.numel()), dtype=torch.uint8, device=self.device)
+        return (self.buf.data_ptr(), self.buf.numel()) if self.buf.numel() else (0, 0)
 
 
 class ErrorPeek:

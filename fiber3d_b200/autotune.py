@@ -140,6 +140,14 @@ def tune(kernel: str, r_source, r_target, density, normal=None, *, self_mode="re
     return _lib.PairShape(*best)
 
 
+def cached(kernel: str, precision: str, self_mode: str, ns: int, nt: int) -> _lib.PairShape | None:
+    """The tuned shape of this sum's bucket if one is known (no tuning)."""
+    with _lock:
+        _load()
+        v = _cache.get(_key(kernel, precision, self_mode, ns, nt))
+    return _lib.PairShape(*v) if v is not None else None
+
+
 def table() -> dict:
     """The cached shapes (for reports)."""
     with _lock:

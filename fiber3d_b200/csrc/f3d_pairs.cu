@@ -25,6 +25,8 @@
 // and the last CTA of a target block (self-resetting counter) adds the
 // partials in split order, so results are deterministic run to run.
 #include <algorithm>
+#include <climits>
+#include <type_traits>
 
 #include "f3d_common.cuh"
 
@@ -70,9 +72,16 @@ struct Stage {
   static constexpr size_t bytes = ((data_bytes + (kGrp ? 4 * kTile : 0)) + 127) / 128 * 128;
 };
 
+// Bytes of the FP64 accumulator snapshot: [TPT][3] (DUAL: twice) doubles per
+// thread (sized for TPT <= 2).
+template <int PREC, bool DUAL>
+constexpr size_t snapshot_bytes() {
+  return PREC == F3D_FP64 ? static_cast<size_t>(2) * 3 * (DUAL ? 2 : 1) * 8 * kBlock : 0;
+}
+
 template <int KIND, int MODE, int PREC, bool DUAL = false>
 constexpr size_t pair_smem_bytes() {
-  return 128 + 2 * Stage<KIND, MODE, PREC, DUAL>::bytes;
+  return 128 + 2 * Stage<KIND, MODE, PREC, DUAL>::bytes + snapshot_bytes<PREC, DUAL>();
 }
 
 // Reciprocal square roots in FP64.  y0 = rsqrt.approx.ftz.f64(x) (PTX; about
@@ -165,7 +174,7 @@ __device__ __forceinline__ f32x2 fma2(f32x2 a, f32x2 b, f32x2 c) {
 // into out and dens2 into out2, each with exactly the arithmetic of a single
 // sum -- the geometry (r, 1/r, 1/r^3) is computed once for both.
 template <int KIND, int MODE, int PREC, int TPT, int SL, bool DUAL = false>
-__global__ void __launch_bounds__(kBlock) pair_kernel(const PairArgs a) {
+__global__ void __launch_bounds__(kBlock, (PREC == F3D_FP64 && !DUAL) ? ((TPT == 1) ? 7 : 5) : 1) pair_kernel(const PairArgs a) {
   static_assert(!DUAL || (PREC == F3D_FP64 && KIND == F3D_KERNEL_OSEEN), "dual sums: FP64 Oseen");
   using St = Stage<KIND, MODE, PREC, DUAL>;
   constexpr int TG = kBlock / SL;
@@ -242,24 +251,64 @@ __global__ void __launch_bounds__(kBlock) pair_kernel(const PairArgs a) {
   const long long eps2_bits = __double_as_longlong(a.eps2);
   const float eps2f = static_cast<float>(a.eps2), reg2f = static_cast<float>(a.reg2);
 
+  // ---- FP64: which tiles need the per-pair rules ----------------------------
+  // A tile runs the "careful" loop (skip rule, regularisation of close pairs,
+  // per pair) only where a skipped pair can occur: for SKIP_INDEX a tile whose
+  // source indices meet this warp's target indices, for SKIP_GROUP one whose
+  // group-id range meets this warp's, always for SKIP_CLOSE and for a tail
+  // tile.  Every other tile runs the plain arithmetic and tracks the smallest
+  // r^2 it met (its high word, on the integer pipe); if that could be below
+  // eps^2, the thread's accumulators are restored from a shared-memory
+  // snapshot and the tile is redone carefully.  The result is the careful
+  // loop's in every case.
+  const int lane = tid & 31;
+  const int eps2_hi = __double2hiint(a.eps2);
+  int64_t w_lo = INT64_MAX, w_hi = INT64_MIN;  // SKIP_INDEX: this warp's target index range
+  int w_glo = INT32_MAX, w_ghi = INT32_MIN;    // SKIP_GROUP: its target group-id range
+  if (PREC == F3D_FP64 && MODE == F3D_SELF_SKIP_INDEX) {
+#pragma unroll
+    for (int k = 0; k < TPT; ++k) {
+      w_lo = min(w_lo, tidx[k]);
+      w_hi = max(w_hi, tidx[k]);
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+      w_lo = min(w_lo, static_cast<int64_t>(__shfl_xor_sync(0xffffffffu, static_cast<long long>(w_lo), off)));
+      w_hi = max(w_hi, static_cast<int64_t>(__shfl_xor_sync(0xffffffffu, static_cast<long long>(w_hi), off)));
+    }
+  }
+  if (PREC == F3D_FP64 && MODE == F3D_SELF_SKIP_GROUP) {
+    int glo = INT32_MAX, ghi = INT32_MIN;
+#pragma unroll
+    for (int k = 0; k < TPT; ++k) {
+      glo = min(glo, tgrp[k]);
+      ghi = max(ghi, tgrp[k]);
+    }
+    w_glo = __reduce_min_sync(0xffffffffu, glo);
+    w_ghi = __reduce_max_sync(0xffffffffu, ghi);
+  }
+  double *snap = reinterpret_cast<double *>(stages + 2 * St::bytes) + tid;  // [TPT*3*(1+DUAL)][kBlock]
+
   // ---- one tile of `cnt` sources starting at global index `sbase` --------
   auto compute_tile = [&](const unsigned char *buf, int cnt, int64_t sbase) {
     if (PREC == F3D_FP64) {
-      for (int s = sl; s < cnt; s += SL) {
-        const double *pos = reinterpret_cast<const double *>(buf + St::off_pos);
-        const double *den = reinterpret_cast<const double *>(buf + St::off_dens);
-        const double *nrm = reinterpret_cast<const double *>(buf + St::off_nrm);
+      const double *pos = reinterpret_cast<const double *>(buf + St::off_pos);
+      const double *den = reinterpret_cast<const double *>(buf + St::off_dens);
+      const double *nrm = reinterpret_cast<const double *>(buf + St::off_nrm);
+      const double *den2 = reinterpret_cast<const double *>(buf + St::off_dens2);
+      const int32_t *grp = reinterpret_cast<const int32_t *>(buf + St::off_grp);
+      // source s against this thread's targets; CAREFUL applies the skip and
+      // close-pair rules, else the minimum high word of r^2 goes to hmin
+      auto one_source = [&](int s, auto careful_tag, int &hmin) {
+        constexpr bool CAREFUL = decltype(careful_tag)::value;
         const double sx = pos[3 * s], sy = pos[3 * s + 1], sz = pos[3 * s + 2];
         const double d0 = den[3 * s], d1 = den[3 * s + 1], d2 = den[3 * s + 2];
         double n0 = 0.0, n1 = 0.0, n2 = 0.0;
         if (KIND == F3D_KERNEL_STRESSLET) { n0 = nrm[3 * s]; n1 = nrm[3 * s + 1]; n2 = nrm[3 * s + 2]; }
         double e0 = 0.0, e1 = 0.0, e2 = 0.0;
-        if (DUAL) {
-          const double *den2 = reinterpret_cast<const double *>(buf + St::off_dens2);
-          e0 = den2[3 * s]; e1 = den2[3 * s + 1]; e2 = den2[3 * s + 2];
-        }
+        if (DUAL) { e0 = den2[3 * s]; e1 = den2[3 * s + 1]; e2 = den2[3 * s + 2]; }
         int32_t sg = 0;
-        if (MODE == F3D_SELF_SKIP_GROUP) sg = reinterpret_cast<const int32_t *>(buf + St::off_grp)[s];
+        if (CAREFUL && MODE == F3D_SELF_SKIP_GROUP) sg = grp[s];
 #pragma unroll
         for (int k = 0; k < TPT; ++k) {
           const double dx = txd[k] - sx, dy = tyd[k] - sy, dz = tzd[k] - sz;
@@ -267,14 +316,19 @@ __global__ void __launch_bounds__(kBlock) pair_kernel(const PairArgs a) {
           // skipped pairs (and, in SKIP_CLOSE, close ones) are dropped by a
           // select on the final factor, so their r2 may stay 0
           bool skip = false;
-          if (MODE == F3D_SELF_SKIP_INDEX) skip = (sbase + s == tidx[k]);
-          if (MODE == F3D_SELF_SKIP_GROUP) skip = (sg == tgrp[k]);
-          const bool close = !skip && (__double_as_longlong(r2) < eps2_bits);
-          if (MODE == F3D_SELF_SKIP_CLOSE) skip = close;
-          else r2 = regularise(r2, close, reg2);
+          if (CAREFUL) {
+            if (MODE == F3D_SELF_SKIP_INDEX) skip = (sbase + s == tidx[k]);
+            if (MODE == F3D_SELF_SKIP_GROUP) skip = (sg == tgrp[k]);
+            const bool close = !skip && (__double_as_longlong(r2) < eps2_bits);
+            if (MODE == F3D_SELF_SKIP_CLOSE) skip = close;
+            else r2 = regularise(r2, close, reg2);
+          } else {
+            hmin = min(hmin, __double2hiint(r2));
+          }
+          constexpr bool kSel = CAREFUL && (MODE != F3D_SELF_REGULARISE);
           if (KIND == F3D_KERNEL_OSEEN || KIND == F3D_KERNEL_ROTLET) {
             double ri = rsqrt_refined(r2);
-            if (MODE != F3D_SELF_REGULARISE) ri = skip ? 0.0 : ri;
+            if (kSel) ri = skip ? 0.0 : ri;
             const double ri3 = ri * ri * ri;
             if (KIND == F3D_KERNEL_OSEEN) {
               const double rf = fma(dx, d0, fma(dy, d1, dz * d2));
@@ -300,12 +354,50 @@ __global__ void __launch_bounds__(kBlock) pair_kernel(const PairArgs a) {
             const double rd = fma(dx, d0, fma(dy, d1, dz * d2));
             const double rn = fma(dx, m0, fma(dy, m1, dz * m2));
             double f0 = times_rsqrt5(rd * rn, r2);
-            if (MODE != F3D_SELF_REGULARISE) f0 = skip ? 0.0 : f0;
+            if (kSel) f0 = skip ? 0.0 : f0;
             acc[k][0] = fma(f0, dx, acc[k][0]);
             acc[k][1] = fma(f0, dy, acc[k][1]);
             acc[k][2] = fma(f0, dz, acc[k][2]);
           }
         }
+      };
+      bool careful = (MODE == F3D_SELF_SKIP_CLOSE) || (cnt < kTile);
+      if (MODE == F3D_SELF_SKIP_INDEX) careful = careful || (sbase <= w_hi && sbase + cnt > w_lo);
+      if (MODE == F3D_SELF_SKIP_GROUP && !careful) {
+        int glo = INT32_MAX, ghi = INT32_MIN;
+        for (int s = lane; s < cnt; s += 32) {
+          glo = min(glo, grp[s]);
+          ghi = max(ghi, grp[s]);
+        }
+        glo = __reduce_min_sync(0xffffffffu, glo);
+        ghi = __reduce_max_sync(0xffffffffu, ghi);
+        careful = (glo <= w_ghi && ghi >= w_glo);
+      }
+      int hmin = INT32_MAX;
+      if (!careful) {
+#pragma unroll
+        for (int k = 0; k < TPT; ++k)
+#pragma unroll
+          for (int c = 0; c < 3; ++c) {
+            snap[(k * 3 + c) * kBlock] = acc[k][c];
+            if (DUAL) snap[((TPT + k) * 3 + c) * kBlock] = acc2[k][c];
+          }
+#pragma unroll 1
+        for (int s = sl; s < kTile; s += SL) one_source(s, std::false_type{}, hmin);
+        if (hmin <= eps2_hi) {
+          // a pair within eps (or r^2 = 0) met without the rules: redo the tile
+#pragma unroll
+          for (int k = 0; k < TPT; ++k)
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+              acc[k][c] = snap[(k * 3 + c) * kBlock];
+              if (DUAL) acc2[k][c] = snap[((TPT + k) * 3 + c) * kBlock];
+            }
+          careful = true;
+        }
+      }
+      if (careful) {
+        for (int s = sl; s < cnt; s += SL) one_source(s, std::true_type{}, hmin);
       }
     } else {
       // sources in pairs (2q, 2q + 1); a record of 6 x 16 bytes holds

@@ -138,36 +138,128 @@ def pair_sum(kernel: str, r_source, r_target, density, normal=None, *, eta=1.0, 
         out = torch.empty(3 * nt, dtype=torch.float64, device=dev)
     elif out.numel() != 3 * nt or out.dtype != torch.float64 or not out.is_contiguous():
         raise ValueError("out must be a contiguous float64 tensor of length 3*Nt")
-    k = _lib.KERNEL[kernel]
-    p = _resolve_precision(precision)
-    m = _lib.SELF_MODE[self_mode]
-    shp = ctypes.byref(shape) if shape is not None else None
-    nbytes = ctypes.c_size_t(0)
-    _lib.call("f3d_pair_workspace_bytes", k, p, ns, nt, shp, ctypes.byref(nbytes))
-    ws_ptr, ws_len = _lib.Workspace.get(dev).ensure(nbytes.value)
-    _lib.call("f3d_pair_sum", k, p, m, _lib.ptr(rs), _lib.ptr(rt), _lib.ptr(d), _lib.ptr(n),
-              _lib.ptr(gs), _lib.ptr(gt), _lib.ptr(out), ns, nt, float(eta), float(reg),
-              float(epsilon_distance), int(bool(accumulate)), shp, ws_ptr, ws_len,
-              _lib.stream_handle(dev))
+    _launch(dev, _lib.KERNEL[kernel], _resolve_precision(precision), _lib.SELF_MODE[self_mode], rs, rt, d, n,
+            gs, gt, out, float(eta), float(reg), float(epsilon_distance), accumulate, shape)
     return out
+
+
+_ws_bytes: dict = {}
+
+
+def _launch(dev, k: int, p: int, m: int, rs, rt, d, n, gs, gt, out, eta: float, reg: float, eps: float,
+            accumulate: bool, shape) -> None:
+    """One f3d_pair_sum on validated device tensors (the workspace size of a
+    (kernel, precision, sizes, shape) is asked of the library once)."""
+    ns, nt = rs.shape[0], rt.shape[0]
+    shp = ctypes.byref(shape) if shape is not None else None
+    key = (k, p, ns, nt, None if shape is None else (shape.tpt, shape.sl, shape.nsplit, shape.use_tma))
+    nbytes = _ws_bytes.get(key)
+    if nbytes is None:
+        nb = ctypes.c_size_t(0)
+        _lib.call("f3d_pair_workspace_bytes", k, p, ns, nt, shp, ctypes.byref(nb))
+        nbytes = _ws_bytes[key] = nb.value
+    ws_ptr, ws_len = _lib.Workspace.get(dev).ensure(nbytes)
+    _lib.call("f3d_pair_sum", k, p, m, _lib.ptr(rs), _lib.ptr(rt), _lib.ptr(d), _lib.ptr(n),
+              _lib.ptr(gs), _lib.ptr(gt), _lib.ptr(out), ns, nt, eta, reg, eps, int(bool(accumulate)), shp,
+              ws_ptr, ws_len, _lib.stream_handle(dev))
+
+
+def _host_points(x, name: str):
+    """A host (N, 3) float64 array (numpy or CPU tensor) -> (contiguous array
+    or tensor kept alive, its address, N)."""
+    if isinstance(x, torch.Tensor):
+        t = x.detach()
+        if t.dtype != torch.float64 or not t.is_contiguous():
+            t = t.to(torch.float64).contiguous()
+        n = t.numel()
+        ptr = t.data_ptr()
+    else:
+        t = np.ascontiguousarray(np.asarray(x, dtype=np.float64))
+        n = t.size
+        ptr = t.ctypes.data
+    if n % 3 != 0:
+        raise ValueError(f"{name}: size {n} is not a multiple of 3")
+    return t, ptr, n // 3
+
+
+def _drop_in_host(kernel, r_source, r_target, density, normal, self_mode, eta, reg, epsilon_distance,
+                  precision, shape, dev):
+    """All inputs on the host and the launch shape known: one library call
+    stages the inputs, runs the sum, copies the result back and waits
+    (f3d_pair_sum_host)."""
+    rs, p_rs, ns = _host_points(r_source, "r_source")
+    if r_target is r_source:
+        rt, p_rt, nt = rs, p_rs, ns
+    else:
+        rt, p_rt, nt = _host_points(r_target, "r_target")
+    d, p_d, nd = _host_points(density, "density")
+    p_n, nn = None, None
+    if normal is not None:
+        nrm, p_n, nn = _host_points(normal, "normal")
+    if nd != ns or (nn is not None and nn != (nt if kernel == "traction" else ns)):
+        raise ValueError("density / normal point counts do not match the points")
+    k, p, m = _lib.KERNEL[kernel], _resolve_precision(precision), _lib.SELF_MODE[self_mode]
+    out = torch.empty(3 * nt, dtype=torch.float64, pin_memory=True)
+    if nt == 0:
+        return out.numpy()
+    shp = ctypes.byref(shape) if shape is not None else None
+    key = (k, p, ns, nt, None if shape is None else (shape.tpt, shape.sl, shape.nsplit, shape.use_tma))
+    nbytes = _ws_bytes.get(key)
+    if nbytes is None:
+        nb = ctypes.c_size_t(0)
+        _lib.call("f3d_pair_workspace_bytes", k, p, ns, nt, shp, ctypes.byref(nb))
+        nbytes = _ws_bytes[key] = nb.value
+    ws_ptr, ws_len = _lib.Workspace.get(dev).ensure(nbytes)
+    hb = ctypes.c_size_t(0)
+    _lib.call("f3d_pair_host_bytes", k, ns, nt, int(p_rs == p_rt), ctypes.byref(hb))
+    st_ptr, st_len = _lib.Staging.get(dev).ensure(hb.value)
+    status = _lib.lib().f3d_pair_sum_host(k, p, m, p_rs, p_rt, p_d, p_n, out.data_ptr(), ns, nt, float(eta),
+                                          float(reg), float(epsilon_distance), shp, st_ptr, st_len, ws_ptr, ws_len,
+                                          _lib.stream_handle(dev))
+    if status != _lib.F3D_OK:
+        if status == _lib.F3D_ERR_TIMEOUT:
+            _lib.Workspace.reset_all()
+        _lib.check("f3d_pair_sum_host", status)
+    return out.numpy()
 
 
 def _drop_in(kernel, r_source, r_target, density, normal, self_mode, eta, reg, epsilon_distance,
              precision, shape):
     """A pair-sum drop-in: inputs to the device once, the autotuned launch
-    shape unless one is given, the sum, the output back like the inputs."""
+    shape unless one is given, the sum, the output back like the inputs.
+    With every input on the host and the shape known (given, tuned earlier
+    for this size bucket, or the library default when tuning is off), one
+    library call does it all."""
     host = _any_host(r_source, r_target, density, normal)
     dev = _device()
+    if host and not any(isinstance(x, torch.Tensor) and x.is_cuda for x in (r_source, r_target, density, normal)):
+        if shape is None and AUTOTUNE:
+            from . import autotune
+            ns_, nt_ = np.size(r_source) // 3, np.size(r_target) // 3
+            if isinstance(r_source, torch.Tensor):
+                ns_ = r_source.numel() // 3
+            if isinstance(r_target, torch.Tensor):
+                nt_ = r_target.numel() // 3
+            shp = autotune.cached(kernel, precision, self_mode, ns_, nt_)
+            if shp is not None:
+                return _drop_in_host(kernel, r_source, r_target, density, normal, self_mode, eta, reg,
+                                     epsilon_distance, precision, shp, dev)
+        else:
+            return _drop_in_host(kernel, r_source, r_target, density, normal, self_mode, eta, reg,
+                                 epsilon_distance, precision, shape, dev)
     rs = _to_dev(r_source, dev, "r_source")
     rt = rs if r_target is r_source else _to_dev(r_target, dev, "r_target")
     d = _to_dev(density, dev, "density")
     n = _to_dev(normal, dev, "normal") if normal is not None else None
+    if d.shape[0] != rs.shape[0] or (n is not None and n.shape[0] != (rt if kernel == "traction" else rs).shape[0]):
+        raise ValueError("density / normal point counts do not match the points")
     if shape is None and AUTOTUNE and rs.shape[0] and rt.shape[0]:
         from . import autotune
         shape = autotune.tune(kernel, rs, rt, d, n, self_mode=self_mode, precision=precision, eta=eta,
                               reg=reg, epsilon_distance=epsilon_distance)
-    u = pair_sum(kernel, rs, rt, d, n, eta=eta, reg=reg, epsilon_distance=epsilon_distance,
-                 self_mode=self_mode, precision=precision, shape=shape)
+    u = torch.empty(3 * rt.shape[0], dtype=torch.float64, device=dev)
+    _launch(dev, _lib.KERNEL[kernel], _resolve_precision(precision), _lib.SELF_MODE[self_mode], rs, rt, d, n,
+            None, None, u, float(eta), float(reg), float(epsilon_distance), False, shape)
     return _out(u, host, kernel)
 
 

@@ -141,6 +141,26 @@ int f3d_pair_sum(int kernel, int precision, int self_mode,
                  int accumulate, const f3d_pair_shape *shape,
                  void *workspace, size_t workspace_bytes, void *stream);
 
+/* The same sum from HOST memory in one call, for host-side bindings (the
+   numpy-in, numpy-out functions of fiber3d's kernels.kernels,
+   python/kernels/kernels.py:214-1264): r_source (ns x 3), r_target (nt x 3;
+   pass the r_source pointer itself for a sum over one point set, which is
+   then copied once), density (ns x 3), normal (stresslet: ns x 3 source
+   normals; traction: nt x 3 target normals; else NULL) are copied to
+   `device_buffer` (f3d_pair_host_bytes of them, 256-byte aligned), the sum
+   runs on `stream` with `workspace` as f3d_pair_sum's, the result is copied
+   into `out` (nt x 3, host) and the stream is synchronised.  Page-locked
+   host buffers make the copies asynchronous.  Returns F3D_OK, an argument
+   status, or the first status a kernel recorded in the device error word
+   (then cleared), e.g. F3D_ERR_TIMEOUT.  F3D_SELF_SKIP_GROUP is not
+   accepted (no group ids on this path). */
+int f3d_pair_host_bytes(int kernel, int64_t ns, int64_t nt, int same_points, size_t *bytes);
+int f3d_pair_sum_host(int kernel, int precision, int self_mode, const double *r_source,
+                      const double *r_target, const double *density, const double *normal, double *out,
+                      int64_t ns, int64_t nt, double eta, double reg, double epsilon_distance,
+                      const f3d_pair_shape *shape, void *device_buffer, size_t device_bytes,
+                      void *workspace, size_t workspace_bytes, void *stream);
+
 /* Resident CTAs per SM of the pair kernel that a sum of this kernel,
    precision, self mode (dual: the two-density FP64 Oseen pass) and launch
    shape would run (cudaOccupancyMaxActiveBlocksPerMultiprocessor), so that

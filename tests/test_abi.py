@@ -155,3 +155,12 @@ def test_autotune_candidates_fill_whole_waves():
     for waves in (1, 2, 3, 4):
         assert (waves * 888) // 63 in splits
     assert all(c[3] in (0, -1) for c in cands)
+
+
+def test_host_entry_argument_checks(dll):
+    nb = ctypes.c_size_t(0)
+    assert dll.f3d_pair_host_bytes(1, 100, 50, 0, ctypes.byref(nb)) == 0 and nb.value > 0
+    assert dll.f3d_pair_host_bytes(9, 100, 50, 0, ctypes.byref(nb)) == 5
+    # group ids are not accepted on the host path; nothing is launched
+    assert dll.f3d_pair_sum_host(0, 0, 2, None, None, None, None, None, 10, 10, 1.0, 5e-3, 1e-5,
+                                 None, None, 0, None, 0, None) == 5

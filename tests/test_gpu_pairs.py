@@ -351,3 +351,46 @@ def test_occupancy_query(L):
         for tpt, sl in ((1, 1), (2, 1), (1, 8), (1, 32)):
             n = autotune.occupancy(kind, "fp64", "skip_group", tpt, sl)
             assert 1 <= n <= 16
+
+
+@pytest.mark.parametrize("kind,mode", [("stresslet", "skip_index"), ("oseen", "regularise"),
+                                       ("traction", "skip_index"), ("rotlet", "regularise")])
+def test_host_entry_matches_device_entry(L, kind, mode):
+    """f3d_pair_sum_host (host buffers in and out, one call) equals
+    f3d_pair_sum on device copies of the same inputs, bit for bit."""
+    import ctypes
+    rng = np.random.default_rng(5)
+    n = 900
+    x = rng.random((n, 3)) * 3
+    xt = x if mode == "skip_index" else rng.random((700, 3)) * 3
+    d = rng.normal(size=(n, 3))
+    nr = rng.normal(size=(xt.shape[0] if kind == "traction" else n, 3)) if kind in ("stresslet", "traction") else None
+    from fiber3d_b200 import kernels as K
+    ref = K.pair_sum(kind, x, xt, d, nr, self_mode=mode).cpu().numpy()
+    k, p, m = L.KERNEL[kind], L.PRECISION["fp64"], L.SELF_MODE[mode]
+    nt = xt.shape[0]
+    out = np.empty(3 * nt)
+    hb = ctypes.c_size_t(0)
+    L.call("f3d_pair_host_bytes", k, n, nt, int(xt is x), ctypes.byref(hb))
+    stage = torch.empty(hb.value, dtype=torch.uint8, device="cuda")
+    wb = ctypes.c_size_t(0)
+    L.call("f3d_pair_workspace_bytes", k, p, n, nt, None, ctypes.byref(wb))
+    ws = torch.zeros(max(wb.value, 1), dtype=torch.uint8, device="cuda")
+    ptr = lambda a: a.ctypes.data if a is not None else None
+    L.call("f3d_pair_sum_host", k, p, m, ptr(x), ptr(xt), ptr(d), ptr(nr), ptr(out), n, nt, 1.0, 5e-3, 1e-5,
+           None, stage.data_ptr(), stage.numel(), ws.data_ptr(), ws.numel(), L.stream_handle())
+    assert np.array_equal(out, ref)
+
+
+def test_drop_in_host_fast_path_repeatable(K):
+    """The second call of a size bucket takes the one-call host path; it
+    gives the oracle's sum like the first."""
+    rng = np.random.default_rng(6)
+    x = rng.random((1500, 3)) * 4
+    nr = rng.normal(size=(1500, 3))
+    d = rng.normal(size=(1500, 3))
+    ref = O.stresslet_kernel_times_normal_times_density(x, nr, d)
+    a = K.stresslet_kernel_times_normal_times_density_numba(x, nr, d)
+    b = K.stresslet_kernel_times_normal_times_density_numba(x, nr, d)
+    assert rel_err(a, ref) < TOL64 and rel_err(b, ref) < TOL64
+    assert isinstance(b, np.ndarray) and b.shape == (4500,)
