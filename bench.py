@@ -167,13 +167,13 @@ def measured_peak(L, precision: str, torch):
     st = L.stream_handle()
     prec = L.PRECISION[precision]
     for _ in range(2):
-        L.call("f3d_probe_fma", prec, 4096, L.ptr(sink), ctypes.byref(flops), st)
+        L.call("f3d_probe_fma", prec, 8192, L.ptr(sink), ctypes.byref(flops), st)
     torch.cuda.synchronize()
     best = 0.0
     for _ in range(5):
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
-        L.call("f3d_probe_fma", prec, 4096, L.ptr(sink), ctypes.byref(flops), st)
+        L.call("f3d_probe_fma", prec, 8192, L.ptr(sink), ctypes.byref(flops), st)
         e1.record()
         e1.synchronize()
         best = max(best, flops.value / (e0.elapsed_time(e1) * 1e-3))
@@ -197,11 +197,27 @@ def gpu_arm(args, rank, world, local):
     out = torch.empty(trg.numel(), dtype=torch.float64, device=dev)
     flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=dev)
 
+    # the sum over the node set itself (j == i skipped) and, for the
+    # stresslet workload, onto the ball points: two calls, each at the launch
+    # shape the autotuner picks for it (the self-sum may take the symmetric
+    # form, which evaluates each unordered pair once)
     from fiber3d_b200 import autotune
-    shapes = {p: autotune.tune(kind, src, trg, dens, nrm, self_mode="skip_group", src_group=gs,
-                               trg_group=gt, precision=p) for p in ("fp64", "fp32c")}
-    launches_per_step = 1
+    n_src = src.shape[0]
+    out_self, out_vol = out[:3 * n_src], out[3 * n_src:]
+    vol = trg[n_src:] if trg.shape[0] > n_src else None
+    shapes = {p: autotune.tune(kind, src, src, dens, nrm, self_mode="skip_index", precision=p)
+              for p in ("fp64", "fp32c")}
+    shapes_vol = {p: autotune.tune(kind, src, vol, dens, nrm, self_mode="regularise", precision=p)
+                  for p in ("fp64", "fp32c")} if vol is not None else {}
+    launches_per_step = 2 if vol is not None else 1
     subtract = None
+
+    def pairs(precision):
+        K.pair_sum(kind, src, src, dens, nrm, self_mode="skip_index", precision=precision, out=out_self,
+                   shape=shapes[precision])
+        if vol is not None:
+            K.pair_sum(kind, src, vol, dens, nrm, self_mode="regularise", precision=precision, out=out_vol,
+                       shape=shapes_vol[precision])
     if kind == "stresslet":
         # the periphery operator's rows on the node targets (tstep.py:1097-1104):
         # res = v - E mu - mu + n sum(n.q), E the singularity-subtraction vectors
@@ -211,15 +227,14 @@ def gpu_arm(args, rank, world, local):
         E = singularity_vectors(src, nrm, wts, 1.0, 5e-3, 1e-5)
         res = torch.empty(3 * n_nodes, dtype=torch.float64, device=dev)
         scratch = torch.zeros(1, dtype=torch.float64, device=dev)
-        launches_per_step = 2
+        launches_per_step += 1
 
         def subtract():
             L.call("f3d_shell_residual", L.ptr(out), L.ptr(E), L.ptr(wts), L.ptr(nrm), L.ptr(dens), L.ptr(res),
                    n_nodes, L.ptr(scratch), L.stream_handle(dev))
 
     def step(precision="fp64"):
-        K.pair_sum(kind, src, trg, dens, nrm, self_mode="skip_group", src_group=gs, trg_group=gt,
-                   precision=precision, out=out, shape=shapes[precision])
+        pairs(precision)
         if subtract is not None:
             subtract()
 
@@ -237,8 +252,7 @@ def gpu_arm(args, rank, world, local):
             e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
             torch.cuda.nvtx.range_push(f"timed_pairs_{precision}")
             e0.record()
-            K.pair_sum(kind, src, trg, dens, nrm, self_mode="skip_group", src_group=gs, trg_group=gt,
-                       precision=precision, out=out, shape=shapes[precision])
+            pairs(precision)
             e1.record()
             if subtract is not None:
                 subtract()
@@ -275,7 +289,10 @@ def gpu_arm(args, rank, world, local):
 
     # e2e through the drop-in API from pinned host buffers
     host = {k: torch.as_tensor(wl[k]).pin_memory() for k in ("nodes", "dens", "nrm", "vol") if wl[k] is not None}
-    h2d = sum(t.numel() * t.element_size() for t in host.values())
+    nbytes = lambda *ks: sum(host[k].numel() * host[k].element_size() for k in ks)
+    # what the calls below copy to the device: each call its own inputs
+    h2d = (nbytes("nodes", "nrm", "dens") + nbytes("nodes", "vol", "nrm", "dens") if kind == "stresslet"
+           else nbytes("nodes", "dens"))
 
     def e2e_step():
         if kind == "stresslet":
@@ -308,7 +325,10 @@ def gpu_arm(args, rank, world, local):
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
         "config": workload_config(args.workload, wl),
         "parallelism": f"replicas x{world}",
-        "launch_shape": {p: [v.tpt, v.sl, v.nsplit, v.use_tma] for p, v in shapes.items()},
+        "launch_shape": {"self_sum": {p: [v.tpt, v.sl, v.nsplit, v.use_tma] for p, v in shapes.items()},
+                         "ball_targets": {p: [v.tpt, v.sl, v.nsplit, v.use_tma] for p, v in shapes_vol.items()},
+                         "note": "[tpt, sl, nsplit, use_tma]; sl = -1 is the symmetric self-sum "
+                                 "(pair_sym_kernel: each unordered pair once)"},
         "roofline": {"bound": "fp64", "achieved": achieved / 1e12, "peak": peak64 / 1e12,
                      "unit": "TFLOP/s", "frac": achieved / peak64,
                      "kernel_ms_avg": kern_avg,
@@ -318,7 +338,9 @@ def gpu_arm(args, rank, world, local):
                      "traffic_unit": "bytes per launch (ncu dram__bytes_read.sum + dram__bytes_write.sum)",
                      "note": f"{flop_pair} algorithmic flop per pair (rsqrt not counted); peak = "
                              "measured FP64 FMA rate of this GPU (f3d_probe_fma)",
-                     "kernel": f"pair_kernel<{kind}, skip_group, fp64>"},
+                     "kernel": f"{kind} self-sum (pair_sym_kernel if launch_shape.self_sum.fp64[1] == -1, "
+                               "else pair_kernel) + pair_kernel source->target onto the ball points; "
+                               "both launches inside the event pair"},
         "timed_output_vs_default_shape_max_rel": check64,
         "fp32c": {"value": pairs / (ms32 * 1e-3) * world, "ms_per_step": ms32,
                   "max_rel_err_vs_fp64": err32, "peak_fp32_tflops": peak32 / 1e12},

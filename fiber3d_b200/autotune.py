@@ -41,12 +41,25 @@ def _bucket(n: int) -> int:
 _names: dict[int, str] = {}
 
 
-def _key(kernel, precision, self_mode, ns, nt) -> str:
+def _key(kernel, precision, self_mode, ns, nt, same=False) -> str:
+    """Cache key: GPU, sum, size buckets, and whether the sum runs over one
+    point set (sources are the targets, which allows the symmetric form)."""
     dev = torch.cuda.current_device()
     name = _names.get(dev)
     if name is None:
         name = _names[dev] = torch.cuda.get_device_name(dev).replace(" ", "_")
-    return f"{name}|{kernel}|{precision}|{self_mode}|{_bucket(ns)}|{_bucket(nt)}"
+    one = "|self" if (same and ns == nt) else ""
+    return f"{name}|{kernel}|{precision}|{self_mode}|{_bucket(ns)}|{_bucket(nt)}{one}"
+
+
+# the symmetric self-sum's launch shape (f3d_pair_shape.sl = -1)
+SYMMETRIC = (1, -1, 0, -1)
+SYM_MAX_POINTS = 192 * 128
+
+
+def symmetric_eligible(kernel, precision, self_mode, ns, nt, same) -> bool:
+    return (same and ns == nt and 0 < ns <= SYM_MAX_POINTS and precision == "fp64"
+            and kernel in ("oseen", "stresslet") and self_mode in ("skip_index", "skip_group"))
 
 
 def _load():
@@ -108,9 +121,10 @@ def tune(kernel: str, r_source, r_target, density, normal=None, *, self_mode="re
     from . import kernels as K
     ns = int(r_source.shape[0] if hasattr(r_source, "shape") and len(r_source.shape) == 2 else len(r_source) // 3)
     nt = int(r_target.shape[0] if hasattr(r_target, "shape") and len(r_target.shape) == 2 else len(r_target) // 3)
+    same = r_target is r_source and (self_mode != "skip_group" or trg_group is src_group)
     with _lock:
         _load()
-        key = _key(kernel, precision, self_mode, ns, nt)
+        key = _key(kernel, precision, self_mode, ns, nt, same)
         if key in _cache and not force:
             return _lib.PairShape(*_cache[key])
     sms = torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
@@ -119,9 +133,15 @@ def tune(kernel: str, r_source, r_target, density, normal=None, *, self_mode="re
     out = K.pair_sum(kernel, r_source, r_target, density, normal, **kw)
     best, best_t = None, float("inf")
     occ = lambda tpt, sl: occupancy(kernel, precision, self_mode, tpt, sl)
-    for cand in candidates(nt, sms, occ):
+    cands = candidates(nt, sms, occ)
+    if symmetric_eligible(kernel, precision, self_mode, ns, nt, same):
+        cands.append(SYMMETRIC)
+    for cand in cands:
         shp = _lib.PairShape(*cand)
-        K.pair_sum(kernel, r_source, r_target, density, normal, shape=shp, out=out, **kw)
+        try:
+            K.pair_sum(kernel, r_source, r_target, density, normal, shape=shp, out=out, **kw)
+        except _lib.F3DError:
+            continue  # a shape this sum cannot take
         torch.cuda.synchronize()
         t = float("inf")
         for _ in range(reps):
@@ -140,11 +160,12 @@ def tune(kernel: str, r_source, r_target, density, normal=None, *, self_mode="re
     return _lib.PairShape(*best)
 
 
-def cached(kernel: str, precision: str, self_mode: str, ns: int, nt: int) -> _lib.PairShape | None:
+def cached(kernel: str, precision: str, self_mode: str, ns: int, nt: int,
+           same: bool = False) -> _lib.PairShape | None:
     """The tuned shape of this sum's bucket if one is known (no tuning)."""
     with _lock:
         _load()
-        v = _cache.get(_key(kernel, precision, self_mode, ns, nt))
+        v = _cache.get(_key(kernel, precision, self_mode, ns, nt, same))
     return _lib.PairShape(*v) if v is not None else None
 
 

@@ -29,6 +29,7 @@
 #include <type_traits>
 
 #include "f3d_common.cuh"
+#include "f3d_pair_math.cuh"
 
 namespace f3d {
 
@@ -82,50 +83,6 @@ constexpr size_t snapshot_bytes() {
 template <int KIND, int MODE, int PREC, bool DUAL = false>
 constexpr size_t pair_smem_bytes() {
   return 128 + 2 * Stage<KIND, MODE, PREC, DUAL>::bytes + snapshot_bytes<PREC, DUAL>();
-}
-
-// Reciprocal square roots in FP64.  y0 = rsqrt.approx.ftz.f64(x) (PTX; about
-// 2^-22 relative error) is a seed; with u = y0^2 and e = 1 - x u (one FMA,
-// exact to rounding), x^(-1/2) = y0 (1 - e)^(-1/2) and x^(-5/2) =
-// y0 u^2 (1 - e)^(-5/2).  The binomial series to second order,
-//   (1 - e)^(-1/2) = 1 + e/2 + 3e^2/8,   (1 - e)^(-5/2) = 1 + 5e/2 + 35e^2/8,
-// leaves O(e^3) ~ 2^-66: below double rounding.  (The first is one
-// Halley-type step for 1/sqrt(x); folding the second into the power r^-5
-// that the stresslet needs saves the separate refinement.)  For x = 0 the
-// result is not finite; callers discard such pairs with a select.
-__device__ __forceinline__ double rsqrt_seed(double x) {
-  double y;
-  asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
-  return y;
-}
-
-__device__ __forceinline__ double rsqrt_refined(double x) {
-  const double y = rsqrt_seed(x);
-  const double e = fma(-x, y * y, 1.0);
-  return fma(y * e, fma(0.375, e, 0.5), y);
-}
-
-// q * x^(-5/2) for x > 0.
-__device__ __forceinline__ double times_rsqrt5(double q, double x) {
-  const double y = rsqrt_seed(x);
-  const double u = y * y;
-  const double e = fma(-x, u, 1.0);
-  const double qy5 = (q * y) * (u * u);
-  return fma(qy5 * e, fma(4.375, e, 2.5), qy5);
-}
-
-// Adds reg2 to r2 where r2 < eps2 (compared on the IEEE bit patterns, which
-// order like the values for non-negative doubles, on the integer pipe).  Such
-// pairs are rare, so the add runs in a branch that a warp takes only when one
-// of its lanes needs it: the common path spends no FP64 instruction on it.
-// The vote covers exactly the lanes executing it, and each lane's own
-// predicate is part of its vote, so the result does not depend on
-// convergence.
-__device__ __forceinline__ double regularise(double r2, bool close, double reg2) {
-  if (__any_sync(__activemask(), close)) {
-    if (close) r2 += reg2;
-  }
-  return r2;
 }
 
 __device__ __forceinline__ void two_sum(float &s, float &c, float x) {
@@ -698,8 +655,16 @@ __global__ void pack_fp32_sources(const double *rs, const double *dens, const do
 }
 
 // ---------------------------------------------------------------- host ----
+// The symmetric self-sum (f3d_pairs_sym.cu).
+size_t sym_partial_bytes(int64_t n);
+bool sym_fits(int64_t n);
+int pair_sym_launch(int kernel, int self_mode, const double *x, const double *dens, const double *nrm,
+                    const int32_t *grp, double *out, int64_t n, double eta, double reg, double eps, int accumulate,
+                    double *partial, unsigned *counters, int *occupancy, cudaStream_t st);
+
 struct Plan {
   int tpt, sl, nsplit, use_tma;
+  bool sym;  // shape.sl == -1: the symmetric self-sum
   int64_t ntb, tiles_per_split;
   size_t off_counters, off_partial, off_packed, bytes;
 };
@@ -708,6 +673,26 @@ static int make_plan(int kernel, int precision, int64_t ns, int64_t nt, const f3
                      Plan *p, bool dual = false) {
   if (kernel < 0 || kernel > 3 || precision < 0 || precision > 1) return F3D_ERR_ARG;
   if (ns < 0 || nt < 0) return F3D_ERR_SHAPE;
+  p->sym = false;
+  if (shape && shape->sl == -1) {
+    // symmetric self-sum: FP64 Oseen or stresslet over one point set
+    if (dual || precision != F3D_FP64 || !(kernel == F3D_KERNEL_OSEEN || kernel == F3D_KERNEL_STRESSLET))
+      return F3D_ERR_ARG;
+    if (ns != nt) return F3D_ERR_SHAPE;
+    if (!sym_fits(ns)) return F3D_ERR_TOO_LARGE;
+    p->sym = true;
+    p->tpt = 1;
+    p->sl = -1;
+    p->nsplit = 1;
+    p->use_tma = 0;
+    p->ntb = (ns + kBlock - 1) / kBlock;
+    p->tiles_per_split = 0;
+    p->off_counters = 0;
+    p->off_partial = kCounterBytes;
+    p->off_packed = kCounterBytes;
+    p->bytes = ns > 0 ? kCounterBytes + round_up(sym_partial_bytes(ns), 256) : 0;
+    return F3D_OK;
+  }
   int tpt = shape && shape->tpt ? shape->tpt : 0;
   int sl = shape && shape->sl ? shape->sl : 0;
   if (sl == 0) sl = (nt >= 4096) ? 1 : (nt >= 512 ? 8 : 32);
@@ -819,6 +804,7 @@ static int pair_sum_core(int kernel, int precision, int self_mode, const double 
   if (rc) return rc;
   if (self_mode < 0 || self_mode > 3) return F3D_ERR_ARG;
   if (dual && self_mode == F3D_SELF_SKIP_CLOSE) return F3D_ERR_ARG;
+  if (p.sym && !(self_mode == F3D_SELF_SKIP_INDEX || self_mode == F3D_SELF_SKIP_GROUP)) return F3D_ERR_ARG;
   if (nt == 0) return F3D_OK;
   if (!rt || !out) return F3D_ERR_NULL;
   if (ns > 0 && (!rs || !dens)) return F3D_ERR_NULL;
@@ -842,6 +828,13 @@ static int pair_sum_core(int kernel, int precision, int self_mode, const double 
   if (p.bytes > 0 && (!ws || ws_bytes < p.bytes)) return F3D_ERR_WORKSPACE;
   if (ws && !aligned(ws, 256)) return F3D_ERR_ALIGN;
   unsigned char *w = static_cast<unsigned char *>(ws);
+  if (p.sym) {
+    // one point set: sources and targets (and their group ids) must be the same arrays
+    if (rs != rt || (self_mode == F3D_SELF_SKIP_GROUP && gs != gt)) return F3D_ERR_ARG;
+    return pair_sym_launch(kernel, self_mode, rs, dens, nrm, gs, out, ns, eta, reg, eps, accumulate,
+                           reinterpret_cast<double *>(w + p.off_partial), reinterpret_cast<unsigned *>(w),
+                           nullptr, st);
+  }
 
   PairArgs a{};
   a.rs = rs; a.rt = rt; a.dens = dens; a.nrm = nrm;
@@ -990,6 +983,13 @@ int f3d_pair_occupancy(int kernel, int precision, int self_mode, int dual, const
   if (self_mode < 0 || self_mode > 3) return F3D_ERR_ARG;
   if (dual && (kernel != F3D_KERNEL_OSEEN || precision != F3D_FP64 || self_mode == F3D_SELF_SKIP_CLOSE))
     return F3D_ERR_ARG;
+  if (shape && shape->sl == -1) {
+    if (dual || precision != F3D_FP64 || !(kernel == F3D_KERNEL_OSEEN || kernel == F3D_KERNEL_STRESSLET) ||
+        !(self_mode == F3D_SELF_SKIP_INDEX || self_mode == F3D_SELF_SKIP_GROUP))
+      return F3D_ERR_ARG;
+    return f3d::pair_sym_launch(kernel, self_mode, nullptr, nullptr, nullptr, nullptr, nullptr, 1, 1.0, 0.0, 0.0, 0,
+                                nullptr, nullptr, ctas_per_sm, nullptr);
+  }
   // the shape's own tpt/sl (make_plan picks defaults for a 1-target sum)
   if (shape && shape->tpt) p.tpt = shape->tpt;
   if (shape && shape->sl) p.sl = shape->sl;

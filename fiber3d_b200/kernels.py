@@ -235,12 +235,9 @@ def _drop_in(kernel, r_source, r_target, density, normal, self_mode, eta, reg, e
     if host and not any(isinstance(x, torch.Tensor) and x.is_cuda for x in (r_source, r_target, density, normal)):
         if shape is None and AUTOTUNE:
             from . import autotune
-            ns_, nt_ = np.size(r_source) // 3, np.size(r_target) // 3
-            if isinstance(r_source, torch.Tensor):
-                ns_ = r_source.numel() // 3
-            if isinstance(r_target, torch.Tensor):
-                nt_ = r_target.numel() // 3
-            shp = autotune.cached(kernel, precision, self_mode, ns_, nt_)
+            size = lambda a: a.numel() if isinstance(a, torch.Tensor) else np.size(a)
+            shp = autotune.cached(kernel, precision, self_mode, size(r_source) // 3, size(r_target) // 3,
+                                  same=r_target is r_source)
             if shp is not None:
                 return _drop_in_host(kernel, r_source, r_target, density, normal, self_mode, eta, reg,
                                      epsilon_distance, precision, shp, dev)

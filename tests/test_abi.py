@@ -164,3 +164,15 @@ def test_host_entry_argument_checks(dll):
     # group ids are not accepted on the host path; nothing is launched
     assert dll.f3d_pair_sum_host(0, 0, 2, None, None, None, None, None, 10, 10, 1.0, 5e-3, 1e-5,
                                  None, None, 0, None, 0, None) == 5
+
+
+def test_symmetric_shape_plan_checks(dll):
+    shp = _lib.PairShape(1, -1, 0, -1)
+    nb = ctypes.c_size_t(0)
+    assert dll.f3d_pair_workspace_bytes(1, 0, 12000, 12000, ctypes.byref(shp), ctypes.byref(nb)) == 0
+    assert nb.value >= 94 * 94 * 128 * 3 * 8          # T^2 partial tiles
+    assert dll.f3d_pair_workspace_bytes(1, 0, 12000, 4096, ctypes.byref(shp), ctypes.byref(nb)) == 2  # ns != nt
+    assert dll.f3d_pair_workspace_bytes(1, 1, 1000, 1000, ctypes.byref(shp), ctypes.byref(nb)) == 5   # FP32C
+    assert dll.f3d_pair_workspace_bytes(2, 0, 1000, 1000, ctypes.byref(shp), ctypes.byref(nb)) == 5   # rotlet
+    assert dll.f3d_pair_workspace_bytes(0, 0, 192 * 128 + 1, 192 * 128 + 1, ctypes.byref(shp),
+                                        ctypes.byref(nb)) == 10

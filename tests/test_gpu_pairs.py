@@ -394,3 +394,90 @@ def test_drop_in_host_fast_path_repeatable(K):
     b = K.stresslet_kernel_times_normal_times_density_numba(x, nr, d)
     assert rel_err(a, ref) < TOL64 and rel_err(b, ref) < TOL64
     assert isinstance(b, np.ndarray) and b.shape == (4500,)
+
+
+def test_drop_in_host_fast_path_cpu_tensors(K):
+    """The one-call host path also takes CPU (and page-locked) torch tensors."""
+    rng = np.random.default_rng(7)
+    x = rng.random((1300, 3)) * 4
+    f = rng.normal(size=(1300, 3))
+    ref = O.oseen_kernel_times_density(x, f)
+    for pin in (False, True):
+        xt, ft = torch.as_tensor(x), torch.as_tensor(f)
+        if pin:
+            xt, ft = xt.pin_memory(), ft.pin_memory()
+        for _ in range(2):
+            u = K.oseen_kernel_times_density_numba(xt, ft)
+            assert isinstance(u, np.ndarray) and rel_err(u, ref) < TOL64
+
+
+SYM = (1, -1, 0, -1)
+
+
+@pytest.mark.parametrize("kind", ["oseen", "stresslet"])
+@pytest.mark.parametrize("n", [1, 127, 128, 129, 300, 1000, 5000])
+def test_symmetric_self_sum_skip_index(K, L, kind, n):
+    """The symmetric form (each unordered pair once) against the C oracle,
+    with a duplicated point and a sub-epsilon pair (the careful redo)."""
+    rng = np.random.default_rng(n + 13)
+    x = rng.random((n, 3)) * 3
+    if n > 40:
+        x[10] = x[11]
+        x[30] = x[31] + 3e-6
+    d = rng.normal(size=(n, 3)); nr = rng.normal(size=(n, 3))
+    ref = pairs_c.pair_sum(kind, x, x, d, nr if kind == "stresslet" else None, self_mode="skip_index")
+    xt = torch.as_tensor(x, device="cuda")
+    u = K.pair_sum(kind, xt, xt, d, nr if kind == "stresslet" else None, self_mode="skip_index",
+                   shape=L.PairShape(*SYM))
+    assert rel_err(u.cpu().numpy(), ref) < TOL64
+    # deterministic, and accumulate adds to what is there
+    u2 = K.pair_sum(kind, xt, xt, d, nr if kind == "stresslet" else None, self_mode="skip_index",
+                    shape=L.PairShape(*SYM))
+    assert torch.equal(u, u2)
+    K.pair_sum(kind, xt, xt, d, nr if kind == "stresslet" else None, self_mode="skip_index",
+               shape=L.PairShape(*SYM), out=u2, accumulate=True)
+    assert rel_err(u2.cpu().numpy(), 2 * ref) < TOL64
+
+
+@pytest.mark.parametrize("kind", ["oseen", "stresslet"])
+@pytest.mark.parametrize("nfib,npts", [(20, 32), (70, 32), (9, 24)])
+def test_symmetric_self_sum_skip_group(K, L, kind, nfib, npts):
+    """Fibers: pairs within one fiber skipped, in the symmetric form."""
+    from fiber3d_b200 import geometry
+    rng = np.random.default_rng(nfib * 7 + npts)
+    x = np.concatenate(geometry.perturbed_fibers(rng, nfib, npts, 2.0, 3.0))
+    grp = np.repeat(np.arange(nfib), npts).astype(np.int32)
+    d = rng.normal(size=x.shape); nr = rng.normal(size=x.shape)
+    ref = pairs_c.pair_sum(kind, x, x, d, nr if kind == "stresslet" else None, self_mode="skip_group",
+                           src_group=grp, trg_group=grp)
+    xt = torch.as_tensor(x, device="cuda")
+    g = torch.as_tensor(grp, device="cuda")
+    u = K.pair_sum(kind, xt, xt, d, nr if kind == "stresslet" else None, self_mode="skip_group", src_group=g,
+                   trg_group=g, shape=L.PairShape(*SYM))
+    assert rel_err(u.cpu().numpy(), ref) < TOL64
+
+
+def test_symmetric_config2_self_sum(K, L):
+    """The 12000-node sphere's double-layer self-sum in the symmetric form
+    against the regular kernel (full size) and sampled C-oracle rows."""
+    from fiber3d_b200 import geometry
+    nodes, normals, w, mu, vol = geometry.stresslet_sphere_workload(seed=2)
+    q = mu * w[:, None]
+    xt = torch.as_tensor(nodes, device="cuda")
+    a = K.pair_sum("stresslet", xt, xt, q, normals, self_mode="skip_index", shape=L.PairShape(*SYM))
+    b = K.pair_sum("stresslet", xt, xt, q, normals, self_mode="skip_index", shape=L.PairShape(1, 1, 0, 0))
+    assert rel_err(a.cpu().numpy(), b.cpu().numpy()) < 1e-13
+
+
+def test_symmetric_rejects_other_sums(K, L):
+    rng = np.random.default_rng(3)
+    x = rng.random((200, 3)); y = rng.random((200, 3)); d = rng.normal(size=(200, 3))
+    with pytest.raises(L.F3DError):   # two point sets
+        K.pair_sum("oseen", x, y, d, self_mode="skip_index", shape=L.PairShape(*SYM))
+    with pytest.raises(L.F3DError):   # FP32C
+        xt = torch.as_tensor(x, device="cuda")
+        K.pair_sum("oseen", xt, xt, d, self_mode="skip_index", precision="fp32c", shape=L.PairShape(*SYM))
+    big = torch.zeros((192 * 128 + 1, 3), dtype=torch.float64, device="cuda")
+    with pytest.raises(L.F3DError) as e:
+        K.pair_sum("oseen", big, big, big, self_mode="skip_index", shape=L.PairShape(*SYM))
+    assert e.value.status == 10
