@@ -212,7 +212,7 @@ def gpu_arm(args, rank, world, local):
     launches_per_step = 2 if vol is not None else 1
     subtract = None
 
-    def pairs(precision):
+    def pair_sums(precision):
         K.pair_sum(kind, src, src, dens, nrm, self_mode="skip_index", precision=precision, out=out_self,
                    shape=shapes[precision])
         if vol is not None:
@@ -234,7 +234,7 @@ def gpu_arm(args, rank, world, local):
                    n_nodes, L.ptr(scratch), L.stream_handle(dev))
 
     def step(precision="fp64"):
-        pairs(precision)
+        pair_sums(precision)
         if subtract is not None:
             subtract()
 
@@ -252,7 +252,7 @@ def gpu_arm(args, rank, world, local):
             e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
             torch.cuda.nvtx.range_push(f"timed_pairs_{precision}")
             e0.record()
-            pairs(precision)
+            pair_sums(precision)
             e1.record()
             if subtract is not None:
                 subtract()

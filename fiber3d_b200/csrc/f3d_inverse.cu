@@ -19,8 +19,10 @@
 // k = n-1 .. 0 gives A^-1.
 //
 // One CTA per block holds the whole NMAX x NMAX matrix in registers.  Lane l
-// of warp w owns rows R*l .. R*l+R-1 (R = NMAX/32) of columns 8w .. 8w+7, so
-// a column lives in one warp and a row is spread over all warps.  That makes
+// of warp w owns rows l, l+32, .. (R = NMAX/32 of them) of columns 8w ..
+// 8w+7, so a column lives in one warp and a row is spread over all warps;
+// rows interleaved across lanes keep every shared-memory access of a column
+// conflict-free.  That makes
 // the pivot step cheap for everyone but one warp:
 //   * the warp that owns column k+1 updates its tile for step k, then finds
 //     pivot k+1 on its own (two warp reductions, no shared memory), computes
@@ -92,7 +94,7 @@ __device__ __forceinline__ void inv_search_publish(const double (&a)[InvShape<NM
   unsigned key = 0u, row = 0xFFFFFFFFu;
 #pragma unroll
   for (int i = 0; i < R; ++i) {
-    const int r = lane * R + i;
+    const int r = i * 32 + lane;
     if (r >= k && r < n) {
       const unsigned kq = static_cast<unsigned>(
           static_cast<unsigned long long>(__double_as_longlong(fabs(a[i][JJ]))) >> 32);
@@ -103,7 +105,7 @@ __device__ __forceinline__ void inv_search_publish(const double (&a)[InvShape<NM
   const unsigned pmin = __reduce_min_sync(0xffffffffu, (row != 0xFFFFFFFFu && key == kmax) ? row : 0xFFFFFFFFu);
   const int p = pmin < static_cast<unsigned>(n) ? static_cast<int>(pmin) : k;
 #pragma unroll
-  for (int i = 0; i < R; ++i) sm.col[par][lane * R + i] = a[i][JJ];
+  for (int i = 0; i < R; ++i) sm.col[par][i * 32 + lane] = a[i][JJ];
   __syncwarp();
   if (lane == 0) {
     const double pv = sm.col[par][p];
@@ -138,13 +140,13 @@ __device__ __forceinline__ void inverse_step(double (&a)[InvShape<NMAX>::kRPL][k
     for (int i = 0; i < R; ++i) a[i][M] = 0.0;
   }
   // rows k and p of this warp's columns, through the per-warp buffer
-  if (lane == k / R) {
+  if (lane == k % 32) {
 #pragma unroll
-    for (int j = 0; j < kInvCPW; ++j) sm.rk[warp][j] = tile_at<R>(a, k % R, j);
+    for (int j = 0; j < kInvCPW; ++j) sm.rk[warp][j] = tile_at<R>(a, k / 32, j);
   }
-  if (lane == p / R) {
+  if (lane == p % 32) {
 #pragma unroll
-    for (int j = 0; j < kInvCPW; ++j) sm.rp[warp][j] = tile_at<R>(a, p % R, j);
+    for (int j = 0; j < kInvCPW; ++j) sm.rp[warp][j] = tile_at<R>(a, p / 32, j);
   }
   __syncwarp();
   // one FMA per element: a_ij <- base_ij - f_i u_j with u = old row p (u_k = 1
@@ -155,7 +157,7 @@ __device__ __forceinline__ void inverse_step(double (&a)[InvShape<NMAX>::kRPL][k
   bool isk[R], isp[R];
 #pragma unroll
   for (int i = 0; i < R; ++i) {
-    const int r = lane * R + i;
+    const int r = i * 32 + lane;
     isk[i] = (r == k);
     isp[i] = (r == p) && !isk[i];
     const double ci = sm.col[par][isp[i] ? k : r];
@@ -197,7 +199,7 @@ __global__ void __launch_bounds__(InvShape<NMAX>::kThreads, 1)
   double a[R][kInvCPW];
 #pragma unroll
   for (int i = 0; i < R; ++i) {
-    const int r = lane * R + i;
+    const int r = i * 32 + lane;
 #pragma unroll
     for (int j = 0; j < kInvCPW; ++j) {
       const int c = c0 + j;
@@ -237,7 +239,7 @@ __global__ void __launch_bounds__(InvShape<NMAX>::kThreads, 1)
   float *M32 = A32 ? A32 + moff[b] : nullptr;
 #pragma unroll
   for (int i = 0; i < R; ++i) {
-    const int r = lane * R + i;
+    const int r = i * 32 + lane;
     if (r >= n) continue;
 #pragma unroll
     for (int j = 0; j < kInvCPW; ++j) {
