@@ -197,27 +197,18 @@ def gpu_arm(args, rank, world, local):
     out = torch.empty(trg.numel(), dtype=torch.float64, device=dev)
     flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=dev)
 
-    # the sum over the node set itself (j == i skipped) and, for the
-    # stresslet workload, onto the ball points: two calls, each at the launch
-    # shape the autotuner picks for it (the self-sum may take the symmetric
-    # form, which evaluates each unordered pair once)
+    # one launch: targets = [nodes; ball points], sources = nodes, the pair
+    # j == i skipped through group ids (node index; -1 on the ball points)
     from fiber3d_b200 import autotune
-    n_src = src.shape[0]
-    out_self, out_vol = out[:3 * n_src], out[3 * n_src:]
-    vol = trg[n_src:] if trg.shape[0] > n_src else None
-    shapes = {p: autotune.tune(kind, src, src, dens, nrm, self_mode="skip_index", precision=p)
-              for p in ("fp64", "fp32c")}
-    shapes_vol = {p: autotune.tune(kind, src, vol, dens, nrm, self_mode="regularise", precision=p)
-                  for p in ("fp64", "fp32c")} if vol is not None else {}
-    launches_per_step = 2 if vol is not None else 1
-    subtract = None
+    shapes = {p: autotune.tune(kind, src, trg, dens, nrm, self_mode="skip_group", src_group=gs,
+                               trg_group=gt, precision=p) for p in ("fp64", "fp32c")}
+    launches_per_step = 1
 
     def pair_sums(precision):
-        K.pair_sum(kind, src, src, dens, nrm, self_mode="skip_index", precision=precision, out=out_self,
-                   shape=shapes[precision])
-        if vol is not None:
-            K.pair_sum(kind, src, vol, dens, nrm, self_mode="regularise", precision=precision, out=out_vol,
-                       shape=shapes_vol[precision])
+        K.pair_sum(kind, src, trg, dens, nrm, self_mode="skip_group", src_group=gs, trg_group=gt,
+                   precision=precision, out=out, shape=shapes[precision])
+
+    subtract = None
     if kind == "stresslet":
         # the periphery operator's rows on the node targets (tstep.py:1097-1104):
         # res = v - E mu - mu + n sum(n.q), E the singularity-subtraction vectors
@@ -325,10 +316,7 @@ def gpu_arm(args, rank, world, local):
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
         "config": workload_config(args.workload, wl),
         "parallelism": f"replicas x{world}",
-        "launch_shape": {"self_sum": {p: [v.tpt, v.sl, v.nsplit, v.use_tma] for p, v in shapes.items()},
-                         "ball_targets": {p: [v.tpt, v.sl, v.nsplit, v.use_tma] for p, v in shapes_vol.items()},
-                         "note": "[tpt, sl, nsplit, use_tma]; sl = -1 is the symmetric self-sum "
-                                 "(pair_sym_kernel: each unordered pair once)"},
+        "launch_shape": {p: [v.tpt, v.sl, v.nsplit, v.use_tma] for p, v in shapes.items()},
         "roofline": {"bound": "fp64", "achieved": achieved / 1e12, "peak": peak64 / 1e12,
                      "unit": "TFLOP/s", "frac": achieved / peak64,
                      "kernel_ms_avg": kern_avg,
@@ -338,9 +326,7 @@ def gpu_arm(args, rank, world, local):
                      "traffic_unit": "bytes per launch (ncu dram__bytes_read.sum + dram__bytes_write.sum)",
                      "note": f"{flop_pair} algorithmic flop per pair (rsqrt not counted); peak = "
                              "measured FP64 FMA rate of this GPU (f3d_probe_fma)",
-                     "kernel": f"{kind} self-sum (pair_sym_kernel if launch_shape.self_sum.fp64[1] == -1, "
-                               "else pair_kernel) + pair_kernel source->target onto the ball points; "
-                               "both launches inside the event pair"},
+                     "kernel": f"pair_kernel<{kind}, skip_group, fp64>"},
         "timed_output_vs_default_shape_max_rel": check64,
         "fp32c": {"value": pairs / (ms32 * 1e-3) * world, "ms_per_step": ms32,
                   "max_rel_err_vs_fp64": err32, "peak_fp32_tflops": peak32 / 1e12},

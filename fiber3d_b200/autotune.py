@@ -100,7 +100,7 @@ def candidates(nt: int, sms: int, occ=None):
     `occ(tpt, sl)` is known, splits that fill 1-4 whole waves of resident
     CTAs (no partly-filled last wave)."""
     out = []
-    for tpt, sl in ((1, 1), (2, 1), (1, 8), (1, 32)):
+    for tpt, sl in ((1, 1), (2, 1), (4, 1), (1, 8), (1, 32)):
         tpb = (128 // sl) * tpt
         ntb = max(1, -(-nt // tpb))
         splits = {max(1, -(-per_sm * sms // ntb)) for per_sm in (4, 8, 16)}

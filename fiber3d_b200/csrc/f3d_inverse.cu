@@ -149,29 +149,40 @@ __device__ __forceinline__ void inverse_step(double (&a)[InvShape<NMAX>::kRPL][k
     for (int j = 0; j < kInvCPW; ++j) sm.rp[warp][j] = tile_at<R>(a, p / 32, j);
   }
   __syncwarp();
-  // one FMA per element: a_ij <- base_ij - f_i u_j with u = old row p (u_k = 1
-  // in the owner's column k) and, per row:  row k: f = -1/a_pk, base = 0;
-  // row p (!= k): f = a_kk / a_pk, base = old row k;  others: f = a_ik / a_pk,
-  // base = a_ij
-  double f[R];
-  bool isk[R], isp[R];
+  // One FMA per element on every row: a_ij <- a_ij - (a_ik / a_pk) u_j with
+  // u = old row p (u_k = 1 in the owner's column k).  On row k this gives
+  // old row k - (a_kk / a_pk) u, which is exactly the new row p; on row p it
+  // gives nothing useful.  The two lanes holding rows k and p then put the
+  // right values in place: row k <- u / a_pk, row p <- old row k - (a_kk /
+  // a_pk) u.  (With p == k only the first.)  No per-element selects.
+  double u[kInvCPW];
+#pragma unroll
+  for (int j = 0; j < kInvCPW; ++j) u[j] = sm.rp[warp][j];
+  if (own) u[M] = 1.0;
 #pragma unroll
   for (int i = 0; i < R; ++i) {
-    const int r = i * 32 + lane;
-    isk[i] = (r == k);
-    isp[i] = (r == p) && !isk[i];
-    const double ci = sm.col[par][isp[i] ? k : r];
-    f[i] = isk[i] ? -pinv : ci * pinv;
+    const double f = sm.col[par][i * 32 + lane] * pinv;
+#pragma unroll
+    for (int j = 0; j < kInvCPW; ++j) a[i][j] = fma(-f, u[j], a[i][j]);
   }
+  if (lane == k % 32) {
+    const int slot = k / 32;
 #pragma unroll
-  for (int j = 0; j < kInvCPW; ++j) {
-    const double uj = (own && j == M) ? 1.0 : sm.rp[warp][j];
-    const double rkj = sm.rk[warp][j];
+    for (int q = 0; q < R; ++q)
+      if (q == slot) {
 #pragma unroll
-    for (int i = 0; i < R; ++i) {
-      const double base = isk[i] ? 0.0 : (isp[i] ? rkj : a[i][j]);
-      a[i][j] = fma(-f[i], uj, base);
-    }
+        for (int j = 0; j < kInvCPW; ++j) a[q][j] = u[j] * pinv;
+      }
+  }
+  if (p != k && lane == p % 32) {
+    const int slot = p / 32;
+    const double fk = sm.col[par][k] * pinv;
+#pragma unroll
+    for (int q = 0; q < R; ++q)
+      if (q == slot) {
+#pragma unroll
+        for (int j = 0; j < kInvCPW; ++j) a[q][j] = fma(-fk, u[j], sm.rk[warp][j]);
+      }
   }
   // the owner of column k + 1 finds the next pivot while the others finish
   const int k1 = k + 1;

@@ -74,15 +74,15 @@ struct Stage {
 };
 
 // Bytes of the FP64 accumulator snapshot: [TPT][3] (DUAL: twice) doubles per
-// thread (sized for TPT <= 2).
-template <int PREC, bool DUAL>
+// thread.
+template <int PREC, int TPT, bool DUAL>
 constexpr size_t snapshot_bytes() {
-  return PREC == F3D_FP64 ? static_cast<size_t>(2) * 3 * (DUAL ? 2 : 1) * 8 * kBlock : 0;
+  return PREC == F3D_FP64 ? static_cast<size_t>(TPT) * 3 * (DUAL ? 2 : 1) * 8 * kBlock : 0;
 }
 
-template <int KIND, int MODE, int PREC, bool DUAL = false>
+template <int KIND, int MODE, int PREC, int TPT, bool DUAL = false>
 constexpr size_t pair_smem_bytes() {
-  return 128 + 2 * Stage<KIND, MODE, PREC, DUAL>::bytes + snapshot_bytes<PREC, DUAL>();
+  return 128 + 2 * Stage<KIND, MODE, PREC, DUAL>::bytes + snapshot_bytes<PREC, TPT, DUAL>();
 }
 
 __device__ __forceinline__ void two_sum(float &s, float &c, float x) {
@@ -131,7 +131,8 @@ __device__ __forceinline__ f32x2 fma2(f32x2 a, f32x2 b, f32x2 c) {
 // into out and dens2 into out2, each with exactly the arithmetic of a single
 // sum -- the geometry (r, 1/r, 1/r^3) is computed once for both.
 template <int KIND, int MODE, int PREC, int TPT, int SL, bool DUAL = false>
-__global__ void __launch_bounds__(kBlock, (PREC == F3D_FP64 && !DUAL) ? ((TPT == 1) ? 7 : 5) : 1) pair_kernel(const PairArgs a) {
+__global__ void __launch_bounds__(kBlock, (PREC == F3D_FP64 && !DUAL) ? ((TPT == 1) ? 7 : (TPT == 2) ? 5 : 3) : 1)
+    pair_kernel(const PairArgs a) {
   static_assert(!DUAL || (PREC == F3D_FP64 && KIND == F3D_KERNEL_OSEEN), "dual sums: FP64 Oseen");
   using St = Stage<KIND, MODE, PREC, DUAL>;
   constexpr int TG = kBlock / SL;
@@ -697,7 +698,8 @@ static int make_plan(int kernel, int precision, int64_t ns, int64_t nt, const f3
   int sl = shape && shape->sl ? shape->sl : 0;
   if (sl == 0) sl = (nt >= 4096) ? 1 : (nt >= 512 ? 8 : 32);
   if (tpt == 0) tpt = 1;
-  if (!(tpt == 1 || tpt == 2)) return F3D_ERR_ARG;
+  if (!(tpt == 1 || tpt == 2 || tpt == 4)) return F3D_ERR_ARG;
+  if (tpt == 4 && (precision != F3D_FP64 || dual)) return F3D_ERR_ARG;  // four targets per thread: FP64 only
   if (!(sl == 1 || sl == 8 || sl == 32)) return F3D_ERR_ARG;
   if (sl != 1 && tpt != 1) return F3D_ERR_ARG;
   const int64_t tpb = static_cast<int64_t>(kBlock / sl) * tpt;
@@ -743,7 +745,7 @@ static int make_plan(int kernel, int precision, int64_t ns, int64_t nt, const f3
 
 template <int KIND, int MODE, int PREC, int TPT, int SL, bool DUAL = false>
 static int launch_one(const PairArgs &a, int64_t ntb, int nsplit, cudaStream_t st) {
-  constexpr size_t smem = pair_smem_bytes<KIND, MODE, PREC, DUAL>();
+  constexpr size_t smem = pair_smem_bytes<KIND, MODE, PREC, TPT, DUAL>();
   auto kfn = pair_kernel<KIND, MODE, PREC, TPT, SL, DUAL>;
   static bool attr_set[64] = {false};
   int dev = 0;
@@ -768,6 +770,9 @@ template <int KIND, int MODE, int PREC, bool DUAL = false>
 static int dispatch_shape(const PairArgs &a, const Plan &p, cudaStream_t st) {
   if (p.sl == 1 && p.tpt == 1) return launch_one<KIND, MODE, PREC, 1, 1, DUAL>(a, p.ntb, p.nsplit, st);
   if (p.sl == 1 && p.tpt == 2) return launch_one<KIND, MODE, PREC, 2, 1, DUAL>(a, p.ntb, p.nsplit, st);
+  if constexpr (PREC == F3D_FP64 && !DUAL) {
+    if (p.sl == 1 && p.tpt == 4) return launch_one<KIND, MODE, PREC, 4, 1, DUAL>(a, p.ntb, p.nsplit, st);
+  }
   if (p.sl == 8) return launch_one<KIND, MODE, PREC, 1, 8, DUAL>(a, p.ntb, p.nsplit, st);
   return launch_one<KIND, MODE, PREC, 1, 32, DUAL>(a, p.ntb, p.nsplit, st);
 }

@@ -81,7 +81,8 @@ def test_config1_golden(K, golden_config1):
 
 
 SHAPES = [(1, 1, 0, 0), (2, 1, 0, 0), (1, 8, 0, 0), (1, 32, 0, 0), (1, 1, 1, 0), (1, 1, 5, 0),
-          (1, 1, 3, -1), (2, 1, 0, -1), (1, 32, 7, -1), (1, 1, 19, -1), (2, 1, 38, -1)]
+          (1, 1, 3, -1), (2, 1, 0, -1), (1, 32, 7, -1), (1, 1, 19, -1), (2, 1, 38, -1), (4, 1, 0, 0),
+          (4, 1, 9, -1)]
 
 
 @pytest.mark.parametrize("shape", SHAPES)
