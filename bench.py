@@ -167,13 +167,13 @@ def measured_peak(L, precision: str, torch):
     st = L.stream_handle()
     prec = L.PRECISION[precision]
     for _ in range(2):
-        L.call("f3d_probe_fma", prec, 8192, L.ptr(sink), ctypes.byref(flops), st)
+        L.call("f3d_probe_fma", prec, 2000, L.ptr(sink), ctypes.byref(flops), st)
     torch.cuda.synchronize()
     best = 0.0
     for _ in range(5):
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
-        L.call("f3d_probe_fma", prec, 8192, L.ptr(sink), ctypes.byref(flops), st)
+        L.call("f3d_probe_fma", prec, 2000, L.ptr(sink), ctypes.byref(flops), st)
         e1.record()
         e1.synchronize()
         best = max(best, flops.value / (e0.elapsed_time(e1) * 1e-3))

@@ -1,10 +1,25 @@
 """fiber3d_b200 — the hydrodynamic hot path of fiber3d on one NVIDIA B200.
 
 Modules
-  kernels   drop-in replacement of fiber3d's ``kernels.kernels`` (same names
-            and signatures), running hand-written sm_100a CUDA through the C
-            ABI declared in include/fiber3d_b200.h
-  geometry  seeded synthetic geometry (Fibonacci sphere, fibers)
-  build     nvcc recipe for the in-tree shared library
+  kernels       drop-in replacement of fiber3d's ``kernels.kernels`` (all its
+                functions, same names and signatures), running hand-written
+                sm_100a CUDA through the C ABI of include/fiber3d_b200.h
+  _lib          ctypes binding of that C ABI, workspaces, the device error word
+  autotune      launch-shape tuner of the pair kernels (cached per GPU)
+  hydro         the time step's linear system on the device: RHS, matvec,
+                block preconditioner, advance, grid velocity
+  gmres         right-preconditioned restarted GMRES on the device, FP64 and
+                mixed precision with iterative refinement
+  blocklu       batched block factorisations / inverses of the fiber blocks
+  fibers        fiber resolutions (finite differences, barycentric matrices)
+  warmstart     GMRES initial guess: extrapolation + learned per-fiber correction
+  flowstart     the (positions, background velocity) -> (tensions, forces)
+                network form of the learned guess
+  quadrature    drop-in for fiber3d's RBF surface quadrature
+  output        fiber3d's output and restart files
+  tstep_bridge  solver-level drop-in for fiber3d's tstep (GMRES on the device)
+  geometry      seeded synthetic geometry (Fibonacci sphere, fibers, problems)
+  replicas      multi-process bookkeeping (barrier, max over ranks)
+  build         nvcc recipe for the in-tree shared library
 """
-__version__ = "0.1.0"
+__version__ = "0.2.0"

@@ -34,6 +34,7 @@
 // Blocks smaller than NMAX are padded with the identity, which the sweeps
 // leave untouched.
 #include <algorithm>
+#include <type_traits>
 
 #include "f3d_common.cuh"
 
@@ -72,13 +73,19 @@ __device__ __forceinline__ double reciprocal(double x) {
   return fma(y, fma(e, e, e), y);
 }
 
-// Row `i` (a runtime index < R) of this lane's tile, column j.
-template <int R>
-__device__ __forceinline__ double tile_at(const double (&a)[R][kInvCPW], int i, int j) {
-  double v = a[0][j];
-#pragma unroll
-  for (int q = 1; q < R; ++q) v = (i == q) ? a[q][j] : v;
-  return v;
+// Calls f(integral_constant<int, slot>) for a slot (< R) that is the same in
+// every lane of the warp: a uniform branch to a body whose register index is
+// a compile-time constant (no per-element selects, no local memory).
+template <int R, typename F>
+__device__ __forceinline__ void on_slot(int slot, F &&f) {
+  if (slot == 0) f(std::integral_constant<int, 0>{});
+  if constexpr (R > 1) {
+    if (slot == 1) f(std::integral_constant<int, 1>{});
+  }
+  if constexpr (R > 2) {
+    if (slot == 2) f(std::integral_constant<int, 2>{});
+    if (slot == 3) f(std::integral_constant<int, 3>{});
+  }
 }
 
 // Pivot search on column slot JJ of the owner warp for step k, and publication
@@ -139,15 +146,20 @@ __device__ __forceinline__ void inverse_step(double (&a)[InvShape<NMAX>::kRPL][k
 #pragma unroll
     for (int i = 0; i < R; ++i) a[i][M] = 0.0;
   }
-  // rows k and p of this warp's columns, through the per-warp buffer
-  if (lane == k % 32) {
+  // rows k and p of this warp's columns, through the per-warp buffer (the
+  // tile slot of a row, row / 32, is the same in every lane)
+  on_slot<R>(k / 32, [&](auto q) {
+    if (lane == k % 32) {
 #pragma unroll
-    for (int j = 0; j < kInvCPW; ++j) sm.rk[warp][j] = tile_at<R>(a, k / 32, j);
-  }
-  if (lane == p % 32) {
+      for (int j = 0; j < kInvCPW; ++j) sm.rk[warp][j] = a[decltype(q)::value][j];
+    }
+  });
+  on_slot<R>(p / 32, [&](auto q) {
+    if (lane == p % 32) {
 #pragma unroll
-    for (int j = 0; j < kInvCPW; ++j) sm.rp[warp][j] = tile_at<R>(a, p / 32, j);
-  }
+      for (int j = 0; j < kInvCPW; ++j) sm.rp[warp][j] = a[decltype(q)::value][j];
+    }
+  });
   __syncwarp();
   // One FMA per element on every row: a_ij <- a_ij - (a_ik / a_pk) u_j with
   // u = old row p (u_k = 1 in the owner's column k).  On row k this gives
@@ -165,24 +177,20 @@ __device__ __forceinline__ void inverse_step(double (&a)[InvShape<NMAX>::kRPL][k
 #pragma unroll
     for (int j = 0; j < kInvCPW; ++j) a[i][j] = fma(-f, u[j], a[i][j]);
   }
-  if (lane == k % 32) {
-    const int slot = k / 32;
+  on_slot<R>(k / 32, [&](auto q) {
+    if (lane == k % 32) {
 #pragma unroll
-    for (int q = 0; q < R; ++q)
-      if (q == slot) {
-#pragma unroll
-        for (int j = 0; j < kInvCPW; ++j) a[q][j] = u[j] * pinv;
-      }
-  }
-  if (p != k && lane == p % 32) {
-    const int slot = p / 32;
+      for (int j = 0; j < kInvCPW; ++j) a[decltype(q)::value][j] = u[j] * pinv;
+    }
+  });
+  if (p != k) {
     const double fk = sm.col[par][k] * pinv;
+    on_slot<R>(p / 32, [&](auto q) {
+      if (lane == p % 32) {
 #pragma unroll
-    for (int q = 0; q < R; ++q)
-      if (q == slot) {
-#pragma unroll
-        for (int j = 0; j < kInvCPW; ++j) a[q][j] = fma(-fk, u[j], sm.rk[warp][j]);
+        for (int j = 0; j < kInvCPW; ++j) a[decltype(q)::value][j] = fma(-fk, u[j], sm.rk[warp][j]);
       }
+    });
   }
   // the owner of column k + 1 finds the next pivot while the others finish
   const int k1 = k + 1;

@@ -16,11 +16,13 @@
 //
 // Decomposition: tiles of 128 points; one CTA per tile pair (I, J), I <= J.
 // Thread t holds target i = 128 I + t and its partial sum in registers; tile
-// J's sources are staged in shared memory and every thread of a warp meets
-// the same source together (broadcast loads).  The target-side terms of four
-// consecutive sources are summed over the warp with a reduce-scatter of
-// shuffles (18 shuffles and adds per four sources), then over the CTA's
-// four warps in shared memory.  Each CTA writes two partials: tile I's
+// J's sources are staged in shared memory (one array per component).  A warp
+// meets the sources of tile J 32 at a time, rotating: at step s lane l pairs
+// its target with source (l + s) mod 32 of the group, whose position and
+// running source-side sum it holds in registers and hands to lane l - 1
+// after the step (six shuffles per step), its density and normal read from
+// shared memory.  After 32 steps lane l holds source l's sum over the warp's
+// targets; the CTA's four warps' sums are added in shared memory.  Each CTA writes two partials: tile I's
 // (slot J) and tile J's (slot I); a diagonal CTA (I == J) evaluates its tile
 // from the target side only and writes slot I.  Each tile thus receives
 // exactly T partials (T = number of tiles); the CTA that delivers the last
@@ -64,9 +66,11 @@ bool sym_fits(int64_t n) { return (n + kSymTile - 1) / kSymTile <= kSymMaxTiles;
 template <int KIND, int MODE>
 __global__ void __launch_bounds__(kSymTile) pair_sym_kernel(const SymArgs a) {
   constexpr bool kNrm = (KIND == F3D_KERNEL_STRESSLET);
-  __shared__ __align__(16) double s_pos[3 * kSymTile];
-  __shared__ __align__(16) double s_den[3 * kSymTile];
-  __shared__ __align__(16) double s_nrm[kNrm ? 3 * kSymTile : 1];
+  // sources of tile J, one array per component (conflict-free when the
+  // lanes of a warp read different sources)
+  __shared__ __align__(16) double s_x[3][kSymTile];
+  __shared__ __align__(16) double s_d[3][kSymTile];
+  __shared__ __align__(16) double s_n[kNrm ? 3 : 1][kSymTile];
   __shared__ int32_t s_grp[kSymTile];
   __shared__ __align__(16) double s_accj[kSymTile / 32][kSymTile][3];
   __shared__ int s_flags;
@@ -96,13 +100,18 @@ __global__ void __launch_bounds__(kSymTile) pair_sym_kernel(const SymArgs a) {
   // tile J's sources
   const int64_t j0 = static_cast<int64_t>(J) * kSymTile;
   const int cnt = static_cast<int>(min(static_cast<int64_t>(kSymTile), a.n - j0));
-  for (int q = tid; q < 3 * cnt; q += kSymTile) {
-    s_pos[q] = a.x[3 * j0 + q];
-    s_den[q] = a.dens[3 * j0 + q];
-    if (kNrm) s_nrm[q] = a.nrm[3 * j0 + q];
+  {
+    // past the end: far away, zero density and normal (their terms vanish)
+    const bool sv = tid < cnt;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      s_x[c][tid] = sv ? a.x[3 * (j0 + tid) + c] : 1e30;
+      s_d[c][tid] = sv ? a.dens[3 * (j0 + tid) + c] : 0.0;
+      if (kNrm) s_n[c][tid] = sv ? a.nrm[3 * (j0 + tid) + c] : 0.0;
+    }
   }
   if (MODE == F3D_SELF_SKIP_GROUP)
-    for (int q = tid; q < cnt; q += kSymTile) s_grp[q] = a.grp[j0 + q];
+    s_grp[tid] = tid < cnt ? a.grp[j0 + tid] : INT32_MIN;
   __syncthreads();
 
   const long long eps2_bits = __double_as_longlong(a.eps2);
@@ -113,13 +122,13 @@ __global__ void __launch_bounds__(kSymTile) pair_sym_kernel(const SymArgs a) {
   if (I == J) {
     // one tile: every ordered pair from the target's side, with the rules
     for (int s = 0; s < cnt; ++s) {
-      const double dx = xi0 - s_pos[3 * s], dy = xi1 - s_pos[3 * s + 1], dz = xi2 - s_pos[3 * s + 2];
+      const double dx = xi0 - s_x[0][s], dy = xi1 - s_x[1][s], dz = xi2 - s_x[2][s];
       double r2 = fma(dx, dx, fma(dy, dy, dz * dz));
       bool skip = (s == tid);
       if (MODE == F3D_SELF_SKIP_GROUP) skip = skip || (s_grp[s] == gi);
       const bool close = !skip && (__double_as_longlong(r2) < eps2_bits);
       r2 = regularise(r2, close, reg2);
-      const double d0 = s_den[3 * s], d1 = s_den[3 * s + 1], d2 = s_den[3 * s + 2];
+      const double d0 = s_d[0][s], d1 = s_d[1][s], d2 = s_d[2][s];
       if (KIND == F3D_KERNEL_OSEEN) {
         double ri = rsqrt_refined(r2);
         ri = skip ? 0.0 : ri;
@@ -129,7 +138,7 @@ __global__ void __launch_bounds__(kSymTile) pair_sym_kernel(const SymArgs a) {
         acc2 = fma(g, dz, fma(ri, d2, acc2));
       } else {
         const double rd = fma(dx, d0, fma(dy, d1, dz * d2));
-        const double rn = fma(dx, s_nrm[3 * s], fma(dy, s_nrm[3 * s + 1], dz * s_nrm[3 * s + 2]));
+        const double rn = fma(dx, s_n[0][s], fma(dy, s_n[1][s], dz * s_n[2][s]));
         double f = times_rsqrt5(rd * rn, r2);
         f = skip ? 0.0 : f;
         acc0 = fma(f, dx, acc0);
@@ -170,81 +179,63 @@ __global__ void __launch_bounds__(kSymTile) pair_sym_kernel(const SymArgs a) {
       const bool rules = (pass == 1);
       acc0 = acc1 = acc2 = 0.0;
       int hmin = INT32_MAX;
-      for (int s0 = 0; s0 < cnt; s0 += 4) {
-        double c[4][3];
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-          c[q][0] = c[q][1] = c[q][2] = 0.0;
-          const int s = s0 + q;
-          if (s < cnt) {
-            const double dx = xi0 - s_pos[3 * s], dy = xi1 - s_pos[3 * s + 1], dz = xi2 - s_pos[3 * s + 2];
-            double r2 = fma(dx, dx, fma(dy, dy, dz * dz));
-            bool skip = !iv;
-            if (rules) {
-              if (MODE == F3D_SELF_SKIP_GROUP) skip = skip || (s_grp[s] == gi);
-              if (!skip && __double_as_longlong(r2) < eps2_bits) r2 += reg2;
-            } else if (iv) {
-              hmin = min(hmin, __double2hiint(r2));
-            }
-            const double d0 = s_den[3 * s], d1 = s_den[3 * s + 1], d2 = s_den[3 * s + 2];
-            if (KIND == F3D_KERNEL_OSEEN) {
-              double ri = rsqrt_refined(r2);
-              ri = skip ? 0.0 : ri;
-              const double ri3 = ri * ri * ri;
-              const double g = ri3 * fma(dx, d0, fma(dy, d1, dz * d2));
-              const double h = ri3 * fma(dx, di0, fma(dy, di1, dz * di2));
-              acc0 = fma(g, dx, fma(ri, d0, acc0));
-              acc1 = fma(g, dy, fma(ri, d1, acc1));
-              acc2 = fma(g, dz, fma(ri, d2, acc2));
-              c[q][0] = fma(h, dx, ri * di0);
-              c[q][1] = fma(h, dy, ri * di1);
-              c[q][2] = fma(h, dz, ri * di2);
-            } else {
-              double R5 = rsqrt5(r2);
-              R5 = skip ? 0.0 : R5;
-              const double n0 = s_nrm[3 * s], n1 = s_nrm[3 * s + 1], n2 = s_nrm[3 * s + 2];
-              const double f = (fma(dx, d0, fma(dy, d1, dz * d2)) * fma(dx, n0, fma(dy, n1, dz * n2))) * R5;
-              const double h = -(fma(dx, di0, fma(dy, di1, dz * di2)) * fma(dx, ni0, fma(dy, ni1, dz * ni2))) * R5;
-              acc0 = fma(f, dx, acc0);
-              acc1 = fma(f, dy, acc1);
-              acc2 = fma(f, dz, acc2);
-              c[q][0] = h * dx;
-              c[q][1] = h * dy;
-              c[q][2] = h * dz;
-            }
+      for (int sb = 0; sb < cnt; sb += 32) {
+        // the group's source at this lane: position and source-side sum rotate
+        int m = lane;
+        double px = s_x[0][sb + m], py = s_x[1][sb + m], pz = s_x[2][sb + m];
+        double aj0 = 0.0, aj1 = 0.0, aj2 = 0.0;
+        for (int st = 0; st < 32; ++st) {
+          const int js = sb + m;
+          const double dx = xi0 - px, dy = xi1 - py, dz = xi2 - pz;
+          double r2 = fma(dx, dx, fma(dy, dy, dz * dz));
+          bool skip = !iv;
+          if (rules) {
+            if (MODE == F3D_SELF_SKIP_GROUP) skip = skip || (s_grp[js] == gi);
+            if (!skip && __double_as_longlong(r2) < eps2_bits) r2 += reg2;
+          } else if (iv) {
+            hmin = min(hmin, __double2hiint(r2));
           }
+          const double d0 = s_d[0][js], d1 = s_d[1][js], d2 = s_d[2][js];
+          if (KIND == F3D_KERNEL_OSEEN) {
+            double ri = rsqrt_refined(r2);
+            ri = skip ? 0.0 : ri;
+            const double ri3 = ri * ri * ri;
+            const double g = ri3 * fma(dx, d0, fma(dy, d1, dz * d2));
+            const double h = ri3 * fma(dx, di0, fma(dy, di1, dz * di2));
+            acc0 = fma(g, dx, fma(ri, d0, acc0));
+            acc1 = fma(g, dy, fma(ri, d1, acc1));
+            acc2 = fma(g, dz, fma(ri, d2, acc2));
+            aj0 = fma(h, dx, fma(ri, di0, aj0));
+            aj1 = fma(h, dy, fma(ri, di1, aj1));
+            aj2 = fma(h, dz, fma(ri, di2, aj2));
+          } else {
+            double R5 = rsqrt5(r2);
+            R5 = skip ? 0.0 : R5;
+            const double n0 = s_n[0][js], n1 = s_n[1][js], n2 = s_n[2][js];
+            const double f = (fma(dx, d0, fma(dy, d1, dz * d2)) * fma(dx, n0, fma(dy, n1, dz * n2))) * R5;
+            const double h = (fma(dx, di0, fma(dy, di1, dz * di2)) * fma(dx, ni0, fma(dy, ni1, dz * ni2))) * R5;
+            acc0 = fma(f, dx, acc0);
+            acc1 = fma(f, dy, acc1);
+            acc2 = fma(f, dz, acc2);
+            aj0 = fma(-h, dx, aj0);
+            aj1 = fma(-h, dy, aj1);
+            aj2 = fma(-h, dz, aj2);
+          }
+          // hand the source (position and its running sum) to lane - 1
+          const int from = (lane + 1) & 31;
+          px = __shfl_sync(0xffffffffu, px, from);
+          py = __shfl_sync(0xffffffffu, py, from);
+          pz = __shfl_sync(0xffffffffu, pz, from);
+          aj0 = __shfl_sync(0xffffffffu, aj0, from);
+          aj1 = __shfl_sync(0xffffffffu, aj1, from);
+          aj2 = __shfl_sync(0xffffffffu, aj2, from);
+          m = (m + 1) & 31;
         }
-        // warp sums of the four sources' terms: reduce-scatter by halves
-        // (lane bit 4 keeps sources {0,1} or {2,3}, bit 3 one of those),
-        // then a butterfly over lane bits 2..0
-        const bool b4 = (lane & 16) != 0, b3 = (lane & 8) != 0;
-        double k1[2][3];
-#pragma unroll
-        for (int v = 0; v < 2; ++v)
-#pragma unroll
-          for (int m = 0; m < 3; ++m) {
-            const double keep = b4 ? c[2 + v][m] : c[v][m];
-            const double send = b4 ? c[v][m] : c[2 + v][m];
-            k1[v][m] = keep + __shfl_xor_sync(0xffffffffu, send, 16);
-          }
-        double k2[3];
-#pragma unroll
-        for (int m = 0; m < 3; ++m) {
-          const double keep = b3 ? k1[1][m] : k1[0][m];
-          const double send = b3 ? k1[0][m] : k1[1][m];
-          k2[m] = keep + __shfl_xor_sync(0xffffffffu, send, 8);
-        }
-#pragma unroll
-        for (int off = 4; off > 0; off >>= 1)
-#pragma unroll
-          for (int m = 0; m < 3; ++m) k2[m] += __shfl_xor_sync(0xffffffffu, k2[m], off);
-        if ((lane & 7) == 0) {
-          const int s = s0 + (b4 ? 2 : 0) + (b3 ? 1 : 0);
-          if (s < cnt) {
-            s_accj[warp][s][0] = k2[0];
-            s_accj[warp][s][1] = k2[1];
-            s_accj[warp][s][2] = k2[2];
-          }
+        // after a full turn lane l holds source sb + l again
+        if (sb + lane < cnt) {
+          s_accj[warp][sb + lane][0] = aj0;
+          s_accj[warp][sb + lane][1] = aj1;
+          s_accj[warp][sb + lane][2] = aj2;
         }
       }
       // a pair within eps met by the plain pass: redo with the rules

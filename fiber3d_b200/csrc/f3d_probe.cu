@@ -1,6 +1,6 @@
 // Throughput probes used as measured roofline denominators: FP64 / FP32
 // fused multiply-add rate of this GPU.  Each thread runs 8 independent FMA
-// chains, 32 FMAs per loop trip, so the pipes, not the dependency latency or
+// chains, 192 FMAs per loop trip, so the pipes, not the dependency latency or
 // the loop overhead, set the rate; the caller gives it enough iterations
 // (about 2 ms) that the launch ramp does not count.
 #include "f3d_common.cuh"
@@ -14,7 +14,7 @@ __global__ void fma_probe_kernel(T *out, int iters, T a, T b) {
   for (int k = 0; k < 8; ++k) c[k] = static_cast<T>(threadIdx.x + k);
   for (int i = 0; i < iters; ++i) {
 #pragma unroll
-    for (int u = 0; u < 4; ++u)
+    for (int u = 0; u < 24; ++u)
 #pragma unroll
       for (int k = 0; k < 8; ++k) c[k] = c[k] * a + b;
   }
@@ -41,7 +41,7 @@ int f3d_probe_fma(int precision, int iters, double *sink, double *flops, void *s
   } else {
     return F3D_ERR_ARG;
   }
-  *flops = 2.0 * 32.0 * static_cast<double>(iters) * blocks * threads;
+  *flops = 2.0 * 192.0 * static_cast<double>(iters) * blocks * threads;
   return f3d::launch_status();
 }
 

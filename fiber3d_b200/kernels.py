@@ -144,6 +144,7 @@ def pair_sum(kernel: str, r_source, r_target, density, normal=None, *, eta=1.0, 
 
 
 _ws_bytes: dict = {}
+_tuned: dict = {}  # host fast path: (device, sum, sizes, one point set) -> tuned launch shape
 
 
 def _launch(dev, k: int, p: int, m: int, rs, rt, d, n, gs, gt, out, eta: float, reg: float, eps: float,
@@ -234,10 +235,15 @@ def _drop_in(kernel, r_source, r_target, density, normal, self_mode, eta, reg, e
     dev = _device()
     if host and not any(isinstance(x, torch.Tensor) and x.is_cuda for x in (r_source, r_target, density, normal)):
         if shape is None and AUTOTUNE:
-            from . import autotune
             size = lambda a: a.numel() if isinstance(a, torch.Tensor) else np.size(a)
-            shp = autotune.cached(kernel, precision, self_mode, size(r_source) // 3, size(r_target) // 3,
-                                  same=r_target is r_source)
+            key = (dev.index, kernel, precision, self_mode, size(r_source) // 3, size(r_target) // 3,
+                   r_target is r_source)
+            shp = _tuned.get(key)
+            if shp is None:
+                from . import autotune
+                shp = autotune.cached(kernel, precision, self_mode, key[4], key[5], same=key[6])
+                if shp is not None:
+                    _tuned[key] = shp
             if shp is not None:
                 return _drop_in_host(kernel, r_source, r_target, density, normal, self_mode, eta, reg,
                                      epsilon_distance, precision, shp, dev)

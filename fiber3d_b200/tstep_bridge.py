@@ -16,10 +16,12 @@ The periphery preconditioner is built once per periphery and reused.
 fiber3d starts GMRES from zero (tstep.py:1209).  With
 ``warm_start="extrapolate"`` the solver keeps the last three solutions of
 its own calls and starts from their quadratic extrapolation
-(``warmstart.extrapolate``); GMRES still runs to fiber3d's tolerance, so a
-history that does not match the step (a rejected step, a changed system)
-costs iterations, never accuracy.  The history is dropped whenever the
-system size changes.
+(``warmstart.extrapolate``); with ``warm_start="learned"`` and a trained
+``warmstart.LearnedWarmStart`` as ``model``, from that extrapolation
+corrected per fiber by the network once four solutions are known.  GMRES
+still runs to fiber3d's tolerance, so a history that does not match the
+step (a rejected step, a changed system) costs iterations, never accuracy.
+The history is dropped whenever the system size changes.
 """
 from __future__ import annotations
 
@@ -55,10 +57,14 @@ def problem_from_tstep(ts) -> Problem:
 class GpuGmres:
     """Callable with the signature fiber3d uses for ``gmres.gmres``."""
 
-    def __init__(self, ts, mixed: bool = False, restart: int = 100, warm_start: str | None = None):
-        if warm_start not in (None, "extrapolate"):
-            raise ValueError("warm_start must be None or 'extrapolate'")
+    def __init__(self, ts, mixed: bool = False, restart: int = 100, warm_start: str | None = None,
+                 model=None):
+        if warm_start not in (None, "extrapolate", "learned"):
+            raise ValueError("warm_start must be None, 'extrapolate' or 'learned'")
+        if warm_start == "learned" and model is None:
+            raise ValueError("warm_start='learned' needs a trained warmstart.LearnedWarmStart as model")
         self.ts = ts
+        self.model = model
         self.mixed = mixed
         self.restart = restart
         self.warm_start = warm_start
@@ -80,12 +86,14 @@ class GpuGmres:
             if self._history and self._history[-1].numel() != sysd.size:
                 self._history = []
             if self._history:
-                from .warmstart import extrapolate
-                x0 = extrapolate(self._history)
+                from .warmstart import extrapolate, learned_guess
+                x0 = (learned_guess(sysd, self._history, self.model) if self.warm_start == "learned"
+                      else extrapolate(self._history))
         res = sysd.solve(tol=tol, restart=min(restart or self.restart, 255), maxiter=maxiter or 200,
                          mixed=self.mixed, x0=x0)
         if self.warm_start is not None:
-            self._history = (self._history + [res["x"]])[-3:]
+            from .warmstart import HISTORY
+            self._history = (self._history + [res["x"]])[-HISTORY:]
         if callback is not None:
             for h in res["history"][1:]:
                 callback(h)
@@ -93,10 +101,10 @@ class GpuGmres:
         return res["x"].cpu().numpy(), int(res["info"])
 
 
-def install(ts, mixed: bool = False, warm_start: str | None = None):
+def install(ts, mixed: bool = False, warm_start: str | None = None, model=None):
     """Route fiber3d's GMRES call through the GPU solver for time stepper `ts`."""
     import importlib
     gm = importlib.import_module("bpm_utilities.gmres")
-    solver = GpuGmres(ts, mixed=mixed, warm_start=warm_start)
+    solver = GpuGmres(ts, mixed=mixed, warm_start=warm_start, model=model)
     gm.gmres = solver
     return solver

@@ -69,3 +69,18 @@ def test_bridge_warm_start(mixed):
     assert rel_err(x2, g["sol"]) < 1e-7
     with pytest.raises(ValueError):
         GpuGmres(fake_tstep(g), warm_start="learned")
+
+
+def test_bridge_learned_warm_start():
+    """warm_start="learned" takes a LearnedWarmStart; on systems it does not
+    apply to (fibers of other resolutions) it is the extrapolation, and the
+    answer meets fiber3d's tolerance either way."""
+    from fiber3d_b200.tstep_bridge import GpuGmres
+    from fiber3d_b200.warmstart import LearnedWarmStart
+    g = load_golden("step_small.npz")
+    solver = GpuGmres(fake_tstep(g), mixed=True, warm_start="learned", model=LearnedWarmStart(seed=0))
+    tol = float(g["tol"])
+    for _ in range(5):
+        x, info = solver(None, g["rhs"], tol=tol)
+        assert info == 0 and rel_err(x, g["sol"]) < 1e-7
+    assert len(solver._history) == 4
