@@ -91,6 +91,7 @@ SIGNATURES: dict[str, list] = {
     "f3d_singularity_vectors_workspace_bytes": [_I64, ctypes.POINTER(_SZ)],
     "f3d_singularity_vectors": [_P, _P, _P, _P, _I64, _D, _D, _D, _P, _SZ, _P],
     "f3d_shell_residual": [_P, _P, _P, _P, _P, _P, _I64, _P, _P],
+    "f3d_block3_gemv": [_P, _P, _P, _I64, _P],
     "f3d_body_residual": [ctypes.c_int32, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P],
     "f3d_surface_dense": [_I, _P, _P, _P, _P, _P, _P, _I64, _I64, _D, _D, _D, _P],
     "f3d_rotate_blocks": [_P, _P, _P, _P, ctypes.c_int32, _I, _P],

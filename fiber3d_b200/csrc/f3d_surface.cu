@@ -57,6 +57,18 @@ __global__ void __launch_bounds__(1024) normal_dot_kernel(const double *nrm, con
   }
 }
 
+// y_i = B_i x_i for n row-major 3 x 3 blocks B (9 doubles per node).
+__global__ void block3_gemv_kernel(const double *__restrict__ B, const double *__restrict__ x, double *y,
+                                   int64_t n) {
+  const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double *b = B + 9 * i;
+  const double x0 = x[3 * i], x1 = x[3 * i + 1], x2 = x[3 * i + 2];
+  y[3 * i] = fma(b[0], x0, fma(b[1], x1, b[2] * x2));
+  y[3 * i + 1] = fma(b[3], x0, fma(b[4], x1, b[5] * x2));
+  y[3 * i + 2] = fma(b[6], x0, fma(b[7], x1, b[8] * x2));
+}
+
 // res_i = v_i - E_i mu_i - mu_i + n_i s   (mu = q / w)
 __global__ void shell_residual_kernel(const double *__restrict__ v, const double *__restrict__ E,
                                       const double *__restrict__ w, const double *__restrict__ nrm,
@@ -407,6 +419,16 @@ int f3d_shell_residual(const double *v, const double *E, const double *weights,
   if (rc) return rc;
   f3d::shell_residual_kernel<<<static_cast<unsigned>((n + 255) / 256), 256, 0, st>>>(
       v, E, weights, normals, q, scratch, res, n);
+  return f3d::launch_status();
+}
+
+int f3d_block3_gemv(const double *B, const double *x, double *y, int64_t n, void *stream) {
+  if (n < 0) return F3D_ERR_SHAPE;
+  if (n == 0) return F3D_OK;
+  if (!B || !x || !y) return F3D_ERR_NULL;
+  if (x == y) return F3D_ERR_ARG;
+  f3d::block3_gemv_kernel<<<static_cast<unsigned>((n + 255) / 256), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+      B, x, y, n);
   return f3d::launch_status();
 }
 

@@ -154,11 +154,22 @@ class PhaseTimers:
 
 class ShellOperator:
     """Device data of a periphery: nodes, normals, weights, singularity
-    vectors E and the explicit inverse of the dense shell operator (FP64, and
-    an FP32 copy for mixed precision).  Built once per periphery."""
+    vectors E and its preconditioner, built once per periphery.
+
+    pc="dense" (fiber3d's choice, the LU of the dense shell operator,
+    tstep.py:327-348): the explicit inverse of that operator in FP64, with
+    FP32 and row-scaled FP16 copies for the inner solves of mixed precision;
+    O(N^2) memory (10.4 + 5.2 + 2.6 GB at 12000 nodes).
+    pc="block": the inverses of its 3 x 3 diagonal blocks,
+    B_i = -(E_i + I) / w_i + n_i n_i^T (the double layer's own diagonal block
+    is zero), O(N) memory and no factorisation; GMRES then resolves the
+    periphery's nonlocal coupling itself (more iterations, same answer)."""
 
     def __init__(self, shell: Shell, eta=1.0, reg=5e-3, eps_dist=1e-5, device=None,
-                 build_inverse=True):
+                 build_inverse=True, pc: str = "dense"):
+        if pc not in ("dense", "block"):
+            raise ValueError("pc must be 'dense' or 'block'")
+        self.pc = pc
         dev = device or torch.device("cuda", torch.cuda.current_device())
         self.device = dev
         t = lambda a: torch.as_tensor(np.ascontiguousarray(a, dtype=np.float64), device=dev)
@@ -171,8 +182,19 @@ class ShellOperator:
         self.inv64 = None
         self.inv32 = None
         self.inv16 = None
-        if build_inverse:
+        self.block_inv = None
+        if pc == "block":
+            self.build_block_inverse()
+        elif build_inverse:
             self.build_inverse()
+
+    def build_block_inverse(self):
+        """Inverses of the dense operator's 3 x 3 diagonal blocks (set-up, host)."""
+        E = self.E.cpu().numpy().reshape(-1, 3, 3)
+        w = self.weights.cpu().numpy()
+        nr = self.normals.cpu().numpy()
+        B = -(E + np.eye(3)) / w[:, None, None] + nr[:, :, None] * nr[:, None, :]
+        self.block_inv = torch.as_tensor(np.linalg.inv(B).reshape(-1, 9), device=self.device).contiguous()
 
     def dense(self) -> torch.Tensor:
         m = 3 * self.n
@@ -202,9 +224,13 @@ class ShellOperator:
                   _lib.ptr(self.scale16), _lib.ptr(self.diag16), _lib.stream_handle(self.device))
 
     def apply(self, x: torch.Tensor, y: torch.Tensor, storage: str = "fp64") -> torch.Tensor:
-        """y = P_shell^-1 x from the FP64, FP32 or FP16 copy of the inverse."""
+        """y = P_shell^-1 x from the FP64, FP32 or FP16 copy of the inverse
+        (pc="block": the 3 x 3 block inverses, in FP64 whatever `storage`)."""
         m = 3 * self.n
         st = _lib.stream_handle(self.device)
+        if self.pc == "block":
+            _lib.call("f3d_block3_gemv", _lib.ptr(self.block_inv), _lib.ptr(x), _lib.ptr(y), self.n, st)
+            return y
         if storage == "fp16":
             _lib.call("f3d_gemv_f16", _lib.ptr(self.inv16), m, _lib.ptr(self.scale16), _lib.ptr(self.diag16), 3,
                       _lib.ptr(x), _lib.ptr(y), m, m, st)
@@ -273,7 +299,7 @@ class HydroSystem:
 
     def __init__(self, problem: Problem, shell_op: ShellOperator | None = None, device=None,
                  tune: bool = False, fiber_pc: str = "auto", inner_shell_pc: str = "fp16",
-                 pc_refresh: int | str = 1):
+                 pc_refresh: int | str = 1, shell_pc: str = "dense"):
         self.p = problem
         dev = device or torch.device("cuda", torch.cuda.current_device())
         self.device = dev
@@ -303,7 +329,7 @@ class HydroSystem:
         self.body_ref_n = [np.asarray(b.ref_normals, dtype=np.float64).reshape(-1, 3) for b in P.bodies]
         # ---- shell
         if P.shell is not None:
-            self.shell = shell_op or ShellOperator(P.shell, P.eta, P.reg, P.eps_dist, dev)
+            self.shell = shell_op or ShellOperator(P.shell, P.eta, P.reg, P.eps_dist, dev, pc=shell_pc)
             nS = self.shell.n
         else:
             self.shell = None

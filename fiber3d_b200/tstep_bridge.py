@@ -58,7 +58,7 @@ class GpuGmres:
     """Callable with the signature fiber3d uses for ``gmres.gmres``."""
 
     def __init__(self, ts, mixed: bool = False, restart: int = 100, warm_start: str | None = None,
-                 model=None):
+                 model=None, shell_pc: str = "dense"):
         if warm_start not in (None, "extrapolate", "learned"):
             raise ValueError("warm_start must be None, 'extrapolate' or 'learned'")
         if warm_start == "learned" and model is None:
@@ -68,6 +68,7 @@ class GpuGmres:
         self.mixed = mixed
         self.restart = restart
         self.warm_start = warm_start
+        self.shell_pc = shell_pc
         self._history = []
         self._shell = None
         self.last = None
@@ -76,7 +77,7 @@ class GpuGmres:
                  callback=None, **kw):
         P = problem_from_tstep(self.ts)
         if P.shell is not None and self._shell is None:
-            self._shell = ShellOperator(P.shell, P.eta, P.reg, P.eps_dist)
+            self._shell = ShellOperator(P.shell, P.eta, P.reg, P.eps_dist, pc=self.shell_pc)
         sysd = HydroSystem(P, shell_op=self._shell)
         if sysd.size != np.size(b):
             raise ValueError(f"system size {sysd.size} != len(b) {np.size(b)}")

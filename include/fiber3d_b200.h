@@ -417,6 +417,13 @@ int f3d_shell_residual(const double *v, const double *E, const double *weights,
                        const double *normals, const double *q, double *res, int64_t n,
                        double *scratch, void *stream);
 
+/* y_i = B_i x_i for n row-major 3 x 3 blocks (B: 9n doubles; x, y: 3n,
+   distinct).  Applies the block-diagonal (node-local) periphery
+   preconditioner, the inverses of the 3 x 3 diagonal blocks of the dense
+   shell operator of tstep/tstep.py:327-347: a matrix-free alternative to
+   its LU (tstep.py:348) for peripheries whose dense inverse does not fit. */
+int f3d_block3_gemv(const double *B, const double *x, double *y, int64_t n, void *stream);
+
 /* Rigid-body rows of the matvec (tstep/tstep.py:1118-1143): for body b with
    unknowns x[x_off[b]..] = [lambda (3nb), U, Omega]:
    res = v - E mu - (U + Omega x r) on the nodes and -K^T lambda + (U, Omega). */

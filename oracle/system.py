@@ -365,6 +365,15 @@ class HydroSystem:
         r = self.shell_apply(np.asarray(y_shell)) - np.asarray(x_shell)
         return float(np.linalg.norm(r) / np.linalg.norm(x_shell))
 
+    def shell_block_pc(self, x_shell):
+        """Block-Jacobi alternative to the shell LU: each node's 3 x 3 diagonal
+        block of the dense operator of tstep.py:327-347 (the double layer
+        skips i == j, so the block is -(E_i + I) / w_i + n_i n_i^T) solved
+        on its own."""
+        s = self.shell
+        B = -(self.E_shell + np.eye(3)) / s.weights[:, None, None] + s.normals[:, :, None] * s.normals[:, None, :]
+        return np.linalg.solve(B, np.asarray(x_shell).reshape(-1, 3, 1)).reshape(-1)
+
     def pc(self, x):
         """P_inv (tstep.py:950-994).  Without the dense shell the shell block
         of the result is NaN (use shell_pc_residual for it)."""

@@ -176,3 +176,14 @@ def test_symmetric_shape_plan_checks(dll):
     assert dll.f3d_pair_workspace_bytes(2, 0, 1000, 1000, ctypes.byref(shp), ctypes.byref(nb)) == 5   # rotlet
     assert dll.f3d_pair_workspace_bytes(0, 0, 192 * 128 + 1, 192 * 128 + 1, ctypes.byref(shp),
                                         ctypes.byref(nb)) == 10
+
+
+def test_block3_gemv_argument_checks(dll):
+    """The block-Jacobi periphery preconditioner's entry checks its sizes,
+    pointers and aliasing before any launch."""
+    NULL, SHAPE, ARG = 1, 2, 5
+    p, q = ctypes.c_void_p(256), ctypes.c_void_p(512)
+    assert dll.f3d_block3_gemv(None, None, None, 0, None) == 0
+    assert dll.f3d_block3_gemv(p, p, q, -1, None) == SHAPE
+    assert dll.f3d_block3_gemv(None, p, q, 4, None) == NULL
+    assert dll.f3d_block3_gemv(p, q, q, 4, None) == ARG

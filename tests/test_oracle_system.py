@@ -77,3 +77,16 @@ def test_reference_grid():
     g = geometry.ellipsoid_grid()
     assert g.shape[0] == int(gg["grid_count"])
     assert np.array_equal(g[gg["grid_index"]], gg["grid_points"])
+
+
+def test_shell_block_pc_is_the_dense_operators_diagonal(step):
+    """The block-Jacobi periphery preconditioner inverts exactly the 3 x 3
+    diagonal blocks of the dense shell operator (pinned above through the
+    preconditioner probes)."""
+    _, sys_ = step
+    M = sys_.M_shell
+    n = sys_.nshell
+    x = np.random.default_rng(0).normal(size=3 * n)
+    ref = np.concatenate([np.linalg.solve(M[3 * i:3 * i + 3, 3 * i:3 * i + 3], x[3 * i:3 * i + 3])
+                          for i in range(n)])
+    assert rel_err(sys_.shell_block_pc(x), ref) < 1e-13
