@@ -197,16 +197,19 @@ def gpu_arm(args, rank, world, local):
     out = torch.empty(trg.numel(), dtype=torch.float64, device=dev)
     flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=dev)
 
-    # one launch: targets = [nodes; ball points], sources = nodes, the pair
-    # j == i skipped through group ids (node index; -1 on the ball points)
+    # one launch over one array: targets = [nodes; ball points], sources =
+    # its first n points (the nodes), the pair j == i skipped; the autotuner
+    # chooses among the regular launch shapes and (FP64) the symmetric form,
+    # which evaluates each node pair once and the ball points one-sided
     from fiber3d_b200 import autotune
-    shapes = {p: autotune.tune(kind, src, trg, dens, nrm, self_mode="skip_group", src_group=gs,
-                               trg_group=gt, precision=p) for p in ("fp64", "fp32c")}
+    src = trg[:dens.shape[0]]
+    shapes = {p: autotune.tune(kind, src, trg, dens, nrm, self_mode="skip_index", precision=p)
+              for p in ("fp64", "fp32c")}
     launches_per_step = 1
 
     def pair_sums(precision):
-        K.pair_sum(kind, src, trg, dens, nrm, self_mode="skip_group", src_group=gs, trg_group=gt,
-                   precision=precision, out=out, shape=shapes[precision])
+        K.pair_sum(kind, src, trg, dens, nrm, self_mode="skip_index", precision=precision, out=out,
+                   shape=shapes[precision])
 
     subtract = None
     if kind == "stresslet":

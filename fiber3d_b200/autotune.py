@@ -43,12 +43,13 @@ _names: dict[int, str] = {}
 
 def _key(kernel, precision, self_mode, ns, nt, same=False) -> str:
     """Cache key: GPU, sum, size buckets, and whether the sum runs over one
-    point set (sources are the targets, which allows the symmetric form)."""
+    point set (the sources are the first ns targets, which allows the
+    symmetric form)."""
     dev = torch.cuda.current_device()
     name = _names.get(dev)
     if name is None:
         name = _names[dev] = torch.cuda.get_device_name(dev).replace(" ", "_")
-    one = "|self" if (same and ns == nt) else ""
+    one = "|self" if (same and nt >= ns) else ""
     return f"{name}|{kernel}|{precision}|{self_mode}|{_bucket(ns)}|{_bucket(nt)}{one}"
 
 
@@ -58,8 +59,20 @@ SYM_MAX_POINTS = 192 * 128
 
 
 def symmetric_eligible(kernel, precision, self_mode, ns, nt, same) -> bool:
-    return (same and ns == nt and 0 < ns <= SYM_MAX_POINTS and precision == "fp64"
+    """Whether the symmetric form can run this sum: FP64 Oseen or stresslet
+    with a self rule, over one array whose first ns points are the sources
+    (further targets after them are summed one-sided in the same launch)."""
+    return (same and nt >= ns and 0 < ns <= SYM_MAX_POINTS and precision == "fp64"
             and kernel in ("oseen", "stresslet") and self_mode in ("skip_index", "skip_group"))
+
+
+def _same_array(a, b) -> bool:
+    """b is a, or both are device tensors starting at the same address
+    (a = b[:ns], the sources as the first points of the targets)."""
+    if a is b:
+        return True
+    return (isinstance(a, torch.Tensor) and isinstance(b, torch.Tensor) and a.is_cuda and b.is_cuda
+            and a.data_ptr() == b.data_ptr())
 
 
 def _load():
@@ -121,7 +134,8 @@ def tune(kernel: str, r_source, r_target, density, normal=None, *, self_mode="re
     from . import kernels as K
     ns = int(r_source.shape[0] if hasattr(r_source, "shape") and len(r_source.shape) == 2 else len(r_source) // 3)
     nt = int(r_target.shape[0] if hasattr(r_target, "shape") and len(r_target.shape) == 2 else len(r_target) // 3)
-    same = r_target is r_source and (self_mode != "skip_group" or trg_group is src_group)
+    same = (nt >= ns and _same_array(r_source, r_target)
+            and (self_mode != "skip_group" or _same_array(src_group, trg_group)))
     with _lock:
         _load()
         key = _key(kernel, precision, self_mode, ns, nt, same)

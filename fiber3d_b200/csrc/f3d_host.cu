@@ -4,6 +4,8 @@
 // kernels.kernels functions take and return numpy arrays) makes one call per
 // sum instead of a sequence of allocations, copies and launches.  The kernel
 // is the one f3d_pair_sum runs; only the staging differs.
+#include <algorithm>
+
 #include "f3d_common.cuh"
 
 namespace f3d {
@@ -19,7 +21,9 @@ struct HostLayout {
 };
 
 // Device staging of one host sum: [r_source][r_target unless the same
-// points][density][normal if any][out], each 256-byte aligned.
+// points][density][normal if any][out], each 256-byte aligned.  With the
+// same points (one array holding the sources as its first ns points) the
+// points region holds max(ns, nt) points.
 static HostLayout host_layout(int kernel, int64_t ns, int64_t nt, bool same) {
   HostLayout L{};
   size_t o = 0;
@@ -28,7 +32,7 @@ static HostLayout host_layout(int kernel, int64_t ns, int64_t nt, bool same) {
     o += round_up(n * sizeof(double), 256);
     return at;
   };
-  L.rs = take(3 * static_cast<size_t>(ns));
+  L.rs = take(3 * static_cast<size_t>(same ? std::max(ns, nt) : ns));
   L.rt = same ? L.rs : take(3 * static_cast<size_t>(nt));
   L.dens = take(3 * static_cast<size_t>(ns));
   L.nrm = (kernel == F3D_KERNEL_STRESSLET) ? take(3 * static_cast<size_t>(ns))
@@ -76,7 +80,8 @@ int f3d_pair_sum_host(int kernel, int precision, int self_mode, const double *r_
   auto h2d = [&](void *dst, const void *src, size_t n) {
     return n == 0 || cudaMemcpyAsync(dst, src, n, cudaMemcpyHostToDevice, st) == cudaSuccess;
   };
-  if (!h2d(d_rs, r_source, sb) || (!same && !h2d(d_rt, r_target, tb)) || !h2d(d_dens, density, sb) ||
+  if (!h2d(d_rs, r_source, same ? std::max(sb, tb) : sb) || (!same && !h2d(d_rt, r_target, tb)) ||
+      !h2d(d_dens, density, sb) ||
       (has_nrm && !h2d(d_nrm, normal, kernel == F3D_KERNEL_TRACTION ? tb : sb)))
     return F3D_ERR_CUDA;
   int rc = f3d::pair_sum_impl(kernel, precision, self_mode, d_rs, d_rt, d_dens, d_nrm, nullptr, nullptr, d_out, ns,

@@ -18,47 +18,28 @@
 // After n steps the array holds (PA)^-1; swapping columns k and p_k for
 // k = n-1 .. 0 gives A^-1.
 //
-// One CTA per block holds the whole NMAX x NMAX matrix in registers.  Lane l
-// of warp w owns rows l, l+32, .. (R = NMAX/32 of them) of columns 8w ..
-// 8w+7, so a column lives in one warp and a row is spread over all warps;
-// rows interleaved across lanes keep every shared-memory access of a column
-// conflict-free.  That makes
-// the pivot step cheap for everyone but one warp:
-//   * the warp that owns column k+1 updates its tile for step k, then finds
-//     pivot k+1 on its own (two warp reductions, no shared memory), computes
-//     the reciprocal, and publishes column k+1, p and 1/a_pk to shared
-//     memory (double buffered);
-//   * one CTA barrier per step; after it every warp swaps rows k and p of its
-//     own columns through a small per-warp buffer (one lane writes each row,
-//     __syncwarp, all read) and applies the rank-1 sweep to its tile.
+// One CTA per block holds the whole NMAX x NMAX matrix in registers: thread
+// t owns an 8 x 4 tile (rows 8*(t/(NMAX/4)) .., columns 4*(t%(NMAX/4)) ..),
+// so a warp covers whole rows.  Per step the owners of column k publish it to
+// shared memory (the pivot search is then done redundantly by every warp, no
+// extra barrier), the owners of rows k and p publish those rows, and every
+// thread applies the rank-1 sweep to its tile: two barriers per step.
 // Blocks smaller than NMAX are padded with the identity, which the sweeps
 // leave untouched.
 #include <algorithm>
-#include <type_traits>
 
 #include "f3d_common.cuh"
 
 namespace f3d {
 
-constexpr int kInvCPW = 8;  // columns per warp
+constexpr int kInvTR = 8;  // tile rows per thread
+constexpr int kInvTC = 4;  // tile columns per thread
 
 template <int NMAX>
 struct InvShape {
-  static constexpr int kRPL = NMAX / 32;        // rows per lane
-  static constexpr int kWarps = NMAX / kInvCPW;  // 4, 8, 16
-  static constexpr int kThreads = 32 * kWarps;   // 128, 256, 512
-};
-
-template <int NMAX>
-struct InvSmem {
-  double col[2][NMAX];                           // published pivot column, by step parity
-  double pinv[2];
-  int piv[2];
-  int zero[2];
-  double rk[InvShape<NMAX>::kWarps][kInvCPW];    // per warp: old row k of its columns
-  double rp[InvShape<NMAX>::kWarps][kInvCPW];    // per warp: old row p
-  int pivots[NMAX];
-  int dest[NMAX];
+  static constexpr int kColTiles = NMAX / kInvTC;
+  static constexpr int kRowTiles = NMAX / kInvTR;
+  static constexpr int kThreads = kColTiles * kRowTiles;
 };
 
 // 1/x for the pivot: the hardware approximation (rcp.approx.ftz.f64, about
@@ -73,129 +54,112 @@ __device__ __forceinline__ double reciprocal(double x) {
   return fma(y, fma(e, e, e), y);
 }
 
-// Calls f(integral_constant<int, slot>) for a slot (< R) that is the same in
-// every lane of the warp: a uniform branch to a body whose register index is
-// a compile-time constant (no per-element selects, no local memory).
-template <int R, typename F>
-__device__ __forceinline__ void on_slot(int slot, F &&f) {
-  if (slot == 0) f(std::integral_constant<int, 0>{});
-  if constexpr (R > 1) {
-    if (slot == 1) f(std::integral_constant<int, 1>{});
+// Step k = kb + M of the Gauss-Jordan sweep on the register tiles.
+// Column k is published to shared memory and zeroed in the tiles; the pivot
+// row is read back with its column-k entry taken as 1, so that one update
+//   a_ij <- a_ij - (c_i / pv) u_j
+// gives every entry: a_kj = u_j / pv on the pivot row (which is overwritten),
+// a_ik = -c_i / pv in column k, and the elimination elsewhere.
+template <int NMAX, int M>
+__device__ __forceinline__ void inverse_step(double (&a)[kInvTR][kInvTC], int kb, int n, int r0,
+                                             int c0, int ct, int rt, int lane, int tid,
+                                             double (*s_col)[NMAX], double (*s_row)[2][NMAX],
+                                             int *s_piv, int &first_zero) {
+  constexpr int II = M % kInvTR;  // tile row of row k in its owner
+  constexpr int JJ = M % kInvTC;  // tile column of column k in its owner
+  const int k = kb + M;
+  if (k >= NMAX) return;
+  const int par = k & 1;
+  // (a) publish column k, zero it in the tiles
+  if (ct == k / kInvTC) {
+#pragma unroll
+    for (int i = 0; i < kInvTR; ++i) {
+      s_col[par][r0 + i] = a[i][JJ];
+      a[i][JJ] = 0.0;
+    }
   }
-  if constexpr (R > 2) {
-    if (slot == 2) f(std::integral_constant<int, 2>{});
-    if (slot == 3) f(std::integral_constant<int, 3>{});
-  }
-}
-
-// Pivot search on column slot JJ of the owner warp for step k, and publication
-// of that column, the pivot row index and the pivot's reciprocal (buffer par).
-// The pivot is the first row p in [k, n) whose magnitude has the largest
-// leading 32 bits (sign, exponent, 20 mantissa bits): a pivot within a factor
-// 1 - 2^-20 of the column maximum -- threshold partial pivoting, as stable as
-// the exact maximum.
-template <int NMAX, int JJ>
-__device__ __forceinline__ void inv_search_publish(const double (&a)[InvShape<NMAX>::kRPL][kInvCPW], int k,
-                                                   int n, int lane, InvSmem<NMAX> &sm, int par) {
-  constexpr int R = InvShape<NMAX>::kRPL;
+  __syncthreads();
+  // (b) pivot, found by every warp: the first row p >= k whose magnitude
+  // has the largest leading 32 bits (sign, exponent, 20 mantissa bits), i.e.
+  // a pivot within a factor 1 - 2^-20 of the column maximum -- threshold
+  // partial pivoting, as stable as the exact maximum.  Two warp reductions.
   unsigned key = 0u, row = 0xFFFFFFFFu;
 #pragma unroll
-  for (int i = 0; i < R; ++i) {
-    const int r = i * 32 + lane;
+  for (int q = 0; q < NMAX / 32; ++q) {
+    const int r = lane + 32 * q;
     if (r >= k && r < n) {
-      const unsigned kq = static_cast<unsigned>(
-          static_cast<unsigned long long>(__double_as_longlong(fabs(a[i][JJ]))) >> 32);
+      const unsigned kq =
+          static_cast<unsigned>(static_cast<unsigned long long>(__double_as_longlong(fabs(s_col[par][r]))) >> 32);
       if (row == 0xFFFFFFFFu || kq > key) { key = kq; row = static_cast<unsigned>(r); }
     }
   }
   const unsigned kmax = __reduce_max_sync(0xffffffffu, row != 0xFFFFFFFFu ? key : 0u);
   const unsigned pmin = __reduce_min_sync(0xffffffffu, (row != 0xFFFFFFFFu && key == kmax) ? row : 0xFFFFFFFFu);
   const int p = pmin < static_cast<unsigned>(n) ? static_cast<int>(pmin) : k;
-#pragma unroll
-  for (int i = 0; i < R; ++i) sm.col[par][i * 32 + lane] = a[i][JJ];
-  __syncwarp();
-  if (lane == 0) {
-    const double pv = sm.col[par][p];
-    const bool zero = !(fabs(pv) >= 2.2250738585072014e-308);  // zero, subnormal or NaN
-    sm.piv[par] = p;
-    sm.zero[par] = zero ? 1 : 0;
-    sm.pinv[par] = zero ? 0.0 : reciprocal(pv);
+  // (c) publish rows k and p (column k already zero); 16-byte stores
+  if (rt == k / kInvTR) {
+    double2 *dst = reinterpret_cast<double2 *>(&s_row[par][0][c0]);
+    dst[0] = make_double2(a[II][0], a[II][1]);
+    dst[1] = make_double2(a[II][2], a[II][3]);
   }
-}
-
-// Step k = kb + M (M < 8, so the owner's column slot M is a compile-time
-// register index).  Ends with the step's one CTA barrier.
-template <int NMAX, int M>
-__device__ __forceinline__ void inverse_step(double (&a)[InvShape<NMAX>::kRPL][kInvCPW], int kb, int n,
-                                             int lane, int warp, int tid, InvSmem<NMAX> &sm,
-                                             int &first_zero) {
-  constexpr int R = InvShape<NMAX>::kRPL;
-  const int k = kb + M;
-  if (k >= n) return;  // uniform across the CTA
-  const int par = k & 1;
-  const int p = sm.piv[par];
-  const double pinv = sm.pinv[par];
-  if (tid == 0) {
-    sm.pivots[k] = p;
-    if (sm.zero[par] && first_zero == 0) first_zero = k + 1;
-  }
-  const bool own = (warp == kb / kInvCPW);
-  // the owner's column k is now in sm.col: zero it in the tile, so that the
-  // one update below also produces the new column k
-  if (own) {
+  if (rt == p / kInvTR) {
+    const int ip = p % kInvTR;
+    double v[kInvTC];
 #pragma unroll
-    for (int i = 0; i < R; ++i) a[i][M] = 0.0;
-  }
-  // rows k and p of this warp's columns, through the per-warp buffer (the
-  // tile slot of a row, row / 32, is the same in every lane)
-  on_slot<R>(k / 32, [&](auto q) {
-    if (lane == k % 32) {
+    for (int j = 0; j < kInvTC; ++j) {
+      v[j] = a[0][j];
 #pragma unroll
-      for (int j = 0; j < kInvCPW; ++j) sm.rk[warp][j] = a[decltype(q)::value][j];
+      for (int i = 1; i < kInvTR; ++i) v[j] = (ip == i) ? a[i][j] : v[j];
     }
-  });
-  on_slot<R>(p / 32, [&](auto q) {
-    if (lane == p % 32) {
-#pragma unroll
-      for (int j = 0; j < kInvCPW; ++j) sm.rp[warp][j] = a[decltype(q)::value][j];
-    }
-  });
-  __syncwarp();
-  // One FMA per element on every row: a_ij <- a_ij - (a_ik / a_pk) u_j with
-  // u = old row p (u_k = 1 in the owner's column k).  On row k this gives
-  // old row k - (a_kk / a_pk) u, which is exactly the new row p; on row p it
-  // gives nothing useful.  The two lanes holding rows k and p then put the
-  // right values in place: row k <- u / a_pk, row p <- old row k - (a_kk /
-  // a_pk) u.  (With p == k only the first.)  No per-element selects.
-  double u[kInvCPW];
-#pragma unroll
-  for (int j = 0; j < kInvCPW; ++j) u[j] = sm.rp[warp][j];
-  if (own) u[M] = 1.0;
-#pragma unroll
-  for (int i = 0; i < R; ++i) {
-    const double f = sm.col[par][i * 32 + lane] * pinv;
-#pragma unroll
-    for (int j = 0; j < kInvCPW; ++j) a[i][j] = fma(-f, u[j], a[i][j]);
+    double2 *dst = reinterpret_cast<double2 *>(&s_row[par][1][c0]);
+    dst[0] = make_double2(v[0], v[1]);
+    dst[1] = make_double2(v[2], v[3]);
   }
-  on_slot<R>(k / 32, [&](auto q) {
-    if (lane == k % 32) {
-#pragma unroll
-      for (int j = 0; j < kInvCPW; ++j) a[decltype(q)::value][j] = u[j] * pinv;
-    }
-  });
-  if (p != k) {
-    const double fk = sm.col[par][k] * pinv;
-    on_slot<R>(p / 32, [&](auto q) {
-      if (lane == p % 32) {
-#pragma unroll
-        for (int j = 0; j < kInvCPW; ++j) a[decltype(q)::value][j] = fma(-fk, u[j], sm.rk[warp][j]);
-      }
-    });
-  }
-  // the owner of column k + 1 finds the next pivot while the others finish
-  const int k1 = k + 1;
-  if (k1 < n && warp == k1 / kInvCPW) inv_search_publish<NMAX, (M + 1) % kInvCPW>(a, k1, n, lane, sm, par ^ 1);
+  if (tid == 0) s_piv[k] = p;
   __syncthreads();
+  // (d) swap rows k and p, then the update
+  const double pv = s_col[par][p];
+  const bool zero_pivot = !(fabs(pv) >= 2.2250738585072014e-308);  // zero, subnormal or NaN
+  if (zero_pivot && first_zero == 0) first_zero = k + 1;
+  const double pinv = zero_pivot ? 0.0 : reciprocal(pv);
+  double u[kInvTC];
+  {
+    const double2 *src = reinterpret_cast<const double2 *>(&s_row[par][1][c0]);
+    const double2 u01 = src[0], u23 = src[1];
+    u[0] = u01.x; u[1] = u01.y; u[2] = u23.x; u[3] = u23.y;
+  }
+  if (ct == k / kInvTC) u[JJ] = 1.0;
+  double c[kInvTR];
+  {
+    const double2 *src = reinterpret_cast<const double2 *>(&s_col[par][r0]);
+#pragma unroll
+    for (int i = 0; i < kInvTR / 2; ++i) {
+      const double2 cc = src[i];
+      c[2 * i] = cc.x;
+      c[2 * i + 1] = cc.y;
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < kInvTR; ++i) {
+    const int r = r0 + i;
+    if (r == k) {
+#pragma unroll
+      for (int j = 0; j < kInvTC; ++j) a[i][j] = u[j] * pinv;
+    } else {
+      double ci;
+      if (r == p) {
+        const double2 *src = reinterpret_cast<const double2 *>(&s_row[par][0][c0]);
+        const double2 w01 = src[0], w23 = src[1];
+        a[i][0] = w01.x; a[i][1] = w01.y; a[i][2] = w23.x; a[i][3] = w23.y;
+        ci = s_col[par][k];
+      } else {
+        ci = c[i];
+      }
+      const double f = ci * pinv;
+#pragma unroll
+      for (int j = 0; j < kInvTC; ++j) a[i][j] = fma(-f, u[j], a[i][j]);
+    }
+  }
 }
 
 template <int NMAX>
@@ -204,68 +168,70 @@ __global__ void __launch_bounds__(InvShape<NMAX>::kThreads, 1)
                            const int32_t *__restrict__ sizes, int count, float *__restrict__ A32,
                            int32_t *__restrict__ info) {
   using S = InvShape<NMAX>;
-  constexpr int R = S::kRPL;
-  __shared__ __align__(16) InvSmem<NMAX> sm;
+  __shared__ __align__(16) double s_col[2][NMAX];
+  __shared__ __align__(16) double s_row[2][2][NMAX];  // [parity][0: old row k, 1: old row p][col]
+  __shared__ int s_piv[NMAX];
+  __shared__ int s_dest[NMAX];
   const int b = blockIdx.x;
   if (b >= count) return;
   const int n = sizes[b];
   if (n <= 0 || n > NMAX) return;
-  double *Mb = A + moff[b];
+  double *M = A + moff[b];
   const int tid = threadIdx.x;
-  const int lane = tid & 31, warp = tid >> 5;
-  const int c0 = warp * kInvCPW;
+  const int lane = tid & 31;
+  const int ct = tid % S::kColTiles, rt = tid / S::kColTiles;
+  const int c0 = ct * kInvTC, r0 = rt * kInvTR;
 
-  double a[R][kInvCPW];
+  double a[kInvTR][kInvTC];
 #pragma unroll
-  for (int i = 0; i < R; ++i) {
-    const int r = i * 32 + lane;
+  for (int i = 0; i < kInvTR; ++i) {
+    const int r = r0 + i;
 #pragma unroll
-    for (int j = 0; j < kInvCPW; ++j) {
+    for (int j = 0; j < kInvTC; ++j) {
       const int c = c0 + j;
-      a[i][j] = (r < n && c < n) ? Mb[static_cast<int64_t>(r) * n + c] : (r == c ? 1.0 : 0.0);
+      a[i][j] = (r < n && c < n) ? M[static_cast<int64_t>(r) * n + c] : (r == c ? 1.0 : 0.0);
     }
   }
   int first_zero = 0;
-  if (warp == 0) inv_search_publish<NMAX, 0>(a, 0, n, lane, sm, 0);
-  __syncthreads();
-  // steps in groups of 8, so that the owner's column slot is a compile-time
-  // index inside a step; steps past n return at once
-  for (int kb = 0; kb < n; kb += kInvCPW) {
-    inverse_step<NMAX, 0>(a, kb, n, lane, warp, tid, sm, first_zero);
-    inverse_step<NMAX, 1>(a, kb, n, lane, warp, tid, sm, first_zero);
-    inverse_step<NMAX, 2>(a, kb, n, lane, warp, tid, sm, first_zero);
-    inverse_step<NMAX, 3>(a, kb, n, lane, warp, tid, sm, first_zero);
-    inverse_step<NMAX, 4>(a, kb, n, lane, warp, tid, sm, first_zero);
-    inverse_step<NMAX, 5>(a, kb, n, lane, warp, tid, sm, first_zero);
-    inverse_step<NMAX, 6>(a, kb, n, lane, warp, tid, sm, first_zero);
-    inverse_step<NMAX, 7>(a, kb, n, lane, warp, tid, sm, first_zero);
+  // Steps run in groups of kInvTR so that k % kInvTR and k % kInvTC are
+  // compile-time constants inside a step (no runtime register indexing).
+  // Steps past n pivot on the identity padding and change nothing.
+  for (int kb = 0; kb < n; kb += kInvTR) {
+    inverse_step<NMAX, 0>(a, kb, n, r0, c0, ct, rt, lane, tid, s_col, s_row, s_piv, first_zero);
+    inverse_step<NMAX, 1>(a, kb, n, r0, c0, ct, rt, lane, tid, s_col, s_row, s_piv, first_zero);
+    inverse_step<NMAX, 2>(a, kb, n, r0, c0, ct, rt, lane, tid, s_col, s_row, s_piv, first_zero);
+    inverse_step<NMAX, 3>(a, kb, n, r0, c0, ct, rt, lane, tid, s_col, s_row, s_piv, first_zero);
+    inverse_step<NMAX, 4>(a, kb, n, r0, c0, ct, rt, lane, tid, s_col, s_row, s_piv, first_zero);
+    inverse_step<NMAX, 5>(a, kb, n, r0, c0, ct, rt, lane, tid, s_col, s_row, s_piv, first_zero);
+    inverse_step<NMAX, 6>(a, kb, n, r0, c0, ct, rt, lane, tid, s_col, s_row, s_piv, first_zero);
+    inverse_step<NMAX, 7>(a, kb, n, r0, c0, ct, rt, lane, tid, s_col, s_row, s_piv, first_zero);
   }
   // column unscramble: X P, swaps (k, p_k) for k = n-1 .. 0
   __syncthreads();
   if (tid == 0) {
-    for (int j = 0; j < n; ++j) sm.dest[j] = j;  // dest[j] = source column of final column j
+    for (int j = 0; j < n; ++j) s_dest[j] = j;  // s_dest[j] = source column of final column j
     for (int k = n - 1; k >= 0; --k) {
-      const int p = sm.pivots[k];
-      const int t = sm.dest[k];
-      sm.dest[k] = sm.dest[p];
-      sm.dest[p] = t;
+      const int p = s_piv[k];
+      const int t = s_dest[k];
+      s_dest[k] = s_dest[p];
+      s_dest[p] = t;
     }
     // invert: final position of source column c
-    for (int j = 0; j < n; ++j) sm.pivots[sm.dest[j]] = j;
+    for (int j = 0; j < n; ++j) s_piv[s_dest[j]] = j;
     info[b] = first_zero;
   }
   __syncthreads();
   float *M32 = A32 ? A32 + moff[b] : nullptr;
 #pragma unroll
-  for (int i = 0; i < R; ++i) {
-    const int r = i * 32 + lane;
+  for (int i = 0; i < kInvTR; ++i) {
+    const int r = r0 + i;
     if (r >= n) continue;
 #pragma unroll
-    for (int j = 0; j < kInvCPW; ++j) {
+    for (int j = 0; j < kInvTC; ++j) {
       const int c = c0 + j;
       if (c >= n) continue;
-      const int64_t o = static_cast<int64_t>(r) * n + sm.pivots[c];
-      Mb[o] = a[i][j];
+      const int64_t o = static_cast<int64_t>(r) * n + s_piv[c];
+      M[o] = a[i][j];
       if (M32) M32[o] = static_cast<float>(a[i][j]);
     }
   }

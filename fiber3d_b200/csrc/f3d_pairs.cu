@@ -657,11 +657,11 @@ __global__ void pack_fp32_sources(const double *rs, const double *dens, const do
 
 // ---------------------------------------------------------------- host ----
 // The symmetric self-sum (f3d_pairs_sym.cu).
-size_t sym_partial_bytes(int64_t n);
-bool sym_fits(int64_t n);
+size_t sym_partial_bytes(int64_t n, int64_t nt);
+bool sym_fits(int64_t n, int64_t nt);
 int pair_sym_launch(int kernel, int self_mode, const double *x, const double *dens, const double *nrm,
-                    const int32_t *grp, double *out, int64_t n, double eta, double reg, double eps, int accumulate,
-                    double *partial, unsigned *counters, int *occupancy, cudaStream_t st);
+                    const int32_t *grp, double *out, int64_t n, int64_t nt, double eta, double reg, double eps,
+                    int accumulate, double *partial, unsigned *counters, int *occupancy, cudaStream_t st);
 
 struct Plan {
   int tpt, sl, nsplit, use_tma;
@@ -676,11 +676,12 @@ static int make_plan(int kernel, int precision, int64_t ns, int64_t nt, const f3
   if (ns < 0 || nt < 0) return F3D_ERR_SHAPE;
   p->sym = false;
   if (shape && shape->sl == -1) {
-    // symmetric self-sum: FP64 Oseen or stresslet over one point set
+    // symmetric self-sum: FP64 Oseen or stresslet over one point set (the
+    // first ns of the nt targets), further targets one-sided
     if (dual || precision != F3D_FP64 || !(kernel == F3D_KERNEL_OSEEN || kernel == F3D_KERNEL_STRESSLET))
       return F3D_ERR_ARG;
-    if (ns != nt) return F3D_ERR_SHAPE;
-    if (!sym_fits(ns)) return F3D_ERR_TOO_LARGE;
+    if (nt < ns) return F3D_ERR_SHAPE;
+    if (!sym_fits(ns, nt)) return F3D_ERR_TOO_LARGE;
     p->sym = true;
     p->tpt = 1;
     p->sl = -1;
@@ -691,7 +692,7 @@ static int make_plan(int kernel, int precision, int64_t ns, int64_t nt, const f3
     p->off_counters = 0;
     p->off_partial = kCounterBytes;
     p->off_packed = kCounterBytes;
-    p->bytes = ns > 0 ? kCounterBytes + round_up(sym_partial_bytes(ns), 256) : 0;
+    p->bytes = ns > 0 ? kCounterBytes + round_up(sym_partial_bytes(ns, nt), 256) : 0;
     return F3D_OK;
   }
   int tpt = shape && shape->tpt ? shape->tpt : 0;
@@ -816,7 +817,7 @@ static int pair_sum_core(int kernel, int precision, int self_mode, const double 
   if (kernel == F3D_KERNEL_STRESSLET && ns > 0 && !nrm) return F3D_ERR_NULL;
   if (kernel == F3D_KERNEL_TRACTION && !nrm) return F3D_ERR_NULL;  // target normals
   if (self_mode == F3D_SELF_SKIP_GROUP && (!gt || (ns > 0 && !gs))) return F3D_ERR_NULL;
-  if (self_mode == F3D_SELF_SKIP_INDEX && ns != nt) return F3D_ERR_SHAPE;
+  if (self_mode == F3D_SELF_SKIP_INDEX && nt < ns) return F3D_ERR_SHAPE;
   if (!aligned(rs, 8) || !aligned(rt, 8) || !aligned(dens, 8) || !aligned(nrm, 8) ||
       !aligned(out, 8) || !aligned(gs, 4) || !aligned(gt, 4))
     return F3D_ERR_ALIGN;
@@ -834,9 +835,10 @@ static int pair_sum_core(int kernel, int precision, int self_mode, const double 
   if (ws && !aligned(ws, 256)) return F3D_ERR_ALIGN;
   unsigned char *w = static_cast<unsigned char *>(ws);
   if (p.sym) {
-    // one point set: sources and targets (and their group ids) must be the same arrays
+    // one point set: the sources are the first ns targets (and their group
+    // ids the first ns target group ids), passed as the same arrays
     if (rs != rt || (self_mode == F3D_SELF_SKIP_GROUP && gs != gt)) return F3D_ERR_ARG;
-    return pair_sym_launch(kernel, self_mode, rs, dens, nrm, gs, out, ns, eta, reg, eps, accumulate,
+    return pair_sym_launch(kernel, self_mode, rs, dens, nrm, gs, out, ns, nt, eta, reg, eps, accumulate,
                            reinterpret_cast<double *>(w + p.off_partial), reinterpret_cast<unsigned *>(w),
                            nullptr, st);
   }
@@ -992,8 +994,8 @@ int f3d_pair_occupancy(int kernel, int precision, int self_mode, int dual, const
     if (dual || precision != F3D_FP64 || !(kernel == F3D_KERNEL_OSEEN || kernel == F3D_KERNEL_STRESSLET) ||
         !(self_mode == F3D_SELF_SKIP_INDEX || self_mode == F3D_SELF_SKIP_GROUP))
       return F3D_ERR_ARG;
-    return f3d::pair_sym_launch(kernel, self_mode, nullptr, nullptr, nullptr, nullptr, nullptr, 1, 1.0, 0.0, 0.0, 0,
-                                nullptr, nullptr, ctas_per_sm, nullptr);
+    return f3d::pair_sym_launch(kernel, self_mode, nullptr, nullptr, nullptr, nullptr, nullptr, 1, 1, 1.0, 0.0, 0.0,
+                                0, nullptr, nullptr, ctas_per_sm, nullptr);
   }
   // the shape's own tpt/sl (make_plan picks defaults for a 1-target sum)
   if (shape && shape->tpt) p.tpt = shape->tpt;

@@ -3,7 +3,9 @@
 // 214-287) and the stresslet sum of stresslet_kernel_times_normal_times_
 // density_numba (kernels.py:1123-1183), j == i skipped, and the same sums
 // with the pairs of one group (fiber) skipped (tstep_utils.py:653-700,
-// 812-851).
+// 812-851).  Further targets that are not sources (the off-surface points of
+// a double-layer evaluation) may follow the n sources in the same array;
+// they are summed one-sided in the same launch.
 //
 // A pair (i, j) contributes to target i through source j's density (and
 // normal) and to target j through source i's; both terms share r = x_i - x_j,
@@ -11,29 +13,37 @@
 // is therefore evaluated once:
 //   Oseen:     u_i += d_j/r + (r.d_j) r/r^3,   u_j += d_i/r + (r.d_i) r/r^3
 //   stresslet: v_i += (r.d_j)(r.n_j) r/r^5,    v_j -= (r.d_i)(r.n_i) r/r^5
-// (the prefactor is applied once per target, as everywhere).  About 19-20
-// FP64 instructions per ordered pair instead of 24-25.
+// (the prefactor is applied once per target, as everywhere): about 18 FP64
+// instructions per ordered pair instead of 25-26.
 //
-// Decomposition: tiles of 128 points; one CTA per tile pair (I, J), I <= J.
-// Thread t holds target i = 128 I + t and its partial sum in registers; tile
-// J's sources are staged in shared memory (one array per component).  A warp
-// meets the sources of tile J 32 at a time, rotating: at step s lane l pairs
-// its target with source (l + s) mod 32 of the group, whose position and
-// running source-side sum it holds in registers and hands to lane l - 1
-// after the step (six shuffles per step), its density and normal read from
-// shared memory.  After 32 steps lane l holds source l's sum over the warp's
-// targets; the CTA's four warps' sums are added in shared memory.  Each CTA writes two partials: tile I's
-// (slot J) and tile J's (slot I); a diagonal CTA (I == J) evaluates its tile
-// from the target side only and writes slot I.  Each tile thus receives
-// exactly T partials (T = number of tiles); the CTA that delivers the last
-// one (a self-resetting counter per tile) sums them in slot order and
-// writes the result, so the sum is the same run to run.
+// Decomposition: tiles of 128 points; one CTA of 64 threads per work item.
+// Thread t holds targets t and t + 64 of its tile, with their partial sums,
+// in registers.  Items, in this order:
+//   * (I, J), I <= J < T, row by row (a tile's sum is complete once its row
+//     is done, so the tile reductions below spread over the launch);
+//   * (X, J), X >= T: a tile of further targets against source tile J.
+// In an off-diagonal item (I < J) a warp meets tile J's sources 32 at a
+// time, rotating: at step s lane l pairs its two targets with source
+// (l + s) mod 32 of the group, whose position and running source-side sum
+// it holds in registers and hands to lane l - 1 after the step (six
+// shuffles per step, shared by the two targets); the density and normal
+// come from shared memory.  After 32 steps lane l holds source l's sum over
+// the warp's 64 targets; the CTA's two warps' sums are added in shared
+// memory.  Diagonal items (I == J) and further-target items are summed
+// from the target side only.  Each item writes its partial(s) to tile I's
+// slot J (and tile J's slot I); every tile thus receives exactly T partials
+// (T = number of source tiles), and the CTA that delivers the last one (a
+// self-resetting counter per tile) sums them in slot order and writes the
+// result, so the sum is the same run to run.
 //
 // Rules per pair (skip, regularisation of pairs closer than eps) are applied
-// only where they can matter: in diagonal tiles, in tile pairs whose group-id
-// ranges meet (SKIP_GROUP), and in tile pairs where a pair within eps is met
+// only where they can matter: in diagonal items, in items whose group-id
+// ranges meet (SKIP_GROUP), and in items where a pair within eps is met
 // (detected from the smallest r^2 of the plain pass, which is then redone).
+// Tile slots past the end hold far-away points with zero density and normal
+// (targets at +1e30, sources at -1e30), whose terms vanish without a select.
 #include <climits>
+#include <type_traits>
 
 #include "f3d_common.cuh"
 #include "f3d_pair_math.cuh"
@@ -41,233 +51,334 @@
 namespace f3d {
 
 constexpr int kSymTile = 128;
-constexpr int kSymMaxTiles = 192;  // partial storage grows as T^2: 113 MB at 192 tiles
+constexpr int kSymThreads = 64;  // two targets per thread
+constexpr int kSymWarps = kSymThreads / 32;
+constexpr int kSymMaxTiles = 192;
+constexpr size_t kSymMaxPartialBytes = size_t(256) << 20;
 
 struct SymArgs {
-  const double *x, *dens, *nrm;  // n x 3 (nrm: stresslet only)
-  const int32_t *grp;            // n (SKIP_GROUP only)
-  double *out;
-  double *partial;               // [T][T][kSymTile][3]
-  unsigned *counters;            // [T], zero on entry and on exit
-  int *err;
-  int64_t n;
-  int ntiles;
+  const double *x, *dens, *nrm;  // x: nt x 3 (the first n are the sources); dens, nrm: n x 3
+  const int32_t *grp;            // nt (SKIP_GROUP only)
+  double *out;                   // nt x 3
+  double *partial;               // [T + T2][T][kSymTile][3]
+  unsigned *counters;            // [T + T2], zero on entry and on exit
+  int64_t n, nt;
+  int ntiles, nextra;            // T source tiles, T2 tiles of further targets
   int accumulate;
   double eps2, reg2, scale;
 };
 
-size_t sym_partial_bytes(int64_t n) {
-  const int64_t T = (n + kSymTile - 1) / kSymTile;
-  return static_cast<size_t>(T) * T * kSymTile * 3 * sizeof(double);
+static int64_t sym_tiles(int64_t n) { return (n + kSymTile - 1) / kSymTile; }
+
+size_t sym_partial_bytes(int64_t n, int64_t nt) {
+  const int64_t T = sym_tiles(n), T2 = sym_tiles(nt - n);
+  return static_cast<size_t>(T + T2) * static_cast<size_t>(T) * kSymTile * 3 * sizeof(double);
 }
 
-bool sym_fits(int64_t n) { return (n + kSymTile - 1) / kSymTile <= kSymMaxTiles; }
+bool sym_fits(int64_t n, int64_t nt) {
+  if (n < 0 || nt < n) return false;
+  if (n == 0) return true;
+  const int64_t T = sym_tiles(n), T2 = sym_tiles(nt - n);
+  return T <= kSymMaxTiles && T + T2 <= kMaxCounters && sym_partial_bytes(n, nt) <= kSymMaxPartialBytes;
+}
 
 template <int KIND, int MODE>
-__global__ void __launch_bounds__(kSymTile) pair_sym_kernel(const SymArgs a) {
+__global__ void __launch_bounds__(kSymThreads) pair_sym_kernel(const SymArgs a) {
   constexpr bool kNrm = (KIND == F3D_KERNEL_STRESSLET);
+  constexpr bool kGrp = (MODE == F3D_SELF_SKIP_GROUP);
   // sources of tile J, one array per component (conflict-free when the
   // lanes of a warp read different sources)
   __shared__ __align__(16) double s_x[3][kSymTile];
   __shared__ __align__(16) double s_d[3][kSymTile];
   __shared__ __align__(16) double s_n[kNrm ? 3 : 1][kSymTile];
-  __shared__ int32_t s_grp[kSymTile];
-  __shared__ __align__(16) double s_accj[kSymTile / 32][kSymTile][3];
+  __shared__ int32_t s_grp[kGrp ? kSymTile : 1];
+  __shared__ __align__(16) double s_accj[kSymWarps][kSymTile][3];
   __shared__ int s_flags;
-  __shared__ int s_range[kSymTile / 32][4];
+  __shared__ int s_range[kSymWarps][4];
 
-  // item -> (I, J), I <= J:  item = J (J + 1) / 2 + I
-  const int64_t item = blockIdx.x;
-  int J = static_cast<int>((sqrt(8.0 * static_cast<double>(item) + 1.0) - 1.0) * 0.5);
-  while (static_cast<int64_t>(J + 1) * (J + 2) / 2 <= item) ++J;
-  while (static_cast<int64_t>(J) * (J + 1) / 2 > item) --J;
-  const int I = static_cast<int>(item - static_cast<int64_t>(J) * (J + 1) / 2);
   const int T = a.ntiles;
+  const int64_t nsym = static_cast<int64_t>(T) * (T + 1) / 2;
+  const int64_t item = blockIdx.x;
+  int I, J;
+  if (item < nsym) {
+    // row-major upper triangle: row r starts at item r (2T - r + 1) / 2
+    auto start = [T](int r) { return static_cast<int64_t>(r) * (2 * T - r + 1) / 2; };
+    const double b = 2.0 * T + 1.0;
+    I = static_cast<int>((b - sqrt(b * b - 8.0 * static_cast<double>(item))) * 0.5);
+    I = max(0, min(I, T - 1));
+    while (I > 0 && start(I) > item) --I;
+    while (I + 1 < T && start(I + 1) <= item) ++I;
+    J = I + static_cast<int>(item - start(I));
+  } else {
+    const int64_t e = item - nsym;
+    I = T + static_cast<int>(e / T);
+    J = static_cast<int>(e % T);
+  }
+  const bool extra = I >= T;  // a tile of targets that are not sources
+  const bool diag = (I == J);
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
 
-  // this thread's target, with its own density and normal for the terms it
-  // sends to the sources
-  const int64_t i = static_cast<int64_t>(I) * kSymTile + tid;
-  const bool iv = i < a.n;
-  double xi0 = 0.0, xi1 = 0.0, xi2 = 0.0, di0 = 0.0, di1 = 0.0, di2 = 0.0, ni0 = 0.0, ni1 = 0.0, ni2 = 0.0;
-  int32_t gi = INT32_MIN;
-  if (iv) {
-    xi0 = a.x[3 * i]; xi1 = a.x[3 * i + 1]; xi2 = a.x[3 * i + 2];
-    di0 = a.dens[3 * i]; di1 = a.dens[3 * i + 1]; di2 = a.dens[3 * i + 2];
-    if (kNrm) { ni0 = a.nrm[3 * i]; ni1 = a.nrm[3 * i + 1]; ni2 = a.nrm[3 * i + 2]; }
-    if (MODE == F3D_SELF_SKIP_GROUP) gi = a.grp[i];
+  // this thread's targets (k = 0: tile slot tid, k = 1: tid + 64), with their
+  // own density and normal for the terms they send to the sources
+  const int64_t tbase = extra ? a.n + static_cast<int64_t>(I - T) * kSymTile : static_cast<int64_t>(I) * kSymTile;
+  const int64_t tend = extra ? a.nt : a.n;
+  double tx[2][3], td[2][3], tn[2][3];
+  int32_t tg[2];
+  bool tv[2];
+#pragma unroll
+  for (int k = 0; k < 2; ++k) {
+    const int64_t i = tbase + tid + k * kSymThreads;
+    tv[k] = i < tend;
+    tg[k] = INT32_MIN;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      tx[k][c] = tv[k] ? a.x[3 * i + c] : 1e30;
+      td[k][c] = (tv[k] && !extra) ? a.dens[3 * i + c] : 0.0;
+      tn[k][c] = (kNrm && tv[k] && !extra) ? a.nrm[3 * i + c] : 0.0;
+    }
+    if (kGrp && tv[k]) tg[k] = a.grp[i];
   }
   // tile J's sources
   const int64_t j0 = static_cast<int64_t>(J) * kSymTile;
   const int cnt = static_cast<int>(min(static_cast<int64_t>(kSymTile), a.n - j0));
-  {
-    // past the end: far away, zero density and normal (their terms vanish)
-    const bool sv = tid < cnt;
+#pragma unroll
+  for (int k = 0; k < 2; ++k) {
+    const int s = tid + k * kSymThreads;
+    const bool sv = s < cnt;
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-      s_x[c][tid] = sv ? a.x[3 * (j0 + tid) + c] : 1e30;
-      s_d[c][tid] = sv ? a.dens[3 * (j0 + tid) + c] : 0.0;
-      if (kNrm) s_n[c][tid] = sv ? a.nrm[3 * (j0 + tid) + c] : 0.0;
+      s_x[c][s] = sv ? a.x[3 * (j0 + s) + c] : -1e30;
+      s_d[c][s] = sv ? a.dens[3 * (j0 + s) + c] : 0.0;
+      if (kNrm) s_n[c][s] = sv ? a.nrm[3 * (j0 + s) + c] : 0.0;
+    }
+    if (kGrp) s_grp[s] = sv ? a.grp[j0 + s] : INT32_MIN;
+  }
+
+  // group-id ranges of the targets and the sources (SKIP_GROUP): pairs of
+  // one group can occur only if they meet
+  bool careful = diag;
+  if (kGrp && !diag) {
+    int tlo = INT32_MAX, thi = INT32_MIN, slo = INT32_MAX, shi = INT32_MIN;
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+      if (tv[k]) {
+        tlo = min(tlo, tg[k]);
+        thi = max(thi, tg[k]);
+      }
+      const int s = tid + k * kSymThreads;
+      if (s < cnt) {
+        const int32_t g = a.grp[j0 + s];
+        slo = min(slo, g);
+        shi = max(shi, g);
+      }
+    }
+    tlo = __reduce_min_sync(0xffffffffu, tlo);
+    thi = __reduce_max_sync(0xffffffffu, thi);
+    slo = __reduce_min_sync(0xffffffffu, slo);
+    shi = __reduce_max_sync(0xffffffffu, shi);
+    if (lane == 0) {
+      s_range[warp][0] = tlo;
+      s_range[warp][1] = thi;
+      s_range[warp][2] = slo;
+      s_range[warp][3] = shi;
     }
   }
-  if (MODE == F3D_SELF_SKIP_GROUP)
-    s_grp[tid] = tid < cnt ? a.grp[j0 + tid] : INT32_MIN;
   __syncthreads();
+  if (kGrp && !diag) {
+    int TL = s_range[0][0], TH = s_range[0][1], SL = s_range[0][2], SH = s_range[0][3];
+#pragma unroll
+    for (int w = 1; w < kSymWarps; ++w) {
+      TL = min(TL, s_range[w][0]);
+      TH = max(TH, s_range[w][1]);
+      SL = min(SL, s_range[w][2]);
+      SH = max(SH, s_range[w][3]);
+    }
+    careful = (TL <= SH && SL <= TH);
+  }
 
   const long long eps2_bits = __double_as_longlong(a.eps2);
   const int eps2_hi = __double2hiint(a.eps2);
   const double reg2 = a.reg2;
-  double acc0 = 0.0, acc1 = 0.0, acc2 = 0.0;
+  double acc[2][3];
+  int hmin = INT32_MAX;
 
-  if (I == J) {
-    // one tile: every ordered pair from the target's side, with the rules
-    for (int s = 0; s < cnt; ++s) {
-      const double dx = xi0 - s_x[0][s], dy = xi1 - s_x[1][s], dz = xi2 - s_x[2][s];
-      double r2 = fma(dx, dx, fma(dy, dy, dz * dz));
-      bool skip = (s == tid);
-      if (MODE == F3D_SELF_SKIP_GROUP) skip = skip || (s_grp[s] == gi);
-      const bool close = !skip && (__double_as_longlong(r2) < eps2_bits);
-      r2 = regularise(r2, close, reg2);
-      const double d0 = s_d[0][s], d1 = s_d[1][s], d2 = s_d[2][s];
-      if (KIND == F3D_KERNEL_OSEEN) {
-        double ri = rsqrt_refined(r2);
-        ri = skip ? 0.0 : ri;
-        const double g = ri * ri * ri * fma(dx, d0, fma(dy, d1, dz * d2));
-        acc0 = fma(g, dx, fma(ri, d0, acc0));
-        acc1 = fma(g, dy, fma(ri, d1, acc1));
-        acc2 = fma(g, dz, fma(ri, d2, acc2));
-      } else {
-        const double rd = fma(dx, d0, fma(dy, d1, dz * d2));
-        const double rn = fma(dx, s_n[0][s], fma(dy, s_n[1][s], dz * s_n[2][s]));
-        double f = times_rsqrt5(rd * rn, r2);
-        f = skip ? 0.0 : f;
-        acc0 = fma(f, dx, acc0);
-        acc1 = fma(f, dy, acc1);
-        acc2 = fma(f, dz, acc2);
-      }
+  // with the rules: regularise a close pair that is not skipped; without:
+  // note the smallest r^2 (high word) for the close-pair check
+  auto rules = [&](auto rules_tag, double &r2, bool skip) {
+    constexpr bool R = decltype(rules_tag)::value;
+    if (R) {
+      if (!skip && __double_as_longlong(r2) < eps2_bits) r2 += reg2;
+    } else {
+      hmin = min(hmin, __double2hiint(r2));
     }
-  } else {
-    // group ranges of the two tiles (SKIP_GROUP): pairs of one group can
-    // occur only if they meet
-    bool careful = false;
-    if (MODE == F3D_SELF_SKIP_GROUP) {
-      // group-id ranges of tile I (the targets) and tile J (the sources)
-      int tlo = iv ? gi : INT32_MAX, thi = iv ? gi : INT32_MIN;
-      int slo = tid < cnt ? s_grp[tid] : INT32_MAX, shi = tid < cnt ? s_grp[tid] : INT32_MIN;
-      tlo = __reduce_min_sync(0xffffffffu, tlo);
-      thi = __reduce_max_sync(0xffffffffu, thi);
-      slo = __reduce_min_sync(0xffffffffu, slo);
-      shi = __reduce_max_sync(0xffffffffu, shi);
-      if (lane == 0) {
-        s_range[warp][0] = tlo;
-        s_range[warp][1] = thi;
-        s_range[warp][2] = slo;
-        s_range[warp][3] = shi;
-      }
-      __syncthreads();
-      int TL = s_range[0][0], TH = s_range[0][1], SL0 = s_range[0][2], SH = s_range[0][3];
+  };
+
+  // target side only: every source of the tile, read by all lanes at once
+  auto one_sided = [&](auto rules_tag) {
+    constexpr bool R = decltype(rules_tag)::value;
 #pragma unroll
-      for (int w = 1; w < kSymTile / 32; ++w) {
-        TL = min(TL, s_range[w][0]); TH = max(TH, s_range[w][1]);
-        SL0 = min(SL0, s_range[w][2]); SH = max(SH, s_range[w][3]);
+    for (int k = 0; k < 2; ++k) acc[k][0] = acc[k][1] = acc[k][2] = 0.0;
+    for (int s = 0; s < cnt; ++s) {
+      const double p0 = s_x[0][s], p1 = s_x[1][s], p2 = s_x[2][s];
+      const double d0 = s_d[0][s], d1 = s_d[1][s], d2 = s_d[2][s];
+      double n0 = 0.0, n1 = 0.0, n2 = 0.0;
+      if (kNrm) {
+        n0 = s_n[0][s];
+        n1 = s_n[1][s];
+        n2 = s_n[2][s];
       }
-      careful = (TL <= SH && SL0 <= TH);
+      int32_t gj = 0;
+      if (R && kGrp) gj = s_grp[s];
+#pragma unroll
+      for (int k = 0; k < 2; ++k) {
+        const double dx = tx[k][0] - p0, dy = tx[k][1] - p1, dz = tx[k][2] - p2;
+        double r2 = fma(dx, dx, fma(dy, dy, dz * dz));
+        bool skip = false;
+        if (R) skip = kGrp ? (gj == tg[k]) : (diag && s == tid + k * kSymThreads);
+        rules(rules_tag, r2, skip);
+        if (KIND == F3D_KERNEL_OSEEN) {
+          double ri = rsqrt_refined(r2);
+          if (R) ri = skip ? 0.0 : ri;
+          const double g = ri * ri * ri * fma(dx, d0, fma(dy, d1, dz * d2));
+          acc[k][0] = fma(g, dx, fma(ri, d0, acc[k][0]));
+          acc[k][1] = fma(g, dy, fma(ri, d1, acc[k][1]));
+          acc[k][2] = fma(g, dz, fma(ri, d2, acc[k][2]));
+        } else {
+          const double q = fma(dx, d0, fma(dy, d1, dz * d2)) * fma(dx, n0, fma(dy, n1, dz * n2));
+          double f = times_rsqrt5(q, r2);
+          if (R) f = skip ? 0.0 : f;
+          acc[k][0] = fma(f, dx, acc[k][0]);
+          acc[k][1] = fma(f, dy, acc[k][1]);
+          acc[k][2] = fma(f, dz, acc[k][2]);
+        }
+      }
     }
-    // two passes at most: the plain one, then (if a rule can matter) the
-    // careful one from scratch
-    for (int pass = careful ? 1 : 0; pass < 2; ++pass) {
-      const bool rules = (pass == 1);
-      acc0 = acc1 = acc2 = 0.0;
-      int hmin = INT32_MAX;
-      for (int sb = 0; sb < cnt; sb += 32) {
-        // the group's source at this lane: position and source-side sum rotate
-        int m = lane;
-        double px = s_x[0][sb + m], py = s_x[1][sb + m], pz = s_x[2][sb + m];
-        double aj0 = 0.0, aj1 = 0.0, aj2 = 0.0;
-        for (int st = 0; st < 32; ++st) {
-          const int js = sb + m;
-          const double dx = xi0 - px, dy = xi1 - py, dz = xi2 - pz;
+  };
+
+  // both sides: tile J's sources rotate through the warp 32 at a time
+  auto rotating = [&](auto rules_tag) {
+    constexpr bool R = decltype(rules_tag)::value;
+#pragma unroll
+    for (int k = 0; k < 2; ++k) acc[k][0] = acc[k][1] = acc[k][2] = 0.0;
+    const int from = (lane + 1) & 31;
+    for (int sb = 0; sb < cnt; sb += 32) {
+      int m = lane;
+      double px = s_x[0][sb + m], py = s_x[1][sb + m], pz = s_x[2][sb + m];
+      double aj0 = 0.0, aj1 = 0.0, aj2 = 0.0;
+#pragma unroll 2
+      for (int st = 0; st < 32; ++st) {
+        const int js = sb + m;
+        const double d0 = s_d[0][js], d1 = s_d[1][js], d2 = s_d[2][js];
+        double n0 = 0.0, n1 = 0.0, n2 = 0.0;
+        if (kNrm) {
+          n0 = s_n[0][js];
+          n1 = s_n[1][js];
+          n2 = s_n[2][js];
+        }
+        int32_t gj = 0;
+        if (R && kGrp) gj = s_grp[js];
+#pragma unroll
+        for (int k = 0; k < 2; ++k) {
+          const double dx = tx[k][0] - px, dy = tx[k][1] - py, dz = tx[k][2] - pz;
           double r2 = fma(dx, dx, fma(dy, dy, dz * dz));
-          bool skip = !iv;
-          if (rules) {
-            if (MODE == F3D_SELF_SKIP_GROUP) skip = skip || (s_grp[js] == gi);
-            if (!skip && __double_as_longlong(r2) < eps2_bits) r2 += reg2;
-          } else if (iv) {
-            hmin = min(hmin, __double2hiint(r2));
-          }
-          const double d0 = s_d[0][js], d1 = s_d[1][js], d2 = s_d[2][js];
+          const bool skip = R && kGrp && (gj == tg[k]);
+          rules(rules_tag, r2, skip);
           if (KIND == F3D_KERNEL_OSEEN) {
             double ri = rsqrt_refined(r2);
-            ri = skip ? 0.0 : ri;
+            if (R) ri = skip ? 0.0 : ri;
             const double ri3 = ri * ri * ri;
             const double g = ri3 * fma(dx, d0, fma(dy, d1, dz * d2));
-            const double h = ri3 * fma(dx, di0, fma(dy, di1, dz * di2));
-            acc0 = fma(g, dx, fma(ri, d0, acc0));
-            acc1 = fma(g, dy, fma(ri, d1, acc1));
-            acc2 = fma(g, dz, fma(ri, d2, acc2));
-            aj0 = fma(h, dx, fma(ri, di0, aj0));
-            aj1 = fma(h, dy, fma(ri, di1, aj1));
-            aj2 = fma(h, dz, fma(ri, di2, aj2));
+            const double h = ri3 * fma(dx, td[k][0], fma(dy, td[k][1], dz * td[k][2]));
+            acc[k][0] = fma(g, dx, fma(ri, d0, acc[k][0]));
+            acc[k][1] = fma(g, dy, fma(ri, d1, acc[k][1]));
+            acc[k][2] = fma(g, dz, fma(ri, d2, acc[k][2]));
+            aj0 = fma(h, dx, fma(ri, td[k][0], aj0));
+            aj1 = fma(h, dy, fma(ri, td[k][1], aj1));
+            aj2 = fma(h, dz, fma(ri, td[k][2], aj2));
           } else {
             double R5 = rsqrt5(r2);
-            R5 = skip ? 0.0 : R5;
-            const double n0 = s_n[0][js], n1 = s_n[1][js], n2 = s_n[2][js];
+            if (R) R5 = skip ? 0.0 : R5;
             const double f = (fma(dx, d0, fma(dy, d1, dz * d2)) * fma(dx, n0, fma(dy, n1, dz * n2))) * R5;
-            const double h = (fma(dx, di0, fma(dy, di1, dz * di2)) * fma(dx, ni0, fma(dy, ni1, dz * ni2))) * R5;
-            acc0 = fma(f, dx, acc0);
-            acc1 = fma(f, dy, acc1);
-            acc2 = fma(f, dz, acc2);
+            const double h = (fma(dx, td[k][0], fma(dy, td[k][1], dz * td[k][2])) *
+                              fma(dx, tn[k][0], fma(dy, tn[k][1], dz * tn[k][2]))) *
+                             R5;
+            acc[k][0] = fma(f, dx, acc[k][0]);
+            acc[k][1] = fma(f, dy, acc[k][1]);
+            acc[k][2] = fma(f, dz, acc[k][2]);
             aj0 = fma(-h, dx, aj0);
             aj1 = fma(-h, dy, aj1);
             aj2 = fma(-h, dz, aj2);
           }
-          // hand the source (position and its running sum) to lane - 1
-          const int from = (lane + 1) & 31;
-          px = __shfl_sync(0xffffffffu, px, from);
-          py = __shfl_sync(0xffffffffu, py, from);
-          pz = __shfl_sync(0xffffffffu, pz, from);
-          aj0 = __shfl_sync(0xffffffffu, aj0, from);
-          aj1 = __shfl_sync(0xffffffffu, aj1, from);
-          aj2 = __shfl_sync(0xffffffffu, aj2, from);
-          m = (m + 1) & 31;
         }
-        // after a full turn lane l holds source sb + l again
-        if (sb + lane < cnt) {
-          s_accj[warp][sb + lane][0] = aj0;
-          s_accj[warp][sb + lane][1] = aj1;
-          s_accj[warp][sb + lane][2] = aj2;
-        }
+        // hand the source (position and its running sum) to lane - 1
+        px = __shfl_sync(0xffffffffu, px, from);
+        py = __shfl_sync(0xffffffffu, py, from);
+        pz = __shfl_sync(0xffffffffu, pz, from);
+        aj0 = __shfl_sync(0xffffffffu, aj0, from);
+        aj1 = __shfl_sync(0xffffffffu, aj1, from);
+        aj2 = __shfl_sync(0xffffffffu, aj2, from);
+        m = (m + 1) & 31;
       }
-      // a pair within eps met by the plain pass: redo with the rules
-      if (pass == 0 && !__syncthreads_or(hmin <= eps2_hi)) break;
-      if (pass == 0) __syncthreads();
+      // after a full turn lane l holds source sb + l again
+      s_accj[warp][sb + lane][0] = aj0;
+      s_accj[warp][sb + lane][1] = aj1;
+      s_accj[warp][sb + lane][2] = aj2;
     }
-    __syncthreads();
-    // tile J's partial from this CTA: the four warps' sums, in warp order
-    if (tid < cnt) {
-      double* pj = a.partial + ((static_cast<int64_t>(J) * T + I) * kSymTile + tid) * 3;
+  };
+
+  using Plain = std::integral_constant<bool, false>;
+  using Careful = std::integral_constant<bool, true>;
+  if (diag) {
+    one_sided(Careful{});
+  } else {
+    // the plain pass, redone with the rules if a pair within eps was met
+    bool redo = careful;
+    if (!careful) {
+      if (extra)
+        one_sided(Plain{});
+      else
+        rotating(Plain{});
+      redo = __syncthreads_or(hmin <= eps2_hi);
+    }
+    if (redo) {
+      __syncthreads();
+      if (extra)
+        one_sided(Careful{});
+      else
+        rotating(Careful{});
+    }
+  }
+  __syncthreads();
+  const int64_t slot_stride = static_cast<int64_t>(kSymTile) * 3;
+  // tile J's partial from this item (slot I): the two warps' sums, in warp order
+  if (!diag && !extra) {
+    double *pj = a.partial + (static_cast<int64_t>(J) * T + I) * slot_stride;
 #pragma unroll
-      for (int m = 0; m < 3; ++m) {
-        double v = s_accj[0][tid][m];
+    for (int k = 0; k < 2; ++k) {
+      const int s = tid + k * kSymThreads;
 #pragma unroll
-        for (int w = 1; w < kSymTile / 32; ++w) v += s_accj[w][tid][m];
-        __stcg(pj + m, v);
+      for (int c = 0; c < 3; ++c) {
+        double v = s_accj[0][s][c];
+#pragma unroll
+        for (int w = 1; w < kSymWarps; ++w) v += s_accj[w][s][c];
+        __stcg(pj + 3 * s + c, v);
       }
     }
   }
-  // tile I's partial from this CTA
+  // tile I's partial from this item (slot J)
   {
-    double *pi = a.partial + ((static_cast<int64_t>(I) * T + J) * kSymTile + tid) * 3;
-    __stcg(pi, acc0);
-    __stcg(pi + 1, acc1);
-    __stcg(pi + 2, acc2);
+    double *pi = a.partial + (static_cast<int64_t>(I) * T + J) * slot_stride;
+#pragma unroll
+    for (int k = 0; k < 2; ++k)
+#pragma unroll
+      for (int c = 0; c < 3; ++c) __stcg(pi + 3 * (tid + k * kSymThreads) + c, acc[k][c]);
   }
   __threadfence();
   __syncthreads();
   if (tid == 0) {
     int f = 0;
     if (atomicAdd(&a.counters[I], 1u) == static_cast<unsigned>(T - 1)) f |= 1;
-    if (I != J && atomicAdd(&a.counters[J], 1u) == static_cast<unsigned>(T - 1)) f |= 2;
+    if (!diag && !extra && atomicAdd(&a.counters[J], 1u) == static_cast<unsigned>(T - 1)) f |= 2;
     s_flags = f;
   }
   __syncthreads();
@@ -276,19 +387,26 @@ __global__ void __launch_bounds__(kSymTile) pair_sym_kernel(const SymArgs a) {
     if (!(flags & (1 << which))) continue;
     __threadfence();
     const int X = which == 0 ? I : J;
-    const int64_t t = static_cast<int64_t>(X) * kSymTile + tid;
-    if (t < a.n) {
-      double v0 = 0.0, v1 = 0.0, v2 = 0.0;
-      for (int slot = 0; slot < T; ++slot) {
-        const double *p = a.partial + ((static_cast<int64_t>(X) * T + slot) * kSymTile + tid) * 3;
-        v0 += __ldcg(p);
-        v1 += __ldcg(p + 1);
-        v2 += __ldcg(p + 2);
+    const int64_t xbase = X < T ? static_cast<int64_t>(X) * kSymTile : a.n + static_cast<int64_t>(X - T) * kSymTile;
+    const int64_t xend = X < T ? a.n : a.nt;
+    const double *p = a.partial + static_cast<int64_t>(X) * T * slot_stride;
+    double v[2][3] = {{0.0, 0.0, 0.0}, {0.0, 0.0, 0.0}};
+#pragma unroll 4
+    for (int slot = 0; slot < T; ++slot) {
+      const double *q = p + slot * slot_stride;
+#pragma unroll
+      for (int k = 0; k < 2; ++k)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) v[k][c] += __ldcg(q + 3 * (tid + k * kSymThreads) + c);
+    }
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+      const int64_t t = xbase + tid + k * kSymThreads;
+      if (t < xend) {
+        double *o = a.out + 3 * t;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) o[c] = a.accumulate ? o[c] + v[k][c] * a.scale : v[k][c] * a.scale;
       }
-      v0 *= a.scale; v1 *= a.scale; v2 *= a.scale;
-      double *o = a.out + 3 * t;
-      if (a.accumulate) { v0 += o[0]; v1 += o[1]; v2 += o[2]; }
-      o[0] = v0; o[1] = v1; o[2] = v2;
     }
     if (tid == 0) a.counters[X] = 0u;
   }
@@ -298,36 +416,47 @@ template <int KIND, int MODE>
 static int sym_launch_one(const SymArgs &a, int *occupancy, cudaStream_t st) {
   auto kfn = pair_sym_kernel<KIND, MODE>;
   if (occupancy)
-    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(occupancy, kfn, kSymTile, 0) == cudaSuccess
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(occupancy, kfn, kSymThreads, 0) == cudaSuccess
                ? F3D_OK
                : F3D_ERR_CUDA;
-  const int64_t items = static_cast<int64_t>(a.ntiles) * (a.ntiles + 1) / 2;
-  kfn<<<static_cast<unsigned>(items), kSymTile, 0, st>>>(a);
+  const int64_t items =
+      static_cast<int64_t>(a.ntiles) * (a.ntiles + 1) / 2 + static_cast<int64_t>(a.nextra) * a.ntiles;
+  kfn<<<static_cast<unsigned>(items), kSymThreads, 0, st>>>(a);
   return launch_status();
 }
 
 // The symmetric self-sum (kernel OSEEN or STRESSLET, FP64, mode SKIP_INDEX or
-// SKIP_GROUP) over n points; partial: sym_partial_bytes(n) of workspace;
-// counters: the pair workspace's counter region.  With occupancy non-null,
-// only reports the kernel's resident CTAs per SM.
+// SKIP_GROUP) over the first n of nt points, the rest summed as targets only;
+// partial: sym_partial_bytes(n, nt) of workspace; counters: the pair
+// workspace's counter region.  With occupancy non-null, only reports the
+// kernel's resident CTAs per SM.
 int pair_sym_launch(int kernel, int self_mode, const double *x, const double *dens, const double *nrm,
-                    const int32_t *grp, double *out, int64_t n, double eta, double reg, double eps, int accumulate,
-                    double *partial, unsigned *counters, int *occupancy, cudaStream_t st) {
+                    const int32_t *grp, double *out, int64_t n, int64_t nt, double eta, double reg, double eps,
+                    int accumulate, double *partial, unsigned *counters, int *occupancy, cudaStream_t st) {
   SymArgs a{};
-  a.x = x; a.dens = dens; a.nrm = nrm; a.grp = grp; a.out = out;
-  a.partial = partial; a.counters = counters; a.err = device_error_word();
+  a.x = x;
+  a.dens = dens;
+  a.nrm = nrm;
+  a.grp = grp;
+  a.out = out;
+  a.partial = partial;
+  a.counters = counters;
   a.n = n;
-  a.ntiles = static_cast<int>((n + kSymTile - 1) / kSymTile);
+  a.nt = nt;
+  a.ntiles = static_cast<int>(sym_tiles(n));
+  a.nextra = static_cast<int>(sym_tiles(nt - n));
   a.accumulate = accumulate ? 1 : 0;
   a.eps2 = eps * eps;
   a.reg2 = reg * reg;
   a.scale = (kernel == F3D_KERNEL_STRESSLET) ? -3.0 / (4.0 * kPi * eta) : 1.0 / (8.0 * kPi * eta);
   if (kernel == F3D_KERNEL_OSEEN) {
-    return self_mode == F3D_SELF_SKIP_INDEX ? sym_launch_one<F3D_KERNEL_OSEEN, F3D_SELF_SKIP_INDEX>(a, occupancy, st)
-                                            : sym_launch_one<F3D_KERNEL_OSEEN, F3D_SELF_SKIP_GROUP>(a, occupancy, st);
+    return self_mode == F3D_SELF_SKIP_INDEX
+               ? sym_launch_one<F3D_KERNEL_OSEEN, F3D_SELF_SKIP_INDEX>(a, occupancy, st)
+               : sym_launch_one<F3D_KERNEL_OSEEN, F3D_SELF_SKIP_GROUP>(a, occupancy, st);
   }
-  return self_mode == F3D_SELF_SKIP_INDEX ? sym_launch_one<F3D_KERNEL_STRESSLET, F3D_SELF_SKIP_INDEX>(a, occupancy, st)
-                                          : sym_launch_one<F3D_KERNEL_STRESSLET, F3D_SELF_SKIP_GROUP>(a, occupancy, st);
+  return self_mode == F3D_SELF_SKIP_INDEX
+             ? sym_launch_one<F3D_KERNEL_STRESSLET, F3D_SELF_SKIP_INDEX>(a, occupancy, st)
+             : sym_launch_one<F3D_KERNEL_STRESSLET, F3D_SELF_SKIP_GROUP>(a, occupancy, st);
 }
 
 }  // namespace f3d

@@ -130,7 +130,7 @@ def pair_sum(kernel: str, r_source, r_target, density, normal=None, *, eta=1.0, 
     gs = gt = None
     if self_mode == "skip_group":
         gs = torch.as_tensor(src_group, dtype=torch.int32, device=dev).contiguous()
-        gt = torch.as_tensor(trg_group, dtype=torch.int32, device=dev).contiguous()
+        gt = gs if trg_group is src_group else torch.as_tensor(trg_group, dtype=torch.int32, device=dev).contiguous()
         if gs.numel() != rs.shape[0] or gt.numel() != rt.shape[0]:
             raise ValueError("group id arrays must have one entry per point")
     ns, nt = rs.shape[0], rt.shape[0]

@@ -55,8 +55,9 @@ typedef enum f3d_self_mode {
   /* every pair is summed; a pair with |r| < eps uses sqrt(r^2 + reg^2)
      (kernels.py:794-846, 856-908, 1186-1217)                                */
   F3D_SELF_REGULARISE = 0,
-  /* sources == targets; the pair j == i is skipped, any other pair with
-     |r| < eps is regularised (kernels.py:214-287, 1123-1183)               */
+  /* the sources are the first ns targets (nt >= ns); the pair j == i is
+     skipped, any other pair with |r| < eps is regularised (kernels.py:
+     214-287, 1123-1183).  Targets past ns skip nothing.                     */
   F3D_SELF_SKIP_INDEX = 1,
   /* pairs whose int32 group ids are equal are skipped (same fiber);
      others are regularised as in F3D_SELF_REGULARISE. This fuses
@@ -78,8 +79,17 @@ typedef enum f3d_precision {
 
 /* Launch shape of a pair kernel.  All-zero means "library default". */
 typedef struct f3d_pair_shape {
-  int32_t tpt;     /* targets per thread: 1 or 2                              */
-  int32_t sl;      /* source lanes per target group: 1, 8 or 32               */
+  int32_t tpt;     /* targets per thread: 1, 2 or 4 (4: FP64 only)           */
+  int32_t sl;      /* source lanes per target group: 1, 8 or 32; or -1: the
+                      symmetric form of a sum over one point set (each
+                      unordered pair evaluated once, both directions
+                      summed): FP64 Oseen or stresslet, F3D_SELF_SKIP_INDEX
+                      or F3D_SELF_SKIP_GROUP, r_target the r_source pointer
+                      itself (the sources are its first ns points; targets
+                      past ns are summed one-sided in the same launch) and,
+                      for SKIP_GROUP, trg_group the src_group pointer; up
+                      to 24576 sources.  tpt, nsplit and use_tma are then
+                      ignored.                                              */
   int32_t nsplit;  /* source splits (grid.y); 0 = derive from the SM count    */
   int32_t use_tma; /* 0 or 1: stage full source tiles with cp.async.bulk
                       (default); -1: stage them with plain loads            */
@@ -129,8 +139,8 @@ int f3d_pair_workspace_bytes(int kernel, int precision, int64_t ns, int64_t nt,
 
 /* General source->target sum.  `normal` is read only for the stresslet.
    `src_group`/`trg_group` are read only for F3D_SELF_SKIP_GROUP.
-   For F3D_SELF_SKIP_INDEX, r_target must hold the same points as r_source
-   (ns == nt).  If `accumulate` is non-zero the result is added to `out`,
+   For F3D_SELF_SKIP_INDEX, the first ns points of r_target must be the
+   sources (nt >= ns).  If `accumulate` is non-zero the result is added to `out`,
    otherwise `out` is overwritten. */
 int f3d_pair_sum(int kernel, int precision, int self_mode,
                  const double *r_source, const double *r_target,
@@ -144,8 +154,8 @@ int f3d_pair_sum(int kernel, int precision, int self_mode,
 /* The same sum from HOST memory in one call, for host-side bindings (the
    numpy-in, numpy-out functions of fiber3d's kernels.kernels,
    python/kernels/kernels.py:214-1264): r_source (ns x 3), r_target (nt x 3;
-   pass the r_source pointer itself for a sum over one point set, which is
-   then copied once), density (ns x 3), normal (stresslet: ns x 3 source
+   pass the r_source pointer itself for a sum over one point set, whose
+   max(ns, nt) points are then copied once), density (ns x 3), normal (stresslet: ns x 3 source
    normals; traction: nt x 3 target normals; else NULL) are copied to
    `device_buffer` (f3d_pair_host_bytes of them, 256-byte aligned), the sum
    runs on `stream` with `workspace` as f3d_pair_sum's, the result is copied

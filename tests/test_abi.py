@@ -75,8 +75,8 @@ def test_workspace_query_and_argument_checks(dll):
     one = _lib.PairShape(1, 8, 1, 0)
     assert dll.f3d_pair_workspace_bytes(1, 1, 1000, 100, ctypes.byref(one), ctypes.byref(nbytes)) == 0
     assert nbytes.value >= (256 << 10) + 1000 * 12 * 4
-    # skip-index needs ns == nt
-    assert dll.f3d_pair_sum(0, 0, 1, 8, 8, 8, None, None, None, 8, 10, 11, 1.0, 5e-3, 1e-5, 0,
+    # skip-index needs the sources as the first targets (nt >= ns)
+    assert dll.f3d_pair_sum(0, 0, 1, 8, 8, 8, None, None, None, 8, 11, 10, 1.0, 5e-3, 1e-5, 0,
                             None, None, 0, None) == 2
 
 
@@ -171,7 +171,12 @@ def test_symmetric_shape_plan_checks(dll):
     nb = ctypes.c_size_t(0)
     assert dll.f3d_pair_workspace_bytes(1, 0, 12000, 12000, ctypes.byref(shp), ctypes.byref(nb)) == 0
     assert nb.value >= 94 * 94 * 128 * 3 * 8          # T^2 partial tiles
-    assert dll.f3d_pair_workspace_bytes(1, 0, 12000, 4096, ctypes.byref(shp), ctypes.byref(nb)) == 2  # ns != nt
+    assert dll.f3d_pair_workspace_bytes(1, 0, 12000, 4096, ctypes.byref(shp), ctypes.byref(nb)) == 2  # nt < ns
+    # further targets after the sources: (T + T2) x T partial tiles
+    assert dll.f3d_pair_workspace_bytes(1, 0, 12000, 16096, ctypes.byref(shp), ctypes.byref(nb)) == 0
+    assert nb.value >= (94 + 32) * 94 * 128 * 3 * 8
+    # partial storage above 256 MiB: too large
+    assert dll.f3d_pair_workspace_bytes(1, 0, 256, 256 + 128 * 50000, ctypes.byref(shp), ctypes.byref(nb)) == 10
     assert dll.f3d_pair_workspace_bytes(1, 1, 1000, 1000, ctypes.byref(shp), ctypes.byref(nb)) == 5   # FP32C
     assert dll.f3d_pair_workspace_bytes(2, 0, 1000, 1000, ctypes.byref(shp), ctypes.byref(nb)) == 5   # rotlet
     assert dll.f3d_pair_workspace_bytes(0, 0, 192 * 128 + 1, 192 * 128 + 1, ctypes.byref(shp),

@@ -470,6 +470,66 @@ def test_symmetric_config2_self_sum(K, L):
     assert rel_err(a.cpu().numpy(), b.cpu().numpy()) < 1e-13
 
 
+@pytest.mark.parametrize("kind", ["oseen", "stresslet"])
+@pytest.mark.parametrize("mode", ["skip_index", "skip_group"])
+@pytest.mark.parametrize("n,m", [(127, 1), (300, 129), (1000, 700), (129, 300)])
+def test_symmetric_with_further_targets(K, L, kind, mode, n, m):
+    """Sources as the first n of n + m targets: the symmetric launch sums the
+    further m targets one-sided in the same launch.  Against the C oracle and
+    the regular kernel, with coincident and sub-epsilon pairs among the
+    sources, between a further target and a source, and (skip_group)
+    further targets in a source's group."""
+    rng = np.random.default_rng(n * 31 + m)
+    x = rng.random((n + m, 3)) * 3
+    x[n] = x[5]                    # a further target on a source: regularised
+    if m > 2:
+        x[n + 2] = x[7] + 4e-6     # and one within eps of a source
+    if n > 40:
+        x[10] = x[11]
+        x[30] = x[31] + 3e-6
+    d = rng.normal(size=(n, 3)); nr = rng.normal(size=(n, 3))
+    nrm = nr if kind == "stresslet" else None
+    kw = {}
+    if mode == "skip_group":
+        grp = (np.arange(n + m) // 16).astype(np.int32)
+        grp[n + 1:] = rng.integers(0, n // 16 + 1, size=m - 1) if m > 1 else grp[n + 1:]
+        kw = dict(src_group=grp[:n], trg_group=grp)
+    ref = pairs_c.pair_sum(kind, x[:n], x, d, nrm, self_mode=mode, **kw)
+    xt = torch.as_tensor(x, device="cuda")
+    if mode == "skip_group":
+        g = torch.as_tensor(grp, device="cuda")
+        kw = dict(src_group=g[:n], trg_group=g)
+    u = K.pair_sum(kind, xt[:n], xt, d, nrm, self_mode=mode, shape=L.PairShape(*SYM), **kw)
+    assert rel_err(u.cpu().numpy(), ref) < TOL64
+    v = K.pair_sum(kind, xt[:n], xt, d, nrm, self_mode=mode, shape=L.PairShape(1, 1, 0, 0), **kw)
+    assert rel_err(v.cpu().numpy(), ref) < TOL64
+    u2 = K.pair_sum(kind, xt[:n], xt, d, nrm, self_mode=mode, shape=L.PairShape(*SYM), **kw)
+    assert torch.equal(u, u2)
+
+
+def test_symmetric_config2_step(K, L):
+    """The 12000-node sphere's double layer on its own nodes (j != i) and on
+    4096 ball points, as one symmetric launch over one array, against the
+    regular kernel over the same array (full size)."""
+    from fiber3d_b200 import geometry
+    nodes, normals, w, mu, vol = geometry.stresslet_sphere_workload(seed=2)
+    q = mu * w[:, None]
+    xt = torch.as_tensor(np.concatenate([nodes, vol]), device="cuda")
+    n = nodes.shape[0]
+    a = K.pair_sum("stresslet", xt[:n], xt, q, normals, self_mode="skip_index", shape=L.PairShape(*SYM))
+    b = K.pair_sum("stresslet", xt[:n], xt, q, normals, self_mode="skip_index", shape=L.PairShape(1, 1, 0, 0))
+    assert rel_err(a.cpu().numpy(), b.cpu().numpy()) < 1e-13
+    idx = np.r_[0:50, n - 50:n + 50, xt.shape[0] - 50:xt.shape[0]]
+    ref = pairs_c.pair_sum("stresslet", nodes, xt.cpu().numpy()[idx], q, normals)
+    # the sampled rows: j == i skipped for the sphere nodes among them
+    for r, i in enumerate(idx):
+        if i < n:
+            ref[3 * r:3 * r + 3] = pairs_c.pair_sum("stresslet", np.delete(nodes, i, 0), nodes[i:i + 1],
+                                                    np.delete(q, i, 0), np.delete(normals, i, 0))
+    got = a.cpu().numpy().reshape(-1, 3)[idx].reshape(-1)
+    assert rel_err(got, ref) < 1e-12
+
+
 def test_symmetric_rejects_other_sums(K, L):
     rng = np.random.default_rng(3)
     x = rng.random((200, 3)); y = rng.random((200, 3)); d = rng.normal(size=(200, 3))
