@@ -159,8 +159,9 @@ class ClockSampler:
 
 
 # -------------------------------------------------------------- GPU arm ---
-def measured_peak(L, precision: str, torch):
-    """FMA throughput (FLOP/s) of this GPU from the library's probe kernel."""
+def measured_peak(L, precision: str, torch, gpu_index: int = 0):
+    """FMA throughput (FLOP/s) of this GPU from the library's probe kernel,
+    with the SM clock sampled while it runs."""
     import ctypes
     sink = torch.zeros(1, dtype=torch.float64, device="cuda")
     flops = ctypes.c_double(0)
@@ -170,14 +171,15 @@ def measured_peak(L, precision: str, torch):
         L.call("f3d_probe_fma", prec, 2000, L.ptr(sink), ctypes.byref(flops), st)
     torch.cuda.synchronize()
     best = 0.0
-    for _ in range(5):
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record()
-        L.call("f3d_probe_fma", prec, 2000, L.ptr(sink), ctypes.byref(flops), st)
-        e1.record()
-        e1.synchronize()
-        best = max(best, flops.value / (e0.elapsed_time(e1) * 1e-3))
-    return best
+    with ClockSampler(gpu_index) as clk:
+        for _ in range(8):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            L.call("f3d_probe_fma", prec, 2000, L.ptr(sink), ctypes.byref(flops), st)
+            e1.record()
+            e1.synchronize()
+            best = max(best, flops.value / (e0.elapsed_time(e1) * 1e-3))
+    return best, clk.summary()
 
 
 def gpu_arm(args, rank, world, local):
@@ -259,8 +261,8 @@ def gpu_arm(args, rank, world, local):
             kernel_times.extend(a.elapsed_time(b) for a, b, _ in evs)
         return [a.elapsed_time(c) for a, _, c in evs]
 
-    peak64 = measured_peak(L, "fp64", torch)
-    peak32 = measured_peak(L, "fp32c", torch)
+    peak64, peak64_clocks = measured_peak(L, "fp64", torch, local)
+    peak32, _ = measured_peak(L, "fp32c", torch, local)
     kern_ms = []
     with ClockSampler(local) as clk:
         t_ms = timed("fp64", args.steps, args.warmup, kernel_times=kern_ms)
@@ -327,9 +329,13 @@ def gpu_arm(args, rank, world, local):
                      # of it (read 1.391 MB, write 0): the sources stay in L2
                      "traffic": 1391104 if args.workload == "stresslet_sphere" else None,
                      "traffic_unit": "bytes per launch (ncu dram__bytes_read.sum + dram__bytes_write.sum)",
-                     "note": f"{flop_pair} algorithmic flop per pair (rsqrt not counted); peak = "
-                             "measured FP64 FMA rate of this GPU (f3d_probe_fma)",
-                     "kernel": f"pair_kernel<{kind}, skip_group, fp64>"},
+                     "note": f"{flop_pair} algorithmic flop per ordered pair (rsqrt not counted; the "
+                             "symmetric form evaluates each unordered pair once for both directions); peak = "
+                             "measured FP64 FMA rate of this GPU (f3d_probe_fma), with the SM clock seen "
+                             "while it ran",
+                     "peak_clocks": peak64_clocks,
+                     "kernel": (f"pair_sym_kernel<{kind}, skip_index>" if shapes["fp64"].sl == -1
+                                else f"pair_kernel<{kind}, skip_index, fp64>")},
         "timed_output_vs_default_shape_max_rel": check64,
         "fp32c": {"value": pairs / (ms32 * 1e-3) * world, "ms_per_step": ms32,
                   "max_rel_err_vs_fp64": err32, "peak_fp32_tflops": peak32 / 1e12},

@@ -5,9 +5,9 @@ the inverses of the 3 x 3 diagonal blocks of fiber3d's dense shell operator
 * f3d_block3_gemv applied to N(0, 1) vectors: 1e-13 against the oracle's
   block solves (oracle/system.py shell_block_pc), itself pinned to the dense
   operator's diagonal blocks on CPU;
-* a step solved with it reaches the oracle's true residual and the same
-  solution as with the dense inverse (within 1e-6 of an FP64 solve to 1e-11,
-  the bar of the dense preconditioner's own test), FP64 and mixed;
+* a step solved with it meets its tolerance as the oracle's true residual
+  (FP64 and mixed), and solved to 1e-12 it gives the dense inverse's
+  solution to 1e-8;
 * its GMRES needs more iterations than the dense inverse (the periphery's
   nonlocal coupling is left to GMRES) but no O(N^2) memory.
 """
@@ -63,15 +63,24 @@ def test_pc_keeps_the_other_blocks(setup):
 
 
 @pytest.mark.parametrize("mixed,tol", [(False, 1e-8), (True, 1e-9)])
-def test_solve_reaches_the_same_solution(setup, mixed, tol):
+def test_solve_meets_the_oracle_residual(setup, mixed, tol):
     _, blk, dense, op = setup
     rb = blk.solve(tol=tol, restart=100, maxiter=400, mixed=mixed)
-    xb = rb["x"].cpu().numpy()
-    assert op.true_residual(xb) < tol
-    xr = dense.solve(tol=1e-11, restart=100)["x"].cpu().numpy()
-    assert np.linalg.norm(xb - xr) / np.linalg.norm(xr) < 1e-6
+    assert rb["info"] == 0
+    assert op.true_residual(rb["x"].cpu().numpy()) < tol
     rd = dense.solve(tol=tol, restart=100, mixed=mixed)
     assert rb["iterations"] >= rd["iterations"]
+
+
+def test_tight_solutions_agree(setup):
+    """Both preconditioners solve the same system: to 1e-12 their solutions
+    agree to the operator's conditioning times that residual.  (At 1e-8 each
+    solution is only within ~kappa * 1e-8 ~ 1e-6 of the exact one, in
+    directions that depend on the preconditioner.)"""
+    _, blk, dense, op = setup
+    xb = blk.solve(tol=1e-12, restart=100, maxiter=600)["x"].cpu().numpy()
+    xr = dense.solve(tol=1e-12, restart=100)["x"].cpu().numpy()
+    assert np.linalg.norm(xb - xr) / np.linalg.norm(xr) < 1e-8
 
 
 def test_bad_option():
