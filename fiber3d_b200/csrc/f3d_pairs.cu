@@ -661,7 +661,8 @@ size_t sym_partial_bytes(int64_t n, int64_t nt);
 bool sym_fits(int64_t n, int64_t nt);
 int pair_sym_launch(int kernel, int self_mode, const double *x, const double *dens, const double *nrm,
                     const int32_t *grp, double *out, int64_t n, int64_t nt, double eta, double reg, double eps,
-                    int accumulate, double *partial, unsigned *counters, int *occupancy, cudaStream_t st);
+                    int accumulate, double *partial, unsigned *counters, int *occupancy, cudaStream_t st,
+                    const double *dens2, double *out2, bool dual);
 
 struct Plan {
   int tpt, sl, nsplit, use_tma;
@@ -677,8 +678,9 @@ static int make_plan(int kernel, int precision, int64_t ns, int64_t nt, const f3
   p->sym = false;
   if (shape && shape->sl == -1) {
     // symmetric self-sum: FP64 Oseen or stresslet over one point set (the
-    // first ns of the nt targets), further targets one-sided
-    if (dual || precision != F3D_FP64 || !(kernel == F3D_KERNEL_OSEEN || kernel == F3D_KERNEL_STRESSLET))
+    // first ns of the nt targets), further targets one-sided; the
+    // two-density Oseen form keeps two partial arrays
+    if (precision != F3D_FP64 || !(kernel == F3D_KERNEL_OSEEN || kernel == F3D_KERNEL_STRESSLET))
       return F3D_ERR_ARG;
     if (nt < ns) return F3D_ERR_SHAPE;
     if (!sym_fits(ns, nt)) return F3D_ERR_TOO_LARGE;
@@ -692,7 +694,7 @@ static int make_plan(int kernel, int precision, int64_t ns, int64_t nt, const f3
     p->off_counters = 0;
     p->off_partial = kCounterBytes;
     p->off_packed = kCounterBytes;
-    p->bytes = ns > 0 ? kCounterBytes + round_up(sym_partial_bytes(ns, nt), 256) : 0;
+    p->bytes = ns > 0 ? kCounterBytes + round_up((dual ? 2 : 1) * sym_partial_bytes(ns, nt), 256) : 0;
     return F3D_OK;
   }
   int tpt = shape && shape->tpt ? shape->tpt : 0;
@@ -840,7 +842,7 @@ static int pair_sum_core(int kernel, int precision, int self_mode, const double 
     if (rs != rt || (self_mode == F3D_SELF_SKIP_GROUP && gs != gt)) return F3D_ERR_ARG;
     return pair_sym_launch(kernel, self_mode, rs, dens, nrm, gs, out, ns, nt, eta, reg, eps, accumulate,
                            reinterpret_cast<double *>(w + p.off_partial), reinterpret_cast<unsigned *>(w),
-                           nullptr, st);
+                           nullptr, st, dens2, out2, dual);
   }
 
   PairArgs a{};
@@ -991,11 +993,11 @@ int f3d_pair_occupancy(int kernel, int precision, int self_mode, int dual, const
   if (dual && (kernel != F3D_KERNEL_OSEEN || precision != F3D_FP64 || self_mode == F3D_SELF_SKIP_CLOSE))
     return F3D_ERR_ARG;
   if (shape && shape->sl == -1) {
-    if (dual || precision != F3D_FP64 || !(kernel == F3D_KERNEL_OSEEN || kernel == F3D_KERNEL_STRESSLET) ||
+    if (precision != F3D_FP64 || !(kernel == F3D_KERNEL_OSEEN || kernel == F3D_KERNEL_STRESSLET) ||
         !(self_mode == F3D_SELF_SKIP_INDEX || self_mode == F3D_SELF_SKIP_GROUP))
       return F3D_ERR_ARG;
     return f3d::pair_sym_launch(kernel, self_mode, nullptr, nullptr, nullptr, nullptr, nullptr, 1, 1, 1.0, 0.0, 0.0,
-                                0, nullptr, nullptr, ctas_per_sm, nullptr);
+                                0, nullptr, nullptr, ctas_per_sm, nullptr, nullptr, nullptr, dual != 0);
   }
   // the shape's own tpt/sl (make_plan picks defaults for a 1-target sum)
   if (shape && shape->tpt) p.tpt = shape->tpt;

@@ -42,6 +42,10 @@
 // (detected from the smallest r^2 of the plain pass, which is then redone).
 // Tile slots past the end hold far-away points with zero density and normal
 // (targets at +1e30, sources at -1e30), whose terms vanish without a select.
+//
+// The Oseen sum also has a two-density form (DUAL): two densities over the
+// same pairs, the geometry once, each sum with the single form's exact
+// arithmetic and order, so that each equals its single sum bit for bit.
 #include <climits>
 #include <type_traits>
 
@@ -58,9 +62,10 @@ constexpr size_t kSymMaxPartialBytes = size_t(256) << 20;
 
 struct SymArgs {
   const double *x, *dens, *nrm;  // x: nt x 3 (the first n are the sources); dens, nrm: n x 3
+  const double *dens2;           // n x 3 (DUAL only)
   const int32_t *grp;            // nt (SKIP_GROUP only)
-  double *out;                   // nt x 3
-  double *partial;               // [T + T2][T][kSymTile][3]
+  double *out, *out2;            // nt x 3 (out2: DUAL only)
+  double *partial, *partial2;    // [T + T2][T][kSymTile][3] (partial2: DUAL only)
   unsigned *counters;            // [T + T2], zero on entry and on exit
   int64_t n, nt;
   int ntiles, nextra;            // T source tiles, T2 tiles of further targets
@@ -82,17 +87,19 @@ bool sym_fits(int64_t n, int64_t nt) {
   return T <= kSymMaxTiles && T + T2 <= kMaxCounters && sym_partial_bytes(n, nt) <= kSymMaxPartialBytes;
 }
 
-template <int KIND, int MODE>
+template <int KIND, int MODE, bool DUAL>
 __global__ void __launch_bounds__(kSymThreads) pair_sym_kernel(const SymArgs a) {
+  static_assert(!DUAL || KIND == F3D_KERNEL_OSEEN, "the two-density form is Oseen only");
   constexpr bool kNrm = (KIND == F3D_KERNEL_STRESSLET);
   constexpr bool kGrp = (MODE == F3D_SELF_SKIP_GROUP);
+  constexpr int ND = DUAL ? 2 : 1;  // densities
   // sources of tile J, one array per component (conflict-free when the
   // lanes of a warp read different sources)
   __shared__ __align__(16) double s_x[3][kSymTile];
-  __shared__ __align__(16) double s_d[3][kSymTile];
+  __shared__ __align__(16) double s_d[ND][3][kSymTile];
   __shared__ __align__(16) double s_n[kNrm ? 3 : 1][kSymTile];
   __shared__ int32_t s_grp[kGrp ? kSymTile : 1];
-  __shared__ __align__(16) double s_accj[kSymWarps][kSymTile][3];
+  __shared__ __align__(16) double s_accj[ND][kSymWarps][kSymTile][3];
   __shared__ int s_flags;
   __shared__ int s_range[kSymWarps][4];
 
@@ -122,7 +129,7 @@ __global__ void __launch_bounds__(kSymThreads) pair_sym_kernel(const SymArgs a) 
   // own density and normal for the terms they send to the sources
   const int64_t tbase = extra ? a.n + static_cast<int64_t>(I - T) * kSymTile : static_cast<int64_t>(I) * kSymTile;
   const int64_t tend = extra ? a.nt : a.n;
-  double tx[2][3], td[2][3], tn[2][3];
+  double tx[2][3], td[ND][2][3], tn[2][3];
   int32_t tg[2];
   bool tv[2];
 #pragma unroll
@@ -133,7 +140,8 @@ __global__ void __launch_bounds__(kSymThreads) pair_sym_kernel(const SymArgs a) 
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
       tx[k][c] = tv[k] ? a.x[3 * i + c] : 1e30;
-      td[k][c] = (tv[k] && !extra) ? a.dens[3 * i + c] : 0.0;
+      td[0][k][c] = (tv[k] && !extra) ? a.dens[3 * i + c] : 0.0;
+      if (DUAL) td[ND - 1][k][c] = (tv[k] && !extra) ? a.dens2[3 * i + c] : 0.0;
       tn[k][c] = (kNrm && tv[k] && !extra) ? a.nrm[3 * i + c] : 0.0;
     }
     if (kGrp && tv[k]) tg[k] = a.grp[i];
@@ -148,7 +156,8 @@ __global__ void __launch_bounds__(kSymThreads) pair_sym_kernel(const SymArgs a) 
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
       s_x[c][s] = sv ? a.x[3 * (j0 + s) + c] : -1e30;
-      s_d[c][s] = sv ? a.dens[3 * (j0 + s) + c] : 0.0;
+      s_d[0][c][s] = sv ? a.dens[3 * (j0 + s) + c] : 0.0;
+      if (DUAL) s_d[ND - 1][c][s] = sv ? a.dens2[3 * (j0 + s) + c] : 0.0;
       if (kNrm) s_n[c][s] = sv ? a.nrm[3 * (j0 + s) + c] : 0.0;
     }
     if (kGrp) s_grp[s] = sv ? a.grp[j0 + s] : INT32_MIN;
@@ -199,7 +208,7 @@ __global__ void __launch_bounds__(kSymThreads) pair_sym_kernel(const SymArgs a) 
   const long long eps2_bits = __double_as_longlong(a.eps2);
   const int eps2_hi = __double2hiint(a.eps2);
   const double reg2 = a.reg2;
-  double acc[2][3];
+  double acc[ND][2][3];
   int hmin = INT32_MAX;
 
   // with the rules: regularise a close pair that is not skipped; without:
@@ -217,10 +226,16 @@ __global__ void __launch_bounds__(kSymThreads) pair_sym_kernel(const SymArgs a) 
   auto one_sided = [&](auto rules_tag) {
     constexpr bool R = decltype(rules_tag)::value;
 #pragma unroll
-    for (int k = 0; k < 2; ++k) acc[k][0] = acc[k][1] = acc[k][2] = 0.0;
+    for (int q = 0; q < ND; ++q)
+#pragma unroll
+      for (int k = 0; k < 2; ++k) acc[q][k][0] = acc[q][k][1] = acc[q][k][2] = 0.0;
     for (int s = 0; s < cnt; ++s) {
       const double p0 = s_x[0][s], p1 = s_x[1][s], p2 = s_x[2][s];
-      const double d0 = s_d[0][s], d1 = s_d[1][s], d2 = s_d[2][s];
+      double sd[ND][3];
+#pragma unroll
+      for (int q = 0; q < ND; ++q)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) sd[q][c] = s_d[q][c][s];
       double n0 = 0.0, n1 = 0.0, n2 = 0.0;
       if (kNrm) {
         n0 = s_n[0][s];
@@ -239,17 +254,21 @@ __global__ void __launch_bounds__(kSymThreads) pair_sym_kernel(const SymArgs a) 
         if (KIND == F3D_KERNEL_OSEEN) {
           double ri = rsqrt_refined(r2);
           if (R) ri = skip ? 0.0 : ri;
-          const double g = ri * ri * ri * fma(dx, d0, fma(dy, d1, dz * d2));
-          acc[k][0] = fma(g, dx, fma(ri, d0, acc[k][0]));
-          acc[k][1] = fma(g, dy, fma(ri, d1, acc[k][1]));
-          acc[k][2] = fma(g, dz, fma(ri, d2, acc[k][2]));
+          const double ri3 = ri * ri * ri;
+#pragma unroll
+          for (int q = 0; q < ND; ++q) {
+            const double g = ri3 * fma(dx, sd[q][0], fma(dy, sd[q][1], dz * sd[q][2]));
+            acc[q][k][0] = fma(g, dx, fma(ri, sd[q][0], acc[q][k][0]));
+            acc[q][k][1] = fma(g, dy, fma(ri, sd[q][1], acc[q][k][1]));
+            acc[q][k][2] = fma(g, dz, fma(ri, sd[q][2], acc[q][k][2]));
+          }
         } else {
-          const double q = fma(dx, d0, fma(dy, d1, dz * d2)) * fma(dx, n0, fma(dy, n1, dz * n2));
-          double f = times_rsqrt5(q, r2);
+          const double qq = fma(dx, sd[0][0], fma(dy, sd[0][1], dz * sd[0][2])) * fma(dx, n0, fma(dy, n1, dz * n2));
+          double f = times_rsqrt5(qq, r2);
           if (R) f = skip ? 0.0 : f;
-          acc[k][0] = fma(f, dx, acc[k][0]);
-          acc[k][1] = fma(f, dy, acc[k][1]);
-          acc[k][2] = fma(f, dz, acc[k][2]);
+          acc[0][k][0] = fma(f, dx, acc[0][k][0]);
+          acc[0][k][1] = fma(f, dy, acc[0][k][1]);
+          acc[0][k][2] = fma(f, dz, acc[0][k][2]);
         }
       }
     }
@@ -259,16 +278,24 @@ __global__ void __launch_bounds__(kSymThreads) pair_sym_kernel(const SymArgs a) 
   auto rotating = [&](auto rules_tag) {
     constexpr bool R = decltype(rules_tag)::value;
 #pragma unroll
-    for (int k = 0; k < 2; ++k) acc[k][0] = acc[k][1] = acc[k][2] = 0.0;
+    for (int q = 0; q < ND; ++q)
+#pragma unroll
+      for (int k = 0; k < 2; ++k) acc[q][k][0] = acc[q][k][1] = acc[q][k][2] = 0.0;
     const int from = (lane + 1) & 31;
     for (int sb = 0; sb < cnt; sb += 32) {
       int m = lane;
       double px = s_x[0][sb + m], py = s_x[1][sb + m], pz = s_x[2][sb + m];
-      double aj0 = 0.0, aj1 = 0.0, aj2 = 0.0;
+      double aj[ND][3];
+#pragma unroll
+      for (int q = 0; q < ND; ++q) aj[q][0] = aj[q][1] = aj[q][2] = 0.0;
 #pragma unroll 2
       for (int st = 0; st < 32; ++st) {
         const int js = sb + m;
-        const double d0 = s_d[0][js], d1 = s_d[1][js], d2 = s_d[2][js];
+        double sd[ND][3];
+#pragma unroll
+        for (int q = 0; q < ND; ++q)
+#pragma unroll
+          for (int c = 0; c < 3; ++c) sd[q][c] = s_d[q][c][js];
         double n0 = 0.0, n1 = 0.0, n2 = 0.0;
         if (kNrm) {
           n0 = s_n[0][js];
@@ -287,42 +314,48 @@ __global__ void __launch_bounds__(kSymThreads) pair_sym_kernel(const SymArgs a) 
             double ri = rsqrt_refined(r2);
             if (R) ri = skip ? 0.0 : ri;
             const double ri3 = ri * ri * ri;
-            const double g = ri3 * fma(dx, d0, fma(dy, d1, dz * d2));
-            const double h = ri3 * fma(dx, td[k][0], fma(dy, td[k][1], dz * td[k][2]));
-            acc[k][0] = fma(g, dx, fma(ri, d0, acc[k][0]));
-            acc[k][1] = fma(g, dy, fma(ri, d1, acc[k][1]));
-            acc[k][2] = fma(g, dz, fma(ri, d2, acc[k][2]));
-            aj0 = fma(h, dx, fma(ri, td[k][0], aj0));
-            aj1 = fma(h, dy, fma(ri, td[k][1], aj1));
-            aj2 = fma(h, dz, fma(ri, td[k][2], aj2));
+#pragma unroll
+            for (int q = 0; q < ND; ++q) {
+              const double g = ri3 * fma(dx, sd[q][0], fma(dy, sd[q][1], dz * sd[q][2]));
+              const double h = ri3 * fma(dx, td[q][k][0], fma(dy, td[q][k][1], dz * td[q][k][2]));
+              acc[q][k][0] = fma(g, dx, fma(ri, sd[q][0], acc[q][k][0]));
+              acc[q][k][1] = fma(g, dy, fma(ri, sd[q][1], acc[q][k][1]));
+              acc[q][k][2] = fma(g, dz, fma(ri, sd[q][2], acc[q][k][2]));
+              aj[q][0] = fma(h, dx, fma(ri, td[q][k][0], aj[q][0]));
+              aj[q][1] = fma(h, dy, fma(ri, td[q][k][1], aj[q][1]));
+              aj[q][2] = fma(h, dz, fma(ri, td[q][k][2], aj[q][2]));
+            }
           } else {
             double R5 = rsqrt5(r2);
             if (R) R5 = skip ? 0.0 : R5;
-            const double f = (fma(dx, d0, fma(dy, d1, dz * d2)) * fma(dx, n0, fma(dy, n1, dz * n2))) * R5;
-            const double h = (fma(dx, td[k][0], fma(dy, td[k][1], dz * td[k][2])) *
+            const double f =
+                (fma(dx, sd[0][0], fma(dy, sd[0][1], dz * sd[0][2])) * fma(dx, n0, fma(dy, n1, dz * n2))) * R5;
+            const double h = (fma(dx, td[0][k][0], fma(dy, td[0][k][1], dz * td[0][k][2])) *
                               fma(dx, tn[k][0], fma(dy, tn[k][1], dz * tn[k][2]))) *
                              R5;
-            acc[k][0] = fma(f, dx, acc[k][0]);
-            acc[k][1] = fma(f, dy, acc[k][1]);
-            acc[k][2] = fma(f, dz, acc[k][2]);
-            aj0 = fma(-h, dx, aj0);
-            aj1 = fma(-h, dy, aj1);
-            aj2 = fma(-h, dz, aj2);
+            acc[0][k][0] = fma(f, dx, acc[0][k][0]);
+            acc[0][k][1] = fma(f, dy, acc[0][k][1]);
+            acc[0][k][2] = fma(f, dz, acc[0][k][2]);
+            aj[0][0] = fma(-h, dx, aj[0][0]);
+            aj[0][1] = fma(-h, dy, aj[0][1]);
+            aj[0][2] = fma(-h, dz, aj[0][2]);
           }
         }
-        // hand the source (position and its running sum) to lane - 1
+        // hand the source (position and its running sums) to lane - 1
         px = __shfl_sync(0xffffffffu, px, from);
         py = __shfl_sync(0xffffffffu, py, from);
         pz = __shfl_sync(0xffffffffu, pz, from);
-        aj0 = __shfl_sync(0xffffffffu, aj0, from);
-        aj1 = __shfl_sync(0xffffffffu, aj1, from);
-        aj2 = __shfl_sync(0xffffffffu, aj2, from);
+#pragma unroll
+        for (int q = 0; q < ND; ++q)
+#pragma unroll
+          for (int c = 0; c < 3; ++c) aj[q][c] = __shfl_sync(0xffffffffu, aj[q][c], from);
         m = (m + 1) & 31;
       }
       // after a full turn lane l holds source sb + l again
-      s_accj[warp][sb + lane][0] = aj0;
-      s_accj[warp][sb + lane][1] = aj1;
-      s_accj[warp][sb + lane][2] = aj2;
+#pragma unroll
+      for (int q = 0; q < ND; ++q)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) s_accj[q][warp][sb + lane][c] = aj[q][c];
     }
   };
 
@@ -350,28 +383,30 @@ __global__ void __launch_bounds__(kSymThreads) pair_sym_kernel(const SymArgs a) 
   }
   __syncthreads();
   const int64_t slot_stride = static_cast<int64_t>(kSymTile) * 3;
-  // tile J's partial from this item (slot I): the two warps' sums, in warp order
-  if (!diag && !extra) {
-    double *pj = a.partial + (static_cast<int64_t>(J) * T + I) * slot_stride;
 #pragma unroll
-    for (int k = 0; k < 2; ++k) {
-      const int s = tid + k * kSymThreads;
+  for (int q = 0; q < ND; ++q) {
+    double *const part = q == 0 ? a.partial : a.partial2;
+    // tile J's partial from this item (slot I): the two warps' sums, in warp order
+    if (!diag && !extra) {
+      double *pj = part + (static_cast<int64_t>(J) * T + I) * slot_stride;
 #pragma unroll
-      for (int c = 0; c < 3; ++c) {
-        double v = s_accj[0][s][c];
+      for (int k = 0; k < 2; ++k) {
+        const int s = tid + k * kSymThreads;
 #pragma unroll
-        for (int w = 1; w < kSymWarps; ++w) v += s_accj[w][s][c];
-        __stcg(pj + 3 * s + c, v);
+        for (int c = 0; c < 3; ++c) {
+          double v = s_accj[q][0][s][c];
+#pragma unroll
+          for (int w = 1; w < kSymWarps; ++w) v += s_accj[q][w][s][c];
+          __stcg(pj + 3 * s + c, v);
+        }
       }
     }
-  }
-  // tile I's partial from this item (slot J)
-  {
-    double *pi = a.partial + (static_cast<int64_t>(I) * T + J) * slot_stride;
+    // tile I's partial from this item (slot J)
+    double *pi = part + (static_cast<int64_t>(I) * T + J) * slot_stride;
 #pragma unroll
     for (int k = 0; k < 2; ++k)
 #pragma unroll
-      for (int c = 0; c < 3; ++c) __stcg(pi + 3 * (tid + k * kSymThreads) + c, acc[k][c]);
+      for (int c = 0; c < 3; ++c) __stcg(pi + 3 * (tid + k * kSymThreads) + c, acc[q][k][c]);
   }
   __threadfence();
   __syncthreads();
@@ -389,32 +424,36 @@ __global__ void __launch_bounds__(kSymThreads) pair_sym_kernel(const SymArgs a) 
     const int X = which == 0 ? I : J;
     const int64_t xbase = X < T ? static_cast<int64_t>(X) * kSymTile : a.n + static_cast<int64_t>(X - T) * kSymTile;
     const int64_t xend = X < T ? a.n : a.nt;
-    const double *p = a.partial + static_cast<int64_t>(X) * T * slot_stride;
-    double v[2][3] = {{0.0, 0.0, 0.0}, {0.0, 0.0, 0.0}};
+#pragma unroll
+    for (int q = 0; q < ND; ++q) {
+      const double *p = (q == 0 ? a.partial : a.partial2) + static_cast<int64_t>(X) * T * slot_stride;
+      double v[2][3] = {{0.0, 0.0, 0.0}, {0.0, 0.0, 0.0}};
 #pragma unroll 4
-    for (int slot = 0; slot < T; ++slot) {
-      const double *q = p + slot * slot_stride;
+      for (int slot = 0; slot < T; ++slot) {
+        const double *ps = p + slot * slot_stride;
 #pragma unroll
-      for (int k = 0; k < 2; ++k)
+        for (int k = 0; k < 2; ++k)
 #pragma unroll
-        for (int c = 0; c < 3; ++c) v[k][c] += __ldcg(q + 3 * (tid + k * kSymThreads) + c);
-    }
+          for (int c = 0; c < 3; ++c) v[k][c] += __ldcg(ps + 3 * (tid + k * kSymThreads) + c);
+      }
+      double *const outq = q == 0 ? a.out : a.out2;
 #pragma unroll
-    for (int k = 0; k < 2; ++k) {
-      const int64_t t = xbase + tid + k * kSymThreads;
-      if (t < xend) {
-        double *o = a.out + 3 * t;
+      for (int k = 0; k < 2; ++k) {
+        const int64_t t = xbase + tid + k * kSymThreads;
+        if (t < xend) {
+          double *o = outq + 3 * t;
 #pragma unroll
-        for (int c = 0; c < 3; ++c) o[c] = a.accumulate ? o[c] + v[k][c] * a.scale : v[k][c] * a.scale;
+          for (int c = 0; c < 3; ++c) o[c] = a.accumulate ? o[c] + v[k][c] * a.scale : v[k][c] * a.scale;
+        }
       }
     }
     if (tid == 0) a.counters[X] = 0u;
   }
 }
 
-template <int KIND, int MODE>
+template <int KIND, int MODE, bool DUAL>
 static int sym_launch_one(const SymArgs &a, int *occupancy, cudaStream_t st) {
-  auto kfn = pair_sym_kernel<KIND, MODE>;
+  auto kfn = pair_sym_kernel<KIND, MODE, DUAL>;
   if (occupancy)
     return cudaOccupancyMaxActiveBlocksPerMultiprocessor(occupancy, kfn, kSymThreads, 0) == cudaSuccess
                ? F3D_OK
@@ -427,19 +466,24 @@ static int sym_launch_one(const SymArgs &a, int *occupancy, cudaStream_t st) {
 
 // The symmetric self-sum (kernel OSEEN or STRESSLET, FP64, mode SKIP_INDEX or
 // SKIP_GROUP) over the first n of nt points, the rest summed as targets only;
-// partial: sym_partial_bytes(n, nt) of workspace; counters: the pair
-// workspace's counter region.  With occupancy non-null, only reports the
-// kernel's resident CTAs per SM.
+// with dens2/out2 (Oseen only) the two-density form.  partial:
+// sym_partial_bytes(n, nt) of workspace, twice that for two densities;
+// counters: the pair workspace's counter region.  With occupancy non-null,
+// only reports the kernel's resident CTAs per SM.
 int pair_sym_launch(int kernel, int self_mode, const double *x, const double *dens, const double *nrm,
                     const int32_t *grp, double *out, int64_t n, int64_t nt, double eta, double reg, double eps,
-                    int accumulate, double *partial, unsigned *counters, int *occupancy, cudaStream_t st) {
+                    int accumulate, double *partial, unsigned *counters, int *occupancy, cudaStream_t st,
+                    const double *dens2, double *out2, bool dual) {
   SymArgs a{};
   a.x = x;
   a.dens = dens;
+  a.dens2 = dens2;
   a.nrm = nrm;
   a.grp = grp;
   a.out = out;
+  a.out2 = out2;
   a.partial = partial;
+  a.partial2 = partial ? partial + sym_partial_bytes(n, nt) / sizeof(double) : nullptr;
   a.counters = counters;
   a.n = n;
   a.nt = nt;
@@ -449,14 +493,19 @@ int pair_sym_launch(int kernel, int self_mode, const double *x, const double *de
   a.eps2 = eps * eps;
   a.reg2 = reg * reg;
   a.scale = (kernel == F3D_KERNEL_STRESSLET) ? -3.0 / (4.0 * kPi * eta) : 1.0 / (8.0 * kPi * eta);
+  if (kernel == F3D_KERNEL_OSEEN && dual) {
+    return self_mode == F3D_SELF_SKIP_INDEX
+               ? sym_launch_one<F3D_KERNEL_OSEEN, F3D_SELF_SKIP_INDEX, true>(a, occupancy, st)
+               : sym_launch_one<F3D_KERNEL_OSEEN, F3D_SELF_SKIP_GROUP, true>(a, occupancy, st);
+  }
   if (kernel == F3D_KERNEL_OSEEN) {
     return self_mode == F3D_SELF_SKIP_INDEX
-               ? sym_launch_one<F3D_KERNEL_OSEEN, F3D_SELF_SKIP_INDEX>(a, occupancy, st)
-               : sym_launch_one<F3D_KERNEL_OSEEN, F3D_SELF_SKIP_GROUP>(a, occupancy, st);
+               ? sym_launch_one<F3D_KERNEL_OSEEN, F3D_SELF_SKIP_INDEX, false>(a, occupancy, st)
+               : sym_launch_one<F3D_KERNEL_OSEEN, F3D_SELF_SKIP_GROUP, false>(a, occupancy, st);
   }
   return self_mode == F3D_SELF_SKIP_INDEX
-             ? sym_launch_one<F3D_KERNEL_STRESSLET, F3D_SELF_SKIP_INDEX>(a, occupancy, st)
-             : sym_launch_one<F3D_KERNEL_STRESSLET, F3D_SELF_SKIP_GROUP>(a, occupancy, st);
+             ? sym_launch_one<F3D_KERNEL_STRESSLET, F3D_SELF_SKIP_INDEX, false>(a, occupancy, st)
+             : sym_launch_one<F3D_KERNEL_STRESSLET, F3D_SELF_SKIP_GROUP, false>(a, occupancy, st);
 }
 
 }  // namespace f3d
