@@ -326,8 +326,10 @@ def gpu_arm(args, rank, world, local):
                      "unit": "TFLOP/s", "frac": achieved / peak64,
                      "kernel_ms_avg": kern_avg,
                      # DRAM bytes per launch of this kernel on this workload, from an ncu capture
-                     # of it (read 1.391 MB, write 0): the sources stay in L2
-                     "traffic": 1391104 if args.workload == "stresslet_sphere" else None,
+                     # of it: symmetric form read 997.9 KB + write 29.2 KB (its tile partials stay
+                     # in L2); one-sided form read 1.391 MB, write 0
+                     "traffic": (None if args.workload != "stresslet_sphere"
+                                 else 1027072 if shapes["fp64"].sl == -1 else 1391104),
                      "traffic_unit": "bytes per launch (ncu dram__bytes_read.sum + dram__bytes_write.sum)",
                      "note": f"{flop_pair} algorithmic flop per ordered pair (rsqrt not counted; the "
                              "symmetric form evaluates each unordered pair once for both directions); peak = "
