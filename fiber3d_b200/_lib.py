@@ -92,6 +92,12 @@ SIGNATURES: dict[str, list] = {
     "f3d_singularity_vectors": [_P, _P, _P, _P, _I64, _D, _D, _D, _P, _SZ, _P],
     "f3d_shell_residual": [_P, _P, _P, _P, _P, _P, _I64, _P, _P],
     "f3d_block3_gemv": [_P, _P, _P, _I64, _P],
+    "f3d_fmm_create": [_I, _I, _P, _P, _P, _P],
+    "f3d_fmm_destroy": [_P],
+    "f3d_fmm_set_box": [_P, _P, _D],
+    "f3d_fmm_set_points": [_P, _I64, _P, _I64, _P, _I64, _P, _P],
+    "f3d_fmm_evaluate": [_P, _P, _P, _P, _P, _P, _D, _P],
+    "f3d_fmm_tree_info": [_P, _P, _P, _P, _P],
     "f3d_body_residual": [ctypes.c_int32, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P],
     "f3d_surface_dense": [_I, _P, _P, _P, _P, _P, _P, _I64, _I64, _D, _D, _D, _P],
     "f3d_rotate_blocks": [_P, _P, _P, _P, ctypes.c_int32, _I, _P],

@@ -327,27 +327,71 @@ def oseen_kernel_source_target_pycuda(r_source, r_target, density, eta=1.0, epsi
                     epsilon_distance, "fp64", None)
 
 
+def _fmm_handle(kwargs):
+    """The package FMM behind a ``fmm_PVel`` argument (a ``stkfmm.STKFMM`` of
+    this package, or an ``fmm.FMM``), else None."""
+    h = kwargs.get("fmm_PVel")
+    if h is None:
+        return None
+    from . import fmm as F, stkfmm as S
+    if isinstance(h, S.STKFMM):
+        return h.fmm
+    if isinstance(h, F.FMM):
+        return h
+    raise TypeError("fmm_PVel must be a fiber3d_b200.stkfmm.STKFMM or fiber3d_b200.fmm.FMM")
+
+
+def _fmm_sum(fmm, r_sl, r_dl, r_target, f_sl, normal, dens_dl, eta, host):
+    """The FMM evaluation of the reference's *_stkfmm functions: the tree is
+    rebuilt only when the sources or targets changed (kernels.py:1328-1352),
+    its box the bounding cube with a 10 % margin (:1339-1348)."""
+    dev = fmm.device
+    pts = [None if a is None else _to_dev(a, dev, name) for a, name in
+           ((r_sl, "r_source_SL"), (r_dl, "r_source_DL"), (r_target, "r_target"))]
+    pts = [None if p is None or p.shape[0] == 0 else p for p in pts]
+    last = getattr(fmm, "_drop_in_points", None)
+    same = last is not None and all(
+        (a is None and b is None) or (a is not None and b is not None and a.shape == b.shape and torch.equal(a, b))
+        for a, b in zip(pts, last))
+    if not same:
+        fmm.set_points(*pts)
+        fmm._drop_in_points = [None if p is None else p.clone() for p in pts]
+    u = fmm.evaluate(sl_density=None if pts[0] is None else _to_dev(f_sl, dev, "density_SL"),
+                     dl_normal=None if pts[1] is None else _to_dev(normal, dev, "normal"),
+                     dl_density=None if pts[1] is None else _to_dev(dens_dl, dev, "density_DL"), eta=eta)
+    return _out(u, host, "fmm")
+
+
 def oseen_kernel_source_target_stkfmm(r_source, r_target, density, eta=1.0, reg=5e-3,
                                       epsilon_distance=1e-5, *args, **kwargs):
-    """Stand-in for fiber3d's STKFMM Stokeslet (kernels.py:1298-1364): the
-    same velocity, u_t = 1/(8 pi eta) sum_s [f/r + (r.f) r/r^3], by direct
-    summation on the GPU (exact, where the FMM is accurate to its expansion
-    order).  Like the FMM's kernel it regularises nothing and leaves out
-    coincident source-target pairs.  ``reg``, ``epsilon_distance`` and the
-    FMM handle (``fmm_PVel``) are accepted and unused, as in fiber3d."""
+    """fiber3d's STKFMM Stokeslet (kernels.py:1298-1364):
+    u_t = 1/(8 pi eta) sum_s [f/r + (r.f) r/r^3], nothing regularised,
+    coincident source-target pairs left out.  With ``fmm_PVel`` (this
+    package's ``stkfmm.STKFMM`` or ``fmm.FMM``) by the GPU FMM, accurate to
+    its expansion order, the tree kept while the points do not change; without
+    it by direct summation on the GPU (exact).  ``reg`` and
+    ``epsilon_distance`` are accepted and unused, as in fiber3d."""
+    fmm = _fmm_handle(kwargs)
+    if fmm is not None:
+        return _fmm_sum(fmm, r_source, None, r_target, density, None, None, eta,
+                        _any_host(r_source, r_target, density))
     return _drop_in("oseen", r_source, r_target, density, None, "skip_close", eta, 0.0,
                     COINCIDENT, "fp64", None)
 
 
 def stresslet_kernel_source_target_stkfmm(r_source, r_target, normal, density, eta=1.0, reg=5e-3,
                                           epsilon_distance=1e-5, *args, **kwargs):
-    """Stand-in for fiber3d's STKFMM double layer (kernels.py:1367-1419):
-    v_t = -3/(4 pi eta) sum_s (r.n_s)(r.d_s) r / r^5 by direct summation.
-    fiber3d hands the FMM the double-layer tensor 2 (n (x) d) (:1410) because
-    STKFMM's double-layer kernel carries half of fiber3d's prefactor; the
-    product is this stresslet sum, the one fiber3d checks the FMM against
-    (kernels/test_stkfmm.py).  Coincident pairs are left out, nothing is
-    regularised."""
+    """fiber3d's STKFMM double layer (kernels.py:1367-1419):
+    v_t = -3/(4 pi eta) sum_s (r.n_s)(r.d_s) r / r^5.  fiber3d hands the FMM
+    the double-layer tensor 2 (n (x) d) (:1410) because STKFMM's double-layer
+    kernel carries half of fiber3d's prefactor; the product is this stresslet
+    sum, the one fiber3d checks the FMM against (kernels/test_stkfmm.py).
+    Coincident pairs are left out, nothing is regularised.  By the GPU FMM
+    with ``fmm_PVel``, else by direct summation."""
+    fmm = _fmm_handle(kwargs)
+    if fmm is not None:
+        return _fmm_sum(fmm, None, r_source, r_target, None, normal, density, eta,
+                        _any_host(r_source, r_target, normal, density))
     return _drop_in("stresslet", r_source, r_target, density, normal, "skip_close", eta, 0.0,
                     COINCIDENT, "fp64", None)
 
@@ -355,11 +399,15 @@ def stresslet_kernel_source_target_stkfmm(r_source, r_target, normal, density, e
 def single_double_layer_kernel_source_target_stkfmm(r_source_SL, r_source_DL, r_target, normal,
                                                     density_SL, density_DL, eta=1.0, reg=5e-3,
                                                     epsilon_distance=1e-5, *args, **kwargs):
-    """Stand-in for fiber3d's combined STKFMM evaluation (kernels.py:1422-1485):
-    the Stokeslet sum of density_SL at r_source_SL plus the double layer of
+    """fiber3d's combined STKFMM evaluation (kernels.py:1422-1485): the
+    Stokeslet sum of density_SL at r_source_SL plus the double layer of
     (normal, density_DL) at r_source_DL (fiber3d's 2 (n (x) d) tensor, :1476),
-    on the same targets, by direct summation; coincident pairs left out."""
+    on the same targets; coincident pairs left out.  By the GPU FMM with
+    ``fmm_PVel``, else by direct summation."""
     host = _any_host(r_source_SL, r_source_DL, r_target, normal, density_SL, density_DL)
+    fmm = _fmm_handle(kwargs)
+    if fmm is not None:
+        return _fmm_sum(fmm, r_source_SL, r_source_DL, r_target, density_SL, normal, density_DL, eta, host)
     dev = _device()
     rt = _to_dev(r_target, dev, "r_target")
     u = torch.zeros(3 * rt.shape[0], dtype=torch.float64, device=dev)

@@ -651,6 +651,52 @@ int f3d_surface_quadrature(const double *nodes, int64_t n, const int32_t *triang
                            const double *gradient, double *weights, int32_t *neighbors, void *workspace,
                            size_t workspace_bytes, void *stream);
 
+/* ---- fast multipole method: the STKFMM PVel sums (kernels.py:1298-1485) --
+   fiber3d's useFMM path (tstep/tstep.py:116-137) evaluates its Stokeslet
+   (single layer) and stresslet (double layer) sums with the external STKFMM
+   library (kernel-independent FMM, PVel kernel).  These entries are this
+   library's own KIFMM on one GPU with the same inputs and outputs (velocity
+   only): a uniform octree of depth 2..8, equivalent densities (Stokeslet +
+   potential source) on cube surfaces of `order` points per edge, the
+   near field (27 neighbour leaves) summed directly with coincident points
+   (|r| < 1e-150) excluded, as STKFMM's kernels exclude them.
+   All point and value arrays are device memory on `stream`'s device.    */
+typedef struct f3d_fmm f3d_fmm;
+
+/* A handle for expansions of `order` (even, 4..16; n = 6 (order - 1)^2 + 2
+   surface points) and leaves of about `max_pts` sources.  `surface` (n x 3:
+   the unit cube's surface points of the order grid), `uc2ue` and `dc2de`
+   (4n x 3n each, row-major: the pseudo-inverses that map a check potential
+   on the surface at 2.95 (upward) or 1.05 (downward) half-widths to an
+   equivalent density on the surface at 1.05 or 2.95) are host arrays the
+   caller computes once per order (fiber3d_b200/fmm.py).  STKFMM(order,
+   max_pts, ...) of the reference.                                         */
+int f3d_fmm_create(int order, int max_pts, const double *surface, const double *uc2ue, const double *dc2de,
+                   f3d_fmm **fmm);
+int f3d_fmm_destroy(f3d_fmm *fmm);
+/* The tree's cube: lower corner lo[3] and side `width` (stkfmm.setBox);
+   every point must lie inside it.  Without it set_points takes the
+   bounding cube of all points with a 10 % margin per side
+   (kernels.py:1339-1348).                                                */
+int f3d_fmm_set_box(f3d_fmm *fmm, const double *lo, double width);
+/* Single-layer sources (nsl x 3), double-layer sources (ndl x 3) and
+   targets (ntrg x 3); sorts them into the tree (stkfmm.setPoints +
+   setupTree).  Counts up to 2^31 - 1 each.                               */
+int f3d_fmm_set_points(f3d_fmm *fmm, int64_t nsl, const double *src_sl, int64_t ndl, const double *src_dl,
+                       int64_t ntrg, const double *trg, void *stream);
+/* out (ntrg x 3) = [single layer of sl_density (nsl x 3, forces) + double
+   layer of the tensors D (ndl x 9, D_jk per source, the STKFMM layout; or,
+   when dl_tensor is NULL, D = 2 n (x) d from dl_normal and dl_density,
+   ndl x 3 each, fiber3d's convention at kernels.py:1410)] / eta:
+   u_i = sum f_j / (8 pi) (delta_ij / r + r_i r_j / r^3)
+         - 3 / (8 pi) sum r_i (r^T D r) / r^5,  r = target - source
+   (stkfmm.evaluateFMM, velocity components).                             */
+int f3d_fmm_evaluate(f3d_fmm *fmm, const double *sl_density, const double *dl_normal, const double *dl_density,
+                     const double *dl_tensor, double *out, double eta, void *stream);
+/* The tree of the last set_points: depth, non-empty source and target
+   leaves, box (lo[3], width).                                            */
+int f3d_fmm_tree_info(const f3d_fmm *fmm, int *depth, int64_t *src_leaves, int64_t *trg_leaves, double *box);
+
 #ifdef __cplusplus
 }
 #endif
