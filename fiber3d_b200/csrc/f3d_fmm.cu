@@ -933,10 +933,13 @@ int reserve_expansions(f3d_fmm *h) {
   return reserve(h->ybuf, ymax * n3 * sizeof(double));
 }
 
-void launch_gemm(const GemmOp &op, cudaStream_t st) {
-  if (op.ncols <= 0) return;
-  const dim3 grid(static_cast<unsigned>((op.rows + GBM - 1) / GBM), static_cast<unsigned>((op.ncols + GBN - 1) / GBN));
+int launch_gemm(const GemmOp &op, cudaStream_t st) {
+  if (op.ncols <= 0) return F3D_OK;
+  const int64_t ytiles = (static_cast<int64_t>(op.ncols) + GBN - 1) / GBN;
+  if (ytiles > 65535) return F3D_ERR_TOO_LARGE;  // more boxes in a level than one launch covers
+  const dim3 grid(static_cast<unsigned>((op.rows + GBM - 1) / GBM), static_cast<unsigned>(ytiles));
   fmm_gemm_kernel<<<grid, GTHREADS, 0, st>>>(op);
+  return launch_status();
 }
 
 GemmOp stored_op(const double *A, int rows, int K, const double *X, int ldx, double *Y, int ldy, int ncols,
@@ -1120,8 +1123,10 @@ int f3d_fmm_evaluate(f3d_fmm *h, const double *sl_density, const double *dl_norm
     const dim3 grid(static_cast<unsigned>(leaf.nsrc), static_cast<unsigned>((n + 127) / 128));
     p2m_check_kernel<<<grid, 128, 0, st>>>(h->geo, L, as<int>(leaf.src_keys), src, surf, n, Y);
     const double hL = h->geo.width / static_cast<double>(2 << L);
-    launch_gemm(stored_op(as<double>(h->uc2ue), n4, n3, Y, n3, as<double>(leaf.phi), n4, leaf.nsrc, hL), st);
-    if ((rc = launch_status())) return rc;
+    if ((rc = launch_status()) ||
+        (rc = launch_gemm(stored_op(as<double>(h->uc2ue), n4, n3, Y, n3, as<double>(leaf.phi), n4, leaf.nsrc, hL),
+                          st)))
+      return rc;
   }
   for (int l = L - 1; l >= 2; --l) {
     Level &lv = h->lev[l], &below = h->lev[l + 1];
@@ -1151,9 +1156,9 @@ int f3d_fmm_evaluate(f3d_fmm *h, const double *sl_density, const double *dl_norm
     op.ldy = n3;
     op.ncols = lv.nsrc;
     op.scale = 1.0;
-    launch_gemm(op, st);
-    launch_gemm(stored_op(as<double>(h->uc2ue), n4, n3, Y, n3, as<double>(lv.phi), n4, lv.nsrc, 1.0), st);
-    if ((rc = launch_status())) return rc;
+    if ((rc = launch_gemm(op, st)) ||
+        (rc = launch_gemm(stored_op(as<double>(h->uc2ue), n4, n3, Y, n3, as<double>(lv.phi), n4, lv.nsrc, 1.0), st)))
+      return rc;
   }
   // downward pass: interaction lists, the parent's local expansion, then
   // equivalent densities
@@ -1199,7 +1204,7 @@ int f3d_fmm_evaluate(f3d_fmm *h, const double *sl_density, const double *dl_norm
             ++t;
           }
       op.nterms = t;  // 189
-      launch_gemm(op, st);
+      if ((rc = launch_gemm(op, st))) return rc;
       if (l > 2) {
         GemmOp pp{};
         pp.mode = 1;
@@ -1227,11 +1232,11 @@ int f3d_fmm_evaluate(f3d_fmm *h, const double *sl_density, const double *dl_norm
         pp.ncols = c1 - c0;
         pp.scale = 1.0;
         pp.accumulate = 1;
-        launch_gemm(pp, st);
+        if ((rc = launch_gemm(pp, st))) return rc;
       }
     }
-    launch_gemm(stored_op(as<double>(h->dc2de), n4, n3, Y, n3, as<double>(lv.psi), n4, lv.ntrg, 1.0), st);
-    if ((rc = launch_status())) return rc;
+    if ((rc = launch_gemm(stored_op(as<double>(h->dc2de), n4, n3, Y, n3, as<double>(lv.psi), n4, lv.ntrg, 1.0), st)))
+      return rc;
   }
   // near field and the local expansions at the targets
   NearArgs na{};
