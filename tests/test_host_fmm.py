@@ -52,7 +52,7 @@ def sources():
     return y, rng.normal(size=(150, 3)), rng.normal(size=(150, 3)), rng.normal(size=(150, 3))
 
 
-@pytest.mark.parametrize("order,tol_sl,tol_dl", [(6, 5e-5, 1e-3), (8, 1e-6, 2e-5)])
+@pytest.mark.parametrize("order,tol_sl,tol_dl", [(6, 5e-5, 1e-3), (8, 1e-6, 2e-5), (10, 2e-7, 3e-6)])
 @pytest.mark.parametrize("h", [1.0, 0.125])
 def test_upward_equivalent_density(sources, order, tol_sl, tol_dl, h):
     """Sources in a box of half-width h: their velocity on the upward check
@@ -71,7 +71,7 @@ def test_upward_equivalent_density(sources, order, tol_sl, tol_dl, h):
         assert rel(u, field(far)) < tol
 
 
-@pytest.mark.parametrize("order,tol", [(6, 1e-3), (8, 3e-5)])
+@pytest.mark.parametrize("order,tol", [(6, 1e-3), (8, 3e-5), (10, 1e-6)])
 def test_downward_equivalent_density(sources, order, tol):
     """Sources well outside a unit box: their velocity on the downward check
     surface, times dc2de, is a density on the downward equivalent surface
