@@ -451,47 +451,93 @@ __global__ void __launch_bounds__(128) p2m_check_kernel(const Geometry g, int le
 }
 
 // ------------------------------------------------------------ gathered GEMM --
-// Y[slot(col)][row] (+)= scale * sum_t sum_k A_t[row][k] X[src(col, t)][k]
+// Y[slot(col)][row] (+)= scale * sum_t sum_k A_t[row][k] X_t[src(col, t)][k]
+//
+// A is either a stored matrix (the pseudo-inverses) or generated from K4
+// between check points (crad * surface) and a term's equivalent points
+// (off_t + erad_t * surface), with the source component scaled by qscale_t.
+// Terms: M2M, the 8 children of the column's box; M2L, the column's
+// interaction list (189 boxes of the 6 x 6 x 6 children of its parent's
+// neighbours that are not its own neighbours; which 189 depends on the
+// box's octant in its parent) and optionally the parent's local expansion.
+// The columns of M2L are grouped by octant; a CTA's 64 columns share one.
+// Terms are split over grid.z; each split writes its own partial and a
+// second kernel adds the partials in split order (deterministic).
 constexpr int GBM = 96, GBN = 64, GBK = 32, GTHREADS = 128;
-constexpr int kMaxTerms = 189;
+constexpr int kM2LTerms = 189;
 
-enum SourceRule { SRC_SAME = 0, SRC_CHILD = 1, SRC_NEIGHBOR = 2, SRC_PARENT = 3 };
+enum GenMode { GEN_STORED = 0, GEN_M2M = 1, GEN_M2L = 2 };
 
 struct GemmOp {
   double *Y;
   int ldy, rows, accumulate;
   double scale;
+  double *partial;  // nsplit > 1: [nsplit][nslots][ldy]
+  int nslots, nsplit;
   int ncols;
-  const int *cols;      // column -> box slot (output row of Y and lookups); null: identity
-  const int *box_keys;  // box slot -> Morton key at `level`
+  const int *cols;  // column -> box slot (null: identity)
+  int oct_col_start[9], oct_tile_start[9];  // column groups by octant (M2L); else one group
+  const int *box_keys;
   int level;
-  // A: stored (mode 0, rows x K, row-major) or generated (mode 1, K4)
   int mode;
   const double *A;
   int lda, K;
   const double *surf;
   int n;
-  double crad, erad, qscale;
-  int nterms;
-  double off[kMaxTerms][3];  // equivalent-surface centre of each term (generated)
-  int ioff[kMaxTerms][3];    // neighbour offset of each term (SRC_NEIGHBOR)
-  int rule;
-  const int *table;  // dense slot table of the sources' level
-  const double *X;
+  double crad;
+  int nterms, parent;
+  unsigned char m2l_idx[8][kM2LTerms];  // a*36 + b*6 + d of each interaction box, per octant
+  const int *table;   // sources of this level (M2L) or of the level below (M2M)
+  const int *table2;  // targets of the level above (the parent term)
+  const double *X, *X2;
   int ldx;
 };
 
-__device__ __forceinline__ int source_slot(const GemmOp &op, int slot, int t) {
-  if (op.rule == SRC_SAME) return slot;
+struct TermGeom {
+  double off[3];
+  double erad, qscale;
+};
+
+__device__ __forceinline__ TermGeom term_geom(const GemmOp &op, int oct, int t) {
+  TermGeom g;
+  const int cx = (oct >> 2) & 1, cy = (oct >> 1) & 1, cz = oct & 1;
+  if (op.mode == GEN_M2M) {
+    g.off[0] = (t & 4) ? 0.5 : -0.5;
+    g.off[1] = (t & 2) ? 0.5 : -0.5;
+    g.off[2] = (t & 1) ? 0.5 : -0.5;
+    g.erad = 0.5 * kRin;
+    g.qscale = 0.5;
+  } else if (op.parent && t == op.nterms - 1) {
+    // the parent's downward equivalent surface in this box's units
+    g.off[0] = cx ? -1.0 : 1.0;
+    g.off[1] = cy ? -1.0 : 1.0;
+    g.off[2] = cz ? -1.0 : 1.0;
+    g.erad = 2.0 * kRout;
+    g.qscale = 2.0;
+  } else {
+    const int idx = op.m2l_idx[oct][t];
+    g.off[0] = 2.0 * (idx / 36 - 2 - cx);
+    g.off[1] = 2.0 * ((idx / 6) % 6 - 2 - cy);
+    g.off[2] = 2.0 * (idx % 6 - 2 - cz);
+    g.erad = kRin;
+    g.qscale = 1.0;
+  }
+  return g;
+}
+
+__device__ __forceinline__ int source_slot(const GemmOp &op, int oct, int slot, int t) {
+  if (op.mode == GEN_STORED) return slot;
   const int key = op.box_keys[slot];
-  if (op.rule == SRC_CHILD) return op.table[(key << 3) | t];
-  if (op.rule == SRC_PARENT) return op.table[key >> 3];
+  if (op.mode == GEN_M2M) return op.table[(key << 3) | t];
+  if (op.parent && t == op.nterms - 1) return op.table2[key >> 3];
   int ix, iy, iz;
   unmorton(static_cast<uint32_t>(key), ix, iy, iz);
+  const int idx = op.m2l_idx[oct][t];
+  const int cx = (oct >> 2) & 1, cy = (oct >> 1) & 1, cz = oct & 1;
+  ix += idx / 36 - 2 - cx;
+  iy += (idx / 6) % 6 - 2 - cy;
+  iz += idx % 6 - 2 - cz;
   const int m = 1 << op.level;
-  ix += op.ioff[t][0];
-  iy += op.ioff[t][1];
-  iz += op.ioff[t][2];
   if (ix < 0 || iy < 0 || iz < 0 || ix >= m || iy >= m || iz >= m) return -1;
   return op.table[morton(ix, iy, iz)];
 }
@@ -502,7 +548,15 @@ __global__ void __launch_bounds__(GTHREADS) fmm_gemm_kernel(const __grid_constan
   __shared__ int s_src[GBN];
   __shared__ int s_any;
   const int tid = threadIdx.x;
-  const int row0 = blockIdx.x * GBM, col0 = blockIdx.y * GBN;
+  const int row0 = blockIdx.x * GBM;
+  // the column tile's octant group
+  const int tile = blockIdx.y;
+  int oct = 0;
+  while (oct < 7 && tile >= op.oct_tile_start[oct + 1]) ++oct;
+  const int col0 = op.oct_col_start[oct] + (tile - op.oct_tile_start[oct]) * GBN;
+  const int col_end = op.oct_col_start[oct + 1];
+  const int tps = (op.nterms + op.nsplit - 1) / op.nsplit;
+  const int t_lo = blockIdx.z * tps, t_hi = min(op.nterms, t_lo + tps);
   const int tr = tid >> 3, tc = tid & 7;  // 16 row groups of 6, 8 column groups of 8
   double acc[6][8];
 #pragma unroll
@@ -510,20 +564,24 @@ __global__ void __launch_bounds__(GTHREADS) fmm_gemm_kernel(const __grid_constan
 #pragma unroll
     for (int j = 0; j < 8; ++j) acc[i][j] = 0.0;
 
-  for (int t = 0; t < op.nterms; ++t) {
+  for (int t = t_lo; t < t_hi; ++t) {
     if (tid == 0) s_any = 0;
     __syncthreads();
     if (tid < GBN) {
       const int col = col0 + tid;
       int s = -1;
-      if (col < op.ncols) s = source_slot(op, op.cols ? op.cols[col] : col, t);
+      if (col < col_end) s = source_slot(op, oct, op.cols ? op.cols[col] : col, t);
       s_src[tid] = s;
       if (s >= 0) s_any = 1;
     }
     __syncthreads();
     if (!s_any) continue;
+    const bool par = op.mode == GEN_M2L && op.parent && t == op.nterms - 1;
+    const double *X = par ? op.X2 : op.X;
+    TermGeom g{};
+    if (op.mode != GEN_STORED) g = term_geom(op, oct, t);
     for (int k0 = 0; k0 < op.K; k0 += GBK) {
-      if (op.mode == 0) {
+      if (op.mode == GEN_STORED) {
         for (int e = tid; e < GBM * GBK; e += GTHREADS) {
           const int r = e / GBK, kk = e % GBK;
           const int row = row0 + r, k = k0 + kk;
@@ -536,9 +594,9 @@ __global__ void __launch_bounds__(GTHREADS) fmm_gemm_kernel(const __grid_constan
           const int cp = row0 / 3 + ci, ep = k0 / 4 + ei;
           double v[3][4];
           if (cp < op.n && ep < op.n) {
-            const double r0 = op.crad * op.surf[3 * cp] - (op.off[t][0] + op.erad * op.surf[3 * ep]);
-            const double r1 = op.crad * op.surf[3 * cp + 1] - (op.off[t][1] + op.erad * op.surf[3 * ep + 1]);
-            const double r2 = op.crad * op.surf[3 * cp + 2] - (op.off[t][2] + op.erad * op.surf[3 * ep + 2]);
+            const double r0 = op.crad * op.surf[3 * cp] - (g.off[0] + g.erad * op.surf[3 * ep]);
+            const double r1 = op.crad * op.surf[3 * cp + 1] - (g.off[1] + g.erad * op.surf[3 * ep + 1]);
+            const double r2 = op.crad * op.surf[3 * cp + 2] - (g.off[2] + g.erad * op.surf[3 * ep + 2]);
             const double ri = rsqrt_refined(fma(r0, r0, fma(r1, r1, r2 * r2)));
             const double ri3 = ri * ri * ri;
             const double r[3] = {r0, r1, r2};
@@ -546,7 +604,7 @@ __global__ void __launch_bounds__(GTHREADS) fmm_gemm_kernel(const __grid_constan
             for (int i = 0; i < 3; ++i) {
 #pragma unroll
               for (int j = 0; j < 3; ++j) v[i][j] = fma(r[i] * r[j], ri3, i == j ? ri : 0.0);
-              v[i][3] = r[i] * ri3 * op.qscale;
+              v[i][3] = r[i] * ri3 * g.qscale;
             }
           } else {
 #pragma unroll
@@ -563,7 +621,7 @@ __global__ void __launch_bounds__(GTHREADS) fmm_gemm_kernel(const __grid_constan
       for (int e = tid; e < GBN * GBK; e += GTHREADS) {
         const int c = e / GBK, kk = e % GBK;
         const int s = s_src[c], k = k0 + kk;
-        Xs[kk][c] = (s >= 0 && k < op.K) ? op.X[static_cast<int64_t>(s) * op.ldx + k] : 0.0;
+        Xs[kk][c] = (s >= 0 && k < op.K) ? X[static_cast<int64_t>(s) * op.ldx + k] : 0.0;
       }
       __syncthreads();
 #pragma unroll 4
@@ -584,16 +642,39 @@ __global__ void __launch_bounds__(GTHREADS) fmm_gemm_kernel(const __grid_constan
 #pragma unroll
   for (int j = 0; j < 8; ++j) {
     const int col = col0 + 8 * tc + j;
-    if (col >= op.ncols) continue;
+    if (col >= col_end) continue;
     const int slot = op.cols ? op.cols[col] : col;
-    double *y = op.Y + static_cast<int64_t>(slot) * op.ldy;
+    if (op.nsplit > 1) {
+      double *p = op.partial + (static_cast<int64_t>(blockIdx.z) * op.nslots + slot) * op.ldy;
 #pragma unroll
-    for (int i = 0; i < 6; ++i) {
-      const int row = row0 + 6 * tr + i;
-      if (row < op.rows) y[row] = op.accumulate ? fma(op.scale, acc[i][j], y[row]) : op.scale * acc[i][j];
+      for (int i = 0; i < 6; ++i) {
+        const int row = row0 + 6 * tr + i;
+        if (row < op.rows) p[row] = acc[i][j];
+      }
+    } else {
+      double *y = op.Y + static_cast<int64_t>(slot) * op.ldy;
+#pragma unroll
+      for (int i = 0; i < 6; ++i) {
+        const int row = row0 + 6 * tr + i;
+        if (row < op.rows) y[row] = op.accumulate ? fma(op.scale, acc[i][j], y[row]) : op.scale * acc[i][j];
+      }
     }
   }
 }
+
+// Y[slot][row] (+)= scale * sum over splits of the partials, in split order
+__global__ void split_sum_kernel(const double *__restrict__ partial, int nsplit, int64_t nslots, int ldy, int rows,
+                                 double scale, int accumulate, double *Y) {
+  const int64_t e = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (e >= nslots * rows) return;
+  const int64_t slot = e / rows;
+  const int row = static_cast<int>(e - slot * rows);
+  double v = 0.0;
+  for (int z = 0; z < nsplit; ++z) v += partial[(z * nslots + slot) * ldy + row];
+  double *y = Y + slot * ldy + row;
+  *y = accumulate ? fma(scale, v, *y) : scale * v;
+}
+
 
 // ------------------------------------------------------------ near field + L2P --
 struct NearArgs {
@@ -776,7 +857,7 @@ struct f3d_fmm {
   DevBuf x_sl, x_dl, x_trg;             // sorted coordinates
   DevBuf f_sl, d_dl, dl_tmp;            // sorted densities (3 and 9 per point)
   DevBuf sl_start, sl_end, dl_start, dl_end, trg_start, trg_end;
-  DevBuf flags, tile_sums, scalars, okv, ybuf, out_sorted, bbox;
+  DevBuf flags, tile_sums, scalars, okv, ybuf, out_sorted, bbox, split_partial;
   Level lev[kMaxDepth + 1];
 };
 
@@ -933,19 +1014,49 @@ int reserve_expansions(f3d_fmm *h) {
   return reserve(h->ybuf, ymax * n3 * sizeof(double));
 }
 
-int launch_gemm(const GemmOp &op, cudaStream_t st) {
+// Launches a gathered GEMM over all its column groups.  Columns without
+// groups (not M2L) form one group.  The terms are split over grid.z so that
+// the launch fills the GPU at least twice over (capped at 32 splits and at
+// 256 MiB of partial sums); the splits' partials are then added in order.
+int launch_gemm(GemmOp op, const int *group_start, DevBuf &partial, cudaStream_t st) {
   if (op.ncols <= 0) return F3D_OK;
-  const int64_t ytiles = (static_cast<int64_t>(op.ncols) + GBN - 1) / GBN;
-  if (ytiles > 65535) return F3D_ERR_TOO_LARGE;  // more boxes in a level than one launch covers
-  const dim3 grid(static_cast<unsigned>((op.rows + GBM - 1) / GBM), static_cast<unsigned>(ytiles));
+  int tiles = 0;
+  op.oct_tile_start[0] = 0;
+  for (int c = 0; c < 8; ++c) {
+    const int c0 = group_start ? group_start[c] : (c == 0 ? 0 : op.ncols);
+    const int c1 = group_start ? group_start[c + 1] : op.ncols;
+    op.oct_col_start[c] = c0;
+    tiles += (c1 - c0 + GBN - 1) / GBN;
+    op.oct_tile_start[c + 1] = tiles;
+  }
+  op.oct_col_start[8] = group_start ? group_start[8] : op.ncols;
+  if (tiles > 65535) return F3D_ERR_TOO_LARGE;  // more boxes in a level than one launch covers
+  const int rtiles = (op.rows + GBM - 1) / GBM;
+  const int64_t want = 4 * static_cast<int64_t>(sm_count());
+  int nsplit = static_cast<int>(std::min<int64_t>({(want + int64_t(rtiles) * tiles - 1) / (int64_t(rtiles) * tiles),
+                                                   int64_t(op.nterms), int64_t(32)}));
+  const size_t per_split = static_cast<size_t>(op.nslots) * op.ldy * sizeof(double);
+  nsplit = std::max(1, std::min<int>(nsplit, static_cast<int>((size_t(256) << 20) / std::max<size_t>(per_split, 1))));
+  op.nsplit = nsplit;
+  if (nsplit > 1) {
+    int rc = reserve(partial, nsplit * per_split);
+    if (rc) return rc;
+    op.partial = as<double>(partial);
+  }
+  const dim3 grid(static_cast<unsigned>(rtiles), static_cast<unsigned>(tiles), static_cast<unsigned>(nsplit));
   fmm_gemm_kernel<<<grid, GTHREADS, 0, st>>>(op);
+  if (nsplit > 1) {
+    const int64_t ne = static_cast<int64_t>(op.nslots) * op.rows;
+    split_sum_kernel<<<blocks(ne), 256, 0, st>>>(op.partial, nsplit, op.nslots, op.ldy, op.rows, op.scale,
+                                                 op.accumulate, op.Y);
+  }
   return launch_status();
 }
 
 GemmOp stored_op(const double *A, int rows, int K, const double *X, int ldx, double *Y, int ldy, int ncols,
                  double scale) {
   GemmOp op{};
-  op.mode = 0;
+  op.mode = GEN_STORED;
   op.A = A;
   op.lda = K;
   op.K = K;
@@ -955,9 +1066,9 @@ GemmOp stored_op(const double *A, int rows, int K, const double *X, int ldx, dou
   op.Y = Y;
   op.ldy = ldy;
   op.ncols = ncols;
+  op.nslots = ncols;
   op.scale = scale;
   op.nterms = 1;
-  op.rule = SRC_SAME;
   return op;
 }
 
@@ -1000,7 +1111,7 @@ int f3d_fmm_destroy(f3d_fmm *h) {
   for (DevBuf *b : {&h->surf, &h->uc2ue, &h->dc2de, &h->kv_sl, &h->kv_dl, &h->kv_trg, &h->x_sl, &h->x_dl, &h->x_trg,
                     &h->f_sl, &h->d_dl, &h->dl_tmp, &h->sl_start, &h->sl_end, &h->dl_start, &h->dl_end,
                     &h->trg_start, &h->trg_end, &h->flags, &h->tile_sums, &h->scalars, &h->okv, &h->ybuf,
-                    &h->out_sorted, &h->bbox})
+                    &h->out_sorted, &h->bbox, &h->split_partial})
     release(*b);
   for (Level &lv : h->lev)
     for (DevBuf *b : {&lv.src_table, &lv.trg_table, &lv.src_keys, &lv.trg_keys, &lv.trg_cols, &lv.phi, &lv.psi})
@@ -1119,34 +1230,27 @@ int f3d_fmm_evaluate(f3d_fmm *h, const double *sl_density, const double *dl_norm
   double *Y = as<double>(h->ybuf);
   // upward pass: leaf check potentials, then equivalent densities
   Level &leaf = h->lev[L];
+  DevBuf &part = h->split_partial;
   {
     const dim3 grid(static_cast<unsigned>(leaf.nsrc), static_cast<unsigned>((n + 127) / 128));
     p2m_check_kernel<<<grid, 128, 0, st>>>(h->geo, L, as<int>(leaf.src_keys), src, surf, n, Y);
     const double hL = h->geo.width / static_cast<double>(2 << L);
     if ((rc = launch_status()) ||
         (rc = launch_gemm(stored_op(as<double>(h->uc2ue), n4, n3, Y, n3, as<double>(leaf.phi), n4, leaf.nsrc, hL),
-                          st)))
+                          nullptr, part, st)))
       return rc;
   }
   for (int l = L - 1; l >= 2; --l) {
     Level &lv = h->lev[l], &below = h->lev[l + 1];
     if (lv.nsrc == 0) continue;
     GemmOp op{};
-    op.mode = 1;
+    op.mode = GEN_M2M;
     op.rows = n3;
     op.K = n4;
     op.surf = surf;
     op.n = n;
     op.crad = kRout;
-    op.erad = 0.5 * kRin;
-    op.qscale = 0.5;
     op.nterms = 8;
-    for (int c = 0; c < 8; ++c) {
-      op.off[c][0] = (c & 4) ? 0.5 : -0.5;
-      op.off[c][1] = (c & 2) ? 0.5 : -0.5;
-      op.off[c][2] = (c & 1) ? 0.5 : -0.5;
-    }
-    op.rule = SRC_CHILD;
     op.table = as<int>(below.src_table);
     op.box_keys = as<int>(lv.src_keys);
     op.level = l;
@@ -1155,87 +1259,59 @@ int f3d_fmm_evaluate(f3d_fmm *h, const double *sl_density, const double *dl_norm
     op.Y = Y;
     op.ldy = n3;
     op.ncols = lv.nsrc;
+    op.nslots = lv.nsrc;
     op.scale = 1.0;
-    if ((rc = launch_gemm(op, st)) ||
-        (rc = launch_gemm(stored_op(as<double>(h->uc2ue), n4, n3, Y, n3, as<double>(lv.phi), n4, lv.nsrc, 1.0), st)))
+    if ((rc = launch_gemm(op, nullptr, part, st)) ||
+        (rc = launch_gemm(stored_op(as<double>(h->uc2ue), n4, n3, Y, n3, as<double>(lv.phi), n4, lv.nsrc, 1.0),
+                          nullptr, part, st)))
       return rc;
   }
-  // downward pass: interaction lists, the parent's local expansion, then
-  // equivalent densities
+  // downward pass: the interaction lists and the parent's local expansion
+  // in one launch per level, then the equivalent densities
   for (int l = 2; l <= L; ++l) {
     Level &lv = h->lev[l];
     if (lv.ntrg == 0) continue;
+    GemmOp op{};
+    op.mode = GEN_M2L;
+    op.rows = n3;
+    op.K = n4;
+    op.surf = surf;
+    op.n = n;
+    op.crad = kRin;
+    op.table = as<int>(lv.src_table);
+    op.box_keys = as<int>(lv.trg_keys);
+    op.level = l;
+    op.X = as<double>(lv.phi);
+    op.ldx = n4;
+    op.Y = Y;
+    op.ldy = n3;
+    op.cols = as<int>(lv.trg_cols);
+    op.ncols = lv.ntrg;
+    op.nslots = lv.ntrg;
+    op.scale = 1.0;
+    op.accumulate = 0;
     for (int c = 0; c < 8; ++c) {
-      const int c0 = lv.oct_start[c], c1 = lv.oct_start[c + 1];
-      if (c1 == c0) continue;
       const int cx = (c >> 2) & 1, cy = (c >> 1) & 1, cz = c & 1;
-      GemmOp op{};
-      op.mode = 1;
-      op.rows = n3;
-      op.K = n4;
-      op.surf = surf;
-      op.n = n;
-      op.crad = kRin;
-      op.erad = kRin;
-      op.qscale = 1.0;
-      op.rule = SRC_NEIGHBOR;
-      op.table = as<int>(lv.src_table);
-      op.box_keys = as<int>(lv.trg_keys);
-      op.level = l;
-      op.X = as<double>(lv.phi);
-      op.ldx = n4;
-      op.Y = Y;
-      op.ldy = n3;
-      op.cols = as<int>(lv.trg_cols) + c0;
-      op.ncols = c1 - c0;
-      op.scale = 1.0;
-      op.accumulate = 0;
       int t = 0;
-      for (int ox = -2 - cx; ox <= 3 - cx; ++ox)
-        for (int oy = -2 - cy; oy <= 3 - cy; ++oy)
-          for (int oz = -2 - cz; oz <= 3 - cz; ++oz) {
+      for (int a = 0; a < 6; ++a)
+        for (int b = 0; b < 6; ++b)
+          for (int d = 0; d < 6; ++d) {
+            const int ox = a - 2 - cx, oy = b - 2 - cy, oz = d - 2 - cz;
             if (std::max(std::abs(ox), std::max(std::abs(oy), std::abs(oz))) < 2) continue;
-            op.ioff[t][0] = ox;
-            op.ioff[t][1] = oy;
-            op.ioff[t][2] = oz;
-            op.off[t][0] = 2.0 * ox;
-            op.off[t][1] = 2.0 * oy;
-            op.off[t][2] = 2.0 * oz;
-            ++t;
+            op.m2l_idx[c][t++] = static_cast<unsigned char>(36 * a + 6 * b + d);
           }
-      op.nterms = t;  // 189
-      if ((rc = launch_gemm(op, st))) return rc;
-      if (l > 2) {
-        GemmOp pp{};
-        pp.mode = 1;
-        pp.rows = n3;
-        pp.K = n4;
-        pp.surf = surf;
-        pp.n = n;
-        pp.crad = kRin;
-        pp.erad = 2.0 * kRout;
-        pp.qscale = 2.0;
-        pp.nterms = 1;
-        // the parent's centre in this box's units
-        pp.off[0][0] = cx ? -1.0 : 1.0;
-        pp.off[0][1] = cy ? -1.0 : 1.0;
-        pp.off[0][2] = cz ? -1.0 : 1.0;
-        pp.rule = SRC_PARENT;
-        pp.table = as<int>(h->lev[l - 1].trg_table);
-        pp.box_keys = as<int>(lv.trg_keys);
-        pp.level = l;
-        pp.X = as<double>(h->lev[l - 1].psi);
-        pp.ldx = n4;
-        pp.Y = Y;
-        pp.ldy = n3;
-        pp.cols = as<int>(lv.trg_cols) + c0;
-        pp.ncols = c1 - c0;
-        pp.scale = 1.0;
-        pp.accumulate = 1;
-        if ((rc = launch_gemm(pp, st))) return rc;
-      }
+      if (t != kM2LTerms) return F3D_ERR_ARG;
     }
-    if ((rc = launch_gemm(stored_op(as<double>(h->dc2de), n4, n3, Y, n3, as<double>(lv.psi), n4, lv.ntrg, 1.0), st)))
+    op.nterms = kM2LTerms;
+    if (l > 2) {
+      op.parent = 1;
+      op.nterms = kM2LTerms + 1;
+      op.table2 = as<int>(h->lev[l - 1].trg_table);
+      op.X2 = as<double>(h->lev[l - 1].psi);
+    }
+    if ((rc = launch_gemm(op, lv.oct_start, part, st)) ||
+        (rc = launch_gemm(stored_op(as<double>(h->dc2de), n4, n3, Y, n3, as<double>(lv.psi), n4, lv.ntrg, 1.0),
+                          nullptr, part, st)))
       return rc;
   }
   // near field and the local expansions at the targets
