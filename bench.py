@@ -958,6 +958,126 @@ def block_pc_measure(args, dev, steps, warmup, cpu_seconds):
             "cpu_sample": f"scipy.linalg.lu_factor + lu_solve over all {args.nblocks} blocks, {nb_cpu} pass(es)"}
 
 
+def fmm_workload(n: int, seed: int = 0):
+    """fiber3d's own FMM check (kernels/test_stkfmm.py:39-53): n single-layer
+    sources, n double-layer sources and n targets uniform in a cube of side
+    (4 pi 2n / (3e-3))^(1/3) (volume fraction 1e-3), N(0, 1) densities and
+    normals.  Seeded synthetic stand-in of the same shape."""
+    rng = np.random.default_rng(seed)
+    side = (4 * np.pi * 2 * n / (3 * 1e-3)) ** (1 / 3)
+    return dict(sl=rng.random((n, 3)) * side, dl=rng.random((n, 3)) * side, trg=rng.random((n, 3)) * side,
+                f=rng.normal(size=(n, 3)), nrm=rng.normal(size=(n, 3)), dens=rng.normal(size=(n, 3)), side=side)
+
+
+def fmm_arm(args, rank, world, local):
+    """The FMM (fiber3d's useFMM path, kernels.py:1298-1485): one step = one
+    evaluation of the single + double layer at the targets on a built tree.
+    value: equivalent pair interactions per second, (n_SL + n_DL) n_trg / time.
+    Reported beside it: the tree build, the direct GPU sum of the same
+    velocities and the FMM's error against it, the far-field roofline."""
+    import torch
+    from fiber3d_b200 import fmm as F, kernels as K, replicas, stkfmm
+    from fiber3d_b200 import _lib as L
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    n = args.fmm_n
+    w = fmm_workload(n, seed=rank)
+    t = {k: torch.as_tensor(v, device=dev) for k, v in w.items() if k != "side"}
+    m = F.FMM(order=args.fmm_order, max_pts=args.fmm_max_pts, device=dev)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    m.set_points(t["sl"], t["dl"], t["trg"])
+    torch.cuda.synchronize()
+    setup_ms = (time.perf_counter() - t0) * 1e3
+    out = torch.empty(3 * n, dtype=torch.float64, device=dev)
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=dev)
+    evaluate = lambda: m.evaluate(sl_density=t["f"], dl_normal=t["nrm"], dl_density=t["dens"], out=out)
+    for _ in range(args.warmup):
+        evaluate()
+    torch.cuda.synchronize()
+    replicas.barrier()
+    evs = []
+    with ClockSampler(local) as clk:
+        for _ in range(args.steps):
+            flush.fill_(1)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            evaluate()
+            e1.record()
+            evs.append((e0, e1))
+        torch.cuda.synchronize()
+    replicas.barrier()
+    ms = [a.elapsed_time(b) for a, b in evs]
+    total_ms, = replicas.max_over_ranks([sum(ms)], dev)
+    pairs = 2 * n * n
+    value = replicas.aggregate_rate(pairs, args.steps, world, total_ms)
+    # the direct sum of the same velocities (exact FP64, coincident pairs excluded)
+    ref = torch.zeros(3 * n, dtype=torch.float64, device=dev)
+    kw = dict(self_mode="skip_close", epsilon_distance=1e-150, reg=0.0, out=ref, accumulate=True)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    K.pair_sum("oseen", t["sl"], t["trg"], t["f"], **kw)
+    K.pair_sum("stresslet", t["dl"], t["trg"], t["dens"], t["nrm"], **kw)
+    e1.record()
+    e1.synchronize()
+    direct_ms = e0.elapsed_time(e1)
+    err_l2 = float(torch.linalg.vector_norm(out - ref) / torch.linalg.vector_norm(ref))
+    err_inf = float((out - ref).abs().max() / ref.abs().max())
+    peak64, _ = measured_peak(L, "fp64", torch, local)
+    flops = m.far_field_flops()
+    info = m.tree_info()
+    # e2e: fiber3d's combined call on host arrays with an stkfmm handle (the
+    # tree is built on the first call and kept while the points are the same)
+    h = stkfmm.STKFMM(args.fmm_order, args.fmm_max_pts, stkfmm.PAXIS.NONE, stkfmm.KERNEL(stkfmm.KERNEL.PVel))
+    call = lambda: K.single_double_layer_kernel_source_target_stkfmm(w["sl"], w["dl"], w["trg"], w["nrm"], w["f"],
+                                                                     w["dens"], fmm_PVel=h)
+    for _ in range(2):
+        call()
+    te = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        call()
+        te.append(time.perf_counter() - t0)
+    e2e_s = statistics.median(te)
+    # CPU: the C/OpenMP restatement of the direct sums on a target sample
+    from oracle import pairs_c
+    hc = host_cores()
+    nt_cpu = min(n, 256)
+    t0 = time.perf_counter()
+    pairs_c.pair_sum("oseen", w["sl"], w["trg"][:nt_cpu], w["f"], epsilon_distance=0.0, reg=0.0)
+    pairs_c.pair_sum("stresslet", w["dl"], w["trg"][:nt_cpu], w["dens"], w["nrm"], epsilon_distance=0.0, reg=0.0)
+    cpu_rate = 2 * n * nt_cpu / (time.perf_counter() - t0)
+    line = {
+        "metric": f"FMM equivalent Stokes pair interactions per second (FP64, order {args.fmm_order})",
+        "value": value, "unit": "pairs/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic (seeded): fiber3d's STKFMM check shape (kernels/test_stkfmm.py)",
+        "config": {"workload": "fmm", "n_single_layer": n, "n_double_layer": n, "n_targets": n,
+                   "cube_side": w["side"], "order": args.fmm_order, "max_pts": args.fmm_max_pts,
+                   "l2": "flushed between steps (256 MiB write, outside the event pairs)"},
+        "parallelism": f"replicas x{world}",
+        "tree": {**info, "setup_ms": setup_ms},
+        "accuracy_vs_direct": {"rel_l2": err_l2, "rel_linf": err_inf},
+        "direct_gpu_ms": direct_ms, "speedup_vs_direct_gpu": direct_ms / (total_ms / args.steps),
+        "roofline": {"bound": "fp64", "kernel": "fmm_gemm_kernel (interaction lists)",
+                     "achieved": flops / (total_ms / args.steps * 1e-3) / 1e12, "peak": peak64 / 1e12,
+                     "unit": "TFLOP/s", "frac": flops / (total_ms / args.steps * 1e-3) / peak64,
+                     "note": "far-field flops per evaluation (2 (3n)(4n) per interaction-list entry) over the "
+                             "whole evaluation's time: a lower bound of the GEMM kernel's own rate"},
+        "cpu_baseline": {"value": cpu_rate, "unit": "pairs/s", "cores": hc["threads"], **hc, "kind": "port",
+                         "sample": f"direct sums onto {nt_cpu} targets (C/OpenMP restatement of fiber3d's numba "
+                                   "loops, the sums fiber3d checks STKFMM against)"},
+        "e2e": {"value": pairs / e2e_s, "unit": "pairs/s", "h2d_bytes_per_step": 18 * n * 8,
+                "d2h_bytes_per_step": 3 * n * 8,
+                "path": "fiber3d_b200.kernels.single_double_layer_kernel_source_target_stkfmm, numpy in/out, "
+                        "stkfmm handle"},
+        "clocks": clk.summary(),
+        "gpu_launches": m.last_launches() * args.steps,
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 def block_pc_arm(args, rank, world, local):
     import torch
     torch.cuda.set_device(local)
@@ -1026,7 +1146,10 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="stresslet_sphere",
                     choices=["stresslet_sphere", "oseen_fibers", "hydro_step", "block_pc",
-                             "surface_quadrature"])
+                             "surface_quadrature", "fmm"])
+    ap.add_argument("--fmm-n", type=int, default=1000000, help="points of each kind of the FMM workload")
+    ap.add_argument("--fmm-order", type=int, default=8)
+    ap.add_argument("--fmm-max-pts", type=int, default=1000)
     ap.add_argument("--nblocks", type=int, default=2000)
     ap.add_argument("--train-seeds", type=int, nargs="*", default=list(range(11, 19)))
     ap.add_argument("--train-steps", type=int, default=40)
@@ -1068,6 +1191,8 @@ def main():
             block_pc_arm(args, rank, world, local)
         elif args.workload == "surface_quadrature":
             quadrature_arm(args, rank, world, local)
+        elif args.workload == "fmm":
+            fmm_arm(args, rank, world, local)
         else:
             gpu_arm(args, rank, world, local)
     finally:

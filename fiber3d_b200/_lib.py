@@ -97,7 +97,8 @@ SIGNATURES: dict[str, list] = {
     "f3d_fmm_set_box": [_P, _P, _D],
     "f3d_fmm_set_points": [_P, _I64, _P, _I64, _P, _I64, _P, _P],
     "f3d_fmm_evaluate": [_P, _P, _P, _P, _P, _P, _D, _P],
-    "f3d_fmm_tree_info": [_P, _P, _P, _P, _P],
+    "f3d_fmm_tree_info": [_P, _P, _P, _P, _P, _P],
+    "f3d_fmm_last_launches": [_P, _P],
     "f3d_body_residual": [ctypes.c_int32, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P],
     "f3d_surface_dense": [_I, _P, _P, _P, _P, _P, _P, _I64, _I64, _D, _D, _D, _P],
     "f3d_rotate_blocks": [_P, _P, _P, _P, ctypes.c_int32, _I, _P],

@@ -304,6 +304,28 @@ __global__ void octant_keys_kernel(const int *__restrict__ keys, int nbox, int64
   atomicAdd(&oct_count[oct], 1u);
 }
 
+// number of non-empty source boxes in the interaction lists of a level's
+// target boxes (the M2L work: each is one 3n x 4n block product)
+__global__ void count_m2l_kernel(const int *__restrict__ trg_keys, int ntrg, const int *__restrict__ src_table,
+                                 int level, unsigned long long *count) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  unsigned c = 0;
+  if (i < ntrg) {
+    int bx, by, bz;
+    unmorton(static_cast<uint32_t>(trg_keys[i]), bx, by, bz);
+    const int px = bx >> 1, py = by >> 1, pz = bz >> 1, m = 1 << level;
+    for (int x = 2 * px - 2; x < 2 * px + 4; ++x)
+      for (int y = 2 * py - 2; y < 2 * py + 4; ++y)
+        for (int z = 2 * pz - 2; z < 2 * pz + 4; ++z) {
+          if (x < 0 || y < 0 || z < 0 || x >= m || y >= m || z >= m) continue;
+          if (max(abs(x - bx), max(abs(y - by), abs(z - bz))) < 2) continue;
+          c += src_table[morton(x, y, z)] >= 0;
+        }
+  }
+  for (int d = 16; d > 0; d >>= 1) c += __shfl_down_sync(0xffffffffu, c, d);
+  if ((threadIdx.x & 31) == 0 && c) atomicAdd(count, static_cast<unsigned long long>(c));
+}
+
 __global__ void low_words_kernel(const uint64_t *__restrict__ kv, int64_t n, int *out) {
   const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
   if (i < n) out[i] = static_cast<int>(static_cast<uint32_t>(kv[i]));
@@ -858,6 +880,8 @@ struct f3d_fmm {
   DevBuf f_sl, d_dl, dl_tmp;            // sorted densities (3 and 9 per point)
   DevBuf sl_start, sl_end, dl_start, dl_end, trg_start, trg_end;
   DevBuf flags, tile_sums, scalars, okv, ybuf, out_sorted, bbox, split_partial;
+  int64_t m2l_pairs = 0;  // non-empty interaction-list entries over all levels
+  int launches = 0;       // kernels the last evaluate launched
   Level lev[kMaxDepth + 1];
 };
 
@@ -997,6 +1021,18 @@ int build_tree(f3d_fmm *h, cudaStream_t st) {
     lv.oct_start[0] = 0;
     for (int c = 0; c < 8; ++c) lv.oct_start[c + 1] = lv.oct_start[c] + static_cast<int>(ocount[c]);
   }
+  // the far-field work of this tree, for reports
+  unsigned long long *pc = reinterpret_cast<unsigned long long *>(as<unsigned>(h->scalars) + 48);
+  if (cudaMemsetAsync(pc, 0, sizeof(unsigned long long), st) != cudaSuccess) return F3D_ERR_CUDA;
+  for (int l = 2; l <= L; ++l) {
+    Level &lv = h->lev[l];
+    if (lv.ntrg > 0)
+      count_m2l_kernel<<<blocks(lv.ntrg), 256, 0, st>>>(as<int>(lv.trg_keys), lv.ntrg, as<int>(lv.src_table), l, pc);
+  }
+  if ((rc = launch_status())) return rc;
+  unsigned long long pairs = 0;
+  if ((rc = sync_read(&pairs, pc, sizeof(pairs), st))) return rc;
+  h->m2l_pairs = static_cast<int64_t>(pairs);
   return F3D_OK;
 }
 
@@ -1018,7 +1054,7 @@ int reserve_expansions(f3d_fmm *h) {
 // groups (not M2L) form one group.  The terms are split over grid.z so that
 // the launch fills the GPU at least twice over (capped at 32 splits and at
 // 256 MiB of partial sums); the splits' partials are then added in order.
-int launch_gemm(GemmOp op, const int *group_start, DevBuf &partial, cudaStream_t st) {
+int launch_gemm(GemmOp op, const int *group_start, DevBuf &partial, cudaStream_t st, int *launches) {
   if (op.ncols <= 0) return F3D_OK;
   int tiles = 0;
   op.oct_tile_start[0] = 0;
@@ -1045,10 +1081,12 @@ int launch_gemm(GemmOp op, const int *group_start, DevBuf &partial, cudaStream_t
   }
   const dim3 grid(static_cast<unsigned>(rtiles), static_cast<unsigned>(tiles), static_cast<unsigned>(nsplit));
   fmm_gemm_kernel<<<grid, GTHREADS, 0, st>>>(op);
+  ++*launches;
   if (nsplit > 1) {
     const int64_t ne = static_cast<int64_t>(op.nslots) * op.rows;
     split_sum_kernel<<<blocks(ne), 256, 0, st>>>(op.partial, nsplit, op.nslots, op.ldy, op.rows, op.scale,
                                                  op.accumulate, op.Y);
+    ++*launches;
   }
   return launch_status();
 }
@@ -1206,15 +1244,21 @@ int f3d_fmm_evaluate(f3d_fmm *h, const double *sl_density, const double *dl_norm
       (rc = reserve(h->d_dl, std::max<size_t>(ndl, 1) * 9 * sizeof(double))) ||
       (rc = reserve(h->out_sorted, static_cast<size_t>(ntrg) * 3 * sizeof(double))))
     return rc;
-  if (nsl) gather_kernel<<<blocks(3 * nsl), 256, 0, st>>>(sl_density, as<uint64_t>(h->kv_sl), nsl, 3, as<double>(h->f_sl));
+  h->launches = 0;
+  if (nsl) {
+    gather_kernel<<<blocks(3 * nsl), 256, 0, st>>>(sl_density, as<uint64_t>(h->kv_sl), nsl, 3, as<double>(h->f_sl));
+    ++h->launches;
+  }
   if (ndl) {
     const double *D = dl_tensor;
     if (!D) {
       if ((rc = reserve(h->dl_tmp, static_cast<size_t>(ndl) * 9 * sizeof(double)))) return rc;
       dl_tensor_kernel<<<blocks(9 * ndl), 256, 0, st>>>(dl_normal, dl_density, ndl, as<double>(h->dl_tmp));
+      ++h->launches;
       D = as<double>(h->dl_tmp);
     }
     gather_kernel<<<blocks(9 * ndl), 256, 0, st>>>(D, as<uint64_t>(h->kv_dl), ndl, 9, as<double>(h->d_dl));
+    ++h->launches;
   }
   if ((rc = launch_status())) return rc;
   SourceSet src{};
@@ -1234,10 +1278,11 @@ int f3d_fmm_evaluate(f3d_fmm *h, const double *sl_density, const double *dl_norm
   {
     const dim3 grid(static_cast<unsigned>(leaf.nsrc), static_cast<unsigned>((n + 127) / 128));
     p2m_check_kernel<<<grid, 128, 0, st>>>(h->geo, L, as<int>(leaf.src_keys), src, surf, n, Y);
+    ++h->launches;
     const double hL = h->geo.width / static_cast<double>(2 << L);
     if ((rc = launch_status()) ||
         (rc = launch_gemm(stored_op(as<double>(h->uc2ue), n4, n3, Y, n3, as<double>(leaf.phi), n4, leaf.nsrc, hL),
-                          nullptr, part, st)))
+                          nullptr, part, st, &h->launches)))
       return rc;
   }
   for (int l = L - 1; l >= 2; --l) {
@@ -1261,9 +1306,9 @@ int f3d_fmm_evaluate(f3d_fmm *h, const double *sl_density, const double *dl_norm
     op.ncols = lv.nsrc;
     op.nslots = lv.nsrc;
     op.scale = 1.0;
-    if ((rc = launch_gemm(op, nullptr, part, st)) ||
+    if ((rc = launch_gemm(op, nullptr, part, st, &h->launches)) ||
         (rc = launch_gemm(stored_op(as<double>(h->uc2ue), n4, n3, Y, n3, as<double>(lv.phi), n4, lv.nsrc, 1.0),
-                          nullptr, part, st)))
+                          nullptr, part, st, &h->launches)))
       return rc;
   }
   // downward pass: the interaction lists and the parent's local expansion
@@ -1309,9 +1354,9 @@ int f3d_fmm_evaluate(f3d_fmm *h, const double *sl_density, const double *dl_norm
       op.table2 = as<int>(h->lev[l - 1].trg_table);
       op.X2 = as<double>(h->lev[l - 1].psi);
     }
-    if ((rc = launch_gemm(op, lv.oct_start, part, st)) ||
+    if ((rc = launch_gemm(op, lv.oct_start, part, st, &h->launches)) ||
         (rc = launch_gemm(stored_op(as<double>(h->dc2de), n4, n3, Y, n3, as<double>(lv.psi), n4, lv.ntrg, 1.0),
-                          nullptr, part, st)))
+                          nullptr, part, st, &h->launches)))
       return rc;
   }
   // near field and the local expansions at the targets
@@ -1329,14 +1374,23 @@ int f3d_fmm_evaluate(f3d_fmm *h, const double *sl_density, const double *dl_norm
   na.n = n;
   na.out = as<double>(h->out_sorted);
   near_l2p_kernel<<<static_cast<unsigned>(leaf.ntrg), 128, 0, st>>>(na);
+  h->launches += 2;  // with the scatter below
   scatter_kernel<<<blocks(3 * ntrg), 256, 0, st>>>(as<double>(h->out_sorted), as<uint64_t>(h->kv_trg), ntrg,
                                                    1.0 / eta, out);
   return launch_status();
 }
 
-int f3d_fmm_tree_info(const f3d_fmm *h, int *depth, int64_t *src_leaves, int64_t *trg_leaves, double *box) {
+int f3d_fmm_last_launches(const f3d_fmm *h, int *launches) {
+  if (!h || !launches) return F3D_ERR_NULL;
+  *launches = h->launches;
+  return F3D_OK;
+}
+
+int f3d_fmm_tree_info(const f3d_fmm *h, int *depth, int64_t *src_leaves, int64_t *trg_leaves, double *box,
+                      int64_t *m2l_pairs) {
   if (!h || !depth) return F3D_ERR_NULL;
   *depth = h->depth;
+  if (m2l_pairs) *m2l_pairs = h->depth ? h->m2l_pairs : 0;
   if (src_leaves) *src_leaves = h->depth ? h->lev[h->depth].nsrc : 0;
   if (trg_leaves) *trg_leaves = h->depth ? h->lev[h->depth].ntrg : 0;
   if (box) {

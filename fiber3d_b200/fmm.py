@@ -164,8 +164,20 @@ class FMM:
 
     def tree_info(self) -> dict:
         depth = ctypes.c_int(0)
-        ns, nt = ctypes.c_int64(0), ctypes.c_int64(0)
+        ns, nt, m2l = ctypes.c_int64(0), ctypes.c_int64(0), ctypes.c_int64(0)
         box = (ctypes.c_double * 4)()
-        _lib.call("f3d_fmm_tree_info", self._h, ctypes.byref(depth), ctypes.byref(ns), ctypes.byref(nt), box)
+        _lib.call("f3d_fmm_tree_info", self._h, ctypes.byref(depth), ctypes.byref(ns), ctypes.byref(nt), box,
+                  ctypes.byref(m2l))
         return {"depth": depth.value, "source_leaves": ns.value, "target_leaves": nt.value,
-                "box_lo": list(box[:3]), "box_width": box[3]}
+                "box_lo": list(box[:3]), "box_width": box[3], "m2l_pairs": m2l.value}
+
+    def last_launches(self) -> int:
+        """Kernels the last evaluate launched."""
+        v = ctypes.c_int(0)
+        _lib.call("f3d_fmm_last_launches", self._h, ctypes.byref(v))
+        return v.value
+
+    def far_field_flops(self) -> float:
+        """Algorithmic FP64 flops of the interaction lists per evaluation:
+        2 (3n)(4n) per non-empty entry (the dominant far-field work)."""
+        return 2.0 * 3 * self.nsurf * 4 * self.nsurf * self.tree_info()["m2l_pairs"]

@@ -694,8 +694,13 @@ int f3d_fmm_set_points(f3d_fmm *fmm, int64_t nsl, const double *src_sl, int64_t 
 int f3d_fmm_evaluate(f3d_fmm *fmm, const double *sl_density, const double *dl_normal, const double *dl_density,
                      const double *dl_tensor, double *out, double eta, void *stream);
 /* The tree of the last set_points: depth, non-empty source and target
-   leaves, box (lo[3], width).                                            */
-int f3d_fmm_tree_info(const f3d_fmm *fmm, int *depth, int64_t *src_leaves, int64_t *trg_leaves, double *box);
+   leaves, box (lo[3], width), and the number of non-empty entries of all
+   target boxes' interaction lists (each one 3n x 4n block product of the
+   far field); any output pointer but depth may be NULL.                   */
+int f3d_fmm_tree_info(const f3d_fmm *fmm, int *depth, int64_t *src_leaves, int64_t *trg_leaves, double *box,
+                      int64_t *m2l_pairs);
+/* Kernels the last f3d_fmm_evaluate launched (for launch accounting). */
+int f3d_fmm_last_launches(const f3d_fmm *fmm, int *launches);
 
 #ifdef __cplusplus
 }
