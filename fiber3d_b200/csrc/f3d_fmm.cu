@@ -579,7 +579,9 @@ __global__ void __launch_bounds__(GTHREADS) fmm_gemm_kernel(const __grid_constan
   const int col_end = op.oct_col_start[oct + 1];
   const int tps = (op.nterms + op.nsplit - 1) / op.nsplit;
   const int t_lo = blockIdx.z * tps, t_hi = min(op.nterms, t_lo + tps);
-  const int tr = tid >> 3, tc = tid & 7;  // 16 row groups of 6, 8 column groups of 8
+  // thread (tr, tc) owns rows tr + 16 i (i < 6) and columns tc + 8 j (j < 8):
+  // the 8 column groups of a warp read 8 consecutive words (no bank conflict)
+  const int tr = tid >> 3, tc = tid & 7;
   double acc[6][8];
 #pragma unroll
   for (int i = 0; i < 6; ++i)
@@ -611,8 +613,9 @@ __global__ void __launch_bounds__(GTHREADS) fmm_gemm_kernel(const __grid_constan
         }
       } else {
         // 32 check points x 8 equivalent points: one 3 x 4 block of K4 each
+        // (a warp takes 32 consecutive check points of one equivalent point)
         for (int pp = tid; pp < (GBM / 3) * (GBK / 4); pp += GTHREADS) {
-          const int ci = pp / (GBK / 4), ei = pp % (GBK / 4);
+          const int ci = pp % (GBM / 3), ei = pp / (GBM / 3);
           const int cp = row0 / 3 + ci, ep = k0 / 4 + ei;
           double v[3][4];
           if (cp < op.n && ep < op.n) {
@@ -650,9 +653,9 @@ __global__ void __launch_bounds__(GTHREADS) fmm_gemm_kernel(const __grid_constan
       for (int kk = 0; kk < GBK; ++kk) {
         double a[6], x[8];
 #pragma unroll
-        for (int i = 0; i < 6; ++i) a[i] = As[kk][6 * tr + i];
+        for (int i = 0; i < 6; ++i) a[i] = As[kk][tr + 16 * i];
 #pragma unroll
-        for (int j = 0; j < 8; ++j) x[j] = Xs[kk][8 * tc + j];
+        for (int j = 0; j < 8; ++j) x[j] = Xs[kk][tc + 8 * j];
 #pragma unroll
         for (int i = 0; i < 6; ++i)
 #pragma unroll
@@ -663,21 +666,21 @@ __global__ void __launch_bounds__(GTHREADS) fmm_gemm_kernel(const __grid_constan
   }
 #pragma unroll
   for (int j = 0; j < 8; ++j) {
-    const int col = col0 + 8 * tc + j;
+    const int col = col0 + tc + 8 * j;
     if (col >= col_end) continue;
     const int slot = op.cols ? op.cols[col] : col;
     if (op.nsplit > 1) {
       double *p = op.partial + (static_cast<int64_t>(blockIdx.z) * op.nslots + slot) * op.ldy;
 #pragma unroll
       for (int i = 0; i < 6; ++i) {
-        const int row = row0 + 6 * tr + i;
+        const int row = row0 + tr + 16 * i;
         if (row < op.rows) p[row] = acc[i][j];
       }
     } else {
       double *y = op.Y + static_cast<int64_t>(slot) * op.ldy;
 #pragma unroll
       for (int i = 0; i < 6; ++i) {
-        const int row = row0 + 6 * tr + i;
+        const int row = row0 + tr + 16 * i;
         if (row < op.rows) y[row] = op.accumulate ? fma(op.scale, acc[i][j], y[row]) : op.scale * acc[i][j];
       }
     }
