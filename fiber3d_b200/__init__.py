@@ -15,6 +15,9 @@ Modules
   warmstart     GMRES initial guess: extrapolation + learned per-fiber correction
   flowstart     the (positions, background velocity) -> (tensions, forces)
                 network form of the learned guess
+  fmm           GPU fast multipole method for the Stokes single and double
+                layer (fiber3d's useFMM path): operators and the device handle
+  stkfmm        STKFMM's Python API, as fiber3d calls it, over fmm
   quadrature    drop-in for fiber3d's RBF surface quadrature
   output        fiber3d's output and restart files
   tstep_bridge  solver-level drop-in for fiber3d's tstep (GMRES on the device)
