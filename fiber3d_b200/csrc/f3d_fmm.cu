@@ -716,6 +716,8 @@ struct NearArgs {
   double *out;                          // sorted targets x 3
 };
 
+// Two targets per thread (t and t + 128 of a 256-target block of the leaf):
+// each staged source serves both.
 __global__ void __launch_bounds__(128) near_l2p_kernel(const NearArgs a) {
   __shared__ double sp[128][3], sv[128][9];
   const int leaf = blockIdx.x;
@@ -726,58 +728,78 @@ __global__ void __launch_bounds__(128) near_l2p_kernel(const NearArgs a) {
   unmorton(static_cast<uint32_t>(key), bx, by, bz);
   const int m = 1 << a.level;
   const int64_t t0 = a.trg_start[leaf], t1 = a.trg_end[leaf];
-  for (int64_t tb = t0; tb < t1; tb += 128) {
-    const int64_t i = tb + threadIdx.x;
-    const bool iv = i < t1;
-    double x[3] = {0.0, 0.0, 0.0};
-    if (iv) {
+  for (int64_t tb = t0; tb < t1; tb += 256) {
+    double x[2][3];
+    bool iv[2];
 #pragma unroll
-      for (int d = 0; d < 3; ++d) x[d] = a.xt[3 * i + d];
+    for (int q = 0; q < 2; ++q) {
+      const int64_t i = tb + threadIdx.x + 128 * q;
+      iv[q] = i < t1;
+#pragma unroll
+      for (int d = 0; d < 3; ++d) x[q][d] = iv[q] ? a.xt[3 * i + d] : c[d];
     }
-    double us[3] = {0.0, 0.0, 0.0}, ud[3] = {0.0, 0.0, 0.0}, uf[3] = {0.0, 0.0, 0.0};
+    double us[2][3] = {}, ud[2][3] = {}, uf[2][3] = {};
     for (int nb = 0; nb < 27; ++nb) {
       const int nx = bx + nb / 9 - 1, ny = by + (nb / 3) % 3 - 1, nz = bz + nb % 3 - 1;
       if (nx < 0 || ny < 0 || nz < 0 || nx >= m || ny >= m || nz >= m) continue;
       const int slot = a.src_table[morton(nx, ny, nz)];
       if (slot < 0) continue;
-      for (int type = 0; type < 2; ++type) {
-        const int64_t j0 = type == 0 ? a.src.sl_start[slot] : a.src.dl_start[slot];
-        const int64_t j1 = type == 0 ? a.src.sl_end[slot] : a.src.dl_end[slot];
-        const double *px = type == 0 ? a.src.xsl : a.src.xdl;
-        const double *pv = type == 0 ? a.src.fsl : a.src.ddl;
-        const int nv = type == 0 ? 3 : 9;
-        for (int64_t jb = j0; jb < j1; jb += 128) {
-          const int cnt = static_cast<int>(min(static_cast<int64_t>(128), j1 - jb));
-          __syncthreads();
-          if (threadIdx.x < cnt) {
-            const int64_t j = jb + threadIdx.x;
+      // single layer
+      for (int64_t jb = a.src.sl_start[slot], j1 = a.src.sl_end[slot]; jb < j1; jb += 128) {
+        const int cnt = static_cast<int>(min(static_cast<int64_t>(128), j1 - jb));
+        __syncthreads();
+        if (threadIdx.x < cnt) {
+          const int64_t j = jb + threadIdx.x;
 #pragma unroll
-            for (int d = 0; d < 3; ++d) sp[threadIdx.x][d] = px[3 * j + d];
-            for (int q = 0; q < nv; ++q) sv[threadIdx.x][q] = pv[nv * j + q];
+          for (int d = 0; d < 3; ++d) {
+            sp[threadIdx.x][d] = a.src.xsl[3 * j + d];
+            sv[threadIdx.x][d] = a.src.fsl[3 * j + d];
           }
-          __syncthreads();
-          for (int s = 0; s < cnt; ++s) {
-            const double r0 = x[0] - sp[s][0], r1 = x[1] - sp[s][1], r2 = x[2] - sp[s][2];
+        }
+        __syncthreads();
+        for (int s = 0; s < cnt; ++s) {
+          const double p0 = sp[s][0], p1 = sp[s][1], p2 = sp[s][2];
+          const double f0 = sv[s][0], f1 = sv[s][1], f2 = sv[s][2];
+#pragma unroll
+          for (int q = 0; q < 2; ++q) {
+            const double r0 = x[q][0] - p0, r1 = x[q][1] - p1, r2 = x[q][2] - p2;
             const double d2 = fma(r0, r0, fma(r1, r1, r2 * r2));
-            const bool use = d2 > kCoincident2;
-            if (type == 0) {
-              double ri = rsqrt_refined(d2);
-              ri = use ? ri : 0.0;
-              const double g3 = ri * ri * ri * fma(r0, sv[s][0], fma(r1, sv[s][1], r2 * sv[s][2]));
-              us[0] = fma(g3, r0, fma(ri, sv[s][0], us[0]));
-              us[1] = fma(g3, r1, fma(ri, sv[s][1], us[1]));
-              us[2] = fma(g3, r2, fma(ri, sv[s][2], us[2]));
-            } else {
-              const double *D = sv[s];
-              const double q = r0 * fma(D[0], r0, fma(D[1], r1, D[2] * r2)) +
-                               r1 * fma(D[3], r0, fma(D[4], r1, D[5] * r2)) +
-                               r2 * fma(D[6], r0, fma(D[7], r1, D[8] * r2));
-              double f = times_rsqrt5(q, d2);
-              f = use ? f : 0.0;
-              ud[0] = fma(f, r0, ud[0]);
-              ud[1] = fma(f, r1, ud[1]);
-              ud[2] = fma(f, r2, ud[2]);
-            }
+            double ri = rsqrt_refined(d2);
+            ri = d2 > kCoincident2 ? ri : 0.0;
+            const double g3 = ri * ri * ri * fma(r0, f0, fma(r1, f1, r2 * f2));
+            us[q][0] = fma(g3, r0, fma(ri, f0, us[q][0]));
+            us[q][1] = fma(g3, r1, fma(ri, f1, us[q][1]));
+            us[q][2] = fma(g3, r2, fma(ri, f2, us[q][2]));
+          }
+        }
+      }
+      // double layer
+      for (int64_t jb = a.src.dl_start[slot], j1 = a.src.dl_end[slot]; jb < j1; jb += 128) {
+        const int cnt = static_cast<int>(min(static_cast<int64_t>(128), j1 - jb));
+        __syncthreads();
+        if (threadIdx.x < cnt) {
+          const int64_t j = jb + threadIdx.x;
+#pragma unroll
+          for (int d = 0; d < 3; ++d) sp[threadIdx.x][d] = a.src.xdl[3 * j + d];
+#pragma unroll
+          for (int e = 0; e < 9; ++e) sv[threadIdx.x][e] = a.src.ddl[9 * j + e];
+        }
+        __syncthreads();
+        for (int s = 0; s < cnt; ++s) {
+          const double p0 = sp[s][0], p1 = sp[s][1], p2 = sp[s][2];
+          const double *D = sv[s];
+#pragma unroll
+          for (int q = 0; q < 2; ++q) {
+            const double r0 = x[q][0] - p0, r1 = x[q][1] - p1, r2 = x[q][2] - p2;
+            const double d2 = fma(r0, r0, fma(r1, r1, r2 * r2));
+            const double qq = r0 * fma(D[0], r0, fma(D[1], r1, D[2] * r2)) +
+                              r1 * fma(D[3], r0, fma(D[4], r1, D[5] * r2)) +
+                              r2 * fma(D[6], r0, fma(D[7], r1, D[8] * r2));
+            double f = times_rsqrt5(qq, d2);
+            f = d2 > kCoincident2 ? f : 0.0;
+            ud[q][0] = fma(f, r0, ud[q][0]);
+            ud[q][1] = fma(f, r1, ud[q][1]);
+            ud[q][2] = fma(f, r2, ud[q][2]);
           }
         }
       }
@@ -793,23 +815,31 @@ __global__ void __launch_bounds__(128) near_l2p_kernel(const NearArgs a) {
 #pragma unroll
         for (int d = 0; d < 3; ++d) sp[threadIdx.x][d] = c[d] + kRout * h * a.surf[3 * k + d];
 #pragma unroll
-        for (int q = 0; q < 3; ++q) sv[threadIdx.x][q] = psi[4 * k + q];
+        for (int e = 0; e < 3; ++e) sv[threadIdx.x][e] = psi[4 * k + e];
         sv[threadIdx.x][3] = h * psi[4 * k + 3];
       }
       __syncthreads();
       for (int s = 0; s < cnt; ++s) {
-        const double r0 = x[0] - sp[s][0], r1 = x[1] - sp[s][1], r2 = x[2] - sp[s][2];
-        const double ri = rsqrt_refined(fma(r0, r0, fma(r1, r1, r2 * r2)));
-        const double g3 = ri * ri * ri * (fma(r0, sv[s][0], fma(r1, sv[s][1], r2 * sv[s][2])) + sv[s][3]);
-        uf[0] = fma(g3, r0, fma(ri, sv[s][0], uf[0]));
-        uf[1] = fma(g3, r1, fma(ri, sv[s][1], uf[1]));
-        uf[2] = fma(g3, r2, fma(ri, sv[s][2], uf[2]));
+        const double p0 = sp[s][0], p1 = sp[s][1], p2 = sp[s][2];
+        const double f0 = sv[s][0], f1 = sv[s][1], f2 = sv[s][2], fq = sv[s][3];
+#pragma unroll
+        for (int q = 0; q < 2; ++q) {
+          const double r0 = x[q][0] - p0, r1 = x[q][1] - p1, r2 = x[q][2] - p2;
+          const double ri = rsqrt_refined(fma(r0, r0, fma(r1, r1, r2 * r2)));
+          const double g3 = ri * ri * ri * (fma(r0, f0, fma(r1, f1, r2 * f2)) + fq);
+          uf[q][0] = fma(g3, r0, fma(ri, f0, uf[q][0]));
+          uf[q][1] = fma(g3, r1, fma(ri, f1, uf[q][1]));
+          uf[q][2] = fma(g3, r2, fma(ri, f2, uf[q][2]));
+        }
       }
     }
-    if (iv) {
-      const double cs = 1.0 / (8.0 * kPi), cd = -3.0 / (8.0 * kPi);
+    const double cs = 1.0 / (8.0 * kPi), cd = -3.0 / (8.0 * kPi);
 #pragma unroll
-      for (int d = 0; d < 3; ++d) a.out[3 * i + d] = fma(cs, us[d], fma(cd, ud[d], uf[d]));
+    for (int q = 0; q < 2; ++q) {
+      if (!iv[q]) continue;
+      const int64_t i = tb + threadIdx.x + 128 * q;
+#pragma unroll
+      for (int d = 0; d < 3; ++d) a.out[3 * i + d] = fma(cs, us[q][d], fma(cd, ud[q][d], uf[q][d]));
     }
   }
 }
