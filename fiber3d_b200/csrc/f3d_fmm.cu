@@ -564,9 +564,23 @@ __device__ __forceinline__ int source_slot(const GemmOp &op, int oct, int slot, 
   return op.table[morton(ix, iy, iz)];
 }
 
+// One m8n8k4 FP64 tensor-core product: d (8 x 8, two values per lane) +=
+// a (8 x 4, one per lane) b (4 x 8, one per lane).  Lane l holds a[l / 4][l % 4],
+// b[l % 4][l / 4] and d[l / 4][2 (l % 4) + {0, 1}].
+__device__ __forceinline__ void dmma_8x8x4(double &d0, double &d1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
+               : "+d"(d0), "+d"(d1)
+               : "d"(a), "d"(b));
+}
+
+// Shared tiles are k-major with row strides of 8 (mod 16) doubles, so that a
+// warp's fragment loads (4 k by 8 rows or columns) hit each bank twice, the
+// minimum for 32 eight-byte words.
+constexpr int kAStride = GBM + 8, kXStride = GBN + 8;
+
 __global__ void __launch_bounds__(GTHREADS) fmm_gemm_kernel(const __grid_constant__ GemmOp op) {
-  __shared__ double As[GBK][GBM + 1];
-  __shared__ double Xs[GBK][GBN + 1];
+  __shared__ double As[GBK][kAStride];
+  __shared__ double Xs[GBK][kXStride];
   __shared__ int s_src[GBN];
   __shared__ int s_any;
   const int tid = threadIdx.x;
@@ -579,14 +593,15 @@ __global__ void __launch_bounds__(GTHREADS) fmm_gemm_kernel(const __grid_constan
   const int col_end = op.oct_col_start[oct + 1];
   const int tps = (op.nterms + op.nsplit - 1) / op.nsplit;
   const int t_lo = blockIdx.z * tps, t_hi = min(op.nterms, t_lo + tps);
-  // thread (tr, tc) owns rows tr + 16 i (i < 6) and columns tc + 8 j (j < 8):
-  // the 8 column groups of a warp read 8 consecutive words (no bank conflict)
-  const int tr = tid >> 3, tc = tid & 7;
-  double acc[6][8];
+  // 2 x 2 warps, each a 48 x 32 block of the 96 x 64 tile: 6 x 4 tiles of 8 x 8
+  // on the FP64 tensor cores
+  const int lane = tid & 31, warp = tid >> 5;
+  const int wr = (warp >> 1) * 48, wc = (warp & 1) * 32;
+  double acc[6][4][2];
 #pragma unroll
   for (int i = 0; i < 6; ++i)
 #pragma unroll
-    for (int j = 0; j < 8; ++j) acc[i][j] = 0.0;
+    for (int j = 0; j < 4; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
 
   for (int t = t_lo; t < t_hi; ++t) {
     if (tid == 0) s_any = 0;
@@ -649,39 +664,39 @@ __global__ void __launch_bounds__(GTHREADS) fmm_gemm_kernel(const __grid_constan
         Xs[kk][c] = (s >= 0 && k < op.K) ? X[static_cast<int64_t>(s) * op.ldx + k] : 0.0;
       }
       __syncthreads();
-#pragma unroll 4
-      for (int kk = 0; kk < GBK; ++kk) {
-        double a[6], x[8];
+#pragma unroll 2
+      for (int k4 = 0; k4 < GBK; k4 += 4) {
+        double a[6], b[4];
 #pragma unroll
-        for (int i = 0; i < 6; ++i) a[i] = As[kk][tr + 16 * i];
+        for (int i = 0; i < 6; ++i) a[i] = As[k4 + (lane & 3)][wr + 8 * i + (lane >> 2)];
 #pragma unroll
-        for (int j = 0; j < 8; ++j) x[j] = Xs[kk][tc + 8 * j];
+        for (int j = 0; j < 4; ++j) b[j] = Xs[k4 + (lane & 3)][wc + 8 * j + (lane >> 2)];
 #pragma unroll
         for (int i = 0; i < 6; ++i)
 #pragma unroll
-          for (int j = 0; j < 8; ++j) acc[i][j] = fma(a[i], x[j], acc[i][j]);
+          for (int j = 0; j < 4; ++j) dmma_8x8x4(acc[i][j][0], acc[i][j][1], a[i], b[j]);
       }
       __syncthreads();
     }
   }
 #pragma unroll
-  for (int j = 0; j < 8; ++j) {
-    const int col = col0 + tc + 8 * j;
-    if (col >= col_end) continue;
-    const int slot = op.cols ? op.cols[col] : col;
-    if (op.nsplit > 1) {
-      double *p = op.partial + (static_cast<int64_t>(blockIdx.z) * op.nslots + slot) * op.ldy;
+  for (int j = 0; j < 4; ++j) {
+#pragma unroll
+    for (int e = 0; e < 2; ++e) {
+      const int col = col0 + wc + 8 * j + 2 * (lane & 3) + e;
+      if (col >= col_end) continue;
+      const int slot = op.cols ? op.cols[col] : col;
+      double *y = op.nsplit > 1 ? op.partial + (static_cast<int64_t>(blockIdx.z) * op.nslots + slot) * op.ldy
+                                : op.Y + static_cast<int64_t>(slot) * op.ldy;
 #pragma unroll
       for (int i = 0; i < 6; ++i) {
-        const int row = row0 + tr + 16 * i;
-        if (row < op.rows) p[row] = acc[i][j];
-      }
-    } else {
-      double *y = op.Y + static_cast<int64_t>(slot) * op.ldy;
-#pragma unroll
-      for (int i = 0; i < 6; ++i) {
-        const int row = row0 + tr + 16 * i;
-        if (row < op.rows) y[row] = op.accumulate ? fma(op.scale, acc[i][j], y[row]) : op.scale * acc[i][j];
+        const int row = row0 + wr + 8 * i + (lane >> 2);
+        if (row >= op.rows) continue;
+        const double v = acc[i][j][e];
+        if (op.nsplit > 1)
+          y[row] = v;
+        else
+          y[row] = op.accumulate ? fma(op.scale, v, y[row]) : op.scale * v;
       }
     }
   }
