@@ -578,9 +578,16 @@ __device__ __forceinline__ void dmma_8x8x4(double &d0, double &d1, double a, dou
 // minimum for 32 eight-byte words.
 constexpr int kAStride = GBM + 8, kXStride = GBN + 8;
 
+// Two shared stages: while one K slice is on the tensor cores, the next
+// slice's densities are in flight to registers and its operator values are
+// formed into the other stage.  One barrier per slice.
+constexpr size_t kGemmSmem = 2 * sizeof(double) * GBK * (kAStride + kXStride);
+constexpr int kXPerThread = GBN * GBK / GTHREADS;  // 16
+
 __global__ void __launch_bounds__(GTHREADS) fmm_gemm_kernel(const __grid_constant__ GemmOp op) {
-  __shared__ double As[GBK][kAStride];
-  __shared__ double Xs[GBK][kXStride];
+  extern __shared__ __align__(16) double smem[];
+  double (*As)[GBK][kAStride] = reinterpret_cast<double (*)[GBK][kAStride]>(smem);
+  double (*Xs)[GBK][kXStride] = reinterpret_cast<double (*)[GBK][kXStride]>(smem + 2 * GBK * kAStride);
   __shared__ int s_src[GBN];
   __shared__ int s_any;
   const int tid = threadIdx.x;
@@ -603,80 +610,125 @@ __global__ void __launch_bounds__(GTHREADS) fmm_gemm_kernel(const __grid_constan
 #pragma unroll
     for (int j = 0; j < 4; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
 
-  for (int t = t_lo; t < t_hi; ++t) {
-    if (tid == 0) s_any = 0;
-    __syncthreads();
-    if (tid < GBN) {
-      const int col = col0 + tid;
-      int s = -1;
-      if (col < col_end) s = source_slot(op, oct, op.cols ? op.cols[col] : col, t);
-      s_src[tid] = s;
-      if (s >= 0) s_any = 1;
-    }
-    __syncthreads();
-    if (!s_any) continue;
-    const bool par = op.mode == GEN_M2L && op.parent && t == op.nterms - 1;
-    const double *X = par ? op.X2 : op.X;
-    TermGeom g{};
-    if (op.mode != GEN_STORED) g = term_geom(op, oct, t);
-    for (int k0 = 0; k0 < op.K; k0 += GBK) {
-      if (op.mode == GEN_STORED) {
-        for (int e = tid; e < GBM * GBK; e += GTHREADS) {
-          const int r = e / GBK, kk = e % GBK;
-          const int row = row0 + r, k = k0 + kk;
-          As[kk][r] = (row < op.rows && k < op.K) ? op.A[static_cast<int64_t>(row) * op.lda + k] : 0.0;
-        }
-      } else {
-        // 32 check points x 8 equivalent points: one 3 x 4 block of K4 each
-        // (a warp takes 32 consecutive check points of one equivalent point)
-        for (int pp = tid; pp < (GBM / 3) * (GBK / 4); pp += GTHREADS) {
-          const int ci = pp % (GBM / 3), ei = pp / (GBM / 3);
-          const int cp = row0 / 3 + ci, ep = k0 / 4 + ei;
-          double v[3][4];
-          if (cp < op.n && ep < op.n) {
-            const double r0 = op.crad * op.surf[3 * cp] - (g.off[0] + g.erad * op.surf[3 * ep]);
-            const double r1 = op.crad * op.surf[3 * cp + 1] - (g.off[1] + g.erad * op.surf[3 * ep + 1]);
-            const double r2 = op.crad * op.surf[3 * cp + 2] - (g.off[2] + g.erad * op.surf[3 * ep + 2]);
-            const double ri = rsqrt_refined(fma(r0, r0, fma(r1, r1, r2 * r2)));
-            const double ri3 = ri * ri * ri;
-            const double r[3] = {r0, r1, r2};
-#pragma unroll
-            for (int i = 0; i < 3; ++i) {
-#pragma unroll
-              for (int j = 0; j < 3; ++j) v[i][j] = fma(r[i] * r[j], ri3, i == j ? ri : 0.0);
-              v[i][3] = r[i] * ri3 * g.qscale;
-            }
-          } else {
-#pragma unroll
-            for (int i = 0; i < 3; ++i)
-#pragma unroll
-              for (int j = 0; j < 4; ++j) v[i][j] = 0.0;
-          }
-#pragma unroll
-          for (int i = 0; i < 3; ++i)
-#pragma unroll
-            for (int j = 0; j < 4; ++j) As[4 * ei + j][3 * ci + i] = v[i][j];
-        }
-      }
-      for (int e = tid; e < GBN * GBK; e += GTHREADS) {
-        const int c = e / GBK, kk = e % GBK;
-        const int s = s_src[c], k = k0 + kk;
-        Xs[kk][c] = (s >= 0 && k < op.K) ? X[static_cast<int64_t>(s) * op.ldx + k] : 0.0;
+  // the first term at or after t with a source in this tile (its source
+  // slots in s_src); t_hi if none.  Every thread runs it (barriers).
+  auto find_term = [&](int t) {
+    for (; t < t_hi; ++t) {
+      if (tid == 0) s_any = 0;
+      __syncthreads();
+      if (tid < GBN) {
+        const int col = col0 + tid;
+        int sl = -1;
+        if (col < col_end) sl = source_slot(op, oct, op.cols ? op.cols[col] : col, t);
+        s_src[tid] = sl;
+        if (sl >= 0) s_any = 1;
       }
       __syncthreads();
+      if (s_any) break;
+    }
+    return t;
+  };
+  auto load_x = [&](double (&xr)[kXPerThread], int t, int k0) {
+    const bool par = op.mode == GEN_M2L && op.parent && t == op.nterms - 1;
+    const double *X = par ? op.X2 : op.X;
+#pragma unroll
+    for (int m = 0; m < kXPerThread; ++m) {
+      const int e = tid + GTHREADS * m;
+      const int c = e / GBK, kk = e % GBK;
+      const int sl = s_src[c], k = k0 + kk;
+      xr[m] = (sl >= 0 && k < op.K) ? X[static_cast<int64_t>(sl) * op.ldx + k] : 0.0;
+    }
+  };
+  auto store_x = [&](int b, const double (&xr)[kXPerThread]) {
+#pragma unroll
+    for (int m = 0; m < kXPerThread; ++m) {
+      const int e = tid + GTHREADS * m;
+      Xs[b][e % GBK][e / GBK] = xr[m];
+    }
+  };
+  auto fill_a = [&](int b, int t, int k0) {
+    if (op.mode == GEN_STORED) {
+      for (int e = tid; e < GBM * GBK; e += GTHREADS) {
+        const int r = e / GBK, kk = e % GBK;
+        const int row = row0 + r, k = k0 + kk;
+        As[b][kk][r] = (row < op.rows && k < op.K) ? op.A[static_cast<int64_t>(row) * op.lda + k] : 0.0;
+      }
+      return;
+    }
+    const TermGeom g = term_geom(op, oct, t);
+    // 32 check points x 8 equivalent points: one 3 x 4 block of K4 each (a
+    // warp takes 32 consecutive check points of one equivalent point)
+    for (int pp = tid; pp < (GBM / 3) * (GBK / 4); pp += GTHREADS) {
+      const int ci = pp % (GBM / 3), ei = pp / (GBM / 3);
+      const int cp = row0 / 3 + ci, ep = k0 / 4 + ei;
+      double v[3][4];
+      if (cp < op.n && ep < op.n) {
+        const double r0 = op.crad * op.surf[3 * cp] - (g.off[0] + g.erad * op.surf[3 * ep]);
+        const double r1 = op.crad * op.surf[3 * cp + 1] - (g.off[1] + g.erad * op.surf[3 * ep + 1]);
+        const double r2 = op.crad * op.surf[3 * cp + 2] - (g.off[2] + g.erad * op.surf[3 * ep + 2]);
+        const double ri = rsqrt_refined(fma(r0, r0, fma(r1, r1, r2 * r2)));
+        const double ri3 = ri * ri * ri;
+        const double r[3] = {r0, r1, r2};
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+#pragma unroll
+          for (int j = 0; j < 3; ++j) v[i][j] = fma(r[i] * r[j], ri3, i == j ? ri : 0.0);
+          v[i][3] = r[i] * ri3 * g.qscale;
+        }
+      } else {
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+          for (int j = 0; j < 4; ++j) v[i][j] = 0.0;
+      }
+#pragma unroll
+      for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) As[b][4 * ei + j][3 * ci + i] = v[i][j];
+    }
+  };
+
+  int t = find_term(t_lo);
+  if (t < t_hi) {
+    int k0 = 0, b = 0;
+    {
+      double xr[kXPerThread];
+      load_x(xr, t, 0);
+      fill_a(0, t, 0);
+      store_x(0, xr);
+    }
+    __syncthreads();
+    while (true) {
+      // the next slice: the same term's next K block, or the next term with a source
+      int nt = t, nk0 = k0 + GBK;
+      if (nk0 >= op.K) {
+        nk0 = 0;
+        nt = find_term(t + 1);
+      }
+      const bool next = nt < t_hi;
+      double xr[kXPerThread];
+      if (next) load_x(xr, nt, nk0);
 #pragma unroll 2
       for (int k4 = 0; k4 < GBK; k4 += 4) {
-        double a[6], b[4];
+        double a[6], bb[4];
 #pragma unroll
-        for (int i = 0; i < 6; ++i) a[i] = As[k4 + (lane & 3)][wr + 8 * i + (lane >> 2)];
+        for (int i = 0; i < 6; ++i) a[i] = As[b][k4 + (lane & 3)][wr + 8 * i + (lane >> 2)];
 #pragma unroll
-        for (int j = 0; j < 4; ++j) b[j] = Xs[k4 + (lane & 3)][wc + 8 * j + (lane >> 2)];
+        for (int j = 0; j < 4; ++j) bb[j] = Xs[b][k4 + (lane & 3)][wc + 8 * j + (lane >> 2)];
 #pragma unroll
         for (int i = 0; i < 6; ++i)
 #pragma unroll
-          for (int j = 0; j < 4; ++j) dmma_8x8x4(acc[i][j][0], acc[i][j][1], a[i], b[j]);
+          for (int j = 0; j < 4; ++j) dmma_8x8x4(acc[i][j][0], acc[i][j][1], a[i], bb[j]);
+      }
+      if (next) {
+        fill_a(b ^ 1, nt, nk0);
+        store_x(b ^ 1, xr);
       }
       __syncthreads();
+      if (!next) break;
+      t = nt;
+      k0 = nk0;
+      b ^= 1;
     }
   }
 #pragma unroll
@@ -1127,8 +1179,11 @@ int launch_gemm(GemmOp op, const int *group_start, DevBuf &partial, cudaStream_t
     if (rc) return rc;
     op.partial = as<double>(partial);
   }
+  if (cudaFuncSetAttribute(fmm_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           static_cast<int>(kGemmSmem)) != cudaSuccess)
+    return F3D_ERR_CUDA;
   const dim3 grid(static_cast<unsigned>(rtiles), static_cast<unsigned>(tiles), static_cast<unsigned>(nsplit));
-  fmm_gemm_kernel<<<grid, GTHREADS, 0, st>>>(op);
+  fmm_gemm_kernel<<<grid, GTHREADS, kGemmSmem, st>>>(op);
   ++*launches;
   if (nsplit > 1) {
     const int64_t ne = static_cast<int64_t>(op.nslots) * op.rows;
