@@ -564,30 +564,9 @@ __device__ __forceinline__ int source_slot(const GemmOp &op, int oct, int slot, 
   return op.table[morton(ix, iy, iz)];
 }
 
-// One m8n8k4 FP64 tensor-core product: d (8 x 8, two values per lane) +=
-// a (8 x 4, one per lane) b (4 x 8, one per lane).  Lane l holds a[l / 4][l % 4],
-// b[l % 4][l / 4] and d[l / 4][2 (l % 4) + {0, 1}].
-__device__ __forceinline__ void dmma_8x8x4(double &d0, double &d1, double a, double b) {
-  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
-               : "+d"(d0), "+d"(d1)
-               : "d"(a), "d"(b));
-}
-
-// Shared tiles are k-major with row strides of 8 (mod 16) doubles, so that a
-// warp's fragment loads (4 k by 8 rows or columns) hit each bank twice, the
-// minimum for 32 eight-byte words.
-constexpr int kAStride = GBM + 8, kXStride = GBN + 8;
-
-// Two shared stages: while one K slice is on the tensor cores, the next
-// slice's densities are in flight to registers and its operator values are
-// formed into the other stage.  One barrier per slice.
-constexpr size_t kGemmSmem = 2 * sizeof(double) * GBK * (kAStride + kXStride);
-constexpr int kXPerThread = GBN * GBK / GTHREADS;  // 16
-
 __global__ void __launch_bounds__(GTHREADS) fmm_gemm_kernel(const __grid_constant__ GemmOp op) {
-  extern __shared__ __align__(16) double smem[];
-  double (*As)[GBK][kAStride] = reinterpret_cast<double (*)[GBK][kAStride]>(smem);
-  double (*Xs)[GBK][kXStride] = reinterpret_cast<double (*)[GBK][kXStride]>(smem + 2 * GBK * kAStride);
+  __shared__ double As[GBK][GBM + 1];
+  __shared__ double Xs[GBK][GBN + 1];
   __shared__ int s_src[GBN];
   __shared__ int s_any;
   const int tid = threadIdx.x;
@@ -600,155 +579,109 @@ __global__ void __launch_bounds__(GTHREADS) fmm_gemm_kernel(const __grid_constan
   const int col_end = op.oct_col_start[oct + 1];
   const int tps = (op.nterms + op.nsplit - 1) / op.nsplit;
   const int t_lo = blockIdx.z * tps, t_hi = min(op.nterms, t_lo + tps);
-  // 2 x 2 warps, each a 48 x 32 block of the 96 x 64 tile: 6 x 4 tiles of 8 x 8
-  // on the FP64 tensor cores
-  const int lane = tid & 31, warp = tid >> 5;
-  const int wr = (warp >> 1) * 48, wc = (warp & 1) * 32;
-  double acc[6][4][2];
+  // thread (tr, tc) owns rows tr + 16 i (i < 6) and columns tc + 8 j (j < 8):
+  // the 8 column groups of a warp read 8 consecutive words (no bank conflict)
+  const int tr = tid >> 3, tc = tid & 7;
+  double acc[6][8];
 #pragma unroll
   for (int i = 0; i < 6; ++i)
 #pragma unroll
-    for (int j = 0; j < 4; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+    for (int j = 0; j < 8; ++j) acc[i][j] = 0.0;
 
-  // the first term at or after t with a source in this tile (its source
-  // slots in s_src); t_hi if none.  Every thread runs it (barriers).
-  auto find_term = [&](int t) {
-    for (; t < t_hi; ++t) {
-      if (tid == 0) s_any = 0;
-      __syncthreads();
-      if (tid < GBN) {
-        const int col = col0 + tid;
-        int sl = -1;
-        if (col < col_end) sl = source_slot(op, oct, op.cols ? op.cols[col] : col, t);
-        s_src[tid] = sl;
-        if (sl >= 0) s_any = 1;
-      }
-      __syncthreads();
-      if (s_any) break;
-    }
-    return t;
-  };
-  auto load_x = [&](double (&xr)[kXPerThread], int t, int k0) {
-    const bool par = op.mode == GEN_M2L && op.parent && t == op.nterms - 1;
-    const double *X = par ? op.X2 : op.X;
-#pragma unroll
-    for (int m = 0; m < kXPerThread; ++m) {
-      const int e = tid + GTHREADS * m;
-      const int c = e / GBK, kk = e % GBK;
-      const int sl = s_src[c], k = k0 + kk;
-      xr[m] = (sl >= 0 && k < op.K) ? X[static_cast<int64_t>(sl) * op.ldx + k] : 0.0;
-    }
-  };
-  auto store_x = [&](int b, const double (&xr)[kXPerThread]) {
-#pragma unroll
-    for (int m = 0; m < kXPerThread; ++m) {
-      const int e = tid + GTHREADS * m;
-      Xs[b][e % GBK][e / GBK] = xr[m];
-    }
-  };
-  auto fill_a = [&](int b, int t, int k0) {
-    if (op.mode == GEN_STORED) {
-      for (int e = tid; e < GBM * GBK; e += GTHREADS) {
-        const int r = e / GBK, kk = e % GBK;
-        const int row = row0 + r, k = k0 + kk;
-        As[b][kk][r] = (row < op.rows && k < op.K) ? op.A[static_cast<int64_t>(row) * op.lda + k] : 0.0;
-      }
-      return;
-    }
-    const TermGeom g = term_geom(op, oct, t);
-    // 32 check points x 8 equivalent points: one 3 x 4 block of K4 each (a
-    // warp takes 32 consecutive check points of one equivalent point)
-    for (int pp = tid; pp < (GBM / 3) * (GBK / 4); pp += GTHREADS) {
-      const int ci = pp % (GBM / 3), ei = pp / (GBM / 3);
-      const int cp = row0 / 3 + ci, ep = k0 / 4 + ei;
-      double v[3][4];
-      if (cp < op.n && ep < op.n) {
-        const double r0 = op.crad * op.surf[3 * cp] - (g.off[0] + g.erad * op.surf[3 * ep]);
-        const double r1 = op.crad * op.surf[3 * cp + 1] - (g.off[1] + g.erad * op.surf[3 * ep + 1]);
-        const double r2 = op.crad * op.surf[3 * cp + 2] - (g.off[2] + g.erad * op.surf[3 * ep + 2]);
-        const double ri = rsqrt_refined(fma(r0, r0, fma(r1, r1, r2 * r2)));
-        const double ri3 = ri * ri * ri;
-        const double r[3] = {r0, r1, r2};
-#pragma unroll
-        for (int i = 0; i < 3; ++i) {
-#pragma unroll
-          for (int j = 0; j < 3; ++j) v[i][j] = fma(r[i] * r[j], ri3, i == j ? ri : 0.0);
-          v[i][3] = r[i] * ri3 * g.qscale;
-        }
-      } else {
-#pragma unroll
-        for (int i = 0; i < 3; ++i)
-#pragma unroll
-          for (int j = 0; j < 4; ++j) v[i][j] = 0.0;
-      }
-#pragma unroll
-      for (int i = 0; i < 3; ++i)
-#pragma unroll
-        for (int j = 0; j < 4; ++j) As[b][4 * ei + j][3 * ci + i] = v[i][j];
-    }
-  };
-
-  int t = find_term(t_lo);
-  if (t < t_hi) {
-    int k0 = 0, b = 0;
-    {
-      double xr[kXPerThread];
-      load_x(xr, t, 0);
-      fill_a(0, t, 0);
-      store_x(0, xr);
+  for (int t = t_lo; t < t_hi; ++t) {
+    if (tid == 0) s_any = 0;
+    __syncthreads();
+    if (tid < GBN) {
+      const int col = col0 + tid;
+      int s = -1;
+      if (col < col_end) s = source_slot(op, oct, op.cols ? op.cols[col] : col, t);
+      s_src[tid] = s;
+      if (s >= 0) s_any = 1;
     }
     __syncthreads();
-    while (true) {
-      // the next slice: the same term's next K block, or the next term with a source
-      int nt = t, nk0 = k0 + GBK;
-      if (nk0 >= op.K) {
-        nk0 = 0;
-        nt = find_term(t + 1);
+    if (!s_any) continue;
+    const bool par = op.mode == GEN_M2L && op.parent && t == op.nterms - 1;
+    const double *X = par ? op.X2 : op.X;
+    TermGeom g{};
+    if (op.mode != GEN_STORED) g = term_geom(op, oct, t);
+    for (int k0 = 0; k0 < op.K; k0 += GBK) {
+      if (op.mode == GEN_STORED) {
+        for (int e = tid; e < GBM * GBK; e += GTHREADS) {
+          const int r = e / GBK, kk = e % GBK;
+          const int row = row0 + r, k = k0 + kk;
+          As[kk][r] = (row < op.rows && k < op.K) ? op.A[static_cast<int64_t>(row) * op.lda + k] : 0.0;
+        }
+      } else {
+        // 32 check points x 8 equivalent points: one 3 x 4 block of K4 each
+        // (a warp takes 32 consecutive check points of one equivalent point)
+        for (int pp = tid; pp < (GBM / 3) * (GBK / 4); pp += GTHREADS) {
+          const int ci = pp % (GBM / 3), ei = pp / (GBM / 3);
+          const int cp = row0 / 3 + ci, ep = k0 / 4 + ei;
+          double v[3][4];
+          if (cp < op.n && ep < op.n) {
+            const double r0 = op.crad * op.surf[3 * cp] - (g.off[0] + g.erad * op.surf[3 * ep]);
+            const double r1 = op.crad * op.surf[3 * cp + 1] - (g.off[1] + g.erad * op.surf[3 * ep + 1]);
+            const double r2 = op.crad * op.surf[3 * cp + 2] - (g.off[2] + g.erad * op.surf[3 * ep + 2]);
+            const double ri = rsqrt_refined(fma(r0, r0, fma(r1, r1, r2 * r2)));
+            const double ri3 = ri * ri * ri;
+            const double r[3] = {r0, r1, r2};
+#pragma unroll
+            for (int i = 0; i < 3; ++i) {
+#pragma unroll
+              for (int j = 0; j < 3; ++j) v[i][j] = fma(r[i] * r[j], ri3, i == j ? ri : 0.0);
+              v[i][3] = r[i] * ri3 * g.qscale;
+            }
+          } else {
+#pragma unroll
+            for (int i = 0; i < 3; ++i)
+#pragma unroll
+              for (int j = 0; j < 4; ++j) v[i][j] = 0.0;
+          }
+#pragma unroll
+          for (int i = 0; i < 3; ++i)
+#pragma unroll
+            for (int j = 0; j < 4; ++j) As[4 * ei + j][3 * ci + i] = v[i][j];
+        }
       }
-      const bool next = nt < t_hi;
-      double xr[kXPerThread];
-      if (next) load_x(xr, nt, nk0);
-#pragma unroll 2
-      for (int k4 = 0; k4 < GBK; k4 += 4) {
-        double a[6], bb[4];
+      for (int e = tid; e < GBN * GBK; e += GTHREADS) {
+        const int c = e / GBK, kk = e % GBK;
+        const int s = s_src[c], k = k0 + kk;
+        Xs[kk][c] = (s >= 0 && k < op.K) ? X[static_cast<int64_t>(s) * op.ldx + k] : 0.0;
+      }
+      __syncthreads();
+#pragma unroll 4
+      for (int kk = 0; kk < GBK; ++kk) {
+        double a[6], x[8];
 #pragma unroll
-        for (int i = 0; i < 6; ++i) a[i] = As[b][k4 + (lane & 3)][wr + 8 * i + (lane >> 2)];
+        for (int i = 0; i < 6; ++i) a[i] = As[kk][tr + 16 * i];
 #pragma unroll
-        for (int j = 0; j < 4; ++j) bb[j] = Xs[b][k4 + (lane & 3)][wc + 8 * j + (lane >> 2)];
+        for (int j = 0; j < 8; ++j) x[j] = Xs[kk][tc + 8 * j];
 #pragma unroll
         for (int i = 0; i < 6; ++i)
 #pragma unroll
-          for (int j = 0; j < 4; ++j) dmma_8x8x4(acc[i][j][0], acc[i][j][1], a[i], bb[j]);
-      }
-      if (next) {
-        fill_a(b ^ 1, nt, nk0);
-        store_x(b ^ 1, xr);
+          for (int j = 0; j < 8; ++j) acc[i][j] = fma(a[i], x[j], acc[i][j]);
       }
       __syncthreads();
-      if (!next) break;
-      t = nt;
-      k0 = nk0;
-      b ^= 1;
     }
   }
 #pragma unroll
-  for (int j = 0; j < 4; ++j) {
-#pragma unroll
-    for (int e = 0; e < 2; ++e) {
-      const int col = col0 + wc + 8 * j + 2 * (lane & 3) + e;
-      if (col >= col_end) continue;
-      const int slot = op.cols ? op.cols[col] : col;
-      double *y = op.nsplit > 1 ? op.partial + (static_cast<int64_t>(blockIdx.z) * op.nslots + slot) * op.ldy
-                                : op.Y + static_cast<int64_t>(slot) * op.ldy;
+  for (int j = 0; j < 8; ++j) {
+    const int col = col0 + tc + 8 * j;
+    if (col >= col_end) continue;
+    const int slot = op.cols ? op.cols[col] : col;
+    if (op.nsplit > 1) {
+      double *p = op.partial + (static_cast<int64_t>(blockIdx.z) * op.nslots + slot) * op.ldy;
 #pragma unroll
       for (int i = 0; i < 6; ++i) {
-        const int row = row0 + wr + 8 * i + (lane >> 2);
-        if (row >= op.rows) continue;
-        const double v = acc[i][j][e];
-        if (op.nsplit > 1)
-          y[row] = v;
-        else
-          y[row] = op.accumulate ? fma(op.scale, v, y[row]) : op.scale * v;
+        const int row = row0 + tr + 16 * i;
+        if (row < op.rows) p[row] = acc[i][j];
+      }
+    } else {
+      double *y = op.Y + static_cast<int64_t>(slot) * op.ldy;
+#pragma unroll
+      for (int i = 0; i < 6; ++i) {
+        const int row = row0 + tr + 16 * i;
+        if (row < op.rows) y[row] = op.accumulate ? fma(op.scale, acc[i][j], y[row]) : op.scale * acc[i][j];
       }
     }
   }
@@ -1179,11 +1112,8 @@ int launch_gemm(GemmOp op, const int *group_start, DevBuf &partial, cudaStream_t
     if (rc) return rc;
     op.partial = as<double>(partial);
   }
-  if (cudaFuncSetAttribute(fmm_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           static_cast<int>(kGemmSmem)) != cudaSuccess)
-    return F3D_ERR_CUDA;
   const dim3 grid(static_cast<unsigned>(rtiles), static_cast<unsigned>(tiles), static_cast<unsigned>(nsplit));
-  fmm_gemm_kernel<<<grid, GTHREADS, kGemmSmem, st>>>(op);
+  fmm_gemm_kernel<<<grid, GTHREADS, 0, st>>>(op);
   ++*launches;
   if (nsplit > 1) {
     const int64_t ne = static_cast<int64_t>(op.nslots) * op.rows;
