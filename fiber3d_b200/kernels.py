@@ -329,7 +329,9 @@ def oseen_kernel_source_target_pycuda(r_source, r_target, density, eta=1.0, epsi
 
 def _fmm_handle(kwargs):
     """The package FMM behind a ``fmm_PVel`` argument (a ``stkfmm.STKFMM`` of
-    this package, or an ``fmm.FMM``), else None."""
+    this package, or an ``fmm.FMM``), else None: any other handle (one of the
+    external STKFMM library, say) is accepted and left unused, and the sum is
+    then the exact direct one."""
     h = kwargs.get("fmm_PVel")
     if h is None:
         return None
@@ -338,7 +340,7 @@ def _fmm_handle(kwargs):
         return h.fmm
     if isinstance(h, F.FMM):
         return h
-    raise TypeError("fmm_PVel must be a fiber3d_b200.stkfmm.STKFMM or fiber3d_b200.fmm.FMM")
+    return None
 
 
 def _fmm_sum(fmm, r_sl, r_dl, r_target, f_sl, normal, dens_dl, eta, host):

@@ -83,6 +83,23 @@ def test_stkfmm_stand_ins(K, g):
     assert rel_err(w, g["fmm_sdl_u"]) < TOL
 
 
+def test_stkfmm_functions_on_the_gpu_fmm(K, g):
+    """With this package's stkfmm handle the same functions run the GPU FMM:
+    against fiber3d's own direct sums (the values STKFMM is checked
+    against), to the FMM's order-10 accuracy."""
+    from fiber3d_b200 import stkfmm
+    mk = lambda: stkfmm.STKFMM(10, 64, stkfmm.PAXIS.NONE, stkfmm.KERNEL(stkfmm.KERNEL.PVel))
+    u = K.oseen_kernel_source_target_stkfmm(g["fmm_rs"], g["fmm_rt"], g["fmm_f"], fmm_PVel=mk())
+    assert rel_err(u, g["fmm_oseen_u"]) < 1e-6
+    u = K.oseen_kernel_source_target_stkfmm(g["fmm_rs"], g["fmm_rt"], g["fmm_f"], 2.0, fmm_PVel=mk())
+    assert rel_err(u, g["fmm_eta_u"]) < 1e-6
+    v = K.stresslet_kernel_source_target_stkfmm(g["fmm_rs"], g["fmm_rt"], g["fmm_n"], g["fmm_d"], fmm_PVel=mk())
+    assert rel_err(v, g["fmm_stresslet_v"]) < 1e-6
+    w = K.single_double_layer_kernel_source_target_stkfmm(g["fmm_rs"], g["fmm_rdl"], g["fmm_rt"], g["fmm_ndl"],
+                                                          g["fmm_f"], g["fmm_ddl"], fmm_PVel=mk())
+    assert rel_err(w, g["fmm_sdl_u"]) < 1e-6
+
+
 def test_skip_close_fp32c_drops_coincident_pairs(K, g):
     from fiber3d_b200 import kernels
     u = kernels.pair_sum("oseen", torch.as_tensor(g["fmm_rs"], device="cuda"),
