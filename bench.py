@@ -445,11 +445,49 @@ def cpu_baseline(wl, seconds: float):
                       "(cores = OpenMP threads used)"}
 
 
+def fmm_reference_arm(args, world):
+    """The FMM workload's reference: fiber3d's direct numba sums (what its
+    STKFMM path is checked against; STKFMM itself is not available), restated
+    in C/OpenMP, on all host threads, over a target sample per step."""
+    from oracle import pairs_c
+    n = args.fmm_n
+    w = fmm_workload(n, seed=0)
+    hc = host_cores()
+    nt = max(16, min(n, int(2e9 / (2 * n))))  # about 1 s of CPU work per step
+    rates = []
+    for step in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
+        pairs_c.pair_sum("oseen", w["sl"], w["trg"][:nt], w["f"], epsilon_distance=0.0, reg=0.0)
+        pairs_c.pair_sum("stresslet", w["dl"], w["trg"][:nt], w["dens"], w["nrm"], epsilon_distance=0.0, reg=0.0)
+        if step >= args.warmup:
+            rates.append(2 * n * nt / (time.perf_counter() - t0))
+    value = statistics.median(rates)
+    line = {
+        "impl": "reference",
+        "metric": f"FMM equivalent Stokes pair interactions per second (FP64, order {args.fmm_order})",
+        "value": value, "unit": "pairs/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 2 * n * n / value * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic (seeded): fiber3d's STKFMM check shape (kernels/test_stkfmm.py)",
+        "config": {"workload": "fmm", "n_single_layer": n, "n_double_layer": n, "n_targets": n,
+                   "cube_side": w["side"], "order": args.fmm_order, "max_pts": args.fmm_max_pts,
+                   "l2": "flushed between steps (256 MiB write, outside the event pairs)"},
+        "parallelism": f"host cores (rank 0 of {world})",
+        "cpu_baseline": {"value": value, "unit": "pairs/s", "cores": hc["threads"], **hc, "kind": "port",
+                         "sample": f"direct sums onto {nt} of {n} targets per step (C/OpenMP restatement of "
+                                   "fiber3d's numba loops; STKFMM, fiber3d's CPU FMM, is not installed)"},
+        "e2e": {"value": value, "unit": "pairs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
 def reference_arm(args, rank, world):
     if rank != 0:
         return
     if args.workload == "surface_quadrature":
         quadrature_reference_arm(args, world)
+        return
+    if args.workload == "fmm":
+        fmm_reference_arm(args, world)
         return
     wl = make_workload(args.workload)
     hc = host_cores()

@@ -54,3 +54,21 @@ def test_reference_arm_other_ranks_exit_without_work():
     res = subprocess.run(cmd, capture_output=True, text=True, timeout=120, cwd=ROOT, env=env)
     assert res.returncode == 0, res.stderr
     assert not [ln for ln in res.stdout.splitlines() if ln.startswith("{")]
+
+
+def test_fmm_reference_arm_prints_one_line():
+    """The FMM workload's reference arm (fiber3d's direct sums, which its
+    STKFMM path is checked against) on a small case: one line, the FMM
+    arm's metric and config keys."""
+    cmd = [sys.executable, str(ROOT / "bench.py"), "--impl", "reference", "--workload", "fmm",
+           "--fmm-n", "5000", "--steps", "1", "--warmup", "1"]
+    res = subprocess.run(cmd, capture_output=True, text=True, timeout=300, cwd=ROOT)
+    assert res.returncode == 0, res.stderr
+    lines = [ln for ln in res.stdout.splitlines() if ln.startswith("{")]
+    assert len(lines) == 1
+    d = json.loads(lines[0])
+    assert d["impl"] == "reference" and d["unit"] == "pairs/s" and d["higher_is_better"] is True
+    assert d["metric"].startswith("FMM equivalent Stokes pair interactions per second")
+    c = d["config"]
+    assert c["workload"] == "fmm" and c["n_single_layer"] == c["n_double_layer"] == c["n_targets"] == 5000
+    assert d["value"] > 0 and d["cpu_baseline"]["kind"] == "port"
