@@ -593,7 +593,7 @@ def hydro_arm(args, rank, world, local, warmup=None, steps=None, emit=True):
     P = geometry.hydro_step_problem(seed=3, nshell=args.nshell, nfib=args.nfib, shell_radius=args.shell_radius,
         fiber_ball=args.fiber_ball, body_shell=args.body_shell)
     t0 = time.perf_counter()
-    shell = H.ShellOperator(P.shell, P.eta, P.reg, P.eps_dist, dev)
+    shell = H.ShellOperator(P.shell, P.eta, P.reg, P.eps_dist, dev, pc=args.shell_pc)
     torch.cuda.synchronize()
     setup_s = time.perf_counter() - t0
     out, xs = {}, {}
@@ -793,7 +793,7 @@ def hydro_arm(args, rank, world, local, warmup=None, steps=None, emit=True):
                        "shell_radius": args.shell_radius, "fiber_ball": args.fiber_ball,
                        "body_shell": args.body_shell,
                        "system_size": int(3 * args.nshell + 4 * 1206 + 4 * 32 * args.nfib),
-                       "shell_setup_s": setup_s}, "step": out}
+                       "shell_pc": args.shell_pc, "shell_setup_s": setup_s}, "step": out}
     if rank == 0 and emit:
         print(json.dumps(line), flush=True)
     return line
@@ -1200,6 +1200,9 @@ def main():
     ap.add_argument("--fiber-ball", type=float, default=5.0, help="radius of the ball holding the fiber centres")
     ap.add_argument("--body-shell", type=float, default=7.5, help="distance of the body centres from the origin")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    ap.add_argument("--shell-pc", default="dense", choices=["dense", "block"],
+                    help="periphery preconditioner of the time step: the dense inverse (fiber3d's LU) or "
+                         "the block-Jacobi one")
     ap.add_argument("--no-step", action="store_true",
                     help="pair throughput only (skip the embedded time-step comparison)")
     ap.add_argument("--no-flownet", action="store_true",
