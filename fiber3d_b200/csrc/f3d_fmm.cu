@@ -487,6 +487,7 @@ __global__ void __launch_bounds__(128) p2m_check_kernel(const Geometry g, int le
 // second kernel adds the partials in split order (deterministic).
 constexpr int GBM = 96, GBN = 64, GBK = 32, GTHREADS = 128;
 constexpr int kM2LTerms = 189;
+constexpr int kFarTerms = 316;  // level 2: every box at distance >= 2, (7^3 - 3^3) offsets
 
 enum GenMode { GEN_STORED = 0, GEN_M2M = 1, GEN_M2L = 2 };
 
@@ -509,6 +510,8 @@ struct GemmOp {
   double crad;
   int nterms, parent;
   unsigned char m2l_idx[8][kM2LTerms];  // a*36 + b*6 + d of each interaction box, per octant
+  int all_offsets;                      // level 2: the terms are the 316 far offsets, no octant groups
+  unsigned short far_idx[kFarTerms];    // a*49 + b*7 + d of each offset (a, b, d - 3)
   const int *table;   // sources of this level (M2L) or of the level below (M2M)
   const int *table2;  // targets of the level above (the parent term)
   const double *X, *X2;
@@ -536,6 +539,13 @@ __device__ __forceinline__ TermGeom term_geom(const GemmOp &op, int oct, int t) 
     g.off[2] = cz ? -1.0 : 1.0;
     g.erad = 2.0 * kRout;
     g.qscale = 2.0;
+  } else if (op.all_offsets) {
+    const int idx = op.far_idx[t];
+    g.off[0] = 2.0 * (idx / 49 - 3);
+    g.off[1] = 2.0 * ((idx / 7) % 7 - 3);
+    g.off[2] = 2.0 * (idx % 7 - 3);
+    g.erad = kRin;
+    g.qscale = 1.0;
   } else {
     const int idx = op.m2l_idx[oct][t];
     g.off[0] = 2.0 * (idx / 36 - 2 - cx);
@@ -554,11 +564,18 @@ __device__ __forceinline__ int source_slot(const GemmOp &op, int oct, int slot, 
   if (op.parent && t == op.nterms - 1) return op.table2[key >> 3];
   int ix, iy, iz;
   unmorton(static_cast<uint32_t>(key), ix, iy, iz);
-  const int idx = op.m2l_idx[oct][t];
-  const int cx = (oct >> 2) & 1, cy = (oct >> 1) & 1, cz = oct & 1;
-  ix += idx / 36 - 2 - cx;
-  iy += (idx / 6) % 6 - 2 - cy;
-  iz += idx % 6 - 2 - cz;
+  if (op.all_offsets) {
+    const int idx = op.far_idx[t];
+    ix += idx / 49 - 3;
+    iy += (idx / 7) % 7 - 3;
+    iz += idx % 7 - 3;
+  } else {
+    const int idx = op.m2l_idx[oct][t];
+    const int cx = (oct >> 2) & 1, cy = (oct >> 1) & 1, cz = oct & 1;
+    ix += idx / 36 - 2 - cx;
+    iy += (idx / 6) % 6 - 2 - cy;
+    iz += idx % 6 - 2 - cz;
+  }
   const int m = 1 << op.level;
   if (ix < 0 || iy < 0 || iz < 0 || ix >= m || iy >= m || iz >= m) return -1;
   return op.table[morton(ix, iy, iz)];
@@ -1381,13 +1398,28 @@ int f3d_fmm_evaluate(f3d_fmm *h, const double *sl_density, const double *dl_norm
       if (t != kM2LTerms) return F3D_ERR_ARG;
     }
     op.nterms = kM2LTerms;
+    const int *groups = lv.oct_start;
+    if (l == 2) {
+      // every level-1 box neighbours every other: the interaction list of a
+      // level-2 box is every box at distance >= 2, whatever its octant
+      int t = 0;
+      for (int a = 0; a < 7; ++a)
+        for (int b = 0; b < 7; ++b)
+          for (int d = 0; d < 7; ++d)
+            if (std::max(std::abs(a - 3), std::max(std::abs(b - 3), std::abs(d - 3))) >= 2)
+              op.far_idx[t++] = static_cast<unsigned short>(49 * a + 7 * b + d);
+      if (t != kFarTerms) return F3D_ERR_ARG;
+      op.all_offsets = 1;
+      op.nterms = kFarTerms;
+      groups = nullptr;
+    }
     if (l > 2) {
       op.parent = 1;
       op.nterms = kM2LTerms + 1;
       op.table2 = as<int>(h->lev[l - 1].trg_table);
       op.X2 = as<double>(h->lev[l - 1].psi);
     }
-    if ((rc = launch_gemm(op, lv.oct_start, part, st, &h->launches)) ||
+    if ((rc = launch_gemm(op, groups, part, st, &h->launches)) ||
         (rc = launch_gemm(stored_op(as<double>(h->dc2de), n4, n3, Y, n3, as<double>(lv.psi), n4, lv.ntrg, 1.0),
                           nullptr, part, st, &h->launches)))
       return rc;
