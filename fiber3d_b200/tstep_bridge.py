@@ -102,10 +102,10 @@ class GpuGmres:
         return res["x"].cpu().numpy(), int(res["info"])
 
 
-def install(ts, mixed: bool = False, warm_start: str | None = None, model=None):
+def install(ts, mixed: bool = False, warm_start: str | None = None, model=None, shell_pc: str = "dense"):
     """Route fiber3d's GMRES call through the GPU solver for time stepper `ts`."""
     import importlib
     gm = importlib.import_module("bpm_utilities.gmres")
-    solver = GpuGmres(ts, mixed=mixed, warm_start=warm_start, model=model)
+    solver = GpuGmres(ts, mixed=mixed, warm_start=warm_start, model=model, shell_pc=shell_pc)
     gm.gmres = solver
     return solver
