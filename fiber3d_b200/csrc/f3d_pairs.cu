@@ -702,7 +702,7 @@ static int make_plan(int kernel, int precision, int64_t ns, int64_t nt, const f3
   if (sl == 0) sl = (nt >= 4096) ? 1 : (nt >= 512 ? 8 : 32);
   if (tpt == 0) tpt = 1;
   if (!(tpt == 1 || tpt == 2 || tpt == 4)) return F3D_ERR_ARG;
-  if (tpt == 4 && (precision != F3D_FP64 || dual)) return F3D_ERR_ARG;  // four targets per thread: FP64 only
+  if (tpt == 4 && precision != F3D_FP64) return F3D_ERR_ARG;  // four targets per thread: FP64 only
   if (!(sl == 1 || sl == 8 || sl == 32)) return F3D_ERR_ARG;
   if (sl != 1 && tpt != 1) return F3D_ERR_ARG;
   const int64_t tpb = static_cast<int64_t>(kBlock / sl) * tpt;
@@ -773,7 +773,7 @@ template <int KIND, int MODE, int PREC, bool DUAL = false>
 static int dispatch_shape(const PairArgs &a, const Plan &p, cudaStream_t st) {
   if (p.sl == 1 && p.tpt == 1) return launch_one<KIND, MODE, PREC, 1, 1, DUAL>(a, p.ntb, p.nsplit, st);
   if (p.sl == 1 && p.tpt == 2) return launch_one<KIND, MODE, PREC, 2, 1, DUAL>(a, p.ntb, p.nsplit, st);
-  if constexpr (PREC == F3D_FP64 && !DUAL) {
+  if constexpr (PREC == F3D_FP64) {
     if (p.sl == 1 && p.tpt == 4) return launch_one<KIND, MODE, PREC, 4, 1, DUAL>(a, p.ntb, p.nsplit, st);
   }
   if (p.sl == 8) return launch_one<KIND, MODE, PREC, 1, 8, DUAL>(a, p.ntb, p.nsplit, st);

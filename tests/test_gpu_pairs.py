@@ -254,7 +254,8 @@ def test_fp32c_single_split_keeps_shared_counters(K, L):
         assert rel_err(u, ref) < TOL32
 
 
-@pytest.mark.parametrize("shape", [(1, 1, 0, 0), (2, 1, 5, -1), (1, 8, 3, 0), (1, 32, 0, -1), (2, 1, 1, 0)])
+@pytest.mark.parametrize("shape", [(1, 1, 0, 0), (2, 1, 5, -1), (1, 8, 3, 0), (1, 32, 0, -1), (2, 1, 1, 0),
+                                   (4, 1, 3, -1), (4, 1, 0, 0)])
 @pytest.mark.parametrize("mode", ["regularise", "skip_group"])
 def test_oseen_dual_equals_two_sums(L, shape, mode):
     """f3d_oseen_dual gives, bit for bit, the two FP64 Oseen sums it fuses."""
