@@ -660,7 +660,12 @@ int f3d_surface_quadrature(const double *nodes, int64_t n, const int32_t *triang
    potential source) on cube surfaces of `order` points per edge, the
    near field (27 neighbour leaves) summed directly with coincident points
    (|r| < 1e-150) excluded, as STKFMM's kernels exclude them.
-   All point and value arrays are device memory on `stream`'s device.    */
+   All point and value arrays are device memory of the device that was
+   current at f3d_fmm_create, which must be current for every call on the
+   handle; the handle allocates its tree and expansions there itself
+   (cudaMalloc in set_points / evaluate, kept for reuse) and frees them in
+   f3d_fmm_destroy.  A handle is not safe for concurrent calls: give each
+   host thread or stream its own.                                          */
 typedef struct f3d_fmm f3d_fmm;
 
 /* A handle for expansions of `order` (even, 4..16; n = 6 (order - 1)^2 + 2
