@@ -23,9 +23,11 @@
 //     translation (M2M, M2L, L2L) is generated on the fly from the geometry
 //     inside a gathered FP64 GEMM: a CTA tile of check-point rows times
 //     box columns, the K dimension running over the terms of the operator
-//     (8 children, up to 189 interaction-list boxes, 1 parent) and each
-//     term's 4n equivalent-density components; the kernel values are formed
-//     into shared memory for each K slice and reused by all 64 columns.
+//     (8 children, up to 189 interaction-list boxes and the parent; at level
+//     2, where every level-1 box neighbours every other, the 316 far
+//     offsets) and each term's 4n equivalent-density components; the kernel
+//     values are formed into shared memory for each K slice and reused by
+//     all 64 columns, on the FP64 FMA pipe.
 //   * Near field (the 27 neighbour leaves, both kernels, coincident points
 //     excluded) and the local expansion's evaluation at the targets (L2P)
 //     run in one kernel per target leaf.
