@@ -83,6 +83,25 @@ def test_deep_tree_is_deterministic(cube):
     assert torch.allclose(e, a / 2.5, rtol=1e-15, atol=0)
 
 
+def test_clustered_points_reach_the_deepest_tree():
+    """Two tight clusters far apart and leaves of ~2 sources: the depth
+    reaches 8 (dense slot tables of 2^24 boxes), most boxes are empty, and
+    the far field passes through six levels of translations."""
+    from fiber3d_b200 import fmm as F
+    rng = np.random.default_rng(12)
+    a = rng.normal(size=(1500, 3)) * 1e-3
+    b = rng.normal(size=(1500, 3)) * 1e-3 + np.array([1.0, 0.5, -0.25])
+    src = np.concatenate([a, b])
+    trg = np.concatenate([a[:700] + 2e-4, b[:700] - 2e-4])
+    f, nrm, dens = rng.normal(size=src.shape), rng.normal(size=src.shape), rng.normal(size=src.shape)
+    m = F.FMM(order=8, max_pts=2)
+    m.set_points(src, src, trg)
+    assert m.tree_info()["depth"] == 8
+    u = m.evaluate(sl_density=f, dl_normal=nrm, dl_density=dens).cpu().numpy()
+    ref = direct(src, f, src, nrm, dens, trg)
+    assert rel(u, ref) < TOL[8]
+
+
 def test_against_c_oracle():
     """A small case against the C oracle directly (no pair regularised:
     epsilon 0; no coincident points)."""
