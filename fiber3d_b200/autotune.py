@@ -55,7 +55,7 @@ def _key(kernel, precision, self_mode, ns, nt, same=False) -> str:
 
 # the symmetric self-sum's launch shape (f3d_pair_shape.sl = -1)
 SYMMETRIC = (1, -1, 0, -1)
-SYM_MAX_POINTS = 192 * 128
+SYM_MAX_POINTS = 1024 * 128
 
 
 def symmetric_eligible(kernel, precision, self_mode, ns, nt, same) -> bool:

@@ -57,8 +57,10 @@ namespace f3d {
 constexpr int kSymTile = 128;
 constexpr int kSymThreads = 64;  // two targets per thread
 constexpr int kSymWarps = kSymThreads / 32;
-constexpr int kSymMaxTiles = 192;
-constexpr size_t kSymMaxPartialBytes = size_t(256) << 20;
+// Partial storage grows as T (T + T2) x 3 KB: 28 MB for the 12000-node sphere,
+// 1 GB for 64000 fiber points onto 85600 targets; the caps keep it within 2 GiB.
+constexpr int kSymMaxTiles = 1024;
+constexpr size_t kSymMaxPartialBytes = size_t(2) << 30;
 
 struct SymArgs {
   const double *x, *dens, *nrm;  // x: nt x 3 (the first n are the sources); dens, nrm: n x 3

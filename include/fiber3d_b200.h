@@ -87,9 +87,13 @@ typedef struct f3d_pair_shape {
                       or F3D_SELF_SKIP_GROUP, r_target the r_source pointer
                       itself (the sources are its first ns points; targets
                       past ns are summed one-sided in the same launch) and,
-                      for SKIP_GROUP, trg_group the src_group pointer; up
-                      to 24576 sources.  tpt, nsplit and use_tma are then
-                      ignored.                                              */
+                      for SKIP_GROUP, trg_group the src_group pointer.
+                      Its workspace holds 3072 T (T + T2) bytes of
+                      partial sums, T = ceil(ns / 128), T2 =
+                      ceil((nt - ns) / 128) (twice that for the
+                      two-density Oseen pass), at most 2 GiB, and
+                      T <= 1024 (131072 sources).  tpt, nsplit and
+                      use_tma are then ignored.                             */
   int32_t nsplit;  /* source splits (grid.y); 0 = derive from the SM count    */
   int32_t use_tma; /* 0 or 1: stage full source tiles with cp.async.bulk
                       (default); -1: stage them with plain loads            */

@@ -175,12 +175,16 @@ def test_symmetric_shape_plan_checks(dll):
     # further targets after the sources: (T + T2) x T partial tiles
     assert dll.f3d_pair_workspace_bytes(1, 0, 12000, 16096, ctypes.byref(shp), ctypes.byref(nb)) == 0
     assert nb.value >= (94 + 32) * 94 * 128 * 3 * 8
-    # partial storage above 256 MiB: too large
-    assert dll.f3d_pair_workspace_bytes(1, 0, 256, 256 + 128 * 50000, ctypes.byref(shp), ctypes.byref(nb)) == 10
+    # partial storage above 2 GiB: too large
+    assert dll.f3d_pair_workspace_bytes(1, 0, 1024 * 128, 1024 * 128 + 128 * 100, ctypes.byref(shp),
+                                        ctypes.byref(nb)) == 10
     assert dll.f3d_pair_workspace_bytes(1, 1, 1000, 1000, ctypes.byref(shp), ctypes.byref(nb)) == 5   # FP32C
     assert dll.f3d_pair_workspace_bytes(2, 0, 1000, 1000, ctypes.byref(shp), ctypes.byref(nb)) == 5   # rotlet
-    assert dll.f3d_pair_workspace_bytes(0, 0, 192 * 128 + 1, 192 * 128 + 1, ctypes.byref(shp),
+    assert dll.f3d_pair_workspace_bytes(0, 0, 1024 * 128 + 1, 1024 * 128 + 1, ctypes.byref(shp),
                                         ctypes.byref(nb)) == 10
+    # 64000 fiber points onto 85600 targets (the largest time step): 1 GB of partials
+    assert dll.f3d_pair_workspace_bytes(0, 0, 64000, 85600, ctypes.byref(shp), ctypes.byref(nb)) == 0
+    assert nb.value >= 500 * (500 + 169) * 3072
 
 
 def test_block3_gemv_argument_checks(dll):

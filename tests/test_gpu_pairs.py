@@ -563,6 +563,42 @@ def test_symmetric_config2_step(K, L):
     assert rel_err(got, ref) < 1e-12
 
 
+def test_symmetric_largest_step_sum(K, L):
+    """The largest time step's fiber Oseen sum (2000 fibers x 32 points onto
+    the 85600 points of fibers, bodies and periphery, pairs within a fiber
+    skipped): 500 source tiles, 1 GB of partial sums; the symmetric form
+    against the regular kernel at full size, single and two-density."""
+    import ctypes
+    from fiber3d_b200 import geometry
+    P = geometry.hydro_step_problem(seed=3, nfib=2000, nshell=20000, shell_radius=12.0, fiber_ball=8.0,
+                                    body_shell=9.5)
+    fib = np.concatenate(P.fibers)
+    rest = np.concatenate([b.nodes() for b in P.bodies]
+                          + [P.shell.nodes])
+    x = torch.as_tensor(np.concatenate([fib, rest]), device="cuda")
+    n = fib.shape[0]
+    g = torch.as_tensor(np.concatenate([np.repeat(np.arange(2000), 32), -1 - np.arange(rest.shape[0])])
+                        .astype(np.int32), device="cuda")
+    rng = np.random.default_rng(1)
+    f1 = torch.as_tensor(rng.normal(size=(n, 3)), device="cuda")
+    f2 = torch.as_tensor(rng.normal(size=(n, 3)), device="cuda")
+    kw = dict(self_mode="skip_group", src_group=g[:n], trg_group=g)
+    a = K.pair_sum("oseen", x[:n], x, f1, shape=L.PairShape(*SYM), **kw)
+    b = K.pair_sum("oseen", x[:n], x, f1, shape=L.PairShape(4, 1, 0, -1), **kw)
+    assert rel_err(a.cpu().numpy(), b.cpu().numpy()) < 1e-13
+    shp = L.PairShape(*SYM)
+    nb = ctypes.c_size_t(0)
+    L.call("f3d_oseen_dual_workspace_bytes", n, x.shape[0], ctypes.byref(shp), ctypes.byref(nb))
+    ws = torch.zeros(nb.value, dtype=torch.uint8, device="cuda")
+    o1, o2 = torch.empty_like(a), torch.empty_like(a)
+    L.call("f3d_oseen_dual", L.SELF_MODE["skip_group"], L.ptr(x), L.ptr(x), L.ptr(f1), L.ptr(f2), L.ptr(g),
+           L.ptr(g), L.ptr(o1), L.ptr(o2), n, x.shape[0], 1.0, 5e-3, 1e-5, 0, ctypes.byref(shp), L.ptr(ws),
+           ws.numel(), L.stream_handle())
+    assert torch.equal(o1, a)
+    c = K.pair_sum("oseen", x[:n], x, f2, shape=shp, **kw)
+    assert torch.equal(o2, c)
+
+
 def test_symmetric_rejects_other_sums(K, L):
     rng = np.random.default_rng(3)
     x = rng.random((200, 3)); y = rng.random((200, 3)); d = rng.normal(size=(200, 3))
@@ -571,7 +607,7 @@ def test_symmetric_rejects_other_sums(K, L):
     with pytest.raises(L.F3DError):   # FP32C
         xt = torch.as_tensor(x, device="cuda")
         K.pair_sum("oseen", xt, xt, d, self_mode="skip_index", precision="fp32c", shape=L.PairShape(*SYM))
-    big = torch.zeros((192 * 128 + 1, 3), dtype=torch.float64, device="cuda")
+    big = torch.zeros((1024 * 128 + 1, 3), dtype=torch.float64, device="cuda")
     with pytest.raises(L.F3DError) as e:
         K.pair_sum("oseen", big, big, big, self_mode="skip_index", shape=L.PairShape(*SYM))
     assert e.value.status == 10
