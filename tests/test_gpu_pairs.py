@@ -573,7 +573,7 @@ def test_symmetric_largest_step_sum(K, L):
     P = geometry.hydro_step_problem(seed=3, nfib=2000, nshell=20000, shell_radius=12.0, fiber_ball=8.0,
                                     body_shell=9.5)
     fib = np.concatenate(P.fibers)
-    rest = np.concatenate([b.nodes() for b in P.bodies]
+    rest = np.concatenate([b.nodes for b in P.bodies]
                           + [P.shell.nodes])
     x = torch.as_tensor(np.concatenate([fib, rest]), device="cuda")
     n = fib.shape[0]
