@@ -1219,6 +1219,12 @@ def main():
     if args.impl == "reference":
         reference_arm(args, rank, world)
         return
+    # launch shapes are tuned on this run's own sums: a shape file left by
+    # other programs holds shapes tuned on other sizes of the same
+    # power-of-two size bucket
+    if "FIBER3D_B200_TUNE" not in os.environ:
+        import tempfile
+        os.environ["FIBER3D_B200_TUNE"] = os.path.join(tempfile.mkdtemp(prefix="f3d_bench_"), "pair_shapes.json")
     if world > 1:
         import datetime
         import torch

@@ -426,26 +426,57 @@ __global__ void __launch_bounds__(kSymThreads) pair_sym_kernel(const SymArgs a) 
     const int X = which == 0 ? I : J;
     const int64_t xbase = X < T ? static_cast<int64_t>(X) * kSymTile : a.n + static_cast<int64_t>(X - T) * kSymTile;
     const int64_t xend = X < T ? a.n : a.nt;
+    // A slot is the tile's 128 x 3 sums in output order; thread tid sums the
+    // pairs of doubles tid, tid + 64 and tid + 128 of every slot (16-byte
+    // loads, eight slots in flight), in slot order.
+    const int nvals = 3 * static_cast<int>(min(static_cast<int64_t>(kSymTile), xend - xbase));
 #pragma unroll
     for (int q = 0; q < ND; ++q) {
-      const double *p = (q == 0 ? a.partial : a.partial2) + static_cast<int64_t>(X) * T * slot_stride;
-      double v[2][3] = {{0.0, 0.0, 0.0}, {0.0, 0.0, 0.0}};
-#pragma unroll 4
-      for (int slot = 0; slot < T; ++slot) {
-        const double *ps = p + slot * slot_stride;
+      const double2 *p =
+          reinterpret_cast<const double2 *>((q == 0 ? a.partial : a.partial2) + static_cast<int64_t>(X) * T * slot_stride);
+      double2 v[3];
 #pragma unroll
-        for (int k = 0; k < 2; ++k)
+      for (int m = 0; m < 3; ++m) v[m] = make_double2(0.0, 0.0);
+      constexpr int kPairsPerSlot = kSymTile * 3 / 2;
+      int slot = 0;
+      for (; slot + 8 <= T; slot += 8) {
+        double2 r[8][3];
 #pragma unroll
-          for (int c = 0; c < 3; ++c) v[k][c] += __ldcg(ps + 3 * (tid + k * kSymThreads) + c);
+        for (int u = 0; u < 8; ++u)
+#pragma unroll
+          for (int m = 0; m < 3; ++m) r[u][m] = __ldcg(p + (slot + u) * kPairsPerSlot + tid + m * kSymThreads);
+#pragma unroll
+        for (int u = 0; u < 8; ++u)
+#pragma unroll
+          for (int m = 0; m < 3; ++m) {
+            v[m].x += r[u][m].x;
+            v[m].y += r[u][m].y;
+          }
       }
-      double *const outq = q == 0 ? a.out : a.out2;
+      for (; slot < T; ++slot)
 #pragma unroll
-      for (int k = 0; k < 2; ++k) {
-        const int64_t t = xbase + tid + k * kSymThreads;
-        if (t < xend) {
-          double *o = outq + 3 * t;
+        for (int m = 0; m < 3; ++m) {
+          const double2 r = __ldcg(p + slot * kPairsPerSlot + tid + m * kSymThreads);
+          v[m].x += r.x;
+          v[m].y += r.y;
+        }
+      double *const o = (q == 0 ? a.out : a.out2) + 3 * xbase;
+      const bool vec = (reinterpret_cast<uintptr_t>(o) & 15) == 0;
 #pragma unroll
-          for (int c = 0; c < 3; ++c) o[c] = a.accumulate ? o[c] + v[k][c] * a.scale : v[k][c] * a.scale;
+      for (int m = 0; m < 3; ++m) {
+        const int f = 2 * (tid + m * kSymThreads);
+        double2 w = make_double2(v[m].x * a.scale, v[m].y * a.scale);
+        if (vec && f + 1 < nvals) {
+          double2 *o2 = reinterpret_cast<double2 *>(o + f);
+          if (a.accumulate) {
+            const double2 old = *o2;
+            w.x += old.x;
+            w.y += old.y;
+          }
+          *o2 = w;
+        } else {
+          if (f < nvals) o[f] = a.accumulate ? o[f] + w.x : w.x;
+          if (f + 1 < nvals) o[f + 1] = a.accumulate ? o[f + 1] + w.y : w.y;
         }
       }
     }

@@ -144,6 +144,7 @@ def pair_sum(kernel: str, r_source, r_target, density, normal=None, *, eta=1.0, 
 
 
 _ws_bytes: dict = {}
+_host_bytes: dict = {}  # (kernel, ns, nt, one point set) -> f3d_pair_host_bytes
 _tuned: dict = {}  # host fast path: (device, sum, sizes, one point set) -> tuned launch shape
 
 
@@ -169,9 +170,9 @@ def _host_points(x, name: str):
     """A host (N, 3) float64 array (numpy or CPU tensor) -> (contiguous array
     or tensor kept alive, its address, N)."""
     if isinstance(x, torch.Tensor):
-        t = x.detach()
+        t = x
         if t.dtype != torch.float64 or not t.is_contiguous():
-            t = t.to(torch.float64).contiguous()
+            t = t.detach().to(torch.float64).contiguous()
         n = t.numel()
         ptr = t.data_ptr()
     else:
@@ -211,9 +212,13 @@ def _drop_in_host(kernel, r_source, r_target, density, normal, self_mode, eta, r
         _lib.call("f3d_pair_workspace_bytes", k, p, ns, nt, shp, ctypes.byref(nb))
         nbytes = _ws_bytes[key] = nb.value
     ws_ptr, ws_len = _lib.Workspace.get(dev).ensure(nbytes)
-    hb = ctypes.c_size_t(0)
-    _lib.call("f3d_pair_host_bytes", k, ns, nt, int(p_rs == p_rt), ctypes.byref(hb))
-    st_ptr, st_len = _lib.Staging.get(dev).ensure(hb.value)
+    hkey = (k, ns, nt, p_rs == p_rt)
+    hbytes = _host_bytes.get(hkey)
+    if hbytes is None:
+        hb = ctypes.c_size_t(0)
+        _lib.call("f3d_pair_host_bytes", k, ns, nt, int(p_rs == p_rt), ctypes.byref(hb))
+        hbytes = _host_bytes[hkey] = hb.value
+    st_ptr, st_len = _lib.Staging.get(dev).ensure(hbytes)
     status = _lib.lib().f3d_pair_sum_host(k, p, m, p_rs, p_rt, p_d, p_n, out.data_ptr(), ns, nt, float(eta),
                                           float(reg), float(epsilon_distance), shp, st_ptr, st_len, ws_ptr, ws_len,
                                           _lib.stream_handle(dev))

@@ -164,7 +164,11 @@ int f3d_pair_sum(int kernel, int precision, int self_mode,
    `device_buffer` (f3d_pair_host_bytes of them, 256-byte aligned), the sum
    runs on `stream` with `workspace` as f3d_pair_sum's, the result is copied
    into `out` (nt x 3, host) and the stream is synchronised.  Page-locked
-   host buffers make the copies asynchronous.  Returns F3D_OK, an argument
+   host buffers that the device can address (cudaHostAlloc, or
+   cudaHostRegister under unified addressing) skip the copies: when every
+   input is one, a single staging kernel reads them all, and such an `out`
+   (8-byte aligned) is written by the pair kernel itself.  Other host
+   memory is copied with cudaMemcpyAsync.  Returns F3D_OK, an argument
    status, or the first status a kernel recorded in the device error word
    (then cleared), e.g. F3D_ERR_TIMEOUT.  F3D_SELF_SKIP_GROUP is not
    accepted (no group ids on this path). */
