@@ -19,6 +19,7 @@ LIBPATH = Path(__file__).resolve().parent / "_lib" / "libfiber3d_b200.so"
 # status codes (f3d_status)
 F3D_OK = 0
 F3D_ERR_TIMEOUT = 8
+F3D_ERR_SINGULAR = 9
 
 # enums
 KERNEL = {"oseen": 0, "stresslet": 1, "rotlet": 2, "traction": 3}
@@ -92,6 +93,7 @@ SIGNATURES: dict[str, list] = {
     "f3d_singularity_vectors": [_P, _P, _P, _P, _I64, _D, _D, _D, _P, _SZ, _P],
     "f3d_shell_residual": [_P, _P, _P, _P, _P, _P, _I64, _P, _P],
     "f3d_block3_gemv": [_P, _P, _P, _I64, _P],
+    "f3d_shell_block_inverse": [_P, _P, _P, _P, _I64, _P, _P],
     "f3d_fmm_create": [_I, _I, _P, _P, _P, _P],
     "f3d_fmm_destroy": [_P],
     "f3d_fmm_set_box": [_P, _P, _D],
@@ -143,6 +145,8 @@ SIGNATURES: dict[str, list] = {
                                _P],
     "f3d_warmstart_guess": [_P, _P, _P, _I64, _I64, ctypes.c_int32, ctypes.c_int32, _P, _P, _P, _P, _P],
     "f3d_batched_inverse": [_P, _P, _P, ctypes.c_int32, ctypes.c_int32, _P, _P, _P],
+    "f3d_dense_inverse_workspace_bytes": [_I64, _I64, _P],
+    "f3d_dense_inverse": [_P, _I64, _I64, _P, _SZ, _P],
     "f3d_block_gemv": [_I, _P, _P, _P, _P, ctypes.c_int32, ctypes.c_int32, _P, _P, _P],
 }
 _RESTYPE = {"f3d_version": ctypes.c_char_p, "f3d_status_string": ctypes.c_char_p,

@@ -55,6 +55,11 @@ __device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *bar, uint32_t by
                : "memory");
 }
 
+// One arrival on `bar` (no transaction bytes).
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(bar)) : "memory");
+}
+
 // 1-D bulk copy global -> shared, completion signalled on `bar` as tx bytes.
 // dst, src 16-byte aligned; bytes a multiple of 16.  No multicast.
 __device__ __forceinline__ void bulk_copy_g2s(void *dst, const void *src, uint32_t bytes,

@@ -69,6 +69,43 @@ __global__ void block3_gemv_kernel(const double *__restrict__ B, const double *_
   y[3 * i + 2] = fma(b[6], x0, fma(b[7], x1, b[8] * x2));
 }
 
+// Binv_i = B_i^-1, B_i = -(E_i + I) / w_i + n_i n_i^T: the 3 x 3 diagonal
+// blocks of the dense shell operator.  The inverse is the adjugate over the
+// determinant (cofactor expansion with fused products); a block whose
+// determinant is zero or not finite is counted in *info.
+__global__ void shell_block_inverse_kernel(const double *__restrict__ E, const double *__restrict__ w,
+                                           const double *__restrict__ nrm, double *Binv, int64_t n,
+                                           int32_t *info) {
+  const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double inv_w = 1.0 / w[i];
+  const double n0 = nrm[3 * i], n1 = nrm[3 * i + 1], n2 = nrm[3 * i + 2];
+  const double nn[3] = {n0, n1, n2};
+  double b[3][3];
+#pragma unroll
+  for (int r = 0; r < 3; ++r)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) b[r][c] = fma(nn[r], nn[c], -(E[9 * i + 3 * r + c] + (r == c ? 1.0 : 0.0)) * inv_w);
+  const double c00 = fma(b[1][1], b[2][2], -b[1][2] * b[2][1]);
+  const double c01 = fma(b[1][2], b[2][0], -b[1][0] * b[2][2]);
+  const double c02 = fma(b[1][0], b[2][1], -b[1][1] * b[2][0]);
+  const double det = fma(b[0][0], c00, fma(b[0][1], c01, b[0][2] * c02));
+  if (!(det != 0.0) || !isfinite(det)) {
+    if (info) atomicAdd(info, 1);
+  }
+  const double id = 1.0 / det;
+  double *o = Binv + 9 * i;
+  o[0] = c00 * id;
+  o[1] = fma(b[0][2], b[2][1], -b[0][1] * b[2][2]) * id;
+  o[2] = fma(b[0][1], b[1][2], -b[0][2] * b[1][1]) * id;
+  o[3] = c01 * id;
+  o[4] = fma(b[0][0], b[2][2], -b[0][2] * b[2][0]) * id;
+  o[5] = fma(b[0][2], b[1][0], -b[0][0] * b[1][2]) * id;
+  o[6] = c02 * id;
+  o[7] = fma(b[0][1], b[2][0], -b[0][0] * b[2][1]) * id;
+  o[8] = fma(b[0][0], b[1][1], -b[0][1] * b[1][0]) * id;
+}
+
 // res_i = v_i - E_i mu_i - mu_i + n_i s   (mu = q / w)
 __global__ void shell_residual_kernel(const double *__restrict__ v, const double *__restrict__ E,
                                       const double *__restrict__ w, const double *__restrict__ nrm,
@@ -429,6 +466,16 @@ int f3d_block3_gemv(const double *B, const double *x, double *y, int64_t n, void
   if (x == y) return F3D_ERR_ARG;
   f3d::block3_gemv_kernel<<<static_cast<unsigned>((n + 255) / 256), 256, 0, static_cast<cudaStream_t>(stream)>>>(
       B, x, y, n);
+  return f3d::launch_status();
+}
+
+int f3d_shell_block_inverse(const double *E, const double *weights, const double *normals, double *Binv,
+                            int64_t n, int32_t *info, void *stream) {
+  if (n < 0) return F3D_ERR_SHAPE;
+  if (n == 0) return F3D_OK;
+  if (!E || !weights || !normals || !Binv) return F3D_ERR_NULL;
+  f3d::shell_block_inverse_kernel<<<static_cast<unsigned>((n + 255) / 256), 256, 0,
+                                    static_cast<cudaStream_t>(stream)>>>(E, weights, normals, Binv, n, info);
   return f3d::launch_status();
 }
 

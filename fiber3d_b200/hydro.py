@@ -183,18 +183,23 @@ class ShellOperator:
         self.inv32 = None
         self.inv16 = None
         self.block_inv = None
+        self.ld = 3 * self.n
         if pc == "block":
             self.build_block_inverse()
         elif build_inverse:
             self.build_inverse()
 
     def build_block_inverse(self):
-        """Inverses of the dense operator's 3 x 3 diagonal blocks (set-up, host)."""
-        E = self.E.cpu().numpy().reshape(-1, 3, 3)
-        w = self.weights.cpu().numpy()
-        nr = self.normals.cpu().numpy()
-        B = -(E + np.eye(3)) / w[:, None, None] + nr[:, :, None] * nr[:, None, :]
-        self.block_inv = torch.as_tensor(np.linalg.inv(B).reshape(-1, 9), device=self.device).contiguous()
+        """Inverses of the dense operator's 3 x 3 diagonal blocks
+        (f3d_shell_block_inverse, on the device)."""
+        self.block_inv = torch.empty((self.n, 9), dtype=torch.float64, device=self.device)
+        info = torch.zeros(1, dtype=torch.int32, device=self.device)
+        _lib.call("f3d_shell_block_inverse", _lib.ptr(self.E), _lib.ptr(self.weights), _lib.ptr(self.normals),
+                  _lib.ptr(self.block_inv), self.n, _lib.ptr(info), _lib.stream_handle(self.device))
+        bad = int(info.item())
+        if bad:
+            raise _lib.F3DError("f3d_shell_block_inverse", _lib.F3D_ERR_SINGULAR,
+                                f"{bad} singular 3 x 3 periphery blocks")
 
     def dense(self) -> torch.Tensor:
         m = 3 * self.n
@@ -205,22 +210,29 @@ class ShellOperator:
         return M
 
     def build_inverse(self):
-        """Explicit inverse of the dense shell operator (one-time set-up; the
-        LU factorisation itself is cuSOLVER's via torch.linalg)."""
-        M = self.dense()
-        self.inv64 = torch.linalg.inv(M)
-        del M
-        self.inv32 = torch.empty(self.inv64.shape, dtype=torch.float32, device=self.device)
-        _lib.call("f3d_cast_to_float", _lib.ptr(self.inv64), _lib.ptr(self.inv32), self.inv64.numel(),
+        """Explicit inverse of the dense shell operator (one-time set-up):
+        the operator is written into a buffer padded to a multiple of 128
+        rows and inverted in place there (f3d_dense_inverse); inv64 and inv32
+        are the top-left 3n x 3n views, row stride self.ld."""
+        m = 3 * self.n
+        self.ld = ld = dense_inverse_ld(m)
+        full = torch.empty((ld, ld), dtype=torch.float64, device=self.device)
+        _lib.call("f3d_surface_dense", 0, _lib.ptr(self.nodes), _lib.ptr(self.normals), _lib.ptr(self.E),
+                  _lib.ptr(self.weights), None, _lib.ptr(full), self.n, ld, self.eta, self.reg, self.eps,
                   _lib.stream_handle(self.device))
+        dense_inverse(full, m)
+        self.inv64 = full[:m, :m]
+        full32 = torch.empty((ld, ld), dtype=torch.float32, device=self.device)
+        _lib.call("f3d_cast_to_float", _lib.ptr(full), _lib.ptr(full32), full.numel(),
+                  _lib.stream_handle(self.device))
+        self.inv32 = full32[:m, :m]
         # FP16 rows scaled by powers of two, the 3x3 node blocks on the
         # diagonal kept in FP64 (the inverse of this second-kind operator is
         # dominated by them; the rest spans a few decades per row)
-        m = 3 * self.n
         self.inv16 = torch.empty((m, m), dtype=torch.float16, device=self.device)
         self.scale16 = torch.empty(m, dtype=torch.float32, device=self.device)
         self.diag16 = torch.empty((m, 3), dtype=torch.float64, device=self.device)
-        _lib.call("f3d_quantize_rows_f16", _lib.ptr(self.inv64), m, m, m, 3, _lib.ptr(self.inv16), m,
+        _lib.call("f3d_quantize_rows_f16", _lib.ptr(self.inv64), ld, m, m, 3, _lib.ptr(self.inv16), m,
                   _lib.ptr(self.scale16), _lib.ptr(self.diag16), _lib.stream_handle(self.device))
 
     def apply(self, x: torch.Tensor, y: torch.Tensor, storage: str = "fp64") -> torch.Tensor:
@@ -236,9 +248,32 @@ class ShellOperator:
                       _lib.ptr(x), _lib.ptr(y), m, m, st)
         else:
             M = self.inv64 if storage == "fp64" else self.inv32
-            _lib.call("f3d_gemv", _lib.PRECISION["fp64" if storage == "fp64" else "fp32c"], _lib.ptr(M), m,
+            _lib.call("f3d_gemv", _lib.PRECISION["fp64" if storage == "fp64" else "fp32c"], _lib.ptr(M), self.ld,
                       _lib.ptr(x), _lib.ptr(y), m, m, st)
         return y
+
+
+def dense_inverse_ld(m: int) -> int:
+    """Rows (and row stride) of the buffer f3d_dense_inverse inverts an
+    m x m matrix in: m rounded up to a multiple of 128."""
+    return -(-m // 128) * 128
+
+
+def dense_inverse(A: torch.Tensor, m: int) -> torch.Tensor:
+    """Inverts the m x m top-left corner of the square FP64 device buffer A
+    (dense_inverse_ld(m) rows or more, row stride A.shape[1]) in place
+    (f3d_dense_inverse: blocked Gauss-Jordan elimination on the device);
+    the padding becomes the identity.  Raises on a singular pivot block."""
+    if A.dtype != torch.float64 or not A.is_cuda or not A.is_contiguous() or A.dim() != 2:
+        raise ValueError("A must be a contiguous 2-D float64 CUDA tensor")
+    ld = A.shape[1]
+    if A.shape[0] < dense_inverse_ld(m) or ld < dense_inverse_ld(m):
+        raise ValueError(f"A must have at least {dense_inverse_ld(m)} rows and columns for m = {m}")
+    nb = ctypes.c_size_t(0)
+    _lib.call("f3d_dense_inverse_workspace_bytes", m, ld, ctypes.byref(nb))
+    ws = torch.empty(max(nb.value, 1), dtype=torch.uint8, device=A.device)
+    _lib.call("f3d_dense_inverse", _lib.ptr(A), m, ld, _lib.ptr(ws), ws.numel(), _lib.stream_handle(A.device))
+    return A
 
 
 def singularity_vectors(nodes, normals, weights, eta, reg, eps) -> torch.Tensor:
@@ -522,10 +557,14 @@ class HydroSystem:
             w = self.body_w[a:b].contiguous()
             E = singularity_vectors(ref, refn, w, P.eta, P.reg, P.eps_dist)
             n = b - a
-            A = torch.empty((3 * n + 6, 3 * n + 6), dtype=torch.float64, device=self.device)
+            mb = 3 * n + 6
+            ldb = dense_inverse_ld(mb)
+            A = torch.empty((ldb, ldb), dtype=torch.float64, device=self.device)
             _lib.call("f3d_surface_dense", 1, _lib.ptr(ref), _lib.ptr(refn), _lib.ptr(E), _lib.ptr(w),
-                      _lib.ptr(origin), _lib.ptr(A), n, 3 * n + 6, P.eta, P.reg, P.eps_dist, st)
-            self.body_inv.append(torch.linalg.inv(A))
+                      _lib.ptr(origin), _lib.ptr(A), n, ldb, P.eta, P.reg, P.eps_dist, st)
+            dense_inverse(A, mb)
+            self.body_inv.append(A[:mb, :mb].contiguous())
+            del A
         # all body inverses back to back, applied by one batched GEMV
         m = np.array([3 * n + 6 for n in self.nb], dtype=np.int64)
         moff = np.concatenate([[0], np.cumsum(m * m)[:-1]]).astype(np.int64)

@@ -350,6 +350,26 @@ int f3d_batched_lu_solve(const double *LU, const int64_t *matrix_offsets,
 int f3d_batched_inverse(double *A, const int64_t *matrix_offsets, const int32_t *sizes,
                         int32_t count, int32_t max_n, float *A32, int32_t *info, void *stream);
 
+/* Explicit inverse of one dense FP64 matrix, in place: blocked Gauss-Jordan
+   elimination over 128-row blocks, each step an FP64 GEMM of rank 128 over
+   the whole matrix (2 n^3 flops, as LU plus inversion), partial pivoting
+   inside each 128 x 128 pivot block (no row exchange between blocks: stable
+   for the second-kind operators inverted here, whose diagonal blocks carry
+   the 1/w-scaled identity).  Replaces scipy.linalg.lu_factor of the dense
+   shell operator (tstep/tstep.py:327-348) and of the rigid-body blocks
+   (tstep/tstep_utils.py:1341-1386); the preconditioner then applies the
+   inverse as a product.  A: row-major with leading dimension ld (even),
+   at least np = n rounded up to a multiple of 128 rows of ld >= np
+   doubles, 16-byte aligned, the matrix in its top-left n x n corner; the
+   call sets the padding to the identity (which stays the identity) and
+   leaves the inverse in the top-left corner.  workspace:
+   f3d_dense_inverse_workspace_bytes(n, ld) bytes, 256-byte aligned.
+   Synchronises `stream`.  F3D_ERR_SINGULAR when a pivot block is singular
+   to working precision. */
+int f3d_dense_inverse_workspace_bytes(int64_t n, int64_t ld, size_t *bytes);
+int f3d_dense_inverse(double *A, int64_t n, int64_t ld, void *workspace, size_t workspace_bytes,
+                      void *stream);
+
 /* y + vector_offsets[b] = M_b (x + vector_offsets[b]) for every block, M_b
    row-major sizes[b] x sizes[b] at M + matrix_offsets[b]; M is double
    (F3D_FP64) or float (F3D_FP32C); x, y double, distinct.  FP64 sums. */
@@ -441,6 +461,14 @@ int f3d_shell_residual(const double *v, const double *E, const double *weights,
    shell operator of tstep/tstep.py:327-347: a matrix-free alternative to
    its LU (tstep.py:348) for peripheries whose dense inverse does not fit. */
 int f3d_block3_gemv(const double *B, const double *x, double *y, int64_t n, void *stream);
+
+/* Binv (9n doubles, row-major 3 x 3 blocks) = the inverses of those diagonal
+   blocks, B_i = -(E_i + I) / w_i + n_i n_i^T (E: 9n singularity vectors as
+   f3d_singularity_vectors writes them; weights n; normals 3n), by adjugate
+   over determinant.  When info (one device int32, zeroed by the caller) is
+   non-NULL, every block whose determinant is zero or not finite adds 1. */
+int f3d_shell_block_inverse(const double *E, const double *weights, const double *normals, double *Binv,
+                            int64_t n, int32_t *info, void *stream);
 
 /* Rigid-body rows of the matvec (tstep/tstep.py:1118-1143): for body b with
    unknowns x[x_off[b]..] = [lambda (3nb), U, Omega]:

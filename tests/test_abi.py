@@ -196,3 +196,33 @@ def test_block3_gemv_argument_checks(dll):
     assert dll.f3d_block3_gemv(p, p, q, -1, None) == SHAPE
     assert dll.f3d_block3_gemv(None, p, q, 4, None) == NULL
     assert dll.f3d_block3_gemv(p, q, q, 4, None) == ARG
+
+
+def test_shell_block_inverse_argument_checks(dll):
+    NULL, SHAPE = 1, 2
+    p = ctypes.c_void_p(256)
+    assert dll.f3d_shell_block_inverse(None, None, None, None, 0, None, None) == 0
+    assert dll.f3d_shell_block_inverse(p, p, p, p, -1, None, None) == SHAPE
+    assert dll.f3d_shell_block_inverse(p, None, p, p, 4, None, None) == NULL
+
+
+def test_dense_inverse_sizes_and_checks(dll):
+    """Workspace of the dense inverse: a 128 x 128 pivot block, the saved
+    block row (128 x ld) and one info word per 128-row step; the entry
+    checks sizes, pointers, the leading dimension, alignment and the
+    workspace before any CUDA call."""
+    NULL, SHAPE, ALIGN, WORKSPACE = 1, 2, 3, 4
+    nb = ctypes.c_size_t(0)
+    assert dll.f3d_dense_inverse_workspace_bytes(300, 384, ctypes.byref(nb)) == 0
+    need = nb.value
+    assert need >= 128 * 128 * 8 + 128 * 384 * 8 + 3 * 4
+    assert dll.f3d_dense_inverse_workspace_bytes(-1, 0, ctypes.byref(nb)) == SHAPE
+    assert dll.f3d_dense_inverse_workspace_bytes(3, 128, None) == NULL
+    A, ws = ctypes.c_void_p(4096), ctypes.c_void_p(8192)
+    assert dll.f3d_dense_inverse(None, 0, 0, None, 0, None) == 0
+    assert dll.f3d_dense_inverse(A, -3, 384, ws, need, None) == SHAPE
+    assert dll.f3d_dense_inverse(None, 300, 384, ws, need, None) == NULL
+    assert dll.f3d_dense_inverse(A, 300, 300, ws, need, None) == SHAPE      # ld below 384
+    assert dll.f3d_dense_inverse(A, 300, 385, ws, need, None) == SHAPE      # odd ld
+    assert dll.f3d_dense_inverse(ctypes.c_void_p(4104), 300, 384, ws, need, None) == ALIGN
+    assert dll.f3d_dense_inverse(A, 300, 384, ws, need - 1, None) == WORKSPACE

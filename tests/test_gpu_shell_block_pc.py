@@ -88,3 +88,31 @@ def test_bad_option():
     P = geometry.hydro_step_problem(seed=5, nfib=4, nshell=200, shell_radius=10.0, nbody=0)
     with pytest.raises(ValueError):
         H.ShellOperator(P.shell, pc="lu")
+
+
+def test_singular_blocks_are_counted():
+    """A block made exactly singular (E_i = -I and n_i = e_z give
+    B_i = diag(0, 0, 1) in any rounding) is counted in info; the others are
+    the inverses numpy finds."""
+    from fiber3d_b200 import _lib
+    rng = np.random.default_rng(3)
+    n = 5
+    nrm = rng.normal(size=(n, 3))
+    nrm /= np.linalg.norm(nrm, axis=1, keepdims=True)
+    w = rng.uniform(0.05, 0.2, n)
+    E = rng.normal(size=(n, 3, 3)) * 0.1 - 0.5 * np.eye(3)
+    E[2] = -np.eye(3)
+    nrm[2] = [0.0, 0.0, 1.0]
+    # device copies held for the call (a temporary freed right after its
+    # pointer is taken could be handed to the next copy before the kernel runs)
+    dE, dw, dn = (torch.as_tensor(np.ascontiguousarray(a), device="cuda") for a in (E.reshape(n, 9), w, nrm))
+    out = torch.empty((n, 9), dtype=torch.float64, device="cuda")
+    info = torch.zeros(1, dtype=torch.int32, device="cuda")
+    _lib.call("f3d_shell_block_inverse", _lib.ptr(dE), _lib.ptr(dw), _lib.ptr(dn),
+              _lib.ptr(out), n, _lib.ptr(info), _lib.stream_handle(torch.device("cuda")))
+    assert int(info.item()) == 1
+    B = -(E + np.eye(3)) / w[:, None, None] + nrm[:, :, None] * nrm[:, None, :]
+    got = out.cpu().numpy().reshape(n, 3, 3)
+    for i in (0, 1, 3, 4):
+        ref = np.linalg.inv(B[i])
+        assert np.abs(got[i] - ref).max() < 1e-13 * np.abs(ref).max()
