@@ -166,7 +166,7 @@ def measured_peak(L, precision: str, torch, gpu_index: int = 0):
     sink = torch.zeros(1, dtype=torch.float64, device="cuda")
     flops = ctypes.c_double(0)
     st = L.stream_handle()
-    prec = L.PRECISION[precision]
+    prec = {"fp64": 0, "fp32c": 1, "fp64_mma": 2}[precision]
     for _ in range(2):
         L.call("f3d_probe_fma", prec, 2000, L.ptr(sink), ctypes.byref(flops), st)
     torch.cuda.synchronize()
@@ -480,8 +480,50 @@ def fmm_reference_arm(args, world):
     print(json.dumps(line), flush=True)
 
 
+def dense_inverse_reference_arm(args, world):
+    """The dense_inverse workload's reference: fiber3d's scipy.linalg.lu_factor
+    of the dense shell operator (tstep.py:348) on the host cores, the operator
+    built by the oracle's restatement (tstep.py:327-347) for a sphere of
+    args.dense_cpu_nodes nodes and the time scaled by the cube of the size."""
+    import scipy.linalg as sla
+    from fiber3d_b200 import geometry
+    from oracle import kernels_np as KN, system as S
+    ns = max(200, min(args.nshell, int(args.dense_cpu_nodes)))
+    nodes, normals = geometry.fibonacci_sphere(ns, args.shell_radius)
+    w = np.full(ns, 4.0 * np.pi * args.shell_radius ** 2 / ns)
+    E = S.singularity_vectors(nodes, normals, w, 1.0)
+    M = KN.stresslet_kernel_times_normal_dense(nodes, normals, eta=1.0)
+    for i in range(ns):
+        M[3 * i:3 * i + 3, 3 * i:3 * i + 3] -= E[i] / w[i] + np.eye(3) / w[i]
+    M += KN.complementary_kernel(None, normals)
+    times = []
+    for step in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
+        sla.lu_factor(M)
+        if step >= args.warmup:
+            times.append(time.perf_counter() - t0)
+    m, ms_ = 3 * args.nshell, 3 * ns
+    value = statistics.median(times) * (m / ms_) ** 3 * 1e3
+    hc = host_cores()
+    line = {"impl": "reference", "metric": "periphery preconditioner set-up: dense inverse (ms)", "value": value,
+            "unit": "ms", "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": value,
+            "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (Fibonacci sphere)",
+            "config": {"workload": "dense_inverse", "nodes": int(args.nshell), "matrix": int(m),
+                       "radius": args.shell_radius},
+            "parallelism": f"host cores (rank 0 of {world})",
+            "cpu_baseline": {"value": value, "unit": "ms", "cores": hc["threads"], **hc, "kind": "reference",
+                             "sample": f"scipy.linalg.lu_factor of the {ms_} x {ms_} operator of a {ns}-node "
+                                       f"sphere, scaled by ({m}/{ms_})^3"},
+            "e2e": {"value": value, "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
 def reference_arm(args, rank, world):
     if rank != 0:
+        return
+    if args.workload == "dense_inverse":
+        dense_inverse_reference_arm(args, world)
         return
     if args.workload == "surface_quadrature":
         quadrature_reference_arm(args, world)
@@ -916,6 +958,130 @@ def quadrature_arm(args, rank, world, local):
     return line
 
 
+def dense_inverse_arm(args, rank, world, local):
+    """The periphery preconditioner's set-up: the dense shell operator of an
+    args.nshell-node sphere (Fibonacci nodes, equal-area weights, radius
+    args.shell_radius; tstep.py:327-347) inverted in place by
+    f3d_dense_inverse (blocked Gauss-Jordan, FP64 tensor-core updates).  A
+    step is one inversion of the 3N x 3N matrix (a fresh copy each time).
+    fiber3d factors this matrix with scipy.linalg.lu_factor (tstep.py:348):
+    that call on the host cores, timed on a smaller sphere and scaled by the
+    cube of the size, is the CPU baseline; cuSOLVER's inverse
+    (torch.linalg.inv) of the same matrix is reported beside it."""
+    import ctypes
+    import torch
+    from fiber3d_b200 import _lib as L, geometry, hydro as H, replicas
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    steps, warmup = max(1, min(args.steps, 3)), min(args.warmup, 1)
+
+    def operator(n):
+        nodes, normals = geometry.fibonacci_sphere(n, args.shell_radius)
+        w = np.full(n, 4.0 * np.pi * args.shell_radius ** 2 / n)
+        sh = H.ShellOperator(H.Shell(nodes, normals, w), 1.0, 5e-3, 1e-5, dev, build_inverse=False)
+        m = 3 * n
+        ld = H.dense_inverse_ld(m)
+        M = torch.zeros((ld, ld), dtype=torch.float64, device=dev)
+        L.call("f3d_surface_dense", 0, L.ptr(sh.nodes), L.ptr(sh.normals), L.ptr(sh.E), L.ptr(sh.weights), None,
+               L.ptr(M), n, ld, 1.0, 5e-3, 1e-5, L.stream_handle(dev))
+        return (nodes, normals, w), M, m
+
+    host, M0, m = operator(args.nshell)
+    ld = M0.shape[0]
+    A = torch.empty_like(M0)
+    nb = ctypes.c_size_t(0)
+    L.call("f3d_dense_inverse_workspace_bytes", m, ld, ctypes.byref(nb))
+    ws = torch.empty(nb.value, dtype=torch.uint8, device=dev)
+
+    def invert():
+        L.call("f3d_dense_inverse", L.ptr(A), m, ld, L.ptr(ws), ws.numel(), L.stream_handle(dev))
+
+    for _ in range(warmup):
+        A.copy_(M0)
+        invert()
+    times = []
+    with ClockSampler(local) as clk:
+        replicas.barrier()
+        for _ in range(steps):
+            A.copy_(M0)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            invert()
+            e1.record()
+            e1.synchronize()
+            times.append(e0.elapsed_time(e1))
+        replicas.barrier()
+    ms = replicas.max_over_ranks([statistics.median(times)], dev)[0]
+    # accuracy: residual of the inverse on a random vector, and cuSOLVER's inverse
+    g = torch.Generator(device=dev).manual_seed(1)
+    x = torch.randn(m, generator=g, device=dev, dtype=torch.float64)
+    Mm = M0[:m, :m]
+    res = float(torch.linalg.vector_norm(Mm @ (A[:m, :m] @ x) - x) / torch.linalg.vector_norm(x))
+    X = A[:m, :m].clone()
+    del A
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    ref = torch.linalg.inv(Mm)
+    torch.cuda.synchronize()
+    lib_s = time.perf_counter() - t0
+    diff = float(torch.linalg.matrix_norm(X - ref) / torch.linalg.matrix_norm(ref))
+    del ref, X
+    # end to end: the ShellOperator set-up from host arrays (singularity
+    # vectors, dense operator, inverse, FP32 and row-scaled FP16 copies)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    sh = H.ShellOperator(H.Shell(*host), 1.0, 5e-3, 1e-5, dev)
+    torch.cuda.synchronize()
+    e2e_s = time.perf_counter() - t0
+    del sh
+    torch.cuda.empty_cache()
+    peak, peak_clk = measured_peak(L, "fp64_mma", torch, local)
+    npad = ld
+    flops = 2.0 * float(npad) ** 3
+    achieved = flops / (ms * 1e-3)
+    line = {"metric": "periphery preconditioner set-up: dense inverse (ms)", "value": ms, "unit": "ms",
+            "n_gpus": world, "steps": steps, "warmup": warmup, "ms_per_step": ms, "higher_is_better": False,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (Fibonacci sphere)",
+            "config": {"workload": "dense_inverse", "nodes": int(args.nshell), "matrix": int(m),
+                       "padded": int(npad), "radius": args.shell_radius,
+                       "l2": f"matrix {m * m * 8 / 1e9:.1f} GB, far above L2"},
+            "roofline": {"bound": "fp64-tensor", "achieved": achieved / 1e12, "peak": peak / 1e12,
+                         "unit": "TFLOP/s", "frac": achieved / peak, "traffic": None,
+                         "kernel": "gj_update_kernel (with the per-step pivot-block inverse and panel)",
+                         "note": "2 np^3 flops of the whole call (np = matrix size padded to 128); peak = "
+                                 "measured FP64 tensor-core MMA rate (f3d_probe_fma precision 2)",
+                         "peak_clocks": peak_clk},
+            "checks": {"residual_M_Xv_minus_v": res, "rel_diff_vs_cusolver_inverse": diff},
+            "library_baseline": {"torch_linalg_inv_ms": lib_s * 1e3,
+                                 "note": "cuSOLVER getrf + getri through torch on the same matrix"},
+            "e2e": {"value": e2e_s * 1e3, "unit": "ms",
+                    "h2d_bytes_per_step": int(sum(a.nbytes for a in host)), "d2h_bytes_per_step": 0,
+                    "path": "ShellOperator(Shell(nodes, normals, weights)) from host arrays"},
+            "gpu_launches": int(steps * (3 * (npad // 128) + 1)),
+            "clocks": clk.summary()}
+    if rank == 0 and world == 1:
+        import scipy.linalg as sla
+        ns = max(200, min(args.nshell, int(args.dense_cpu_nodes)))
+        _, Ms, ms_ = operator(ns)
+        Mh = Ms[:ms_, :ms_].cpu().numpy()
+        del Ms
+        reps, t_cpu = 0, 0.0
+        while reps < 1 or (t_cpu < args.cpu_seconds and reps < 5):
+            t0 = time.perf_counter()
+            sla.lu_factor(Mh)
+            t_cpu += time.perf_counter() - t0
+            reps += 1
+        per = t_cpu / reps
+        line["cpu_baseline"] = {"value": per * (m / ms_) ** 3 * 1e3, "unit": "ms", "cores": os.cpu_count(),
+                                "kind": "reference",
+                                "sample": f"scipy.linalg.lu_factor (fiber3d's call) of the {ms_} x {ms_} operator "
+                                          f"of a {ns}-node sphere, {per:.2f} s, scaled by ({m}/{ms_})^3; "
+                                          "LU only (2/3 n^3), threads as the host LAPACK uses them"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    return line
+
+
 def block_pc_measure(args, dev, steps, warmup, cpu_seconds):
     """Batched block-diagonal preconditioner (config 4): 2000 fibers with
     point counts uniform in {16, 24, 32, 48, 64} (geometry of the step
@@ -1184,7 +1350,9 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="stresslet_sphere",
                     choices=["stresslet_sphere", "oseen_fibers", "hydro_step", "block_pc",
-                             "surface_quadrature", "fmm"])
+                             "surface_quadrature", "fmm", "dense_inverse"])
+    ap.add_argument("--dense-cpu-nodes", type=int, default=3000,
+                    help="sphere of the CPU lu_factor sample of the dense_inverse workload")
     ap.add_argument("--fmm-n", type=int, default=1000000, help="points of each kind of the FMM workload")
     ap.add_argument("--fmm-order", type=int, default=8)
     ap.add_argument("--fmm-max-pts", type=int, default=1000)
@@ -1240,6 +1408,8 @@ def main():
             quadrature_arm(args, rank, world, local)
         elif args.workload == "fmm":
             fmm_arm(args, rank, world, local)
+        elif args.workload == "dense_inverse":
+            dense_inverse_arm(args, rank, world, local)
         else:
             gpu_arm(args, rank, world, local)
     finally:

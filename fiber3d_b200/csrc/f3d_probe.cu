@@ -1,5 +1,5 @@
 // Throughput probes used as measured roofline denominators: FP64 / FP32
-// fused multiply-add rate of this GPU.  Each thread runs 8 independent FMA
+// fused multiply-add rate of this GPU, and its FP64 tensor-core (MMA) rate.  Each thread runs 8 independent FMA
 // chains, 192 FMAs per loop trip, so the pipes, not the dependency latency or
 // the loop overhead, set the rate; the caller gives it enough iterations
 // (about 2 ms) that the launch ramp does not count.
@@ -24,6 +24,38 @@ __global__ void fma_probe_kernel(T *out, int iters, T a, T b) {
   if (s == static_cast<T>(-1.2345)) out[0] = s;  // keeps the chains live
 }
 
+// FP64 tensor-core rate: each warp keeps 4 independent m16n8k16 f64 MMAs
+// in flight, 24 per loop trip (4096 flops each).
+__global__ void mma_f64_probe_kernel(double *out, int iters) {
+  double a[8], b[4], c[4][4];
+#pragma unroll
+  for (int k = 0; k < 8; ++k) a[k] = 1e-3 * (threadIdx.x + k);
+#pragma unroll
+  for (int k = 0; k < 4; ++k) b[k] = 1e-3 * (static_cast<int>(threadIdx.x) - k);
+#pragma unroll
+  for (int s = 0; s < 4; ++s)
+#pragma unroll
+    for (int k = 0; k < 4; ++k) c[s][k] = 0.0;
+  for (int i = 0; i < iters; ++i) {
+#pragma unroll
+    for (int u = 0; u < 6; ++u)
+#pragma unroll
+      for (int s = 0; s < 4; ++s)
+        asm volatile(
+            "mma.sync.aligned.m16n8k16.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5,%6,%7,%8,%9,%10,%11}, "
+            "{%12,%13,%14,%15}, {%0,%1,%2,%3};"
+            : "+d"(c[s][0]), "+d"(c[s][1]), "+d"(c[s][2]), "+d"(c[s][3])
+            : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(a[4]), "d"(a[5]), "d"(a[6]), "d"(a[7]), "d"(b[0]),
+              "d"(b[1]), "d"(b[2]), "d"(b[3]));
+  }
+  double t = 0.0;
+#pragma unroll
+  for (int s = 0; s < 4; ++s)
+#pragma unroll
+    for (int k = 0; k < 4; ++k) t += c[s][k];
+  if (t == -1.2345) out[0] = t;  // keeps the chains live
+}
+
 }  // namespace f3d
 
 extern "C" {
@@ -38,6 +70,10 @@ int f3d_probe_fma(int precision, int iters, double *sink, double *flops, void *s
   } else if (precision == F3D_FP32C) {
     f3d::fma_probe_kernel<float><<<blocks, threads, 0, st>>>(reinterpret_cast<float *>(sink), iters,
                                                              0.999999f, 1e-7f);
+  } else if (precision == 2) {
+    f3d::mma_f64_probe_kernel<<<blocks, threads, 0, st>>>(sink, iters);
+    *flops = 24.0 * 4096.0 * static_cast<double>(iters) * blocks * (threads / 32);
+    return f3d::launch_status();
   } else {
     return F3D_ERR_ARG;
   }

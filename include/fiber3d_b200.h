@@ -128,9 +128,9 @@ uint64_t f3d_wait_limit_ns(void);
    reporting path without any fault.  No counterpart in fiber3d. */
 int f3d_selftest_bounded_wait(uint64_t limit_ns, void *stream);
 
-/* Launches an FMA-throughput probe (precision F3D_FP64 or F3D_FP32C = FP32)
-   on `stream`; *flops receives the floating-point operations it performs
-   (an FMA counts 2).  Timing it gives the measured pipe peak used as the
+/* Launches an FMA-throughput probe (precision F3D_FP64 or F3D_FP32C = FP32;
+   2 = FP64 tensor-core MMA, mma.sync m16n8k16) on `stream`; *flops receives
+   the floating-point operations it performs (an FMA counts 2).  Timing it gives the measured pipe peak used as the
    roofline denominator of the pair kernels.  `sink` is an 8-byte device
    scratch word that is written only in a case that never occurs. */
 int f3d_probe_fma(int precision, int iters, double *sink, double *flops, void *stream);
