@@ -164,18 +164,6 @@ __global__ void __launch_bounds__(kGjThreads, 1) gj_panel_kernel(const GjArgs a)
   }
 }
 
-// D += A B on the FP64 tensor cores for one 16 x 8 x 16 step: a[i] holds
-// A(g + 8 (i & 1), t + 4 (i >> 1)), b[j] holds B(t + 4 j, g), d[i] holds
-// D(g + 8 (i >> 1), 2 t + (i & 1)), with g = lane / 4, t = lane % 4.
-__device__ __forceinline__ void mma_f64_16816(double (&d)[4], const double (&a)[8], const double (&b)[4]) {
-  asm volatile(
-      "mma.sync.aligned.m16n8k16.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5,%6,%7,%8,%9,%10,%11}, "
-      "{%12,%13,%14,%15}, {%0,%1,%2,%3};"
-      : "+d"(d[0]), "+d"(d[1]), "+d"(d[2]), "+d"(d[3])
-      : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(a[4]), "d"(a[5]), "d"(a[6]), "d"(a[7]), "d"(b[0]),
-        "d"(b[1]), "d"(b[2]), "d"(b[3]));
-}
-
 // The update of every tile outside the panel columns, persistent: CTA x
 // takes tiles x, x + gridDim.x, ... (row-major over (I, J), J skipping the
 // panel), its chunks one continuous stream through a three-stage ring

@@ -237,6 +237,170 @@ __global__ void __launch_bounds__(InvShape<NMAX>::kThreads, 1)
   }
 }
 
+// Blocked Gauss-Jordan for blocks of 33..128 rows (NMAX 64 or 128): one CTA
+// per block, the block in shared memory (padded with the identity), 16
+// pivots per panel.
+//  * Panel: NMAX threads, one row each with the row's 16 panel entries in
+//    registers, run the 16 sweeps restricted to the panel columns.  Partial
+//    pivoting: the pivot of step k is the first row whose |a_ik|, rounded
+//    toward zero to float with its last 8 mantissa bits cleared, is largest
+//    among the rows not yet pivoted (a pivot within 2^-16 of the column
+//    maximum).  The key (those bits, then 128 - row) makes the search one
+//    warp max-reduction and a max over the warps; each warp's winner posts
+//    its row with its key, so a step needs one barrier (posts double
+//    buffered by step parity).  Rows are never exchanged: the pivot rows are
+//    recorded instead (perm).
+//  * Update: every other column moves by W R (W the panel after its sweeps,
+//    R the old entries of the panel's 16 pivot rows), the pivot rows
+//    themselves starting from zero: one m16n8k16 step on the FP64 tensor
+//    cores per 16 x 8 tile.
+// Sweeping pivot (perm[k], k) for every k leaves X with X[perm[k], j] =
+// (PA)^-1 (k, j), so A^-1 (k, perm[j]) = X[perm[k], j].
+template <int NMAX>
+struct TcInv {
+  static constexpr int kS = NMAX + 4;  // block row stride (doubles): B-fragment reads 4t + g apart
+  static constexpr int kWS = 20;       // W panel row stride: A-fragment reads 4g + t apart
+  static constexpr int kPanels = NMAX / 16;
+  static constexpr int kThreads = 256;
+  static constexpr size_t kSmem =
+      (static_cast<size_t>(NMAX) * kS + static_cast<size_t>(NMAX) * kWS + 16 * static_cast<size_t>(kS)) *
+      sizeof(double);
+};
+
+template <int NMAX>
+__global__ void __launch_bounds__(256, 1)
+    batched_inverse_tc_kernel(double *__restrict__ A, const int64_t *__restrict__ moff,
+                              const int32_t *__restrict__ sizes, int count, float *__restrict__ A32,
+                              int32_t *__restrict__ info) {
+  using T = TcInv<NMAX>;
+  constexpr int S = T::kS;
+  extern __shared__ __align__(16) unsigned char tc_smem[];
+  double *X = reinterpret_cast<double *>(tc_smem);  // [NMAX][S]
+  double *Ws = X + NMAX * S;                         // [NMAX][kWS]
+  double *Rs = Ws + NMAX * T::kWS;                   // [16][S]
+  __shared__ unsigned s_key[2][NMAX / 32];
+  __shared__ __align__(16) double s_cand[2][NMAX / 32][16];  // each warp's best row, by step parity
+  __shared__ int s_perm[NMAX];   // pivot row of step k
+  __shared__ int s_iperm[NMAX];  // step whose pivot is row r
+  __shared__ int s_panel[NMAX];  // panel in which row r was a pivot (-1: not yet)
+  const int b = blockIdx.x;
+  if (b >= count) return;
+  const int n = sizes[b];
+  if (n <= 0 || n > NMAX) return;
+  double *M = A + moff[b];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  for (int e = tid; e < NMAX * NMAX; e += T::kThreads) {
+    const int r = e / NMAX, c = e % NMAX;
+    X[r * S + c] = (r < n && c < n) ? M[static_cast<int64_t>(r) * n + c] : (r == c ? 1.0 : 0.0);
+  }
+  for (int r = tid; r < NMAX; r += T::kThreads) s_panel[r] = -1;
+  __syncthreads();
+  int first_zero = 0;  // kept by thread 0
+  for (int p = 0; p < T::kPanels; ++p) {
+    const int c0 = 16 * p;
+    if (tid < NMAX) {
+      const int i = tid;
+      double v[16];
+#pragma unroll
+      for (int j = 0; j < 16; ++j) v[j] = X[i * S + c0 + j];
+      bool done = s_panel[i] >= 0;
+#pragma unroll
+      for (int jj = 0; jj < 16; ++jj) {
+        const int par = jj & 1;
+        // pivot key: |a_ik| as a float rounded toward zero, last 8 mantissa
+        // bits replaced by 128 - row (first row among equals; never 0 for a
+        // row not yet pivoted); pivoted rows 0
+        const unsigned key =
+            done ? 0u : ((__float_as_uint(__double2float_rz(fabs(v[jj]))) & ~255u) | static_cast<unsigned>(128 - i));
+        const unsigned wmax = __reduce_max_sync(0xffffffffu, key);
+        if (key == wmax) {  // this warp's winner posts its row (live keys are distinct; a warp
+                            // with no live row posts garbage under key 0, which never wins)
+          s_key[par][warp] = wmax;
+#pragma unroll
+          for (int j = 0; j < 16; ++j) s_cand[par][warp][j] = v[j];
+        }
+        asm volatile("bar.sync 1, %0;" ::"r"(NMAX) : "memory");
+        unsigned best = s_key[par][0];
+        int bw = 0;
+#pragma unroll
+        for (int w = 1; w < NMAX / 32; ++w)
+          if (s_key[par][w] > best) {
+            best = s_key[par][w];
+            bw = w;
+          }
+        const int pr = 128 - static_cast<int>(best & 255u);
+        const double *prow = s_cand[par][bw];
+        if (i == pr) {
+          s_perm[c0 + jj] = i;
+          s_panel[i] = p;
+          done = true;
+        }
+        const double d = prow[jj];
+        if (tid == 0 && first_zero == 0 && !(fabs(d) >= 2.2250738585072014e-308)) first_zero = c0 + jj + 1;
+        const double inv = reciprocal(d);
+        if (i == pr) {
+#pragma unroll
+          for (int j = 0; j < 16; ++j) v[j] = (j == jj) ? inv : v[j] * inv;
+        } else {
+          const double l = v[jj] * inv;
+#pragma unroll
+          for (int j = 0; j < 16; ++j) v[j] = (j == jj) ? -l : fma(-l, prow[j], v[j]);
+        }
+      }
+#pragma unroll
+      for (int j = 0; j < 16; ++j) {
+        X[i * S + c0 + j] = v[j];
+        Ws[i * T::kWS + j] = v[j];
+      }
+    }
+    __syncthreads();
+    // the panel's pivot rows as they were before the panel
+    for (int e = tid; e < 16 * NMAX; e += T::kThreads) {
+      const int jj = e / NMAX, c = e % NMAX;
+      Rs[jj * S + c] = X[s_perm[c0 + jj] * S + c];
+    }
+    __syncthreads();
+    // every column tile outside the panel: X <- [row not a pivot of this
+    // panel] X + W R, on the tensor cores
+    {
+      constexpr int kRT = NMAX / 16, kCT = NMAX / 8, kStride = 8 / kRT;
+      const int g = lane >> 2, t = lane & 3;
+      const int rt = warp % kRT;
+      const int r0 = 16 * rt + g, r1 = r0 + 8;
+      double af[8];
+#pragma unroll
+      for (int q = 0; q < 8; ++q) af[q] = Ws[(16 * rt + g + 8 * (q & 1)) * T::kWS + t + 4 * (q >> 1)];
+      const bool keep0 = s_panel[r0] != p, keep1 = s_panel[r1] != p;
+      for (int ct = warp / kRT; ct < kCT; ct += kStride) {
+        if ((ct >> 1) == p) continue;  // the panel's own two column tiles
+        const int c = 8 * ct;
+        double bf[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) bf[j] = Rs[(t + 4 * j) * S + c + g];
+        double2 *x0 = reinterpret_cast<double2 *>(X + r0 * S + c + 2 * t);
+        double2 *x1 = reinterpret_cast<double2 *>(X + r1 * S + c + 2 * t);
+        const double2 o0 = *x0, o1 = *x1;
+        double dd[4] = {keep0 ? o0.x : 0.0, keep0 ? o0.y : 0.0, keep1 ? o1.x : 0.0, keep1 ? o1.y : 0.0};
+        mma_f64_16816(dd, af, bf);
+        *x0 = make_double2(dd[0], dd[1]);
+        *x1 = make_double2(dd[2], dd[3]);
+      }
+    }
+    __syncthreads();
+  }
+  // A^-1 (k, c) = X[perm[k], iperm[c]]: coalesced stores of the block's rows
+  for (int k = tid; k < NMAX; k += T::kThreads) s_iperm[s_perm[k]] = k;
+  __syncthreads();
+  float *M32 = A32 ? A32 + moff[b] : nullptr;
+  for (int e = tid; e < n * n; e += T::kThreads) {
+    const int k = e / n, c = e % n;
+    const double v = X[s_perm[k] * S + s_iperm[c]];
+    M[e] = v;
+    if (M32) M32[e] = static_cast<float>(v);
+  }
+  if (tid == 0) info[b] = first_zero;
+}
+
 // y_b = M_b x_b for every block b (M row-major n_b x n_b at moff[b], x and y
 // at voff[b]).  One CTA per block, 8 lanes per row (16-byte loads where the
 // block is aligned), FP64 accumulation.
@@ -301,11 +465,19 @@ int f3d_batched_inverse(double *A, const int64_t *matrix_offsets, const int32_t 
     f3d::batched_inverse_kernel<32><<<count, f3d::InvShape<32>::kThreads, 0, st>>>(
         A, matrix_offsets, sizes, count, A32, info);
   } else if (max_n <= 64) {
-    f3d::batched_inverse_kernel<64><<<count, f3d::InvShape<64>::kThreads, 0, st>>>(
-        A, matrix_offsets, sizes, count, A32, info);
+    using T = f3d::TcInv<64>;
+    if (cudaFuncSetAttribute(f3d::batched_inverse_tc_kernel<64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             static_cast<int>(T::kSmem)) != cudaSuccess)
+      return F3D_ERR_CUDA;
+    f3d::batched_inverse_tc_kernel<64><<<count, T::kThreads, T::kSmem, st>>>(A, matrix_offsets, sizes, count, A32,
+                                                                             info);
   } else {
-    f3d::batched_inverse_kernel<128><<<count, f3d::InvShape<128>::kThreads, 0, st>>>(
-        A, matrix_offsets, sizes, count, A32, info);
+    using T = f3d::TcInv<128>;
+    if (cudaFuncSetAttribute(f3d::batched_inverse_tc_kernel<128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             static_cast<int>(T::kSmem)) != cudaSuccess)
+      return F3D_ERR_CUDA;
+    f3d::batched_inverse_tc_kernel<128><<<count, T::kThreads, T::kSmem, st>>>(A, matrix_offsets, sizes, count,
+                                                                              A32, info);
   }
   return f3d::launch_status();
 }

@@ -343,7 +343,8 @@ int f3d_batched_lu_solve(const double *LU, const int64_t *matrix_offsets,
    when A32 is non-null also writes an FP32 copy at the same offsets.
    info[b] is 0 or the 1-based step of the first zero (or subnormal) pivot.
    Pivoting takes a row whose |a_pk| is within a factor 1 - 2^-20 of the
-   column maximum (the first such row).  max_n <= 128
+   column maximum (the first such row; blocks of more than 32 rows: within
+   2^-16, on the FP64 tensor cores by blocked Gauss-Jordan).  max_n <= 128
    (else F3D_ERR_TOO_LARGE: use the LU).  With f3d_block_gemv this evaluates
    the fiber blocks of P_inv (tstep/tstep.py:950-994) as products with the
    explicit block inverses instead of per-block lu_solve. */
