@@ -488,6 +488,10 @@ __global__ void __launch_bounds__(128) p2m_check_kernel(const Geometry g, int le
 // Terms are split over grid.z; each split writes its own partial and a
 // second kernel adds the partials in split order (deterministic).
 constexpr int GBM = 96, GBN = 64, GBK = 32, GTHREADS = 128;
+// shared row strides (doubles), 4 mod 16: the tensor-core fragment reads of
+// a half-warp (A: k = t + 4q, row g; B: k = t + 4j, column g) hit 16
+// different bank pairs
+constexpr int GAS = GBM + 4, GXS = GBN + 4;
 constexpr int kM2LTerms = 189;
 constexpr int kFarTerms = 316;  // level 2: every box at distance >= 2, (7^3 - 3^3) offsets
 
@@ -584,8 +588,8 @@ __device__ __forceinline__ int source_slot(const GemmOp &op, int oct, int slot, 
 }
 
 __global__ void __launch_bounds__(GTHREADS) fmm_gemm_kernel(const __grid_constant__ GemmOp op) {
-  __shared__ double As[GBK][GBM + 1];
-  __shared__ double Xs[GBK][GBN + 1];
+  __shared__ __align__(16) double As[GBK][GAS];
+  __shared__ __align__(16) double Xs[GBK][GXS];
   __shared__ int s_src[GBN];
   __shared__ int s_any;
   const int tid = threadIdx.x;
@@ -598,14 +602,20 @@ __global__ void __launch_bounds__(GTHREADS) fmm_gemm_kernel(const __grid_constan
   const int col_end = op.oct_col_start[oct + 1];
   const int tps = (op.nterms + op.nsplit - 1) / op.nsplit;
   const int t_lo = blockIdx.z * tps, t_hi = min(op.nterms, t_lo + tps);
-  // thread (tr, tc) owns rows tr + 16 i (i < 6) and columns tc + 8 j (j < 8):
-  // the 8 column groups of a warp read 8 consecutive words (no bank conflict)
-  const int tr = tid >> 3, tc = tid & 7;
-  double acc[6][8];
+  // FP64 tensor cores (mma.sync m16n8k16): warp w computes rows
+  // 48 (w / 2) .. + 47 and columns 32 (w % 2) .. + 31 of the tile as 3 x 4
+  // tiles of 16 x 8; lane = 4 lg + t4 holds rows lg, lg + 8 and columns
+  // 2 t4, 2 t4 + 1 of each
+  const int lane = tid & 31, warp = tid >> 5;
+  const int lg = lane >> 2, t4 = lane & 3;
+  const int wr = 48 * (warp >> 1), wc = 32 * (warp & 1);
+  double acc[3][4][4];
 #pragma unroll
-  for (int i = 0; i < 6; ++i)
+  for (int mi = 0; mi < 3; ++mi)
 #pragma unroll
-    for (int j = 0; j < 8; ++j) acc[i][j] = 0.0;
+    for (int ni = 0; ni < 4; ++ni)
+#pragma unroll
+      for (int i = 0; i < 4; ++i) acc[mi][ni][i] = 0.0;
 
   for (int t = t_lo; t < t_hi; ++t) {
     if (tid == 0) s_any = 0;
@@ -668,42 +678,47 @@ __global__ void __launch_bounds__(GTHREADS) fmm_gemm_kernel(const __grid_constan
         Xs[kk][c] = (s >= 0 && k < op.K) ? X[static_cast<int64_t>(s) * op.ldx + k] : 0.0;
       }
       __syncthreads();
-#pragma unroll 4
-      for (int kk = 0; kk < GBK; ++kk) {
-        double a[6], x[8];
 #pragma unroll
-        for (int i = 0; i < 6; ++i) a[i] = As[kk][tr + 16 * i];
+      for (int ks = 0; ks < GBK; ks += 16) {
+        double bf[4][4];
 #pragma unroll
-        for (int j = 0; j < 8; ++j) x[j] = Xs[kk][tc + 8 * j];
+        for (int ni = 0; ni < 4; ++ni)
 #pragma unroll
-        for (int i = 0; i < 6; ++i)
+          for (int j = 0; j < 4; ++j) bf[ni][j] = Xs[ks + t4 + 4 * j][wc + 8 * ni + lg];
 #pragma unroll
-          for (int j = 0; j < 8; ++j) acc[i][j] = fma(a[i], x[j], acc[i][j]);
+        for (int mi = 0; mi < 3; ++mi) {
+          double af[8];
+#pragma unroll
+          for (int q = 0; q < 8; ++q) af[q] = As[ks + t4 + 4 * (q >> 1)][wr + 16 * mi + lg + 8 * (q & 1)];
+#pragma unroll
+          for (int ni = 0; ni < 4; ++ni) mma_f64_16816(acc[mi][ni], af, bf[ni]);
+        }
       }
       __syncthreads();
     }
   }
 #pragma unroll
-  for (int j = 0; j < 8; ++j) {
-    const int col = col0 + tc + 8 * j;
-    if (col >= col_end) continue;
-    const int slot = op.cols ? op.cols[col] : col;
-    if (op.nsplit > 1) {
-      double *p = op.partial + (static_cast<int64_t>(blockIdx.z) * op.nslots + slot) * op.ldy;
+  for (int ni = 0; ni < 4; ++ni)
 #pragma unroll
-      for (int i = 0; i < 6; ++i) {
-        const int row = row0 + tr + 16 * i;
-        if (row < op.rows) p[row] = acc[i][j];
-      }
-    } else {
-      double *y = op.Y + static_cast<int64_t>(slot) * op.ldy;
+    for (int e = 0; e < 2; ++e) {
+      const int col = col0 + wc + 8 * ni + 2 * t4 + e;
+      if (col >= col_end) continue;
+      const int slot = op.cols ? op.cols[col] : col;
+      double *y = op.nsplit > 1 ? op.partial + (static_cast<int64_t>(blockIdx.z) * op.nslots + slot) * op.ldy
+                                : op.Y + static_cast<int64_t>(slot) * op.ldy;
 #pragma unroll
-      for (int i = 0; i < 6; ++i) {
-        const int row = row0 + tr + 16 * i;
-        if (row < op.rows) y[row] = op.accumulate ? fma(op.scale, acc[i][j], y[row]) : op.scale * acc[i][j];
-      }
+      for (int mi = 0; mi < 3; ++mi)
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const int row = row0 + wr + 16 * mi + lg + 8 * h;
+          if (row >= op.rows) continue;
+          const double v = acc[mi][ni][2 * h + e];
+          if (op.nsplit > 1)
+            y[row] = v;
+          else
+            y[row] = op.accumulate ? fma(op.scale, v, y[row]) : op.scale * v;
+        }
     }
-  }
 }
 
 // Y[slot][row] (+)= scale * sum over splits of the partials, in split order

@@ -91,8 +91,10 @@ def test_fiber_blocks_of_reference_step():
         assert rel_err(y, px[o:]) < 1e-10
 
 
-@pytest.mark.parametrize("sizes", [[128] * 40, [4, 16, 33, 64, 100, 128, 7], [32, 1, 32, 17]])
+@pytest.mark.parametrize("sizes", [[128] * 40, [4, 16, 33, 64, 100, 128, 7], [32, 1, 32, 17], [128] * 512])
 def test_inverse_and_block_gemv_match_numpy(sizes):
+    """Blocks of at most 32 rows take the register-tiled kernel, 33-128 the
+    blocked tensor-core one; 512 blocks of 128 are the 512-fiber step's."""
     from fiber3d_b200.blocklu import BlockLU
     rng = np.random.default_rng(sum(sizes))
     blocks = random_blocks(rng, sizes)
@@ -115,12 +117,13 @@ def test_inverse_and_block_gemv_match_numpy(sizes):
         off += n
 
 
-def test_inverse_zero_pivot_reported():
+@pytest.mark.parametrize("n", [8, 64, 128])
+def test_inverse_zero_pivot_reported(n):
     from fiber3d_b200.blocklu import BlockLU
-    A = np.eye(8)
+    A = np.eye(n)
     A[3, :] = 0.0
-    lu = BlockLU([8, 8])
-    lu.load([np.eye(8), A])
+    lu = BlockLU([n, n])
+    lu.load([np.eye(n), A])
     lu.invert()
     with pytest.raises(ZeroDivisionError):
         lu.check()
