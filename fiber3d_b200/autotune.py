@@ -56,6 +56,7 @@ def _key(kernel, precision, self_mode, ns, nt, same=False) -> str:
 # the symmetric self-sum's launch shape (f3d_pair_shape.sl = -1)
 SYMMETRIC = (1, -1, 0, -1)
 SYM_MAX_POINTS = 1024 * 128
+TILE = (1, -2, 0, -1)
 
 
 def symmetric_eligible(kernel, precision, self_mode, ns, nt, same) -> bool:
@@ -64,6 +65,14 @@ def symmetric_eligible(kernel, precision, self_mode, ns, nt, same) -> bool:
     (further targets after them are summed one-sided in the same launch)."""
     return (same and nt >= ns and 0 < ns <= SYM_MAX_POINTS and precision == "fp64"
             and kernel in ("oseen", "stresslet") and self_mode in ("skip_index", "skip_group"))
+
+
+def tile_eligible(kernel, precision, self_mode, ns, nt) -> bool:
+    """Whether the tile form (the symmetric kernel's target-side items for a
+    plain source -> target sum) can run this sum: FP64 Oseen or stresslet,
+    close pairs regularised, at most 1024 source tiles."""
+    return (0 < ns <= SYM_MAX_POINTS and nt > 0 and precision == "fp64"
+            and kernel in ("oseen", "stresslet") and self_mode == "regularise")
 
 
 def _same_array(a, b) -> bool:
@@ -150,6 +159,8 @@ def tune(kernel: str, r_source, r_target, density, normal=None, *, self_mode="re
     cands = candidates(nt, sms, occ)
     if symmetric_eligible(kernel, precision, self_mode, ns, nt, same):
         cands.append(SYMMETRIC)
+    if tile_eligible(kernel, precision, self_mode, ns, nt):
+        cands.append(TILE)
     for cand in cands:
         shp = _lib.PairShape(*cand)
         try:

@@ -663,10 +663,18 @@ int pair_sym_launch(int kernel, int self_mode, const double *x, const double *de
                     const int32_t *grp, double *out, int64_t n, int64_t nt, double eta, double reg, double eps,
                     int accumulate, double *partial, unsigned *counters, int *occupancy, cudaStream_t st,
                     const double *dens2, double *out2, bool dual);
+// Its tile form for plain source -> target sums.
+size_t tile_partial_bytes(int64_t ns, int64_t nt);
+bool tile_fits(int64_t ns, int64_t nt);
+int pair_tile_launch(int kernel, const double *xs, const double *dens, const double *nrm, const double *xt,
+                     double *out, int64_t ns, int64_t nt, double eta, double reg, double eps, int accumulate,
+                     double *partial, unsigned *counters, int *occupancy, cudaStream_t st, const double *dens2,
+                     double *out2, bool dual);
 
 struct Plan {
   int tpt, sl, nsplit, use_tma;
-  bool sym;  // shape.sl == -1: the symmetric self-sum
+  bool sym;   // shape.sl == -1: the symmetric self-sum
+  bool tile;  // shape.sl == -2: the tile form of a source -> target sum
   int64_t ntb, tiles_per_split;
   size_t off_counters, off_partial, off_packed, bytes;
 };
@@ -676,6 +684,27 @@ static int make_plan(int kernel, int precision, int64_t ns, int64_t nt, const f3
   if (kernel < 0 || kernel > 3 || precision < 0 || precision > 1) return F3D_ERR_ARG;
   if (ns < 0 || nt < 0) return F3D_ERR_SHAPE;
   p->sym = false;
+  p->tile = false;
+  if (shape && shape->sl == -2) {
+    // tile form: FP64 Oseen or stresslet, sources and targets in their own
+    // arrays, two targets per thread on 128-point tiles (the symmetric
+    // kernel's target-side items)
+    if (precision != F3D_FP64 || !(kernel == F3D_KERNEL_OSEEN || kernel == F3D_KERNEL_STRESSLET))
+      return F3D_ERR_ARG;
+    if (!tile_fits(ns, nt)) return F3D_ERR_TOO_LARGE;
+    p->tile = true;
+    p->tpt = 2;
+    p->sl = -2;
+    p->nsplit = 1;
+    p->use_tma = 0;
+    p->ntb = (nt + kBlock - 1) / kBlock;
+    p->tiles_per_split = 0;
+    p->off_counters = 0;
+    p->off_partial = kCounterBytes;
+    p->off_packed = kCounterBytes;
+    p->bytes = (ns > 0 && nt > 0) ? kCounterBytes + round_up((dual ? 2 : 1) * tile_partial_bytes(ns, nt), 256) : 0;
+    return F3D_OK;
+  }
   if (shape && shape->sl == -1) {
     // symmetric self-sum: FP64 Oseen or stresslet over one point set (the
     // first ns of the nt targets), further targets one-sided; the
@@ -813,6 +842,7 @@ static int pair_sum_core(int kernel, int precision, int self_mode, const double 
   if (self_mode < 0 || self_mode > 3) return F3D_ERR_ARG;
   if (dual && self_mode == F3D_SELF_SKIP_CLOSE) return F3D_ERR_ARG;
   if (p.sym && !(self_mode == F3D_SELF_SKIP_INDEX || self_mode == F3D_SELF_SKIP_GROUP)) return F3D_ERR_ARG;
+  if (p.tile && self_mode != F3D_SELF_REGULARISE) return F3D_ERR_ARG;
   if (nt == 0) return F3D_OK;
   if (!rt || !out) return F3D_ERR_NULL;
   if (ns > 0 && (!rs || !dens)) return F3D_ERR_NULL;
@@ -844,6 +874,10 @@ static int pair_sum_core(int kernel, int precision, int self_mode, const double 
                            reinterpret_cast<double *>(w + p.off_partial), reinterpret_cast<unsigned *>(w),
                            nullptr, st, dens2, out2, dual);
   }
+  if (p.tile)
+    return pair_tile_launch(kernel, rs, dens, nrm, rt, out, ns, nt, eta, reg, eps, accumulate,
+                            reinterpret_cast<double *>(w + p.off_partial), reinterpret_cast<unsigned *>(w), nullptr,
+                            st, dens2, out2, dual);
 
   PairArgs a{};
   a.rs = rs; a.rt = rt; a.dens = dens; a.nrm = nrm;
@@ -998,6 +1032,11 @@ int f3d_pair_occupancy(int kernel, int precision, int self_mode, int dual, const
       return F3D_ERR_ARG;
     return f3d::pair_sym_launch(kernel, self_mode, nullptr, nullptr, nullptr, nullptr, nullptr, 1, 1, 1.0, 0.0, 0.0,
                                 0, nullptr, nullptr, ctas_per_sm, nullptr, nullptr, nullptr, dual != 0);
+  }
+  if (shape && shape->sl == -2) {
+    if (self_mode != F3D_SELF_REGULARISE) return F3D_ERR_ARG;
+    return f3d::pair_tile_launch(kernel, nullptr, nullptr, nullptr, nullptr, nullptr, 1, 1, 1.0, 0.0, 0.0, 0,
+                                 nullptr, nullptr, ctas_per_sm, nullptr, nullptr, nullptr, dual != 0);
   }
   // the shape's own tpt/sl (make_plan picks defaults for a 1-target sum)
   if (shape && shape->tpt) p.tpt = shape->tpt;

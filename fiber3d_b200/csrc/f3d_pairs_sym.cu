@@ -46,6 +46,12 @@
 // The Oseen sum also has a two-density form (DUAL): two densities over the
 // same pairs, the geometry once, each sum with the single form's exact
 // arithmetic and order, so that each equals its single sum bit for bit.
+//
+// The same items serve a plain source -> target sum (the tile form: xt set,
+// the targets in an array of their own): there are no symmetric items, every
+// item is a tile of targets against a tile of sources, summed from the target
+// side with two targets per thread, close pairs regularised; partials and
+// counters are then kept for the target tiles only (tile0 = T).
 #include <climits>
 #include <type_traits>
 
@@ -69,8 +75,10 @@ struct SymArgs {
   double *out, *out2;            // nt x 3 (out2: DUAL only)
   double *partial, *partial2;    // [T + T2][T][kSymTile][3] (partial2: DUAL only)
   unsigned *counters;            // [T + T2], zero on entry and on exit
+  const double *xt;              // tile form: nt x 3 targets (x then holds the n sources only)
   int64_t n, nt;
   int ntiles, nextra;            // T source tiles, T2 tiles of further targets
+  int tile0;                     // first tile with partials and a counter (tile form: T)
   int accumulate;
   double eps2, reg2, scale;
 };
@@ -80,6 +88,18 @@ static int64_t sym_tiles(int64_t n) { return (n + kSymTile - 1) / kSymTile; }
 size_t sym_partial_bytes(int64_t n, int64_t nt) {
   const int64_t T = sym_tiles(n), T2 = sym_tiles(nt - n);
   return static_cast<size_t>(T + T2) * static_cast<size_t>(T) * kSymTile * 3 * sizeof(double);
+}
+
+// Tile form: [T2][T][kSymTile][3] partials, T2 = target tiles.
+size_t tile_partial_bytes(int64_t ns, int64_t nt) {
+  return static_cast<size_t>(sym_tiles(nt)) * static_cast<size_t>(sym_tiles(ns)) * kSymTile * 3 * sizeof(double);
+}
+
+bool tile_fits(int64_t ns, int64_t nt) {
+  if (ns < 0 || nt < 0) return false;
+  if (ns == 0 || nt == 0) return true;
+  return sym_tiles(ns) <= kSymMaxTiles && sym_tiles(nt) <= kMaxCounters &&
+         tile_partial_bytes(ns, nt) <= kSymMaxPartialBytes;
 }
 
 bool sym_fits(int64_t n, int64_t nt) {
@@ -106,7 +126,7 @@ __global__ void __launch_bounds__(kSymThreads) pair_sym_kernel(const SymArgs a) 
   __shared__ int s_range[kSymWarps][4];
 
   const int T = a.ntiles;
-  const int64_t nsym = static_cast<int64_t>(T) * (T + 1) / 2;
+  const int64_t nsym = a.xt ? 0 : static_cast<int64_t>(T) * (T + 1) / 2;
   const int64_t item = blockIdx.x;
   int I, J;
   if (item < nsym) {
@@ -129,8 +149,10 @@ __global__ void __launch_bounds__(kSymThreads) pair_sym_kernel(const SymArgs a) 
 
   // this thread's targets (k = 0: tile slot tid, k = 1: tid + 64), with their
   // own density and normal for the terms they send to the sources
-  const int64_t tbase = extra ? a.n + static_cast<int64_t>(I - T) * kSymTile : static_cast<int64_t>(I) * kSymTile;
+  const int64_t tbase =
+      extra ? (a.xt ? 0 : a.n) + static_cast<int64_t>(I - T) * kSymTile : static_cast<int64_t>(I) * kSymTile;
   const int64_t tend = extra ? a.nt : a.n;
+  const double *const xtrg = (extra && a.xt) ? a.xt : a.x;
   double tx[2][3], td[ND][2][3], tn[2][3];
   int32_t tg[2];
   bool tv[2];
@@ -141,7 +163,7 @@ __global__ void __launch_bounds__(kSymThreads) pair_sym_kernel(const SymArgs a) 
     tg[k] = INT32_MIN;
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-      tx[k][c] = tv[k] ? a.x[3 * i + c] : 1e30;
+      tx[k][c] = tv[k] ? xtrg[3 * i + c] : 1e30;
       td[0][k][c] = (tv[k] && !extra) ? a.dens[3 * i + c] : 0.0;
       if (DUAL) td[ND - 1][k][c] = (tv[k] && !extra) ? a.dens2[3 * i + c] : 0.0;
       tn[k][c] = (kNrm && tv[k] && !extra) ? a.nrm[3 * i + c] : 0.0;
@@ -404,7 +426,7 @@ __global__ void __launch_bounds__(kSymThreads) pair_sym_kernel(const SymArgs a) 
       }
     }
     // tile I's partial from this item (slot J)
-    double *pi = part + (static_cast<int64_t>(I) * T + J) * slot_stride;
+    double *pi = part + (static_cast<int64_t>(I - a.tile0) * T + J) * slot_stride;
 #pragma unroll
     for (int k = 0; k < 2; ++k)
 #pragma unroll
@@ -414,7 +436,7 @@ __global__ void __launch_bounds__(kSymThreads) pair_sym_kernel(const SymArgs a) 
   __syncthreads();
   if (tid == 0) {
     int f = 0;
-    if (atomicAdd(&a.counters[I], 1u) == static_cast<unsigned>(T - 1)) f |= 1;
+    if (atomicAdd(&a.counters[I - a.tile0], 1u) == static_cast<unsigned>(T - 1)) f |= 1;
     if (!diag && !extra && atomicAdd(&a.counters[J], 1u) == static_cast<unsigned>(T - 1)) f |= 2;
     s_flags = f;
   }
@@ -424,7 +446,8 @@ __global__ void __launch_bounds__(kSymThreads) pair_sym_kernel(const SymArgs a) 
     if (!(flags & (1 << which))) continue;
     __threadfence();
     const int X = which == 0 ? I : J;
-    const int64_t xbase = X < T ? static_cast<int64_t>(X) * kSymTile : a.n + static_cast<int64_t>(X - T) * kSymTile;
+    const int64_t xbase =
+        X < T ? static_cast<int64_t>(X) * kSymTile : (a.xt ? 0 : a.n) + static_cast<int64_t>(X - T) * kSymTile;
     const int64_t xend = X < T ? a.n : a.nt;
     // A slot is the tile's 128 x 3 sums in output order; thread tid sums the
     // pairs of doubles tid, tid + 64 and tid + 128 of every slot (16-byte
@@ -433,7 +456,8 @@ __global__ void __launch_bounds__(kSymThreads) pair_sym_kernel(const SymArgs a) 
 #pragma unroll
     for (int q = 0; q < ND; ++q) {
       const double2 *p =
-          reinterpret_cast<const double2 *>((q == 0 ? a.partial : a.partial2) + static_cast<int64_t>(X) * T * slot_stride);
+          reinterpret_cast<const double2 *>((q == 0 ? a.partial : a.partial2) +
+                                            static_cast<int64_t>(X - a.tile0) * T * slot_stride);
       double2 v[3];
 #pragma unroll
       for (int m = 0; m < 3; ++m) v[m] = make_double2(0.0, 0.0);
@@ -480,7 +504,7 @@ __global__ void __launch_bounds__(kSymThreads) pair_sym_kernel(const SymArgs a) 
         }
       }
     }
-    if (tid == 0) a.counters[X] = 0u;
+    if (tid == 0) a.counters[X - a.tile0] = 0u;
   }
 }
 
@@ -491,8 +515,8 @@ static int sym_launch_one(const SymArgs &a, int *occupancy, cudaStream_t st) {
     return cudaOccupancyMaxActiveBlocksPerMultiprocessor(occupancy, kfn, kSymThreads, 0) == cudaSuccess
                ? F3D_OK
                : F3D_ERR_CUDA;
-  const int64_t items =
-      static_cast<int64_t>(a.ntiles) * (a.ntiles + 1) / 2 + static_cast<int64_t>(a.nextra) * a.ntiles;
+  const int64_t items = (a.xt ? 0 : static_cast<int64_t>(a.ntiles) * (a.ntiles + 1) / 2) +
+                        static_cast<int64_t>(a.nextra) * a.ntiles;
   kfn<<<static_cast<unsigned>(items), kSymThreads, 0, st>>>(a);
   return launch_status();
 }
@@ -539,6 +563,42 @@ int pair_sym_launch(int kernel, int self_mode, const double *x, const double *de
   return self_mode == F3D_SELF_SKIP_INDEX
              ? sym_launch_one<F3D_KERNEL_STRESSLET, F3D_SELF_SKIP_INDEX, false>(a, occupancy, st)
              : sym_launch_one<F3D_KERNEL_STRESSLET, F3D_SELF_SKIP_GROUP, false>(a, occupancy, st);
+}
+
+// The tile form of a plain source -> target sum (kernel OSEEN or STRESSLET,
+// FP64, close pairs regularised as F3D_SELF_REGULARISE does): ns sources in
+// xs, nt targets in xt; with dens2/out2 (Oseen only) the two-density form.
+// partial: tile_partial_bytes(ns, nt) of workspace, twice that for two
+// densities.  With occupancy non-null, only reports resident CTAs per SM.
+int pair_tile_launch(int kernel, const double *xs, const double *dens, const double *nrm, const double *xt,
+                     double *out, int64_t ns, int64_t nt, double eta, double reg, double eps, int accumulate,
+                     double *partial, unsigned *counters, int *occupancy, cudaStream_t st, const double *dens2,
+                     double *out2, bool dual) {
+  SymArgs a{};
+  a.x = xs;
+  a.xt = xt;
+  a.dens = dens;
+  a.dens2 = dens2;
+  a.nrm = nrm;
+  a.out = out;
+  a.out2 = out2;
+  a.partial = partial;
+  a.partial2 = partial ? partial + tile_partial_bytes(ns, nt) / sizeof(double) : nullptr;
+  a.counters = counters;
+  a.n = ns;
+  a.nt = nt;
+  a.ntiles = static_cast<int>(sym_tiles(ns));
+  a.nextra = static_cast<int>(sym_tiles(nt));
+  a.tile0 = a.ntiles;
+  a.accumulate = accumulate ? 1 : 0;
+  a.eps2 = eps * eps;
+  a.reg2 = reg * reg;
+  a.scale = (kernel == F3D_KERNEL_STRESSLET) ? -3.0 / (4.0 * kPi * eta) : 1.0 / (8.0 * kPi * eta);
+  // the target-side items skip nothing and regularise close pairs in every mode
+  if (kernel == F3D_KERNEL_OSEEN)
+    return dual ? sym_launch_one<F3D_KERNEL_OSEEN, F3D_SELF_SKIP_INDEX, true>(a, occupancy, st)
+                : sym_launch_one<F3D_KERNEL_OSEEN, F3D_SELF_SKIP_INDEX, false>(a, occupancy, st);
+  return sym_launch_one<F3D_KERNEL_STRESSLET, F3D_SELF_SKIP_INDEX, false>(a, occupancy, st);
 }
 
 }  // namespace f3d

@@ -93,7 +93,15 @@ typedef struct f3d_pair_shape {
                       ceil((nt - ns) / 128) (twice that for the
                       two-density Oseen pass), at most 2 GiB, and
                       T <= 1024 (131072 sources).  tpt, nsplit and
-                      use_tma are then ignored.                             */
+                      use_tma are then ignored.
+                      Or -2: the tile form of a source -> target sum (the
+                      symmetric kernel's target-side items: 128-point
+                      tiles, two targets per thread, per-tile partials
+                      summed in a fixed order): FP64 Oseen or stresslet,
+                      F3D_SELF_REGULARISE; workspace 3072 T T2 bytes,
+                      T = ceil(ns / 128) <= 1024, T2 = ceil(nt / 128),
+                      at most 2 GiB (twice for the two-density Oseen
+                      pass).                                                 */
   int32_t nsplit;  /* source splits (grid.y); 0 = derive from the SM count    */
   int32_t use_tma; /* 0 or 1: stage full source tiles with cp.async.bulk
                       (default); -1: stage them with plain loads            */

@@ -187,6 +187,26 @@ def test_symmetric_shape_plan_checks(dll):
     assert nb.value >= 500 * (500 + 169) * 3072
 
 
+def test_tile_shape_plan_checks(dll):
+    """The tile form (sl = -2) of a source -> target sum: T x T2 partial
+    tiles of 3 KB, FP64 Oseen / stresslet only, close pairs regularised
+    only (checked before any memory is touched)."""
+    shp = _lib.PairShape(1, -2, 0, -1)
+    nb = ctypes.c_size_t(0)
+    # 12000 sphere nodes onto the 4096 ball points: 94 x 32 tiles
+    assert dll.f3d_pair_workspace_bytes(1, 0, 12000, 4096, ctypes.byref(shp), ctypes.byref(nb)) == 0
+    assert nb.value >= 94 * 32 * 128 * 3 * 8
+    assert dll.f3d_pair_workspace_bytes(0, 0, 100, 100000, ctypes.byref(shp), ctypes.byref(nb)) == 0
+    assert dll.f3d_pair_workspace_bytes(1, 1, 1000, 1000, ctypes.byref(shp), ctypes.byref(nb)) == 5   # FP32C
+    assert dll.f3d_pair_workspace_bytes(2, 0, 1000, 1000, ctypes.byref(shp), ctypes.byref(nb)) == 5   # rotlet
+    assert dll.f3d_pair_workspace_bytes(0, 0, 1024 * 128 + 1, 10, ctypes.byref(shp), ctypes.byref(nb)) == 10
+    assert dll.f3d_pair_workspace_bytes(0, 0, 1024 * 128, 1024 * 128, ctypes.byref(shp),
+                                        ctypes.byref(nb)) == 10                                      # > 2 GiB
+    for mode in (1, 2, 3):
+        assert dll.f3d_pair_sum(0, 0, mode, None, None, None, None, None, None, None, 10, 10, 1.0, 5e-3, 1e-5, 0,
+                                ctypes.byref(shp), None, 0, None) == 5
+
+
 def test_block3_gemv_argument_checks(dll):
     """The block-Jacobi periphery preconditioner's entry checks its sizes,
     pointers and aliasing before any launch."""

@@ -611,3 +611,82 @@ def test_symmetric_rejects_other_sums(K, L):
     with pytest.raises(L.F3DError) as e:
         K.pair_sum("oseen", big, big, big, self_mode="skip_index", shape=L.PairShape(*SYM))
     assert e.value.status == 10
+
+
+TILE = (1, -2, 0, -1)
+
+
+@pytest.mark.parametrize("kind", ["oseen", "stresslet"])
+@pytest.mark.parametrize("ns,nt", [(1, 1), (127, 129), (128, 3), (1000, 257), (3000, 4097)])
+def test_tile_form_source_target(K, L, kind, ns, nt):
+    """The tile form of a source -> target sum (sl = -2) against the C oracle,
+    with a target on a source (coincident: regularised) and a sub-epsilon
+    pair (the careful redo); deterministic; accumulate adds to the output."""
+    rng = np.random.default_rng(ns * 7 + nt)
+    xs, xt = rng.random((ns, 3)) * 3, rng.random((nt, 3)) * 3
+    if ns > 40 and nt > 40:
+        xt[5] = xs[7]
+        xt[20] = xs[30] + 3e-6
+    d, nr = rng.normal(size=(ns, 3)), rng.normal(size=(ns, 3))
+    n_arg = nr if kind == "stresslet" else None
+    ref = pairs_c.pair_sum(kind, xs, xt, d, n_arg)
+    s, t = torch.as_tensor(xs, device="cuda"), torch.as_tensor(xt, device="cuda")
+    shp = L.PairShape(*TILE)
+    u = K.pair_sum(kind, s, t, d, n_arg, shape=shp)
+    assert rel_err(u.cpu().numpy(), ref) < TOL64
+    u2 = K.pair_sum(kind, s, t, d, n_arg, shape=shp)
+    assert torch.equal(u, u2)
+    K.pair_sum(kind, s, t, d, n_arg, shape=shp, out=u2, accumulate=True)
+    assert rel_err(u2.cpu().numpy(), 2 * ref) < TOL64
+
+
+def test_tile_form_config2_ball_targets(K, L):
+    """fiber3d's second config-2 call (the 12000-node double layer onto the
+    4096 ball points) in the tile form: equal to the regular kernel to
+    rounding, sampled rows against the C oracle; the host entry point takes
+    the same shape."""
+    from fiber3d_b200 import geometry
+    nodes, normals, w, mu, vol = geometry.stresslet_sphere_workload(seed=2)
+    q = mu * w[:, None]
+    s, t = torch.as_tensor(nodes, device="cuda"), torch.as_tensor(vol, device="cuda")
+    a = K.pair_sum("stresslet", s, t, q, normals, shape=L.PairShape(*TILE))
+    b = K.pair_sum("stresslet", s, t, q, normals, shape=L.PairShape(1, 1, 0, 0))
+    assert rel_err(a.cpu().numpy(), b.cpu().numpy()) < TOL64
+    ref = pairs_c.pair_sum("stresslet", nodes, vol[:300], q, normals)
+    assert rel_err(a.cpu().numpy()[:900], ref) < TOL64
+    h = K.stresslet_kernel_source_target_numba(nodes, vol, normals, q, shape=L.PairShape(*TILE))
+    assert np.array_equal(np.asarray(h).reshape(-1), a.cpu().numpy())
+
+
+@pytest.mark.parametrize("ns,nt", [(300, 700), (5000, 129)])
+def test_tile_form_oseen_dual_equals_two_sums(L, ns, nt):
+    """The two-density Oseen pass in the tile form gives, bit for bit, the two
+    tile-form sums it fuses."""
+    import ctypes
+    from fiber3d_b200 import kernels as K
+    rng = np.random.default_rng(ns + nt)
+    s = torch.tensor(rng.random((ns, 3)) * 4.0, device="cuda")
+    t = torch.tensor(rng.random((nt, 3)) * 4.0, device="cuda")
+    d1, d2 = (torch.tensor(rng.normal(size=(ns, 3)), device="cuda") for _ in range(2))
+    shp = L.PairShape(*TILE)
+    r1 = K.pair_sum("oseen", s, t, d1, shape=shp).clone()
+    r2 = K.pair_sum("oseen", s, t, d2, shape=shp).clone()
+    nb = ctypes.c_size_t(0)
+    L.call("f3d_oseen_dual_workspace_bytes", ns, nt, ctypes.byref(shp), ctypes.byref(nb))
+    ws = torch.zeros(max(nb.value, 256), dtype=torch.uint8, device="cuda")
+    o1, o2 = torch.empty_like(r1), torch.empty_like(r2)
+    for _ in range(2):  # the tile counters return to zero between calls
+        L.call("f3d_oseen_dual", L.SELF_MODE["regularise"], L.ptr(s), L.ptr(t), L.ptr(d1), L.ptr(d2), None, None,
+               L.ptr(o1), L.ptr(o2), ns, nt, 1.0, 5e-3, 1e-5, 0, ctypes.byref(shp), L.ptr(ws), ws.numel(),
+               L.stream_handle())
+        assert torch.equal(o1, r1) and torch.equal(o2, r2)
+
+
+def test_tile_form_rejects_other_rules(K, L):
+    s = torch.rand(200, 3, dtype=torch.float64, device="cuda")
+    d = torch.rand(200, 3, dtype=torch.float64, device="cuda")
+    for mode in ("skip_index", "skip_close"):
+        with pytest.raises(L.F3DError):
+            K.pair_sum("oseen", s, s, d, self_mode=mode, shape=L.PairShape(*TILE))
+    with pytest.raises(L.F3DError):
+        K.pair_sum("rotlet", s, s, d, shape=L.PairShape(*TILE))
