@@ -672,8 +672,13 @@ __global__ void __launch_bounds__(GTHREADS) fmm_gemm_kernel(const __grid_constan
             for (int j = 0; j < 4; ++j) As[4 * ei + j][3 * ci + i] = v[i][j];
         }
       }
+      // a warp gathers 4 boxes x 8 consecutive k (64-byte runs of each box's
+      // densities); its stores then fill the 16 bank pairs twice over
+      // (4 kk + c over the stride 4 mod 16), the minimum for 256 bytes
       for (int e = tid; e < GBN * GBK; e += GTHREADS) {
-        const int c = e / GBK, kk = e % GBK;
+        const int blk = e >> 5;
+        const int c = 4 * (blk % (GBN / 4)) + (e & 3);
+        const int kk = 8 * (blk / (GBN / 4)) + ((e >> 2) & 7);
         const int s = s_src[c], k = k0 + kk;
         Xs[kk][c] = (s >= 0 && k < op.K) ? X[static_cast<int64_t>(s) * op.ldx + k] : 0.0;
       }
