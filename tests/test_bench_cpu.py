@@ -25,8 +25,9 @@ def test_quadrature_reference_arm_prints_one_line():
 
 
 def test_default_reference_arm_prints_one_line():
-    """The arm the driver runs beside the GPU one: the C restatement of
-    fiber3d's pair loop on the default workload's metric and config."""
+    """bench.py's reference arm (`--impl reference`), timed beside the GPU
+    one: the C restatement of fiber3d's pair loop on the default workload's
+    metric and config."""
     cmd = [sys.executable, str(ROOT / "bench.py"), "--impl", "reference", "--steps", "1", "--warmup", "3",
            "--cpu-seconds", "0.5"]
     res = subprocess.run(cmd, capture_output=True, text=True, timeout=600, cwd=ROOT)
