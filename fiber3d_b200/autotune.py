@@ -160,7 +160,7 @@ def tune(kernel: str, r_source, r_target, density, normal=None, *, self_mode="re
     if symmetric_eligible(kernel, precision, self_mode, ns, nt, same):
         cands.append(SYMMETRIC)
     if tile_eligible(kernel, precision, self_mode, ns, nt):
-        cands.append(TILE)
+        cands += [(1, -2, 1, -1), (1, -2, 2, -1)]  # whole or half source tiles
     for cand in cands:
         shp = _lib.PairShape(*cand)
         try:

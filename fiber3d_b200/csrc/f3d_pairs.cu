@@ -664,12 +664,12 @@ int pair_sym_launch(int kernel, int self_mode, const double *x, const double *de
                     int accumulate, double *partial, unsigned *counters, int *occupancy, cudaStream_t st,
                     const double *dens2, double *out2, bool dual);
 // Its tile form for plain source -> target sums.
-size_t tile_partial_bytes(int64_t ns, int64_t nt);
-bool tile_fits(int64_t ns, int64_t nt);
+size_t tile_partial_bytes(int64_t ns, int64_t nt, int sub);
+bool tile_fits(int64_t ns, int64_t nt, int sub);
 int pair_tile_launch(int kernel, const double *xs, const double *dens, const double *nrm, const double *xt,
                      double *out, int64_t ns, int64_t nt, double eta, double reg, double eps, int accumulate,
                      double *partial, unsigned *counters, int *occupancy, cudaStream_t st, const double *dens2,
-                     double *out2, bool dual);
+                     double *out2, bool dual, int sub);
 
 struct Plan {
   int tpt, sl, nsplit, use_tma;
@@ -691,18 +691,24 @@ static int make_plan(int kernel, int precision, int64_t ns, int64_t nt, const f3
     // kernel's target-side items)
     if (precision != F3D_FP64 || !(kernel == F3D_KERNEL_OSEEN || kernel == F3D_KERNEL_STRESSLET))
       return F3D_ERR_ARG;
-    if (!tile_fits(ns, nt)) return F3D_ERR_TOO_LARGE;
+    // source sub-tiles: 1 (128 points, the default) or 2 (64 points: twice
+    // the items, for sums too small to fill the GPU; on the 12000-node sphere
+    // onto 4096 points, 2.5 waves of whole items, the halves measured slower)
+    int sub = shape->nsplit == 0 ? 1 : shape->nsplit;
+    if (sub != 1 && sub != 2) return F3D_ERR_ARG;
+    if (!tile_fits(ns, nt, sub)) return F3D_ERR_TOO_LARGE;
     p->tile = true;
     p->tpt = 2;
     p->sl = -2;
-    p->nsplit = 1;
+    p->nsplit = sub;
     p->use_tma = 0;
     p->ntb = (nt + kBlock - 1) / kBlock;
     p->tiles_per_split = 0;
     p->off_counters = 0;
     p->off_partial = kCounterBytes;
     p->off_packed = kCounterBytes;
-    p->bytes = (ns > 0 && nt > 0) ? kCounterBytes + round_up((dual ? 2 : 1) * tile_partial_bytes(ns, nt), 256) : 0;
+    p->bytes =
+        (ns > 0 && nt > 0) ? kCounterBytes + round_up((dual ? 2 : 1) * tile_partial_bytes(ns, nt, sub), 256) : 0;
     return F3D_OK;
   }
   if (shape && shape->sl == -1) {
@@ -877,7 +883,7 @@ static int pair_sum_core(int kernel, int precision, int self_mode, const double 
   if (p.tile)
     return pair_tile_launch(kernel, rs, dens, nrm, rt, out, ns, nt, eta, reg, eps, accumulate,
                             reinterpret_cast<double *>(w + p.off_partial), reinterpret_cast<unsigned *>(w), nullptr,
-                            st, dens2, out2, dual);
+                            st, dens2, out2, dual, p.nsplit);
 
   PairArgs a{};
   a.rs = rs; a.rt = rt; a.dens = dens; a.nrm = nrm;
@@ -1036,7 +1042,7 @@ int f3d_pair_occupancy(int kernel, int precision, int self_mode, int dual, const
   if (shape && shape->sl == -2) {
     if (self_mode != F3D_SELF_REGULARISE) return F3D_ERR_ARG;
     return f3d::pair_tile_launch(kernel, nullptr, nullptr, nullptr, nullptr, nullptr, 1, 1, 1.0, 0.0, 0.0, 0,
-                                 nullptr, nullptr, ctas_per_sm, nullptr, nullptr, nullptr, dual != 0);
+                                 nullptr, nullptr, ctas_per_sm, nullptr, nullptr, nullptr, dual != 0, 1);
   }
   // the shape's own tpt/sl (make_plan picks defaults for a 1-target sum)
   if (shape && shape->tpt) p.tpt = shape->tpt;

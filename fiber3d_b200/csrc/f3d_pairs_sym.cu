@@ -79,6 +79,7 @@ struct SymArgs {
   int64_t n, nt;
   int ntiles, nextra;            // T source tiles, T2 tiles of further targets
   int tile0;                     // first tile with partials and a counter (tile form: T)
+  int sub;                       // tile form: source sub-tiles per 128-point tile (1 or 2; else 1)
   int accumulate;
   double eps2, reg2, scale;
 };
@@ -90,16 +91,23 @@ size_t sym_partial_bytes(int64_t n, int64_t nt) {
   return static_cast<size_t>(T + T2) * static_cast<size_t>(T) * kSymTile * 3 * sizeof(double);
 }
 
-// Tile form: [T2][T][kSymTile][3] partials, T2 = target tiles.
-size_t tile_partial_bytes(int64_t ns, int64_t nt) {
-  return static_cast<size_t>(sym_tiles(nt)) * static_cast<size_t>(sym_tiles(ns)) * kSymTile * 3 * sizeof(double);
+// Tile form: [T2][T sub][kSymTile][3] partials, T2 = target tiles, each
+// 128-point source tile taken as `sub` sub-tiles (one partial each).
+static int64_t tile_slots(int64_t ns, int sub) {
+  const int64_t w = sub == 2 ? kSymTile / 2 : kSymTile;
+  return (ns + w - 1) / w;
 }
 
-bool tile_fits(int64_t ns, int64_t nt) {
+size_t tile_partial_bytes(int64_t ns, int64_t nt, int sub) {
+  return static_cast<size_t>(sym_tiles(nt)) * static_cast<size_t>(tile_slots(ns, sub)) * kSymTile * 3 *
+         sizeof(double);
+}
+
+bool tile_fits(int64_t ns, int64_t nt, int sub) {
   if (ns < 0 || nt < 0) return false;
   if (ns == 0 || nt == 0) return true;
   return sym_tiles(ns) <= kSymMaxTiles && sym_tiles(nt) <= kMaxCounters &&
-         tile_partial_bytes(ns, nt) <= kSymMaxPartialBytes;
+         tile_partial_bytes(ns, nt, sub) <= kSymMaxPartialBytes;
 }
 
 bool sym_fits(int64_t n, int64_t nt) {
@@ -108,6 +116,8 @@ bool sym_fits(int64_t n, int64_t nt) {
   const int64_t T = sym_tiles(n), T2 = sym_tiles(nt - n);
   return T <= kSymMaxTiles && T + T2 <= kMaxCounters && sym_partial_bytes(n, nt) <= kSymMaxPartialBytes;
 }
+
+__device__ __forceinline__ int64_t tile_slots_dev(int64_t ns, int w) { return (ns + w - 1) / w; }
 
 template <int KIND, int MODE, bool DUAL>
 __global__ void __launch_bounds__(kSymThreads) pair_sym_kernel(const SymArgs a) {
@@ -127,6 +137,10 @@ __global__ void __launch_bounds__(kSymThreads) pair_sym_kernel(const SymArgs a) 
 
   const int T = a.ntiles;
   const int64_t nsym = a.xt ? 0 : static_cast<int64_t>(T) * (T + 1) / 2;
+  // partial slots per tile (one per source tile, or per source sub-tile in
+  // the tile form) and the width of the item's source tile
+  const int src_w = (a.xt && a.sub == 2) ? kSymTile / 2 : kSymTile;
+  const int S = a.xt ? static_cast<int>(tile_slots_dev(a.n, src_w)) : T;
   const int64_t item = blockIdx.x;
   int I, J;
   if (item < nsym) {
@@ -140,11 +154,11 @@ __global__ void __launch_bounds__(kSymThreads) pair_sym_kernel(const SymArgs a) 
     J = I + static_cast<int>(item - start(I));
   } else {
     const int64_t e = item - nsym;
-    I = T + static_cast<int>(e / T);
-    J = static_cast<int>(e % T);
+    I = T + static_cast<int>(e / S);
+    J = static_cast<int>(e % S);
   }
   const bool extra = I >= T;  // a tile of targets that are not sources
-  const bool diag = (I == J);
+  const bool diag = !a.xt && (I == J);
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
 
   // this thread's targets (k = 0: tile slot tid, k = 1: tid + 64), with their
@@ -171,8 +185,8 @@ __global__ void __launch_bounds__(kSymThreads) pair_sym_kernel(const SymArgs a) 
     if (kGrp && tv[k]) tg[k] = a.grp[i];
   }
   // tile J's sources
-  const int64_t j0 = static_cast<int64_t>(J) * kSymTile;
-  const int cnt = static_cast<int>(min(static_cast<int64_t>(kSymTile), a.n - j0));
+  const int64_t j0 = static_cast<int64_t>(J) * src_w;
+  const int cnt = static_cast<int>(min(static_cast<int64_t>(src_w), a.n - j0));
 #pragma unroll
   for (int k = 0; k < 2; ++k) {
     const int s = tid + k * kSymThreads;
@@ -426,7 +440,7 @@ __global__ void __launch_bounds__(kSymThreads) pair_sym_kernel(const SymArgs a) 
       }
     }
     // tile I's partial from this item (slot J)
-    double *pi = part + (static_cast<int64_t>(I - a.tile0) * T + J) * slot_stride;
+    double *pi = part + (static_cast<int64_t>(I - a.tile0) * S + J) * slot_stride;
 #pragma unroll
     for (int k = 0; k < 2; ++k)
 #pragma unroll
@@ -436,7 +450,7 @@ __global__ void __launch_bounds__(kSymThreads) pair_sym_kernel(const SymArgs a) 
   __syncthreads();
   if (tid == 0) {
     int f = 0;
-    if (atomicAdd(&a.counters[I - a.tile0], 1u) == static_cast<unsigned>(T - 1)) f |= 1;
+    if (atomicAdd(&a.counters[I - a.tile0], 1u) == static_cast<unsigned>(S - 1)) f |= 1;
     if (!diag && !extra && atomicAdd(&a.counters[J], 1u) == static_cast<unsigned>(T - 1)) f |= 2;
     s_flags = f;
   }
@@ -457,13 +471,13 @@ __global__ void __launch_bounds__(kSymThreads) pair_sym_kernel(const SymArgs a) 
     for (int q = 0; q < ND; ++q) {
       const double2 *p =
           reinterpret_cast<const double2 *>((q == 0 ? a.partial : a.partial2) +
-                                            static_cast<int64_t>(X - a.tile0) * T * slot_stride);
+                                            static_cast<int64_t>(X - a.tile0) * S * slot_stride);
       double2 v[3];
 #pragma unroll
       for (int m = 0; m < 3; ++m) v[m] = make_double2(0.0, 0.0);
       constexpr int kPairsPerSlot = kSymTile * 3 / 2;
       int slot = 0;
-      for (; slot + 8 <= T; slot += 8) {
+      for (; slot + 8 <= S; slot += 8) {
         double2 r[8][3];
 #pragma unroll
         for (int u = 0; u < 8; ++u)
@@ -477,7 +491,7 @@ __global__ void __launch_bounds__(kSymThreads) pair_sym_kernel(const SymArgs a) 
             v[m].y += r[u][m].y;
           }
       }
-      for (; slot < T; ++slot)
+      for (; slot < S; ++slot)
 #pragma unroll
         for (int m = 0; m < 3; ++m) {
           const double2 r = __ldcg(p + slot * kPairsPerSlot + tid + m * kSymThreads);
@@ -515,8 +529,9 @@ static int sym_launch_one(const SymArgs &a, int *occupancy, cudaStream_t st) {
     return cudaOccupancyMaxActiveBlocksPerMultiprocessor(occupancy, kfn, kSymThreads, 0) == cudaSuccess
                ? F3D_OK
                : F3D_ERR_CUDA;
-  const int64_t items = (a.xt ? 0 : static_cast<int64_t>(a.ntiles) * (a.ntiles + 1) / 2) +
-                        static_cast<int64_t>(a.nextra) * a.ntiles;
+  const int64_t items = a.xt ? static_cast<int64_t>(a.nextra) * tile_slots(a.n, a.sub)
+                             : static_cast<int64_t>(a.ntiles) * (a.ntiles + 1) / 2 +
+                                   static_cast<int64_t>(a.nextra) * a.ntiles;
   kfn<<<static_cast<unsigned>(items), kSymThreads, 0, st>>>(a);
   return launch_status();
 }
@@ -573,7 +588,7 @@ int pair_sym_launch(int kernel, int self_mode, const double *x, const double *de
 int pair_tile_launch(int kernel, const double *xs, const double *dens, const double *nrm, const double *xt,
                      double *out, int64_t ns, int64_t nt, double eta, double reg, double eps, int accumulate,
                      double *partial, unsigned *counters, int *occupancy, cudaStream_t st, const double *dens2,
-                     double *out2, bool dual) {
+                     double *out2, bool dual, int sub) {
   SymArgs a{};
   a.x = xs;
   a.xt = xt;
@@ -583,13 +598,14 @@ int pair_tile_launch(int kernel, const double *xs, const double *dens, const dou
   a.out = out;
   a.out2 = out2;
   a.partial = partial;
-  a.partial2 = partial ? partial + tile_partial_bytes(ns, nt) / sizeof(double) : nullptr;
+  a.partial2 = partial ? partial + tile_partial_bytes(ns, nt, sub) / sizeof(double) : nullptr;
   a.counters = counters;
   a.n = ns;
   a.nt = nt;
   a.ntiles = static_cast<int>(sym_tiles(ns));
   a.nextra = static_cast<int>(sym_tiles(nt));
   a.tile0 = a.ntiles;
+  a.sub = sub == 2 ? 2 : 1;
   a.accumulate = accumulate ? 1 : 0;
   a.eps2 = eps * eps;
   a.reg2 = reg * reg;

@@ -98,10 +98,13 @@ typedef struct f3d_pair_shape {
                       symmetric kernel's target-side items: 128-point
                       tiles, two targets per thread, per-tile partials
                       summed in a fixed order): FP64 Oseen or stresslet,
-                      F3D_SELF_REGULARISE; workspace 3072 T T2 bytes,
-                      T = ceil(ns / 128) <= 1024, T2 = ceil(nt / 128),
-                      at most 2 GiB (twice for the two-density Oseen
-                      pass).                                                 */
+                      F3D_SELF_REGULARISE; nsplit 1 (or 0) or 2 takes
+                      the sources in tiles of 128 or 64 points (64:
+                      twice the items, for sums too small to fill the
+                      GPU); workspace 3072 S T2 bytes, S =
+                      ceil(ns / 128) or ceil(ns / 64), T2 = ceil(nt /
+                      128), ns <= 131072, at most 2 GiB (twice for the
+                      two-density Oseen pass).                              */
   int32_t nsplit;  /* source splits (grid.y); 0 = derive from the SM count    */
   int32_t use_tma; /* 0 or 1: stage full source tiles with cp.async.bulk
                       (default); -1: stage them with plain loads            */

@@ -205,6 +205,15 @@ def test_tile_shape_plan_checks(dll):
     for mode in (1, 2, 3):
         assert dll.f3d_pair_sum(0, 0, mode, None, None, None, None, None, None, None, 10, 10, 1.0, 5e-3, 1e-5, 0,
                                 ctypes.byref(shp), None, 0, None) == 5
+    # nsplit picks 128- or 64-point source tiles: the half tiles keep twice the partials
+    b1, b2 = ctypes.c_size_t(0), ctypes.c_size_t(0)
+    assert dll.f3d_pair_workspace_bytes(1, 0, 12000, 40960, ctypes.byref(_lib.PairShape(1, -2, 1, -1)),
+                                        ctypes.byref(b1)) == 0
+    assert dll.f3d_pair_workspace_bytes(1, 0, 12000, 40960, ctypes.byref(_lib.PairShape(1, -2, 2, -1)),
+                                        ctypes.byref(b2)) == 0
+    assert b2.value - 256 * 1024 == 2 * (b1.value - 256 * 1024) == 2 * 94 * 320 * 3072
+    assert dll.f3d_pair_workspace_bytes(1, 0, 100, 100, ctypes.byref(_lib.PairShape(1, -2, 3, -1)),
+                                        ctypes.byref(b1)) == 5
 
 
 def test_block3_gemv_argument_checks(dll):

@@ -616,12 +616,15 @@ def test_symmetric_rejects_other_sums(K, L):
 TILE = (1, -2, 0, -1)
 
 
+@pytest.mark.parametrize("sub", [0, 1, 2])
 @pytest.mark.parametrize("kind", ["oseen", "stresslet"])
 @pytest.mark.parametrize("ns,nt", [(1, 1), (127, 129), (128, 3), (1000, 257), (3000, 4097)])
-def test_tile_form_source_target(K, L, kind, ns, nt):
-    """The tile form of a source -> target sum (sl = -2) against the C oracle,
-    with a target on a source (coincident: regularised) and a sub-epsilon
-    pair (the careful redo); deterministic; accumulate adds to the output."""
+def test_tile_form_source_target(K, L, kind, ns, nt, sub):
+    """The tile form of a source -> target sum (sl = -2; nsplit 1 or 2:
+    128- or 64-point source tiles, 0: chosen from the size) against the C
+    oracle, with a target on a source (coincident: regularised) and a
+    sub-epsilon pair (the careful redo); deterministic; accumulate adds to
+    the output."""
     rng = np.random.default_rng(ns * 7 + nt)
     xs, xt = rng.random((ns, 3)) * 3, rng.random((nt, 3)) * 3
     if ns > 40 and nt > 40:
@@ -631,7 +634,7 @@ def test_tile_form_source_target(K, L, kind, ns, nt):
     n_arg = nr if kind == "stresslet" else None
     ref = pairs_c.pair_sum(kind, xs, xt, d, n_arg)
     s, t = torch.as_tensor(xs, device="cuda"), torch.as_tensor(xt, device="cuda")
-    shp = L.PairShape(*TILE)
+    shp = L.PairShape(1, -2, sub, -1)
     u = K.pair_sum(kind, s, t, d, n_arg, shape=shp)
     assert rel_err(u.cpu().numpy(), ref) < TOL64
     u2 = K.pair_sum(kind, s, t, d, n_arg, shape=shp)
@@ -652,14 +655,18 @@ def test_tile_form_config2_ball_targets(K, L):
     a = K.pair_sum("stresslet", s, t, q, normals, shape=L.PairShape(*TILE))
     b = K.pair_sum("stresslet", s, t, q, normals, shape=L.PairShape(1, 1, 0, 0))
     assert rel_err(a.cpu().numpy(), b.cpu().numpy()) < TOL64
+    for sub in (1, 2):
+        c = K.pair_sum("stresslet", s, t, q, normals, shape=L.PairShape(1, -2, sub, -1))
+        assert rel_err(c.cpu().numpy(), b.cpu().numpy()) < TOL64
     ref = pairs_c.pair_sum("stresslet", nodes, vol[:300], q, normals)
     assert rel_err(a.cpu().numpy()[:900], ref) < TOL64
     h = K.stresslet_kernel_source_target_numba(nodes, vol, normals, q, shape=L.PairShape(*TILE))
     assert np.array_equal(np.asarray(h).reshape(-1), a.cpu().numpy())
 
 
+@pytest.mark.parametrize("sub", [1, 2])
 @pytest.mark.parametrize("ns,nt", [(300, 700), (5000, 129)])
-def test_tile_form_oseen_dual_equals_two_sums(L, ns, nt):
+def test_tile_form_oseen_dual_equals_two_sums(L, ns, nt, sub):
     """The two-density Oseen pass in the tile form gives, bit for bit, the two
     tile-form sums it fuses."""
     import ctypes
@@ -668,7 +675,7 @@ def test_tile_form_oseen_dual_equals_two_sums(L, ns, nt):
     s = torch.tensor(rng.random((ns, 3)) * 4.0, device="cuda")
     t = torch.tensor(rng.random((nt, 3)) * 4.0, device="cuda")
     d1, d2 = (torch.tensor(rng.normal(size=(ns, 3)), device="cuda") for _ in range(2))
-    shp = L.PairShape(*TILE)
+    shp = L.PairShape(1, -2, sub, -1)
     r1 = K.pair_sum("oseen", s, t, d1, shape=shp).clone()
     r2 = K.pair_sum("oseen", s, t, d2, shape=shp).clone()
     nb = ctypes.c_size_t(0)
