@@ -26,12 +26,13 @@
 //
 // Per step: the pivot block is copied out and inverted (one CTA), the old
 // block row is copied to R, gj_panel_kernel forms W in place in the panel
-// columns (one CTA per 128-row tile), and gj_update_kernel updates every
-// other 128 x 128 tile: one persistent CTA per SM (256 threads with 8 x 8
-// FP64 accumulators each) walks its tiles with one continuous stream of
-// operand chunks (16 k, cp.async, double buffered, one barrier per chunk)
-// across tile boundaries; a tile's old values arrive by bulk copies during
-// its K loop (one mbarrier, bounded wait) and are added in its epilogue.
+// columns (one CTA per 128-row tile, 8 x 8 FP64 FMA accumulators per
+// thread), and gj_update_kernel updates every other 128 x 128 tile on the
+// FP64 tensor cores: one persistent CTA per SM (8 warps of 64 x 32 outputs,
+// mma.sync m16n8k16) walks its tiles with one continuous stream of operand
+// chunks (32 k, cp.async, a three-stage ring, one barrier per chunk) across
+// tile boundaries; a tile's old values are prefetched into L2 when its first
+// chunk is requested and added in its epilogue.
 #include <algorithm>
 #include <vector>
 
@@ -76,8 +77,7 @@ struct GjArgs {
   const double *Q;  // 128 x 128: inverse of the step's pivot block
   int64_t ld;
   int s;            // step: pivot block index
-  int *err;
-  uint64_t wait_ns;
+  int *err;         // the device error word (read by the host after the last step)
 };
 
 // Thread (tx, ty) owns rows 2ty + 32q + e and columns 2tx + 32q + e
@@ -402,7 +402,6 @@ int f3d_dense_inverse(double *A, int64_t n, int64_t ld, void *workspace, size_t 
   a.Q = Q;
   a.ld = ld;
   a.err = device_error_word();
-  a.wait_ns = wait_limit_ns();
   if (!a.err) return F3D_ERR_CUDA;
   const size_t row_bytes = static_cast<size_t>(ld) * sizeof(double);
   for (int s = 0; s < tiles; ++s) {
