@@ -18,14 +18,17 @@
 // After n steps the array holds (PA)^-1; swapping columns k and p_k for
 // k = n-1 .. 0 gives A^-1.
 //
-// One CTA per block holds the whole NMAX x NMAX matrix in registers: thread
-// t owns an 8 x 4 tile (rows 8*(t/(NMAX/4)) .., columns 4*(t%(NMAX/4)) ..),
-// so a warp covers whole rows.  Per step the owners of column k publish it to
+// Blocks of up to 32 rows (batched_inverse_kernel<32>): one CTA per block
+// holds the whole NMAX x NMAX matrix in registers, thread t an 8 x 4 tile
+// (rows 8*(t/(NMAX/4)) .., columns 4*(t%(NMAX/4)) ..), so a warp covers
+// whole rows.  Per step the owners of column k publish it to
 // shared memory (the pivot search is then done redundantly by every warp, no
 // extra barrier), the owners of rows k and p publish those rows, and every
 // thread applies the rank-1 sweep to its tile: two barriers per step.
 // Blocks smaller than NMAX are padded with the identity, which the sweeps
-// leave untouched.
+// leave untouched.  Blocks of 33..128 rows take the blocked form
+// (batched_inverse_tc_kernel): 16-column panels, no row exchanges, and the
+// rank-16 updates on the FP64 tensor cores.
 #include <algorithm>
 
 #include "f3d_common.cuh"
