@@ -27,7 +27,8 @@
 //     2, where every level-1 box neighbours every other, the 316 far
 //     offsets) and each term's 4n equivalent-density components; the kernel
 //     values are formed into shared memory for each K slice and reused by
-//     all 64 columns, on the FP64 FMA pipe.
+//     all 64 columns, the products on the FP64 tensor cores (mma.sync
+//     m16n8k16).
 //   * Near field (the 27 neighbour leaves, both kernels, coincident points
 //     excluded) and the local expansion's evaluation at the targets (L2P)
 //     run in one kernel per target leaf.
